@@ -1,0 +1,261 @@
+#!/usr/bin/env python
+"""Benchmark of the fully-coupled density-based step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload forward_step_2d|...]
+
+Metric: cell-iterations per second (cells x nonlinear iterations / s) of
+the implicit step (flux + residual, Roe Jacobian assembly, preconditioner
+set-up, Krylov solve, field update, time-step control) on one workload.
+`value` is device time of whole steps with the state resident in HBM
+(CUDA events on the library's stream); `e2e` is the same metric through
+the C ABI with the state copied host->device before and device->host
+after every step.  Multi-GPU runs are independent replicas (the path does
+not shard on one GPU's worth of mesh), one per rank, max time over ranks.
+
+The `reference` arm times the CPU restatement of the reference's step
+(the FP64 oracle; rhoDST itself needs foam-extend, absent on this box) on
+the same workload and configuration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+
+def workload(name: str):
+    from rhodst_b200 import cases
+    if name == "forward_step_2d":
+        c = cases.forward_step_c1()
+        desc = {"workload": "forward_step_2d", "mesh": "120x40 minus step, hex, one cell thick",
+                "cells": c.mesh.n_cells, "internal_faces": c.mesh.n_internal_faces,
+                "flux": "Kurganov", "reconstruction": "OSPRE/OSPREV", "ddt": "Euler, CFL 0.8 global dt",
+                "solver": "GMRES(20), 1 restart cycle", "preconditioner": "block Jacobi",
+                "precision": "fp64"}
+        return c, desc
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        smax = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# Algorithmic (compulsory) bytes per launch of each kernel class; S = bytes
+# per stored matrix scalar, Bk = N + 2F blocks, 4-byte column indices.
+def algorithmic_bytes(kind: str, N: int, F: int, S: int, precon: str) -> float:
+    Bk = N + 2 * F
+    if kind == "spmv":
+        return 25 * S * Bk + 4 * Bk + 40 * N + 40 * N
+    if kind == "precond":
+        if precon == "diagonal":
+            return 25 * S * N + 40 * N + 40 * N
+        return 25 * S * Bk + 4 * Bk + 3 * 40 * N
+    if kind == "flux":
+        # q (64 B) + gradient (192 B) per cell, 72 B geometry + 40 B flux per face
+        return 256 * N + 112 * F
+    if kind == "assemble":
+        return 25 * S * Bk + 4 * Bk + 104 * N + 72 * F
+    if kind == "factor":
+        return 2 * (25 * S * Bk + 4 * Bk) + 25 * S * N
+    return 0.0
+
+
+def run_ours(args, rank, world):
+    import torch
+    import rhodst_b200
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    case, desc = workload(args.workload)
+    opts = dict(case.options)
+    opts["profile"] = True
+    s = rhodst_b200.Solver(case.mesh, case.bcs, opts)
+    s.set_primitive(case.p, case.U, case.T)
+    N, F = case.mesh.n_cells, case.mesh.n_internal_faces
+    # L2 flush buffer (larger than the 126 MB L2), written on the library's stream
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB
+    for _ in range(args.warmup):
+        s.step(1)
+    stats0 = {k: s.kernel_stats(k) for k in ("spmv", "precond", "flux", "assemble", "factor", "orth", "update")}
+    launches0 = s.launch_count()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    step_ms = []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            s.step(1)                      # returns after its own stream synchronize
+            step_ms.append(s.last_step_ms())
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches = s.launch_count() - launches0
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * N * args.steps / (total_ms * 1e-3)
+    # dominant kernel class over the timed region -> roofline
+    stats = {k: tuple(np.subtract(s.kernel_stats(k), stats0[k])) for k in stats0}
+    dom = max(stats, key=lambda k: stats[k][1])
+    n_l, ms_l = stats[dom]
+    S = 8 if case.options.get("precision", "fp64") == "fp64" else (4 if case.options["precision"] == "fp32" else 2)
+    precon = case.options["solvers"]["W"]["preconditioner"]
+    peak, peak_kind = measured_peaks()
+    roof = None
+    if n_l > 0 and ms_l > 0:
+        by = algorithmic_bytes(dom, N, F, S, precon)
+        ach = by / (ms_l / n_l * 1e-3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
+                "bytes_per_launch": by, "launches": int(n_l), "avg_launch_us": round(ms_l / n_l * 1e3, 3),
+                "traffic": None,
+                "share_of_step": round(ms_l / max(total_ms, 1e-9), 4),
+                "note": "working set below L2 (126 MB): L2-resident bandwidth" if
+                        (25 * S * (N + 2 * F)) < 100e6 else "HBM-resident"}
+    # e2e through the C ABI with host buffers: H2D state, step, D2H state
+    rho, rhoU, rhoE = s.conservative()
+    e2e_steps = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.set_conservative(rho, rhoU, rhoE)
+        s.step(1)
+        rho, rhoU, rhoE = s.conservative()
+    e2e_t = time.perf_counter() - t0
+    e2e = {"value": world * N * e2e_steps / e2e_t, "unit": "cell-iter/s",
+           "h2d_bytes_per_step": int(rho.nbytes + rhoU.nbytes + rhoE.nbytes + 8 * 8 * N),
+           "d2h_bytes_per_step": int(rho.nbytes + rhoU.nbytes + rhoE.nbytes)}
+    line = {"metric": "cell_iterations_per_s", "value": value, "unit": "cell-iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (generated mesh, uniform Mach-3 inflow initial state)",
+            "config": dict(desc, l2="flushed: 256 MB written between timed steps",
+                           parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches), "roofline": roof}
+    return line, case
+
+
+def cpu_baseline(case, budget_s: float, steps_max: int, warmup: int = 1):
+    """The oracle (CPU restatement of the reference step, single thread) on
+    a bounded sample of the same workload."""
+    from tests.oracle_lib import OracleSolver
+    o = OracleSolver(case.mesh, case.bcs, case.options)
+    o.set_primitive(case.p, case.U, case.T)
+    o.step(warmup)
+    n = 0
+    t0 = time.perf_counter()
+    while n < steps_max and (time.perf_counter() - t0) < budget_s:
+        o.step(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    N = case.mesh.n_cells
+    return {"value": N * n / dt, "unit": "cell-iter/s", "cores": 1, "kind": "port",
+            "sample": f"{n} steps of the same workload after {warmup} warm-up step(s), {dt:.2f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="forward_step_2d")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        case, desc = workload(args.workload)
+        cb = cpu_baseline(case, budget_s=args.cpu_budget, steps_max=args.steps, warmup=min(args.warmup, 3))
+        line = {"impl": "reference", "metric": "cell_iterations_per_s", "value": cb["value"], "unit": "cell-iter/s",
+                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(desc, note="rhoDST needs foam-extend 4.1 (absent); CPU FP64 restatement timed"),
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    if world > 1:
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    line, case = run_ours(args, rank, world)
+    if rank == 0:
+        line["cpu_baseline"] = cpu_baseline(case, budget_s=args.cpu_budget, steps_max=1000, warmup=1)
+        print(json.dumps(line))
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

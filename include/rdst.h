@@ -1,0 +1,216 @@
+/*
+ * rdst.h -- C ABI of the B200 fully-coupled density-based step.
+ *
+ * This is the drop-in boundary for rhoDST's implicit step
+ * (libraries/finiteVolume/iteration/Single/Single.C:80-104 of rhoDST).  A
+ * foam-extend host (an `iteration` subclass selected as
+ * `timeIntegration GPU;`) marshals its fvMesh arrays and dictionary entries
+ * into the structs below and calls rdst_step() where Single::iterate ran:
+ *
+ *   rhoDSTFlux_.computeFluxDST()        -> flux + residual kernels
+ *   fvmDST::ddt(W) + fvmDST::fluxDST()  -> Jacobian/assembly kernels
+ *   Eqn.solve(true)                     -> block GMRES/BiCGStab kernels
+ *   #include "updateFields.H"           -> update kernel
+ *   turbulence_.correct()               -> Spalart-Allmaras kernels
+ *   runTime_.setCourantDST()            -> time-step kernels
+ *
+ * Plain C99: pointers and sizes only, no exceptions cross the ABI.  Host
+ * arrays are borrowed for the duration of a call.  All device memory is
+ * owned by the context and released by rdst_destroy().
+ *
+ * Array conventions follow foam's fvMesh:
+ *   faces [0, n_internal_faces) are internal (owner < neighbour),
+ *   faces [n_internal_faces, n_faces) are boundary faces grouped by patch;
+ *   vectors are AoS xyz triplets ("N x 3").
+ */
+#ifndef RDST_H
+#define RDST_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Mirrors the reference's FatalError exits
+ * (newbaseFluxDST.C:72-82, JacobianDST.C:80-89, newIteration.C:67-76) as
+ * RDST_ERR_CONFIG; the message is available from rdst_last_error(). */
+typedef enum rdst_status {
+    RDST_OK = 0,
+    RDST_ERR_CONFIG = 1,      /* unknown selector name / bad option value   */
+    RDST_ERR_MESH = 2,        /* inconsistent mesh arrays                   */
+    RDST_ERR_CUDA = 3,        /* CUDA runtime error                         */
+    RDST_ERR_DIVERGED = 4,    /* NaN or non-positive rho/p after an update  */
+    RDST_ERR_TIMEOUT = 5,     /* a bounded device wait gave up              */
+    RDST_ERR_UNSUPPORTED = 6, /* a reference option this path rejects       */
+    RDST_ERR_ARG = 7          /* null pointer / size out of range           */
+} rdst_status;
+
+/* Patch geometric type (foam polyPatch type). */
+enum {
+    RDST_PATCH_PATCH = 0,
+    RDST_PATCH_WALL = 1,
+    RDST_PATCH_SYMMETRY = 2,   /* symmetryPlane */
+    RDST_PATCH_EMPTY = 3       /* 2D front/back: carries no flux */
+};
+
+/* Boundary condition of one primitive field on one patch (foam
+ * fvPatchField type).  p and T use FIXED_VALUE/ZERO_GRADIENT/
+ * INLET_OUTLET/SYMMETRY/FARFIELD; U uses all of them (SLIP = symmetry
+ * treatment on a non-symmetry patch; FIXED_VALUE with 0 = no-slip wall). */
+enum {
+    RDST_BC_FIXED_VALUE = 0,
+    RDST_BC_ZERO_GRADIENT = 1,
+    RDST_BC_INLET_OUTLET = 2,
+    RDST_BC_SYMMETRY = 3,
+    RDST_BC_SLIP = 4,
+    RDST_BC_FARFIELD = 5       /* farField{Pressure,Velocity,Temperature}DST */
+};
+
+typedef struct rdst_patch {
+    int32_t start;             /* first face of the patch (foam face index) */
+    int32_t size;
+    int32_t type;              /* RDST_PATCH_*                               */
+    int32_t bc_p, bc_U, bc_T;  /* RDST_BC_* per primitive field              */
+    double p_value;            /* fixedValue / inletValue / far-field p_inf  */
+    double U_value[3];
+    double T_value;
+    double nuTilda_value;      /* SA: fixed/inlet value of nuTilda           */
+} rdst_patch;
+
+typedef struct rdst_mesh {
+    int32_t n_cells;
+    int32_t n_internal_faces;
+    int32_t n_faces;            /* internal + boundary                        */
+    int32_t n_patches;
+    const int32_t* owner;       /* [n_faces]                                  */
+    const int32_t* neighbour;   /* [n_internal_faces]                         */
+    const double* Sf;           /* [n_faces*3] face area vectors              */
+    const double* Cf;           /* [n_faces*3] face centres                   */
+    const double* magSf;        /* [n_faces]                                  */
+    const double* weights;      /* [n_faces] linear interpolation weights     */
+    const double* deltaCoeffs;  /* [n_faces]                                  */
+    const double* C;            /* [n_cells*3] cell centres                   */
+    const double* V;            /* [n_cells]   cell volumes                   */
+    const rdst_patch* patches;  /* [n_patches]                                */
+    const double* wall_distance;/* [n_cells] or NULL (needed by SA models)    */
+} rdst_mesh;
+
+/* Per-step report (the reference's Info output + residual history). */
+typedef struct rdst_step_report {
+    double time;               /* physical time after the step               */
+    double deltaT;             /* physical time step used by the step        */
+    double courant;            /* global Courant (transient) / mean (steady) */
+    double res_l2[5];          /* ||R_k * V||_2 over cells, k = rho..rhoE    */
+    double res_mag;            /* sqrt(sum_cells |R|^2): the CFL-ramp norm
+                                  of timeDST::setCourantDST (timeDST.C:330)  */
+    double lin_initial[5];     /* linear solver initial residual (normalised)*/
+    double lin_final[5];       /* linear solver final residual               */
+    int32_t lin_iterations;    /* GMRES restarts / BiCGStab iterations       */
+    int32_t flags;             /* bit0: field bounding was active            */
+    double rdt_min, rdt_max;   /* min/max of the local 1/dtau                */
+    double t_flux_ms, t_jacobian_ms, t_precond_ms, t_krylov_ms, t_update_ms;
+} rdst_step_report;
+
+typedef struct rdst_ctx rdst_ctx;
+
+/* Create a context.  `keys`/`values` are the dictionary entries that select
+ * the path, with foam's names (dotted for sub-dictionaries), e.g.
+ *   "fluxScheme" "Kurganov"          (rhoDSTDict; newbaseFluxDST.C:64-84)
+ *   "Jacobian" "Roe"                 (rhoDSTDict; JacobianDST.C:72-91)
+ *   "timeIntegration.timeIntegration" "Single"
+ *   "timeControls.neighbouring" "true" ...
+ *   "ddtSchemes.default" "Euler" | "steadyStateDST"
+ *   "interpolationSchemes.reconstruct(rho)" "OSPRE"
+ *   "solvers.W.solver" "GMRES" | "BiCGStab"
+ *   "solvers.W.preconditioner" "ILUC0" | "diagonal" | "none"
+ *   "fieldBounds.p" "0.001 10000"
+ *   "thermo.R" / "thermo.Cp" / "transport.mu" / "transport.Pr" ...
+ * Unknown selector values return RDST_ERR_CONFIG; reference options this
+ * path rejects (directWaveSpeed false, AMG, dual2ndDST) RDST_ERR_UNSUPPORTED.
+ * Replaces createFields.H:115-152 (flux, Jacobian and iteration selection)
+ * and timeDST::initialize (timeDST.C:67-208). */
+rdst_status rdst_create(const rdst_mesh* mesh, int32_t n_options,
+                        const char* const* keys, const char* const* values,
+                        rdst_ctx** out);
+
+/* Initial state from primitive fields (createFields.H:21-72):
+ * rho = p psi, rhoU = rho U, rhoE = rho (h Cv/Cp + |U|^2/2).
+ * nuTilda may be NULL for laminar runs. */
+rdst_status rdst_set_primitive(rdst_ctx* ctx, const double* p, const double* U,
+                               const double* T, const double* nuTilda);
+
+/* Conservative state in and out (geometricFieldDST::set / retrieve).  The
+ * first state set on a context also initialises the time control
+ * (timeDST::initialize); later calls replace the fields only and keep the
+ * Courant history, like foam fields written between time steps. */
+rdst_status rdst_set_conservative(rdst_ctx* ctx, const double* rho,
+                                  const double* rhoU, const double* rhoE);
+rdst_status rdst_get_conservative(rdst_ctx* ctx, double* rho, double* rhoU,
+                                  double* rhoE);
+rdst_status rdst_get_primitive(rdst_ctx* ctx, double* p, double* U, double* T,
+                               double* nuTilda);
+
+/* Advance n_steps implicit steps (Single::iterate, Single.C:80-104).
+ * `reports` may be NULL or hold n_steps entries. */
+rdst_status rdst_step(rdst_ctx* ctx, int32_t n_steps, rdst_step_report* reports);
+
+/* Evaluate the residual R(W) of the current state (computeFluxDST +
+ * calcFields, baseFluxDST.C:223-255): out[n_cells*5], per unit volume,
+ * components (rho, rhoU_x, rhoU_y, rhoU_z, rhoE). */
+rdst_status rdst_residual(rdst_ctx* ctx, double* out);
+
+/* Assemble the block system of the current state without solving and copy
+ * it out in foam's LDU layout (fluxDST.C:73-127 + fvmDST.C:77-143):
+ * diag[n_cells*25], upper[n_internal_faces*25] (row owner, column
+ * neighbour), lower[n_internal_faces*25], source[n_cells*5]; each 5x5 block
+ * row-major.  Any pointer may be NULL. */
+rdst_status rdst_assemble(rdst_ctx* ctx, double* diag, double* upper,
+                          double* lower, double* source);
+
+/* Pressure (+ viscous) force on one patch, projected on the lift and drag
+ * directions and normalised by (q_inf * A_ref): the forceCoeffs function
+ * object used by the reference's RAE2822 / oneraM6Turb cases.
+ * out[0] = C_l, out[1] = C_d, out[2] = C_m about `cofr` around `pitch_axis`. */
+rdst_status rdst_forces(rdst_ctx* ctx, int32_t patch, const double lift_dir[3],
+                        const double drag_dir[3], const double cofr[3],
+                        const double pitch_axis[3], double p_ref,
+                        double q_ref_times_area, double l_ref, double out[3]);
+
+/* Message of the last failing call on this context ("" if none). */
+const char* rdst_last_error(const rdst_ctx* ctx);
+
+/* Release the context and all its device memory. */
+void rdst_destroy(rdst_ctx* ctx);
+
+/* Host-only helper (no GPU needed): recursive coordinate bisection of the
+ * cell centres into n_parts parts, out_part[n_cells].  The GPU library uses
+ * the same partition for its subdomain ILU(0) (block-Jacobi across parts,
+ * as foam-extend's ILUC0 behaves across processor patches). */
+rdst_status rdst_partition_cells(int32_t n_cells, const double* C,
+                                 int32_t n_parts, int32_t* out_part);
+
+/* Instrumentation (no reference counterpart).
+ * rdst_stream: the CUDA stream (cudaStream_t) all of the context's kernels
+ * run on, so a caller can record its own events around rdst_step.
+ * rdst_launch_count: kernels launched by this context so far.
+ * rdst_last_step_ms: device time of the last rdst_step call, from CUDA
+ * events recorded on the context's stream at entry and after its last
+ * kernel.
+ * rdst_kernel_stats: with the option "profile" "true", the library records
+ * CUDA events around every launch of the named kernel class inside
+ * rdst_step ("spmv", "precond", "flux", "assemble", "factor", "orth",
+ * "update") and returns its launch count and summed device time. */
+void* rdst_stream(rdst_ctx* ctx);
+int64_t rdst_launch_count(const rdst_ctx* ctx);
+double rdst_last_step_ms(const rdst_ctx* ctx);
+rdst_status rdst_kernel_stats(rdst_ctx* ctx, const char* kernel, int64_t* launches, double* total_ms);
+
+/* Library identification (e.g. "rdst-b200 sm_100a"). */
+const char* rdst_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RDST_H */

@@ -1,0 +1,134 @@
+"""Case definitions: mesh + boundary conditions + dictionary entries +
+initial fields for the workloads the step is exercised and measured on.
+
+Each builder returns a :class:`Case`; the dictionaries use the reference's
+key names (system/rhoDSTDict, fvSchemes, fvSolution, fieldBounds and
+constant/thermophysicalProperties of the rhoDST tutorials).
+"""
+from __future__ import annotations
+
+import copy
+import dataclasses
+import math
+from typing import Any, Dict, Optional
+
+import numpy as np
+
+from . import mesh as _mesh
+
+# normalisedGas of tutorials/forwardStep/constant/thermophysicalProperties:
+# "normalisedGas 1 11640.3 2.5 0 0 1" -> molWeight 11640.3, Cp 2.5, mu 0, Pr 1
+R_UNIVERSAL = 8314.47
+NORMALISED_GAS = {"R": R_UNIVERSAL / 11640.3, "Cp": 2.5}
+# air (RAE2822 tutorial thermophysicalProperties: molWeight 28.9, Cp 1005,
+# Sutherland As 1.458e-6, Ts 110.4, Pr 0.72)
+AIR = {"R": R_UNIVERSAL / 28.9, "Cp": 1005.0}
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    mesh: _mesh.PolyMesh
+    bcs: Dict[str, Dict[str, Any]]
+    options: Dict[str, Any]
+    p: np.ndarray
+    U: np.ndarray
+    T: np.ndarray
+    nuTilda: Optional[np.ndarray] = None
+    steps: int = 1
+    force_patch: Optional[str] = None
+    force_dirs: Optional[Dict[str, Any]] = None
+
+    def with_options(self, **updates) -> "Case":
+        c = copy.copy(self)
+        o = copy.deepcopy(self.options)
+        for k, v in updates.items():
+            _set_dotted(o, k, v)
+        c.options = o
+        return c
+
+
+def _set_dotted(d: dict, key: str, value) -> None:
+    parts = key.split(".")
+    for p in parts[:-1]:
+        d = d.setdefault(p, {})
+    d[parts[-1]] = value
+
+
+def forward_step_c1(refine: int = 1, solver: str = "GMRES", preconditioner: str = "diagonal",
+                    n_directions: int = 20, max_iter: int = 1) -> Case:
+    """2D inviscid Mach-3 forward-facing step (120x40 minus the step = 4032
+    cells at refine=1): Kurganov flux, OSPRE/OSPREV reconstruction, Euler
+    implicit step at a fixed global CFL 0.8 (global dt from the
+    neighbouring face definition), block-GMRES(20) with block-Jacobi, one
+    restart cycle per step.  BCs follow tutorials/forwardStep/0/{p,U,T}."""
+    m = _mesh.forward_step_2d(refine)
+    U0 = (3.0, 0.0, 0.0)
+    bcs = {
+        "inlet": {"p": ("fixedValue", 1.0), "U": ("fixedValue", U0), "T": ("fixedValue", 1.0)},
+        "outlet": {"p": "zeroGradient", "U": ("inletOutlet", U0), "T": ("inletOutlet", 1.0)},
+        "bottom": {"p": "symmetryPlane", "U": "symmetryPlane", "T": "symmetryPlane"},
+        "top": {"p": "symmetryPlane", "U": "symmetryPlane", "T": "symmetryPlane"},
+        "obstacle": {"p": "zeroGradient", "U": "slip", "T": "zeroGradient"},
+    }
+    options = {
+        "fluxScheme": "Kurganov",
+        "Jacobian": "Roe",
+        "timeIntegration": {"timeIntegration": "Single"},
+        "timeControls": {"adjustTimeStep": True, "neighbouring": True,
+                         "initialCo": 0.8, "minCo": 0.8, "maxCo": 0.8},
+        "ddtSchemes": {"default": "Euler"},
+        "interpolationSchemes": {"reconstruct(rho)": "OSPRE", "reconstruct(U)": "OSPREV",
+                                 "reconstruct(T)": "OSPRE"},
+        "solvers": {"W": {"solver": solver, "preconditioner": preconditioner,
+                          "nDirections": n_directions, "tolerance": 1e-14, "relTol": 0.0,
+                          "maxIter": max_iter, "minIter": 1}},
+        "fieldBounds": {"rho": (0.001, 10000.0), "p": (0.001, 10000.0), "T": (0.001, 10000.0)},
+        "thermo": dict(NORMALISED_GAS),
+    }
+    N = m.n_cells
+    return Case("forwardStep2D", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N),
+                steps=1000)
+
+
+def farfield_state(mach: float, alpha_deg: float, T_inf: float, p_inf: float, gas: dict):
+    g = gas["Cp"] / (gas["Cp"] - gas["R"])
+    a = math.sqrt(g * gas["R"] * T_inf)
+    al = math.radians(alpha_deg)
+    U = (mach * a * math.cos(al), mach * a * math.sin(al), 0.0)
+    return U
+
+
+def naca0012_inviscid(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: float = 2.3,
+                      flux: str = "AUSM+up", limiter: str = "Venkatakrishnan",
+                      n_directions: int = 30, preconditioner: str = "ILUC0") -> Case:
+    """NACA0012 C-mesh with characteristic far field, Euler equations,
+    local time stepping at CFL 50 (steadyStateDST), block-GMRES(30) with
+    block ILU(0).  The inviscid counterpart of the turbulent airfoil case
+    (same mesh, flow angle and Mach number)."""
+    m = _mesh.naca_cmesh(ni, nj)
+    gas = dict(NORMALISED_GAS)
+    U0 = farfield_state(mach, alpha, 1.0, 1.0, gas)
+    bcs = {
+        "airfoil": {"p": "zeroGradient", "U": "slip", "T": "zeroGradient"},
+        "farfield": {"p": ("farField", 1.0), "U": ("farField", U0), "T": ("farField", 1.0)},
+    }
+    vlim = "Venkatakrishnan" if limiter == "Venkatakrishnan" else limiter + "V"
+    options = {
+        "fluxScheme": flux,
+        "Jacobian": "Roe",
+        "timeControls": {"neighbouring": False, "initialCo": 50.0, "minCo": 0.1, "maxCo": 50.0},
+        "ddtSchemes": {"default": "steadyStateDST"},
+        "interpolationSchemes": {"reconstruct(rho)": limiter, "reconstruct(U)": vlim,
+                                 "reconstruct(T)": limiter},
+        "solvers": {"W": {"solver": "GMRES", "preconditioner": preconditioner,
+                          "nDirections": n_directions, "tolerance": 1e-12, "relTol": 0.0,
+                          "maxIter": 1, "minIter": 1}},
+        "fieldBounds": {"rho": (1e-3, 1e4), "p": (1e-3, 1e4), "T": (1e-3, 1e4)},
+        "thermo": gas,
+    }
+    N = m.n_cells
+    al = math.radians(alpha)
+    return Case("naca0012", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N), steps=2000,
+                force_patch="airfoil",
+                force_dirs={"lift": (-math.sin(al), math.cos(al), 0.0), "drag": (math.cos(al), math.sin(al), 0.0)})

@@ -1,0 +1,745 @@
+// kernels.cuh -- sm_100a kernels of the fully-coupled density-based step.
+//
+// Every kernel is a gather (one thread per cell / face / matrix row) with a
+// fixed, face-ordered accumulation order: no floating-point atomics, so
+// results are bitwise reproducible run to run.  The path is HBM/L2 bound
+// (no dense contraction), so none of it uses tensor cores; the levers are
+// coalesced SoA/entry-interleaved layouts, fused per-face arithmetic and
+// single-pass reductions.
+#pragma once
+
+#include "physics.cuh"
+#include "rdst_internal.h"
+
+namespace rdst {
+
+constexpr int TPB = 256;
+
+__device__ __forceinline__ V3 ldv3(const double* a, int n, int i) { return mk(a[i], a[n + i], a[2 * n + i]); }
+
+// ------------------------------------------------------------------ reductions
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+// block-wide sum in a fixed order; result valid in thread 0
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[32];
+    v = warp_sum(v);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+    if (wid == 0) v = warp_sum(v);
+    return v;
+}
+__device__ __forceinline__ double block_min(double v) {
+    __shared__ double sh[32];
+    v = warp_min(v);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? sh[threadIdx.x] : 1e300;
+    if (wid == 0) v = warp_min(v);
+    return v;
+}
+__device__ __forceinline__ double block_max(double v) {
+    __shared__ double sh[32];
+    v = warp_max(v);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? sh[threadIdx.x] : -1e300;
+    if (wid == 0) v = warp_max(v);
+    return v;
+}
+
+// ------------------------------------------------------------------ state / BCs
+struct Bounds { double rho_min, rho_max, p_min, p_max, T_min, T_max; };
+
+// initial state from primitives (createFields.H:21-72)
+__global__ void k_init_state(int N, Thermo th, const double* __restrict__ prim, double* __restrict__ W) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double* P = prim + PW * i;
+    double p = P[0], T = P[1], h = P[2];
+    V3 U = mk(P[3], P[4], P[5]);
+    double rho = p / (th.R * T);
+    W[5 * i + 0] = rho;
+    W[5 * i + 1] = rho * U.x;
+    W[5 * i + 2] = rho * U.y;
+    W[5 * i + 3] = rho * U.z;
+    W[5 * i + 4] = rho * (h * th.Cv / th.Cp + 0.5 * magSqr3(U));
+}
+
+// boundary mass flux before the first flux evaluation: (rho U)_owner . Sf
+__global__ void k_init_phib(DevMesh m, const double* __restrict__ W, double* __restrict__ bs) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.NB) return;
+    int c = m.bcell[b];
+    V3 S = ldv3(m.bSf, m.NB, b);
+    bs[BW * b + 7] = dot3(mk(W[5 * c + 1], W[5 * c + 2], W[5 * c + 3]), S);
+}
+
+// Boundary values of p, U, T from the internal field (fixedValue,
+// zeroGradient, inletOutlet, symmetryPlane/slip, characteristic far field)
+// and rho/rhoU/rhoE rebuilt as updateFields.H:84-93.
+__global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __restrict__ prim, double* __restrict__ bs) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.NB) return;
+    const DevPatch P = m.patches[m.bpatch[b]];
+    const int ci = m.bcell[b];
+    V3 S = ldv3(m.bSf, m.NB, b);
+    double magS = m.bmagSf[b];
+    V3 n = div3(S, magS);
+    const double* Pi = prim + PW * ci;
+    double pI = Pi[0], TI = Pi[1];
+    V3 Ui = mk(Pi[3], Pi[4], Pi[5]);
+    bool outflow = bs[BW * b + 7] >= 0.0;
+    double pb, Tb;
+    V3 Ub;
+    switch (P.bc_p) {
+        case 0: pb = P.p_value; break;
+        case 2: pb = outflow ? pI : P.p_value; break;
+        default: pb = pI; break;
+    }
+    switch (P.bc_T) {
+        case 0: Tb = P.T_value; break;
+        case 2: Tb = outflow ? TI : P.T_value; break;
+        default: Tb = TI; break;
+    }
+    switch (P.bc_U) {
+        case 0: Ub = mk(P.U_value[0], P.U_value[1], P.U_value[2]); break;
+        case 2: Ub = outflow ? Ui : mk(P.U_value[0], P.U_value[1], P.U_value[2]); break;
+        case 3:
+        case 4: Ub = sub3(Ui, scl3(dot3(n, Ui), n)); break;
+        default: Ub = Ui; break;
+    }
+    pb = fmin(fmax(pb, bd.p_min), bd.p_max);
+    double hb = th.Cp * Tb;
+    double psib = 1.0 / (th.R * Tb);
+    double rhob = pb * psib;
+    double* B = bs + BW * b;
+    B[0] = rhob;
+    B[1] = rhob * Ub.x;
+    B[2] = rhob * Ub.y;
+    B[3] = rhob * Ub.z;
+    B[4] = rhob * (hb + 0.5 * magSqr3(Ub)) - pb;
+    B[5] = pb;
+    B[6] = Tb;
+}
+
+// ------------------------------------------------------------------ residual
+// Reconstruction record per cell (and per boundary face):
+// q = (rho, rhoU xyz, rPsi = RT, e = h - p/rho, s) with s = c = sqrt(gamma RT)
+// (Kurganov, AUSM) or the critical speed sqrt(2(g-1)/(g+1) H) (HLL family,
+// AUSM+, AUSM+up; HLLDST.C:130-137).
+__global__ void k_recon(DevMesh m, Thermo th, int use_c, const double* __restrict__ W, const double* __restrict__ prim,
+                        const double* __restrict__ bs, double* __restrict__ q, double* __restrict__ qb) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double g = th.gamma;
+    if (i < m.N) {
+        const double* w5 = W + 5 * i;
+        const double* P = prim + PW * i;
+        double rho = w5[0], rhoE = w5[4], p = P[0], T = P[1], h = P[2];
+        double rPsi = th.R * T;
+        double s;
+        if (use_c) s = sqrt(g * rPsi);
+        else {
+            double H = fmax(rhoE / rho, D_SMALL) + fmax(p / rho, D_SMALL);
+            s = sqrt(2.0 * (g - 1.0) / (g + 1.0) * H);
+        }
+        double* o = q + QW * i;
+        o[0] = rho; o[1] = w5[1]; o[2] = w5[2]; o[3] = w5[3];
+        o[4] = rPsi; o[5] = h - p / rho; o[6] = s; o[7] = 0.0;
+    } else if (i < m.N + m.NB) {
+        int b = i - m.N;
+        const double* B = bs + BW * b;
+        double rho = B[0], rhoE = B[4], p = B[5], T = B[6];
+        double h = th.Cp * T;
+        double rPsi = th.R * T;
+        double s;
+        if (use_c) s = sqrt(g * rPsi);
+        else {
+            double H = fmax(rhoE / rho, D_SMALL) + fmax(p / rho, D_SMALL);
+            s = sqrt(2.0 * (g - 1.0) / (g + 1.0) * H);
+        }
+        double* o = qb + QW * b;
+        o[0] = rho; o[1] = B[1]; o[2] = B[2]; o[3] = B[3];
+        o[4] = rPsi; o[5] = h - p / rho; o[6] = s; o[7] = 0.0;
+    }
+}
+
+// Gauss linear gradient of the 7 recon fields (cell gather over the faces
+// in foam order), plus optionally the Venkatakrishnan limiter per field and
+// the HLLCP pressure-ratio sensor fCells (HLLCPDST.C:131-164).
+__global__ void __launch_bounds__(128) k_grad(DevMesh m, int venkat_mask, double venkat_K, const double* __restrict__ q,
+                                              const double* __restrict__ qb, const double* __restrict__ prim,
+                                              double* __restrict__ g, double* __restrict__ psi,
+                                              double* __restrict__ fcell, int hllcp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.N) return;
+    double acc[21];
+#pragma unroll
+    for (int k = 0; k < 21; ++k) acc[k] = 0.0;
+    const int k0 = m.cf_start[i], k1 = m.cf_start[i + 1];
+    double fmin_c = 1.0;
+    const double pi = prim[PW * i];
+    for (int k = k0; k < k1; ++k) {
+        int code = m.cf_list[k];
+        if (code < m.Fi) {
+            int f = code, o = m.own[f], n = m.nei[f];
+            double wf = m.w[f];
+            V3 S = ldv3(m.Sf, m.Fi, f);
+            const double* qo = q + QW * o;
+            const double* qn = q + QW * n;
+            if (o == i) {
+#pragma unroll
+                for (int j = 0; j < 7; ++j) {
+                    double xf = wf * qo[j] + (1 - wf) * qn[j];
+                    acc[3 * j] += xf * S.x; acc[3 * j + 1] += xf * S.y; acc[3 * j + 2] += xf * S.z;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 7; ++j) {
+                    double xf = wf * qo[j] + (1 - wf) * qn[j];
+                    acc[3 * j] -= xf * S.x; acc[3 * j + 1] -= xf * S.y; acc[3 * j + 2] -= xf * S.z;
+                }
+            }
+            if (hllcp) {
+                double pk = prim[PW * (o == i ? n : o)];
+                fmin_c = fmin(fmin_c, fmin(pi / pk, pk / pi));
+            }
+        } else {
+            int b = code - m.Fi;
+            V3 S = ldv3(m.bSf, m.NB, b);
+            const double* qq = qb + QW * b;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) {
+                double xf = qq[j];
+                acc[3 * j] += xf * S.x; acc[3 * j + 1] += xf * S.y; acc[3 * j + 2] += xf * S.z;
+            }
+        }
+    }
+    const double Vi = m.V[i];
+    double* go = g + GW * i;
+#pragma unroll
+    for (int k = 0; k < 21; ++k) { acc[k] /= Vi; go[k] = acc[k]; }
+    if (hllcp) fcell[i] = fmin_c;
+    if (venkat_mask) {
+        // Venkatakrishnan (1995): psi = min_f phi(dmax|dmin, d2), eps^2 = (K h)^3
+        const double* qi = q + QW * i;
+        double eps2 = pow(venkat_K * cbrt(Vi), 3.0);
+        V3 Ci = ldv3(m.C, m.N, i);
+        for (int j = 0; j < 7; ++j) {
+            if (!((venkat_mask >> j) & 1)) { psi[QW * i + j] = 1.0; continue; }
+            double x = qi[j], mx = x, mn = x;
+            for (int k = k0; k < k1; ++k) {
+                int code = m.cf_list[k];
+                double xo;
+                if (code < m.Fi) { int o = m.own[code]; xo = q[QW * (o == i ? m.nei[code] : o) + j]; }
+                else xo = qb[QW * (code - m.Fi) + j];
+                mx = fmax(mx, xo); mn = fmin(mn, xo);
+            }
+            double dmax = mx - x, dmin = mn - x, p = 1.0;
+            V3 gj = mk(acc[3 * j], acc[3 * j + 1], acc[3 * j + 2]);
+            for (int k = k0; k < k1; ++k) {
+                int code = m.cf_list[k];
+                V3 Cf = code < m.Fi ? ldv3(m.Cf, m.Fi, code) : ldv3(m.bCf, m.NB, code - m.Fi);
+                double d2 = dot3(gj, sub3(Cf, Ci));
+                double ph;
+                if (d2 > 0) ph = ((dmax * dmax + eps2) * d2 + 2 * d2 * d2 * dmax) / (dmax * dmax + 2 * d2 * d2 + dmax * d2 + eps2) / d2;
+                else if (d2 < 0) ph = ((dmin * dmin + eps2) * d2 + 2 * d2 * d2 * dmin) / (dmin * dmin + 2 * d2 * d2 + dmin * d2 + eps2) / d2;
+                else ph = 1.0;
+                p = fmin(p, ph);
+            }
+            psi[QW * i + j] = p;
+        }
+    }
+}
+
+// scalar limited reconstruction to the owner (xo) and neighbour (xn) sides
+__device__ __forceinline__ void recon_scalar(int L, double xP, double xN, V3 gP, V3 gN, V3 d, double w,
+                                             double& xo, double& xn) {
+    double ro = 0, rn = 0;
+    if (L != L_LINEAR && L != L_UPWIND) {
+        double gradf = xN - xP;
+        ro = nvd_r(dot3(d, gP), gradf);
+        rn = nvd_r(dot3(d, gN), gradf);
+    }
+    double wo = side_w(L, true, w, ro), wn = side_w(L, false, w, rn);
+    xo = wo * xP + (1 - wo) * xN;
+    xn = wn * xP + (1 - wn) * xN;
+}
+
+// Face fluxes of all internal faces (reconstruction + scheme), AoS output.
+__global__ void __launch_bounds__(128) k_face_flux(DevMesh m, Thermo th, int scheme, int lr, int lu, int lt,
+                                                   int lowMach, double Mainf, const double* __restrict__ q,
+                                                   const double* __restrict__ g, const double* __restrict__ psi,
+                                                   const double* __restrict__ fcell, double* __restrict__ fl) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.Fi) return;
+    const int o = m.own[f], n = m.nei[f];
+    const double wf = m.w[f];
+    const V3 S = ldv3(m.Sf, m.Fi, f);
+    const double magS = m.magSf[f];
+    const double* qo = q + QW * o;
+    const double* qn = q + QW * n;
+    SideState so, sn;
+    const int Ls[7] = {lr, lu, lu, lu, lt, lt, lt};
+    if (lr == L_VENKAT || lu == L_VENKAT || lt == L_VENKAT) {
+        // all fields Venkatakrishnan-limited or linear/upwind (parse enforces a
+        // single family per case)
+        V3 Cf = ldv3(m.Cf, m.Fi, f);
+        V3 dP = sub3(Cf, ldv3(m.C, m.N, o)), dN = sub3(Cf, ldv3(m.C, m.N, n));
+        double xo[7], xn[7];
+        for (int j = 0; j < 7; ++j) {
+            if (Ls[j] == L_VENKAT) {
+                const double* gP = g + GW * o + 3 * j;
+                const double* gN = g + GW * n + 3 * j;
+                xo[j] = qo[j] + psi[QW * o + j] * (dP.x * gP[0] + dP.y * gP[1] + dP.z * gP[2]);
+                xn[j] = qn[j] + psi[QW * n + j] * (dN.x * gN[0] + dN.y * gN[1] + dN.z * gN[2]);
+            } else {
+                recon_scalar(Ls[j], qo[j], qn[j], mk(0, 0, 0), mk(0, 0, 0), mk(0, 0, 0), wf, xo[j], xn[j]);
+            }
+        }
+        so.rho = xo[0]; so.rhoU = mk(xo[1], xo[2], xo[3]); so.rPsi = xo[4]; so.e = xo[5]; so.s = xo[6];
+        sn.rho = xn[0]; sn.rhoU = mk(xn[1], xn[2], xn[3]); sn.rPsi = xn[4]; sn.e = xn[5]; sn.s = xn[6];
+    } else {
+        const V3 d = ldv3(m.d, m.Fi, f);
+        const bool lim = (lr > L_UPWIND) || (lu > L_UPWIND) || (lt > L_UPWIND);
+        const double* gP = g + GW * o;
+        const double* gN = g + GW * n;
+        auto GV = [&](const double* gg, int j) { return lim ? mk(gg[3 * j], gg[3 * j + 1], gg[3 * j + 2]) : mk(0, 0, 0); };
+        recon_scalar(lr, qo[0], qn[0], GV(gP, 0), GV(gN, 0), d, wf, so.rho, sn.rho);
+        recon_scalar(lt, qo[4], qn[4], GV(gP, 4), GV(gN, 4), d, wf, so.rPsi, sn.rPsi);
+        recon_scalar(lt, qo[5], qn[5], GV(gP, 5), GV(gN, 5), d, wf, so.e, sn.e);
+        recon_scalar(lt, qo[6], qn[6], GV(gP, 6), GV(gN, 6), d, wf, so.s, sn.s);
+        // rhoU with the vector (V) limiter: r from the projection on phi_N - phi_P
+        double ro = 0, rn = 0;
+        V3 xP = mk(qo[1], qo[2], qo[3]), xN = mk(qn[1], qn[2], qn[3]);
+        if (lu > L_UPWIND) {
+            V3 gradfV = sub3(xN, xP);
+            double gradf = dot3(gradfV, gradfV);
+            // (d . grad U)_j = sum_i d_i dU_j/dx_i ; field j = 1+comp, direction i
+            V3 dgP = mk(d.x * gP[3] + d.y * gP[4] + d.z * gP[5], d.x * gP[6] + d.y * gP[7] + d.z * gP[8],
+                        d.x * gP[9] + d.y * gP[10] + d.z * gP[11]);
+            V3 dgN = mk(d.x * gN[3] + d.y * gN[4] + d.z * gN[5], d.x * gN[6] + d.y * gN[7] + d.z * gN[8],
+                        d.x * gN[9] + d.y * gN[10] + d.z * gN[11]);
+            ro = nvd_r(dot3(gradfV, dgP), gradf);
+            rn = nvd_r(dot3(gradfV, dgN), gradf);
+        }
+        double wo = side_w(lu, true, wf, ro), wn = side_w(lu, false, wf, rn);
+        so.rhoU = add3(scl3(wo, xP), scl3(1 - wo, xN));
+        sn.rhoU = add3(scl3(wn, xP), scl3(1 - wn, xN));
+    }
+    double fs = 1.0;
+    if (scheme == F_HLLCP) fs = wf * pow(fcell[o], 3.0) + (1 - wf) * pow(fcell[n], 3.0);
+    FFlux F = face_flux(scheme, so, sn, S, magS, th.gamma, fs, lowMach != 0, Mainf);
+    double* out = fl + 5 * f;
+    out[0] = F.phi; out[1] = F.phiUp.x; out[2] = F.phiUp.y; out[3] = F.phiUp.z; out[4] = F.phiEp;
+}
+
+// Boundary face fluxes: both sides carry the boundary value (foam
+// interpolate() returns the patch value on non-coupled patches).
+__global__ void k_bface_flux(DevMesh m, Thermo th, int scheme, int lowMach, double Mainf, const double* __restrict__ qb,
+                             double* __restrict__ bfl, double* __restrict__ bs) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.NB) return;
+    const double* qq = qb + QW * b;
+    SideState s;
+    s.rho = qq[0]; s.rhoU = mk(qq[1], qq[2], qq[3]); s.rPsi = qq[4]; s.e = qq[5]; s.s = qq[6];
+    FFlux F = face_flux(scheme, s, s, ldv3(m.bSf, m.NB, b), m.bmagSf[b], th.gamma, 1.0, lowMach != 0, Mainf);
+    double* out = bfl + 5 * b;
+    out[0] = F.phi; out[1] = F.phiUp.x; out[2] = F.phiUp.y; out[3] = F.phiUp.z; out[4] = F.phiEp;
+    bs[BW * b + 7] = F.phi;
+}
+
+// calcFields (baseFluxDST.C:223-255): R = div(face fluxes) per unit volume,
+// gathered per cell in foam face order; rhs = -R V (fluxDST.C:124); fused
+// partial sums for |R|^2 (timeDST.C:330) and (R V)^2 per component.
+__global__ void k_residual(DevMesh m, const double* __restrict__ fl, const double* __restrict__ bfl,
+                           double* __restrict__ R, double* __restrict__ rhs, double* __restrict__ partial) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double r[5] = {0, 0, 0, 0, 0};
+    double sq_mag = 0, sq_c[5] = {0, 0, 0, 0, 0};
+    if (i < m.N) {
+        for (int k = m.cf_start[i]; k < m.cf_start[i + 1]; ++k) {
+            int code = m.cf_list[k];
+            const double* F;
+            double sg = 1.0;
+            if (code < m.Fi) { F = fl + 5 * code; sg = (m.own[code] == i) ? 1.0 : -1.0; }
+            else F = bfl + 5 * (code - m.Fi);
+#pragma unroll
+            for (int c = 0; c < 5; ++c) r[c] += sg * F[c];
+        }
+        double Vi = m.V[i];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            double Rc = r[c] / Vi;
+            R[5 * i + c] = Rc;
+            double rv = Rc * Vi;
+            rhs[5 * i + c] = 0.0 - rv;
+            sq_mag += Rc * Rc;
+            sq_c[c] = rv * rv;
+        }
+    }
+    double v = block_sum(sq_mag);
+    if (threadIdx.x == 0) partial[blockIdx.x * 6] = v;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        v = block_sum(sq_c[c]);
+        if (threadIdx.x == 0) partial[blockIdx.x * 6 + 1 + c] = v;
+    }
+}
+
+__global__ void k_residual_finalize(const double* __restrict__ partial, int nb, Scalars* sc) {
+    int c = threadIdx.x;
+    if (c >= 6) return;
+    double s = 0;
+    for (int b = 0; b < nb; ++b) s += partial[b * 6 + c];
+    if (c == 0) sc->res_mag = sqrt(s);
+    else sc->res_l2[c - 1] = sqrt(s);
+}
+
+// ------------------------------------------------------------------ assembly
+__device__ __forceinline__ size_t sidx(const int* slice_off, int r, int k, int e) {
+    size_t slot = (size_t)slice_off[r >> 5] + k;
+    return slot * (32 * 25) + (size_t)e * 32 + (r & 31);
+}
+
+// Roe Jacobian blocks (Roe.C:152-214) assembled straight into the SELL
+// matrix, one row (cell) per thread: off-diagonal (row, column) blocks from
+// the face's upper (row = owner) / lower (row = neighbour) coefficient,
+// the diagonal as ddt + negSumDiag + boundary Jacobians (fluxDST.C:98-112),
+// accumulated in foam face order.
+template <typename MT>
+__global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, SellMat<MT> A, const int* __restrict__ cf_slot,
+                                                  const double* __restrict__ W, const double* __restrict__ prim,
+                                                  const double* __restrict__ bs, const double* __restrict__ rdtc,
+                                                  const Scalars* __restrict__ sc, int steady, double beta) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m.N) return;
+    const double g = th.gamma;
+    double D[25];
+    {
+        double rdt = steady ? rdtc[r] : 1.0 / sc->deltaT;
+        double dg = rdt * m.V[r];
+#pragma unroll
+        for (int e = 0; e < 25; ++e) D[e] = (e % 6 == 0) ? dg : 0.0;
+    }
+    auto cellJ = [&](int c, V3& U, double& phiJ, double& a1, double& cs) {
+        const double* w5 = W + 5 * c;
+        U = div3(mk(w5[1], w5[2], w5[3]), w5[0]);
+        phiJ = 0.5 * (g - 1) * magSqr3(U);
+        a1 = g * w5[4] / w5[0] - phiJ;
+        cs = sqrt(g * th.R * prim[PW * c + 1]);
+    };
+    V3 Ur;
+    double phiJr, a1r, cr;
+    cellJ(r, Ur, phiJr, a1r, cr);
+    double J[25], Jc[25];
+    for (int k = m.cf_start[r]; k < m.cf_start[r + 1]; ++k) {
+        int code = m.cf_list[k];
+        if (code < m.Fi) {
+            const int f = code, o = m.own[f], n = m.nei[f];
+            const bool isOwner = (o == r);
+            const int oc_ = isOwner ? n : o;
+            V3 Uc;
+            double phiJc, a1c, cc;
+            cellJ(oc_, Uc, phiJc, a1c, cc);
+            const double wf = m.w[f];
+            const V3 S = ldv3(m.Sf, m.Fi, f);
+            const double magS = m.magSf[f];
+            const V3 nn = div3(S, magS);
+            V3 Uo = isOwner ? Ur : Uc, Un = isOwner ? Uc : Ur;
+            double co = isOwner ? cr : cc, cn = isOwner ? cc : cr;
+            V3 Uf = add3(scl3(wf, Uo), scl3(1 - wf, Un));
+            double cf = wf * co + (1 - wf) * cn;
+            double amaxSf = fabs(dot3(Uf, S)) + magS * cf;
+            double lambda = 0.5 * amaxSf;
+            calcJ(Ur, g, phiJr, a1r, nn, J);
+            calcJ(Uc, g, phiJc, a1c, nn, Jc);
+            const int slot = cf_slot[k];
+            if (isOwner) {
+#pragma unroll
+                for (int e = 0; e < 25; ++e) {
+                    double I = (e % 6 == 0) ? 1.0 : 0.0;
+                    double lower = -beta * ((J[e] * wf) * magS + I * lambda);
+                    D[e] -= lower;
+                    double upper = beta * ((Jc[e] * (1 - wf)) * magS - I * lambda);
+                    st(&A.val[sidx(A.slice_off, r, slot, e)], upper);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 25; ++e) {
+                    double I = (e % 6 == 0) ? 1.0 : 0.0;
+                    double upper = beta * ((J[e] * (1 - wf)) * magS - I * lambda);
+                    D[e] -= upper;
+                    double lower = -beta * ((Jc[e] * wf) * magS + I * lambda);
+                    st(&A.val[sidx(A.slice_off, r, slot, e)], lower);
+                }
+            }
+        } else {
+            // Roe::computeBoundaryJacobians (Roe.C:274-379)
+            const int b = code - m.Fi;
+            const DevPatch P = m.patches[m.bpatch[b]];
+            const double* B = bs + BW * b;
+            const V3 pSf = ldv3(m.bSf, m.NB, b);
+            const V3 nrm = div3(pSf, m.bmagSf[b]);
+            V3 UB = div3(mk(B[1], B[2], B[3]), B[0]);
+            double pB = B[5], TB = B[6], rhoB = B[0], EB = B[4] / B[0];
+            double rRT = rhoB / pB;
+            double UBS = dot3(UB, pSf);
+            const double Sv[3] = {pSf.x, pSf.y, pSf.z}, Uv[3] = {UB.x, UB.y, UB.z};
+            double dR[25];
+            dR[0] = UBS * rRT;
+            for (int k2 = 0; k2 < 3; ++k2) dR[1 + k2] = rhoB * Sv[k2];
+            dR[4] = -rhoB / TB * UBS;
+            for (int k2 = 0; k2 < 3; ++k2) {
+                dR[(1 + k2) * 5 + 0] = rRT * UBS * Uv[k2] + Sv[k2];
+                for (int l = 0; l < 3; ++l) dR[(1 + k2) * 5 + 1 + l] = rhoB * Uv[k2] * Sv[l] + (k2 == l ? rhoB * UBS : 0.0);
+                dR[(1 + k2) * 5 + 4] = -rhoB / TB * UBS * Uv[k2];
+            }
+            dR[20] = (EB * rRT + 1) * UBS;
+            for (int l = 0; l < 3; ++l) dR[21 + l] = rhoB * UBS * Uv[l] + Sv[l] * (rhoB * EB + pB);
+            dR[24] = rhoB * th.Cv * UBS;
+            // dX/dW at the internal cell
+            const double* w5 = W + 5 * r;
+            V3 UI = Ur;
+            const double UIv[3] = {UI.x, UI.y, UI.z};
+            double rhoEI = w5[4], pI = prim[PW * r], rRho = 1.0 / w5[0];
+            double rRhoCv = rRho / th.Cv;
+            double e = rhoEI * rRho - 0.5 * magSqr3(UI);
+            double RT = pI * rRho;
+            double RCv = RT / e;
+            double dX[25];
+#pragma unroll
+            for (int q2 = 0; q2 < 25; ++q2) dX[q2] = 0.0;
+            dX[0] = RT - RCv * (e - 0.5 * magSqr3(UI));
+            for (int l = 0; l < 3; ++l) dX[1 + l] = -RCv * UIv[l];
+            dX[4] = RCv;
+            for (int k2 = 0; k2 < 3; ++k2) { dX[(1 + k2) * 5] = -rRho * UIv[k2]; dX[(1 + k2) * 5 + 1 + k2] = rRho; }
+            dX[20] = rRhoCv * (0.5 * magSqr3(UI) - e);
+            for (int l = 0; l < 3; ++l) dX[21 + l] = -rRhoCv * UIv[l];
+            dX[24] = rRhoCv;
+            // valueInternalCoeffs
+            double outflow = dpos0(B[7]);
+            auto sc_ = [&](int bc) { return bc == 0 ? 0.0 : (bc == 2 ? outflow : 1.0); };
+            double cdiag[5];
+            cdiag[0] = sc_(P.bc_p);
+            cdiag[4] = sc_(P.bc_T);
+            if (P.bc_U == 0) { cdiag[1] = cdiag[2] = cdiag[3] = 0.0; }
+            else if (P.bc_U == 2) { cdiag[1] = cdiag[2] = cdiag[3] = outflow; }
+            else if (P.bc_U == 3 || P.bc_U == 4) {
+                cdiag[1] = 1 - fabs(nrm.x); cdiag[2] = 1 - fabs(nrm.y); cdiag[3] = 1 - fabs(nrm.z);
+            } else { cdiag[1] = cdiag[2] = cdiag[3] = 1.0; }
+            // pic = (dR . diag(cdiag)) . dX
+            for (int a = 0; a < 5; ++a) {
+                double t1[5];
+                for (int c2 = 0; c2 < 5; ++c2) {
+                    double acc2 = 0;
+                    for (int k2 = 0; k2 < 5; ++k2) acc2 += dR[5 * a + k2] * (k2 == c2 ? cdiag[k2] : 0.0);
+                    t1[c2] = acc2;
+                }
+                for (int c2 = 0; c2 < 5; ++c2) {
+                    double acc2 = 0;
+                    for (int k2 = 0; k2 < 5; ++k2) acc2 += t1[k2] * dX[5 * k2 + c2];
+                    D[5 * a + c2] += beta * acc2;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 25; ++e) st(&A.val[sidx(A.slice_off, r, 0, e)], D[e]);
+}
+
+// ------------------------------------------------------------------ update
+// updateFields.H:40-94: W += dW, bound rho/h/p, U = rhoU/rho,
+// h = Cp/Cv (rhoE/rho - |U|^2/2), T = h/Cp, p = rho R T.
+__global__ void k_update(int N, Thermo th, Bounds bd, const double* __restrict__ dx, double* __restrict__ W,
+                         double* __restrict__ prim, Scalars* sc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int flag = 0;
+    if (i < N) {
+        double* w5 = W + 5 * i;
+        double rho = w5[0] + dx[5 * i + 0];
+        double rUx = w5[1] + dx[5 * i + 1], rUy = w5[2] + dx[5 * i + 2], rUz = w5[3] + dx[5 * i + 3];
+        double rhoE = w5[4] + dx[5 * i + 4];
+        if (rho < bd.rho_min) { rho = bd.rho_min; flag = 1; }
+        if (rho > bd.rho_max) { rho = bd.rho_max; flag = 1; }
+        V3 U = div3(mk(rUx, rUy, rUz), rho);
+        double hh = th.Cp / th.Cv * (rhoE / rho - 0.5 * magSqr3(U));
+        double h = hh;
+        if (h < th.Cp * bd.T_min) { h = th.Cp * bd.T_min; flag = 1; }
+        if (h > th.Cp * bd.T_max) { h = th.Cp * bd.T_max; flag = 1; }
+        double T = h / th.Cp;
+        double p = rho * th.R * T;
+        if (p < bd.p_min) { p = bd.p_min; flag = 1; }
+        if (p > bd.p_max) { p = bd.p_max; flag = 1; }
+        if (!(rho > 0) || !(p > 0) || !isfinite(rhoE) || !isfinite(rho)) flag |= 2;
+        w5[0] = rho; w5[1] = rUx; w5[2] = rUy; w5[3] = rUz; w5[4] = rhoE;
+        double* P = prim + PW * i;
+        P[0] = p; P[1] = T; P[2] = h; P[3] = U.x; P[4] = U.y; P[5] = U.z;
+    }
+    unsigned b = __ballot_sync(0xffffffffu, flag & 1), d = __ballot_sync(0xffffffffu, flag & 2);
+    if ((threadIdx.x & 31) == 0 && (b | d)) atomicOr(&sc->flags, (b ? 1 : 0) | (d ? 2 : 0));
+}
+
+// ------------------------------------------------------------------ time control
+// timeDST::setTransientDeltaT (timeDST.C:275-314): per-face (neighbouring)
+// or per-cell (Blazek) stable step, reduced with min.
+__global__ void k_dt_transient(DevMesh m, Thermo th, int neighbouring, const double* __restrict__ prim,
+                               const double* __restrict__ dS, const Scalars* sc, double* partial) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double g = th.gamma, courant = sc->courant;
+    double v = 1e300;
+    if (neighbouring) {
+        if (i < m.Fi) {
+            int P = m.own[i], Q = m.nei[i];
+            double wf = m.w[i];
+            V3 UP = mk(prim[PW * P + 3], prim[PW * P + 4], prim[PW * P + 5]);
+            V3 UQ = mk(prim[PW * Q + 3], prim[PW * Q + 4], prim[PW * Q + 5]);
+            V3 Uf = add3(scl3(wf, UP), scl3(1 - wf, UQ));
+            double cf = wf * sqrt(g * th.R * prim[PW * P + 1]) + (1 - wf) * sqrt(g * th.R * prim[PW * Q + 1]);
+            V3 S = ldv3(m.Sf, m.Fi, i);
+            double amaxSf = fabs(dot3(Uf, S)) + m.magSf[i] * cf;
+            double dtSf = m.magSf[i] / (amaxSf * m.dc[i]);
+            v = dtSf * courant;
+        }
+    } else if (i < m.N) {
+        double cs = sqrt(g * th.R * prim[PW * i + 1]);
+        double lambdaC = (fabs(prim[PW * i + 3]) + cs) * dS[3 * i] + (fabs(prim[PW * i + 4]) + cs) * dS[3 * i + 1] +
+                         (fabs(prim[PW * i + 5]) + cs) * dS[3 * i + 2];
+        v = courant * m.V[i] / lambdaC;
+    }
+    v = block_min(v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+}
+
+__global__ void k_dt_finalize(const double* partial, int nb, Scalars* sc) {
+    if (threadIdx.x != 0) return;
+    double v = 1e300;
+    for (int b = 0; b < nb; ++b) v = fmin(v, partial[b]);
+    sc->deltaT = v;
+}
+
+// setSteadyStateDeltaT (timeDST.C:218-273): local 1/dtau per cell
+__global__ void k_dt_steady(DevMesh m, Thermo th, int neighbouring, const double* __restrict__ prim,
+                            const double* __restrict__ dS, const double* __restrict__ courantF,
+                            double* __restrict__ rdt, double* partial) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double g = th.gamma;
+    double v = 0;
+    double lo = 1e300, hi = -1e300;
+    if (i < m.N) {
+        if (!neighbouring) {
+            double cs = sqrt(g * th.R * prim[PW * i + 1]);
+            double lambdaC = (fabs(prim[PW * i + 3]) + cs) * dS[3 * i] + (fabs(prim[PW * i + 4]) + cs) * dS[3 * i + 1] +
+                             (fabs(prim[PW * i + 5]) + cs) * dS[3 * i + 2];
+            v = lambdaC / (courantF[i] * m.V[i]);
+        } else {
+            for (int k = m.cf_start[i]; k < m.cf_start[i + 1]; ++k) {
+                int code = m.cf_list[k];
+                if (code < m.Fi) {
+                    int P = m.own[code], Q = m.nei[code];
+                    double wf = m.w[code];
+                    V3 UP = mk(prim[PW * P + 3], prim[PW * P + 4], prim[PW * P + 5]);
+                    V3 UQ = mk(prim[PW * Q + 3], prim[PW * Q + 4], prim[PW * Q + 5]);
+                    V3 Uf = add3(scl3(wf, UP), scl3(1 - wf, UQ));
+                    double cf = wf * sqrt(g * th.R * prim[PW * P + 1]) + (1 - wf) * sqrt(g * th.R * prim[PW * Q + 1]);
+                    v = fmax(v, (sqrt(magSqr3(Uf)) + cf) * m.dc[code]);
+                } else {
+                    int b = code - m.Fi;
+                    if (m.patches[m.bpatch[b]].type != 1) continue;
+                    double pl = 0.5 * m.bdc[b] * sqrt(g * th.R * prim[PW * i + 1]) +
+                                sqrt(magSqr3(mk(prim[PW * i + 3], prim[PW * i + 4], prim[PW * i + 5])));
+                    v = fmax(v, pl);
+                }
+            }
+            v /= courantF[i];
+        }
+        rdt[i] = v;
+        lo = hi = v;
+    }
+    lo = block_min(lo);
+    if (threadIdx.x == 0) partial[2 * blockIdx.x] = lo;
+    hi = block_max(hi);
+    if (threadIdx.x == 0) partial[2 * blockIdx.x + 1] = hi;
+}
+
+__global__ void k_rdt_finalize(const double* partial, int nb, Scalars* sc) {
+    if (threadIdx.x != 0) return;
+    double lo = 1e300, hi = -1e300;
+    for (int b = 0; b < nb; ++b) { lo = fmin(lo, partial[2 * b]); hi = fmax(hi, partial[2 * b + 1]); }
+    sc->rdt_min = lo;
+    sc->rdt_max = hi;
+}
+
+// setCourantDST (timeDST.C:316-443) scalar part: residual-ratio CFL ramp
+__global__ void k_courant_scalar(Scalars* sc, int transient_adjust, double min_co, double max_co) {
+    if (threadIdx.x != 0) return;
+    double residualR = sc->res_mag;
+    if (sc->residual != -1) sc->residualRatio = fmin(fmax(sc->residual / residualR, 0.1), 2.0);
+    sc->residual = residualR;
+    if (transient_adjust) sc->courant = fmin(fmax(sc->courant * sc->residualRatio, min_co), max_co);
+}
+
+// steady branch: per-cell CFL cut on rho / e drops (HiSA rule) and ramp
+__global__ void k_courant_cells(DevMesh m, const double* __restrict__ W, double* __restrict__ rhoOld,
+                                double* __restrict__ eOld, double* __restrict__ courantF, const Scalars* sc,
+                                double min_co, double max_co, double* __restrict__ eNewBuf) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.N) return;
+    auto eN = [&](int c) {
+        const double* w5 = W + 5 * c;
+        V3 U = div3(mk(w5[1], w5[2], w5[3]), w5[0]);
+        return w5[4] / w5[0] - 0.5 * magSqr3(U);
+    };
+    auto drop = [&](int c) {
+        double e = eN(c);
+        return W[5 * c] < 0.95 * rhoOld[c] || e < 0.95 * eOld[c] || e < D_SMALL;
+    };
+    double factor = 1.0;
+    bool di = drop(i);
+    for (int k = m.cf_start[i]; k < m.cf_start[i + 1]; ++k) {
+        int code = m.cf_list[k];
+        if (code >= m.Fi) continue;
+        int o = m.own[code], other = (o == i) ? m.nei[code] : o;
+        if (di) factor = fmin(factor, 0.5);
+        if (drop(other)) factor = fmin(factor, 0.75);
+    }
+    eNewBuf[i] = eN(i);
+    courantF[i] = fmin(fmax(courantF[i] * sc->residualRatio * factor, min_co), max_co);
+}
+
+__global__ void k_store_old(int N, const double* __restrict__ W, const double* __restrict__ eNewBuf,
+                            double* __restrict__ rhoOld, double* __restrict__ eOld) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    rhoOld[i] = W[5 * i];
+    eOld[i] = eNewBuf[i];
+}
+
+__global__ void k_time_advance(Scalars* sc) {
+    if (threadIdx.x == 0) {
+        sc->time += sc->deltaT;
+        sc->flags = 0;
+    }
+}
+
+}  // namespace rdst

@@ -1,0 +1,495 @@
+// linalg.cuh -- block Krylov kernels of the fully-coupled step: SELL-32
+// block SpMV, block-Jacobi and subdomain ILU(0) preconditioners, and the
+// vector/reduction pieces of block GMRES (CGS2 orthogonalisation, Givens
+// least squares on the device) and BiCGStab.  Matrix storage MT may be
+// double, float or bf16; vectors, dot products, Hessenberg and norms are FP64.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace rdst {
+
+// inverse of a 5x5 block (Gauss-Jordan, partial pivoting), in registers
+__device__ __forceinline__ void inv5(const double A[25], double X[25]) {
+    double a[5][10];
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+        for (int j = 0; j < 5; ++j) { a[i][j] = A[5 * i + j]; a[i][j + 5] = (i == j) ? 1.0 : 0.0; }
+    for (int c = 0; c < 5; ++c) {
+        int p = c;
+        for (int r = c + 1; r < 5; ++r) if (fabs(a[r][c]) > fabs(a[p][c])) p = r;
+        if (p != c) for (int j = 0; j < 10; ++j) { double t = a[p][j]; a[p][j] = a[c][j]; a[c][j] = t; }
+        double piv = 1.0 / a[c][c];
+        for (int j = 0; j < 10; ++j) a[c][j] *= piv;
+        for (int r = 0; r < 5; ++r) {
+            if (r == c) continue;
+            double f = a[r][c];
+            if (f != 0.0) for (int j = 0; j < 10; ++j) a[r][j] -= f * a[c][j];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+        for (int j = 0; j < 5; ++j) X[5 * i + j] = a[i][j + 5];
+}
+
+// y = A x  (or y = b - A x when b != nullptr); one row per thread
+template <typename MT>
+__global__ void __launch_bounds__(256) k_spmv(SellMat<MT> A, const double* __restrict__ x, double* __restrict__ y,
+                                              const double* __restrict__ b, const int* __restrict__ active) {
+    if (active && !*active) return;
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.N) return;
+    const int s = r >> 5, lane = r & 31;
+    const int base = A.slice_off[s], width = A.slice_w[s];
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int k = 0; k < width; ++k) {
+        size_t slot = (size_t)(base + k);
+        int c = A.col[slot * 32 + lane];
+        if (c < 0) continue;
+        const double* xc = x + 5 * c;
+        double xv[5] = {xc[0], xc[1], xc[2], xc[3], xc[4]};
+        const MT* v = A.val + slot * (32 * 25) + lane;
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+#pragma unroll
+            for (int j = 0; j < 5; ++j) acc[i] += ld(v + (5 * i + j) * 32) * xv[j];
+    }
+    double* yr = y + 5 * r;
+    if (b) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) yr[i] = b[5 * r + i] - acc[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) yr[i] = acc[i];
+    }
+}
+
+// y = A xbar for a constant 5-vector xbar (normFactor reference field)
+template <typename MT>
+__global__ void k_spmv_const(SellMat<MT> A, const double* __restrict__ xbar, double* __restrict__ y) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.N) return;
+    const int s = r >> 5, lane = r & 31;
+    const int base = A.slice_off[s], width = A.slice_w[s];
+    double acc[5] = {0, 0, 0, 0, 0};
+    double xv[5] = {xbar[0], xbar[1], xbar[2], xbar[3], xbar[4]};
+    for (int k = 0; k < width; ++k) {
+        size_t slot = (size_t)(base + k);
+        if (A.col[slot * 32 + lane] < 0) continue;
+        const MT* v = A.val + slot * (32 * 25) + lane;
+        for (int i = 0; i < 5; ++i)
+            for (int j = 0; j < 5; ++j) acc[i] += ld(v + (5 * i + j) * 32) * xv[j];
+    }
+    for (int i = 0; i < 5; ++i) y[5 * r + i] = acc[i];
+}
+
+// block-Jacobi: dinv = inv(diagonal block), entry-major [25][N]
+template <typename MT>
+__global__ void k_dinv(SellMat<MT> A, MT* __restrict__ dinv) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.N) return;
+    const MT* v = A.val + (size_t)A.slice_off[r >> 5] * (32 * 25) + (r & 31);
+    double D[25], X[25];
+#pragma unroll
+    for (int e = 0; e < 25; ++e) D[e] = ld(v + e * 32);
+    inv5(D, X);
+#pragma unroll
+    for (int e = 0; e < 25; ++e) st(&dinv[(size_t)e * A.N + r], X[e]);
+}
+
+template <typename MT>
+__global__ void k_jacobi(int N, const MT* __restrict__ dinv, const double* __restrict__ x, double* __restrict__ y,
+                         const int* __restrict__ active) {
+    if (active && !*active) return;
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= N) return;
+    double xv[5] = {x[5 * r], x[5 * r + 1], x[5 * r + 2], x[5 * r + 3], x[5 * r + 4]};
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        double a = 0;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) a += ld(&dinv[(size_t)(5 * i + j) * N + r]) * xv[j];
+        y[5 * r + i] = a;
+    }
+}
+
+template <typename MT>
+__global__ void k_copy_identity(int n, const double* __restrict__ x, double* __restrict__ y, const int* __restrict__ active) {
+    if (active && !*active) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = x[i];
+}
+
+// ---------------------------------------------------------------- ILU(0)
+// One CTA per subdomain; rows of a subdomain are contiguous and sorted by
+// wavefront level, so each level is a contiguous row range processed in
+// parallel with a CTA barrier between levels (exact ILU(0) within the
+// subdomain, block-Jacobi between subdomains).
+struct IluDev {
+    int n_parts;
+    const int* part_lvl0;   // [n_parts+1] level index range of each part
+    const int* lvl_off;     // [n_levels+1] row range of each level
+    const int* low_start;   // [N+1]
+    const int* low_slot;    // flat slot (slice slot * 32 + lane) of L_rk / A_rk
+    const int* low_col;
+    const int* up_start;    // [N+1]
+    const int* up_slot;
+    const int* up_col;
+    const int* tr_start;    // [n_low+1]
+    const int* tr_kj;       // flat slot of U_kj
+    const int* tr_rj;       // flat slot of A_rj (-1: diagonal)
+};
+
+__device__ __forceinline__ size_t flat_e(int flat, int e) {
+    return (size_t)(flat >> 5) * (32 * 25) + (size_t)e * 32 + (flat & 31);
+}
+
+template <typename MT>
+__global__ void __launch_bounds__(128) k_ilu_factor(SellMat<MT> LU, MT* __restrict__ dinv, IluDev P) {
+    const int part = blockIdx.x;
+    const int N = LU.N;
+    for (int l = P.part_lvl0[part]; l < P.part_lvl0[part + 1]; ++l) {
+        for (int r = P.lvl_off[l] + threadIdx.x; r < P.lvl_off[l + 1]; r += blockDim.x) {
+            double D[25];
+            const MT* dv = LU.val + (size_t)LU.slice_off[r >> 5] * (32 * 25) + (r & 31);
+#pragma unroll
+            for (int e = 0; e < 25; ++e) D[e] = ld(dv + e * 32);
+            for (int q = P.low_start[r]; q < P.low_start[r + 1]; ++q) {
+                const int sl = P.low_slot[q], k = P.low_col[q];
+                double Ark[25], Lrk[25], Dk[25];
+#pragma unroll
+                for (int e = 0; e < 25; ++e) { Ark[e] = ld(LU.val + flat_e(sl, e)); Dk[e] = ld(dinv + (size_t)e * N + k); }
+#pragma unroll
+                for (int i = 0; i < 5; ++i)
+#pragma unroll
+                    for (int j = 0; j < 5; ++j) {
+                        double a = 0;
+#pragma unroll
+                        for (int t = 0; t < 5; ++t) a += Ark[5 * i + t] * Dk[5 * t + j];
+                        Lrk[5 * i + j] = a;
+                    }
+#pragma unroll
+                for (int e = 0; e < 25; ++e) st(LU.val + flat_e(sl, e), Lrk[e]);
+                for (int t = P.tr_start[q]; t < P.tr_start[q + 1]; ++t) {
+                    const int kj = P.tr_kj[t], rj = P.tr_rj[t];
+                    double U[25];
+#pragma unroll
+                    for (int e = 0; e < 25; ++e) U[e] = ld(LU.val + flat_e(kj, e));
+                    if (rj < 0) {
+#pragma unroll
+                        for (int i = 0; i < 5; ++i)
+#pragma unroll
+                            for (int j = 0; j < 5; ++j) {
+                                double a = 0;
+#pragma unroll
+                                for (int t2 = 0; t2 < 5; ++t2) a += Lrk[5 * i + t2] * U[5 * t2 + j];
+                                D[5 * i + j] -= a;
+                            }
+                    } else {
+                        for (int i = 0; i < 5; ++i)
+                            for (int j = 0; j < 5; ++j) {
+                                double a = 0;
+                                for (int t2 = 0; t2 < 5; ++t2) a += Lrk[5 * i + t2] * U[5 * t2 + j];
+                                MT* p = LU.val + flat_e(rj, 5 * i + j);
+                                st(p, ld(p) - a);
+                            }
+                    }
+                }
+            }
+            double X[25];
+            inv5(D, X);
+#pragma unroll
+            for (int e = 0; e < 25; ++e) st(dinv + (size_t)e * N + r, X[e]);
+        }
+        __syncthreads();
+    }
+}
+
+// x = (LU)^-1 b : forward y_r = b_r - sum L_rk y_k, backward
+// x_r = inv(U_rr)(y_r - sum U_rj x_j), level by level inside the CTA.
+template <typename MT>
+__global__ void __launch_bounds__(128) k_ilu_apply(SellMat<MT> LU, const MT* __restrict__ dinv, IluDev P,
+                                                   const double* __restrict__ b, double* x, const int* __restrict__ active) {
+    if (active && !*active) return;
+    const int part = blockIdx.x;
+    const int N = LU.N;
+    const int l0 = P.part_lvl0[part], l1 = P.part_lvl0[part + 1];
+    for (int l = l0; l < l1; ++l) {
+        for (int r = P.lvl_off[l] + threadIdx.x; r < P.lvl_off[l + 1]; r += blockDim.x) {
+            double y[5] = {b[5 * r], b[5 * r + 1], b[5 * r + 2], b[5 * r + 3], b[5 * r + 4]};
+            for (int q = P.low_start[r]; q < P.low_start[r + 1]; ++q) {
+                const int sl = P.low_slot[q], k = P.low_col[q];
+                double xk[5];
+#pragma unroll
+                for (int j = 0; j < 5; ++j) xk[j] = x[5 * k + j];
+#pragma unroll
+                for (int i = 0; i < 5; ++i)
+#pragma unroll
+                    for (int j = 0; j < 5; ++j) y[i] -= ld(LU.val + flat_e(sl, 5 * i + j)) * xk[j];
+            }
+#pragma unroll
+            for (int i = 0; i < 5; ++i) x[5 * r + i] = y[i];
+        }
+        __syncthreads();
+    }
+    for (int l = l1 - 1; l >= l0; --l) {
+        for (int r = P.lvl_off[l] + threadIdx.x; r < P.lvl_off[l + 1]; r += blockDim.x) {
+            double y[5] = {x[5 * r], x[5 * r + 1], x[5 * r + 2], x[5 * r + 3], x[5 * r + 4]};
+            for (int q = P.up_start[r]; q < P.up_start[r + 1]; ++q) {
+                const int sl = P.up_slot[q], j0 = P.up_col[q];
+                double xj[5];
+#pragma unroll
+                for (int j = 0; j < 5; ++j) xj[j] = x[5 * j0 + j];
+#pragma unroll
+                for (int i = 0; i < 5; ++i)
+#pragma unroll
+                    for (int j = 0; j < 5; ++j) y[i] -= ld(LU.val + flat_e(sl, 5 * i + j)) * xj[j];
+            }
+#pragma unroll
+            for (int i = 0; i < 5; ++i) {
+                double a = 0;
+#pragma unroll
+                for (int j = 0; j < 5; ++j) a += ld(dinv + (size_t)(5 * i + j) * N + r) * y[j];
+                x[5 * r + i] = a;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- vectors
+// deterministic two-stage reductions: fixed grid -> partials -> one block
+constexpr int RED_TPB = 256;
+inline int red_blocks(long n) {
+    long b = (n + RED_TPB * 4 - 1) / (RED_TPB * 4);
+    if (b < 1) b = 1;
+    if (b > 592) b = 592;           // 4 x 148 SMs
+    return (int)b;
+}
+
+// partial[blk * nv + j] = sum_i V_j[i] * w[i], j < nv (nv <= 8 per launch)
+__global__ void __launch_bounds__(RED_TPB) k_multidot(long n, int nv, const double* __restrict__ V, long ldv,
+                                                      const double* __restrict__ w, double* __restrict__ partial,
+                                                      int pstride, const int* __restrict__ active) {
+    if (active && !*active) return;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double wi = w[i];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j < nv) acc[j] += V[j * ldv + i] * wi;
+    }
+    for (int j = 0; j < nv; ++j) {
+        double v = block_sum(acc[j]);
+        if (threadIdx.x == 0) partial[(long)blockIdx.x * pstride + j] = v;
+    }
+}
+
+// out[j] = sum_b partial[b * pstride + j] (fixed order); optional sqrt
+__global__ void k_finalize(const double* __restrict__ partial, int nb, int nv, int pstride, double* __restrict__ out,
+                           int take_sqrt, const int* __restrict__ active) {
+    if (active && !*active) return;
+    int j = blockIdx.x;
+    if (j >= nv) return;
+    double s = 0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(long)b * pstride + j];
+    s = block_sum(s);
+    if (threadIdx.x == 0) out[j] = take_sqrt ? sqrt(s) : s;
+}
+
+// w -= sum_j coef[j] V_j (j < nv); coef on the device
+__global__ void k_maxpy(long n, int nv, const double* __restrict__ V, long ldv, const double* __restrict__ coef,
+                        double* __restrict__ w, double sign, const int* __restrict__ active) {
+    if (active && !*active) return;
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = w[i];
+    for (int j = 0; j < nv; ++j) a -= sign * coef[j] * V[j * ldv + i];
+    w[i] = a;
+}
+
+// x /= *s
+__global__ void k_scale_inv(long n, double* __restrict__ x, const double* __restrict__ s, const int* __restrict__ active) {
+    if (active && !*active) return;
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = x[i] / *s;
+}
+
+// per-component sum |r_c| and the foam normFactor pieces
+__global__ void __launch_bounds__(RED_TPB) k_abs5(int N, const double* __restrict__ r, double* __restrict__ partial) {
+    double a[5] = {0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) a[c] += fabs(r[5 * i + c]);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        double v = block_sum(a[c]);
+        if (threadIdx.x == 0) partial[blockIdx.x * 5 + c] = v;
+    }
+}
+
+// sum over cells of the 5 components (for the average x)
+__global__ void __launch_bounds__(RED_TPB) k_sum5(int N, const double* __restrict__ x, double* __restrict__ partial) {
+    double a[5] = {0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) a[c] += x[5 * i + c];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        double v = block_sum(a[c]);
+        if (threadIdx.x == 0) partial[blockIdx.x * 5 + c] = v;
+    }
+}
+
+// sum_i |Ax_i - pA_i| + |Ax_i + s_i - pA_i| (normFactor, x = W, b = A W + s)
+__global__ void __launch_bounds__(RED_TPB) k_normfactor(int N, const double* __restrict__ Ax, const double* __restrict__ s,
+                                                        const double* __restrict__ pA, int dependentW,
+                                                        double* __restrict__ partial) {
+    double a = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        double s1 = 0, s2 = 0;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            double ax = dependentW ? Ax[5 * i + c] : 0.0;
+            double pa = dependentW ? pA[5 * i + c] : 0.0;
+            double b = ax + s[5 * i + c];
+            s1 += (ax - pa) * (ax - pa);
+            s2 += (b - pa) * (b - pa);
+        }
+        a += sqrt(s1) + sqrt(s2);
+    }
+    a = block_sum(a);
+    if (threadIdx.x == 0) partial[blockIdx.x] = a;
+}
+
+__global__ void k_nf_finalize(const double* __restrict__ partial, int nb, Scalars* sc) {
+    double s = 0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[b];
+    s = block_sum(s);
+    if (threadIdx.x == 0) sc->nf = s + 1.0e-20;
+}
+
+__global__ void k_mean5_finalize(const double* __restrict__ partial, int nb, int N, double* __restrict__ xbar) {
+    int c = threadIdx.x;
+    if (c >= 5) return;
+    double s = 0;
+    for (int b = 0; b < nb; ++b) s += partial[b * 5 + c];
+    xbar[c] = s / N;
+}
+
+// linear residual per component / normFactor -> initial or final
+__global__ void k_linres_finalize(const double* __restrict__ partial, int nb, Scalars* sc, int initial) {
+    int c = threadIdx.x;
+    if (c >= 5) return;
+    double s = 0;
+    for (int b = 0; b < nb; ++b) s += partial[b * 5 + c];
+    double v = s / sc->nf;
+    if (initial) { sc->lin_initial[c] = v; sc->lin_final[c] = v; }
+    else sc->lin_final[c] = v;
+}
+
+// BlockSolverPerformance check: converged if every component below the
+// tolerance, or below relTol x initial, or maxIter reached (after minIter)
+__global__ void k_check(Scalars* sc, double tol, double relTol, int minIter, int maxIter, int count) {
+    if (threadIdx.x != 0) return;
+    if (count) sc->lin_iterations += 1;
+    int it = sc->lin_iterations;
+    bool t = true, r = relTol > 0;
+    for (int c = 0; c < 5; ++c) {
+        if (!(sc->lin_final[c] < tol)) t = false;
+        if (!(sc->lin_final[c] < relTol * sc->lin_initial[c])) r = false;
+    }
+    sc->converged = (it >= minIter) && (t || r || it >= maxIter);
+}
+
+// ---------------------------------------------------------------- GMRES
+__global__ void k_gm_start(Scalars* sc) {
+    if (threadIdx.x != 0) return;
+    for (int i = 0; i < 65; ++i) sc->bh[i] = 0.0;
+    for (int i = 0; i < 64 * 65; ++i) sc->H[i] = 0.0;
+    sc->bh[0] = sc->beta;
+    sc->gm_active = (sc->beta != 0.0);
+    sc->gm_used = 0;
+}
+
+// H[:,i] = h1 + h2 (CGS2), Givens rotations (foam givensRotation), bh
+__global__ void k_gm_givens(Scalars* sc, int i, int m) {
+    if (threadIdx.x != 0 || !sc->gm_active) return;
+    double* H = sc->H;
+    for (int j = 0; j <= i; ++j) H[j * m + i] = sc->hcol[0][j] + sc->hcol[1][j];
+    double beta = sc->beta;
+    for (int j = 0; j < i; ++j) {
+        double Hji = H[j * m + i];
+        H[j * m + i] = sc->cs[j] * Hji - sc->sn[j] * H[(j + 1) * m + i];
+        H[(j + 1) * m + i] = sc->sn[j] * Hji + sc->cs[j] * H[(j + 1) * m + i];
+    }
+    double hh = H[i * m + i], c, s;
+    if (beta == 0.0) { c = 1; s = 0; }
+    else if (fabs(beta) > fabs(hh)) { double tau = -hh / beta; s = 1.0 / sqrt(1.0 + tau * tau); c = s * tau; }
+    else { double tau = -beta / hh; c = 1.0 / sqrt(1.0 + tau * tau); s = c * tau; }
+    sc->cs[i] = c;
+    sc->sn[i] = s;
+    double bhi = sc->bh[i];
+    sc->bh[i] = c * bhi - s * sc->bh[i + 1];
+    sc->bh[i + 1] = s * bhi + c * sc->bh[i + 1];
+    H[i * m + i] = c * H[i * m + i] - s * beta;
+    sc->gm_used = i + 1;
+    if (beta == 0.0) sc->gm_active = 0;
+}
+
+__global__ void k_gm_backsub(Scalars* sc, int m) {
+    if (threadIdx.x != 0) return;
+    int used = sc->gm_used;
+    for (int i = used - 1; i >= 0; --i) {
+        double sum = sc->bh[i];
+        for (int j = i + 1; j < used; ++j) sum -= sc->H[i * m + j] * sc->yh[j];
+        sc->yh[i] = sum / sc->H[i * m + i];
+    }
+    for (int i = used; i < m; ++i) sc->yh[i] = 0.0;
+}
+
+// ---------------------------------------------------------------- BiCGStab
+// p = r + beta (p - omega v)
+__global__ void k_bi_p(long n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ p,
+                       const Scalars* sc) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = r[i] + sc->bi_beta * (p[i] - sc->bi_omega * v[i]);
+}
+__global__ void k_bi_scal_rho(Scalars* sc) {       // rho, beta from rw.r
+    if (threadIdx.x != 0) return;
+    sc->bi_rhoOld = sc->bi_rho;
+    sc->bi_rho = sc->hcol[0][0];
+    sc->bi_beta = sc->bi_rho / sc->bi_rhoOld * (sc->bi_alpha / sc->bi_omega);
+}
+__global__ void k_bi_scal_alpha(Scalars* sc) {
+    if (threadIdx.x != 0) return;
+    sc->bi_alpha = sc->bi_rho / sc->hcol[0][0];
+}
+__global__ void k_bi_s(long n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ s,
+                       const Scalars* sc) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) s[i] = r[i] - sc->bi_alpha * v[i];
+}
+__global__ void k_bi_scal_omega(Scalars* sc) {     // omega = (t.s)/(t.t)
+    if (threadIdx.x != 0) return;
+    double tt = sc->hcol[0][0], ts = sc->hcol[0][1];
+    sc->bi_omega = tt > 0 ? ts / tt : 0.0;
+}
+__global__ void k_bi_update(long n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ ph,
+                            const double* __restrict__ sh, const double* __restrict__ s, const double* __restrict__ t,
+                            const Scalars* sc) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] += sc->bi_alpha * ph[i] + sc->bi_omega * sh[i];
+    r[i] = s[i] - sc->bi_omega * t[i];
+}
+__global__ void k_bi_init(Scalars* sc) {
+    if (threadIdx.x != 0) return;
+    sc->bi_rho = 1e300;
+    sc->bi_alpha = 0.0;
+    sc->bi_omega = 1e300;
+}
+
+}  // namespace rdst

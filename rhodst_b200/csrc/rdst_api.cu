@@ -1,0 +1,1118 @@
+// rdst_api.cu -- host side of the B200 fully-coupled step: context set-up
+// (mesh upload, subdomain partition, wavefront levels, SELL-32 block matrix
+// structure, ILU(0) plan), the step driver that replaces
+// Single::iterate (libraries/finiteVolume/iteration/Single/Single.C:80-104)
+// and the C ABI of include/rdst.h.
+#include "../../include/rdst.h"
+#include "rdst_options.h"
+#include "rdst_internal.h"
+#include "linalg.cuh"
+
+#include <algorithm>
+#include <array>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#define RDST_API extern "C" __attribute__((visibility("default")))
+
+using namespace rdst;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& m) : std::runtime_error(m) {}
+};
+
+inline void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+// kernels launched by the calling thread's current context (CKL follows
+// every launch)
+thread_local long* g_launch_counter = nullptr;
+inline void count_launch() { if (g_launch_counter) ++*g_launch_counter; }
+#define CK(x) ck((x), #x)
+#define CKL() (count_launch(), ck(cudaGetLastError(), "kernel launch"))
+
+enum { KS_SPMV = 0, KS_PRECOND, KS_FLUX, KS_ASSEMBLE, KS_FACTOR, KS_ORTH, KS_UPDATE, KS_N };
+const char* const KS_NAMES[KS_N] = {"spmv", "precond", "flux", "assemble", "factor", "orth", "update"};
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        free_();
+        n = count;
+        if (count) CK(cudaMalloc((void**)&p, count * sizeof(T)));
+    }
+    void upload(const std::vector<T>& v, cudaStream_t s) {
+        alloc(v.size());
+        if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void zero(cudaStream_t s) { if (n) CK(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    void free_() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    ~DBuf() { free_(); }
+};
+
+inline int nblk(long n, int tpb) { return (int)std::max<long>(1, (n + tpb - 1) / tpb); }
+
+// recursive coordinate bisection (deterministic: ties broken by index)
+void rcb(const double* C, std::vector<int>& idx, int lo, int hi, int part0, int nparts, int32_t* out) {
+    if (nparts <= 1 || hi - lo <= 1) {
+        for (int i = lo; i < hi; ++i) out[idx[i]] = part0;
+        return;
+    }
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int i = lo; i < hi; ++i)
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(mn[k], C[3 * idx[i] + k]);
+            mx[k] = std::max(mx[k], C[3 * idx[i] + k]);
+        }
+    int ax = 0;
+    for (int k = 1; k < 3; ++k) if (mx[k] - mn[k] > mx[ax] - mn[ax]) ax = k;
+    int n1 = nparts / 2;
+    int mid = lo + (int)((long)(hi - lo) * n1 / nparts);
+    std::nth_element(idx.begin() + lo, idx.begin() + mid, idx.begin() + hi, [&](int a, int b) {
+        double ca = C[3 * a + ax], cb = C[3 * b + ax];
+        return ca < cb || (ca == cb && a < b);
+    });
+    rcb(C, idx, lo, mid, part0, n1, out);
+    rcb(C, idx, mid, hi, part0 + n1, nparts - n1, out);
+}
+
+struct Report5 { rdst_step_report r; };
+
+__global__ void k_report(const Scalars* sc, rdst_step_report* reps, int idx, double dt_used_from_prev) {
+    if (threadIdx.x != 0) return;
+    rdst_step_report& r = reps[idx];
+    r.time = sc->time;
+    r.courant = sc->courant;
+    for (int c = 0; c < 5; ++c) {
+        r.res_l2[c] = sc->res_l2[c];
+        r.lin_initial[c] = sc->lin_initial[c];
+        r.lin_final[c] = sc->lin_final[c];
+    }
+    r.res_mag = sc->res_mag;
+    r.lin_iterations = sc->lin_iterations;
+    r.flags = sc->flags;
+    r.rdt_min = sc->rdt_min;
+    r.rdt_max = sc->rdt_max;
+    r.t_flux_ms = r.t_jacobian_ms = r.t_precond_ms = r.t_krylov_ms = r.t_update_ms = 0.0;
+}
+
+__global__ void k_report_dt(const Scalars* sc, rdst_step_report* reps, int idx) {
+    if (threadIdx.x == 0) reps[idx].deltaT = sc->deltaT;
+}
+
+__global__ void k_mean_courant(const double* __restrict__ cf, int N, rdst_step_report* reps, int idx) {
+    double s = 0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s += cf[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) reps[idx].courant = s / N;
+}
+
+}  // namespace
+
+// ============================================================================
+struct rdst_ctx {
+    Options o;
+    std::string err;
+    cudaStream_t s = nullptr;
+    int dev = 0;
+    // sizes
+    int N = 0, Fi = 0, F = 0, NBall = 0, NB = 0, n_patches = 0;
+    Thermo th{};
+    Bounds bd{};
+    // numbering
+    std::vector<int> perm, iperm;       // perm[internal] = original
+    std::vector<int> bface_orig;        // active bface -> foam face
+    std::vector<double> hV, hC;         // original numbering, for forces
+    std::vector<int> hpatch_start, hpatch_size;
+    std::vector<int> bface_of_face;     // foam boundary face -> active bface (or -1)
+    // device mesh
+    DBuf<int> own, nei, bcell, bpatch, bfaceD, cf_start, cf_list, cf_slot, cc_start, cc_list;
+    DBuf<double> Sf, magSf, w, dc, d, Cf, bSf, bmagSf, bdc, bCf, V, C, dS;
+    DBuf<DevPatch> patches;
+    DevMesh m{};
+    // fields
+    DBuf<double> W, prim, bs, q, qb, g, psi, fcell, fl, bfl, R, rhs, partial;
+    DBuf<double> rdt, courantF, rhoOld, eOld, eNew;
+    DBuf<Scalars> sc;
+    DBuf<rdst_step_report> reps;
+    // matrix
+    int n_slices = 0, n_slots = 0;
+    DBuf<int> slice_off, slice_w, col;
+    void* Aval = nullptr;
+    void* LUval = nullptr;
+    void* dinv = nullptr;
+    size_t mt_size = 8;
+    // ILU plan
+    int n_parts = 1;
+    DBuf<int> part_lvl0, lvl_off, low_start, low_slot, low_col, up_start, up_slot, up_col, tr_start, tr_kj, tr_rj;
+    // Krylov
+    DBuf<double> dx, r, t, Vb, s2, sh, ph, pv, xbar, Ax, pA;
+    int limiter_need_grad = 1, venkat_mask = 0;
+    bool steady = false;
+    bool state_set = false;
+    // graphs
+    cudaGraphExec_t g_pre = nullptr, g_cycle = nullptr, g_post = nullptr;
+    bool graphs_ok = false;
+    // instrumentation
+    long launches = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    struct EvRec { cudaEvent_t a, b; int kind; };
+    std::vector<EvRec> ev_pending;
+    long ks_launches[KS_N] = {0, 0, 0, 0, 0, 0, 0};
+    double ks_ms[KS_N] = {0, 0, 0, 0, 0, 0, 0};
+    cudaEvent_t step_ev[2] = {nullptr, nullptr};
+    double last_step_ms = 0.0;
+    cudaEvent_t get_event() {
+        if (!ev_pool.empty()) { cudaEvent_t e = ev_pool.back(); ev_pool.pop_back(); return e; }
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        return e;
+    }
+    void collect_events() {
+        for (auto& r : ev_pending) {
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, r.a, r.b));
+            ks_ms[r.kind] += ms;
+            ks_launches[r.kind] += 1;
+            ev_pool.push_back(r.a);
+            ev_pool.push_back(r.b);
+        }
+        ev_pending.clear();
+    }
+
+    ~rdst_ctx() {
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        for (auto e : step_ev) if (e) cudaEventDestroy(e);
+        for (auto& r : ev_pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+        if (g_pre) cudaGraphExecDestroy(g_pre);
+        if (g_cycle) cudaGraphExecDestroy(g_cycle);
+        if (g_post) cudaGraphExecDestroy(g_post);
+        if (Aval) cudaFree(Aval);
+        if (LUval) cudaFree(LUval);
+        if (dinv) cudaFree(dinv);
+        if (s) cudaStreamDestroy(s);
+    }
+
+    template <typename MT>
+    SellMat<MT> mat(void* val) const {
+        SellMat<MT> A;
+        A.N = N; A.n_slices = n_slices; A.slice_off = slice_off.p; A.slice_w = slice_w.p; A.col = col.p;
+        A.val = (MT*)val;
+        return A;
+    }
+    IluDev ilu() const {
+        IluDev P;
+        P.n_parts = n_parts; P.part_lvl0 = part_lvl0.p; P.lvl_off = lvl_off.p;
+        P.low_start = low_start.p; P.low_slot = low_slot.p; P.low_col = low_col.p;
+        P.up_start = up_start.p; P.up_slot = up_slot.p; P.up_col = up_col.p;
+        P.tr_start = tr_start.p; P.tr_kj = tr_kj.p; P.tr_rj = tr_rj.p;
+        return P;
+    }
+    long nvec() const { return 5L * N; }
+};
+
+namespace {
+
+// event pair around one kernel launch when the context profiles
+struct Timed {
+    rdst_ctx& c;
+    int kind;
+    cudaEvent_t a = nullptr;
+    Timed(rdst_ctx& c_, int k) : c(c_), kind(k) {
+        if (c.o.profile) { a = c.get_event(); CK(cudaEventRecord(a, c.s)); }
+    }
+    ~Timed() {
+        if (a) {
+            cudaEvent_t b = c.get_event();
+            cudaEventRecord(b, c.s);
+            c.ev_pending.push_back({a, b, kind});
+        }
+    }
+};
+
+struct CounterScope {
+    long* prev;
+    explicit CounterScope(rdst_ctx& c) : prev(g_launch_counter) { g_launch_counter = &c.launches; }
+    ~CounterScope() { g_launch_counter = prev; }
+};
+
+int flux_code(FluxScheme f) { return (int)f; }
+int lim_code(Limiter l) { return (int)l; }
+
+// ---------------------------------------------------------------- set-up
+void build(rdst_ctx& c, const rdst_mesh* mh) {
+    cudaStream_t s = c.s;
+    const int N = mh->n_cells, Fi = mh->n_internal_faces, F = mh->n_faces;
+    c.N = N; c.Fi = Fi; c.F = F; c.NBall = F - Fi; c.n_patches = mh->n_patches;
+    const Options& o = c.o;
+    c.th.R = o.R; c.th.Cp = o.Cp; c.th.Cv = o.Cv(); c.th.gamma = o.gamma();
+    c.bd = Bounds{o.rho_min, o.rho_max, o.p_min, o.p_max, o.T_min, o.T_max};
+    c.steady = (o.ddt == DDT_STEADY);
+    // active boundary faces
+    std::vector<int> fpatch(c.NBall, -1);
+    std::vector<DevPatch> dp(mh->n_patches);
+    for (int p = 0; p < mh->n_patches; ++p) {
+        const rdst_patch& P = mh->patches[p];
+        if (P.start < Fi || P.start + P.size > F || P.size < 0) throw std::invalid_argument("patch range outside the boundary faces");
+        for (int f = P.start; f < P.start + P.size; ++f) fpatch[f - Fi] = p;
+        DevPatch& d = dp[p];
+        d.type = P.type; d.bc_p = P.bc_p; d.bc_U = P.bc_U; d.bc_T = P.bc_T;
+        d.p_value = P.p_value; d.T_value = P.T_value; d.nut_value = P.nuTilda_value;
+        for (int k = 0; k < 3; ++k) d.U_value[k] = P.U_value[k];
+        if (P.bc_p == RDST_BC_FARFIELD || P.bc_U == RDST_BC_FARFIELD || P.bc_T == RDST_BC_FARFIELD)
+            throw ConfigError("farField boundary conditions are not built into this library yet", true);
+        c.hpatch_start.push_back(P.start);
+        c.hpatch_size.push_back(P.size);
+    }
+    c.bface_of_face.assign(c.NBall, -1);
+    for (int b = 0; b < c.NBall; ++b) {
+        if (fpatch[b] < 0) throw std::invalid_argument("boundary face not covered by a patch");
+        if (mh->patches[fpatch[b]].type != RDST_PATCH_EMPTY) {
+            c.bface_of_face[b] = (int)c.bface_orig.size();
+            c.bface_orig.push_back(Fi + b);
+        }
+    }
+    const int NB = (int)c.bface_orig.size();
+    c.NB = NB;
+    for (int f = 0; f < F; ++f)
+        if (mh->owner[f] < 0 || mh->owner[f] >= N) throw std::invalid_argument("owner index out of range");
+    for (int f = 0; f < Fi; ++f)
+        if (mh->neighbour[f] < 0 || mh->neighbour[f] >= N || mh->neighbour[f] == mh->owner[f])
+            throw std::invalid_argument("neighbour index out of range");
+    // cell adjacency (original numbering), faces ascending
+    std::vector<std::vector<int>> cfaces(N);
+    for (int f = 0; f < Fi; ++f) { cfaces[mh->owner[f]].push_back(f); cfaces[mh->neighbour[f]].push_back(f); }
+    for (int b = 0; b < NB; ++b) cfaces[mh->owner[c.bface_orig[b]]].push_back(Fi + b);
+    for (auto& v : cfaces) std::sort(v.begin(), v.end());
+    // partition + wavefront levels for the subdomain ILU(0)
+    std::vector<int> part(N, 0), level(N, 0);
+    int nparts = 1;
+    if (o.precon == PRECON_ILU0) {
+        nparts = o.ilu_parts > 0 ? o.ilu_parts : std::max(1, N / 1536);
+        nparts = std::min(nparts, N);
+        std::vector<int> idx(N);
+        std::iota(idx.begin(), idx.end(), 0);
+        rcb(mh->C, idx, 0, N, 0, nparts, part.data());
+        for (int i = 0; i < N; ++i) {
+            int lv = 0;
+            for (int f : cfaces[i]) {
+                if (f >= Fi) continue;
+                int k = mh->owner[f] == i ? mh->neighbour[f] : mh->owner[f];
+                if (k < i && part[k] == part[i]) lv = std::max(lv, level[k] + 1);
+            }
+            level[i] = lv;
+        }
+    }
+    c.n_parts = nparts;
+    c.perm.resize(N);
+    std::iota(c.perm.begin(), c.perm.end(), 0);
+    if (o.precon == PRECON_ILU0)
+        std::stable_sort(c.perm.begin(), c.perm.end(), [&](int a, int b) {
+            if (part[a] != part[b]) return part[a] < part[b];
+            return level[a] < level[b];
+        });
+    c.iperm.resize(N);
+    for (int r = 0; r < N; ++r) c.iperm[c.perm[r]] = r;
+    // ---- device mesh
+    std::vector<int> own(Fi), nei(Fi);
+    std::vector<double> Sf(3 * (size_t)Fi), magSf(Fi), w(Fi), dc(Fi), d(3 * (size_t)Fi), Cf(3 * (size_t)Fi);
+    for (int f = 0; f < Fi; ++f) {
+        own[f] = c.iperm[mh->owner[f]];
+        nei[f] = c.iperm[mh->neighbour[f]];
+        for (int k = 0; k < 3; ++k) {
+            Sf[k * (size_t)Fi + f] = mh->Sf[3 * f + k];
+            Cf[k * (size_t)Fi + f] = mh->Cf[3 * f + k];
+            d[k * (size_t)Fi + f] = mh->C[3 * mh->neighbour[f] + k] - mh->C[3 * mh->owner[f] + k];
+        }
+        magSf[f] = mh->magSf[f]; w[f] = mh->weights[f]; dc[f] = mh->deltaCoeffs[f];
+    }
+    std::vector<int> bcell(NB), bpatch(NB);
+    std::vector<double> bSf(3 * (size_t)NB), bmagSf(NB), bdc(NB), bCf(3 * (size_t)NB);
+    for (int b = 0; b < NB; ++b) {
+        int f = c.bface_orig[b];
+        bcell[b] = c.iperm[mh->owner[f]];
+        bpatch[b] = fpatch[f - Fi];
+        for (int k = 0; k < 3; ++k) {
+            bSf[k * (size_t)NB + b] = mh->Sf[3 * f + k];
+            bCf[k * (size_t)NB + b] = mh->Cf[3 * f + k];
+        }
+        bmagSf[b] = mh->magSf[f]; bdc[b] = mh->deltaCoeffs[f];
+    }
+    std::vector<double> V(N), C(3 * (size_t)N), dS(3 * (size_t)N, 0.0);
+    c.hV.assign(mh->V, mh->V + N);
+    c.hC.assign(mh->C, mh->C + 3 * (size_t)N);
+    for (int r = 0; r < N; ++r) {
+        int i = c.perm[r];
+        V[r] = mh->V[i];
+        for (int k = 0; k < 3; ++k) C[k * (size_t)N + r] = mh->C[3 * i + k];
+    }
+    // dS = 1/2 sum |Sf| componentwise (timeDST.C:117-153), non-empty faces
+    for (int f = 0; f < F; ++f) {
+        if (f >= Fi && c.bface_of_face[f - Fi] < 0) continue;
+        int ro = c.iperm[mh->owner[f]];
+        for (int k = 0; k < 3; ++k) dS[3 * ro + k] += std::fabs(mh->Sf[3 * f + k]);
+        if (f < Fi) {
+            int rn = c.iperm[mh->neighbour[f]];
+            for (int k = 0; k < 3; ++k) dS[3 * rn + k] += std::fabs(mh->Sf[3 * f + k]);
+        }
+    }
+    for (auto& x : dS) x *= 0.5;
+    // cell -> face CSR in internal row order (codes: f < Fi internal, Fi+b boundary)
+    std::vector<int> cf_start(N + 1, 0), cf_list, cc_start(N + 1, 0), cc_list;
+    for (int r = 0; r < N; ++r) {
+        for (int fc : cfaces[c.perm[r]]) cf_list.push_back(fc);
+        cf_start[r + 1] = (int)cf_list.size();
+    }
+    // SELL-32 structure: slot 0 diagonal, then neighbours by internal column
+    c.n_slices = (N + 31) / 32;
+    std::vector<int> slice_off(c.n_slices + 1, 0), slice_w(c.n_slices, 1);
+    std::vector<std::vector<int>> rowcols(N);
+    for (int r = 0; r < N; ++r) {
+        for (int k = cf_start[r]; k < cf_start[r + 1]; ++k) {
+            int fc = cf_list[k];
+            if (fc >= Fi) continue;
+            int other = own[fc] == r ? nei[fc] : own[fc];
+            rowcols[r].push_back(other);
+            cc_list.push_back(other);
+        }
+        cc_start[r + 1] = (int)cc_list.size();
+        std::sort(rowcols[r].begin(), rowcols[r].end());
+        if (std::adjacent_find(rowcols[r].begin(), rowcols[r].end()) != rowcols[r].end())
+            throw std::invalid_argument("two faces between the same pair of cells");
+    }
+    for (int sl = 0; sl < c.n_slices; ++sl) {
+        int wmax = 1;
+        for (int r = sl * 32; r < std::min(N, sl * 32 + 32); ++r) wmax = std::max(wmax, 1 + (int)rowcols[r].size());
+        slice_w[sl] = wmax;
+        slice_off[sl + 1] = slice_off[sl] + wmax;
+    }
+    c.n_slots = slice_off[c.n_slices];
+    std::vector<int> col((size_t)c.n_slots * 32, -1);
+    auto flat = [&](int r, int k) { return (slice_off[r >> 5] + k) * 32 + (r & 31); };
+    for (int r = 0; r < N; ++r) {
+        col[flat(r, 0)] = r;
+        for (size_t k = 0; k < rowcols[r].size(); ++k) col[flat(r, 1 + (int)k)] = rowcols[r][k];
+    }
+    std::vector<int> cf_slot(cf_list.size(), -1);
+    for (int r = 0; r < N; ++r)
+        for (int k = cf_start[r]; k < cf_start[r + 1]; ++k) {
+            int fc = cf_list[k];
+            if (fc >= Fi) continue;
+            int other = own[fc] == r ? nei[fc] : own[fc];
+            int pos = (int)(std::lower_bound(rowcols[r].begin(), rowcols[r].end(), other) - rowcols[r].begin());
+            cf_slot[k] = 1 + pos;
+        }
+    // ---- ILU plan
+    if (o.precon == PRECON_ILU0) {
+        std::vector<int> ipart(N);
+        for (int r = 0; r < N; ++r) ipart[r] = part[c.perm[r]];
+        std::vector<int> lvl_off, part_lvl0(nparts + 1, 0);
+        for (int r = 0; r < N; ++r) {
+            if (r == 0 || ipart[r] != ipart[r - 1] || level[c.perm[r]] != level[c.perm[r - 1]]) lvl_off.push_back(r);
+        }
+        lvl_off.push_back(N);
+        // part_lvl0: first level index of each part
+        {
+            int li = 0;
+            for (int p = 0; p < nparts; ++p) {
+                part_lvl0[p] = li;
+                while (li < (int)lvl_off.size() - 1 && ipart[lvl_off[li]] == p) ++li;
+            }
+            part_lvl0[nparts] = (int)lvl_off.size() - 1;
+        }
+        std::vector<int> low_start(N + 1, 0), low_slot, low_col, up_start(N + 1, 0), up_slot, up_col;
+        std::vector<int> tr_start(1, 0), tr_kj, tr_rj;
+        for (int r = 0; r < N; ++r) {
+            for (size_t k = 0; k < rowcols[r].size(); ++k) {
+                int cc = rowcols[r][k];
+                if (ipart[cc] != ipart[r]) continue;
+                if (cc < r) { low_slot.push_back(flat(r, 1 + (int)k)); low_col.push_back(cc); }
+                else { up_slot.push_back(flat(r, 1 + (int)k)); up_col.push_back(cc); }
+            }
+            low_start[r + 1] = (int)low_slot.size();
+            up_start[r + 1] = (int)up_slot.size();
+        }
+        for (int r = 0; r < N; ++r) {
+            for (int q = low_start[r]; q < low_start[r + 1]; ++q) {
+                int k = low_col[q];
+                for (int u = up_start[k]; u < up_start[k + 1]; ++u) {
+                    int j = up_col[u];
+                    if (j == r) { tr_kj.push_back(up_slot[u]); tr_rj.push_back(-1); continue; }
+                    auto it = std::lower_bound(rowcols[r].begin(), rowcols[r].end(), j);
+                    if (it != rowcols[r].end() && *it == j && ipart[j] == ipart[r]) {
+                        tr_kj.push_back(up_slot[u]);
+                        tr_rj.push_back(flat(r, 1 + (int)(it - rowcols[r].begin())));
+                    }
+                }
+                tr_start.push_back((int)tr_kj.size());
+            }
+        }
+        c.part_lvl0.upload(part_lvl0, s); c.lvl_off.upload(lvl_off, s);
+        c.low_start.upload(low_start, s); c.low_slot.upload(low_slot, s); c.low_col.upload(low_col, s);
+        c.up_start.upload(up_start, s); c.up_slot.upload(up_slot, s); c.up_col.upload(up_col, s);
+        c.tr_start.upload(tr_start, s); c.tr_kj.upload(tr_kj, s); c.tr_rj.upload(tr_rj, s);
+    }
+    // ---- upload
+    c.own.upload(own, s); c.nei.upload(nei, s); c.Sf.upload(Sf, s); c.magSf.upload(magSf, s); c.w.upload(w, s);
+    c.dc.upload(dc, s); c.d.upload(d, s); c.Cf.upload(Cf, s);
+    c.bcell.upload(bcell, s); c.bpatch.upload(bpatch, s);
+    std::vector<int> bfo(c.bface_orig);
+    c.bfaceD.upload(bfo, s);
+    c.bSf.upload(bSf, s); c.bmagSf.upload(bmagSf, s); c.bdc.upload(bdc, s); c.bCf.upload(bCf, s);
+    c.V.upload(V, s); c.C.upload(C, s); c.dS.upload(dS, s);
+    c.cf_start.upload(cf_start, s); c.cf_list.upload(cf_list, s); c.cf_slot.upload(cf_slot, s);
+    c.cc_start.upload(cc_start, s); c.cc_list.upload(cc_list, s);
+    c.patches.upload(dp, s);
+    c.slice_off.upload(slice_off, s); c.slice_w.upload(slice_w, s); c.col.upload(col, s);
+    DevMesh& m = c.m;
+    m.N = N; m.Fi = Fi; m.NB = NB; m.n_patches = mh->n_patches;
+    m.own = c.own.p; m.nei = c.nei.p; m.Sf = c.Sf.p; m.magSf = c.magSf.p; m.w = c.w.p; m.dc = c.dc.p;
+    m.d = c.d.p; m.Cf = c.Cf.p;
+    m.bcell = c.bcell.p; m.bpatch = c.bpatch.p; m.bface = c.bfaceD.p; m.bSf = c.bSf.p; m.bmagSf = c.bmagSf.p;
+    m.bdc = c.bdc.p; m.bCf = c.bCf.p; m.V = c.V.p; m.C = c.C.p;
+    m.cf_start = c.cf_start.p; m.cf_list = c.cf_list.p; m.cc_start = c.cc_start.p; m.cc_list = c.cc_list.p;
+    m.patches = c.patches.p;
+    // ---- fields
+    c.W.alloc(5L * N); c.prim.alloc((size_t)PW * N); c.bs.alloc((size_t)BW * std::max(NB, 1));
+    c.q.alloc((size_t)QW * N); c.qb.alloc((size_t)QW * std::max(NB, 1)); c.g.alloc((size_t)GW * N);
+    c.psi.alloc((size_t)QW * N); c.fcell.alloc(N); c.fl.alloc(5L * std::max(Fi, 1)); c.bfl.alloc(5L * std::max(NB, 1));
+    c.R.alloc(5L * N); c.rhs.alloc(5L * N);
+    c.rdt.alloc(N); c.courantF.alloc(N); c.rhoOld.alloc(N); c.eOld.alloc(N); c.eNew.alloc(N);
+    c.sc.alloc(1); c.sc.zero(s);
+    int nbmax = std::max(nblk(std::max(N, Fi), TPB), red_blocks(5L * N));
+    c.partial.alloc((size_t)std::max(nbmax, 1) * 72);
+    c.bs.zero(s); c.W.zero(s); c.prim.zero(s); c.psi.zero(s); c.fcell.zero(s);
+    // ---- matrix storage
+    c.mt_size = o.precision == PREC_FP64 ? 8 : (o.precision == PREC_FP32 ? 4 : 2);
+    size_t mbytes = (size_t)c.n_slots * 32 * 25 * c.mt_size;
+    CK(cudaMalloc(&c.Aval, mbytes));
+    CK(cudaMemsetAsync(c.Aval, 0, mbytes, s));
+    if (o.precon == PRECON_ILU0) {
+        CK(cudaMalloc(&c.LUval, mbytes));
+        CK(cudaMemsetAsync(c.LUval, 0, mbytes, s));
+    }
+    if (o.precon != PRECON_NONE) CK(cudaMalloc(&c.dinv, (size_t)25 * N * c.mt_size));
+    // ---- Krylov
+    const long n5 = 5L * N;
+    c.dx.alloc(n5); c.r.alloc(n5); c.t.alloc(n5); c.Ax.alloc(n5); c.pA.alloc(n5); c.xbar.alloc(8);
+    if (o.solver == SOLVER_GMRES) c.Vb.alloc((size_t)(o.n_directions + 1) * n5);
+    else { c.s2.alloc(n5); c.sh.alloc(n5); c.ph.alloc(n5); c.pv.alloc(n5); c.Vb.alloc(2 * n5); }
+    // limiter needs
+    auto vk = [](Limiter l) { return l == LIM_VENKATAKRISHNAN; };
+    c.venkat_mask = (vk(o.lim_rho) ? 1 : 0) | (vk(o.lim_U) ? 0xE : 0) | (vk(o.lim_T) ? 0x70 : 0);
+    CK(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------- step pieces
+template <typename MT>
+struct Ops {
+    static void flux(rdst_ctx& c) {
+        const Options& o = c.o;
+        cudaStream_t s = c.s;
+        const DevMesh& m = c.m;
+        int use_c = (o.flux == FLUX_KURGANOV || o.flux == FLUX_AUSM);
+        k_recon<<<nblk(m.N + m.NB, TPB), TPB, 0, s>>>(m, c.th, use_c, c.W.p, c.prim.p, c.bs.p, c.q.p, c.qb.p);
+        CKL();
+        k_grad<<<nblk(m.N, 128), 128, 0, s>>>(m, c.venkat_mask, o.venkat_K, c.q.p, c.qb.p, c.prim.p, c.g.p, c.psi.p,
+                                             c.fcell.p, o.flux == FLUX_HLLCP);
+        CKL();
+        if (m.Fi > 0) {
+            Timed tm(c, KS_FLUX);
+            k_face_flux<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
+                                                       lim_code(o.lim_T), o.low_mach, o.mainf, c.q.p, c.g.p, c.psi.p,
+                                                       c.fcell.p, c.fl.p);
+            CKL();
+        }
+        if (m.NB > 0)
+            k_bface_flux<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), o.low_mach, o.mainf, c.qb.p, c.bfl.p, c.bs.p);
+        CKL();
+        int nb = nblk(m.N, TPB);
+        k_residual<<<nb, TPB, 0, s>>>(m, c.fl.p, c.bfl.p, c.R.p, c.rhs.p, c.partial.p);
+        CKL();
+        k_residual_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, c.sc.p);
+        CKL();
+    }
+    static void assemble(rdst_ctx& c) {
+        SellMat<MT> A = c.mat<MT>(c.Aval);
+        Timed tm(c, KS_ASSEMBLE);
+        k_assemble<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.m, c.th, A, c.cf_slot.p, c.W.p, c.prim.p, c.bs.p, c.rdt.p,
+                                                        c.sc.p, c.steady ? 1 : 0, c.o.beta);
+        CKL();
+    }
+    static void precond_setup(rdst_ctx& c) {
+        if (c.o.precon == PRECON_DIAGONAL) {
+            k_dinv<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.dinv);
+            CKL();
+        } else if (c.o.precon == PRECON_ILU0) {
+            size_t mbytes = (size_t)c.n_slots * 32 * 25 * sizeof(MT);
+            CK(cudaMemcpyAsync(c.LUval, c.Aval, mbytes, cudaMemcpyDeviceToDevice, c.s));
+            Timed tm(c, KS_FACTOR);
+            k_ilu_factor<MT><<<c.n_parts, 128, 0, c.s>>>(c.mat<MT>(c.LUval), (MT*)c.dinv, c.ilu());
+            CKL();
+        }
+    }
+    static void precond(rdst_ctx& c, const double* in, double* out, const int* active) {
+        Timed tm(c, KS_PRECOND);
+        if (c.o.precon == PRECON_DIAGONAL)
+            k_jacobi<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.N, (const MT*)c.dinv, in, out, active);
+        else if (c.o.precon == PRECON_ILU0)
+            k_ilu_apply<MT><<<c.n_parts, 128, 0, c.s>>>(c.mat<MT>(c.LUval), (const MT*)c.dinv, c.ilu(), in, out, active);
+        else
+            k_copy_identity<MT><<<nblk(c.nvec(), TPB), TPB, 0, c.s>>>((int)c.nvec(), in, out, active);
+        CKL();
+    }
+    static void spmv(rdst_ctx& c, const double* x, double* y, const double* b, const int* active) {
+        Timed tm(c, KS_SPMV);
+        k_spmv<MT><<<nblk(c.N, 256), 256, 0, c.s>>>(c.mat<MT>(c.Aval), x, y, b, active);
+        CKL();
+    }
+    // normFactor + initial residual (dx = 0 -> r = rhs)
+    static void solve_init(rdst_ctx& c) {
+        cudaStream_t s = c.s;
+        const int N = c.N;
+        int nb = red_blocks(N);
+        if (c.o.dependent_W) {
+            spmv(c, c.W.p, c.Ax.p, nullptr, nullptr);
+            k_sum5<<<nb, RED_TPB, 0, s>>>(N, c.W.p, c.partial.p); CKL();
+            k_mean5_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, N, c.xbar.p); CKL();
+            k_spmv_const<MT><<<nblk(N, 256), 256, 0, s>>>(c.mat<MT>(c.Aval), c.xbar.p, c.pA.p); CKL();
+        }
+        k_normfactor<<<nb, RED_TPB, 0, s>>>(N, c.Ax.p, c.rhs.p, c.pA.p, c.o.dependent_W ? 1 : 0, c.partial.p); CKL();
+        k_nf_finalize<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, c.sc.p); CKL();
+        k_abs5<<<nb, RED_TPB, 0, s>>>(N, c.rhs.p, c.partial.p); CKL();
+        k_linres_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, c.sc.p, 1); CKL();
+        CK(cudaMemsetAsync(c.dx.p, 0, sizeof(double) * c.nvec(), s));
+        CK(cudaMemsetAsync(&c.sc.p->lin_iterations, 0, sizeof(int), s));
+        k_check<<<1, 1, 0, s>>>(c.sc.p, c.o.tolerance, c.o.rel_tol, c.o.min_iter, c.o.max_iter, 0); CKL();
+        if (c.o.solver == SOLVER_BICGSTAB) {
+            CK(cudaMemcpyAsync(c.r.p, c.rhs.p, sizeof(double) * c.nvec(), cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(c.Vb.p, c.rhs.p, sizeof(double) * c.nvec(), cudaMemcpyDeviceToDevice, s));  // rw
+            c.pv.zero(s);
+            CK(cudaMemsetAsync(c.ph.p, 0, sizeof(double) * c.nvec(), s));
+            k_bi_init<<<1, 1, 0, s>>>(c.sc.p); CKL();
+        }
+    }
+    static void dot(rdst_ctx& c, const double* a, const double* b, double* out, int sq, const int* active) {
+        long n = c.nvec();
+        int nb = red_blocks(n);
+        k_multidot<<<nb, RED_TPB, 0, c.s>>>(n, 1, a, 0, b, c.partial.p, 8, active); CKL();
+        k_finalize<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, 1, 8, out, sq, active); CKL();
+    }
+    // V^T w for j <= i (chunks of 8), into out[0..i]
+    static void multidot(rdst_ctx& c, int nv, const double* w, double* out, const int* active) {
+        long n = c.nvec();
+        int nb = red_blocks(n);
+        for (int j0 = 0; j0 < nv; j0 += 8) {
+            int cnt = std::min(8, nv - j0);
+            k_multidot<<<nb, RED_TPB, 0, c.s>>>(n, cnt, c.Vb.p + j0 * n, n, w, c.partial.p, 8, active); CKL();
+            k_finalize<<<cnt, RED_TPB, 0, c.s>>>(c.partial.p, nb, cnt, 8, out + j0, 0, active); CKL();
+        }
+    }
+    // one restart cycle of left-preconditioned GMRES(m) with CGS2
+    static void gmres_cycle(rdst_ctx& c) {
+        cudaStream_t s = c.s;
+        const long n = c.nvec();
+        const int m = c.o.n_directions;
+        Scalars* sc = c.sc.p;
+        int* act = &sc->gm_active;
+        double* V0 = c.Vb.p;
+        spmv(c, c.dx.p, c.r.p, c.rhs.p, nullptr);            // r = rhs - A dx
+        precond(c, c.r.p, V0, nullptr);                      // w = M^-1 r
+        dot(c, V0, V0, &sc->beta, 1, nullptr);
+        k_gm_start<<<1, 1, 0, s>>>(sc); CKL();
+        k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, V0, &sc->beta, act); CKL();
+        for (int i = 0; i < m; ++i) {
+            double* Vi = c.Vb.p + i * n;
+            double* w = c.Vb.p + (i + 1) * n;
+            spmv(c, Vi, c.t.p, nullptr, act);
+            precond(c, c.t.p, w, act);
+            {
+                Timed tm(c, KS_ORTH);
+                multidot(c, i + 1, w, sc->hcol[0], act);
+                k_maxpy<<<nblk(n, TPB), TPB, 0, s>>>(n, i + 1, c.Vb.p, n, sc->hcol[0], w, 1.0, act); CKL();
+                multidot(c, i + 1, w, sc->hcol[1], act);
+                k_maxpy<<<nblk(n, TPB), TPB, 0, s>>>(n, i + 1, c.Vb.p, n, sc->hcol[1], w, 1.0, act); CKL();
+            }
+            dot(c, w, w, &sc->beta, 1, act);
+            k_gm_givens<<<1, 1, 0, s>>>(sc, i, m); CKL();
+            if (i < m - 1) { k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, w, &sc->beta, act); CKL(); }
+        }
+        k_gm_backsub<<<1, 1, 0, s>>>(sc, m); CKL();
+        k_maxpy<<<nblk(n, TPB), TPB, 0, s>>>(n, m, c.Vb.p, n, sc->yh, c.dx.p, -1.0, nullptr); CKL();
+        finish_iteration(c);
+    }
+    static void finish_iteration(rdst_ctx& c) {
+        spmv(c, c.dx.p, c.r.p, c.rhs.p, nullptr);
+        int nb = red_blocks(c.N);
+        k_abs5<<<nb, RED_TPB, 0, c.s>>>(c.N, c.r.p, c.partial.p); CKL();
+        k_linres_finalize<<<1, 32, 0, c.s>>>(c.partial.p, nb, c.sc.p, 0); CKL();
+        k_check<<<1, 1, 0, c.s>>>(c.sc.p, c.o.tolerance, c.o.rel_tol, c.o.min_iter, c.o.max_iter, 1); CKL();
+    }
+    // one BiCGStab iteration (van der Vorst, right preconditioned)
+    static void bicgstab_iter(rdst_ctx& c) {
+        cudaStream_t s = c.s;
+        const long n = c.nvec();
+        Scalars* sc = c.sc.p;
+        double* rw = c.Vb.p;
+        double* t2 = c.Vb.p + n;
+        dot(c, rw, c.r.p, &sc->hcol[0][0], 0, nullptr);
+        k_bi_scal_rho<<<1, 1, 0, s>>>(sc); CKL();
+        k_bi_p<<<nblk(n, TPB), TPB, 0, s>>>(n, c.r.p, c.pv.p, c.t.p, sc); CKL();      // t holds p
+        precond(c, c.t.p, c.ph.p, nullptr);
+        spmv(c, c.ph.p, c.pv.p, nullptr, nullptr);                                  // v = A ph
+        dot(c, rw, c.pv.p, &sc->hcol[0][0], 0, nullptr);
+        k_bi_scal_alpha<<<1, 1, 0, s>>>(sc); CKL();
+        k_bi_s<<<nblk(n, TPB), TPB, 0, s>>>(n, c.r.p, c.pv.p, c.s2.p, sc); CKL();
+        precond(c, c.s2.p, c.sh.p, nullptr);
+        spmv(c, c.sh.p, t2, nullptr, nullptr);
+        dot(c, t2, t2, &sc->hcol[0][0], 0, nullptr);
+        dot(c, t2, c.s2.p, &sc->hcol[0][1], 0, nullptr);
+        k_bi_scal_omega<<<1, 1, 0, s>>>(sc); CKL();
+        k_bi_update<<<nblk(n, TPB), TPB, 0, s>>>(n, c.dx.p, c.r.p, c.ph.p, c.sh.p, c.s2.p, t2, sc); CKL();
+        int nb = red_blocks(c.N);
+        k_abs5<<<nb, RED_TPB, 0, s>>>(c.N, c.r.p, c.partial.p); CKL();
+        k_linres_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, sc, 0); CKL();
+        k_check<<<1, 1, 0, s>>>(sc, c.o.tolerance, c.o.rel_tol, c.o.min_iter, c.o.max_iter, 1); CKL();
+    }
+    static void iteration(rdst_ctx& c) {
+        if (c.o.solver == SOLVER_GMRES) gmres_cycle(c);
+        else bicgstab_iter(c);
+    }
+};
+
+void set_steady_dt(rdst_ctx& c) {
+    int nb = nblk(c.N, TPB);
+    k_dt_steady<<<nb, TPB, 0, c.s>>>(c.m, c.th, c.o.neighbouring, c.prim.p, c.dS.p, c.courantF.p, c.rdt.p, c.partial.p);
+    CKL();
+    k_rdt_finalize<<<1, 32, 0, c.s>>>(c.partial.p, nb, c.sc.p);
+    CKL();
+}
+
+void set_transient_dt(rdst_ctx& c) {
+    long n = c.o.neighbouring ? c.Fi : c.N;
+    int nb = nblk(n, TPB);
+    k_dt_transient<<<nb, TPB, 0, c.s>>>(c.m, c.th, c.o.neighbouring, c.prim.p, c.dS.p, c.sc.p, c.partial.p);
+    CKL();
+    k_dt_finalize<<<1, 32, 0, c.s>>>(c.partial.p, nb, c.sc.p);
+    CKL();
+}
+
+// updateFields.H + turbulence (laminar: none) + setCourantDST
+void post_update(rdst_ctx& c) {
+    cudaStream_t s = c.s;
+    {
+        Timed tm(c, KS_UPDATE);
+        k_update<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, c.dx.p, c.W.p, c.prim.p, c.sc.p); CKL();
+    }
+    k_boundary<<<nblk(c.NB, TPB), TPB, 0, s>>>(c.m, c.th, c.bd, c.prim.p, c.bs.p); CKL();
+    k_courant_scalar<<<1, 1, 0, s>>>(c.sc.p, (!c.steady && c.o.adjust_time_step) ? 1 : 0, c.o.min_co, c.o.max_co); CKL();
+    if (c.steady) {
+        k_courant_cells<<<nblk(c.N, TPB), TPB, 0, s>>>(c.m, c.W.p, c.rhoOld.p, c.eOld.p, c.courantF.p, c.sc.p,
+                                                      c.o.min_co, c.o.max_co, c.eNew.p); CKL();
+        k_store_old<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.W.p, c.eNew.p, c.rhoOld.p, c.eOld.p); CKL();
+        set_steady_dt(c);
+    } else if (c.o.adjust_time_step) {
+        set_transient_dt(c);
+    }
+}
+
+__global__ void k_init_time(int N, const double* __restrict__ prim, Thermo th, double* __restrict__ rhoOld,
+                            double* __restrict__ eOld, double* __restrict__ courantF, double co) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    rhoOld[i] = prim[PW * i] / (th.R * prim[PW * i + 1]);
+    eOld[i] = prim[PW * i + 2] * th.Cv / th.Cp;
+    courantF[i] = co;
+}
+
+__global__ void k_init_scalars(Scalars* sc, double time, double dt, double co) {
+    if (threadIdx.x != 0) return;
+    sc->time = time;
+    sc->deltaT = dt;
+    sc->courant = co;
+    sc->residual = -1;
+    sc->residualRatio = 1;
+    sc->flags = 0;
+}
+
+// timeDST::initialize (timeDST.C:67-208) on the freshly set state
+void initialize_time(rdst_ctx& c) {
+    k_init_time<<<nblk(c.N, TPB), TPB, 0, c.s>>>(c.N, c.prim.p, c.th, c.rhoOld.p, c.eOld.p, c.courantF.p, c.o.initial_co);
+    CKL();
+    k_init_scalars<<<1, 1, 0, c.s>>>(c.sc.p, c.o.start_time, c.o.delta_t, c.o.initial_co);
+    CKL();
+    if (c.steady) set_steady_dt(c);
+    else {
+        if (c.o.adjust_time_step) set_transient_dt(c);
+        set_steady_dt(c);
+    }
+}
+
+template <typename MT>
+void pre_solve(rdst_ctx& c) {
+    k_time_advance<<<1, 1, 0, c.s>>>(c.sc.p);
+    CKL();
+    Ops<MT>::flux(c);
+    Ops<MT>::assemble(c);
+    Ops<MT>::precond_setup(c);
+    Ops<MT>::solve_init(c);
+}
+
+template <typename MT>
+void run_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
+    cudaStream_t s = c.s;
+    if ((int)c.reps.n < n) c.reps.alloc(n);
+    if (!c.step_ev[0]) { CK(cudaEventCreate(&c.step_ev[0])); CK(cudaEventCreate(&c.step_ev[1])); }
+    CK(cudaEventRecord(c.step_ev[0], s));
+    const Options& o = c.o;
+    // a step needs no host round trip when the iteration count is fixed by
+    // minIter = maxIter (GMRES restarts / BiCGStab iterations)
+    const bool fixed = (o.min_iter >= o.max_iter);
+    for (int st = 0; st < n; ++st) {
+        k_report_dt<<<1, 1, 0, s>>>(c.sc.p, c.reps.p, st);
+        CKL();
+        pre_solve<MT>(c);
+        int conv = 0;
+        if (!fixed && o.min_iter == 0) {
+            CK(cudaMemcpyAsync(&conv, &c.sc.p->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        for (int it = 1; !conv && it <= o.max_iter; ++it) {
+            Ops<MT>::iteration(c);
+            if (it >= o.max_iter) break;
+            if (it >= o.min_iter) {
+                CK(cudaMemcpyAsync(&conv, &c.sc.p->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+            }
+        }
+        post_update(c);
+        k_report<<<1, 1, 0, s>>>(c.sc.p, c.reps.p, st, 0.0);
+        CKL();
+        if (c.steady) { k_mean_courant<<<1, 256, 0, s>>>(c.courantF.p, c.N, c.reps.p, st); CKL(); }
+    }
+    CK(cudaEventRecord(c.step_ev[1], s));
+    int flags = 0;
+    CK(cudaMemcpyAsync(&flags, &c.sc.p->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (host_reps) CK(cudaMemcpyAsync(host_reps, c.reps.p, sizeof(rdst_step_report) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, c.step_ev[0], c.step_ev[1]));
+        c.last_step_ms = ms;
+    }
+    c.collect_events();
+    if (flags & 2) throw std::domain_error("non-physical state (NaN or non-positive rho/p) after the update");
+}
+
+template <typename F>
+rdst_status guarded(rdst_ctx* c, F&& fn) {
+    if (!c) return RDST_ERR_ARG;
+    CounterScope cs(*c);
+    try {
+        c->err.clear();
+        fn();
+        return RDST_OK;
+    } catch (const ConfigError& e) {
+        c->err = e.what();
+        return e.unsupported ? RDST_ERR_UNSUPPORTED : RDST_ERR_CONFIG;
+    } catch (const CudaError& e) {
+        c->err = e.what();
+        return RDST_ERR_CUDA;
+    } catch (const std::invalid_argument& e) {
+        c->err = e.what();
+        return RDST_ERR_MESH;
+    } catch (const std::domain_error& e) {
+        c->err = e.what();
+        return RDST_ERR_DIVERGED;
+    } catch (const std::exception& e) {
+        c->err = e.what();
+        return RDST_ERR_ARG;
+    }
+}
+
+template <typename Fn>
+void dispatch(rdst_ctx& c, Fn&& fn) {
+    switch (c.o.precision) {
+        case PREC_FP64: fn((double*)nullptr); break;
+        case PREC_FP32: fn((float*)nullptr); break;
+        default: fn((__nv_bfloat16*)nullptr); break;
+    }
+}
+
+void after_state_set(rdst_ctx& c) {
+    k_init_phib<<<nblk(c.NB, TPB), TPB, 0, c.s>>>(c.m, c.W.p, c.bs.p);
+    CKL();
+    k_boundary<<<nblk(c.NB, TPB), TPB, 0, c.s>>>(c.m, c.th, c.bd, c.prim.p, c.bs.p);
+    CKL();
+    initialize_time(c);
+    CK(cudaStreamSynchronize(c.s));
+    c.state_set = true;
+}
+
+}  // namespace
+
+// ============================================================================ ABI
+RDST_API const char* rdst_version(void) { return "rdst-b200 sm_100a"; }
+
+RDST_API rdst_status rdst_create(const rdst_mesh* mesh, int32_t n_options, const char* const* keys,
+                                 const char* const* values, rdst_ctx** out) {
+    if (!mesh || !out || (n_options > 0 && (!keys || !values))) return RDST_ERR_ARG;
+    *out = nullptr;
+    if (mesh->n_cells <= 0 || mesh->n_internal_faces < 0 || mesh->n_faces < mesh->n_internal_faces ||
+        !mesh->owner || (mesh->n_internal_faces > 0 && !mesh->neighbour) || !mesh->Sf || !mesh->Cf ||
+        !mesh->magSf || !mesh->weights || !mesh->deltaCoeffs || !mesh->C || !mesh->V ||
+        (mesh->n_patches > 0 && !mesh->patches))
+        return RDST_ERR_MESH;
+    std::unique_ptr<rdst_ctx> c(new rdst_ctx);
+    try {
+        c->o = parse_options(n_options, keys, values);
+    } catch (const ConfigError& e) {
+        return e.unsupported ? RDST_ERR_UNSUPPORTED : RDST_ERR_CONFIG;
+    }
+    if (c->o.mu > 0 || c->o.As > 0 || c->o.turbulence != TURB_LAMINAR) return RDST_ERR_UNSUPPORTED;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RDST_ERR_CUDA;
+    rdst_status st = guarded(c.get(), [&] {
+        CK(cudaGetDevice(&c->dev));
+        CK(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
+        build(*c, mesh);
+    });
+    if (st != RDST_OK) {
+        fprintf(stderr, "rdst_create: %s\n", c->err.c_str());
+        return st;
+    }
+    *out = c.release();
+    return RDST_OK;
+}
+
+RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const double* U, const double* T,
+                                        const double* nut) {
+    if (!c || !p || !U || !T) return RDST_ERR_ARG;
+    (void)nut;
+    return guarded(c, [&] {
+        std::vector<double> prim((size_t)PW * c->N, 0.0);
+        for (int r = 0; r < c->N; ++r) {
+            int i = c->perm[r];
+            double* P = &prim[(size_t)PW * r];
+            P[0] = p[i]; P[1] = T[i]; P[2] = c->o.Cp * T[i];
+            P[3] = U[3 * i]; P[4] = U[3 * i + 1]; P[5] = U[3 * i + 2];
+        }
+        CK(cudaMemcpyAsync(c->prim.p, prim.data(), prim.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
+        k_init_state<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->th, c->prim.p, c->W.p);
+        CKL();
+        CK(cudaStreamSynchronize(c->s));
+        after_state_set(*c);
+    });
+}
+
+RDST_API rdst_status rdst_set_conservative(rdst_ctx* c, const double* rho, const double* rhoU, const double* rhoE) {
+    if (!c || !rho || !rhoU || !rhoE) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        std::vector<double> W(5L * c->N), prim((size_t)PW * c->N, 0.0);
+        const double Cv = c->o.Cv(), R = c->o.R, Cp = c->o.Cp;
+        for (int r = 0; r < c->N; ++r) {
+            int i = c->perm[r];
+            W[5 * r] = rho[i];
+            for (int k = 0; k < 3; ++k) W[5 * r + 1 + k] = rhoU[3 * i + k];
+            W[5 * r + 4] = rhoE[i];
+            double Ux = rhoU[3 * i] / rho[i], Uy = rhoU[3 * i + 1] / rho[i], Uz = rhoU[3 * i + 2] / rho[i];
+            double e = rhoE[i] / rho[i] - 0.5 * (Ux * Ux + Uy * Uy + Uz * Uz);
+            double T = e / Cv;
+            double* P = &prim[(size_t)PW * r];
+            P[0] = rho[i] * R * T; P[1] = T; P[2] = Cp * T; P[3] = Ux; P[4] = Uy; P[5] = Uz;
+        }
+        CK(cudaMemcpyAsync(c->W.p, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
+        CK(cudaMemcpyAsync(c->prim.p, prim.data(), prim.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
+        if (c->state_set) {
+            // fields replaced between steps: boundary values from the new
+            // internal field, time-control history kept
+            k_boundary<<<nblk(c->NB, TPB), TPB, 0, c->s>>>(c->m, c->th, c->bd, c->prim.p, c->bs.p);
+            CKL();
+            CK(cudaStreamSynchronize(c->s));
+            return;
+        }
+        CK(cudaStreamSynchronize(c->s));
+        after_state_set(*c);
+    });
+}
+
+RDST_API rdst_status rdst_get_conservative(rdst_ctx* c, double* rho, double* rhoU, double* rhoE) {
+    if (!c) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        std::vector<double> W(5L * c->N);
+        CK(cudaMemcpyAsync(W.data(), c->W.p, W.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaStreamSynchronize(c->s));
+        for (int r = 0; r < c->N; ++r) {
+            int i = c->perm[r];
+            if (rho) rho[i] = W[5 * r];
+            if (rhoU) for (int k = 0; k < 3; ++k) rhoU[3 * i + k] = W[5 * r + 1 + k];
+            if (rhoE) rhoE[i] = W[5 * r + 4];
+        }
+    });
+}
+
+RDST_API rdst_status rdst_get_primitive(rdst_ctx* c, double* p, double* U, double* T, double* nut) {
+    if (!c) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        std::vector<double> P((size_t)PW * c->N);
+        CK(cudaMemcpyAsync(P.data(), c->prim.p, P.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaStreamSynchronize(c->s));
+        for (int r = 0; r < c->N; ++r) {
+            int i = c->perm[r];
+            const double* q = &P[(size_t)PW * r];
+            if (p) p[i] = q[0];
+            if (T) T[i] = q[1];
+            if (U) for (int k = 0; k < 3; ++k) U[3 * i + k] = q[3 + k];
+            if (nut) nut[i] = 0.0;
+        }
+    });
+}
+
+RDST_API rdst_status rdst_step(rdst_ctx* c, int32_t n, rdst_step_report* reps) {
+    if (!c || n < 0) return RDST_ERR_ARG;
+    if (!c->state_set) { c->err = "rdst_step before the state was set"; return RDST_ERR_ARG; }
+    return guarded(c, [&] {
+        if (n == 0) return;
+        dispatch(*c, [&](auto* tag) {
+            using MT = std::remove_pointer_t<decltype(tag)>;
+            run_steps<MT>(*c, n, reps);
+        });
+    });
+}
+
+RDST_API rdst_status rdst_residual(rdst_ctx* c, double* out) {
+    if (!c || !out) return RDST_ERR_ARG;
+    if (!c->state_set) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        dispatch(*c, [&](auto* tag) {
+            using MT = std::remove_pointer_t<decltype(tag)>;
+            Ops<MT>::flux(*c);
+        });
+        std::vector<double> R(5L * c->N);
+        CK(cudaMemcpyAsync(R.data(), c->R.p, R.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaStreamSynchronize(c->s));
+        for (int r = 0; r < c->N; ++r)
+            for (int k = 0; k < 5; ++k) out[5 * c->perm[r] + k] = R[5 * r + k];
+    });
+}
+
+RDST_API rdst_status rdst_assemble(rdst_ctx* c, double* diag, double* upper, double* lower, double* source) {
+    if (!c || !c->state_set) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        size_t ms = c->mt_size;
+        std::vector<unsigned char> raw((size_t)c->n_slots * 32 * 25 * ms);
+        dispatch(*c, [&](auto* tag) {
+            using MT = std::remove_pointer_t<decltype(tag)>;
+            Ops<MT>::flux(*c);
+            Ops<MT>::assemble(*c);
+        });
+        CK(cudaMemcpyAsync(raw.data(), c->Aval, raw.size(), cudaMemcpyDeviceToHost, c->s));
+        std::vector<double> rhs(5L * c->N);
+        CK(cudaMemcpyAsync(rhs.data(), c->rhs.p, rhs.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        std::vector<int> slice_off(c->n_slices + 1), col((size_t)c->n_slots * 32);
+        CK(cudaMemcpyAsync(slice_off.data(), c->slice_off.p, slice_off.size() * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaMemcpyAsync(col.data(), c->col.p, col.size() * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+        std::vector<int> own(c->Fi), nei(c->Fi);
+        CK(cudaMemcpyAsync(own.data(), c->own.p, own.size() * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaMemcpyAsync(nei.data(), c->nei.p, nei.size() * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaStreamSynchronize(c->s));
+        auto val = [&](size_t idx) -> double {
+            if (ms == 8) return ((const double*)raw.data())[idx];
+            if (ms == 4) return ((const float*)raw.data())[idx];
+            uint16_t b = ((const uint16_t*)raw.data())[idx];
+            uint32_t u = (uint32_t)b << 16;
+            float f;
+            std::memcpy(&f, &u, 4);
+            return f;
+        };
+        auto block_of = [&](int r, int cc, double* out25) {
+            int s0 = slice_off[r >> 5], wdt = slice_off[(r >> 5) + 1] - s0;
+            for (int k = 0; k < wdt; ++k) {
+                size_t slot = (size_t)(s0 + k);
+                if (col[slot * 32 + (r & 31)] == cc) {
+                    for (int e = 0; e < 25; ++e) out25[e] = val(slot * 800 + (size_t)e * 32 + (r & 31));
+                    return;
+                }
+            }
+            throw std::runtime_error("matrix slot missing");
+        };
+        for (int r = 0; r < c->N; ++r) {
+            int i = c->perm[r];
+            if (diag) block_of(r, r, diag + 25L * i);
+            if (source) for (int k = 0; k < 5; ++k) source[5L * i + k] = rhs[5L * r + k];
+        }
+        for (int f = 0; f < c->Fi; ++f) {
+            if (upper) block_of(own[f], nei[f], upper + 25L * f);
+            if (lower) block_of(nei[f], own[f], lower + 25L * f);
+        }
+    });
+}
+
+RDST_API rdst_status rdst_forces(rdst_ctx* c, int32_t patch, const double lift[3], const double drag[3],
+                                 const double cofr[3], const double axis[3], double p_ref, double qA, double l_ref,
+                                 double out[3]) {
+    if (!c || !lift || !drag || !cofr || !axis || !out) return RDST_ERR_ARG;
+    if (patch < 0 || patch >= c->n_patches) { c->err = "bad patch index"; return RDST_ERR_ARG; }
+    return guarded(c, [&] {
+        std::vector<double> bs((size_t)BW * std::max(c->NB, 1)), Sf(3L * std::max(c->NB, 1)), Cf(3L * std::max(c->NB, 1));
+        CK(cudaMemcpyAsync(bs.data(), c->bs.p, bs.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaMemcpyAsync(Sf.data(), c->bSf.p, Sf.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaMemcpyAsync(Cf.data(), c->bCf.p, Cf.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaStreamSynchronize(c->s));
+        double Fl = 0, Fd = 0, Mm = 0;
+        const int NB = c->NB;
+        for (int f = c->hpatch_start[patch]; f < c->hpatch_start[patch] + c->hpatch_size[patch]; ++f) {
+            int b = c->bface_of_face[f - c->Fi];
+            if (b < 0) continue;
+            double pb = bs[(size_t)BW * b + 5] - p_ref;
+            double dF[3] = {pb * Sf[b], pb * Sf[NB + b], pb * Sf[2L * NB + b]};
+            Fl += dF[0] * lift[0] + dF[1] * lift[1] + dF[2] * lift[2];
+            Fd += dF[0] * drag[0] + dF[1] * drag[1] + dF[2] * drag[2];
+            double rr[3] = {Cf[b] - cofr[0], Cf[NB + b] - cofr[1], Cf[2L * NB + b] - cofr[2]};
+            double mo[3] = {rr[1] * dF[2] - rr[2] * dF[1], rr[2] * dF[0] - rr[0] * dF[2], rr[0] * dF[1] - rr[1] * dF[0]};
+            Mm += mo[0] * axis[0] + mo[1] * axis[1] + mo[2] * axis[2];
+        }
+        out[0] = Fl / qA;
+        out[1] = Fd / qA;
+        out[2] = Mm / (qA * l_ref);
+    });
+}
+
+RDST_API const char* rdst_last_error(const rdst_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+RDST_API void* rdst_stream(rdst_ctx* c) { return c ? (void*)c->s : nullptr; }
+
+RDST_API int64_t rdst_launch_count(const rdst_ctx* c) { return c ? (int64_t)c->launches : 0; }
+
+RDST_API double rdst_last_step_ms(const rdst_ctx* c) { return c ? c->last_step_ms : 0.0; }
+
+RDST_API rdst_status rdst_kernel_stats(rdst_ctx* c, const char* kernel, int64_t* launches, double* total_ms) {
+    if (!c || !kernel || !launches || !total_ms) return RDST_ERR_ARG;
+    for (int k = 0; k < KS_N; ++k)
+        if (std::strcmp(kernel, KS_NAMES[k]) == 0) {
+            *launches = c->ks_launches[k];
+            *total_ms = c->ks_ms[k];
+            return RDST_OK;
+        }
+    c->err = std::string("unknown kernel class ") + kernel;
+    return RDST_ERR_ARG;
+}
+
+RDST_API void rdst_destroy(rdst_ctx* c) { delete c; }
+
+RDST_API rdst_status rdst_partition_cells(int32_t n_cells, const double* C, int32_t n_parts, int32_t* out) {
+    if (n_cells <= 0 || !C || !out || n_parts <= 0) return RDST_ERR_ARG;
+    std::vector<int> idx(n_cells);
+    std::iota(idx.begin(), idx.end(), 0);
+    rcb(C, idx, 0, n_cells, 0, std::min(n_parts, n_cells), out);
+    return RDST_OK;
+}

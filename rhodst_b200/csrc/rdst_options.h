@@ -1,0 +1,267 @@
+// rdst_options.h -- dictionary entries that select and parameterise the
+// fully-coupled step, with the reference's names and defaults.
+//
+// Keys/defaults follow libraries/rhoDST/IOdictDST/IOdictDST.C:89-225
+// (rhoDSTDict), the fvSchemes/fvSolution entries the step reads
+// (tutorials/forwardStep/system/{fvSchemes,fvSolution}) and the thermo /
+// transport coefficients of constant/thermophysicalProperties.  Selector
+// names are those of the reference's run-time selection tables
+// (newbaseFluxDST.C:64-84, JacobianDST.C:72-91, newIteration.C:59-78).
+#pragma once
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace rdst {
+
+enum FluxScheme { FLUX_KURGANOV = 0, FLUX_HLL, FLUX_HLLC, FLUX_HLLCP, FLUX_AUSMPLUS,
+                  FLUX_AUSMPLUSUP, FLUX_AUSM };
+enum Limiter { LIM_LINEAR = 0, LIM_UPWIND, LIM_OSPRE, LIM_VANLEER, LIM_MINMOD, LIM_VANALBADA,
+               LIM_SUPERBEE, LIM_MUSCL, LIM_VENKATAKRISHNAN };
+enum Solver { SOLVER_GMRES = 0, SOLVER_BICGSTAB };
+enum Precon { PRECON_NONE = 0, PRECON_DIAGONAL, PRECON_ILU0 };
+enum Ddt { DDT_EULER = 0, DDT_STEADY };
+enum Precision { PREC_FP64 = 0, PREC_FP32, PREC_BF16 };
+enum Turbulence { TURB_LAMINAR = 0, TURB_SANEG, TURB_SARC1, TURB_SARC2 };
+
+// Thrown by the parser; mapped to RDST_ERR_CONFIG / RDST_ERR_UNSUPPORTED.
+struct ConfigError : std::runtime_error {
+    bool unsupported;
+    ConfigError(const std::string& m, bool u = false) : std::runtime_error(m), unsupported(u) {}
+};
+
+struct Options {
+    // rhoDSTDict
+    FluxScheme flux = FLUX_KURGANOV;
+    bool flux_given = false;
+    std::string jacobian = "Roe";
+    bool dependent_W = true;          // dependentVariable W | deltaW
+    double beta = 1.0;                // timeIntegration.beta
+    bool adjust_time_step = true;     // timeControls.adjustTimeStep
+    bool neighbouring = false;        // timeControls.neighbouring
+    double initial_co = 1.0, min_co = 0.1, max_co = 50.0;
+    bool direct_wave_speed = true;    // HLLC/HLLCP
+    bool low_mach = false;            // AUSM+up
+    double mainf = 0.5;               // AUSM+up
+    double venkat_K = 5.0;            // Venkatakrishnan constant (not in the reference)
+    // fvSchemes
+    Ddt ddt = DDT_EULER;
+    Limiter lim_rho = LIM_OSPRE, lim_U = LIM_OSPRE, lim_T = LIM_OSPRE;
+    // fvSolution: solvers.W
+    Solver solver = SOLVER_BICGSTAB;
+    Precon precon = PRECON_ILU0;
+    int n_directions = 8;
+    double tolerance = 1e-6, rel_tol = 0.0;
+    int max_iter = 1000, min_iter = 0;
+    // fvSolution: fieldBounds (updateFields.H:44-62)
+    double rho_min = 1e-15, rho_max = 1e10, p_min = 1e-15, p_max = 1e10, T_min = 1e-15, T_max = 1e10;
+    // thermophysicalProperties (perfectGas, hConstThermo, const/Sutherland transport)
+    double R = 8314.47 / 28.9, Cp = 1004.5;
+    double mu = 0.0, Pr = 1.0;        // constTransport
+    double As = 0.0, Ts = 0.0;        // sutherlandTransport (As > 0 selects it)
+    double Prt = 0.85;                // turbulent Prandtl number
+    Turbulence turbulence = TURB_LAMINAR;
+    // time
+    double delta_t = 1.0;             // controlDict deltaT (used when adjustTimeStep false)
+    double start_time = 0.0;
+    // B200 additions
+    Precision precision = PREC_FP64;
+    int ilu_parts = 0;                // 0: choose from the mesh size; 1: exact global ILU(0)
+    bool graphs = true;               // capture steps in CUDA graphs
+    bool profile = false;             // event-time kernel classes inside steps
+
+    double gamma() const { return Cp / (Cp - R); }
+    double Cv() const { return Cp - R; }
+};
+
+inline std::string trim(const std::string& s) {
+    size_t a = s.find_first_not_of(" \t\n;"), b = s.find_last_not_of(" \t\n;");
+    return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+inline bool parse_bool(const std::string& k, const std::string& v) {
+    std::string t = trim(v);
+    if (t == "true" || t == "yes" || t == "on" || t == "1") return true;
+    if (t == "false" || t == "no" || t == "off" || t == "0") return false;
+    throw ConfigError("option " + k + ": expected a bool, got '" + v + "'");
+}
+
+inline double parse_double(const std::string& k, const std::string& v) {
+    std::string t = trim(v);
+    char* end = nullptr;
+    double d = std::strtod(t.c_str(), &end);
+    if (t.empty() || *end != '\0' || !std::isfinite(d))
+        throw ConfigError("option " + k + ": expected a number, got '" + v + "'");
+    return d;
+}
+
+inline int parse_int(const std::string& k, const std::string& v) {
+    double d = parse_double(k, v);
+    if (d != std::floor(d)) throw ConfigError("option " + k + ": expected an integer");
+    return (int)d;
+}
+
+inline void parse_pair(const std::string& k, const std::string& v, double& a, double& b) {
+    std::istringstream is(v);
+    std::string s1, s2;
+    is >> s1 >> s2;
+    a = parse_double(k, s1);
+    b = parse_double(k, s2);
+}
+
+inline Limiter parse_limiter(const std::string& k, const std::string& v, bool vector) {
+    std::string t = trim(v);
+    if (t == "linear") return LIM_LINEAR;
+    if (t == "upwind") return LIM_UPWIND;
+    if (t == "Venkatakrishnan") return LIM_VENKATAKRISHNAN;
+    // vector fields take the "V" (direction-aware) variants, scalars the plain ones
+    std::string base = t;
+    if (vector) {
+        if (t.size() < 2 || t.back() != 'V')
+            throw ConfigError("option " + k + ": vector reconstruction needs a V-limiter (e.g. OSPREV), got '" + t + "'", true);
+        base = t.substr(0, t.size() - 1);
+    }
+    if (base == "OSPRE") return LIM_OSPRE;
+    if (base == "vanLeer") return LIM_VANLEER;
+    if (base == "Minmod") return LIM_MINMOD;
+    if (base == "vanAlbada") return LIM_VANALBADA;
+    if (base == "SuperBee") return LIM_SUPERBEE;
+    if (base == "MUSCL") return LIM_MUSCL;
+    throw ConfigError("option " + k + ": unknown interpolation scheme '" + t + "'");
+}
+
+inline FluxScheme parse_flux(const std::string& v) {
+    std::string t = trim(v);
+    if (t == "Kurganov") return FLUX_KURGANOV;
+    if (t == "HLL") return FLUX_HLL;
+    if (t == "HLLC") return FLUX_HLLC;
+    if (t == "HLLCP") return FLUX_HLLCP;
+    if (t == "AUSM+") return FLUX_AUSMPLUS;
+    if (t == "AUSM+up") return FLUX_AUSMPLUSUP;
+    if (t == "AUSM") return FLUX_AUSM;
+    throw ConfigError("Unknown fluxScheme type " + t +
+                      "\nValid fluxScheme types are: (AUSM AUSM+ AUSM+up HLL HLLC HLLCP Kurganov)");
+}
+
+inline Options parse_options(int n, const char* const* keys, const char* const* values) {
+    Options o;
+    std::map<std::string, std::string> kv;
+    for (int i = 0; i < n; ++i) {
+        if (!keys[i] || !values[i]) throw ConfigError("null option key/value");
+        kv[trim(keys[i])] = values[i];
+    }
+    for (auto& it : kv) {
+        const std::string& k = it.first;
+        const std::string& v = it.second;
+        std::string t = trim(v);
+        if (k == "fluxScheme") { o.flux = parse_flux(v); o.flux_given = true; }
+        else if (k == "Jacobian") {
+            if (t != "Roe") throw ConfigError("Unknown Jacobian type " + t + "\nValid Jacobian types are: (Roe)");
+            o.jacobian = t;
+        }
+        else if (k == "dependentVariable") {
+            if (t == "W") o.dependent_W = true;
+            else if (t == "deltaW") o.dependent_W = false;
+            else throw ConfigError("dependentVariable must be W or deltaW");
+        }
+        else if (k == "timeIntegration.timeIntegration") {
+            if (t == "Dual") throw ConfigError("timeIntegration Dual (dual-time stepping) is not on this path", true);
+            if (t != "Single" && t != "GPU")
+                throw ConfigError("Unknown timeIntegration type " + t + "\nValid timeIntegration types are: (Dual Single)");
+        }
+        else if (k == "timeIntegration.beta") o.beta = parse_double(k, v);
+        else if (k == "timeIntegration.innerCorrectTurbulence" || k == "timeIntegration.maxInnerIter") {}
+        else if (k == "timeControls.adjustTimeStep") o.adjust_time_step = parse_bool(k, v);
+        else if (k == "timeControls.neighbouring") o.neighbouring = parse_bool(k, v);
+        else if (k == "timeControls.initialCo") o.initial_co = parse_double(k, v);
+        else if (k == "timeControls.minCo") o.min_co = parse_double(k, v);
+        else if (k == "timeControls.maxCo") o.max_co = parse_double(k, v);
+        else if (k.rfind("residualControls.", 0) == 0) {}
+        else if (k == "directWaveSpeed") {
+            o.direct_wave_speed = parse_bool(k, v);
+            if (!o.direct_wave_speed)
+                throw ConfigError("directWaveSpeed false leaves the HLLC wave speeds unset in the reference (HLLCDST.C:188-215); rejected", true);
+        }
+        else if (k == "lowMach") o.low_mach = parse_bool(k, v);
+        else if (k == "Mainf") o.mainf = parse_double(k, v);
+        else if (k == "addSpectralRadiusToPhysicalBoundaries") parse_bool(k, v);
+        else if (k == "venkatakrishnanK") o.venkat_K = parse_double(k, v);
+        else if (k == "ddtSchemes.default") {
+            if (t == "Euler") o.ddt = DDT_EULER;
+            else if (t == "steadyStateDST") o.ddt = DDT_STEADY;
+            else if (t == "dual2ndDST") throw ConfigError("ddt dual2ndDST belongs to dual-time stepping, not on this path", true);
+            else throw ConfigError("Unknown ddtScheme " + t + "\nValid ddt schemes are: (Euler steadyStateDST dual2ndDST)");
+        }
+        else if (k == "interpolationSchemes.reconstruct(rho)") o.lim_rho = parse_limiter(k, v, false);
+        else if (k == "interpolationSchemes.reconstruct(U)") o.lim_U = parse_limiter(k, v, true);
+        else if (k == "interpolationSchemes.reconstruct(T)") o.lim_T = parse_limiter(k, v, false);
+        else if (k == "solvers.W.solver") {
+            if (t == "GMRES") o.solver = SOLVER_GMRES;
+            else if (t == "BiCGStab") o.solver = SOLVER_BICGSTAB;
+            else if (t == "AMG" || t == "CG" || t == "GaussSeidel" || t == "ILU" || t == "Cholesky" || t == "SAMG")
+                throw ConfigError("block solver " + t + " is not on this path (GMRES, BiCGStab)", true);
+            else throw ConfigError("Unknown block solver " + t + "\nValid solvers are: (BiCGStab GMRES)");
+        }
+        else if (k == "solvers.W.preconditioner") {
+            if (t == "ILUC0" || t == "ILU0" || t == "Cholesky") o.precon = PRECON_ILU0;
+            else if (t == "diagonal" || t == "Jacobi") o.precon = PRECON_DIAGONAL;
+            else if (t == "none") o.precon = PRECON_NONE;
+            else if (t == "AMG" || t == "ILUCp" || t == "GaussSeidel" || t == "SAMG")
+                throw ConfigError("preconditioner " + t + " is not on this path (ILUC0, diagonal, none)", true);
+            else throw ConfigError("Unknown block preconditioner " + t);
+        }
+        else if (k == "solvers.W.nDirections") o.n_directions = parse_int(k, v);
+        else if (k == "solvers.W.tolerance") o.tolerance = parse_double(k, v);
+        else if (k == "solvers.W.relTol") o.rel_tol = parse_double(k, v);
+        else if (k == "solvers.W.maxIter") o.max_iter = parse_int(k, v);
+        else if (k == "solvers.W.minIter") o.min_iter = parse_int(k, v);
+        else if (k == "fieldBounds.rho") parse_pair(k, v, o.rho_min, o.rho_max);
+        else if (k == "fieldBounds.p") parse_pair(k, v, o.p_min, o.p_max);
+        else if (k == "fieldBounds.T") parse_pair(k, v, o.T_min, o.T_max);
+        else if (k == "thermo.R") o.R = parse_double(k, v);
+        else if (k == "thermo.Cp") o.Cp = parse_double(k, v);
+        else if (k == "transport.mu") o.mu = parse_double(k, v);
+        else if (k == "transport.Pr") o.Pr = parse_double(k, v);
+        else if (k == "transport.As") o.As = parse_double(k, v);
+        else if (k == "transport.Ts") o.Ts = parse_double(k, v);
+        else if (k == "transport.Prt") o.Prt = parse_double(k, v);
+        else if (k == "RASModel" || k == "turbulence") {
+            if (t == "laminar") o.turbulence = TURB_LAMINAR;
+            else if (t == "SAneg") o.turbulence = TURB_SANEG;
+            else if (t == "SARC1") o.turbulence = TURB_SARC1;
+            else if (t == "SARC2") o.turbulence = TURB_SARC2;
+            else throw ConfigError("Unknown RASModel " + t + "\nValid models are: (laminar SAneg SARC1 SARC2)");
+        }
+        else if (k == "controlDict.deltaT") o.delta_t = parse_double(k, v);
+        else if (k == "controlDict.startTime") o.start_time = parse_double(k, v);
+        else if (k == "precision") {
+            if (t == "fp64") o.precision = PREC_FP64;
+            else if (t == "fp32") o.precision = PREC_FP32;
+            else if (t == "bf16") o.precision = PREC_BF16;
+            else throw ConfigError("precision must be fp64, fp32 or bf16");
+        }
+        else if (k == "ilu.parts") o.ilu_parts = parse_int(k, v);
+        else if (k == "graphs") o.graphs = parse_bool(k, v);
+        else if (k == "profile") o.profile = parse_bool(k, v);
+        else throw ConfigError("unknown option '" + k + "'");
+    }
+    if (!o.flux_given) throw ConfigError("keyword fluxScheme is undefined in dictionary rhoDSTDict");
+    if (o.n_directions < 1 || o.n_directions > 64) throw ConfigError("solvers.W.nDirections must be in [1,64]");
+    if (o.max_iter < 0 || o.min_iter < 0) throw ConfigError("solvers.W.maxIter/minIter must be >= 0");
+    if (!(o.R > 0) || !(o.Cp > o.R)) throw ConfigError("thermo: need 0 < R < Cp");
+    if (o.lim_U == LIM_VENKATAKRISHNAN) {}
+    return o;
+}
+
+// foam-extend scalar constants (double precision build)
+constexpr double SMALL = 1.0e-15;
+constexpr double VSMALL = 1.0e-300;
+constexpr double SOLVER_SMALL = 1.0e-20;   // lduMatrix::small_ in normFactor
+
+}  // namespace rdst

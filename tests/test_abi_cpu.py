@@ -1,0 +1,72 @@
+"""C ABI checks that need no GPU: the library loads, exports every symbol
+the header declares, host-only entry points work, and configuration errors
+are reported with the reference's selector semantics before any device
+work."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import rhodst_b200
+from rhodst_b200 import _abi, cases
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def header_functions():
+    text = (ROOT / "include" / "rdst.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rdst_[a-z_]+)\s*\(", text)))
+
+
+def test_header_symbols_exported(gpulib):
+    names = header_functions()
+    assert "rdst_step" in names and "rdst_create" in names
+    for n in names:
+        assert hasattr(gpulib, n), n
+
+
+def test_version(gpulib):
+    assert b"sm_100a" in gpulib.rdst_version()
+
+
+def test_partition_host_only():
+    m = cases.forward_step_c1().mesh
+    part = rhodst_b200.partition_cells(m.C, 8)
+    counts = np.bincount(part, minlength=8)
+    assert counts.sum() == m.n_cells and counts.min() >= m.n_cells // 8 - 1
+    part2 = rhodst_b200.partition_cells(m.C, 8)
+    assert np.array_equal(part, part2)
+
+
+@pytest.mark.parametrize("key,value,status", [
+    ("fluxScheme", "Roe", 1),                      # unknown selector -> FatalError analogue
+    ("Jacobian", "Steger", 1),
+    ("solvers.W.solver", "AMG", 6),                # selectable in foam, not on this path
+    ("directWaveSpeed", "false", 6),               # latent reference bug rejected
+    ("ddtSchemes.default", "dual2ndDST", 6),
+    ("timeIntegration.timeIntegration", "Dual", 6),
+    ("interpolationSchemes.reconstruct(U)", "OSPRE", 6),
+    ("solvers.W.nDirections", "0", 1),
+])
+def test_config_errors(key, value, status):
+    case = cases.forward_step_c1().with_options(**{key: value})
+    with pytest.raises(_abi.RdstError) as e:
+        rhodst_b200.Solver(case.mesh, case.bcs, case.options)
+    assert e.value.status == status
+
+
+def test_missing_flux_scheme():
+    case = cases.forward_step_c1()
+    opts = dict(case.options)
+    del opts["fluxScheme"]
+    with pytest.raises(_abi.RdstError) as e:
+        rhodst_b200.Solver(case.mesh, case.bcs, opts)
+    assert e.value.status == 1
+
+
+def test_flatten_options():
+    f = _abi.flatten_options({"a": {"b": True, "c": (1.0, 2)}, "d": 1e-3})
+    assert f == {"a.b": "true", "a.c": "1.0 2", "d": "0.001"}
