@@ -144,6 +144,9 @@ struct Ctx {
     // boundary values (indexed by boundary face b = f - Fi)
     std::vector<double> rho_b, rhoE_b, p_b, T_b, h_b, phi_b;
     std::vector<v3> rhoU_b, U_b;
+    // valueFraction of the mixed-type BCs at their last evaluation
+    // (used by valueInternalCoeffs in the boundary Jacobian)
+    std::vector<double> fp_b, fU_b, fT_b;
     // residual R_ (baseFluxDST R_, per unit volume) and face fluxes
     std::vector<v5> Rv;
     std::vector<double> phi, phiEp;
@@ -172,27 +175,69 @@ void eval_boundary(Ctx& c) {
         const int ci = c.own[f];
         const v3 n = c.Sf[f] / c.magSf[f];
         const bool outflow = c.phi_b[b] >= 0.0;
+        const v3& Ui = c.U[ci];
+        double fp = 0, fU = 0, fT = 0;
+        // characteristic far field (farField*DSTFvPatch*Field.C:144-221):
+        // boundary Mach from the last boundary mass flux, rho_b and c_b
+        double supIn = 0, supOut = 0, subIn = 0, subOut = 0, rho0c0 = 0, cI = 0, pbU = 0;
+        if (P.bc_p == RDST_BC_FARFIELD || P.bc_U == RDST_BC_FARFIELD || P.bc_T == RDST_BC_FARFIELD) {
+            double cb = std::sqrt(c.gamma * c.R * c.T_b[b]);
+            cI = std::sqrt(c.gamma * c.R * c.T[ci]);
+            double mach = c.phi_b[b] / c.rho_b[b] / c.magSf[f] / cb;
+            supIn = neg0(mach + 1);
+            supOut = pos0(mach - 1);
+            subIn = neg(mach) - supIn;
+            subOut = pos0(mach) - supOut;
+            rho0c0 = c.rho[ci] * cI;
+            pbU = 0.5 * (P.p_value + c.p[ci] - rho0c0 * dot(n, P.U_value - Ui));
+        }
         // p
         switch (P.bc_p) {
-            case RDST_BC_FIXED_VALUE: c.p_b[b] = P.p_value; break;
-            case RDST_BC_INLET_OUTLET: c.p_b[b] = outflow ? c.p[ci] : P.p_value; break;
+            case RDST_BC_FIXED_VALUE: c.p_b[b] = P.p_value; fp = 1; break;
+            case RDST_BC_INLET_OUTLET: fp = outflow ? 0.0 : 1.0; c.p_b[b] = outflow ? c.p[ci] : P.p_value; break;
+            case RDST_BC_FARFIELD: {
+                double pb = P.p_value - rho0c0 * dot(n, P.U_value - Ui);
+                double ref = supIn * P.p_value + subIn * pb + subOut * P.p_value;
+                fp = 1 - supOut - 0.5 * subIn;
+                c.p_b[b] = fp * ref + (1 - fp) * c.p[ci];
+                break;
+            }
             default: c.p_b[b] = c.p[ci]; break;
         }
         // T
         switch (P.bc_T) {
-            case RDST_BC_FIXED_VALUE: c.T_b[b] = P.T_value; break;
-            case RDST_BC_INLET_OUTLET: c.T_b[b] = outflow ? c.T[ci] : P.T_value; break;
+            case RDST_BC_FIXED_VALUE: c.T_b[b] = P.T_value; fT = 1; break;
+            case RDST_BC_INLET_OUTLET: fT = outflow ? 0.0 : 1.0; c.T_b[b] = outflow ? c.T[ci] : P.T_value; break;
+            case RDST_BC_FARFIELD: {
+                double TI = c.T[ci], pI = c.p[ci], rhoI = c.rho[ci];
+                double RI = pI / rhoI / TI;
+                double rhoa = P.p_value / P.T_value / RI;
+                double subsInValue = pbU / (rhoa + (pbU - P.p_value) / sqr(cI)) / RI;
+                double sOVF = pbU / (pI + RI * TI * (pbU - pI) / sqr(cI));
+                double ref = supIn * P.T_value + subIn * subsInValue;
+                fT = 1 - supOut - sOVF * subOut;
+                c.T_b[b] = fT * ref + (1 - fT) * TI;
+                break;
+            }
             default: c.T_b[b] = c.T[ci]; break;
         }
         // U
-        const v3& Ui = c.U[ci];
         switch (P.bc_U) {
-            case RDST_BC_FIXED_VALUE: c.U_b[b] = P.U_value; break;
-            case RDST_BC_INLET_OUTLET: c.U_b[b] = outflow ? Ui : P.U_value; break;
+            case RDST_BC_FIXED_VALUE: c.U_b[b] = P.U_value; fU = 1; break;
+            case RDST_BC_INLET_OUTLET: fU = outflow ? 0.0 : 1.0; c.U_b[b] = outflow ? Ui : P.U_value; break;
             case RDST_BC_SYMMETRY:
             case RDST_BC_SLIP: c.U_b[b] = Ui - dot(n, Ui) * n; break;
+            case RDST_BC_FARFIELD: {
+                v3 subsIn = P.U_value - ((P.p_value - pbU) / rho0c0) * n;
+                v3 subsOut = ((c.p[ci] - pbU) / rho0c0) * n;
+                v3 ref = supIn * P.U_value + subIn * subsIn + subOut * subsOut;
+                fU = 1 - supOut - subOut;
+                c.U_b[b] = fU * ref + (1 - fU) * Ui;
+                break;
+            }
             default: c.U_b[b] = Ui; break;
         }
+        c.fp_b[b] = fp; c.fU_b[b] = fU; c.fT_b[b] = fT;
         // bounding of the boundary pressure (boundMinMax acts on the patch values too)
         c.p_b[b] = std::min(std::max(c.p_b[b], c.o.p_min), c.o.p_max);
         c.h_b[b] = c.Cp * c.T_b[b];
@@ -203,29 +248,21 @@ void eval_boundary(Ctx& c) {
     }
 }
 
-// valueInternalCoeffs(weights) of each BC (used by Roe.C:363-365):
-// fixedValue 0, zeroGradient 1, inletOutlet 1 - valueFraction,
-// symmetry/slip: scalar 1, vector 1 - |n_i| per component.
+// valueInternalCoeffs(weights) of each BC (used by Roe.C:363-365): mixed
+// types (fixedValue f=1, zeroGradient f=0, inletOutlet, far field) give
+// 1 - valueFraction from their last evaluation; symmetry/slip vectors
+// 1 - |n_i| per component (basicSymmetry), scalars 1.
 void internal_coeffs(const Ctx& c, int b, double& cp, v3& cu, double& cT) {
     const int f = c.Fi + b;
     const Patch& P = c.patches[c.bpatch[b]];
     const v3 n = c.Sf[f] / c.magSf[f];
-    const double outflow = pos0(c.phi_b[b]);
-    auto sc = [&](int bc) {
-        switch (bc) {
-            case RDST_BC_FIXED_VALUE: return 0.0;
-            case RDST_BC_INLET_OUTLET: return outflow;
-            default: return 1.0;
-        }
-    };
-    cp = sc(P.bc_p);
-    cT = sc(P.bc_T);
-    switch (P.bc_U) {
-        case RDST_BC_FIXED_VALUE: cu = {0, 0, 0}; break;
-        case RDST_BC_INLET_OUTLET: cu = {outflow, outflow, outflow}; break;
-        case RDST_BC_SYMMETRY:
-        case RDST_BC_SLIP: cu = {1 - std::fabs(n[0]), 1 - std::fabs(n[1]), 1 - std::fabs(n[2])}; break;
-        default: cu = {1, 1, 1}; break;
+    cp = 1.0 - c.fp_b[b];
+    cT = 1.0 - c.fT_b[b];
+    if (P.bc_U == RDST_BC_SYMMETRY || P.bc_U == RDST_BC_SLIP)
+        cu = {1 - std::fabs(n[0]), 1 - std::fabs(n[1]), 1 - std::fabs(n[2])};
+    else {
+        double u = 1.0 - c.fU_b[b];
+        cu = {u, u, u};
     }
 }
 
@@ -1364,6 +1401,7 @@ ORACLE_API rdst_status rdsto_create(const rdst_mesh* m, int32_t n_opts, const ch
     c.rhoU.assign(Nn, v3{0, 0, 0}); c.U.assign(Nn, v3{0, 0, 0});
     c.rho_b.assign(NB, 0); c.rhoE_b.assign(NB, 0); c.p_b.assign(NB, 0); c.T_b.assign(NB, 0);
     c.h_b.assign(NB, 0); c.phi_b.assign(NB, 0); c.rhoU_b.assign(NB, v3{0, 0, 0}); c.U_b.assign(NB, v3{0, 0, 0});
+    c.fp_b.assign(NB, 0); c.fU_b.assign(NB, 0); c.fT_b.assign(NB, 0);
     *out = h.release();
     return RDST_OK;
 }
@@ -1382,10 +1420,12 @@ static void init_from_primitive(Ctx& c) {
         c.rhoU[i] = c.rho[i] * c.U[i];
         c.rhoE[i] = c.rho[i] * (c.h[i] * c.Cv / c.Cp + 0.5 * magSqr(c.U[i]));
     }
-    // initial boundary mass flux for inletOutlet: (rho U)_owner . Sf
+    // initial boundary state (before the first BC evaluation): internal
+    // values and mass flux (rho U)_owner . Sf
     for (int b = 0; b < c.NB; ++b) {
-        int f = c.Fi + b;
-        c.phi_b[b] = dot(c.rhoU[c.own[f]], c.Sf[f]);
+        int f = c.Fi + b, ci = c.own[f];
+        c.phi_b[b] = dot(c.rhoU[ci], c.Sf[f]);
+        c.rho_b[b] = c.rho[ci]; c.T_b[b] = c.T[ci]; c.p_b[b] = c.p[ci]; c.U_b[b] = c.U[ci];
     }
     eval_boundary(c);
     initialize_time(c);

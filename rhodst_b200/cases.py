@@ -117,7 +117,7 @@ def naca0012_inviscid(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: fl
     options = {
         "fluxScheme": flux,
         "Jacobian": "Roe",
-        "timeControls": {"neighbouring": False, "initialCo": 50.0, "minCo": 0.1, "maxCo": 50.0},
+        "timeControls": {"neighbouring": False, "initialCo": 2.0, "minCo": 0.1, "maxCo": 50.0},
         "ddtSchemes": {"default": "steadyStateDST"},
         "interpolationSchemes": {"reconstruct(rho)": limiter, "reconstruct(U)": vlim,
                                  "reconstruct(T)": limiter},
@@ -131,4 +131,44 @@ def naca0012_inviscid(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: fl
     al = math.radians(alpha)
     return Case("naca0012", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N), steps=2000,
                 force_patch="airfoil",
+                force_dirs={"lift": (-math.sin(al), math.cos(al), 0.0), "drag": (math.cos(al), math.sin(al), 0.0)})
+
+
+def swept_wing_c3(n_around: int = 192, n_normal: int = 64, n_span: int = 64, n_tip: int = 34,
+                  precision: str = "fp64", n_directions: int = 20, flux: str = "HLLC",
+                  ilu_parts: int = 0) -> Case:
+    """Inviscid swept, tapered NACA0012 wing (taper 0.56, LE sweep 30 deg,
+    semi-span 1.5 root chords) at Mach 0.84, alpha 3.06 deg, HLLC,
+    OSPRE/OSPREV reconstruction, characteristic far field, local time
+    stepping (steadyStateDST, CFL ramp to 50), block-GMRES with subdomain
+    ILU(0); the Jacobian/ILU factors stored in `precision` (fp64 | fp32 |
+    bf16) inside the FP64 defect-correction step.  Default mesh 1.2 M cells."""
+    m = _mesh.swept_wing_oh(n_around, n_normal, n_span, n_tip)
+    gas = dict(NORMALISED_GAS)
+    U0 = farfield_state(0.84, 3.06, 1.0, 1.0, gas)
+    bcs = {
+        "wing": {"p": "zeroGradient", "U": "slip", "T": "zeroGradient"},
+        "farfield": {"p": ("farField", 1.0), "U": ("farField", U0), "T": ("farField", 1.0)},
+        "symmetry": {"p": "symmetryPlane", "U": "symmetryPlane", "T": "symmetryPlane"},
+    }
+    options = {
+        "fluxScheme": flux,
+        "Jacobian": "Roe",
+        "timeControls": {"neighbouring": False, "initialCo": 5.0, "minCo": 0.1, "maxCo": 50.0},
+        "ddtSchemes": {"default": "steadyStateDST"},
+        "interpolationSchemes": {"reconstruct(rho)": "OSPRE", "reconstruct(U)": "OSPREV",
+                                 "reconstruct(T)": "OSPRE"},
+        "solvers": {"W": {"solver": "GMRES", "preconditioner": "ILUC0",
+                          "nDirections": n_directions, "tolerance": 1e-12, "relTol": 0.0,
+                          "maxIter": 1, "minIter": 1}},
+        "fieldBounds": {"rho": (1e-3, 1e4), "p": (1e-3, 1e4), "T": (1e-3, 1e4)},
+        "thermo": gas,
+        "precision": precision,
+    }
+    if ilu_parts:
+        options["ilu"] = {"parts": ilu_parts}
+    N = m.n_cells
+    al = math.radians(3.06)
+    return Case("sweptWing", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N), steps=2000,
+                force_patch="wing",
                 force_dirs={"lift": (-math.sin(al), math.cos(al), 0.0), "drag": (math.cos(al), math.sin(al), 0.0)})

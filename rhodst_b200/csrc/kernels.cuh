@@ -86,19 +86,28 @@ __global__ void k_init_state(int N, Thermo th, const double* __restrict__ prim, 
     W[5 * i + 4] = rho * (h * th.Cv / th.Cp + 0.5 * magSqr3(U));
 }
 
-// boundary mass flux before the first flux evaluation: (rho U)_owner . Sf
-__global__ void k_init_phib(DevMesh m, const double* __restrict__ W, double* __restrict__ bs) {
+// boundary state before the first BC evaluation: internal values and the
+// mass flux (rho U)_owner . Sf
+__global__ void k_init_phib(DevMesh m, const double* __restrict__ W, const double* __restrict__ prim,
+                            double* __restrict__ bs) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.NB) return;
     int c = m.bcell[b];
     V3 S = ldv3(m.bSf, m.NB, b);
-    bs[BW * b + 7] = dot3(mk(W[5 * c + 1], W[5 * c + 2], W[5 * c + 3]), S);
+    double* B = bs + BW * b;
+    B[7] = dot3(mk(W[5 * c + 1], W[5 * c + 2], W[5 * c + 3]), S);
+    B[0] = W[5 * c];
+    B[5] = prim[PW * c];
+    B[6] = prim[PW * c + 1];
 }
 
 // Boundary values of p, U, T from the internal field (fixedValue,
-// zeroGradient, inletOutlet, symmetryPlane/slip, characteristic far field)
-// and rho/rhoU/rhoE rebuilt as updateFields.H:84-93.
-__global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __restrict__ prim, double* __restrict__ bs) {
+// zeroGradient, inletOutlet, symmetryPlane/slip, characteristic far field
+// of farField*DSTFvPatch*Field.C:144-221) and rho/rhoU/rhoE rebuilt as
+// updateFields.H:84-93.  The valueFractions are stored for the boundary
+// Jacobian (valueInternalCoeffs = 1 - valueFraction).
+__global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __restrict__ W,
+                           const double* __restrict__ prim, double* __restrict__ bs) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.NB) return;
     const DevPatch P = m.patches[m.bpatch[b]];
@@ -109,31 +118,70 @@ __global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __rest
     const double* Pi = prim + PW * ci;
     double pI = Pi[0], TI = Pi[1];
     V3 Ui = mk(Pi[3], Pi[4], Pi[5]);
-    bool outflow = bs[BW * b + 7] >= 0.0;
-    double pb, Tb;
+    double* B = bs + BW * b;
+    bool outflow = B[7] >= 0.0;
+    const V3 UInf = mk(P.U_value[0], P.U_value[1], P.U_value[2]);
+    double supIn = 0, supOut = 0, subIn = 0, subOut = 0, rho0c0 = 0, cI = 0, pbU = 0;
+    if (P.bc_p == 5 || P.bc_U == 5 || P.bc_T == 5) {
+        double cb = sqrt(th.gamma * th.R * B[6]);
+        cI = sqrt(th.gamma * th.R * TI);
+        double mach = B[7] / B[0] / magS / cb;
+        supIn = dneg0(mach + 1);
+        supOut = dpos0(mach - 1);
+        subIn = dneg(mach) - supIn;
+        subOut = dpos0(mach) - supOut;
+        rho0c0 = W[5 * ci] * cI;
+        pbU = 0.5 * (P.p_value + pI - rho0c0 * dot3(n, sub3(UInf, Ui)));
+    }
+    double pb, Tb, fp = 0, fU = 0, fT = 0;
     V3 Ub;
     switch (P.bc_p) {
-        case 0: pb = P.p_value; break;
-        case 2: pb = outflow ? pI : P.p_value; break;
+        case 0: pb = P.p_value; fp = 1; break;
+        case 2: fp = outflow ? 0.0 : 1.0; pb = outflow ? pI : P.p_value; break;
+        case 5: {
+            double pbp = P.p_value - rho0c0 * dot3(n, sub3(UInf, Ui));
+            double ref = supIn * P.p_value + subIn * pbp + subOut * P.p_value;
+            fp = 1 - supOut - 0.5 * subIn;
+            pb = fp * ref + (1 - fp) * pI;
+            break;
+        }
         default: pb = pI; break;
     }
     switch (P.bc_T) {
-        case 0: Tb = P.T_value; break;
-        case 2: Tb = outflow ? TI : P.T_value; break;
+        case 0: Tb = P.T_value; fT = 1; break;
+        case 2: fT = outflow ? 0.0 : 1.0; Tb = outflow ? TI : P.T_value; break;
+        case 5: {
+            double rhoI = W[5 * ci];
+            double RI = pI / rhoI / TI;
+            double rhoa = P.p_value / P.T_value / RI;
+            double subsInValue = pbU / (rhoa + (pbU - P.p_value) / sq(cI)) / RI;
+            double sOVF = pbU / (pI + RI * TI * (pbU - pI) / sq(cI));
+            double ref = supIn * P.T_value + subIn * subsInValue;
+            fT = 1 - supOut - sOVF * subOut;
+            Tb = fT * ref + (1 - fT) * TI;
+            break;
+        }
         default: Tb = TI; break;
     }
     switch (P.bc_U) {
-        case 0: Ub = mk(P.U_value[0], P.U_value[1], P.U_value[2]); break;
-        case 2: Ub = outflow ? Ui : mk(P.U_value[0], P.U_value[1], P.U_value[2]); break;
+        case 0: Ub = UInf; fU = 1; break;
+        case 2: fU = outflow ? 0.0 : 1.0; Ub = outflow ? Ui : UInf; break;
         case 3:
         case 4: Ub = sub3(Ui, scl3(dot3(n, Ui), n)); break;
+        case 5: {
+            V3 subsIn = sub3(UInf, scl3((P.p_value - pbU) / rho0c0, n));
+            V3 subsOut = scl3((pI - pbU) / rho0c0, n);
+            V3 ref = add3(add3(scl3(supIn, UInf), scl3(subIn, subsIn)), scl3(subOut, subsOut));
+            fU = 1 - supOut - subOut;
+            Ub = add3(scl3(fU, ref), scl3(1 - fU, Ui));
+            break;
+        }
         default: Ub = Ui; break;
     }
     pb = fmin(fmax(pb, bd.p_min), bd.p_max);
     double hb = th.Cp * Tb;
     double psib = 1.0 / (th.R * Tb);
     double rhob = pb * psib;
-    double* B = bs + BW * b;
     B[0] = rhob;
     B[1] = rhob * Ub.x;
     B[2] = rhob * Ub.y;
@@ -141,6 +189,9 @@ __global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __rest
     B[4] = rhob * (hb + 0.5 * magSqr3(Ub)) - pb;
     B[5] = pb;
     B[6] = Tb;
+    B[8] = fp;
+    B[9] = fU;
+    B[10] = fT;
 }
 
 // ------------------------------------------------------------------ residual
@@ -537,17 +588,13 @@ __global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, SellMat<
             dX[20] = rRhoCv * (0.5 * magSqr3(UI) - e);
             for (int l = 0; l < 3; ++l) dX[21 + l] = -rRhoCv * UIv[l];
             dX[24] = rRhoCv;
-            // valueInternalCoeffs
-            double outflow = dpos0(B[7]);
-            auto sc_ = [&](int bc) { return bc == 0 ? 0.0 : (bc == 2 ? outflow : 1.0); };
+            // valueInternalCoeffs: 1 - valueFraction (mixed types), basicSymmetry
             double cdiag[5];
-            cdiag[0] = sc_(P.bc_p);
-            cdiag[4] = sc_(P.bc_T);
-            if (P.bc_U == 0) { cdiag[1] = cdiag[2] = cdiag[3] = 0.0; }
-            else if (P.bc_U == 2) { cdiag[1] = cdiag[2] = cdiag[3] = outflow; }
-            else if (P.bc_U == 3 || P.bc_U == 4) {
+            cdiag[0] = 1.0 - B[8];
+            cdiag[4] = 1.0 - B[10];
+            if (P.bc_U == 3 || P.bc_U == 4) {
                 cdiag[1] = 1 - fabs(nrm.x); cdiag[2] = 1 - fabs(nrm.y); cdiag[3] = 1 - fabs(nrm.z);
-            } else { cdiag[1] = cdiag[2] = cdiag[3] = 1.0; }
+            } else { cdiag[1] = cdiag[2] = cdiag[3] = 1.0 - B[9]; }
             // pic = (dR . diag(cdiag)) . dX
             for (int a = 0; a < 5; ++a) {
                 double t1[5];
@@ -738,7 +785,7 @@ __global__ void k_store_old(int N, const double* __restrict__ W, const double* _
 __global__ void k_time_advance(Scalars* sc) {
     if (threadIdx.x == 0) {
         sc->time += sc->deltaT;
-        sc->flags = 0;
+        sc->flags &= ~1;       // bounding flag per step; bit1 (non-physical) stays set
     }
 }
 

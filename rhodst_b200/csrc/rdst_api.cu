@@ -87,8 +87,11 @@ void rcb(const double* C, std::vector<int>& idx, int lo, int hi, int part0, int 
 
 struct Report5 { rdst_step_report r; };
 
-__global__ void k_report(const Scalars* sc, rdst_step_report* reps, int idx, double dt_used_from_prev) {
+// report of the current step into reps[sc->step_idx]; advances the slot
+__global__ void k_report(Scalars* sc, rdst_step_report* reps, int cap) {
     if (threadIdx.x != 0) return;
+    int idx = sc->step_idx;
+    if (idx >= cap) return;
     rdst_step_report& r = reps[idx];
     r.time = sc->time;
     r.courant = sc->courant;
@@ -103,17 +106,18 @@ __global__ void k_report(const Scalars* sc, rdst_step_report* reps, int idx, dou
     r.rdt_min = sc->rdt_min;
     r.rdt_max = sc->rdt_max;
     r.t_flux_ms = r.t_jacobian_ms = r.t_precond_ms = r.t_krylov_ms = r.t_update_ms = 0.0;
+    sc->step_idx = idx + 1;
 }
 
-__global__ void k_report_dt(const Scalars* sc, rdst_step_report* reps, int idx) {
-    if (threadIdx.x == 0) reps[idx].deltaT = sc->deltaT;
+__global__ void k_report_dt(const Scalars* sc, rdst_step_report* reps, int cap) {
+    if (threadIdx.x == 0 && sc->step_idx < cap) reps[sc->step_idx].deltaT = sc->deltaT;
 }
 
-__global__ void k_mean_courant(const double* __restrict__ cf, int N, rdst_step_report* reps, int idx) {
+__global__ void k_mean_courant(const double* __restrict__ cf, int N, const Scalars* sc, rdst_step_report* reps, int cap) {
     double s = 0;
     for (int i = threadIdx.x; i < N; i += blockDim.x) s += cf[i];
     s = block_sum(s);
-    if (threadIdx.x == 0) reps[idx].courant = s / N;
+    if (threadIdx.x == 0 && sc->step_idx < cap) reps[sc->step_idx].courant = s / N;
 }
 
 }  // namespace
@@ -159,13 +163,20 @@ struct rdst_ctx {
     int limiter_need_grad = 1, venkat_mask = 0;
     bool steady = false;
     bool state_set = false;
-    // graphs
-    cudaGraphExec_t g_pre = nullptr, g_cycle = nullptr, g_post = nullptr;
-    bool graphs_ok = false;
+    // graphs: whole step (fixed iteration count) or pre / one iteration / post
+    struct EvRec { cudaEvent_t a, b; int kind; };
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        long launches = 0;
+        std::vector<EvRec> events;   // external event records inside the graph
+    };
+    Graph g_step, g_pre, g_cycle, g_post;
+    bool capturing = false;
+    std::vector<EvRec>* capture_events = nullptr;
+    static constexpr int REP_CAP = 1024;
     // instrumentation
     long launches = 0;
     std::vector<cudaEvent_t> ev_pool;
-    struct EvRec { cudaEvent_t a, b; int kind; };
     std::vector<EvRec> ev_pending;
     long ks_launches[KS_N] = {0, 0, 0, 0, 0, 0, 0};
     double ks_ms[KS_N] = {0, 0, 0, 0, 0, 0, 0};
@@ -176,6 +187,14 @@ struct rdst_ctx {
         cudaEvent_t e;
         CK(cudaEventCreate(&e));
         return e;
+    }
+    void collect_graph_events(const Graph& g) {
+        for (auto& r : g.events) {
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, r.a, r.b));
+            ks_ms[r.kind] += ms;
+            ks_launches[r.kind] += 1;
+        }
     }
     void collect_events() {
         for (auto& r : ev_pending) {
@@ -193,9 +212,10 @@ struct rdst_ctx {
         for (auto e : ev_pool) cudaEventDestroy(e);
         for (auto e : step_ev) if (e) cudaEventDestroy(e);
         for (auto& r : ev_pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
-        if (g_pre) cudaGraphExecDestroy(g_pre);
-        if (g_cycle) cudaGraphExecDestroy(g_cycle);
-        if (g_post) cudaGraphExecDestroy(g_post);
+        for (Graph* g : {&g_step, &g_pre, &g_cycle, &g_post}) {
+            if (g->exec) cudaGraphExecDestroy(g->exec);
+            for (auto& r : g->events) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+        }
         if (Aval) cudaFree(Aval);
         if (LUval) cudaFree(LUval);
         if (dinv) cudaFree(dinv);
@@ -228,10 +248,23 @@ struct Timed {
     int kind;
     cudaEvent_t a = nullptr;
     Timed(rdst_ctx& c_, int k) : c(c_), kind(k) {
-        if (c.o.profile) { a = c.get_event(); CK(cudaEventRecord(a, c.s)); }
+        if (!c.o.profile) return;
+        if (c.capturing) {
+            CK(cudaEventCreate(&a));
+            CK(cudaEventRecordWithFlags(a, c.s, cudaEventRecordExternal));
+        } else {
+            a = c.get_event();
+            CK(cudaEventRecord(a, c.s));
+        }
     }
     ~Timed() {
-        if (a) {
+        if (!a) return;
+        if (c.capturing) {
+            cudaEvent_t b;
+            cudaEventCreate(&b);
+            cudaEventRecordWithFlags(b, c.s, cudaEventRecordExternal);
+            c.capture_events->push_back({a, b, kind});
+        } else {
             cudaEvent_t b = c.get_event();
             cudaEventRecord(b, c.s);
             c.ev_pending.push_back({a, b, kind});
@@ -268,8 +301,6 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         d.type = P.type; d.bc_p = P.bc_p; d.bc_U = P.bc_U; d.bc_T = P.bc_T;
         d.p_value = P.p_value; d.T_value = P.T_value; d.nut_value = P.nuTilda_value;
         for (int k = 0; k < 3; ++k) d.U_value[k] = P.U_value[k];
-        if (P.bc_p == RDST_BC_FARFIELD || P.bc_U == RDST_BC_FARFIELD || P.bc_T == RDST_BC_FARFIELD)
-            throw ConfigError("farField boundary conditions are not built into this library yet", true);
         c.hpatch_start.push_back(P.start);
         c.hpatch_size.push_back(P.size);
     }
@@ -488,6 +519,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     c.R.alloc(5L * N); c.rhs.alloc(5L * N);
     c.rdt.alloc(N); c.courantF.alloc(N); c.rhoOld.alloc(N); c.eOld.alloc(N); c.eNew.alloc(N);
     c.sc.alloc(1); c.sc.zero(s);
+    c.reps.alloc(rdst_ctx::REP_CAP);
     int nbmax = std::max(nblk(std::max(N, Fi), TPB), red_blocks(5L * N));
     c.partial.alloc((size_t)std::max(nbmax, 1) * 72);
     c.bs.zero(s); c.W.zero(s); c.prim.zero(s); c.psi.zero(s); c.fcell.zero(s);
@@ -713,7 +745,7 @@ void post_update(rdst_ctx& c) {
         Timed tm(c, KS_UPDATE);
         k_update<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, c.dx.p, c.W.p, c.prim.p, c.sc.p); CKL();
     }
-    k_boundary<<<nblk(c.NB, TPB), TPB, 0, s>>>(c.m, c.th, c.bd, c.prim.p, c.bs.p); CKL();
+    k_boundary<<<nblk(c.NB, TPB), TPB, 0, s>>>(c.m, c.th, c.bd, c.W.p, c.prim.p, c.bs.p); CKL();
     k_courant_scalar<<<1, 1, 0, s>>>(c.sc.p, (!c.steady && c.o.adjust_time_step) ? 1 : 0, c.o.min_co, c.o.max_co); CKL();
     if (c.steady) {
         k_courant_cells<<<nblk(c.N, TPB), TPB, 0, s>>>(c.m, c.W.p, c.rhoOld.p, c.eOld.p, c.courantF.p, c.sc.p,
@@ -768,47 +800,133 @@ void pre_solve(rdst_ctx& c) {
 }
 
 template <typename MT>
+void iterations_direct(rdst_ctx& c) {
+    const Options& o = c.o;
+    int conv = 0;
+    const bool fixed = (o.min_iter >= o.max_iter);
+    if (!fixed && o.min_iter == 0) {
+        CK(cudaMemcpyAsync(&conv, &c.sc.p->converged, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        CK(cudaStreamSynchronize(c.s));
+    }
+    for (int it = 1; !conv && it <= o.max_iter; ++it) {
+        Ops<MT>::iteration(c);
+        if (it >= o.max_iter) break;
+        if (it >= o.min_iter) {
+            CK(cudaMemcpyAsync(&conv, &c.sc.p->converged, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+            CK(cudaStreamSynchronize(c.s));
+        }
+    }
+}
+
+template <typename MT>
+void step_head(rdst_ctx& c) {
+    k_report_dt<<<1, 1, 0, c.s>>>(c.sc.p, c.reps.p, rdst_ctx::REP_CAP);
+    CKL();
+    pre_solve<MT>(c);
+}
+
+void step_tail(rdst_ctx& c) {
+    post_update(c);
+    if (c.steady) { k_mean_courant<<<1, 256, 0, c.s>>>(c.courantF.p, c.N, c.sc.p, c.reps.p, rdst_ctx::REP_CAP); CKL(); }
+    k_report<<<1, 1, 0, c.s>>>(c.sc.p, c.reps.p, rdst_ctx::REP_CAP);
+    CKL();
+}
+
+template <typename Fn>
+void capture(rdst_ctx& c, rdst_ctx::Graph& g, Fn&& body) {
+    cudaGraph_t graph = nullptr;
+    long l0 = c.launches;
+    c.capturing = true;
+    c.capture_events = &g.events;
+    CK(cudaStreamBeginCapture(c.s, cudaStreamCaptureModeThreadLocal));
+    try {
+        body();
+    } catch (...) {
+        cudaStreamEndCapture(c.s, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        c.capturing = false;
+        throw;
+    }
+    CK(cudaStreamEndCapture(c.s, &graph));
+    c.capturing = false;
+    CK(cudaGraphInstantiate(&g.exec, graph, 0));
+    CK(cudaGraphDestroy(graph));
+    g.launches = c.launches - l0;
+    c.launches = l0;
+}
+
+void launch_graph(rdst_ctx& c, rdst_ctx::Graph& g) {
+    CK(cudaGraphLaunch(g.exec, c.s));
+    c.launches += g.launches;
+}
+
+template <typename MT>
 void run_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
     cudaStream_t s = c.s;
-    if ((int)c.reps.n < n) c.reps.alloc(n);
-    if (!c.step_ev[0]) { CK(cudaEventCreate(&c.step_ev[0])); CK(cudaEventCreate(&c.step_ev[1])); }
-    CK(cudaEventRecord(c.step_ev[0], s));
     const Options& o = c.o;
-    // a step needs no host round trip when the iteration count is fixed by
-    // minIter = maxIter (GMRES restarts / BiCGStab iterations)
     const bool fixed = (o.min_iter >= o.max_iter);
-    for (int st = 0; st < n; ++st) {
-        k_report_dt<<<1, 1, 0, s>>>(c.sc.p, c.reps.p, st);
-        CKL();
-        pre_solve<MT>(c);
-        int conv = 0;
-        if (!fixed && o.min_iter == 0) {
-            CK(cudaMemcpyAsync(&conv, &c.sc.p->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
-            CK(cudaStreamSynchronize(s));
+    if (!c.step_ev[0]) { CK(cudaEventCreate(&c.step_ev[0])); CK(cudaEventCreate(&c.step_ev[1])); }
+    if (o.graphs) {
+        if (fixed && !c.g_step.exec)
+            capture(c, c.g_step, [&] {
+                step_head<MT>(c);
+                for (int it = 1; it <= o.max_iter; ++it) Ops<MT>::iteration(c);
+                step_tail(c);
+            });
+        if (!fixed && !c.g_pre.exec) {
+            capture(c, c.g_pre, [&] { step_head<MT>(c); });
+            capture(c, c.g_cycle, [&] { Ops<MT>::iteration(c); });
+            capture(c, c.g_post, [&] { step_tail(c); });
         }
-        for (int it = 1; !conv && it <= o.max_iter; ++it) {
-            Ops<MT>::iteration(c);
-            if (it >= o.max_iter) break;
-            if (it >= o.min_iter) {
-                CK(cudaMemcpyAsync(&conv, &c.sc.p->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
-                CK(cudaStreamSynchronize(s));
+    }
+    int done = 0;
+    double total_ms = 0;
+    while (done < n) {
+        const int chunk = std::min(n - done, rdst_ctx::REP_CAP);
+        CK(cudaMemsetAsync(&c.sc.p->step_idx, 0, sizeof(int), s));
+        CK(cudaEventRecord(c.step_ev[0], s));
+        for (int st = 0; st < chunk; ++st) {
+            if (!o.graphs) {
+                step_head<MT>(c);
+                iterations_direct<MT>(c);
+                step_tail(c);
+            } else if (fixed) {
+                launch_graph(c, c.g_step);
+                if (o.profile) { CK(cudaStreamSynchronize(s)); c.collect_graph_events(c.g_step); }
+            } else {
+                launch_graph(c, c.g_pre);
+                if (o.profile) { CK(cudaStreamSynchronize(s)); c.collect_graph_events(c.g_pre); }
+                int conv = 0;
+                if (o.min_iter == 0) {
+                    CK(cudaMemcpyAsync(&conv, &c.sc.p->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
+                    CK(cudaStreamSynchronize(s));
+                }
+                for (int it = 1; !conv && it <= o.max_iter; ++it) {
+                    launch_graph(c, c.g_cycle);
+                    if (o.profile) { CK(cudaStreamSynchronize(s)); c.collect_graph_events(c.g_cycle); }
+                    if (it >= o.max_iter) break;
+                    if (it >= o.min_iter) {
+                        CK(cudaMemcpyAsync(&conv, &c.sc.p->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
+                        CK(cudaStreamSynchronize(s));
+                    }
+                }
+                launch_graph(c, c.g_post);
+                if (o.profile) { CK(cudaStreamSynchronize(s)); c.collect_graph_events(c.g_post); }
             }
         }
-        post_update(c);
-        k_report<<<1, 1, 0, s>>>(c.sc.p, c.reps.p, st, 0.0);
-        CKL();
-        if (c.steady) { k_mean_courant<<<1, 256, 0, s>>>(c.courantF.p, c.N, c.reps.p, st); CKL(); }
-    }
-    CK(cudaEventRecord(c.step_ev[1], s));
-    int flags = 0;
-    CK(cudaMemcpyAsync(&flags, &c.sc.p->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
-    if (host_reps) CK(cudaMemcpyAsync(host_reps, c.reps.p, sizeof(rdst_step_report) * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    {
+        CK(cudaEventRecord(c.step_ev[1], s));
+        if (host_reps)
+            CK(cudaMemcpyAsync(host_reps + done, c.reps.p, sizeof(rdst_step_report) * chunk, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, c.step_ev[0], c.step_ev[1]));
-        c.last_step_ms = ms;
+        total_ms += ms;
+        done += chunk;
     }
+    c.last_step_ms = total_ms;
+    int flags = 0;
+    CK(cudaMemcpyAsync(&flags, &c.sc.p->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     c.collect_events();
     if (flags & 2) throw std::domain_error("non-physical state (NaN or non-positive rho/p) after the update");
 }
@@ -849,9 +967,9 @@ void dispatch(rdst_ctx& c, Fn&& fn) {
 }
 
 void after_state_set(rdst_ctx& c) {
-    k_init_phib<<<nblk(c.NB, TPB), TPB, 0, c.s>>>(c.m, c.W.p, c.bs.p);
+    k_init_phib<<<nblk(c.NB, TPB), TPB, 0, c.s>>>(c.m, c.W.p, c.prim.p, c.bs.p);
     CKL();
-    k_boundary<<<nblk(c.NB, TPB), TPB, 0, c.s>>>(c.m, c.th, c.bd, c.prim.p, c.bs.p);
+    k_boundary<<<nblk(c.NB, TPB), TPB, 0, c.s>>>(c.m, c.th, c.bd, c.W.p, c.prim.p, c.bs.p);
     CKL();
     initialize_time(c);
     CK(cudaStreamSynchronize(c.s));
@@ -935,7 +1053,7 @@ RDST_API rdst_status rdst_set_conservative(rdst_ctx* c, const double* rho, const
         if (c->state_set) {
             // fields replaced between steps: boundary values from the new
             // internal field, time-control history kept
-            k_boundary<<<nblk(c->NB, TPB), TPB, 0, c->s>>>(c->m, c->th, c->bd, c->prim.p, c->bs.p);
+            k_boundary<<<nblk(c->NB, TPB), TPB, 0, c->s>>>(c->m, c->th, c->bd, c->W.p, c->prim.p, c->bs.p);
             CKL();
             CK(cudaStreamSynchronize(c->s));
             return;

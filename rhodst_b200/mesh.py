@@ -461,44 +461,55 @@ def _two_stage(n: int, first: float, ratio: float) -> np.ndarray:
 
 
 def _hex_signed_volume(pts, cells):
+    """Signed volume of hexes by the divergence theorem over the six faces
+    of the local vertex ordering (robust to collinear corner vertices)."""
     p = pts[cells]
-    d = p[:, 6] - p[:, 0]
-    return np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 3] - p[:, 0]), d)
+    vol = np.zeros(cells.shape[0])
+    for f in _HEX_FACES:
+        a, b, c, d = (p[:, f[k]] for k in range(4))
+        S = 0.5 * np.cross(c - a, d - b)
+        C = 0.25 * (a + b + c + d)
+        vol += np.einsum("ij,ij->i", C, S)
+    return vol / 3.0
 
 
-def swept_wing_oh(n_around: int = 192, n_normal: int = 64, n_span: int = 48, n_tip: int = 24,
+def swept_wing_oh(n_around: int = 192, n_normal: int = 64, n_span: int = 64, n_tip: int = 34,
                   taper: float = 0.56, sweep_deg: float = 30.0, semi_span: float = 1.5,
                   farfield: float = 10.0, first_cell: float = 2e-3) -> PolyMesh:
-    """Extruded NACA0012 swept, tapered wing in an O-H hex mesh.
+    """Extruded NACA0012 swept, tapered wing (root chord 1) in an O-H hex mesh.
 
-    O-mesh around each spanwise section (n_around x n_normal), stacked in
-    n_span stations over the wing and n_tip stations beyond the tip to the
-    far-field side plane; beyond the tip the O-grid's inner ring collapses
-    onto the tip chord line (a thin slot of cells closes the H part).
-    Patches: wing (wall), farfield (patch), symmetry (symmetryPlane).
-    Cell count = n_around * n_normal * (n_span + n_tip).
+    Each spanwise station carries an O-grid (n_around x n_normal) around the
+    local section, with a circular far field of radius `farfield` about the
+    section's mid-chord; n_span cell layers span the wing (z in
+    [0, semi_span]) and n_tip layers continue to the far-field side plane.
+    Beyond the tip the O-grid's inner ring is collapsed onto the tip chord
+    line and its upper/lower points are merged, so that slit is internal;
+    the first layer past the tip closes the wing with a tip cap.
+    Patches: wing (wall), farfield (patch), symmetry (symmetryPlane, z = 0).
+    Cell count = n_around * n_normal * (n_span + n_tip); defaults give
+    192 * 64 * 98 = 1,204,224.
     """
+    if n_around % 2:
+        raise ValueError("n_around must be even")
     sw = math.tan(math.radians(sweep_deg))
     nprof = n_around
-    beta = np.linspace(0.0, 2 * math.pi, nprof + 1)[:-1]
-    xa = 0.5 * (1.0 + np.cos(beta))             # TE(1) -> LE(0) -> TE
+    beta = 2.0 * math.pi * np.arange(nprof) / nprof
+    xa = 0.5 * (1.0 + np.cos(beta))             # TE(1) -> upper -> LE(0) -> lower -> TE
     ya = np.where(beta <= math.pi, 1.0, -1.0) * naca00xx(xa)
-    eta = _stretch(n_normal, first_cell, 1.0)
+    eta = _stretch(n_normal, first_cell / farfield, 1.0)
     zs_w = semi_span * np.linspace(0.0, 1.0, n_span + 1)
     ztip = _stretch(n_tip, semi_span / n_span, farfield - semi_span)
     zs = np.concatenate([zs_w, semi_span + ztip[1:]])
     nk = zs.size
     pts = np.zeros((nprof, n_normal + 1, nk, 3))
-    # far-field circle about the root mid-chord
     thf = np.arctan2(ya, xa - 0.5)
     for k, z in enumerate(zs):
         zw = min(z, semi_span)
-        frac = zw / semi_span
-        chord = 1.0 - (1.0 - taper) * frac
+        chord = 1.0 - (1.0 - taper) * zw / semi_span
         xle = sw * zw
-        thick = 1.0 if z <= semi_span else max(0.0, 1.0 - (z - semi_span) / (0.3 * semi_span))
+        thick = 1.0 if k <= n_span else 0.0
         sx = xle + chord * xa
-        sy = chord * ya * (thick if z > semi_span else 1.0)
+        sy = chord * ya * thick
         cx = xle + 0.5 * chord
         ox = cx + farfield * np.cos(thf)
         oy = farfield * np.sin(thf)
@@ -507,29 +518,36 @@ def swept_wing_oh(n_around: int = 192, n_normal: int = 64, n_span: int = 48, n_t
             pts[:, j, k, 1] = sy + e * (oy - sy)
             pts[:, j, k, 2] = z
     idx = np.arange(pts.shape[0] * pts.shape[1] * pts.shape[2]).reshape(pts.shape[:3])
-    # periodic in i: cell i connects i and (i+1) % nprof
+    for k in range(n_span + 1, nk):          # collapsed ring: merge upper/lower points
+        for i in range(1, nprof // 2):
+            idx[nprof - i, 0, k] = idx[i, 0, k]
     ii, jj, kk = np.meshgrid(np.arange(nprof), np.arange(n_normal), np.arange(nk - 1), indexing="ij")
     ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
     ip = (ii + 1) % nprof
     cells = np.stack([idx[ii, jj, kk], idx[ip, jj, kk], idx[ip, jj + 1, kk], idx[ii, jj + 1, kk],
                       idx[ii, jj, kk + 1], idx[ip, jj, kk + 1], idx[ip, jj + 1, kk + 1],
                       idx[ii, jj + 1, kk + 1]], axis=1)
-    # order cells k-major, then j, then i (section by section)
-    o = np.lexsort((ii, jj, kk))
+    o = np.lexsort((ii, jj, kk))             # section by section, ring by ring
     cells = cells[o]
     ptsf = pts.reshape(-1, 3)
-    # beyond the tip the j=0 ring is degenerate (zero thickness at z>tip+0.3b);
-    # keep it valid by giving the ring a minimum thickness
+    used = np.unique(cells)
+    remap = -np.ones(ptsf.shape[0], dtype=np.int64)
+    remap[used] = np.arange(used.size)
+    ptsf = ptsf[used]
+    cells = remap[cells]
     v = _hex_signed_volume(ptsf, cells)
     if np.any(v < 0):
         cells[v < 0] = cells[v < 0][:, [0, 3, 2, 1, 4, 7, 6, 5]]
+    zmax = zs[-1]
 
     def classify(c, n):
         out = np.full(c.shape[0], 1)
-        out[(np.abs(n[:, 2]) > 0.9) & (np.abs(c[:, 2]) < 1e-9)] = 2
-        out[(np.abs(c[:, 2] - zs[-1]) < 1e-9)] = 1
-        r = np.hypot(c[:, 0] - (sw * np.minimum(c[:, 2], semi_span) + 0.5), c[:, 1])
-        out[(out == 1) & (r < 0.75) & (c[:, 2] <= semi_span + 1e-9)] = 0
+        out[(np.abs(c[:, 2]) < 1e-9) & (np.abs(n[:, 2]) > 0.9)] = 2
+        zc = np.minimum(c[:, 2], semi_span)
+        chord = 1.0 - (1.0 - taper) * zc / semi_span
+        r = np.hypot(c[:, 0] - (sw * zc + 0.5 * chord), c[:, 1])
+        side = np.abs(c[:, 2] - zmax) < 1e-9
+        out[(out == 1) & (r < 0.5 * farfield) & ~side] = 0
         return out
 
     return build_polymesh(ptsf, [("hex", cells)], classify,

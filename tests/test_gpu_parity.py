@@ -145,3 +145,73 @@ def test_mixed_precision_matrix(prec):
     tol = 1e-5 if prec == "fp32" else 1e-2
     for a, b in zip(Wm, W64):
         assert rel(a, b) < tol
+
+
+def small_airfoil(**kw):
+    c = cases.naca0012_inviscid(ni=129, nj=33, **kw)
+    return c.with_options(**{"ilu.parts": 4})
+
+
+@pytest.mark.parametrize("flux,lim", [("AUSM+up", "Venkatakrishnan"), ("HLLC", "OSPRE"), ("Kurganov", "vanLeer")])
+def test_farfield_airfoil_residual(flux, lim):
+    case = small_airfoil(flux=flux, limiter=lim)
+    gpu, ora = pair(case, partition=rhodst_b200.partition_cells(case.mesh.C, 4))
+    rho, rhoU, rhoE = perturbed_state(case, amp=0.02)
+    for s in (gpu, ora):
+        s.set_conservative(rho, rhoU, rhoE)
+    Rg, Ro = gpu.residual(), ora.residual()
+    for k in range(5):
+        assert rel(Rg[:, k], Ro[:, k]) < 1e-11
+    dg, ug, lg, sg = gpu.assemble()
+    do, uo, lo, so = ora.assemble()
+    assert rel(dg, do) < 1e-11 and rel(ug, uo) < 1e-11 and rel(lg, lo) < 1e-11
+
+
+def test_farfield_airfoil_steps():
+    case = small_airfoil()
+    _run_pair(case, 10, partition=rhodst_b200.partition_cells(case.mesh.C, 4), tol=1e-9)
+
+
+def test_wing_small_steps():
+    case = cases.swept_wing_c3(n_around=48, n_normal=16, n_span=8, n_tip=4, ilu_parts=6)
+    _run_pair(case, 4, partition=rhodst_b200.partition_cells(case.mesh.C, 6), tol=1e-9)
+
+
+def test_forces_parity():
+    case = small_airfoil()
+    gpu, ora = pair(case, partition=rhodst_b200.partition_cells(case.mesh.C, 4))
+    for s in (gpu, ora):
+        s.set_primitive(case.p, case.U, case.T)
+        s.step(5)
+    q = 0.5 * 1.4 * 0.73 ** 2   # 1/2 rho U^2 with rho = gamma (p = T = 1 normalised gas)
+    fg = gpu.forces("airfoil", case.force_dirs["lift"], case.force_dirs["drag"], 1.0, q * 0.1)
+    fo = ora.forces("airfoil", case.force_dirs["lift"], case.force_dirs["drag"], 1.0, q * 0.1)
+    for k in ("Cl", "Cd", "Cm"):
+        assert abs(fg[k] - fo[k]) <= 1e-9 * max(abs(fo[k]), 1e-3)
+
+
+@pytest.mark.parametrize("fixed", [True, False])
+def test_graphs_match_direct_launches(fixed):
+    """CUDA-graph replay of the step gives bitwise the same trajectory as
+    direct launches (fixed iteration count: one graph per step; tolerance
+    driven: pre / iteration / post graphs with host convergence reads)."""
+    case = cases.forward_step_c1(n_directions=5 if not fixed else 20, max_iter=1 if fixed else 20)
+    if not fixed:
+        case = case.with_options(**{"solvers.W.tolerance": 1e-11})
+    out = []
+    for graphs in (True, False):
+        s = rhodst_b200.solver_for(case.with_options(graphs=graphs))
+        rep = s.step(6)
+        out.append((np.concatenate([x.ravel() for x in s.conservative()]),
+                    [r["res_mag"] for r in rep], [r["lin_iterations"] for r in rep]))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+
+
+def test_profile_counters():
+    case = cases.forward_step_c1().with_options(profile=True)
+    s = rhodst_b200.solver_for(case)
+    s.step(3)
+    n, ms = s.kernel_stats("spmv")
+    assert n == 3 * 23 and ms > 0          # 20 directions + initial + final residual + W-form A.W
+    assert s.launch_count() > 0 and s.last_step_ms() > 0
