@@ -179,6 +179,17 @@ def run_ours(args, rank, world):
     value = world * N * args.steps / (total_ms * 1e-3)
     # dominant kernel class over the timed region -> roofline
     stats = {k: tuple(np.subtract(s.kernel_stats(k), stats0[k])) for k in stats0}
+    prec0 = case.options.get("precision", "fp64")
+    S0 = 8 if prec0 == "fp64" else (4 if prec0 == "fp32" else 2)
+    pc0 = case.options["solvers"]["W"]["preconditioner"]
+    breakdown = {}
+    for k, (nl_, ms_) in stats.items():
+        if nl_ <= 0:
+            continue
+        by_ = algorithmic_bytes(k, N, F, S0, pc0)
+        breakdown[k] = {"launches": int(nl_), "avg_us": round(ms_ / nl_ * 1e3, 2),
+                        "share_of_step": round(ms_ / max(total_ms, 1e-9), 4),
+                        "GBps": round(by_ / (ms_ / nl_ * 1e-3) / 1e9, 1) if by_ else None}
     dom = max(stats, key=lambda k: stats[k][1])
     n_l, ms_l = stats[dom]
     prec = case.options.get("precision", "fp64")
@@ -216,7 +227,8 @@ def run_ours(args, rank, world):
             "data": "synthetic (generated mesh, uniform Mach-3 inflow initial state)",
             "config": dict(desc, l2="flushed: 256 MB written between timed steps",
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
-            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches), "roofline": roof}
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches), "roofline": roof,
+            "kernels": breakdown}
     return line, case
 
 

@@ -947,7 +947,17 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
         rows[P].push_back({Q, A.u[f]});
         rows[Q].push_back({P, A.l[f]});
     }
-    for (auto& r : rows) std::sort(r.begin(), r.end(), [](auto& a, auto& b) { return a.first < b.first; });
+    // one block per cell pair: faces joining the same pair are summed
+    for (auto& r : rows) {
+        std::sort(r.begin(), r.end(), [](auto& a, auto& b) { return a.first < b.first; });
+        std::vector<std::pair<int, t5>> m;
+        for (auto& e : r) {
+            if (!m.empty() && m.back().first == e.first)
+                for (int k = 0; k < 25; ++k) m.back().second[k] += e.second[k];
+            else m.push_back(e);
+        }
+        r.swap(m);
+    }
     M.rowStart.assign(N + 1, 0);
     for (int i = 0; i < N; ++i) M.rowStart[i + 1] = M.rowStart[i] + (int)rows[i].size();
     M.col.resize(M.rowStart[N]);

@@ -525,7 +525,9 @@ __global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, SellMat<
             double lambda = 0.5 * amaxSf;
             calcJ(Ur, g, phiJr, a1r, nn, J);
             calcJ(Uc, g, phiJc, a1c, nn, Jc);
-            const int slot = cf_slot[k];
+            const int cs = cf_slot[k];
+            const bool accum = cs < 0;          // further face of an already written cell pair
+            const int slot = accum ? -cs - 1 : cs;
             if (isOwner) {
 #pragma unroll
                 for (int e = 0; e < 25; ++e) {
@@ -533,7 +535,8 @@ __global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, SellMat<
                     double lower = -beta * ((J[e] * wf) * magS + I * lambda);
                     D[e] -= lower;
                     double upper = beta * ((Jc[e] * (1 - wf)) * magS - I * lambda);
-                    st(&A.val[sidx(A.slice_off, r, slot, e)], upper);
+                    MT* p = &A.val[sidx(A.slice_off, r, slot, e)];
+                    st(p, accum ? ld(p) + upper : upper);
                 }
             } else {
 #pragma unroll
@@ -542,7 +545,8 @@ __global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, SellMat<
                     double upper = beta * ((J[e] * (1 - wf)) * magS - I * lambda);
                     D[e] -= upper;
                     double lower = -beta * ((Jc[e] * wf) * magS + I * lambda);
-                    st(&A.val[sidx(A.slice_off, r, slot, e)], lower);
+                    MT* p = &A.val[sidx(A.slice_off, r, slot, e)];
+                    st(p, accum ? ld(p) + lower : lower);
                 }
             }
         } else {

@@ -123,20 +123,18 @@ __global__ void k_copy_identity(int n, const double* __restrict__ x, double* __r
 }
 
 // ---------------------------------------------------------------- ILU(0)
-// One CTA per subdomain; rows of a subdomain are contiguous and sorted by
+// One CTA per subdomain.  Rows of a subdomain are contiguous and sorted by
 // wavefront level, so each level is a contiguous row range processed in
 // parallel with a CTA barrier between levels (exact ILU(0) within the
-// subdomain, block-Jacobi between subdomains).
+// subdomain, block-Jacobi between subdomains).  A row's factors are its own
+// SELL slots: 1..nl = L (same-subdomain lower), nl+1..nl+nu = U.
 struct IluDev {
     int n_parts;
     const int* part_lvl0;   // [n_parts+1] level index range of each part
     const int* lvl_off;     // [n_levels+1] row range of each level
-    const int* low_start;   // [N+1]
-    const int* low_slot;    // flat slot (slice slot * 32 + lane) of L_rk / A_rk
-    const int* low_col;
-    const int* up_start;    // [N+1]
-    const int* up_slot;
-    const int* up_col;
+    const int* nlu;         // [N] nl | nu << 8
+    int ml, mu;             // factor slots: L_q at 1+q (q < ml), U_q at 1+ml+q (q < mu)
+    const int* low_start;   // [N+1] prefix of nl (index of the row's first triple range)
     const int* tr_start;    // [n_low+1]
     const int* tr_kj;       // flat slot of U_kj
     const int* tr_rj;       // flat slot of A_rj (-1: diagonal)
@@ -146,21 +144,28 @@ __device__ __forceinline__ size_t flat_e(int flat, int e) {
     return (size_t)(flat >> 5) * (32 * 25) + (size_t)e * 32 + (flat & 31);
 }
 
+constexpr int ILU_TPB = 128;
+constexpr int ILU_MAXNB = 8;
+
 template <typename MT>
-__global__ void __launch_bounds__(128) k_ilu_factor(SellMat<MT> LU, MT* __restrict__ dinv, IluDev P) {
+__global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> LU, MT* __restrict__ dinv, IluDev P) {
     const int part = blockIdx.x;
     const int N = LU.N;
     for (int l = P.part_lvl0[part]; l < P.part_lvl0[part + 1]; ++l) {
         for (int r = P.lvl_off[l] + threadIdx.x; r < P.lvl_off[l + 1]; r += blockDim.x) {
+            const int nl = P.nlu[r] & 255;
+            const size_t base = (size_t)LU.slice_off[r >> 5] * (32 * 25) + (r & 31);
+            const int sbase = LU.slice_off[r >> 5] * 32 + (r & 31);
             double D[25];
-            const MT* dv = LU.val + (size_t)LU.slice_off[r >> 5] * (32 * 25) + (r & 31);
 #pragma unroll
-            for (int e = 0; e < 25; ++e) D[e] = ld(dv + e * 32);
-            for (int q = P.low_start[r]; q < P.low_start[r + 1]; ++q) {
-                const int sl = P.low_slot[q], k = P.low_col[q];
-                double Ark[25], Lrk[25], Dk[25];
+            for (int e = 0; e < 25; ++e) D[e] = ld(LU.val + base + e * 32);
+            int q0 = P.low_start[r];
+            for (int q = 0; q < nl; ++q) {
+                const size_t ob = base + (size_t)(1 + q) * (32 * 25);
+                const int k = LU.col[sbase + (1 + q) * 32];
+                double Ark[25], Dk[25], Lrk[25];
 #pragma unroll
-                for (int e = 0; e < 25; ++e) { Ark[e] = ld(LU.val + flat_e(sl, e)); Dk[e] = ld(dinv + (size_t)e * N + k); }
+                for (int e = 0; e < 25; ++e) { Ark[e] = ld(LU.val + ob + e * 32); Dk[e] = ld(dinv + (size_t)e * N + k); }
 #pragma unroll
                 for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -171,8 +176,8 @@ __global__ void __launch_bounds__(128) k_ilu_factor(SellMat<MT> LU, MT* __restri
                         Lrk[5 * i + j] = a;
                     }
 #pragma unroll
-                for (int e = 0; e < 25; ++e) st(LU.val + flat_e(sl, e), Lrk[e]);
-                for (int t = P.tr_start[q]; t < P.tr_start[q + 1]; ++t) {
+                for (int e = 0; e < 25; ++e) st(LU.val + ob + e * 32, Lrk[e]);
+                for (int t = P.tr_start[q0 + q]; t < P.tr_start[q0 + q + 1]; ++t) {
                     const int kj = P.tr_kj[t], rj = P.tr_rj[t];
                     double U[25];
 #pragma unroll
@@ -207,53 +212,96 @@ __global__ void __launch_bounds__(128) k_ilu_factor(SellMat<MT> LU, MT* __restri
     }
 }
 
-// x = (LU)^-1 b : forward y_r = b_r - sum L_rk y_k, backward
-// x_r = inv(U_rr)(y_r - sum U_rj x_j), level by level inside the CTA.
-template <typename MT>
-__global__ void __launch_bounds__(128) k_ilu_apply(SellMat<MT> LU, const MT* __restrict__ dinv, IluDev P,
-                                                   const double* __restrict__ b, double* x, const int* __restrict__ active) {
+// x = (LU)^-1 b : forward y_r = b_r - sum_k L_rk y_k, backward
+// x_r = inv(U_rr)(y_r - sum_j U_rj x_j), level by level inside the CTA.
+// Five lanes per row (one per output component, six rows per warp): the
+// slot/column/value loads of a row are independent of each other and of
+// the level's data, so a level costs one round trip for the neighbour
+// gathers (written by the previous level of the same CTA) plus the barrier.
+constexpr int ILU_APPLY_TPB = 256;
+
+template <typename MT, int NB>
+__global__ void __launch_bounds__(ILU_APPLY_TPB) k_ilu_apply(SellMat<MT> LU, const MT* __restrict__ dinv, IluDev P,
+                                                             const double* __restrict__ b, double* x,
+                                                             const int* __restrict__ active) {
     if (active && !*active) return;
     const int part = blockIdx.x;
     const int N = LU.N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rsub = lane / 5, comp = lane - 5 * (lane / 5);
+    const bool lane_ok = lane < 30;
+    const int rows_per_pass = (blockDim.x >> 5) * 6;
     const int l0 = P.part_lvl0[part], l1 = P.part_lvl0[part + 1];
+    const int ml = P.ml, mu = P.mu;
     for (int l = l0; l < l1; ++l) {
-        for (int r = P.lvl_off[l] + threadIdx.x; r < P.lvl_off[l + 1]; r += blockDim.x) {
-            double y[5] = {b[5 * r], b[5 * r + 1], b[5 * r + 2], b[5 * r + 3], b[5 * r + 4]};
-            for (int q = P.low_start[r]; q < P.low_start[r + 1]; ++q) {
-                const int sl = P.low_slot[q], k = P.low_col[q];
-                double xk[5];
+        const int r0 = P.lvl_off[l], r1 = P.lvl_off[l + 1];
+        for (int base = 0; base < r1 - r0; base += rows_per_pass) {
+            const int r = r0 + base + warp * 6 + rsub;
+            if (lane_ok && r < r1) {
+                const size_t vb = (size_t)LU.slice_off[r >> 5] * (32 * 25) + (r & 31);
+                const int sb = LU.slice_off[r >> 5] * 32 + (r & 31);
+                int cq[NB];
+                double v[NB][5];
 #pragma unroll
-                for (int j = 0; j < 5; ++j) xk[j] = x[5 * k + j];
+                for (int q = 0; q < NB; ++q) {
+                    cq[q] = (q < ml) ? LU.col[sb + (1 + q) * 32] : -1;
 #pragma unroll
-                for (int i = 0; i < 5; ++i)
+                    for (int j = 0; j < 5; ++j)
+                        v[q][j] = (q < ml) ? ld(LU.val + vb + (size_t)(1 + q) * (32 * 25) + (5 * comp + j) * 32) : 0.0;
+                }
+                double y = b[5 * r + comp];
 #pragma unroll
-                    for (int j = 0; j < 5; ++j) y[i] -= ld(LU.val + flat_e(sl, 5 * i + j)) * xk[j];
+                for (int q = 0; q < NB; ++q) {
+                    if (cq[q] >= 0) {
+                        const double* xk = x + 5 * cq[q];
+#pragma unroll
+                        for (int j = 0; j < 5; ++j) y -= v[q][j] * xk[j];
+                    }
+                }
+                x[5 * r + comp] = y;
             }
-#pragma unroll
-            for (int i = 0; i < 5; ++i) x[5 * r + i] = y[i];
         }
         __syncthreads();
     }
     for (int l = l1 - 1; l >= l0; --l) {
-        for (int r = P.lvl_off[l] + threadIdx.x; r < P.lvl_off[l + 1]; r += blockDim.x) {
-            double y[5] = {x[5 * r], x[5 * r + 1], x[5 * r + 2], x[5 * r + 3], x[5 * r + 4]};
-            for (int q = P.up_start[r]; q < P.up_start[r + 1]; ++q) {
-                const int sl = P.up_slot[q], j0 = P.up_col[q];
-                double xj[5];
+        const int r0 = P.lvl_off[l], r1 = P.lvl_off[l + 1];
+        for (int base = 0; base < r1 - r0; base += rows_per_pass) {
+            const int r = r0 + base + warp * 6 + rsub;
+            const bool act = lane_ok && r < r1;
+            double y = 0.0, di[5] = {0, 0, 0, 0, 0};
+            if (act) {
+                const size_t vb = (size_t)LU.slice_off[r >> 5] * (32 * 25) + (r & 31);
+                const int sb = LU.slice_off[r >> 5] * 32 + (r & 31);
+                int cq[NB];
+                double v[NB][5];
 #pragma unroll
-                for (int j = 0; j < 5; ++j) xj[j] = x[5 * j0 + j];
+                for (int q = 0; q < NB; ++q) {
+                    const int slot = 1 + ml + q;
+                    cq[q] = (q < mu) ? LU.col[sb + slot * 32] : -1;
 #pragma unroll
-                for (int i = 0; i < 5; ++i)
+                    for (int j = 0; j < 5; ++j)
+                        v[q][j] = (q < mu) ? ld(LU.val + vb + (size_t)slot * (32 * 25) + (5 * comp + j) * 32) : 0.0;
+                }
 #pragma unroll
-                    for (int j = 0; j < 5; ++j) y[i] -= ld(LU.val + flat_e(sl, 5 * i + j)) * xj[j];
+                for (int j = 0; j < 5; ++j) di[j] = ld(dinv + (size_t)(5 * comp + j) * N + r);
+                y = x[5 * r + comp];
+#pragma unroll
+                for (int q = 0; q < NB; ++q) {
+                    if (cq[q] >= 0) {
+                        const double* xj = x + 5 * cq[q];
+#pragma unroll
+                        for (int j = 0; j < 5; ++j) y -= v[q][j] * xj[j];
+                    }
+                }
             }
+            // x_r = inv(U_rr) y : gather the row's five components by shuffle
+            double a = 0.0;
 #pragma unroll
-            for (int i = 0; i < 5; ++i) {
-                double a = 0;
-#pragma unroll
-                for (int j = 0; j < 5; ++j) a += ld(dinv + (size_t)(5 * i + j) * N + r) * y[j];
-                x[5 * r + i] = a;
+            for (int j = 0; j < 5; ++j) {
+                double yj = __shfl_sync(0xffffffffu, y, (lane_ok ? 5 * rsub : 0) + j);
+                a += di[j] * yj;
             }
+            if (act) x[5 * r + comp] = a;
         }
         __syncthreads();
     }

@@ -157,7 +157,8 @@ struct rdst_ctx {
     size_t mt_size = 8;
     // ILU plan
     int n_parts = 1;
-    DBuf<int> part_lvl0, lvl_off, low_start, low_slot, low_col, up_start, up_slot, up_col, tr_start, tr_kj, tr_rj;
+    DBuf<int> part_lvl0, lvl_off, low_start, nlu, tr_start, tr_kj, tr_rj;
+    int ilu_ml = 0, ilu_mu = 0;
     // Krylov
     DBuf<double> dx, r, t, Vb, s2, sh, ph, pv, xbar, Ax, pA;
     int limiter_need_grad = 1, venkat_mask = 0;
@@ -232,8 +233,7 @@ struct rdst_ctx {
     IluDev ilu() const {
         IluDev P;
         P.n_parts = n_parts; P.part_lvl0 = part_lvl0.p; P.lvl_off = lvl_off.p;
-        P.low_start = low_start.p; P.low_slot = low_slot.p; P.low_col = low_col.p;
-        P.up_start = up_start.p; P.up_slot = up_slot.p; P.up_col = up_col.p;
+        P.nlu = nlu.p; P.low_start = low_start.p; P.ml = ilu_ml; P.mu = ilu_mu;
         P.tr_start = tr_start.p; P.tr_kj = tr_kj.p; P.tr_rj = tr_rj.p;
         return P;
     }
@@ -403,10 +403,16 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         for (int fc : cfaces[c.perm[r]]) cf_list.push_back(fc);
         cf_start[r + 1] = (int)cf_list.size();
     }
-    // SELL-32 structure: slot 0 diagonal, then neighbours by internal column
+    // SELL-32 structure.  Slot 0 is the diagonal; the off-diagonal slots of a
+    // row are ordered [same-subdomain lower, same-subdomain upper, other
+    // subdomains], each by internal column, so the ILU(0) factors of a row
+    // are its own consecutive slots (no slot indirection in the sweeps).
+    std::vector<int> ipart(N, 0);
+    for (int r = 0; r < N; ++r) ipart[r] = part[c.perm[r]];
     c.n_slices = (N + 31) / 32;
     std::vector<int> slice_off(c.n_slices + 1, 0), slice_w(c.n_slices, 1);
     std::vector<std::vector<int>> rowcols(N);
+    std::vector<int> nl(N, 0), nu(N, 0);
     for (int r = 0; r < N; ++r) {
         for (int k = cf_start[r]; k < cf_start[r + 1]; ++k) {
             int fc = cf_list[k];
@@ -416,13 +422,42 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
             cc_list.push_back(other);
         }
         cc_start[r + 1] = (int)cc_list.size();
-        std::sort(rowcols[r].begin(), rowcols[r].end());
-        if (std::adjacent_find(rowcols[r].begin(), rowcols[r].end()) != rowcols[r].end())
-            throw std::invalid_argument("two faces between the same pair of cells");
+        // several faces may join the same pair of cells (allowed by foam's
+        // polyMesh): one matrix block per pair, the faces accumulate into it
+        auto grp = [&](int cc) { return ipart[cc] != ipart[r] ? 2 : (cc < r ? 0 : 1); };
+        std::sort(rowcols[r].begin(), rowcols[r].end(), [&](int a, int b) {
+            int ga = grp(a), gb = grp(b);
+            return ga != gb ? ga < gb : a < b;
+        });
+        rowcols[r].erase(std::unique(rowcols[r].begin(), rowcols[r].end()), rowcols[r].end());
+        for (int cc : rowcols[r]) { if (grp(cc) == 0) ++nl[r]; else if (grp(cc) == 1) ++nu[r]; }
+        if (nl[r] > 8 || nu[r] > 8) throw std::invalid_argument("a cell has more than 8 lower/upper neighbours");
     }
+    // fixed slot offsets of the factors: L_q at slot 1+q, U_q at slot 1+ML+q
+    // (ML/MU = largest lower/upper count, rows padded with empty slots), the
+    // other-subdomain couplings after them
+    int ML = 0, MU = 0;
+    if (o.precon == PRECON_ILU0)
+        for (int r = 0; r < N; ++r) { ML = std::max(ML, nl[r]); MU = std::max(MU, nu[r]); }
+    c.ilu_ml = ML;
+    c.ilu_mu = MU;
+    auto slot_of_pos = [&](int r, int k) {   // k: index into rowcols[r]
+        if (o.precon != PRECON_ILU0) return 1 + k;
+        if (k < nl[r]) return 1 + k;
+        if (k < nl[r] + nu[r]) return 1 + ML + (k - nl[r]);
+        return 1 + ML + MU + (k - nl[r] - nu[r]);
+    };
+    auto row_len = [&](int r) {
+        if (o.precon != PRECON_ILU0) return 1 + (int)rowcols[r].size();
+        return 1 + ML + MU + (int)rowcols[r].size() - nl[r] - nu[r];
+    };
+    auto pos_of = [&](int r, int cc) {
+        for (size_t k = 0; k < rowcols[r].size(); ++k) if (rowcols[r][k] == cc) return (int)k;
+        return -1;
+    };
     for (int sl = 0; sl < c.n_slices; ++sl) {
         int wmax = 1;
-        for (int r = sl * 32; r < std::min(N, sl * 32 + 32); ++r) wmax = std::max(wmax, 1 + (int)rowcols[r].size());
+        for (int r = sl * 32; r < std::min(N, sl * 32 + 32); ++r) wmax = std::max(wmax, row_len(r));
         slice_w[sl] = wmax;
         slice_off[sl + 1] = slice_off[sl] + wmax;
     }
@@ -431,27 +466,31 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     auto flat = [&](int r, int k) { return (slice_off[r >> 5] + k) * 32 + (r & 31); };
     for (int r = 0; r < N; ++r) {
         col[flat(r, 0)] = r;
-        for (size_t k = 0; k < rowcols[r].size(); ++k) col[flat(r, 1 + (int)k)] = rowcols[r][k];
+        for (size_t k = 0; k < rowcols[r].size(); ++k) col[flat(r, slot_of_pos(r, (int)k))] = rowcols[r][k];
     }
-    std::vector<int> cf_slot(cf_list.size(), -1);
-    for (int r = 0; r < N; ++r)
+    // slot of each cell-face entry: k >= 0 stores the block into slot k, a
+    // negative entry -(k+1) adds it (second and later faces of a cell pair)
+    std::vector<int> cf_slot(cf_list.size(), 0);
+    for (int r = 0; r < N; ++r) {
+        std::vector<char> seen(rowcols[r].size(), 0);
         for (int k = cf_start[r]; k < cf_start[r + 1]; ++k) {
             int fc = cf_list[k];
             if (fc >= Fi) continue;
             int other = own[fc] == r ? nei[fc] : own[fc];
-            int pos = (int)(std::lower_bound(rowcols[r].begin(), rowcols[r].end(), other) - rowcols[r].begin());
-            cf_slot[k] = 1 + pos;
+            int pos = pos_of(r, other);
+            int slot = slot_of_pos(r, pos);
+            cf_slot[k] = seen[pos] ? -(1 + slot) : slot;
+            seen[pos] = 1;
         }
-    // ---- ILU plan
+    }
+    // ---- ILU plan: wavefront levels (contiguous row ranges) per subdomain,
+    // per-row lower/upper counts, and the IKJ update triples
     if (o.precon == PRECON_ILU0) {
-        std::vector<int> ipart(N);
-        for (int r = 0; r < N; ++r) ipart[r] = part[c.perm[r]];
         std::vector<int> lvl_off, part_lvl0(nparts + 1, 0);
         for (int r = 0; r < N; ++r) {
             if (r == 0 || ipart[r] != ipart[r - 1] || level[c.perm[r]] != level[c.perm[r - 1]]) lvl_off.push_back(r);
         }
         lvl_off.push_back(N);
-        // part_lvl0: first level index of each part
         {
             int li = 0;
             for (int p = 0; p < nparts; ++p) {
@@ -460,36 +499,27 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
             }
             part_lvl0[nparts] = (int)lvl_off.size() - 1;
         }
-        std::vector<int> low_start(N + 1, 0), low_slot, low_col, up_start(N + 1, 0), up_slot, up_col;
-        std::vector<int> tr_start(1, 0), tr_kj, tr_rj;
+        std::vector<int> nlu(N), low_start(N + 1, 0), tr_start(1, 0), tr_kj, tr_rj;
         for (int r = 0; r < N; ++r) {
-            for (size_t k = 0; k < rowcols[r].size(); ++k) {
-                int cc = rowcols[r][k];
-                if (ipart[cc] != ipart[r]) continue;
-                if (cc < r) { low_slot.push_back(flat(r, 1 + (int)k)); low_col.push_back(cc); }
-                else { up_slot.push_back(flat(r, 1 + (int)k)); up_col.push_back(cc); }
-            }
-            low_start[r + 1] = (int)low_slot.size();
-            up_start[r + 1] = (int)up_slot.size();
+            nlu[r] = nl[r] | (nu[r] << 8);
+            low_start[r + 1] = low_start[r] + nl[r];
         }
         for (int r = 0; r < N; ++r) {
-            for (int q = low_start[r]; q < low_start[r + 1]; ++q) {
-                int k = low_col[q];
-                for (int u = up_start[k]; u < up_start[k + 1]; ++u) {
-                    int j = up_col[u];
-                    if (j == r) { tr_kj.push_back(up_slot[u]); tr_rj.push_back(-1); continue; }
-                    auto it = std::lower_bound(rowcols[r].begin(), rowcols[r].end(), j);
-                    if (it != rowcols[r].end() && *it == j && ipart[j] == ipart[r]) {
-                        tr_kj.push_back(up_slot[u]);
-                        tr_rj.push_back(flat(r, 1 + (int)(it - rowcols[r].begin())));
-                    }
+            for (int q = 0; q < nl[r]; ++q) {
+                int k = rowcols[r][q];
+                // U_kj for j > k in row k's same-subdomain upper part
+                for (int u = 0; u < nu[k]; ++u) {
+                    int j = rowcols[k][nl[k] + u];
+                    int kj = flat(k, 1 + ML + u);
+                    if (j == r) { tr_kj.push_back(kj); tr_rj.push_back(-1); continue; }
+                    int pj = pos_of(r, j);
+                    if (pj >= 0 && pj < nl[r] + nu[r]) { tr_kj.push_back(kj); tr_rj.push_back(flat(r, slot_of_pos(r, pj))); }
                 }
                 tr_start.push_back((int)tr_kj.size());
             }
         }
         c.part_lvl0.upload(part_lvl0, s); c.lvl_off.upload(lvl_off, s);
-        c.low_start.upload(low_start, s); c.low_slot.upload(low_slot, s); c.low_col.upload(low_col, s);
-        c.up_start.upload(up_start, s); c.up_slot.upload(up_slot, s); c.up_col.upload(up_col, s);
+        c.low_start.upload(low_start, s); c.nlu.upload(nlu, s);
         c.tr_start.upload(tr_start, s); c.tr_kj.upload(tr_kj, s); c.tr_rj.upload(tr_rj, s);
     }
     // ---- upload
@@ -588,7 +618,7 @@ struct Ops {
             size_t mbytes = (size_t)c.n_slots * 32 * 25 * sizeof(MT);
             CK(cudaMemcpyAsync(c.LUval, c.Aval, mbytes, cudaMemcpyDeviceToDevice, c.s));
             Timed tm(c, KS_FACTOR);
-            k_ilu_factor<MT><<<c.n_parts, 128, 0, c.s>>>(c.mat<MT>(c.LUval), (MT*)c.dinv, c.ilu());
+            k_ilu_factor<MT><<<c.n_parts, ILU_TPB, 0, c.s>>>(c.mat<MT>(c.LUval), (MT*)c.dinv, c.ilu());
             CKL();
         }
     }
@@ -596,8 +626,17 @@ struct Ops {
         Timed tm(c, KS_PRECOND);
         if (c.o.precon == PRECON_DIAGONAL)
             k_jacobi<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.N, (const MT*)c.dinv, in, out, active);
-        else if (c.o.precon == PRECON_ILU0)
-            k_ilu_apply<MT><<<c.n_parts, 128, 0, c.s>>>(c.mat<MT>(c.LUval), (const MT*)c.dinv, c.ilu(), in, out, active);
+        else if (c.o.precon == PRECON_ILU0) {
+            const int nb = std::max(c.ilu_ml, c.ilu_mu);
+            auto A = c.mat<MT>(c.LUval);
+            auto P = c.ilu();
+            const MT* di = (const MT*)c.dinv;
+            if (nb <= 2) k_ilu_apply<MT, 2><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
+            else if (nb <= 3) k_ilu_apply<MT, 3><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
+            else if (nb <= 4) k_ilu_apply<MT, 4><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
+            else if (nb <= 6) k_ilu_apply<MT, 6><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
+            else k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
+        }
         else
             k_copy_identity<MT><<<nblk(c.nvec(), TPB), TPB, 0, c.s>>>((int)c.nvec(), in, out, active);
         CKL();
@@ -1168,7 +1207,17 @@ RDST_API rdst_status rdst_assemble(rdst_ctx* c, double* diag, double* upper, dou
             if (diag) block_of(r, r, diag + 25L * i);
             if (source) for (int k = 0; k < 5; ++k) source[5L * i + k] = rhs[5L * r + k];
         }
+        // a cell pair joined by several faces holds one summed block: it is
+        // reported on the pair's first face, the others get zero blocks
+        std::unordered_map<long long, int> first_face;
         for (int f = 0; f < c->Fi; ++f) {
+            long long key = (long long)own[f] * c->N + nei[f];
+            bool dup = !first_face.emplace(key, f).second;
+            if (dup) {
+                if (upper) std::fill(upper + 25L * f, upper + 25L * f + 25, 0.0);
+                if (lower) std::fill(lower + 25L * f, lower + 25L * f + 25, 0.0);
+                continue;
+            }
             if (upper) block_of(own[f], nei[f], upper + 25L * f);
             if (lower) block_of(nei[f], own[f], lower + 25L * f);
         }
