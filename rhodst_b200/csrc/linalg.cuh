@@ -9,6 +9,13 @@
 
 namespace rdst {
 
+// entry e of 5x5 block `flat` in a slice-interleaved store: 32 blocks per
+// 800-entry chunk, entries interleaved by lane (SELL slots, ILU factors,
+// block-Jacobi / pivot inverses with flat = row)
+__device__ __forceinline__ size_t flat_e(int flat, int e) {
+    return (size_t)(flat >> 5) * (32 * 25) + (size_t)e * 32 + (flat & 31);
+}
+
 // inverse of a 5x5 block (Gauss-Jordan, partial pivoting), in registers
 __device__ __forceinline__ void inv5(const double A[25], double X[25]) {
     double a[5][10];
@@ -96,7 +103,7 @@ __global__ void k_dinv(SellMat<MT> A, MT* __restrict__ dinv) {
     for (int e = 0; e < 25; ++e) D[e] = ld(v + e * 32);
     inv5(D, X);
 #pragma unroll
-    for (int e = 0; e < 25; ++e) st(&dinv[(size_t)e * A.N + r], X[e]);
+    for (int e = 0; e < 25; ++e) st(&dinv[flat_e(r, e)], X[e]);
 }
 
 template <typename MT>
@@ -110,7 +117,7 @@ __global__ void k_jacobi(int N, const MT* __restrict__ dinv, const double* __res
     for (int i = 0; i < 5; ++i) {
         double a = 0;
 #pragma unroll
-        for (int j = 0; j < 5; ++j) a += ld(&dinv[(size_t)(5 * i + j) * N + r]) * xv[j];
+        for (int j = 0; j < 5; ++j) a += ld(&dinv[flat_e(r, 5 * i + j)]) * xv[j];
         y[5 * r + i] = a;
     }
 }
@@ -126,46 +133,63 @@ __global__ void k_copy_identity(int n, const double* __restrict__ x, double* __r
 // One CTA per subdomain.  Rows of a subdomain are contiguous and sorted by
 // wavefront level, so each level is a contiguous row range processed in
 // parallel with a CTA barrier between levels (exact ILU(0) within the
-// subdomain, block-Jacobi between subdomains).  A row's factors are its own
-// SELL slots: 1..nl = L (same-subdomain lower), nl+1..nl+nu = U.
+// subdomain, block-Jacobi between subdomains).  The factors are stored in
+// a fixed-width sliced layout of their own: factor slot s (L_q: s = q < ml,
+// U_q: s = ml + q) of row r has id fid = ((r/32)*(ml+mu) + s)*32 + r%32 and
+// its entries at flat_e(fid, e); the Jacobian keeps its SELL layout.
 struct IluDev {
     int n_parts;
     const int* part_lvl0;   // [n_parts+1] level index range of each part
     const int* lvl_off;     // [n_levels+1] row range of each level
     const int* nlu;         // [N] nl | nu << 8
-    int ml, mu;             // factor slots: L_q at 1+q (q < ml), U_q at 1+ml+q (q < mu)
-    const int* low_start;   // [N+1] prefix of nl (index of the row's first triple range)
+    const int* low_start;   // [N+1] prefix of nl (first triple range of the row)
     const int* tr_start;    // [n_low+1]
-    const int* tr_kj;       // flat slot of U_kj
-    const int* tr_rj;       // flat slot of A_rj (-1: diagonal)
+    const int* tr_kj;       // factor id of U_kj
+    const int* tr_rj;       // factor id of A_rj (-1: diagonal)
+    int ml, mu;             // factor slots per row
+    const int* lu_col;      // [fid] column of each factor slot (-1: empty)
+    const int* lu_src;      // [fid] SELL flat slot of the same block in A
 };
 
-__device__ __forceinline__ size_t flat_e(int flat, int e) {
-    return (size_t)(flat >> 5) * (32 * 25) + (size_t)e * 32 + (flat & 31);
-}
+__device__ __forceinline__ int lu_fid(int r, int s, int ms) { return ((r >> 5) * ms + s) * 32 + (r & 31); }
 
 constexpr int ILU_TPB = 128;
-constexpr int ILU_MAXNB = 8;
+
+// same-subdomain blocks of A -> factor storage (fully parallel, before the
+// level-scheduled factorisation); empty slots stay zero
+template <typename MT>
+__global__ void k_ilu_gather(SellMat<MT> A, MT* __restrict__ lu, const int* __restrict__ lu_src, int n_fid) {
+    const int fid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fid >= n_fid) return;
+    const int src = lu_src[fid];
+    if (src < 0) return;
+#pragma unroll
+    for (int e = 0; e < 25; ++e) lu[flat_e(fid, e)] = A.val[flat_e(src, e)];
+}
 
 template <typename MT>
-__global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> LU, MT* __restrict__ dinv, IluDev P) {
+__global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> A, MT* __restrict__ lu, MT* __restrict__ dinv,
+                                                        IluDev P) {
     const int part = blockIdx.x;
-    const int N = LU.N;
+    const int N = A.N;
+    const int ms = P.ml + P.mu;
     for (int l = P.part_lvl0[part]; l < P.part_lvl0[part + 1]; ++l) {
         for (int r = P.lvl_off[l] + threadIdx.x; r < P.lvl_off[l + 1]; r += blockDim.x) {
             const int nl = P.nlu[r] & 255;
-            const size_t base = (size_t)LU.slice_off[r >> 5] * (32 * 25) + (r & 31);
-            const int sbase = LU.slice_off[r >> 5] * 32 + (r & 31);
+            const MT* dv = A.val + (size_t)A.slice_off[r >> 5] * (32 * 25) + (r & 31);
             double D[25];
 #pragma unroll
-            for (int e = 0; e < 25; ++e) D[e] = ld(LU.val + base + e * 32);
-            int q0 = P.low_start[r];
+            for (int e = 0; e < 25; ++e) D[e] = ld(dv + e * 32);
+            const int q0 = P.low_start[r];
             for (int q = 0; q < nl; ++q) {
-                const size_t ob = base + (size_t)(1 + q) * (32 * 25);
-                const int k = LU.col[sbase + (1 + q) * 32];
+                const int fq = lu_fid(r, q, ms);
+                const int k = P.lu_col[fq];
                 double Ark[25], Dk[25], Lrk[25];
 #pragma unroll
-                for (int e = 0; e < 25; ++e) { Ark[e] = ld(LU.val + ob + e * 32); Dk[e] = ld(dinv + (size_t)e * N + k); }
+                for (int e = 0; e < 25; ++e) {
+                    Ark[e] = ld(lu + flat_e(fq, e));
+                    Dk[e] = ld(dinv + flat_e(k, e));
+                }
 #pragma unroll
                 for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -176,12 +200,12 @@ __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> LU, MT* __re
                         Lrk[5 * i + j] = a;
                     }
 #pragma unroll
-                for (int e = 0; e < 25; ++e) st(LU.val + ob + e * 32, Lrk[e]);
+                for (int e = 0; e < 25; ++e) st(lu + flat_e(fq, e), Lrk[e]);
                 for (int t = P.tr_start[q0 + q]; t < P.tr_start[q0 + q + 1]; ++t) {
                     const int kj = P.tr_kj[t], rj = P.tr_rj[t];
                     double U[25];
 #pragma unroll
-                    for (int e = 0; e < 25; ++e) U[e] = ld(LU.val + flat_e(kj, e));
+                    for (int e = 0; e < 25; ++e) U[e] = ld(lu + flat_e(kj, e));
                     if (rj < 0) {
 #pragma unroll
                         for (int i = 0; i < 5; ++i)
@@ -197,7 +221,7 @@ __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> LU, MT* __re
                             for (int j = 0; j < 5; ++j) {
                                 double a = 0;
                                 for (int t2 = 0; t2 < 5; ++t2) a += Lrk[5 * i + t2] * U[5 * t2 + j];
-                                MT* p = LU.val + flat_e(rj, 5 * i + j);
+                                MT* p = lu + flat_e(rj, 5 * i + j);
                                 st(p, ld(p) - a);
                             }
                     }
@@ -206,7 +230,7 @@ __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> LU, MT* __re
             double X[25];
             inv5(D, X);
 #pragma unroll
-            for (int e = 0; e < 25; ++e) st(dinv + (size_t)e * N + r, X[e]);
+            for (int e = 0; e < 25; ++e) st(dinv + flat_e(r, e), X[e]);
         }
         __syncthreads();
     }
@@ -215,39 +239,40 @@ __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> LU, MT* __re
 // x = (LU)^-1 b : forward y_r = b_r - sum_k L_rk y_k, backward
 // x_r = inv(U_rr)(y_r - sum_j U_rj x_j), level by level inside the CTA.
 // Five lanes per row (one per output component, six rows per warp): the
-// slot/column/value loads of a row are independent of each other and of
-// the level's data, so a level costs one round trip for the neighbour
-// gathers (written by the previous level of the same CTA) plus the barrier.
+// column/value loads of a row are independent of each other and of the
+// level's data, so a level costs one round trip for the neighbour gathers
+// (written by the previous level of the same CTA) plus the barrier.
 constexpr int ILU_APPLY_TPB = 256;
 
 template <typename MT, int NB>
-__global__ void __launch_bounds__(ILU_APPLY_TPB) k_ilu_apply(SellMat<MT> LU, const MT* __restrict__ dinv, IluDev P,
+__global__ void __launch_bounds__(ILU_APPLY_TPB) k_ilu_apply(int N, const MT* __restrict__ lu,
+                                                             const MT* __restrict__ dinv, IluDev P,
                                                              const double* __restrict__ b, double* x,
                                                              const int* __restrict__ active) {
     if (active && !*active) return;
     const int part = blockIdx.x;
-    const int N = LU.N;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rsub = lane / 5, comp = lane - 5 * (lane / 5);
     const bool lane_ok = lane < 30;
     const int rows_per_pass = (blockDim.x >> 5) * 6;
     const int l0 = P.part_lvl0[part], l1 = P.part_lvl0[part + 1];
-    const int ml = P.ml, mu = P.mu;
+    const int ml = P.ml, mu = P.mu, ms = ml + mu;
     for (int l = l0; l < l1; ++l) {
         const int r0 = P.lvl_off[l], r1 = P.lvl_off[l + 1];
         for (int base = 0; base < r1 - r0; base += rows_per_pass) {
             const int r = r0 + base + warp * 6 + rsub;
             if (lane_ok && r < r1) {
-                const size_t vb = (size_t)LU.slice_off[r >> 5] * (32 * 25) + (r & 31);
-                const int sb = LU.slice_off[r >> 5] * 32 + (r & 31);
                 int cq[NB];
                 double v[NB][5];
 #pragma unroll
                 for (int q = 0; q < NB; ++q) {
-                    cq[q] = (q < ml) ? LU.col[sb + (1 + q) * 32] : -1;
+                    const int fid = lu_fid(r, q, ms);
+                    cq[q] = (q < ml) ? P.lu_col[fid] : -1;
+                    // empty factor slots hold zeros: the value loads do not
+                    // wait for the column
 #pragma unroll
                     for (int j = 0; j < 5; ++j)
-                        v[q][j] = (q < ml) ? ld(LU.val + vb + (size_t)(1 + q) * (32 * 25) + (5 * comp + j) * 32) : 0.0;
+                        v[q][j] = (q < ml) ? ld(lu + flat_e(fid, 5 * comp + j)) : 0.0;
                 }
                 double y = b[5 * r + comp];
 #pragma unroll
@@ -270,20 +295,18 @@ __global__ void __launch_bounds__(ILU_APPLY_TPB) k_ilu_apply(SellMat<MT> LU, con
             const bool act = lane_ok && r < r1;
             double y = 0.0, di[5] = {0, 0, 0, 0, 0};
             if (act) {
-                const size_t vb = (size_t)LU.slice_off[r >> 5] * (32 * 25) + (r & 31);
-                const int sb = LU.slice_off[r >> 5] * 32 + (r & 31);
                 int cq[NB];
                 double v[NB][5];
 #pragma unroll
                 for (int q = 0; q < NB; ++q) {
-                    const int slot = 1 + ml + q;
-                    cq[q] = (q < mu) ? LU.col[sb + slot * 32] : -1;
+                    const int fid = lu_fid(r, ml + q, ms);
+                    cq[q] = (q < mu) ? P.lu_col[fid] : -1;
 #pragma unroll
                     for (int j = 0; j < 5; ++j)
-                        v[q][j] = (q < mu) ? ld(LU.val + vb + (size_t)slot * (32 * 25) + (5 * comp + j) * 32) : 0.0;
+                        v[q][j] = (q < mu) ? ld(lu + flat_e(fid, 5 * comp + j)) : 0.0;
                 }
 #pragma unroll
-                for (int j = 0; j < 5; ++j) di[j] = ld(dinv + (size_t)(5 * comp + j) * N + r);
+                for (int j = 0; j < 5; ++j) di[j] = ld(dinv + flat_e(r, 5 * comp + j));
                 y = x[5 * r + comp];
 #pragma unroll
                 for (int q = 0; q < NB; ++q) {
@@ -333,6 +356,75 @@ __global__ void __launch_bounds__(RED_TPB) k_multidot(long n, int nv, const doub
         double v = block_sum(acc[j]);
         if (threadIdx.x == 0) partial[(long)blockIdx.x * pstride + j] = v;
     }
+}
+
+// Deterministic block reduction of NV per-thread values: warp shuffles,
+// then one fixed-order sum over the warps; result -> partial[blk*pstride+j].
+template <int NV>
+__device__ __forceinline__ void block_multi_sum(double (&acc)[NV], int nv, double* __restrict__ partial, int pstride) {
+    __shared__ double sh[RED_TPB / 32][NV];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        if (j < nv) {
+            double v = warp_sum(acc[j]);
+            if (lane == 0) sh[wid][j] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        double v = 0;
+        for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) v += sh[w2][threadIdx.x];
+        partial[(long)blockIdx.x * pstride + threadIdx.x] = v;
+    }
+}
+
+// partial[blk][j] = sum_i V_j[i] w[i] for j < nv <= NV (one pass over w)
+template <int NV>
+__global__ void __launch_bounds__(RED_TPB, 2) k_vmultidot(long n, int nv, const double* __restrict__ V, long ldv,
+                                                       const double* __restrict__ w, double* __restrict__ partial,
+                                                       int pstride, const int* __restrict__ active) {
+    if (active && !*active) return;
+    double acc[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double wi = w[i];
+#pragma unroll
+        for (int j = 0; j < NV; ++j)
+            if (j < nv) acc[j] += V[j * ldv + i] * wi;
+    }
+    block_multi_sum<NV>(acc, nv, partial, pstride);
+}
+
+// w -= sum_j coef[j] V_j (j < nv), then in the same pass either the dots
+// V_j . w_new (mode 0: the second CGS2 pass) or w_new . w_new (mode 1)
+template <int NV>
+__global__ void __launch_bounds__(RED_TPB, 2) k_maxpy_dot(long n, int nv, const double* __restrict__ V, long ldv,
+                                                       const double* __restrict__ coef, double* __restrict__ w,
+                                                       double* __restrict__ partial, int pstride, int mode,
+                                                       const int* __restrict__ active) {
+    if (active && !*active) return;
+    __shared__ double cs[NV];
+    if (threadIdx.x < nv) cs[threadIdx.x] = coef[threadIdx.x];
+    __syncthreads();
+    double acc[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double a = w[i];
+        for (int j = 0; j < nv; ++j) a -= cs[j] * V[j * ldv + i];
+        w[i] = a;
+        if (mode == 0) {
+            // second read of V_j[i]: the lines were just fetched (L1 hit)
+#pragma unroll
+            for (int j = 0; j < NV; ++j)
+                if (j < nv) acc[j] += V[j * ldv + i] * a;
+        } else {
+            acc[0] += a * a;
+        }
+    }
+    block_multi_sum<NV>(acc, mode == 0 ? nv : 1, partial, pstride);
 }
 
 // out[j] = sum_b partial[b * pstride + j] (fixed order); optional sqrt

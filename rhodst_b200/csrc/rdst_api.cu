@@ -157,7 +157,8 @@ struct rdst_ctx {
     size_t mt_size = 8;
     // ILU plan
     int n_parts = 1;
-    DBuf<int> part_lvl0, lvl_off, low_start, nlu, tr_start, tr_kj, tr_rj;
+    DBuf<int> part_lvl0, lvl_off, low_start, nlu, tr_start, tr_kj, tr_rj, lu_col, lu_src;
+    int lu_slots = 0;
     int ilu_ml = 0, ilu_mu = 0;
     // Krylov
     DBuf<double> dx, r, t, Vb, s2, sh, ph, pv, xbar, Ax, pA;
@@ -233,7 +234,7 @@ struct rdst_ctx {
     IluDev ilu() const {
         IluDev P;
         P.n_parts = n_parts; P.part_lvl0 = part_lvl0.p; P.lvl_off = lvl_off.p;
-        P.nlu = nlu.p; P.low_start = low_start.p; P.ml = ilu_ml; P.mu = ilu_mu;
+        P.nlu = nlu.p; P.low_start = low_start.p; P.ml = ilu_ml; P.mu = ilu_mu; P.lu_col = lu_col.p; P.lu_src = lu_src.p;
         P.tr_start = tr_start.p; P.tr_kj = tr_kj.p; P.tr_rj = tr_rj.p;
         return P;
     }
@@ -403,16 +404,14 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         for (int fc : cfaces[c.perm[r]]) cf_list.push_back(fc);
         cf_start[r + 1] = (int)cf_list.size();
     }
-    // SELL-32 structure.  Slot 0 is the diagonal; the off-diagonal slots of a
-    // row are ordered [same-subdomain lower, same-subdomain upper, other
-    // subdomains], each by internal column, so the ILU(0) factors of a row
-    // are its own consecutive slots (no slot indirection in the sweeps).
+    // SELL-32 structure for the Jacobian: slot 0 the diagonal, then the
+    // neighbours by internal column (several faces may join one cell pair,
+    // allowed by foam's polyMesh: one block per pair, the faces accumulate).
     std::vector<int> ipart(N, 0);
     for (int r = 0; r < N; ++r) ipart[r] = part[c.perm[r]];
     c.n_slices = (N + 31) / 32;
     std::vector<int> slice_off(c.n_slices + 1, 0), slice_w(c.n_slices, 1);
     std::vector<std::vector<int>> rowcols(N);
-    std::vector<int> nl(N, 0), nu(N, 0);
     for (int r = 0; r < N; ++r) {
         for (int k = cf_start[r]; k < cf_start[r + 1]; ++k) {
             int fc = cf_list[k];
@@ -422,42 +421,16 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
             cc_list.push_back(other);
         }
         cc_start[r + 1] = (int)cc_list.size();
-        // several faces may join the same pair of cells (allowed by foam's
-        // polyMesh): one matrix block per pair, the faces accumulate into it
-        auto grp = [&](int cc) { return ipart[cc] != ipart[r] ? 2 : (cc < r ? 0 : 1); };
-        std::sort(rowcols[r].begin(), rowcols[r].end(), [&](int a, int b) {
-            int ga = grp(a), gb = grp(b);
-            return ga != gb ? ga < gb : a < b;
-        });
+        std::sort(rowcols[r].begin(), rowcols[r].end());
         rowcols[r].erase(std::unique(rowcols[r].begin(), rowcols[r].end()), rowcols[r].end());
-        for (int cc : rowcols[r]) { if (grp(cc) == 0) ++nl[r]; else if (grp(cc) == 1) ++nu[r]; }
-        if (nl[r] > 8 || nu[r] > 8) throw std::invalid_argument("a cell has more than 8 lower/upper neighbours");
     }
-    // fixed slot offsets of the factors: L_q at slot 1+q, U_q at slot 1+ML+q
-    // (ML/MU = largest lower/upper count, rows padded with empty slots), the
-    // other-subdomain couplings after them
-    int ML = 0, MU = 0;
-    if (o.precon == PRECON_ILU0)
-        for (int r = 0; r < N; ++r) { ML = std::max(ML, nl[r]); MU = std::max(MU, nu[r]); }
-    c.ilu_ml = ML;
-    c.ilu_mu = MU;
-    auto slot_of_pos = [&](int r, int k) {   // k: index into rowcols[r]
-        if (o.precon != PRECON_ILU0) return 1 + k;
-        if (k < nl[r]) return 1 + k;
-        if (k < nl[r] + nu[r]) return 1 + ML + (k - nl[r]);
-        return 1 + ML + MU + (k - nl[r] - nu[r]);
-    };
-    auto row_len = [&](int r) {
-        if (o.precon != PRECON_ILU0) return 1 + (int)rowcols[r].size();
-        return 1 + ML + MU + (int)rowcols[r].size() - nl[r] - nu[r];
-    };
     auto pos_of = [&](int r, int cc) {
-        for (size_t k = 0; k < rowcols[r].size(); ++k) if (rowcols[r][k] == cc) return (int)k;
-        return -1;
+        auto it = std::lower_bound(rowcols[r].begin(), rowcols[r].end(), cc);
+        return (it != rowcols[r].end() && *it == cc) ? (int)(it - rowcols[r].begin()) : -1;
     };
     for (int sl = 0; sl < c.n_slices; ++sl) {
         int wmax = 1;
-        for (int r = sl * 32; r < std::min(N, sl * 32 + 32); ++r) wmax = std::max(wmax, row_len(r));
+        for (int r = sl * 32; r < std::min(N, sl * 32 + 32); ++r) wmax = std::max(wmax, 1 + (int)rowcols[r].size());
         slice_w[sl] = wmax;
         slice_off[sl + 1] = slice_off[sl] + wmax;
     }
@@ -466,7 +439,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     auto flat = [&](int r, int k) { return (slice_off[r >> 5] + k) * 32 + (r & 31); };
     for (int r = 0; r < N; ++r) {
         col[flat(r, 0)] = r;
-        for (size_t k = 0; k < rowcols[r].size(); ++k) col[flat(r, slot_of_pos(r, (int)k))] = rowcols[r][k];
+        for (size_t k = 0; k < rowcols[r].size(); ++k) col[flat(r, 1 + (int)k)] = rowcols[r][k];
     }
     // slot of each cell-face entry: k >= 0 stores the block into slot k, a
     // negative entry -(k+1) adds it (second and later faces of a cell pair)
@@ -478,14 +451,49 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
             if (fc >= Fi) continue;
             int other = own[fc] == r ? nei[fc] : own[fc];
             int pos = pos_of(r, other);
-            int slot = slot_of_pos(r, pos);
+            int slot = 1 + pos;
             cf_slot[k] = seen[pos] ? -(1 + slot) : slot;
             seen[pos] = 1;
         }
     }
-    // ---- ILU plan: wavefront levels (contiguous row ranges) per subdomain,
-    // per-row lower/upper counts, and the IKJ update triples
+    // ---- ILU plan.  The factors live in their own ELL layout, factor slot s
+    // x cell: L_q (same-subdomain lower, by column) at s = q < ML, U_q at
+    // s = ML + q; entries interleaved by cell, lu_val[(s*25 + e)*N + r].
+    // Wavefront levels are contiguous row ranges per subdomain.
     if (o.precon == PRECON_ILU0) {
+        std::vector<int> nl(N, 0), nu(N, 0);
+        for (int r = 0; r < N; ++r)
+            for (int cc : rowcols[r])
+                if (ipart[cc] == ipart[r]) { if (cc < r) ++nl[r]; else ++nu[r]; }
+        const int ML = *std::max_element(nl.begin(), nl.end());
+        const int MU = *std::max_element(nu.begin(), nu.end());
+        if (ML > 8 || MU > 8) throw std::invalid_argument("a cell has more than 8 lower/upper neighbours");
+        c.ilu_ml = ML;
+        c.ilu_mu = MU;
+        const int MS = std::max(ML + MU, 1);
+        // factor id of slot s of row r: slices of 32 rows, MS slots each,
+        // entries interleaved by lane (the SELL addressing with width MS)
+        auto lfid = [&](int r, int sl) { return ((r >> 5) * MS + sl) * 32 + (r & 31); };
+        std::vector<int> lu_col((size_t)c.n_slices * MS * 32, -1), lu_src((size_t)c.n_slices * MS * 32, -1);
+        auto fid_of = [&](int r, int cc) {     // factor id of coupling (r, cc), or -1
+            int q = 0;
+            if (cc < r) {
+                for (int x : rowcols[r]) { if (x == cc) return lfid(r, q); if (x < r && ipart[x] == ipart[r]) ++q; }
+            } else {
+                for (int x : rowcols[r]) { if (x == cc) return lfid(r, ML + q); if (x > r && ipart[x] == ipart[r]) ++q; }
+            }
+            return -1;
+        };
+        for (int r = 0; r < N; ++r) {
+            int ql = 0, qu = 0;
+            for (size_t k = 0; k < rowcols[r].size(); ++k) {
+                int cc = rowcols[r][k];
+                if (ipart[cc] != ipart[r]) continue;
+                int sidx = cc < r ? ql++ : ML + qu++;
+                lu_col[lfid(r, sidx)] = cc;
+                lu_src[lfid(r, sidx)] = flat(r, 1 + (int)k);
+            }
+        }
         std::vector<int> lvl_off, part_lvl0(nparts + 1, 0);
         for (int r = 0; r < N; ++r) {
             if (r == 0 || ipart[r] != ipart[r - 1] || level[c.perm[r]] != level[c.perm[r - 1]]) lvl_off.push_back(r);
@@ -499,6 +507,9 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
             }
             part_lvl0[nparts] = (int)lvl_off.size() - 1;
         }
+        // IKJ update triples: for each L_rk (row order, then q), the pairs
+        // (U_kj, A_rj) with j > k in row k's upper factor and in row r's
+        // pattern (j == r: the diagonal, encoded -1)
         std::vector<int> nlu(N), low_start(N + 1, 0), tr_start(1, 0), tr_kj, tr_rj;
         for (int r = 0; r < N; ++r) {
             nlu[r] = nl[r] | (nu[r] << 8);
@@ -506,14 +517,14 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         }
         for (int r = 0; r < N; ++r) {
             for (int q = 0; q < nl[r]; ++q) {
-                int k = rowcols[r][q];
-                // U_kj for j > k in row k's same-subdomain upper part
+                int k = lu_col[lfid(r, q)];
                 for (int u = 0; u < nu[k]; ++u) {
-                    int j = rowcols[k][nl[k] + u];
-                    int kj = flat(k, 1 + ML + u);
+                    int j = lu_col[lfid(k, ML + u)];
+                    int kj = lfid(k, ML + u);
                     if (j == r) { tr_kj.push_back(kj); tr_rj.push_back(-1); continue; }
-                    int pj = pos_of(r, j);
-                    if (pj >= 0 && pj < nl[r] + nu[r]) { tr_kj.push_back(kj); tr_rj.push_back(flat(r, slot_of_pos(r, pj))); }
+                    if (ipart[j] != ipart[r]) continue;
+                    int rj = fid_of(r, j);
+                    if (rj >= 0) { tr_kj.push_back(kj); tr_rj.push_back(rj); }
                 }
                 tr_start.push_back((int)tr_kj.size());
             }
@@ -521,6 +532,8 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         c.part_lvl0.upload(part_lvl0, s); c.lvl_off.upload(lvl_off, s);
         c.low_start.upload(low_start, s); c.nlu.upload(nlu, s);
         c.tr_start.upload(tr_start, s); c.tr_kj.upload(tr_kj, s); c.tr_rj.upload(tr_rj, s);
+        c.lu_col.upload(lu_col, s); c.lu_src.upload(lu_src, s);
+        c.lu_slots = MS;
     }
     // ---- upload
     c.own.upload(own, s); c.nei.upload(nei, s); c.Sf.upload(Sf, s); c.magSf.upload(magSf, s); c.w.upload(w, s);
@@ -559,10 +572,11 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     CK(cudaMalloc(&c.Aval, mbytes));
     CK(cudaMemsetAsync(c.Aval, 0, mbytes, s));
     if (o.precon == PRECON_ILU0) {
-        CK(cudaMalloc(&c.LUval, mbytes));
-        CK(cudaMemsetAsync(c.LUval, 0, mbytes, s));
+        size_t lbytes = (size_t)c.n_slices * c.lu_slots * 32 * 25 * c.mt_size;
+        CK(cudaMalloc(&c.LUval, lbytes));
+        CK(cudaMemsetAsync(c.LUval, 0, lbytes, s));
     }
-    if (o.precon != PRECON_NONE) CK(cudaMalloc(&c.dinv, (size_t)25 * N * c.mt_size));
+    if (o.precon != PRECON_NONE) CK(cudaMalloc(&c.dinv, (size_t)c.n_slices * 32 * 25 * c.mt_size));
     // ---- Krylov
     const long n5 = 5L * N;
     c.dx.alloc(n5); c.r.alloc(n5); c.t.alloc(n5); c.Ax.alloc(n5); c.pA.alloc(n5); c.xbar.alloc(8);
@@ -615,10 +629,11 @@ struct Ops {
             k_dinv<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.dinv);
             CKL();
         } else if (c.o.precon == PRECON_ILU0) {
-            size_t mbytes = (size_t)c.n_slots * 32 * 25 * sizeof(MT);
-            CK(cudaMemcpyAsync(c.LUval, c.Aval, mbytes, cudaMemcpyDeviceToDevice, c.s));
             Timed tm(c, KS_FACTOR);
-            k_ilu_factor<MT><<<c.n_parts, ILU_TPB, 0, c.s>>>(c.mat<MT>(c.LUval), (MT*)c.dinv, c.ilu());
+            const int n_fid = c.n_slices * c.lu_slots * 32;
+            k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, c.lu_src.p, n_fid);
+            CKL();
+            k_ilu_factor<MT><<<c.n_parts, ILU_TPB, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
             CKL();
         }
     }
@@ -628,14 +643,15 @@ struct Ops {
             k_jacobi<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.N, (const MT*)c.dinv, in, out, active);
         else if (c.o.precon == PRECON_ILU0) {
             const int nb = std::max(c.ilu_ml, c.ilu_mu);
-            auto A = c.mat<MT>(c.LUval);
+            const MT* LU = (const MT*)c.LUval;
             auto P = c.ilu();
             const MT* di = (const MT*)c.dinv;
-            if (nb <= 2) k_ilu_apply<MT, 2><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
-            else if (nb <= 3) k_ilu_apply<MT, 3><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
-            else if (nb <= 4) k_ilu_apply<MT, 4><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
-            else if (nb <= 6) k_ilu_apply<MT, 6><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
-            else k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(A, di, P, in, out, active);
+            const int N = c.N;
+            if (nb <= 2) k_ilu_apply<MT, 2><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else if (nb <= 3) k_ilu_apply<MT, 3><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else if (nb <= 4) k_ilu_apply<MT, 4><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else if (nb <= 6) k_ilu_apply<MT, 6><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
         }
         else
             k_copy_identity<MT><<<nblk(c.nvec(), TPB), TPB, 0, c.s>>>((int)c.nvec(), in, out, active);
@@ -688,6 +704,32 @@ struct Ops {
             k_finalize<<<cnt, RED_TPB, 0, c.s>>>(c.partial.p, nb, cnt, 8, out + j0, 0, active); CKL();
         }
     }
+    // V^T w (one pass over w) into out[0..nv)
+    template <int NV>
+    static void vmultidot(rdst_ctx& c, int nv, const double* w, double* out, const int* active) {
+        long n = c.nvec();
+        int nb = red_blocks(n);
+        k_vmultidot<NV><<<nb, RED_TPB, 0, c.s>>>(n, nv, c.Vb.p, n, w, c.partial.p, 64, active); CKL();
+        k_finalize<<<nv, RED_TPB, 0, c.s>>>(c.partial.p, nb, nv, 64, out, 0, active); CKL();
+    }
+    // w -= V coef, fused with the next dots (mode 0) or the norm (mode 1)
+    template <int NV>
+    static void maxpy_dot(rdst_ctx& c, int nv, const double* coef, double* w, double* out, int mode,
+                          const int* active) {
+        long n = c.nvec();
+        int nb = red_blocks(n);
+        k_maxpy_dot<NV><<<nb, RED_TPB, 0, c.s>>>(n, nv, c.Vb.p, n, coef, w, c.partial.p, 64, mode, active); CKL();
+        if (mode == 0) { k_finalize<<<nv, RED_TPB, 0, c.s>>>(c.partial.p, nb, nv, 64, out, 0, active); CKL(); }
+        else { k_finalize<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, 1, 64, out, 1, active); CKL(); }
+    }
+    // CGS2 orthogonalisation of w against V_0..V_i: H[:,i] pieces, beta = |w|
+    template <int NV>
+    static void orth(rdst_ctx& c, int nv, double* w, const int* act) {
+        Scalars* sc = c.sc.p;
+        vmultidot<NV>(c, nv, w, sc->hcol[0], act);
+        maxpy_dot<NV>(c, nv, sc->hcol[0], w, sc->hcol[1], 0, act);
+        maxpy_dot<NV>(c, nv, sc->hcol[1], w, &sc->beta, 1, act);
+    }
     // one restart cycle of left-preconditioned GMRES(m) with CGS2
     static void gmres_cycle(rdst_ctx& c) {
         cudaStream_t s = c.s;
@@ -708,12 +750,12 @@ struct Ops {
             precond(c, c.t.p, w, act);
             {
                 Timed tm(c, KS_ORTH);
-                multidot(c, i + 1, w, sc->hcol[0], act);
-                k_maxpy<<<nblk(n, TPB), TPB, 0, s>>>(n, i + 1, c.Vb.p, n, sc->hcol[0], w, 1.0, act); CKL();
-                multidot(c, i + 1, w, sc->hcol[1], act);
-                k_maxpy<<<nblk(n, TPB), TPB, 0, s>>>(n, i + 1, c.Vb.p, n, sc->hcol[1], w, 1.0, act); CKL();
+                const int nv = i + 1;
+                if (nv <= 8) orth<8>(c, nv, w, act);
+                else if (nv <= 16) orth<16>(c, nv, w, act);
+                else if (nv <= 32) orth<32>(c, nv, w, act);
+                else orth<64>(c, nv, w, act);
             }
-            dot(c, w, w, &sc->beta, 1, act);
             k_gm_givens<<<1, 1, 0, s>>>(sc, i, m); CKL();
             if (i < m - 1) { k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, w, &sc->beta, act); CKL(); }
         }
