@@ -147,6 +147,9 @@ struct Ctx {
     // valueFraction of the mixed-type BCs at their last evaluation
     // (used by valueInternalCoeffs in the boundary Jacobian)
     std::vector<double> fp_b, fU_b, fT_b;
+    // turbulence: mut (cells, boundary faces), nuTilda; viscous switch
+    std::vector<double> mut, mut_b, nut, nut_b;
+    bool viscous = false;
     // residual R_ (baseFluxDST R_, per unit volume) and face fluxes
     std::vector<v5> Rv;
     std::vector<double> phi, phiEp;
@@ -693,6 +696,8 @@ FaceFlux flux_ausm(const Side& o, const Side& n, const v3& Sf, double magSf) {
 // ----------------------------------------------------------------------
 // Residual: reconstruction + face fluxes + calcFields (baseFluxDST.C:223-255)
 // ----------------------------------------------------------------------
+void viscous_terms(Ctx& c);
+double mu_of_T(const Ctx& c, double T);
 void compute_flux(Ctx& c) {
     const double g = c.gamma;
     const bool kt = (c.o.flux == FLUX_KURGANOV || c.o.flux == FLUX_AUSM);
@@ -756,17 +761,105 @@ void compute_flux(Ctx& c) {
     }
     // calcFields: R = [div(phi), div(phiUp), div(phiEp)] (fvc::div = surface sum / V)
     c.Rv.assign(c.N, v5{0, 0, 0, 0, 0});
+    auto div = [&](int i, auto&& val) {
+        double r = 0;
+        for (int f : c.cellFaces[i]) r += ((c.own[f] == i) ? 1.0 : -1.0) * val(f);
+        return r / c.V[i];
+    };
     for (int i = 0; i < c.N; ++i) {
-        v5 r{0, 0, 0, 0, 0};
-        for (int f : c.cellFaces[i]) {
-            double sg = (c.own[f] == i) ? 1.0 : -1.0;
-            r[0] += sg * c.phi[f];
-            r[1] += sg * c.phiUp[f][0];
-            r[2] += sg * c.phiUp[f][1];
-            r[3] += sg * c.phiUp[f][2];
-            r[4] += sg * c.phiEp[f];
+        c.Rv[i][0] = div(i, [&](int f) { return c.phi[f]; });
+        for (int k = 0; k < 3; ++k) c.Rv[i][1 + k] = div(i, [&](int f) { return c.phiUp[f][k]; });
+        c.Rv[i][4] = div(i, [&](int f) { return c.phiEp[f]; });
+    }
+    if (c.viscous) viscous_terms(c);
+}
+
+// Laminar viscosity: constTransport mu, or Sutherland As sqrt(T)/(1 + Ts/T)
+double mu_of_T(const Ctx& c, double T) {
+    if (c.o.As > 0) return c.o.As * std::sqrt(T) / (1.0 + c.o.Ts / T);
+    return c.o.mu;
+}
+
+// Viscous part of baseFluxDST::calcFields (baseFluxDST.C:229-250):
+//   tauMC     = muEff dev2(T(grad U))
+//   sigmaDotU = (interpolate(muEff)|Sf| snGrad(U) + Sf . interpolate(tauMC)) . Up
+//   R_U      -= laplacian(muEff, U) + div(tauMC),  R_E -= div(sigmaDotU)
+// Gauss linear gradient; corrected snGrad  dc (U_N - U_P) + k . (grad U)_f
+// with k = n - d dc (foam-extend nonOrthCorrectionVectors); boundary
+// snGrad = (U_b - U_P) dc_b and boundary gradient
+// grad U_P + n (snGrad_b - n . grad U_P) (gaussGrad::correctBoundaryConditions).
+// No heat-conduction term in the energy equation (as in the reference).
+void viscous_terms(Ctx& c) {
+    typedef std::array<double, 9> t3;
+    std::vector<t3> gU;
+    grad_vector(c, c.U, c.U_b, gU);
+    std::vector<double> muE(c.N), muE_b(c.NB, 0.0);
+    for (int i = 0; i < c.N; ++i) muE[i] = mu_of_T(c, c.T[i]) + c.mut[i];
+    for (int b = 0; b < c.NB; ++b) if (c.active[b]) muE_b[b] = mu_of_T(c, c.T_b[b]) + c.mut_b[b];
+    auto tau_of = [&](const t3& g, double m) {
+        // dev2(T(g)) with T(g)(i,j) = g(j,i): t(i,j) = m (g(j,i) - 2/3 tr(g) d_ij)
+        double tr = g[0] + g[4] + g[8];
+        t3 t;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) t[3 * i + j] = m * (g[3 * j + i] - (i == j ? (2.0 / 3.0) * tr : 0.0));
+        return t;
+    };
+    std::vector<t3> tau(c.N);
+    for (int i = 0; i < c.N; ++i) tau[i] = tau_of(gU[i], muE[i]);
+    std::vector<v3> lap(c.F, v3{0, 0, 0}), tauS(c.F, v3{0, 0, 0});
+    std::vector<double> sig(c.F, 0.0);
+    for (int f = 0; f < c.Fi; ++f) {
+        int P = c.own[f], Q = c.nei[f];
+        double w = c.w[f];
+        v3 n = c.Sf[f] / c.magSf[f];
+        v3 d = c.C[Q] - c.C[P];
+        v3 kc = n - c.dc[f] * d;
+        double muf = w * muE[P] + (1 - w) * muE[Q];
+        v3 sn;
+        for (int j = 0; j < 3; ++j) {
+            double corr = 0;
+            for (int i = 0; i < 3; ++i) corr += kc[i] * (w * gU[P][3 * i + j] + (1 - w) * gU[Q][3 * i + j]);
+            sn[j] = c.dc[f] * (c.U[Q][j] - c.U[P][j]) + corr;
         }
-        for (int k = 0; k < 5; ++k) c.Rv[i][k] = r[k] / c.V[i];
+        v3 ts;
+        for (int j = 0; j < 3; ++j) {
+            double a = 0;
+            for (int i = 0; i < 3; ++i) a += c.Sf[f][i] * (w * tau[P][3 * i + j] + (1 - w) * tau[Q][3 * i + j]);
+            ts[j] = a;
+        }
+        lap[f] = (muf * c.magSf[f]) * sn;
+        tauS[f] = ts;
+        sig[f] = dot(lap[f] + tauS[f], c.Up[f]);
+    }
+    for (int b = 0; b < c.NB; ++b) {
+        if (!c.active[b]) continue;
+        int f = c.Fi + b, P = c.own[f];
+        v3 n = c.Sf[f] / c.magSf[f];
+        v3 snb = c.dc[f] * (c.U_b[b] - c.U[P]);
+        t3 gb = gU[P];
+        for (int j = 0; j < 3; ++j) {
+            double ng = n[0] * gb[j] + n[1] * gb[3 + j] + n[2] * gb[6 + j];
+            for (int i = 0; i < 3; ++i) gb[3 * i + j] += n[i] * (snb[j] - ng);
+        }
+        t3 tb = tau_of(gb, muE_b[b]);
+        v3 ts;
+        for (int j = 0; j < 3; ++j) ts[j] = c.Sf[f][0] * tb[j] + c.Sf[f][1] * tb[3 + j] + c.Sf[f][2] * tb[6 + j];
+        lap[f] = (muE_b[b] * c.magSf[f]) * snb;
+        tauS[f] = ts;
+        sig[f] = dot(lap[f] + tauS[f], c.Up[f]);
+    }
+    auto div = [&](int i, auto&& val) {
+        double r = 0;
+        for (int f : c.cellFaces[i]) r += ((c.own[f] == i) ? 1.0 : -1.0) * val(f);
+        return r / c.V[i];
+    };
+    for (int i = 0; i < c.N; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            double l = div(i, [&](int f) { return lap[f][k]; });
+            double t = div(i, [&](int f) { return tauS[f][k]; });
+            c.Rv[i][1 + k] -= l + t;
+        }
+        c.Rv[i][4] -= div(i, [&](int f) { return sig[f]; });
     }
 }
 
@@ -823,7 +916,17 @@ void assemble(Ctx& c, LDU& A) {
         v3 Uf = c.w[f] * Uc[P] + (1 - c.w[f]) * Uc[Q];
         double cf = c.w[f] * cc[P] + (1 - c.w[f]) * cc[Q];
         double amaxSf = std::fabs(dot(Uf, c.Sf[f])) + c.magSf[f] * cf;
-        lambda[f] = 0.5 * amaxSf;           // + viscous part (zero for inviscid)
+        if (c.viscous) {
+            // + |Sf| (muEff_f + alphaEff_f)/rho_f deltaCoeffs (Roe.C:187-199),
+            // alpha = mu/Pr, alphat = mut/Prt, rho_f = interpolate(p psi)
+            double mP = mu_of_T(c, c.T[P]), mQ = mu_of_T(c, c.T[Q]);
+            double muEf = c.w[f] * (mP + c.mut[P]) + (1 - c.w[f]) * (mQ + c.mut[Q]);
+            double alEf = c.w[f] * (mP / c.o.Pr + c.mut[P] / c.o.Prt) + (1 - c.w[f]) * (mQ / c.o.Pr + c.mut[Q] / c.o.Prt);
+            double rhof = c.w[f] * c.p[P] / (c.R * c.T[P]) + (1 - c.w[f]) * c.p[Q] / (c.R * c.T[Q]);
+            lambda[f] = 0.5 * (amaxSf + c.magSf[f] * (muEf + alEf) / rhof * c.dc[f]);
+        } else {
+            lambda[f] = 0.5 * amaxSf;
+        }
         for (int k = 0; k < 25; ++k) {
             double oc = Jo[k] * c.w[f];          // ownerCoeffs *= weights
             double nc = Jn[k] * (1 - c.w[f]);    // neighbourCoeffs *= (1 - weights)
@@ -1366,7 +1469,7 @@ ORACLE_API rdst_status rdsto_create(const rdst_mesh* m, int32_t n_opts, const ch
     } catch (const ConfigError& e) {
         return e.unsupported ? RDST_ERR_UNSUPPORTED : RDST_ERR_CONFIG;
     }
-    if (c.o.mu > 0 || c.o.As > 0 || c.o.turbulence != TURB_LAMINAR) return RDST_ERR_UNSUPPORTED;
+    if (c.o.turbulence != TURB_LAMINAR) return RDST_ERR_UNSUPPORTED;
     c.N = m->n_cells; c.Fi = m->n_internal_faces; c.F = m->n_faces; c.NB = c.F - c.Fi;
     if (c.N <= 0 || c.Fi < 0 || c.F < c.Fi) return RDST_ERR_MESH;
     c.own.assign(m->owner, m->owner + c.F);
@@ -1412,6 +1515,8 @@ ORACLE_API rdst_status rdsto_create(const rdst_mesh* m, int32_t n_opts, const ch
     c.rho_b.assign(NB, 0); c.rhoE_b.assign(NB, 0); c.p_b.assign(NB, 0); c.T_b.assign(NB, 0);
     c.h_b.assign(NB, 0); c.phi_b.assign(NB, 0); c.rhoU_b.assign(NB, v3{0, 0, 0}); c.U_b.assign(NB, v3{0, 0, 0});
     c.fp_b.assign(NB, 0); c.fU_b.assign(NB, 0); c.fT_b.assign(NB, 0);
+    c.mut.assign(Nn, 0.0); c.mut_b.assign(NB, 0.0); c.nut.assign(Nn, 0.0); c.nut_b.assign(NB, 0.0);
+    c.viscous = (c.o.mu > 0 || c.o.As > 0 || c.o.turbulence != TURB_LAMINAR);
     *out = h.release();
     return RDST_OK;
 }

@@ -172,3 +172,24 @@ def swept_wing_c3(n_around: int = 192, n_normal: int = 64, n_span: int = 64, n_t
     return Case("sweptWing", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N), steps=2000,
                 force_patch="wing",
                 force_dirs={"lift": (-math.sin(al), math.cos(al), 0.0), "drag": (math.cos(al), math.sin(al), 0.0)})
+
+
+def naca0012_laminar(ni: int = 129, nj: int = 33, mach: float = 0.5, alpha: float = 1.0, reynolds: float = 5000.0,
+                     flux: str = "AUSM+up", limiter: str = "vanLeer", sutherland: bool = False) -> Case:
+    """Laminar NACA0012 (no-slip adiabatic wall) with the viscous terms of
+    calcFields; constant viscosity from the chord Reynolds number, or
+    Sutherland's law scaled to the same free-stream viscosity."""
+    c = naca0012_inviscid(ni, nj, mach=mach, alpha=alpha, flux=flux, limiter=limiter, n_directions=20)
+    gas = c.options["thermo"]
+    rho_inf = 1.0 / gas["R"]
+    U_inf = mach * math.sqrt(gas["Cp"] / (gas["Cp"] - gas["R"]) * gas["R"])
+    mu_inf = rho_inf * U_inf * 1.0 / reynolds
+    c.bcs["airfoil"] = {"p": "zeroGradient", "U": ("fixedValue", (0.0, 0.0, 0.0)), "T": "zeroGradient"}
+    if sutherland:
+        Ts = 0.4
+        As = mu_inf * (1.0 + Ts) / 1.0          # mu(T=1) = mu_inf
+        c.options["transport"] = {"As": As, "Ts": Ts, "Pr": 0.72}
+    else:
+        c.options["transport"] = {"mu": mu_inf, "Pr": 0.72}
+    c.name = "naca0012_laminar"
+    return c

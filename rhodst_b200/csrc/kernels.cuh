@@ -71,6 +71,15 @@ __device__ __forceinline__ double block_max(double v) {
 // ------------------------------------------------------------------ state / BCs
 struct Bounds { double rho_min, rho_max, p_min, p_max, T_min, T_max; };
 
+// constTransport mu / Prandtl, or Sutherland mu = As sqrt(T)/(1 + Ts/T)
+struct Transport {
+    double mu, As, Ts, Pr, Prt;
+    int viscous;
+    __device__ __forceinline__ double mu_of_T(double T) const {
+        return As > 0 ? As * sqrt(T) / (1.0 + Ts / T) : mu;
+    }
+};
+
 // initial state from primitives (createFields.H:21-72)
 __global__ void k_init_state(int N, Thermo th, const double* __restrict__ prim, double* __restrict__ W) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -192,6 +201,9 @@ __global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __rest
     B[8] = fp;
     B[9] = fU;
     B[10] = fT;
+    B[12] = Ub.x;
+    B[13] = Ub.y;
+    B[14] = Ub.z;
 }
 
 // ------------------------------------------------------------------ residual
@@ -199,8 +211,9 @@ __global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __rest
 // q = (rho, rhoU xyz, rPsi = RT, e = h - p/rho, s) with s = c = sqrt(gamma RT)
 // (Kurganov, AUSM) or the critical speed sqrt(2(g-1)/(g+1) H) (HLL family,
 // AUSM+, AUSM+up; HLLDST.C:130-137).
-__global__ void k_recon(DevMesh m, Thermo th, int use_c, const double* __restrict__ W, const double* __restrict__ prim,
-                        const double* __restrict__ bs, double* __restrict__ q, double* __restrict__ qb) {
+__global__ void k_recon(DevMesh m, Thermo th, Transport tr, int use_c, const double* __restrict__ W,
+                        const double* __restrict__ prim, const double* __restrict__ bs, const double* __restrict__ mut,
+                        const double* __restrict__ mut_b, double* __restrict__ q, double* __restrict__ qb) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double g = th.gamma;
     if (i < m.N) {
@@ -216,7 +229,8 @@ __global__ void k_recon(DevMesh m, Thermo th, int use_c, const double* __restric
         }
         double* o = q + QW * i;
         o[0] = rho; o[1] = w5[1]; o[2] = w5[2]; o[3] = w5[3];
-        o[4] = rPsi; o[5] = h - p / rho; o[6] = s; o[7] = 0.0;
+        o[4] = rPsi; o[5] = h - p / rho; o[6] = s;
+        o[7] = tr.viscous ? tr.mu_of_T(T) + mut[i] : 0.0;     // muEff
     } else if (i < m.N + m.NB) {
         int b = i - m.N;
         const double* B = bs + BW * b;
@@ -231,7 +245,8 @@ __global__ void k_recon(DevMesh m, Thermo th, int use_c, const double* __restric
         }
         double* o = qb + QW * b;
         o[0] = rho; o[1] = B[1]; o[2] = B[2]; o[3] = B[3];
-        o[4] = rPsi; o[5] = h - p / rho; o[6] = s; o[7] = 0.0;
+        o[4] = rPsi; o[5] = h - p / rho; o[6] = s;
+        o[7] = tr.viscous ? tr.mu_of_T(T) + mut_b[b] : 0.0;
     }
 }
 
@@ -241,7 +256,8 @@ __global__ void k_recon(DevMesh m, Thermo th, int use_c, const double* __restric
 __global__ void __launch_bounds__(128) k_grad(DevMesh m, int venkat_mask, double venkat_K, const double* __restrict__ q,
                                               const double* __restrict__ qb, const double* __restrict__ prim,
                                               double* __restrict__ g, double* __restrict__ psi,
-                                              double* __restrict__ fcell, int hllcp) {
+                                              double* __restrict__ fcell, int hllcp, const double* __restrict__ bs,
+                                              double* __restrict__ gU) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.N) return;
     double acc[21];
@@ -250,6 +266,7 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, int venkat_mask, double
     const int k0 = m.cf_start[i], k1 = m.cf_start[i + 1];
     double fmin_c = 1.0;
     const double pi = prim[PW * i];
+    double aU[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};    // (grad U)_ij = dU_j/dx_i
     for (int k = k0; k < k1; ++k) {
         int code = m.cf_list[k];
         if (code < m.Fi) {
@@ -258,6 +275,16 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, int venkat_mask, double
             V3 S = ldv3(m.Sf, m.Fi, f);
             const double* qo = q + QW * o;
             const double* qn = q + QW * n;
+            if (gU) {
+                const double sg = (o == i) ? 1.0 : -1.0;
+                const double Sv[3] = {sg * S.x, sg * S.y, sg * S.z};
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    double xf = wf * prim[PW * o + 3 + j] + (1 - wf) * prim[PW * n + 3 + j];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) aU[3 * d + j] += Sv[d] * xf;
+                }
+            }
             if (o == i) {
 #pragma unroll
                 for (int j = 0; j < 7; ++j) {
@@ -284,9 +311,20 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, int venkat_mask, double
                 double xf = qq[j];
                 acc[3 * j] += xf * S.x; acc[3 * j + 1] += xf * S.y; acc[3 * j + 2] += xf * S.z;
             }
+            if (gU) {
+                const double Sv[3] = {S.x, S.y, S.z};
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) aU[3 * d + j] += Sv[d] * bs[BW * b + 12 + j];
+            }
         }
     }
     const double Vi = m.V[i];
+    if (gU) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) gU[9 * i + k] = aU[k] / Vi;
+    }
     double* go = g + GW * i;
 #pragma unroll
     for (int k = 0; k < 21; ++k) { acc[k] /= Vi; go[k] = acc[k]; }
@@ -341,7 +379,8 @@ __device__ __forceinline__ void recon_scalar(int L, double xP, double xN, V3 gP,
 __global__ void __launch_bounds__(128) k_face_flux(DevMesh m, Thermo th, int scheme, int lr, int lu, int lt,
                                                    int lowMach, double Mainf, const double* __restrict__ q,
                                                    const double* __restrict__ g, const double* __restrict__ psi,
-                                                   const double* __restrict__ fcell, double* __restrict__ fl) {
+                                                   const double* __restrict__ fcell, double* __restrict__ fl,
+                                                   double* __restrict__ up) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.Fi) return;
     const int o = m.own[f], n = m.nei[f];
@@ -403,12 +442,13 @@ __global__ void __launch_bounds__(128) k_face_flux(DevMesh m, Thermo th, int sch
     FFlux F = face_flux(scheme, so, sn, S, magS, th.gamma, fs, lowMach != 0, Mainf);
     double* out = fl + 5 * f;
     out[0] = F.phi; out[1] = F.phiUp.x; out[2] = F.phiUp.y; out[3] = F.phiUp.z; out[4] = F.phiEp;
+    if (up) { up[3 * f] = F.Up.x; up[3 * f + 1] = F.Up.y; up[3 * f + 2] = F.Up.z; }
 }
 
 // Boundary face fluxes: both sides carry the boundary value (foam
 // interpolate() returns the patch value on non-coupled patches).
 __global__ void k_bface_flux(DevMesh m, Thermo th, int scheme, int lowMach, double Mainf, const double* __restrict__ qb,
-                             double* __restrict__ bfl, double* __restrict__ bs) {
+                             double* __restrict__ bfl, double* __restrict__ bs, double* __restrict__ bup) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.NB) return;
     const double* qq = qb + QW * b;
@@ -418,30 +458,138 @@ __global__ void k_bface_flux(DevMesh m, Thermo th, int scheme, int lowMach, doub
     double* out = bfl + 5 * b;
     out[0] = F.phi; out[1] = F.phiUp.x; out[2] = F.phiUp.y; out[3] = F.phiUp.z; out[4] = F.phiEp;
     bs[BW * b + 7] = F.phi;
+    if (bup) { bup[3 * b] = F.Up.x; bup[3 * b + 1] = F.Up.y; bup[3 * b + 2] = F.Up.z; }
+}
+
+// tau = muEff dev2(T(grad U)): t(i,j) = mu (g(j,i) - 2/3 tr(g) d_ij)
+__device__ __forceinline__ void tau_of(const double g[9], double mu, double t[9]) {
+    const double tr = g[0] + g[4] + g[8];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) t[3 * i + j] = mu * (g[3 * j + i] - (i == j ? (2.0 / 3.0) * tr : 0.0));
+}
+
+// Viscous face terms of calcFields (baseFluxDST.C:229-250) per internal
+// face: lap = muEff_f |Sf| snGrad(U) (corrected: dc (U_N - U_P) +
+// (n - d dc) . (grad U)_f), tauS = Sf . (tau)_f, sig = (lap + tauS) . Up.
+__global__ void __launch_bounds__(128) k_visc_faces(DevMesh m, const double* __restrict__ q, const double* __restrict__ prim,
+                                                    const double* __restrict__ gU, const double* __restrict__ up,
+                                                    double* __restrict__ vf) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.Fi) return;
+    const int P = m.own[f], Q = m.nei[f];
+    const double w = m.w[f], dc = m.dc[f], magS = m.magSf[f];
+    const V3 S = ldv3(m.Sf, m.Fi, f);
+    const V3 n = div3(S, magS);
+    const V3 d = ldv3(m.d, m.Fi, f);
+    const V3 kc = sub3(n, scl3(dc, d));
+    const double muP = q[QW * P + 7], muQ = q[QW * Q + 7];
+    const double muf = w * muP + (1 - w) * muQ;
+    double gP[9], gQ[9], tP[9], tQ[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { gP[k] = gU[9 * P + k]; gQ[k] = gU[9 * Q + k]; }
+    tau_of(gP, muP, tP);
+    tau_of(gQ, muQ, tQ);
+    const double kv[3] = {kc.x, kc.y, kc.z}, Sv[3] = {S.x, S.y, S.z};
+    double lap[3], ts[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        double corr = 0, a = 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            corr += kv[i] * (w * gP[3 * i + j] + (1 - w) * gQ[3 * i + j]);
+            a += Sv[i] * (w * tP[3 * i + j] + (1 - w) * tQ[3 * i + j]);
+        }
+        double sn = dc * (prim[PW * Q + 3 + j] - prim[PW * P + 3 + j]) + corr;
+        lap[j] = (muf * magS) * sn;
+        ts[j] = a;
+    }
+    double sig = (lap[0] + ts[0]) * up[3 * f] + (lap[1] + ts[1]) * up[3 * f + 1] + (lap[2] + ts[2]) * up[3 * f + 2];
+    double* o = vf + 8 * f;
+    o[0] = lap[0]; o[1] = lap[1]; o[2] = lap[2]; o[3] = ts[0]; o[4] = ts[1]; o[5] = ts[2]; o[6] = sig;
+}
+
+// boundary faces: snGrad = (U_b - U_P) dc_b, gradient corrected to the
+// patch snGrad (gaussGrad::correctBoundaryConditions), tau_b from muEff_b
+__global__ void k_visc_bfaces(DevMesh m, const double* __restrict__ qb, const double* __restrict__ prim,
+                              const double* __restrict__ gU, const double* __restrict__ bs,
+                              const double* __restrict__ bup, double* __restrict__ bvf) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.NB) return;
+    const int P = m.bcell[b];
+    const double magS = m.bmagSf[b], dc = m.bdc[b];
+    const V3 S = ldv3(m.bSf, m.NB, b);
+    const double n[3] = {S.x / magS, S.y / magS, S.z / magS}, Sv[3] = {S.x, S.y, S.z};
+    const double* B = bs + BW * b;
+    double snb[3], g[9], t[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) snb[j] = dc * (B[12 + j] - prim[PW * P + 3 + j]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) g[k] = gU[9 * P + k];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        double ng = n[0] * g[j] + n[1] * g[3 + j] + n[2] * g[6 + j];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g[3 * i + j] += n[i] * (snb[j] - ng);
+    }
+    const double mub = qb[QW * b + 7];
+    tau_of(g, mub, t);
+    double lap[3], ts[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        ts[j] = Sv[0] * t[j] + Sv[1] * t[3 + j] + Sv[2] * t[6 + j];
+        lap[j] = (mub * magS) * snb[j];
+    }
+    double sig = (lap[0] + ts[0]) * bup[3 * b] + (lap[1] + ts[1]) * bup[3 * b + 1] + (lap[2] + ts[2]) * bup[3 * b + 2];
+    double* o = bvf + 8 * b;
+    o[0] = lap[0]; o[1] = lap[1]; o[2] = lap[2]; o[3] = ts[0]; o[4] = ts[1]; o[5] = ts[2]; o[6] = sig;
 }
 
 // calcFields (baseFluxDST.C:223-255): R = div(face fluxes) per unit volume,
 // gathered per cell in foam face order; rhs = -R V (fluxDST.C:124); fused
 // partial sums for |R|^2 (timeDST.C:330) and (R V)^2 per component.
 __global__ void k_residual(DevMesh m, const double* __restrict__ fl, const double* __restrict__ bfl,
+                           const double* __restrict__ vf, const double* __restrict__ bvf,
                            double* __restrict__ R, double* __restrict__ rhs, double* __restrict__ partial) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double r[5] = {0, 0, 0, 0, 0};
+    double vs[7] = {0, 0, 0, 0, 0, 0, 0};
     double sq_mag = 0, sq_c[5] = {0, 0, 0, 0, 0};
     if (i < m.N) {
         for (int k = m.cf_start[i]; k < m.cf_start[i + 1]; ++k) {
             int code = m.cf_list[k];
             const double* F;
+            const double* Fv = nullptr;
             double sg = 1.0;
-            if (code < m.Fi) { F = fl + 5 * code; sg = (m.own[code] == i) ? 1.0 : -1.0; }
-            else F = bfl + 5 * (code - m.Fi);
+            if (code < m.Fi) {
+                F = fl + 5 * code;
+                sg = (m.own[code] == i) ? 1.0 : -1.0;
+                if (vf) Fv = vf + 8 * code;
+            } else {
+                F = bfl + 5 * (code - m.Fi);
+                if (bvf) Fv = bvf + 8 * (code - m.Fi);
+            }
 #pragma unroll
             for (int c = 0; c < 5; ++c) r[c] += sg * F[c];
+            if (Fv) {
+#pragma unroll
+                for (int c = 0; c < 7; ++c) vs[c] += sg * Fv[c];
+            }
         }
         double Vi = m.V[i];
+        double Rv[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) Rv[c] = r[c] / Vi;
+        if (vf) {
+            // R_U -= laplacian(muEff,U) + div(tauMC); R_E -= div(sigmaDotU)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Rv[1 + k] -= vs[k] / Vi + vs[3 + k] / Vi;
+            Rv[4] -= vs[6] / Vi;
+        }
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
-            double Rc = r[c] / Vi;
+            double Rc = Rv[c];
             R[5 * i + c] = Rc;
             double rv = Rc * Vi;
             rhs[5 * i + c] = 0.0 - rv;
@@ -479,9 +627,11 @@ __device__ __forceinline__ size_t sidx(const int* slice_off, int r, int k, int e
 // the diagonal as ddt + negSumDiag + boundary Jacobians (fluxDST.C:98-112),
 // accumulated in foam face order.
 template <typename MT>
-__global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, SellMat<MT> A, const int* __restrict__ cf_slot,
+__global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, Transport tr, SellMat<MT> A,
+                                                  const int* __restrict__ cf_slot,
                                                   const double* __restrict__ W, const double* __restrict__ prim,
                                                   const double* __restrict__ bs, const double* __restrict__ rdtc,
+                                                  const double* __restrict__ mut,
                                                   const Scalars* __restrict__ sc, int steady, double beta) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= m.N) return;
@@ -522,7 +672,19 @@ __global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, SellMat<
             V3 Uf = add3(scl3(wf, Uo), scl3(1 - wf, Un));
             double cf = wf * co + (1 - wf) * cn;
             double amaxSf = fabs(dot3(Uf, S)) + magS * cf;
-            double lambda = 0.5 * amaxSf;
+            double lambda;
+            if (tr.viscous) {
+                // + |Sf| (muEff_f + alphaEff_f)/rho_f deltaCoeffs (Roe.C:187-199)
+                const int Po = isOwner ? r : oc_, Qn = isOwner ? oc_ : r;
+                double TP = prim[PW * Po + 1], TQ = prim[PW * Qn + 1];
+                double mP = tr.mu_of_T(TP), mQ = tr.mu_of_T(TQ);
+                double muEf = wf * (mP + mut[Po]) + (1 - wf) * (mQ + mut[Qn]);
+                double alEf = wf * (mP / tr.Pr + mut[Po] / tr.Prt) + (1 - wf) * (mQ / tr.Pr + mut[Qn] / tr.Prt);
+                double rhof = wf * prim[PW * Po] / (th.R * TP) + (1 - wf) * prim[PW * Qn] / (th.R * TQ);
+                lambda = 0.5 * (amaxSf + magS * (muEf + alEf) / rhof * m.dc[f]);
+            } else {
+                lambda = 0.5 * amaxSf;
+            }
             calcJ(Ur, g, phiJr, a1r, nn, J);
             calcJ(Uc, g, phiJc, a1c, nn, Jc);
             const int cs = cf_slot[k];

@@ -146,6 +146,9 @@ struct rdst_ctx {
     // fields
     DBuf<double> W, prim, bs, q, qb, g, psi, fcell, fl, bfl, R, rhs, partial;
     DBuf<double> rdt, courantF, rhoOld, eOld, eNew;
+    // viscous: grad U, face Up, viscous face terms, turbulent viscosity
+    DBuf<double> gU, up, bup, vf, bvf, mut, mut_b;
+    Transport tr{};
     DBuf<Scalars> sc;
     DBuf<rdst_step_report> reps;
     // matrix
@@ -290,6 +293,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     const Options& o = c.o;
     c.th.R = o.R; c.th.Cp = o.Cp; c.th.Cv = o.Cv(); c.th.gamma = o.gamma();
     c.bd = Bounds{o.rho_min, o.rho_max, o.p_min, o.p_max, o.T_min, o.T_max};
+    c.tr = Transport{o.mu, o.As, o.Ts, o.Pr, o.Prt, (o.mu > 0 || o.As > 0 || o.turbulence != TURB_LAMINAR) ? 1 : 0};
     c.steady = (o.ddt == DDT_STEADY);
     // active boundary faces
     std::vector<int> fpatch(c.NBall, -1);
@@ -560,6 +564,11 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     c.q.alloc((size_t)QW * N); c.qb.alloc((size_t)QW * std::max(NB, 1)); c.g.alloc((size_t)GW * N);
     c.psi.alloc((size_t)QW * N); c.fcell.alloc(N); c.fl.alloc(5L * std::max(Fi, 1)); c.bfl.alloc(5L * std::max(NB, 1));
     c.R.alloc(5L * N); c.rhs.alloc(5L * N);
+    c.mut.alloc(N); c.mut.zero(s); c.mut_b.alloc(std::max(NB, 1)); c.mut_b.zero(s);
+    if (c.tr.viscous) {
+        c.gU.alloc(9L * N); c.up.alloc(3L * std::max(Fi, 1)); c.bup.alloc(3L * std::max(NB, 1));
+        c.vf.alloc(8L * std::max(Fi, 1)); c.bvf.alloc(8L * std::max(NB, 1));
+    }
     c.rdt.alloc(N); c.courantF.alloc(N); c.rhoOld.alloc(N); c.eOld.alloc(N); c.eNew.alloc(N);
     c.sc.alloc(1); c.sc.zero(s);
     c.reps.alloc(rdst_ctx::REP_CAP);
@@ -596,23 +605,38 @@ struct Ops {
         cudaStream_t s = c.s;
         const DevMesh& m = c.m;
         int use_c = (o.flux == FLUX_KURGANOV || o.flux == FLUX_AUSM);
-        k_recon<<<nblk(m.N + m.NB, TPB), TPB, 0, s>>>(m, c.th, use_c, c.W.p, c.prim.p, c.bs.p, c.q.p, c.qb.p);
+        const bool visc = c.tr.viscous != 0;
+        k_recon<<<nblk(m.N + m.NB, TPB), TPB, 0, s>>>(m, c.th, c.tr, use_c, c.W.p, c.prim.p, c.bs.p, c.mut.p, c.mut_b.p,
+                                                     c.q.p, c.qb.p);
         CKL();
         k_grad<<<nblk(m.N, 128), 128, 0, s>>>(m, c.venkat_mask, o.venkat_K, c.q.p, c.qb.p, c.prim.p, c.g.p, c.psi.p,
-                                             c.fcell.p, o.flux == FLUX_HLLCP);
+                                             c.fcell.p, o.flux == FLUX_HLLCP, c.bs.p, visc ? c.gU.p : nullptr);
         CKL();
         if (m.Fi > 0) {
             Timed tm(c, KS_FLUX);
             k_face_flux<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
                                                        lim_code(o.lim_T), o.low_mach, o.mainf, c.q.p, c.g.p, c.psi.p,
-                                                       c.fcell.p, c.fl.p);
+                                                       c.fcell.p, c.fl.p, visc ? c.up.p : nullptr);
             CKL();
         }
-        if (m.NB > 0)
-            k_bface_flux<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), o.low_mach, o.mainf, c.qb.p, c.bfl.p, c.bs.p);
-        CKL();
+        if (m.NB > 0) {
+            k_bface_flux<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), o.low_mach, o.mainf, c.qb.p, c.bfl.p,
+                                                        c.bs.p, visc ? c.bup.p : nullptr);
+            CKL();
+        }
+        if (visc) {
+            if (m.Fi > 0) {
+                k_visc_faces<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.q.p, c.prim.p, c.gU.p, c.up.p, c.vf.p);
+                CKL();
+            }
+            if (m.NB > 0) {
+                k_visc_bfaces<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.qb.p, c.prim.p, c.gU.p, c.bs.p, c.bup.p, c.bvf.p);
+                CKL();
+            }
+        }
         int nb = nblk(m.N, TPB);
-        k_residual<<<nb, TPB, 0, s>>>(m, c.fl.p, c.bfl.p, c.R.p, c.rhs.p, c.partial.p);
+        k_residual<<<nb, TPB, 0, s>>>(m, c.fl.p, c.bfl.p, visc ? c.vf.p : nullptr, visc ? c.bvf.p : nullptr, c.R.p,
+                                      c.rhs.p, c.partial.p);
         CKL();
         k_residual_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, c.sc.p);
         CKL();
@@ -620,8 +644,8 @@ struct Ops {
     static void assemble(rdst_ctx& c) {
         SellMat<MT> A = c.mat<MT>(c.Aval);
         Timed tm(c, KS_ASSEMBLE);
-        k_assemble<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.m, c.th, A, c.cf_slot.p, c.W.p, c.prim.p, c.bs.p, c.rdt.p,
-                                                        c.sc.p, c.steady ? 1 : 0, c.o.beta);
+        k_assemble<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.m, c.th, c.tr, A, c.cf_slot.p, c.W.p, c.prim.p, c.bs.p,
+                                                        c.rdt.p, c.mut.p, c.sc.p, c.steady ? 1 : 0, c.o.beta);
         CKL();
     }
     static void precond_setup(rdst_ctx& c) {
@@ -1077,7 +1101,7 @@ RDST_API rdst_status rdst_create(const rdst_mesh* mesh, int32_t n_options, const
     } catch (const ConfigError& e) {
         return e.unsupported ? RDST_ERR_UNSUPPORTED : RDST_ERR_CONFIG;
     }
-    if (c->o.mu > 0 || c->o.As > 0 || c->o.turbulence != TURB_LAMINAR) return RDST_ERR_UNSUPPORTED;
+    if (c->o.turbulence != TURB_LAMINAR) return RDST_ERR_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RDST_ERR_CUDA;
     rdst_status st = guarded(c.get(), [&] {

@@ -9,8 +9,8 @@
 //   faces      : internal faces in foam order, geometry SoA
 //                (Sf xyz, |Sf|, w, deltaCoeffs, C_N - C_P xyz, Cf xyz)
 //   bfaces     : active (non-empty) boundary faces, compact, SoA geometry,
-//                boundary state bs[NB][12] (rho, rhoU xyz, rhoE, p, T, phi,
-//                valueFractions of p, U, T, pad)
+//                boundary state bs[NB][16] (rho, rhoU xyz, rhoE, p, T, phi,
+//                valueFractions of p, U, T, pad, U_b xyz, pad)
 //   cell->face : CSR of face codes in ascending foam face order
 //                (code < Fi: internal face, else Fi + bface)
 //   matrix     : SELL-32 block matrix (slices of 32 rows, slot 0 = diagonal,
@@ -24,10 +24,10 @@
 
 namespace rdst {
 
-constexpr int QW = 8;     // recon record stride (7 used)
+constexpr int QW = 8;     // recon record stride (7 recon fields + muEff)
 constexpr int GW = 24;    // gradient record stride (21 used)
 constexpr int PW = 8;     // prim record stride
-constexpr int BW = 12;    // boundary state stride (rho, rhoU, rhoE, p, T, phi, f_p, f_U, f_T, -)
+constexpr int BW = 16;    // boundary state stride (rho, rhoU, rhoE, p, T, phi, f_p, f_U, f_T, -, U_b xyz, -)
 constexpr int SELL_C = 32;
 
 struct DevPatch {

@@ -215,3 +215,23 @@ def test_profile_counters():
     n, ms = s.kernel_stats("spmv")
     assert n == 3 * 23 and ms > 0          # 20 directions + initial + final residual + W-form A.W
     assert s.launch_count() > 0 and s.last_step_ms() > 0
+
+
+@pytest.mark.parametrize("flux,suth", [("AUSM+up", False), ("Kurganov", True), ("HLLC", False)])
+def test_viscous_residual_and_assembly(flux, suth):
+    case = cases.naca0012_laminar(flux=flux, sutherland=suth).with_options(**{"ilu.parts": 4})
+    gpu, ora = pair(case, partition=rhodst_b200.partition_cells(case.mesh.C, 4))
+    rho, rhoU, rhoE = perturbed_state(case, amp=0.02)
+    for s in (gpu, ora):
+        s.set_conservative(rho, rhoU, rhoE)
+    Rg, Ro = gpu.residual(), ora.residual()
+    for k in range(5):
+        assert rel(Rg[:, k], Ro[:, k]) < 1e-11, k
+    dg, ug, lg, sg = gpu.assemble()
+    do, uo, lo, so = ora.assemble()
+    assert rel(dg, do) < 1e-11 and rel(ug, uo) < 1e-11 and rel(lg, lo) < 1e-11
+
+
+def test_viscous_steps():
+    case = cases.naca0012_laminar().with_options(**{"ilu.parts": 4})
+    _run_pair(case, 8, partition=rhodst_b200.partition_cells(case.mesh.C, 4), tol=1e-9)

@@ -274,3 +274,46 @@ def test_krylov_vs_dense(solver, precon):
     x_ref = np.linalg.solve(A, s)
     x, rep = o.linear_solve()
     assert np.abs(x.ravel() - x_ref).max() <= 1e-9 * np.abs(x_ref).max(), rep
+
+
+def test_viscous_linear_field_interior():
+    """A linear velocity field on a uniform (unjittered) mesh: the Gauss
+    gradient is exact and the stresses are constant, so the viscous momentum
+    terms (laplacian(muEff, U) + div(tauMC)) vanish in interior cells."""
+    nx, ny = 12, 8
+    X = np.linspace(0, 2.0, nx + 1)
+    Y = np.linspace(0, 1.0, ny + 1)
+    Z = np.array([-0.05, 0.05])
+    pts = np.stack(np.meshgrid(X, Y, Z, indexing="ij"), -1).reshape(-1, 3)
+    idx = np.arange(pts.shape[0]).reshape(nx + 1, ny + 1, 2)
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    cells = meshmod._hex_from_lattice(idx, ii.ravel(), jj.ravel(), np.zeros(nx * ny, dtype=int))
+
+    def classify(c, n):
+        out = np.full(c.shape[0], 0)
+        out[np.abs(n[:, 2]) > 0.5] = 1
+        return out
+
+    m = meshmod.build_polymesh(pts, [("hex", cells)], classify, [("walls", meshmod.PATCH), ("fb", meshmod.EMPTY)])
+    base = channel_case("Kurganov", nx=4, ny=2)
+    opts = dict(base.options)
+    opts["interpolationSchemes"] = {"reconstruct(rho)": "linear", "reconstruct(U)": "linear", "reconstruct(T)": "linear"}
+    N = m.n_cells
+    U = np.zeros((N, 3))
+    U[:, 0] = 0.3 + 0.2 * m.C[:, 1] + 0.1 * m.C[:, 0]
+    U[:, 1] = 0.05 * m.C[:, 0] - 0.1 * m.C[:, 1]
+    bcs = {"walls": {"p": "zeroGradient", "U": "zeroGradient", "T": "zeroGradient"}}
+    R = {}
+    for mu in (0.0, 0.01):
+        o2 = dict(opts)
+        o2["transport"] = {"mu": mu, "Pr": 0.72}
+        o = OracleSolver(m, bcs, o2)
+        o.set_primitive(np.ones(N), U, np.ones(N))
+        R[mu] = o.residual()
+    # cells whose neighbours' gradients are all exact (two layers in from the
+    # zero-gradient boundary)
+    interior = (m.C[:, 0] > 2.0 / nx * 2.5) & (m.C[:, 0] < 2.0 - 2.0 / nx * 2.5) & \
+               (m.C[:, 1] > 1.0 / ny * 2.5) & (m.C[:, 1] < 1.0 - 1.0 / ny * 2.5)
+    assert interior.sum() >= 15
+    dR = R[0.01][interior, 1:4] - R[0.0][interior, 1:4]
+    assert np.abs(dR).max() < 1e-11
