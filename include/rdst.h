@@ -72,6 +72,8 @@ typedef struct rdst_patch {
     int32_t size;
     int32_t type;              /* RDST_PATCH_*                               */
     int32_t bc_p, bc_U, bc_T;  /* RDST_BC_* per primitive field              */
+    int32_t bc_nuTilda;        /* SA: FIXED_VALUE / ZERO_GRADIENT /
+                                  INLET_OUTLET (farField: inletOutlet)      */
     double p_value;            /* fixedValue / inletValue / far-field p_inf  */
     double U_value[3];
     double T_value;

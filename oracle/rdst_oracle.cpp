@@ -61,7 +61,7 @@ inline double fsign(double s) { return s >= 0 ? 1.0 : -1.0; }
 inline double sqr(double x) { return x * x; }
 
 struct Patch {
-    int start, size, type, bc_p, bc_U, bc_T;
+    int start, size, type, bc_p, bc_U, bc_T, bc_nut;
     double p_value, T_value, nut_value;
     v3 U_value;
 };
@@ -1414,6 +1414,205 @@ void initialize_time(Ctx& c) {           // timeDST::initialize (timeDST.C:67-20
     }
 }
 
+// ----------------------------------------------------------------------
+// Spalart-Allmaras, segregated nuTilda equation after the coupled update
+// (turbulence_.correct(), Single.C:101): SAneg (SAneg.C:490-605, negative
+// nuTilda and the modified Stilda of Allmaras et al. 2012) and SARC2
+// (SARC2.C:121-155, 425-488).  Discretisation of the foam-extend fvMatrix
+// (restated, not vendored): ddt with the flow's ddt scheme; upwind
+// convection with the flow's face mass flux phi; Gauss linear corrected
+// diffusion; explicit Cb2 |grad nuTilda|^2; implicit Sp parts of the
+// destruction terms; fvMatrix::relax (diagonal made dominant, divided by
+// alpha); solved by a fixed number of point-Jacobi sweeps.
+// ----------------------------------------------------------------------
+struct SACoeffs {
+    double sigmaNut = 0.66666, kappa = 0.41, Cb1 = 0.1355, Cb2 = 0.622, Cw2 = 0.3, Cw3 = 2.0, Cv1 = 7.1, Cv2 = 5.0;
+    double Cn1 = 16.0, Cn2 = 0.7, Cn3 = 0.9, Ct3 = 1.2, Ct4 = 0.5, Cr1 = 1.0, Cr2 = 2.0, Cr3 = 1.0;
+    double Cw1() const { return Cb1 / (kappa * kappa) + (1.0 + Cb2) / sigmaNut; }
+};
+inline double fpos(double s) { return s >= 0 ? 1.0 : 0.0; }   // foam pos(): pos(0) = 1
+inline double fneg(double s) { return s < 0 ? 1.0 : 0.0; }
+
+// nuTilda boundary values: fixedValue, inletOutlet on phi, else zeroGradient
+void eval_nut_boundary(Ctx& c) {
+    for (int b = 0; b < c.NB; ++b) {
+        if (!c.active[b]) continue;
+        const Patch& P = c.patches[c.bpatch[b]];
+        int ci = c.own[c.Fi + b];
+        switch (P.bc_nut) {
+            case RDST_BC_FIXED_VALUE: c.nut_b[b] = P.nut_value; break;
+            case RDST_BC_INLET_OUTLET: c.nut_b[b] = c.phi_b[b] >= 0 ? c.nut[ci] : P.nut_value; break;
+            default: c.nut_b[b] = c.nut[ci]; break;
+        }
+    }
+}
+
+// nuTilda valueFraction (for the implicit boundary coefficients)
+double nut_vf(const Ctx& c, int b) {
+    const Patch& P = c.patches[c.bpatch[b]];
+    if (P.bc_nut == RDST_BC_FIXED_VALUE) return 1.0;
+    if (P.bc_nut == RDST_BC_INLET_OUTLET) return c.phi_b[b] >= 0 ? 0.0 : 1.0;
+    return 0.0;
+}
+
+void update_mut(Ctx& c, const std::vector<double>& fv1c) {
+    const SACoeffs K;
+    const bool neg_sa = c.o.turbulence == TURB_SANEG;
+    for (int i = 0; i < c.N; ++i) {
+        double m = (neg_sa ? std::fabs(fv1c[i]) : fv1c[i]) * c.nut[i] * c.rho[i];
+        c.mut[i] = neg_sa ? std::max(m, 0.0) : m;
+    }
+    for (int b = 0; b < c.NB; ++b) {
+        if (!c.active[b]) continue;
+        if (c.patches[c.bpatch[b]].type == RDST_PATCH_WALL) { c.mut_b[b] = 0.0; continue; }
+        double chi = c.rho_b[b] * c.nut_b[b] / mu_of_T(c, c.T_b[b]);
+        double chi3 = chi * chi * chi;
+        double fv1 = chi3 / (chi3 + std::pow(K.Cv1, 3));
+        c.mut_b[b] = std::max(fv1 * c.nut_b[b] * c.rho_b[b], 0.0);
+    }
+}
+
+void sa_correct(Ctx& c) {
+    const SACoeffs K;
+    const int N = c.N;
+    const bool neg_sa = c.o.turbulence == TURB_SANEG;
+    typedef std::array<double, 9> t3;
+    std::vector<t3> gU;
+    grad_vector(c, c.U, c.U_b, gU);
+    std::vector<v3> gn;
+    grad_scalar(c, c.nut, c.nut_b, gn);
+    std::vector<double> mu(N), chi(N), fv1(N), D(N), diag(N), b(N, 0.0);
+    for (int i = 0; i < N; ++i) {
+        mu[i] = mu_of_T(c, c.T[i]);
+        chi[i] = c.rho[i] * c.nut[i] / mu[i];
+        double chi3 = chi[i] * chi[i] * chi[i];
+        fv1[i] = chi3 / (chi3 + std::pow(K.Cv1, 3));
+        const t3& g = gU[i];
+        double W2 = 0;                       // |skew(gradU)|^2
+        for (int a = 0; a < 3; ++a)
+            for (int q = 0; q < 3; ++q) { double w = 0.5 * (g[3 * a + q] - g[3 * q + a]); W2 += w * w; }
+        double Omega = std::sqrt(2.0) * std::sqrt(W2);
+        double fv2 = 1.0 / std::pow(1.0 + chi[i] / K.Cv2, 3);
+        double kd2 = sqr(K.kappa * c.y[i]);
+        double Stilda;
+        if (neg_sa) {
+            double Sbar = fv2 * c.nut[i] / kd2;
+            Stilda = Omega + fpos(K.Cn2 * Omega + Sbar) * Sbar +
+                     fneg(K.Cn2 * Omega + Sbar) * (Omega * (sqr(K.Cn2) * Omega + K.Cn3 * Sbar)) /
+                         std::max((K.Cn3 - 2.0 * K.Cn2) * Omega - Sbar, SMALL);
+        } else {
+            double cb = chi[i] / K.Cv2;
+            double fv3 = (1.0 + chi[i] * fv1[i]) * (1.0 / K.Cv2) * (3 * (1.0 + cb) + sqr(cb)) / std::pow(1.0 + cb, 3);
+            Stilda = fv3 * std::sqrt(2.0) * std::sqrt(W2) + fv2 * c.nut[i] / kd2;
+        }
+        double r = std::min(c.nut[i] / (std::max(Stilda, SMALL) * kd2), 10.0);
+        double gg = r + K.Cw2 * (std::pow(r, 6) - r);
+        double fw = gg * std::pow((1.0 + std::pow(K.Cw3, 6)) / (std::pow(gg, 6) + std::pow(K.Cw3, 6)), 1.0 / 6.0);
+        double V = c.V[i], rho = c.rho[i], nt = c.nut[i];
+        double rdt = (c.o.ddt == DDT_EULER) ? 1.0 / c.deltaT : c.rDeltaT[i];
+        // fvm::ddt(rho, nuTilda): diag rdt rho V, source rdt rho nuTilda_old V
+        diag[i] = rdt * rho * V;
+        b[i] = rdt * rho * nt * V;
+        // + Cb2/sigma rho |grad nuTilda|^2 (explicit, moved to the right)
+        b[i] += K.Cb2 / K.sigmaNut * rho * magSqr(gn[i]) * V;
+        if (neg_sa) {
+            double ft2 = K.Ct3 * std::exp(-K.Ct4 * sqr(chi[i]));
+            double pp = fpos(nt), nn = fneg(nt);
+            b[i] += pp * K.Cb1 * (1.0 - ft2) * rho * Stilda * nt * V;
+            diag[i] += pp * (K.Cw1() * fw - K.Cb1 / sqr(K.kappa) * ft2) * nt * rho / sqr(c.y[i]) * V;
+            b[i] += nn * K.Cb1 * (1.0 - K.Ct3) * rho * Omega * nt * V;
+            diag[i] -= nn * K.Cw1() * nt * rho / sqr(c.y[i]) * V;
+            double chi3 = chi[i] * chi[i] * chi[i];
+            double fn = fpos(chi[i]) + fneg(chi[i]) * (K.Cn1 + chi3) / (K.Cn1 - chi3);
+            D[i] = (rho * nt * fn + mu[i]) / K.sigmaNut;
+        } else {
+            // SARC2 fr1 (SARC2.C:121-155): rotation/curvature multiplier
+            double S2 = 0, W2b = 0;
+            for (int a = 0; a < 3; ++a)
+                for (int q = 0; q < 3; ++q) {
+                    double sy = 0.5 * (g[3 * a + q] + g[3 * q + a]), sk = 0.5 * (g[3 * a + q] - g[3 * q + a]);
+                    S2 += sy * sy; W2b += sk * sk;
+                }
+            double sqrS = 2.0 * S2, sqrW = 2.0 * W2b;
+            double rStar = std::sqrt(sqrS / std::max(sqrW, SMALL));
+            double rrStar = std::sqrt(sqrW / std::max(sqrS, SMALL));
+            double rTilda = rrStar * (rrStar - 1.0);
+            double fr1 = (1 + K.Cr1) * 2.0 * rStar / (1.0 + rStar) * (1.0 - K.Cr3 * std::atan(K.Cr2 * rTilda)) - K.Cr1;
+            b[i] += K.Cb1 * rho * Stilda * nt * fr1 * V;
+            diag[i] += K.Cw1() * fw * nt * rho / sqr(c.y[i]) * V;
+            D[i] = rho * nt / K.sigmaNut + mu[i];
+        }
+    }
+    // face coefficients: upwind convection with phi, corrected diffusion
+    std::vector<double> up(c.Fi), lo(c.Fi);
+    for (int f = 0; f < c.Fi; ++f) {
+        int P = c.own[f], Q = c.nei[f];
+        double w = c.w[f], ph = c.phi[f];
+        double wu = fpos(ph);
+        double Df = w * D[P] + (1 - w) * D[Q];
+        double dcoef = Df * c.magSf[f] * c.dc[f];
+        // convection: row P: diag += wu phi, upper += (1-wu) phi;
+        //             row Q: diag -= (1-wu) phi, lower += -wu phi
+        diag[P] += wu * ph;
+        diag[Q] -= (1 - wu) * ph;
+        up[f] = (1 - wu) * ph - dcoef;
+        lo[f] = -wu * ph - dcoef;
+        diag[P] += dcoef;
+        diag[Q] += dcoef;
+        // explicit non-orthogonal correction Df |Sf| k . (grad nuTilda)_f
+        v3 n = c.Sf[f] / c.magSf[f];
+        v3 kc = n - c.dc[f] * (c.C[Q] - c.C[P]);
+        double corr = Df * c.magSf[f] * dot(kc, c.w[f] * gn[P] + (1 - c.w[f]) * gn[Q]);
+        b[P] += corr;
+        b[Q] -= corr;
+    }
+    for (int bb = 0; bb < c.NB; ++bb) {
+        if (!c.active[bb]) continue;
+        int f = c.Fi + bb, P = c.own[f];
+        const Patch& Pt = c.patches[c.bpatch[bb]];
+        double fvf = nut_vf(c, bb);
+        double ref = Pt.nut_value;
+        double ph = c.phi_b[bb];
+        // convection through the boundary value f ref + (1-f) nu_P
+        diag[P] += ph * (1 - fvf);
+        b[P] -= ph * fvf * ref;
+        // diffusion: snGrad = f (ref - nu_P) dc
+        // DnuTildaEff evaluated on the boundary values
+        double mub = mu_of_T(c, c.T_b[bb]);
+        double Db;
+        if (neg_sa) {
+            double chib = c.rho_b[bb] * c.nut_b[bb] / mub, chib3 = chib * chib * chib;
+            double fnb = fpos(chib) + fneg(chib) * (K.Cn1 + chib3) / (K.Cn1 - chib3);
+            Db = (c.rho_b[bb] * c.nut_b[bb] * fnb + mub) / K.sigmaNut;
+        } else {
+            Db = c.rho_b[bb] * c.nut_b[bb] / K.sigmaNut + mub;
+        }
+        double dcoef = Db * c.magSf[f] * c.dc[f] * fvf;
+        diag[P] += dcoef;
+        b[P] += dcoef * ref;
+    }
+    // fvMatrix::relax: D0 -> max(D0, sum|offdiag|)/alpha, source += (D - D0) psi
+    std::vector<double> sumOff(N, 0.0);
+    for (int f = 0; f < c.Fi; ++f) { sumOff[c.own[f]] += std::fabs(up[f]); sumOff[c.nei[f]] += std::fabs(lo[f]); }
+    for (int i = 0; i < N; ++i) {
+        double D0 = diag[i];
+        double Dn = std::max(D0, sumOff[i]) / c.o.nut_relax;
+        b[i] += (Dn - D0) * c.nut[i];
+        diag[i] = Dn;
+    }
+    // point-Jacobi sweeps from the current nuTilda
+    std::vector<double> x(c.nut), xn(N);
+    for (int it = 0; it < c.o.nut_sweeps; ++it) {
+        for (int i = 0; i < N; ++i) xn[i] = b[i];
+        for (int f = 0; f < c.Fi; ++f) { xn[c.own[f]] -= up[f] * x[c.nei[f]]; xn[c.nei[f]] -= lo[f] * x[c.own[f]]; }
+        for (int i = 0; i < N; ++i) x[i] = xn[i] / diag[i];
+    }
+    c.nut = x;
+    if (!neg_sa) for (auto& v : c.nut) v = std::max(v, 0.0);
+    eval_nut_boundary(c);
+    update_mut(c, fv1);
+}
+
 double seconds_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -1443,6 +1642,7 @@ void single_iterate(Ctx& c, Report& rep) {
     t0 = std::chrono::steady_clock::now();
     update_fields(c, dx);
     rep.flags = c.bounded ? 1 : 0;
+    if (c.o.turbulence != TURB_LAMINAR) sa_correct(c);      // turbulence_.correct()
     set_courant(c, rep);
     rep.t[4] = seconds_since(t0) * 1e3;
 }
@@ -1469,7 +1669,7 @@ ORACLE_API rdst_status rdsto_create(const rdst_mesh* m, int32_t n_opts, const ch
     } catch (const ConfigError& e) {
         return e.unsupported ? RDST_ERR_UNSUPPORTED : RDST_ERR_CONFIG;
     }
-    if (c.o.turbulence != TURB_LAMINAR) return RDST_ERR_UNSUPPORTED;
+    if (c.o.turbulence != TURB_LAMINAR && !m->wall_distance) return RDST_ERR_MESH;
     c.N = m->n_cells; c.Fi = m->n_internal_faces; c.F = m->n_faces; c.NB = c.F - c.Fi;
     if (c.N <= 0 || c.Fi < 0 || c.F < c.Fi) return RDST_ERR_MESH;
     c.own.assign(m->owner, m->owner + c.F);
@@ -1482,12 +1682,13 @@ ORACLE_API rdst_status rdsto_create(const rdst_mesh* m, int32_t n_opts, const ch
     c.w.assign(m->weights, m->weights + c.F);
     c.dc.assign(m->deltaCoeffs, m->deltaCoeffs + c.F);
     c.V.assign(m->V, m->V + c.N);
+    if (m->wall_distance) c.y.assign(m->wall_distance, m->wall_distance + c.N);
     c.bpatch.assign(c.NB, -1);
     c.active.assign(c.NB, 0);
     for (int p = 0; p < m->n_patches; ++p) {
         const rdst_patch& P = m->patches[p];
-        Patch q{P.start, P.size, P.type, P.bc_p, P.bc_U, P.bc_T, P.p_value, P.T_value, P.nuTilda_value,
-                {P.U_value[0], P.U_value[1], P.U_value[2]}};
+        Patch q{P.start, P.size, P.type, P.bc_p, P.bc_U, P.bc_T, P.bc_nuTilda, P.p_value, P.T_value,
+                P.nuTilda_value, {P.U_value[0], P.U_value[1], P.U_value[2]}};
         c.patches.push_back(q);
         for (int f = P.start; f < P.start + P.size; ++f) {
             if (f < c.Fi || f >= c.F) return RDST_ERR_MESH;
@@ -1550,12 +1751,21 @@ ORACLE_API rdst_status rdsto_set_primitive(rdst_ctx* ctx, const double* p, const
                                            const double* nut) {
     if (!ctx || !p || !U || !T) return RDST_ERR_ARG;
     Ctx& c = ctx->c;
-    (void)nut;
     for (int i = 0; i < c.N; ++i) {
         c.p[i] = p[i]; c.T[i] = T[i];
         c.U[i] = {U[3 * i], U[3 * i + 1], U[3 * i + 2]};
+        c.nut[i] = nut ? nut[i] : 0.0;
     }
     init_from_primitive(c);
+    if (c.o.turbulence != TURB_LAMINAR) {
+        eval_nut_boundary(c);
+        std::vector<double> fv1(c.N);
+        for (int i = 0; i < c.N; ++i) {
+            double chi = c.rho[i] * c.nut[i] / mu_of_T(c, c.T[i]);
+            fv1[i] = chi * chi * chi / (chi * chi * chi + std::pow(7.1, 3));
+        }
+        update_mut(c, fv1);
+    }
     return RDST_OK;
 }
 
@@ -1596,7 +1806,7 @@ ORACLE_API rdst_status rdsto_get_primitive(rdst_ctx* ctx, double* p, double* U, 
         if (p) p[i] = c.p[i];
         if (T) T[i] = c.T[i];
         if (U) for (int k = 0; k < 3; ++k) U[3 * i + k] = c.U[i][k];
-        if (nut) nut[i] = 0.0;
+        if (nut) nut[i] = c.nut[i];
     }
     return RDST_OK;
 }

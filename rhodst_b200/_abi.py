@@ -37,7 +37,7 @@ class RdstError(RuntimeError):
 
 class RdstPatch(ctypes.Structure):
     _fields_ = [("start", c_int32), ("size", c_int32), ("type", c_int32),
-                ("bc_p", c_int32), ("bc_U", c_int32), ("bc_T", c_int32),
+                ("bc_p", c_int32), ("bc_U", c_int32), ("bc_T", c_int32), ("bc_nuTilda", c_int32),
                 ("p_value", c_double), ("U_value", c_double * 3), ("T_value", c_double),
                 ("nuTilda_value", c_double)]
 
@@ -164,8 +164,15 @@ class Solver:
             for k in range(3):
                 P.U_value[k] = float(uv[k])
             P.T_value = float(tv) if tv is not None else 0.0
-            nv = spec.get("nuTilda")
-            P.nuTilda_value = float(nv[1]) if isinstance(nv, tuple) else 0.0
+            nv = spec.get("nuTilda", "zeroGradient")
+            if isinstance(nv, tuple):
+                P.bc_nuTilda = _BC_NAMES[nv[0]]
+                P.nuTilda_value = float(nv[1])
+            else:
+                P.bc_nuTilda = _BC_NAMES[nv]
+                P.nuTilda_value = 0.0
+            if P.bc_nuTilda == BC_FARFIELD:
+                P.bc_nuTilda = BC_INLET_OUTLET
         self._arrays = dict(
             owner=np.ascontiguousarray(m.owner, dtype=np.int32),
             neighbour=np.ascontiguousarray(m.neighbour, dtype=np.int32),

@@ -101,12 +101,12 @@ def farfield_state(mach: float, alpha_deg: float, T_inf: float, p_inf: float, ga
 
 def naca0012_inviscid(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: float = 2.3,
                       flux: str = "AUSM+up", limiter: str = "Venkatakrishnan",
-                      n_directions: int = 30, preconditioner: str = "ILUC0") -> Case:
+                      n_directions: int = 30, preconditioner: str = "ILUC0", first_cell: float = 4e-6) -> Case:
     """NACA0012 C-mesh with characteristic far field, Euler equations,
     local time stepping at CFL 50 (steadyStateDST), block-GMRES(30) with
     block ILU(0).  The inviscid counterpart of the turbulent airfoil case
     (same mesh, flow angle and Mach number)."""
-    m = _mesh.naca_cmesh(ni, nj)
+    m = _mesh.naca_cmesh(ni, nj, first_cell=first_cell)
     gas = dict(NORMALISED_GAS)
     U0 = farfield_state(mach, alpha, 1.0, 1.0, gas)
     bcs = {
@@ -175,11 +175,14 @@ def swept_wing_c3(n_around: int = 192, n_normal: int = 64, n_span: int = 64, n_t
 
 
 def naca0012_laminar(ni: int = 129, nj: int = 33, mach: float = 0.5, alpha: float = 1.0, reynolds: float = 5000.0,
-                     flux: str = "AUSM+up", limiter: str = "vanLeer", sutherland: bool = False) -> Case:
+                     flux: str = "AUSM+up", limiter: str = "vanLeer", sutherland: bool = False,
+                     first_cell: float = 2e-3) -> Case:
     """Laminar NACA0012 (no-slip adiabatic wall) with the viscous terms of
     calcFields; constant viscosity from the chord Reynolds number, or
-    Sutherland's law scaled to the same free-stream viscosity."""
-    c = naca0012_inviscid(ni, nj, mach=mach, alpha=alpha, flux=flux, limiter=limiter, n_directions=20)
+    Sutherland's law scaled to the same free-stream viscosity.  Wall spacing
+    `first_cell` resolves the Re 5000 boundary layer with ~10 cells."""
+    c = naca0012_inviscid(ni, nj, mach=mach, alpha=alpha, flux=flux, limiter=limiter, n_directions=20,
+                          first_cell=first_cell)
     gas = c.options["thermo"]
     rho_inf = 1.0 / gas["R"]
     U_inf = mach * math.sqrt(gas["Cp"] / (gas["Cp"] - gas["R"]) * gas["R"])
@@ -193,3 +196,51 @@ def naca0012_laminar(ni: int = 129, nj: int = 33, mach: float = 0.5, alpha: floa
         c.options["transport"] = {"mu": mu_inf, "Pr": 0.72}
     c.name = "naca0012_laminar"
     return c
+
+
+def naca0012_turbulent(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: float = 2.3,
+                       reynolds: float = 6.5e6, model: str = "SAneg", flux: str = "AUSM+up",
+                       limiter: str = "Venkatakrishnan", n_directions: int = 30, first_cell: float = 4e-6) -> Case:
+    """Steady turbulent NACA0012: C-mesh ni x nj (far field 20 c, wall
+    spacing for y+ ~ 1 growing at 1.15), M 0.73, alpha 2.3 deg, chord
+    Reynolds 6.5e6 with Sutherland air scaled to the normalised gas,
+    Spalart-Allmaras (SAneg default), AUSM+up + Venkatakrishnan, local time
+    stepping ramped to CFL 50, block-GMRES(30) + block ILU(0)."""
+    from . import mesh as _m
+    m = _m.naca_cmesh(ni, nj, first_cell=first_cell)
+    m.wall_distance = _m.wall_distance(m, ["airfoil"])
+    gas = dict(NORMALISED_GAS)
+    U0 = farfield_state(mach, alpha, 1.0, 1.0, gas)
+    rho_inf = 1.0 / gas["R"]
+    mu_inf = rho_inf * math.hypot(U0[0], U0[1]) / reynolds
+    nut_inf = 3.0 * mu_inf / rho_inf                    # nuTilda_inf = 3 nu_inf
+    Ts = 110.4 / 255.556                                # Sutherland T_s / T_inf (air at 255.556 K)
+    bcs = {
+        "airfoil": {"p": "zeroGradient", "U": ("fixedValue", (0.0, 0.0, 0.0)), "T": "zeroGradient",
+                    "nuTilda": ("fixedValue", 0.0)},
+        "farfield": {"p": ("farField", 1.0), "U": ("farField", U0), "T": ("farField", 1.0),
+                     "nuTilda": ("inletOutlet", nut_inf)},
+    }
+    vlim = "Venkatakrishnan" if limiter == "Venkatakrishnan" else limiter + "V"
+    options = {
+        "fluxScheme": flux,
+        "Jacobian": "Roe",
+        "timeControls": {"neighbouring": False, "initialCo": 2.0, "minCo": 0.1, "maxCo": 50.0},
+        "ddtSchemes": {"default": "steadyStateDST"},
+        "interpolationSchemes": {"reconstruct(rho)": limiter, "reconstruct(U)": vlim,
+                                 "reconstruct(T)": limiter},
+        "solvers": {"W": {"solver": "GMRES", "preconditioner": "ILUC0",
+                          "nDirections": n_directions, "tolerance": 1e-12, "relTol": 0.0,
+                          "maxIter": 1, "minIter": 1},
+                    "nuTilda": {"nSweeps": 10}},
+        "relaxationFactors": {"nuTilda": 0.5},
+        "fieldBounds": {"rho": (1e-3, 1e4), "p": (1e-3, 1e4), "T": (1e-3, 1e4)},
+        "thermo": gas,
+        "transport": {"As": mu_inf * (1.0 + Ts), "Ts": Ts, "Pr": 0.72},
+        "RASModel": model,
+    }
+    N = m.n_cells
+    al = math.radians(alpha)
+    return Case("naca0012_SA", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N),
+                nuTilda=np.full(N, nut_inf), steps=4000, force_patch="airfoil",
+                force_dirs={"lift": (-math.sin(al), math.cos(al), 0.0), "drag": (math.cos(al), math.sin(al), 0.0)})

@@ -7,6 +7,7 @@
 #include "rdst_options.h"
 #include "rdst_internal.h"
 #include "linalg.cuh"
+#include "turbulence.cuh"
 
 #include <algorithm>
 #include <array>
@@ -149,6 +150,10 @@ struct rdst_ctx {
     // viscous: grad U, face Up, viscous face terms, turbulent viscosity
     DBuf<double> gU, up, bup, vf, bvf, mut, mut_b;
     Transport tr{};
+    // Spalart-Allmaras
+    DBuf<double> nut, nut_b, ywall, saD, safv1, sadiag, sab, sax2, sagn, safup, saflo, safdP, safdQ, safcorr, sabd, sabb;
+    SAFields sa{};
+    bool turb = false;
     DBuf<Scalars> sc;
     DBuf<rdst_step_report> reps;
     // matrix
@@ -303,7 +308,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         if (P.start < Fi || P.start + P.size > F || P.size < 0) throw std::invalid_argument("patch range outside the boundary faces");
         for (int f = P.start; f < P.start + P.size; ++f) fpatch[f - Fi] = p;
         DevPatch& d = dp[p];
-        d.type = P.type; d.bc_p = P.bc_p; d.bc_U = P.bc_U; d.bc_T = P.bc_T;
+        d.type = P.type; d.bc_p = P.bc_p; d.bc_U = P.bc_U; d.bc_T = P.bc_T; d.bc_nut = P.bc_nuTilda;
         d.p_value = P.p_value; d.T_value = P.T_value; d.nut_value = P.nuTilda_value;
         for (int k = 0; k < 3; ++k) d.U_value[k] = P.U_value[k];
         c.hpatch_start.push_back(P.start);
@@ -565,6 +570,23 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     c.psi.alloc((size_t)QW * N); c.fcell.alloc(N); c.fl.alloc(5L * std::max(Fi, 1)); c.bfl.alloc(5L * std::max(NB, 1));
     c.R.alloc(5L * N); c.rhs.alloc(5L * N);
     c.mut.alloc(N); c.mut.zero(s); c.mut_b.alloc(std::max(NB, 1)); c.mut_b.zero(s);
+    c.turb = (o.turbulence != TURB_LAMINAR);
+    if (c.turb) {
+        if (!mh->wall_distance) throw std::invalid_argument("Spalart-Allmaras needs the wall distance field");
+        std::vector<double> yv(N);
+        for (int r = 0; r < N; ++r) yv[r] = mh->wall_distance[c.perm[r]];
+        c.ywall.upload(yv, s);
+        const size_t nb1 = std::max(NB, 1), fi1 = std::max(Fi, 1);
+        c.nut.alloc(N); c.nut.zero(s); c.nut_b.alloc(nb1); c.nut_b.zero(s);
+        c.saD.alloc(N); c.safv1.alloc(N); c.sadiag.alloc(N); c.sab.alloc(N); c.sax2.alloc(N); c.sagn.alloc(3L * N);
+        c.safup.alloc(fi1); c.saflo.alloc(fi1); c.safdP.alloc(fi1); c.safdQ.alloc(fi1); c.safcorr.alloc(fi1);
+        c.sabd.alloc(nb1); c.sabb.alloc(nb1);
+        SAFields& F = c.sa;
+        F.nut = c.nut.p; F.nut_b = c.nut_b.p; F.mut = c.mut.p; F.mut_b = c.mut_b.p; F.y = c.ywall.p;
+        F.D = c.saD.p; F.fv1 = c.safv1.p; F.diag = c.sadiag.p; F.b = c.sab.p; F.x2 = c.sax2.p; F.gn = c.sagn.p;
+        F.fup = c.safup.p; F.flo = c.saflo.p; F.fdP = c.safdP.p; F.fdQ = c.safdQ.p; F.fcorr = c.safcorr.p;
+        F.bd = c.sabd.p; F.bb = c.sabb.p;
+    }
     if (c.tr.viscous) {
         c.gU.alloc(9L * N); c.up.alloc(3L * std::max(Fi, 1)); c.bup.alloc(3L * std::max(NB, 1));
         c.vf.alloc(8L * std::max(Fi, 1)); c.bvf.alloc(8L * std::max(NB, 1));
@@ -843,7 +865,33 @@ void set_transient_dt(rdst_ctx& c) {
     CKL();
 }
 
-// updateFields.H + turbulence (laminar: none) + setCourantDST
+// Spalart-Allmaras transport (SAneg / SARC2), segregated
+void sa_correct(rdst_ctx& c) {
+    cudaStream_t s = c.s;
+    const DevMesh& m = c.m;
+    const int neg_sa = c.o.turbulence == TURB_SANEG;
+    SAFields F = c.sa;
+    k_sa_grad<<<nblk(c.N, 128), 128, 0, s>>>(m, c.prim.p, c.bs.p, F, c.gU.p); CKL();
+    k_sa_cell<<<nblk(c.N, 128), 128, 0, s>>>(m, c.tr, neg_sa, c.steady ? 1 : 0, c.W.p, c.prim.p, c.gU.p, c.rdt.p,
+                                            c.sc.p, F); CKL();
+    if (m.Fi > 0) { k_sa_faces<<<nblk(m.Fi, TPB), TPB, 0, s>>>(m, c.fl.p, F); CKL(); }
+    if (m.NB > 0) { k_sa_bfaces<<<nblk(m.NB, TPB), TPB, 0, s>>>(m, c.tr, neg_sa, c.bs.p, F); CKL(); }
+    k_sa_assemble<<<nblk(c.N, TPB), TPB, 0, s>>>(m, c.o.nut_relax, F); CKL();
+    // Jacobi sweeps from the current nuTilda, ping-pong nut <-> x2
+    double* xin = c.nut.p;
+    double* xout = c.sax2.p;
+    for (int it = 0; it < c.o.nut_sweeps; ++it) {
+        k_sa_jacobi<<<nblk(c.N, TPB), TPB, 0, s>>>(m, F, xin, xout); CKL();
+        std::swap(xin, xout);
+    }
+    k_sa_finish<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, neg_sa, c.W.p, xin, F); CKL();
+    if (m.NB > 0) {
+        k_sa_bc<<<nblk(m.NB, TPB), TPB, 0, s>>>(m, c.bs.p, F); CKL();
+        k_sa_mutb<<<nblk(m.NB, TPB), TPB, 0, s>>>(m, c.tr, c.bs.p, F); CKL();
+    }
+}
+
+// updateFields.H + turbulence + setCourantDST
 void post_update(rdst_ctx& c) {
     cudaStream_t s = c.s;
     {
@@ -851,6 +899,7 @@ void post_update(rdst_ctx& c) {
         k_update<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, c.dx.p, c.W.p, c.prim.p, c.sc.p); CKL();
     }
     k_boundary<<<nblk(c.NB, TPB), TPB, 0, s>>>(c.m, c.th, c.bd, c.W.p, c.prim.p, c.bs.p); CKL();
+    if (c.turb) sa_correct(c);          // turbulence_.correct()
     k_courant_scalar<<<1, 1, 0, s>>>(c.sc.p, (!c.steady && c.o.adjust_time_step) ? 1 : 0, c.o.min_co, c.o.max_co); CKL();
     if (c.steady) {
         k_courant_cells<<<nblk(c.N, TPB), TPB, 0, s>>>(c.m, c.W.p, c.rhoOld.p, c.eOld.p, c.courantF.p, c.sc.p,
@@ -1101,7 +1150,7 @@ RDST_API rdst_status rdst_create(const rdst_mesh* mesh, int32_t n_options, const
     } catch (const ConfigError& e) {
         return e.unsupported ? RDST_ERR_UNSUPPORTED : RDST_ERR_CONFIG;
     }
-    if (c->o.turbulence != TURB_LAMINAR) return RDST_ERR_UNSUPPORTED;
+    if (c->o.turbulence != TURB_LAMINAR && !mesh->wall_distance) return RDST_ERR_MESH;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RDST_ERR_CUDA;
     rdst_status st = guarded(c.get(), [&] {
@@ -1120,7 +1169,7 @@ RDST_API rdst_status rdst_create(const rdst_mesh* mesh, int32_t n_options, const
 RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const double* U, const double* T,
                                         const double* nut) {
     if (!c || !p || !U || !T) return RDST_ERR_ARG;
-    (void)nut;
+    if (c->turb && !nut) { c->err = "Spalart-Allmaras needs an initial nuTilda"; return RDST_ERR_ARG; }
     return guarded(c, [&] {
         std::vector<double> prim((size_t)PW * c->N, 0.0);
         for (int r = 0; r < c->N; ++r) {
@@ -1134,6 +1183,18 @@ RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const doub
         CKL();
         CK(cudaStreamSynchronize(c->s));
         after_state_set(*c);
+        if (c->turb) {
+            std::vector<double> nv(c->N);
+            for (int r = 0; r < c->N; ++r) nv[r] = nut[c->perm[r]];
+            CK(cudaMemcpyAsync(c->nut.p, nv.data(), nv.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
+            const DevMesh& m = c->m;
+            if (m.NB > 0) { k_sa_bc<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->bs.p, c->sa); CKL(); }
+            k_sa_init_mut<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->tr, c->W.p, c->prim.p, c->sa); CKL();
+            k_sa_finish<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->o.turbulence == TURB_SANEG, c->W.p, c->nut.p, c->sa);
+            CKL();
+            if (m.NB > 0) { k_sa_mutb<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->tr, c->bs.p, c->sa); CKL(); }
+            CK(cudaStreamSynchronize(c->s));
+        }
     });
 }
 
@@ -1186,8 +1247,9 @@ RDST_API rdst_status rdst_get_conservative(rdst_ctx* c, double* rho, double* rho
 RDST_API rdst_status rdst_get_primitive(rdst_ctx* c, double* p, double* U, double* T, double* nut) {
     if (!c) return RDST_ERR_ARG;
     return guarded(c, [&] {
-        std::vector<double> P((size_t)PW * c->N);
+        std::vector<double> P((size_t)PW * c->N), nv(c->turb ? c->N : 0);
         CK(cudaMemcpyAsync(P.data(), c->prim.p, P.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        if (c->turb) CK(cudaMemcpyAsync(nv.data(), c->nut.p, nv.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
         CK(cudaStreamSynchronize(c->s));
         for (int r = 0; r < c->N; ++r) {
             int i = c->perm[r];
@@ -1195,7 +1257,7 @@ RDST_API rdst_status rdst_get_primitive(rdst_ctx* c, double* p, double* U, doubl
             if (p) p[i] = q[0];
             if (T) T[i] = q[1];
             if (U) for (int k = 0; k < 3; ++k) U[3 * i + k] = q[3 + k];
-            if (nut) nut[i] = 0.0;
+            if (nut) nut[i] = c->turb ? nv[r] : 0.0;
         }
     });
 }

@@ -31,7 +31,7 @@ constexpr int BW = 16;    // boundary state stride (rho, rhoU, rhoE, p, T, phi, 
 constexpr int SELL_C = 32;
 
 struct DevPatch {
-    int type, bc_p, bc_U, bc_T;
+    int type, bc_p, bc_U, bc_T, bc_nut;
     double p_value, T_value, nut_value;
     double U_value[3];
 };

@@ -65,8 +65,10 @@ struct Options {
     double R = 8314.47 / 28.9, Cp = 1004.5;
     double mu = 0.0, Pr = 1.0;        // constTransport
     double As = 0.0, Ts = 0.0;        // sutherlandTransport (As > 0 selects it)
-    double Prt = 0.85;                // turbulent Prandtl number
+    double Prt = 1.0;                 // turbulent Prandtl number (SAneg coeffDict default)
     Turbulence turbulence = TURB_LAMINAR;
+    double nut_relax = 1.0;           // relaxationFactors.nuTilda
+    int nut_sweeps = 10;              // point-Jacobi sweeps of the nuTilda system
     // time
     double delta_t = 1.0;             // controlDict deltaT (used when adjustTimeStep false)
     double start_time = 0.0;
@@ -234,10 +236,13 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
         else if (k == "RASModel" || k == "turbulence") {
             if (t == "laminar") o.turbulence = TURB_LAMINAR;
             else if (t == "SAneg") o.turbulence = TURB_SANEG;
-            else if (t == "SARC1") o.turbulence = TURB_SARC1;
+            else if (t == "SARC1")
+                throw ConfigError("RASModel SARC1 (Spalart-Shur rotation/curvature) is not on this path yet", true);
             else if (t == "SARC2") o.turbulence = TURB_SARC2;
             else throw ConfigError("Unknown RASModel " + t + "\nValid models are: (laminar SAneg SARC1 SARC2)");
         }
+        else if (k == "relaxationFactors.nuTilda") o.nut_relax = parse_double(k, v);
+        else if (k == "solvers.nuTilda.nSweeps") o.nut_sweeps = parse_int(k, v);
         else if (k == "controlDict.deltaT") o.delta_t = parse_double(k, v);
         else if (k == "controlDict.startTime") o.start_time = parse_double(k, v);
         else if (k == "precision") {

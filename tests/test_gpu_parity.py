@@ -235,3 +235,38 @@ def test_viscous_residual_and_assembly(flux, suth):
 def test_viscous_steps():
     case = cases.naca0012_laminar().with_options(**{"ilu.parts": 4})
     _run_pair(case, 8, partition=rhodst_b200.partition_cells(case.mesh.C, 4), tol=1e-9)
+
+
+def small_turbulent(model="SAneg"):
+    c = cases.naca0012_turbulent(ni=129, nj=49, model=model)
+    return c.with_options(**{"ilu.parts": 4})
+
+
+@pytest.mark.parametrize("model", ["SAneg", "SARC2"])
+def test_sa_steps(model):
+    case = small_turbulent(model)
+    part = rhodst_b200.partition_cells(case.mesh.C, 4)
+    gpu, ora = pair(case, partition=part)
+    for s in (gpu, ora):
+        s.set_primitive(case.p, case.U, case.T, case.nuTilda)
+    rg, ro = gpu.step(6), ora.step(6)
+    for a, b in zip(rg, ro):
+        assert abs(a["res_mag"] - b["res_mag"]) <= 1e-9 * abs(b["res_mag"])
+    pg, Ug, Tg, ng = gpu.primitive()
+    po, Uo, To, no = ora.primitive()
+    assert rel(pg, po) < 1e-9 and rel(Ug, Uo) < 1e-9 and rel(Tg, To) < 1e-9
+    assert rel(ng, no) < 1e-9
+
+
+def test_sa_residual_with_mut():
+    case = small_turbulent("SAneg")
+    part = rhodst_b200.partition_cells(case.mesh.C, 4)
+    gpu, ora = pair(case, partition=part)
+    for s in (gpu, ora):
+        s.set_primitive(case.p, case.U, case.T, case.nuTilda * 50.0)
+    Rg, Ro = gpu.residual(), ora.residual()
+    for k in range(5):
+        assert rel(Rg[:, k], Ro[:, k]) < 1e-11
+    dg, ug, lg, sg = gpu.assemble()
+    do, uo, lo, so = ora.assemble()
+    assert rel(dg, do) < 1e-11 and rel(ug, uo) < 1e-11
