@@ -54,6 +54,16 @@ def workload(name: str):
                 "solver": "GMRES(20), 1 restart cycle", "preconditioner": "subdomain block ILU(0)",
                 "precision": f"Jacobian/ILU {prec}, residual/vectors fp64", "mach": 0.84, "alpha_deg": 3.06}
         return c, desc
+    if name.startswith("naca0012_sa"):
+        prec = name.split("_")[-1] if name.count("_") >= 2 else "fp64"
+        c = cases.naca0012_turbulent().with_options(precision=prec)
+        desc = {"workload": name, "mesh": "NACA0012 C-mesh 257x65, wall y+~1, far field 20 c",
+                "cells": c.mesh.n_cells, "internal_faces": c.mesh.n_internal_faces,
+                "flux": "AUSM+up", "reconstruction": "Venkatakrishnan", "turbulence": "SAneg",
+                "ddt": "steadyStateDST local dt, CFL ramp 2->50", "solver": "GMRES(30), 1 restart cycle",
+                "preconditioner": "subdomain block ILU(0)", "mach": 0.73, "alpha_deg": 2.3, "reynolds": 6.5e6,
+                "precision": f"Jacobian/ILU {prec}, residual/vectors fp64"}
+        return c, desc
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -250,6 +260,49 @@ def cpu_baseline(case, budget_s: float, steps_max: int, warmup: int = 1):
             "sample": f"{n} steps of the same workload after {warmup} warm-up step(s), {dt:.2f} s"}
 
 
+def run_converge(args):
+    """Steps until the density residual ||R_rho V||_2 drops by args.converge
+    relative to the first step; reports device time, steps and forces."""
+    import torch
+    import rhodst_b200
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    case, desc = workload(args.workload)
+    s = rhodst_b200.solver_for(case)
+    N = case.mesh.n_cells
+    chunk = 50
+    r0 = None
+    steps, dev_ms, hist = 0, 0.0, []
+    t0 = time.perf_counter()
+    while steps < args.max_steps:
+        reps = s.step(chunk)
+        dev_ms += s.last_step_ms()
+        for r in reps:
+            steps += 1
+            if r0 is None:
+                r0 = r["res_l2"][0]
+            hist.append(r["res_l2"][0] / r0)
+        if hist[-1] <= args.converge:
+            break
+    wall = time.perf_counter() - t0
+    hit = next((i + 1 for i, h in enumerate(hist) if h <= args.converge), None)
+    out = {"metric": "time_to_residual_drop", "workload": args.workload, "drop": args.converge,
+           "reached": hit is not None, "steps_to_drop": hit, "steps_run": steps,
+           "device_s": dev_ms * 1e-3, "wall_s": wall, "cells": N,
+           "cell_iterations_per_s": N * steps / (dev_ms * 1e-3),
+           "final_drop": hist[-1], "history_every_50": hist[::50], "config": desc}
+    if case.force_patch:
+        al = case.force_dirs
+        g = case.options["thermo"]
+        U = np.asarray(case.U[0])
+        q = 0.5 * (1.0 / g["R"]) * float(U @ U)
+        area = float(case.mesh.magSf[case.mesh.patch(case.force_patch).start:
+                                     case.mesh.patch(case.force_patch).start + case.mesh.patch(case.force_patch).size].sum())
+        # 2D: chord x span (1 x 0.1); wing: planform semi-span x mean chord
+        ref_area = 0.1 if case.name.startswith("naca") else 1.5 * 0.5 * (1.0 + 0.56)
+        out["forces"] = s.forces(case.force_patch, al["lift"], al["drag"], 1.0, q * ref_area)
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -258,7 +311,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="forward_step_2d")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--converge", type=float, default=0.0,
+                    help="run to this density-residual drop instead of timing fixed steps")
+    ap.add_argument("--max-steps", type=int, default=5000)
     args = ap.parse_args()
+    if args.converge > 0:
+        run_converge(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
