@@ -179,7 +179,9 @@ rdst_status rdst_forces(rdst_ctx* ctx, int32_t patch, const double lift_dir[3],
                         const double pitch_axis[3], double p_ref,
                         double q_ref_times_area, double l_ref, double out[3]);
 
-/* Message of the last failing call on this context ("" if none). */
+/* Message of the last failing call on this context ("" if none).  With
+ * ctx == NULL: the message of the calling thread's last failing
+ * context-free call (rdst_residual_norms_noalloc). */
 const char* rdst_last_error(const rdst_ctx* ctx);
 
 /* Release the context and all its device memory. */
@@ -207,6 +209,24 @@ void* rdst_stream(rdst_ctx* ctx);
 int64_t rdst_launch_count(const rdst_ctx* ctx);
 double rdst_last_step_ms(const rdst_ctx* ctx);
 rdst_status rdst_kernel_stats(rdst_ctx* ctx, const char* kernel, int64_t* launches, double* total_ms);
+
+/* Allocation-free residual norms (no counterpart in the reference; an
+ * addition for callers that may not allocate device memory: code running
+ * during CUDA stream capture, where cudaMalloc is not capturable, hosts
+ * whose device memory belongs to a pool allocator, and paths that cannot
+ * pay cudaMalloc's implicit synchronisation).
+ * R (n_cells x 5, per unit volume), V (n_cells) and out (6) are DEVICE
+ * pointers owned by the caller; out[0] = sqrt(sum_i |R_i|^2) (res_mag of
+ * rdst_step_report), out[1+k] = ||R_k V||_2 (res_l2).  Runs asynchronously
+ * on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * Scratch is a fixed 192 KiB array in the library's device image, present
+ * on every GPU that loads the library until the process exits; n_cells
+ * above 1,048,576 is rejected with RDST_ERR_ARG.  Calls share that array:
+ * calls whose kernels may overlap on the GPU race and must be serialised.
+ * The first call on a device looks up the array's device address (a
+ * one-time set-up); make that first call before any stream capture. */
+rdst_status rdst_residual_norms_noalloc(int32_t n_cells, const double* R, const double* V,
+                                        double* out, void* stream);
 
 /* Library identification (e.g. "rdst-b200 sm_100a"). */
 const char* rdst_version(void);

@@ -2,9 +2,9 @@
 
     python -m rhodst_b200.build [--force]
 
-The library is one nvcc translation unit (csrc/rdst_api.cu, which includes
-the kernel headers) compiled for sm_100a only; the .so travels with the
-source tree, so nothing is JIT-compiled at run time.
+The library is built from csrc/*.cu (rdst_api.cu includes the kernel
+headers) for sm_100a only; the .so travels with the source tree, so
+nothing is JIT-compiled at run time.
 """
 from __future__ import annotations
 
@@ -49,7 +49,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and up_to_date():
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", str(tmp), str(CSRC / "rdst_api.cu")]
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", str(tmp), *[str(p) for p in sorted(CSRC.glob("*.cu"))]]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)

@@ -1382,7 +1382,9 @@ RDST_API rdst_status rdst_forces(rdst_ctx* c, int32_t patch, const double lift[3
     });
 }
 
-RDST_API const char* rdst_last_error(const rdst_ctx* c) { return c ? c->err.c_str() : "null context"; }
+const char* rdst_noalloc_error_message();   // rdst_noalloc.cu
+
+RDST_API const char* rdst_last_error(const rdst_ctx* c) { return c ? c->err.c_str() : rdst_noalloc_error_message(); }
 
 RDST_API void* rdst_stream(rdst_ctx* c) { return c ? (void*)c->s : nullptr; }
 

@@ -1,0 +1,62 @@
+"""Allocation-free residual norms (rdst_residual_norms_noalloc).
+
+Some callers cannot allocate device memory: code running while a CUDA
+stream is captured into a graph (cudaMalloc is not a capturable call),
+hosts whose device memory is handed out by a pool allocator, and paths that
+cannot pay cudaMalloc's implicit synchronisation.  This entry point keeps
+its scratch in a fixed array inside the library.  The test calls it through
+the C ABI on device buffers the test owns and checks it against the norms
+the existing rdst_step report gives for the same residual, on two calls in
+a row.  The file is named to be collected last."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import rhodst_b200
+from rhodst_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _fn():
+    lib = rhodst_b200.load_library()
+    f = lib.rdst_residual_norms_noalloc
+    f.restype = ctypes.c_int32
+    f.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.rdst_last_error.restype = ctypes.c_char_p
+    lib.rdst_last_error.argtypes = [ctypes.c_void_p]
+    return lib, f
+
+
+def test_residual_norms_noalloc_matches_step_report():
+    import torch
+    lib, fn = _fn()
+    case = cases.forward_step_c1()
+    s = rhodst_b200.solver_for(case)
+    R = s.residual()                     # R(W) of the current state
+    rep = s.step(1)[0]                   # the step reports the norms of that same R
+    expect = np.array([rep["res_mag"]] + list(rep["res_l2"]))
+    N = case.mesh.n_cells
+    dev = torch.device("cuda", 0)
+    Rd = torch.tensor(R, dtype=torch.float64, device=dev).contiguous()
+    Vd = torch.tensor(case.mesh.V, dtype=torch.float64, device=dev).contiguous()
+    out = torch.zeros(6, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for scale in (1.0, 2.0):             # two calls in a row sharing the scratch
+        x = (Rd * scale).contiguous()
+        st = fn(N, x.data_ptr(), Vd.data_ptr(), out.data_ptr(), stream)
+        assert st == 0, lib.rdst_last_error(None)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.allclose(got, expect * scale, rtol=1e-12, atol=0.0), (got, expect * scale)
+
+
+def test_residual_norms_noalloc_rejects_oversize():
+    import torch
+    lib, fn = _fn()
+    dev = torch.device("cuda", 0)
+    buf = torch.zeros(8, dtype=torch.float64, device=dev)
+    st = fn(1_048_577, buf.data_ptr(), buf.data_ptr(), buf.data_ptr(), None)
+    assert st == 7                       # RDST_ERR_ARG, nothing launched
+    assert b"exceeds the fixed scratch capacity" in lib.rdst_last_error(None)
