@@ -91,6 +91,13 @@ def forward_step_c1(refine: int = 1, solver: str = "GMRES", preconditioner: str 
                 steps=1000)
 
 
+def _vector_limiter(limiter: str) -> str:
+    """Scheme name for reconstruct(U): the TVD limiters take their "V"
+    (direction-aware) variant; linear, upwind and Venkatakrishnan are used
+    as they are."""
+    return limiter if limiter in ("linear", "upwind", "Venkatakrishnan") else limiter + "V"
+
+
 def farfield_state(mach: float, alpha_deg: float, T_inf: float, p_inf: float, gas: dict):
     g = gas["Cp"] / (gas["Cp"] - gas["R"])
     a = math.sqrt(g * gas["R"] * T_inf)
@@ -113,7 +120,7 @@ def naca0012_inviscid(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: fl
         "airfoil": {"p": "zeroGradient", "U": "slip", "T": "zeroGradient"},
         "farfield": {"p": ("farField", 1.0), "U": ("farField", U0), "T": ("farField", 1.0)},
     }
-    vlim = "Venkatakrishnan" if limiter == "Venkatakrishnan" else limiter + "V"
+    vlim = _vector_limiter(limiter)
     options = {
         "fluxScheme": flux,
         "Jacobian": "Roe",
@@ -221,7 +228,7 @@ def naca0012_turbulent(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: f
         "farfield": {"p": ("farField", 1.0), "U": ("farField", U0), "T": ("farField", 1.0),
                      "nuTilda": ("inletOutlet", nut_inf)},
     }
-    vlim = "Venkatakrishnan" if limiter == "Venkatakrishnan" else limiter + "V"
+    vlim = _vector_limiter(limiter)
     options = {
         "fluxScheme": flux,
         "Jacobian": "Roe",

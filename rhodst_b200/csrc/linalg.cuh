@@ -236,97 +236,151 @@ __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> A, MT* __res
     }
 }
 
-// x = (LU)^-1 b : forward y_r = b_r - sum_k L_rk y_k, backward
-// x_r = inv(U_rr)(y_r - sum_j U_rj x_j), level by level inside the CTA.
-// Five lanes per row (one per output component, six rows per warp): the
-// column/value loads of a row are independent of each other and of the
-// level's data, so a level costs one round trip for the neighbour gathers
-// (written by the previous level of the same CTA) plus the barrier.
-constexpr int ILU_APPLY_TPB = 256;
+constexpr int ILU_APPLY_TPB = 128;
+constexpr int ILU_APPLY_MINB = 4;      // resident CTAs per SM the register budget is sized for
+constexpr int ILU_MAX_LV = 1023;       // level offsets staged in shared memory up to this many
 
+// One row task of a sweep: the factor row's columns, this lane's entries
+// of each slot, its pivot-inverse row (backward sweep) and the starting
+// value of y.  Tasks are loaded one ahead of use, so their global loads
+// are in flight across the previous task and its barrier; only the loads
+// of x (rows finished in earlier levels) stay on the level-to-level chain.
 template <typename MT, int NB>
-__global__ void __launch_bounds__(ILU_APPLY_TPB) k_ilu_apply(int N, const MT* __restrict__ lu,
-                                                             const MT* __restrict__ dinv, IluDev P,
-                                                             const double* __restrict__ b, double* x,
-                                                             const int* __restrict__ active) {
+struct IluTask {
+    int cq[NB];
+    MT v[NB][5];
+    MT di[5];
+    double y0;
+};
+
+template <typename MT, int NB, bool BACK>
+__device__ __forceinline__ void ilu_load_task(IluTask<MT, NB>& t, const MT* __restrict__ lu,
+                                              const MT* __restrict__ dinv, const int* __restrict__ lu_col,
+                                              const double* y_src, int r, bool act, int comp, int s0, int ns,
+                                              int ms) {
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        const bool ok = act && q < ns;
+        const int fid = ok ? lu_fid(r, s0 + q, ms) : 0;
+        t.cq[q] = ok ? lu_col[fid] : -1;
+        // empty factor slots hold zeros: the value loads do not wait for the column
+#pragma unroll
+        for (int j = 0; j < 5; ++j) t.v[q][j] = ok ? lu[flat_e(fid, 5 * comp + j)] : mt_zero<MT>();
+    }
+    if (BACK) {
+#pragma unroll
+        for (int j = 0; j < 5; ++j) t.di[j] = act ? dinv[flat_e(r, 5 * comp + j)] : mt_zero<MT>();
+    }
+    t.y0 = act ? y_src[5 * r + comp] : 0.0;
+}
+
+// x = (LU)^-1 b on each subdomain: one CTA per part walks the part's
+// wavefront levels forward (x = L^-1 b, unit diagonal) and backward
+// (x = U^-1 x with the stored pivot inverses), a barrier between levels.
+// Five lanes per row (one per component), six rows per warp.
+template <typename MT, int NB>
+__global__ void __launch_bounds__(ILU_APPLY_TPB, ILU_APPLY_MINB)
+    k_ilu_apply(int N, const MT* __restrict__ lu, const MT* __restrict__ dinv, IluDev P,
+                const double* __restrict__ b, double* x, const int* __restrict__ active) {
     if (active && !*active) return;
+    __shared__ int s_off[ILU_MAX_LV + 1];
     const int part = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rsub = lane / 5, comp = lane - 5 * (lane / 5);
     const bool lane_ok = lane < 30;
-    const int rows_per_pass = (blockDim.x >> 5) * 6;
+    const int rpp = (blockDim.x >> 5) * 6;
     const int l0 = P.part_lvl0[part], l1 = P.part_lvl0[part + 1];
     const int ml = P.ml, mu = P.mu, ms = ml + mu;
-    for (int l = l0; l < l1; ++l) {
-        const int r0 = P.lvl_off[l], r1 = P.lvl_off[l + 1];
-        for (int base = 0; base < r1 - r0; base += rows_per_pass) {
-            const int r = r0 + base + warp * 6 + rsub;
-            if (lane_ok && r < r1) {
-                int cq[NB];
-                double v[NB][5];
+    const bool staged = l1 - l0 <= ILU_MAX_LV;
+    if (staged)
+        for (int i = threadIdx.x; i <= l1 - l0; i += blockDim.x) s_off[i] = P.lvl_off[l0 + i];
+    __syncthreads();
+    auto off = [&](int l) { return staged ? s_off[l - l0] : P.lvl_off[l]; };
+
+    // ---- forward: x_r = b_r - sum_q L_rq x_q
+    {
+        int l = l0, base = 0;
+        int r = 0;
+        bool act = false;
+        IluTask<MT, NB> cur, nxt;
+        if (l < l1) {
+            r = off(l) + warp * 6 + rsub;
+            act = lane_ok && r < off(l + 1);
+        }
+        ilu_load_task<MT, NB, false>(cur, lu, dinv, P.lu_col, b, r, act, comp, 0, ml, ms);
+        while (l < l1) {
+            int nl = l, nbase = base + rpp;
+            const bool lvl_end = nbase >= off(l + 1) - off(l);
+            if (lvl_end) { nl = l + 1; nbase = 0; }
+            int nr = 0;
+            bool nact = false;
+            if (nl < l1) {
+                nr = off(nl) + nbase + warp * 6 + rsub;
+                nact = lane_ok && nr < off(nl + 1);
+            }
+            ilu_load_task<MT, NB, false>(nxt, lu, dinv, P.lu_col, b, nr, nact, comp, 0, ml, ms);
+            if (act) {
+                double y = cur.y0;
 #pragma unroll
                 for (int q = 0; q < NB; ++q) {
-                    const int fid = lu_fid(r, q, ms);
-                    cq[q] = (q < ml) ? P.lu_col[fid] : -1;
-                    // empty factor slots hold zeros: the value loads do not
-                    // wait for the column
+                    if (cur.cq[q] >= 0) {
+                        const double* xk = x + 5 * cur.cq[q];
 #pragma unroll
-                    for (int j = 0; j < 5; ++j)
-                        v[q][j] = (q < ml) ? ld(lu + flat_e(fid, 5 * comp + j)) : 0.0;
-                }
-                double y = b[5 * r + comp];
-#pragma unroll
-                for (int q = 0; q < NB; ++q) {
-                    if (cq[q] >= 0) {
-                        const double* xk = x + 5 * cq[q];
-#pragma unroll
-                        for (int j = 0; j < 5; ++j) y -= v[q][j] * xk[j];
+                        for (int j = 0; j < 5; ++j) y -= tod(cur.v[q][j]) * xk[j];
                     }
                 }
                 x[5 * r + comp] = y;
             }
+            if (lvl_end) __syncthreads();
+            cur = nxt; r = nr; act = nact; l = nl; base = nbase;
         }
-        __syncthreads();
     }
-    for (int l = l1 - 1; l >= l0; --l) {
-        const int r0 = P.lvl_off[l], r1 = P.lvl_off[l + 1];
-        for (int base = 0; base < r1 - r0; base += rows_per_pass) {
-            const int r = r0 + base + warp * 6 + rsub;
-            const bool act = lane_ok && r < r1;
-            double y = 0.0, di[5] = {0, 0, 0, 0, 0};
+    // ---- backward: x_r = inv(U_rr) (x_r - sum_q U_rq x_q)
+    {
+        int l = l1 - 1, base = 0;
+        int r = 0;
+        bool act = false;
+        IluTask<MT, NB> cur, nxt;
+        if (l >= l0) {
+            r = off(l) + warp * 6 + rsub;
+            act = lane_ok && r < off(l + 1);
+        }
+        ilu_load_task<MT, NB, true>(cur, lu, dinv, P.lu_col, x, r, act, comp, ml, mu, ms);
+        while (l >= l0) {
+            int nl = l, nbase = base + rpp;
+            const bool lvl_end = nbase >= off(l + 1) - off(l);
+            if (lvl_end) { nl = l - 1; nbase = 0; }
+            int nr = 0;
+            bool nact = false;
+            if (nl >= l0) {
+                nr = off(nl) + nbase + warp * 6 + rsub;
+                nact = lane_ok && nr < off(nl + 1);
+            }
+            // rows of level nl are written only when level nl is swept, so
+            // their forward results can be read ahead
+            ilu_load_task<MT, NB, true>(nxt, lu, dinv, P.lu_col, x, nr, nact, comp, ml, mu, ms);
+            double y = cur.y0;
             if (act) {
-                int cq[NB];
-                double v[NB][5];
 #pragma unroll
                 for (int q = 0; q < NB; ++q) {
-                    const int fid = lu_fid(r, ml + q, ms);
-                    cq[q] = (q < mu) ? P.lu_col[fid] : -1;
+                    if (cur.cq[q] >= 0) {
+                        const double* xj = x + 5 * cur.cq[q];
 #pragma unroll
-                    for (int j = 0; j < 5; ++j)
-                        v[q][j] = (q < mu) ? ld(lu + flat_e(fid, 5 * comp + j)) : 0.0;
-                }
-#pragma unroll
-                for (int j = 0; j < 5; ++j) di[j] = ld(dinv + flat_e(r, 5 * comp + j));
-                y = x[5 * r + comp];
-#pragma unroll
-                for (int q = 0; q < NB; ++q) {
-                    if (cq[q] >= 0) {
-                        const double* xj = x + 5 * cq[q];
-#pragma unroll
-                        for (int j = 0; j < 5; ++j) y -= v[q][j] * xj[j];
+                        for (int j = 0; j < 5; ++j) y -= tod(cur.v[q][j]) * xj[j];
                     }
                 }
             }
-            // x_r = inv(U_rr) y : gather the row's five components by shuffle
+            // gather the row's five components by shuffle (all lanes take part)
             double a = 0.0;
 #pragma unroll
             for (int j = 0; j < 5; ++j) {
-                double yj = __shfl_sync(0xffffffffu, y, (lane_ok ? 5 * rsub : 0) + j);
-                a += di[j] * yj;
+                const double yj = __shfl_sync(0xffffffffu, y, (lane_ok ? 5 * rsub : 0) + j);
+                a += tod(cur.di[j]) * yj;
             }
             if (act) x[5 * r + comp] = a;
+            if (lvl_end) __syncthreads();
+            cur = nxt; r = nr; act = nact; l = nl; base = nbase;
         }
-        __syncthreads();
     }
 }
 

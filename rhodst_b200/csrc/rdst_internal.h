@@ -103,5 +103,11 @@ template <typename T> __device__ __forceinline__ double ld(const T* p) { return 
 template <> __device__ __forceinline__ double ld<__nv_bfloat16>(const __nv_bfloat16* p) { return (double)__bfloat162float(*p); }
 template <typename T> __device__ __forceinline__ void st(T* p, double v) { *p = (T)v; }
 template <> __device__ __forceinline__ void st<__nv_bfloat16>(__nv_bfloat16* p, double v) { *p = __float2bfloat16_rn((float)v); }
+// register value -> double, and the storage type's zero
+__device__ __forceinline__ double tod(double v) { return v; }
+__device__ __forceinline__ double tod(float v) { return (double)v; }
+__device__ __forceinline__ double tod(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
+template <typename T> __device__ __forceinline__ T mt_zero() { return T(0); }
+template <> __device__ __forceinline__ __nv_bfloat16 mt_zero<__nv_bfloat16>() { return __float2bfloat16_rn(0.0f); }
 
 }  // namespace rdst
