@@ -2,7 +2,7 @@
 """Benchmark of the fully-coupled density-based step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload forward_step_2d|...]
+                    [--workload swept_wing_fp32|...]
 
 Metric: cell-iterations per second (cells x nonlinear iterations / s) of
 the implicit step (flux + residual, Roe Jacobian assembly, preconditioner
@@ -35,6 +35,13 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 
+def precision_desc(options: dict) -> str:
+    prec = options.get("precision", "fp64")
+    basis = "fp64" if basis_bytes(options) == 8 else "fp32"
+    return (f"Jacobian/ILU {prec}, GMRES basis {basis}; residual, update, dots, Hessenberg "
+            f"and norms fp64")
+
+
 def workload(name: str):
     from rhodst_b200 import cases
     if name == "forward_step_2d":
@@ -52,7 +59,7 @@ def workload(name: str):
                 "cells": c.mesh.n_cells, "internal_faces": c.mesh.n_internal_faces,
                 "flux": "HLLC", "reconstruction": "OSPRE/OSPREV", "ddt": "steadyStateDST local dt, CFL ramp 5->50",
                 "solver": "GMRES(20), 1 restart cycle", "preconditioner": "subdomain block ILU(0)",
-                "precision": f"Jacobian/ILU {prec}, residual/vectors fp64", "mach": 0.84, "alpha_deg": 3.06}
+                "precision": precision_desc(c.options), "mach": 0.84, "alpha_deg": 3.06}
         return c, desc
     if name.startswith("naca0012_sa"):
         prec = name.split("_")[-1] if name.count("_") >= 2 else "fp64"
@@ -62,7 +69,7 @@ def workload(name: str):
                 "flux": "AUSM+up", "reconstruction": "Venkatakrishnan", "turbulence": "SAneg",
                 "ddt": "steadyStateDST local dt, CFL ramp 2->50", "solver": "GMRES(30), 1 restart cycle",
                 "preconditioner": "subdomain block ILU(0)", "mach": 0.73, "alpha_deg": 2.3, "reynolds": 6.5e6,
-                "precision": f"Jacobian/ILU {prec}, residual/vectors fp64"}
+                "precision": precision_desc(c.options)}
         return c, desc
     raise SystemExit(f"unknown workload {name}")
 
@@ -124,10 +131,14 @@ def measured_peaks():
 
 # Algorithmic (compulsory) bytes per launch of each kernel class; S = bytes
 # per stored matrix scalar, Bk = N + 2F blocks, 4-byte column indices.
-def algorithmic_bytes(kind: str, N: int, F: int, S: int, precon: str) -> float:
+def algorithmic_bytes(kind: str, N: int, F: int, S: int, precon: str, vb: int = 8, m: int = 20) -> float:
+    """Bytes one launch of a kernel class must move at least: S bytes per
+    Jacobian/factor entry (8 fp64, 4 fp32, 2 bf16), vb per Krylov basis
+    entry, m GMRES directions per restart cycle."""
     Bk = N + 2 * F
     if kind == "spmv":
-        return 25 * S * Bk + 4 * Bk + 40 * N + 40 * N
+        # matrix + column ids, x (a basis vector: vb per entry), y fp64
+        return 25 * S * Bk + 4 * Bk + 5 * vb * N + 40 * N
     if kind == "precond":
         if precon == "diagonal":
             return 25 * S * N + 40 * N + 40 * N
@@ -140,13 +151,22 @@ def algorithmic_bytes(kind: str, N: int, F: int, S: int, precon: str) -> float:
     if kind == "factor":
         return 2 * (25 * S * Bk + 4 * Bk) + 25 * S * N
     if kind == "orth":
-        # one GMRES direction of CGS2 at the mean basis size: two multi-dots
-        # (read w + j vectors) and two multi-axpys (read j vectors, rw w)
-        return 40 * N * (2 * (ORTH_J + 1) + 2 * (ORTH_J + 2))
+        # one GMRES direction of CGS2 at the mean basis size J = (m+1)/2:
+        # three passes over the J basis vectors (dots; axpy fused with the
+        # second dots; axpy fused with the norm) and five passes over w
+        # (read; read+write; read+write), w in fp64
+        J = (m + 1) / 2.0
+        return N * (3 * J * 5 * vb + 5 * 40)
     return 0.0
 
 
-ORTH_J = 10.5     # mean number of basis vectors per direction for GMRES(20)
+def basis_bytes(options: dict) -> int:
+    """Bytes per Krylov basis entry: fp32 unless the Jacobian is fp64 (the
+    library default), or as set by krylov.basis."""
+    b = options.get("krylov", {}).get("basis") if isinstance(options.get("krylov"), dict) else options.get("krylov.basis")
+    if b is None:
+        b = "fp64" if options.get("precision", "fp64") == "fp64" else "fp32"
+    return 8 if b == "fp64" else 4
 
 
 def run_ours(args, rank, world):
@@ -156,7 +176,7 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     case, desc = workload(args.workload)
     opts = dict(case.options)
-    opts["profile"] = True
+    opts["profile"] = False          # timed steps run without per-kernel events
     s = rhodst_b200.Solver(case.mesh, case.bcs, opts)
     s.set_primitive(case.p, case.U, case.T)
     N, F = case.mesh.n_cells, case.mesh.n_internal_faces
@@ -165,7 +185,6 @@ def run_ours(args, rank, world):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB
     for _ in range(args.warmup):
         s.step(1)
-    stats0 = {k: s.kernel_stats(k) for k in ("spmv", "precond", "flux", "assemble", "factor", "orth", "update")}
     launches0 = s.launch_count()
     if world > 1:
         torch.distributed.barrier()
@@ -187,18 +206,34 @@ def run_ours(args, rank, world):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     value = world * N * args.steps / (total_ms * 1e-3)
-    # dominant kernel class over the timed region -> roofline
-    stats = {k: tuple(np.subtract(s.kernel_stats(k), stats0[k])) for k in stats0}
+    # kernel classes and the roofline of the dominant one: CUDA events around
+    # each launch (on the library's stream) over a separate run of the same
+    # number of steps (capped at 10), L2 flushed between steps as above
+    s.set_profile(True)
+    s.step(1)
+    classes = ("spmv", "precond", "flux", "assemble", "factor", "orth", "update")
+    stats0 = {k: s.kernel_stats(k) for k in classes}
+    prof_steps = min(args.steps, 10)
+    prof_ms = 0.0
+    for _ in range(prof_steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        s.step(1)
+        prof_ms += s.last_step_ms()
+    s.set_profile(False)
+    stats = {k: tuple(np.subtract(s.kernel_stats(k), stats0[k])) for k in classes}
     prec0 = case.options.get("precision", "fp64")
     S0 = 8 if prec0 == "fp64" else (4 if prec0 == "fp32" else 2)
     pc0 = case.options["solvers"]["W"]["preconditioner"]
+    vb0 = basis_bytes(case.options)
+    m0 = int(case.options["solvers"]["W"].get("nDirections", 20))
     breakdown = {}
     for k, (nl_, ms_) in stats.items():
         if nl_ <= 0:
             continue
-        by_ = algorithmic_bytes(k, N, F, S0, pc0)
+        by_ = algorithmic_bytes(k, N, F, S0, pc0, vb0, m0)
         breakdown[k] = {"launches": int(nl_), "avg_us": round(ms_ / nl_ * 1e3, 2),
-                        "share_of_step": round(ms_ / max(total_ms, 1e-9), 4),
+                        "share_of_step": round(ms_ / max(prof_ms, 1e-9), 4),
                         "GBps": round(by_ / (ms_ / nl_ * 1e-3) / 1e9, 1) if by_ else None}
     dom = max(stats, key=lambda k: stats[k][1])
     n_l, ms_l = stats[dom]
@@ -208,13 +243,13 @@ def run_ours(args, rank, world):
     peak, peak_kind = measured_peaks()
     roof = None
     if n_l > 0 and ms_l > 0:
-        by = algorithmic_bytes(dom, N, F, S, precon)
+        by = algorithmic_bytes(dom, N, F, S, precon, vb0, m0)
         ach = by / (ms_l / n_l * 1e-3) / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
                 "bytes_per_launch": by, "launches": int(n_l), "avg_launch_us": round(ms_l / n_l * 1e3, 3),
                 "traffic": None,
-                "share_of_step": round(ms_l / max(total_ms, 1e-9), 4),
+                "share_of_step": round(ms_l / max(prof_ms, 1e-9), 4),
                 "note": "working set below L2 (126 MB): L2-resident bandwidth" if
                         (25 * S * (N + 2 * F)) < 100e6 else "HBM-resident"}
     # e2e through the C ABI with host buffers: H2D state, step, D2H state
@@ -233,12 +268,13 @@ def run_ours(args, rank, world):
     line = {"metric": "cell_iterations_per_s", "value": value, "unit": "cell-iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if prec == "fp64" else f"f64 residual/vectors, {prec} Jacobian+ILU",
+            "dtype": "f64" if prec == "fp64" else (f"f64 residual/dots/Hessenberg, {prec} Jacobian+ILU, "
+                                                  f"{'f32' if vb0 == 4 else 'f64'} Krylov basis"),
             "data": "synthetic (generated mesh, uniform Mach-3 inflow initial state)",
             "config": dict(desc, l2="flushed: 256 MB written between timed steps",
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches), "roofline": roof,
-            "kernels": breakdown}
+            "kernels": breakdown, "kernels_profiled_ms_per_step": round(prof_ms / max(prof_steps, 1), 3)}
     return line, case
 
 
@@ -309,7 +345,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="forward_step_2d")
+    ap.add_argument("--workload", default="swept_wing_fp32",
+                    help="swept_wing_fp32 (default) | swept_wing_fp64 | swept_wing_bf16 | forward_step_2d | "
+                         "naca0012_sa[_fp32]")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--converge", type=float, default=0.0,
                     help="run to this density-residual drop instead of timing fixed steps")

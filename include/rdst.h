@@ -204,11 +204,15 @@ rdst_status rdst_partition_cells(int32_t n_cells, const double* C,
  * rdst_kernel_stats: with the option "profile" "true", the library records
  * CUDA events around every launch of the named kernel class inside
  * rdst_step ("spmv", "precond", "flux", "assemble", "factor", "orth",
- * "update") and returns its launch count and summed device time. */
+ * "update") and returns its launch count and summed device time.
+ * rdst_set_profile: switches that recording on or off for later steps
+ * (the event records add device time of their own, so steps are timed
+ * with it off).  No counterpart in the reference (instrumentation). */
 void* rdst_stream(rdst_ctx* ctx);
 int64_t rdst_launch_count(const rdst_ctx* ctx);
 double rdst_last_step_ms(const rdst_ctx* ctx);
 rdst_status rdst_kernel_stats(rdst_ctx* ctx, const char* kernel, int64_t* launches, double* total_ms);
+rdst_status rdst_set_profile(rdst_ctx* ctx, int32_t on);
 
 /* Allocation-free residual norms (no counterpart in the reference; an
  * addition for callers that may not allocate device memory: code running

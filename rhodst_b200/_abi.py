@@ -120,6 +120,7 @@ def declare(lib: ctypes.CDLL, prefix: str) -> None:
         f("launch_count", ctypes.c_int64, [vp])
         f("last_step_ms", c_double, [vp])
         f("kernel_stats", c_int32, [vp, c_char_p, POINTER(ctypes.c_int64), POINTER(c_double)])
+        f("set_profile", c_int32, [vp, c_int32])
 
 
 def _dptr(a: Optional[np.ndarray]):
@@ -268,6 +269,9 @@ class Solver:
 
     def last_step_ms(self) -> float:
         return float(self._fn("last_step_ms")(self._h))
+
+    def set_profile(self, on: bool) -> None:
+        self._check(self._fn("set_profile")(self._h, 1 if on else 0), "set_profile")
 
     def kernel_stats(self, kernel: str):
         n = ctypes.c_int64()

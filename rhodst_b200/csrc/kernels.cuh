@@ -95,6 +95,39 @@ __global__ void k_init_state(int N, Thermo th, const double* __restrict__ prim, 
     W[5 * i + 4] = rho * (h * th.Cv / th.Cp + 0.5 * magSqr3(U));
 }
 
+// Conservative fields in the caller's cell order (rho[N], rhoU[3N],
+// rhoE[N], staged on the device) -> W and the primitive record in the
+// internal order (perm[r] = caller's index of internal row r).  The
+// arithmetic is written with explicit roundings so that it matches a plain
+// host evaluation of the same formulas bit for bit.
+__global__ void k_set_conservative(int N, Thermo th, const int* __restrict__ perm, const double* __restrict__ rho,
+                                   const double* __restrict__ rhoU, const double* __restrict__ rhoE,
+                                   double* __restrict__ W, double* __restrict__ prim) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= N) return;
+    const int i = perm[r];
+    const double rh = rho[i], mx = rhoU[3 * i], my = rhoU[3 * i + 1], mz = rhoU[3 * i + 2], E = rhoE[i];
+    W[5 * r] = rh; W[5 * r + 1] = mx; W[5 * r + 2] = my; W[5 * r + 3] = mz; W[5 * r + 4] = E;
+    const double Ux = __ddiv_rn(mx, rh), Uy = __ddiv_rn(my, rh), Uz = __ddiv_rn(mz, rh);
+    const double k2 = __dadd_rn(__dadd_rn(__dmul_rn(Ux, Ux), __dmul_rn(Uy, Uy)), __dmul_rn(Uz, Uz));
+    const double e = __dsub_rn(__ddiv_rn(E, rh), __dmul_rn(0.5, k2));
+    const double T = __ddiv_rn(e, th.Cv);
+    double* P = prim + PW * r;
+    P[0] = __dmul_rn(__dmul_rn(rh, th.R), T); P[1] = T; P[2] = __dmul_rn(th.Cp, T);
+    P[3] = Ux; P[4] = Uy; P[5] = Uz;
+}
+
+// W (internal order) -> rho, rhoU, rhoE in the caller's cell order
+__global__ void k_get_conservative(int N, const int* __restrict__ perm, const double* __restrict__ W,
+                                   double* __restrict__ rho, double* __restrict__ rhoU, double* __restrict__ rhoE) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= N) return;
+    const int i = perm[r];
+    rho[i] = W[5 * r];
+    rhoU[3 * i] = W[5 * r + 1]; rhoU[3 * i + 1] = W[5 * r + 2]; rhoU[3 * i + 2] = W[5 * r + 3];
+    rhoE[i] = W[5 * r + 4];
+}
+
 // boundary state before the first BC evaluation: internal values and the
 // mass flux (rho U)_owner . Sf
 __global__ void k_init_phib(DevMesh m, const double* __restrict__ W, const double* __restrict__ prim,

@@ -41,9 +41,10 @@ __device__ __forceinline__ void inv5(const double A[25], double X[25]) {
         for (int j = 0; j < 5; ++j) X[5 * i + j] = a[i][j + 5];
 }
 
-// y = A x  (or y = b - A x when b != nullptr); one row per thread
-template <typename MT>
-__global__ void __launch_bounds__(256) k_spmv(SellMat<MT> A, const double* __restrict__ x, double* __restrict__ y,
+// y = A x  (or y = b - A x when b != nullptr); one row per thread; x in
+// FP64 or (a Krylov basis vector) FP32, products and y in FP64
+template <typename MT, typename XT = double>
+__global__ void __launch_bounds__(256) k_spmv(SellMat<MT> A, const XT* __restrict__ x, double* __restrict__ y,
                                               const double* __restrict__ b, const int* __restrict__ active) {
     if (active && !*active) return;
     int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -55,8 +56,8 @@ __global__ void __launch_bounds__(256) k_spmv(SellMat<MT> A, const double* __res
         size_t slot = (size_t)(base + k);
         int c = A.col[slot * 32 + lane];
         if (c < 0) continue;
-        const double* xc = x + 5 * c;
-        double xv[5] = {xc[0], xc[1], xc[2], xc[3], xc[4]};
+        const XT* xc = x + 5 * c;
+        double xv[5] = {tod(xc[0]), tod(xc[1]), tod(xc[2]), tod(xc[3]), tod(xc[4])};
         const MT* v = A.val + slot * (32 * 25) + lane;
 #pragma unroll
         for (int i = 0; i < 5; ++i)
@@ -274,14 +275,23 @@ __device__ __forceinline__ void ilu_load_task(IluTask<MT, NB>& t, const MT* __re
     t.y0 = act ? y_src[5 * r + comp] : 0.0;
 }
 
+// Tasks of one sweep in order: level by level (forward ascending, backward
+// descending), rpp rows per task.  The cursor is uniform over the CTA.
+struct IluCursor {
+    int l, base;
+};
+
 // x = (LU)^-1 b on each subdomain: one CTA per part walks the part's
 // wavefront levels forward (x = L^-1 b, unit diagonal) and backward
 // (x = U^-1 x with the stored pivot inverses), a barrier between levels.
-// Five lanes per row (one per component), six rows per warp.
+// Five lanes per row (one per component), six rows per warp.  PF tasks
+// are loaded ahead of the one being computed (two with 4- or 2-byte
+// factors, one with 8-byte ones: the register budget of four CTAs per SM).
 template <typename MT, int NB>
 __global__ void __launch_bounds__(ILU_APPLY_TPB, ILU_APPLY_MINB)
     k_ilu_apply(int N, const MT* __restrict__ lu, const MT* __restrict__ dinv, IluDev P,
                 const double* __restrict__ b, double* x, const int* __restrict__ active) {
+    constexpr int PF = sizeof(MT) < 8 ? 2 : 1;
     if (active && !*active) return;
     __shared__ int s_off[ILU_MAX_LV + 1];
     const int part = blockIdx.x;
@@ -297,89 +307,64 @@ __global__ void __launch_bounds__(ILU_APPLY_TPB, ILU_APPLY_MINB)
     __syncthreads();
     auto off = [&](int l) { return staged ? s_off[l - l0] : P.lvl_off[l]; };
 
-    // ---- forward: x_r = b_r - sum_q L_rq x_q
-    {
-        int l = l0, base = 0;
-        int r = 0;
-        bool act = false;
-        IluTask<MT, NB> cur, nxt;
-        if (l < l1) {
-            r = off(l) + warp * 6 + rsub;
-            act = lane_ok && r < off(l + 1);
-        }
-        ilu_load_task<MT, NB, false>(cur, lu, dinv, P.lu_col, b, r, act, comp, 0, ml, ms);
-        while (l < l1) {
-            int nl = l, nbase = base + rpp;
-            const bool lvl_end = nbase >= off(l + 1) - off(l);
-            if (lvl_end) { nl = l + 1; nbase = 0; }
-            int nr = 0;
-            bool nact = false;
-            if (nl < l1) {
-                nr = off(nl) + nbase + warp * 6 + rsub;
-                nact = lane_ok && nr < off(nl + 1);
+#pragma unroll 1
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        const bool back = sweep == 1;
+        const int dir = back ? -1 : 1;
+        const int s0 = back ? ml : 0, ns = back ? mu : ml;
+        const double* ysrc = back ? x : b;
+        IluCursor cur{back ? l1 - 1 : l0, 0};
+        auto in_range = [&](int l) { return back ? l >= l0 : l < l1; };
+        // task queue: slot 0 is computed, slots 1..PF are in flight
+        IluTask<MT, NB> q[PF + 1];
+        int rq[PF + 1];
+        bool aq[PF + 1], eq[PF + 1], vq[PF + 1];
+        auto next = [&](int d) {
+            vq[d] = in_range(cur.l);
+            rq[d] = 0; aq[d] = false; eq[d] = false;
+            if (vq[d]) {
+                const int r0 = off(cur.l), n = off(cur.l + 1) - r0;
+                rq[d] = r0 + cur.base + warp * 6 + rsub;
+                aq[d] = lane_ok && cur.base + warp * 6 + rsub < n;
+                cur.base += rpp;
+                eq[d] = cur.base >= n;
+                if (eq[d]) { cur.l += dir; cur.base = 0; }
             }
-            ilu_load_task<MT, NB, false>(nxt, lu, dinv, P.lu_col, b, nr, nact, comp, 0, ml, ms);
-            if (act) {
-                double y = cur.y0;
+            if (back) ilu_load_task<MT, NB, true>(q[d], lu, dinv, P.lu_col, ysrc, rq[d], aq[d], comp, s0, ns, ms);
+            else ilu_load_task<MT, NB, false>(q[d], lu, dinv, P.lu_col, ysrc, rq[d], aq[d], comp, s0, ns, ms);
+        };
 #pragma unroll
-                for (int q = 0; q < NB; ++q) {
-                    if (cur.cq[q] >= 0) {
-                        const double* xk = x + 5 * cur.cq[q];
+        for (int d = 0; d < PF; ++d) next(d);
+        while (vq[0]) {
+            next(PF);
+            double y = q[0].y0;
+            if (aq[0]) {
 #pragma unroll
-                        for (int j = 0; j < 5; ++j) y -= tod(cur.v[q][j]) * xk[j];
-                    }
-                }
-                x[5 * r + comp] = y;
-            }
-            if (lvl_end) __syncthreads();
-            cur = nxt; r = nr; act = nact; l = nl; base = nbase;
-        }
-    }
-    // ---- backward: x_r = inv(U_rr) (x_r - sum_q U_rq x_q)
-    {
-        int l = l1 - 1, base = 0;
-        int r = 0;
-        bool act = false;
-        IluTask<MT, NB> cur, nxt;
-        if (l >= l0) {
-            r = off(l) + warp * 6 + rsub;
-            act = lane_ok && r < off(l + 1);
-        }
-        ilu_load_task<MT, NB, true>(cur, lu, dinv, P.lu_col, x, r, act, comp, ml, mu, ms);
-        while (l >= l0) {
-            int nl = l, nbase = base + rpp;
-            const bool lvl_end = nbase >= off(l + 1) - off(l);
-            if (lvl_end) { nl = l - 1; nbase = 0; }
-            int nr = 0;
-            bool nact = false;
-            if (nl >= l0) {
-                nr = off(nl) + nbase + warp * 6 + rsub;
-                nact = lane_ok && nr < off(nl + 1);
-            }
-            // rows of level nl are written only when level nl is swept, so
-            // their forward results can be read ahead
-            ilu_load_task<MT, NB, true>(nxt, lu, dinv, P.lu_col, x, nr, nact, comp, ml, mu, ms);
-            double y = cur.y0;
-            if (act) {
+                for (int k = 0; k < NB; ++k) {
+                    if (q[0].cq[k] >= 0) {
+                        const double* xk = x + 5 * q[0].cq[k];
 #pragma unroll
-                for (int q = 0; q < NB; ++q) {
-                    if (cur.cq[q] >= 0) {
-                        const double* xj = x + 5 * cur.cq[q];
-#pragma unroll
-                        for (int j = 0; j < 5; ++j) y -= tod(cur.v[q][j]) * xj[j];
+                        for (int j = 0; j < 5; ++j) y -= tod(q[0].v[k][j]) * xk[j];
                     }
                 }
             }
-            // gather the row's five components by shuffle (all lanes take part)
-            double a = 0.0;
+            if (back) {
+                // x_r = inv(U_rr) y: gather the row's five components by
+                // shuffle (all lanes take part)
+                double a = 0.0;
 #pragma unroll
-            for (int j = 0; j < 5; ++j) {
-                const double yj = __shfl_sync(0xffffffffu, y, (lane_ok ? 5 * rsub : 0) + j);
-                a += tod(cur.di[j]) * yj;
+                for (int j = 0; j < 5; ++j) {
+                    const double yj = __shfl_sync(0xffffffffu, y, (lane_ok ? 5 * rsub : 0) + j);
+                    a += tod(q[0].di[j]) * yj;
+                }
+                y = a;
             }
-            if (act) x[5 * r + comp] = a;
-            if (lvl_end) __syncthreads();
-            cur = nxt; r = nr; act = nact; l = nl; base = nbase;
+            if (aq[0]) x[5 * rq[0] + comp] = y;
+            if (eq[0]) __syncthreads();
+#pragma unroll
+            for (int d = 0; d < PF; ++d) {
+                q[d] = q[d + 1]; rq[d] = rq[d + 1]; aq[d] = aq[d + 1]; eq[d] = eq[d + 1]; vq[d] = vq[d + 1];
+            }
         }
     }
 }
@@ -434,49 +419,123 @@ __device__ __forceinline__ void block_multi_sum(double (&acc)[NV], int nv, doubl
 }
 
 // partial[blk][j] = sum_i V_j[i] w[i] for j < nv <= NV (one pass over w)
-template <int NV>
-__global__ void __launch_bounds__(RED_TPB, 2) k_vmultidot(long n, int nv, const double* __restrict__ V, long ldv,
+// Four consecutive entries of a vector as doubles (16-byte loads; the
+// caller guarantees 4-entry alignment of p), or fewer at the vector's end.
+__device__ __forceinline__ void load4(const double* __restrict__ p, double (&o)[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void load4(const float* __restrict__ p, double (&o)[4]) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+}
+template <typename T>
+__device__ __forceinline__ void load4_tail(const T* __restrict__ p, long rem, double (&o)[4]) {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) o[e] = e < rem ? tod(p[e]) : 0.0;
+}
+template <typename T>
+__device__ __forceinline__ void load4_any(const T* __restrict__ p, long i0, long n, double (&o)[4]) {
+    if (i0 + 4 <= n) load4(p + i0, o);
+    else load4_tail(p + i0, n - i0, o);
+}
+
+// partial[blk * pstride + j] = sum_i V_j[i] w[i], j < nv: four entries per
+// thread and 16-byte loads; V (fp64 or fp32) has a row stride ldv that is
+// a multiple of 4 entries.  Full chunks take a branch-free path so that
+// the loads of all nv vectors are in flight together.
+template <int NV, typename VT = double>
+__global__ void __launch_bounds__(RED_TPB, 2) k_vmultidot(long n, int nv, const VT* __restrict__ V, long ldv,
                                                        const double* __restrict__ w, double* __restrict__ partial,
                                                        int pstride, const int* __restrict__ active) {
     if (active && !*active) return;
     double acc[NV];
 #pragma unroll
     for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const double wi = w[i];
+    const long nc = (n + 3) / 4, nfull = n / 4;
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long)gridDim.x * blockDim.x) {
+        const long i0 = 4 * c;
+        double wv[4];
+        if (c < nfull) {
+            load4(w + i0, wv);
 #pragma unroll
-        for (int j = 0; j < NV; ++j)
-            if (j < nv) acc[j] += V[j * ldv + i] * wi;
+            for (int j = 0; j < NV; ++j)
+                if (j < nv) {
+                    double v[4];
+                    load4(V + j * ldv + i0, v);
+                    acc[j] += v[0] * wv[0] + v[1] * wv[1] + v[2] * wv[2] + v[3] * wv[3];
+                }
+        } else {
+            load4_tail(w + i0, n - i0, wv);
+            for (int j = 0; j < nv && j < NV; ++j) {
+                double v[4];
+                load4_tail(V + j * ldv + i0, n - i0, v);
+                acc[j] += v[0] * wv[0] + v[1] * wv[1] + v[2] * wv[2] + v[3] * wv[3];
+            }
+        }
     }
     block_multi_sum<NV>(acc, nv, partial, pstride);
 }
 
 // w -= sum_j coef[j] V_j (j < nv), then in the same pass either the dots
-// V_j . w_new (mode 0: the second CGS2 pass) or w_new . w_new (mode 1)
-template <int NV>
-__global__ void __launch_bounds__(RED_TPB, 2) k_maxpy_dot(long n, int nv, const double* __restrict__ V, long ldv,
+// V_j . w_new (mode 0: the second CGS2 pass) or w_new . w_new (mode 1);
+// four entries per thread as in k_vmultidot
+template <int NV, typename VT = double>
+__global__ void __launch_bounds__(RED_TPB, 2) k_maxpy_dot(long n, int nv, const VT* __restrict__ V, long ldv,
                                                        const double* __restrict__ coef, double* __restrict__ w,
                                                        double* __restrict__ partial, int pstride, int mode,
                                                        const int* __restrict__ active) {
     if (active && !*active) return;
     __shared__ double cs[NV];
-    if (threadIdx.x < nv) cs[threadIdx.x] = coef[threadIdx.x];
+    if (threadIdx.x < NV) cs[threadIdx.x] = threadIdx.x < nv ? coef[threadIdx.x] : 0.0;
     __syncthreads();
     double acc[NV];
 #pragma unroll
     for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        double a = w[i];
-        for (int j = 0; j < nv; ++j) a -= cs[j] * V[j * ldv + i];
-        w[i] = a;
-        if (mode == 0) {
-            // second read of V_j[i]: the lines were just fetched (L1 hit)
+    const long nc = (n + 3) / 4, nfull = n / 4;
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long)gridDim.x * blockDim.x) {
+        const long i0 = 4 * c;
+        double a[4];
+        if (c < nfull) {
+            load4(w + i0, a);
 #pragma unroll
             for (int j = 0; j < NV; ++j)
-                if (j < nv) acc[j] += V[j * ldv + i] * a;
+                if (j < nv) {
+                    double v[4];
+                    load4(V + j * ldv + i0, v);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) a[e] -= cs[j] * v[e];
+                }
+            reinterpret_cast<double2*>(w + i0)[0] = make_double2(a[0], a[1]);
+            reinterpret_cast<double2*>(w + i0)[1] = make_double2(a[2], a[3]);
+            if (mode == 0) {
+                // second read of V_j: the lines were just fetched (L1 hit)
+#pragma unroll
+                for (int j = 0; j < NV; ++j)
+                    if (j < nv) {
+                        double v[4];
+                        load4(V + j * ldv + i0, v);
+                        acc[j] += v[0] * a[0] + v[1] * a[1] + v[2] * a[2] + v[3] * a[3];
+                    }
+            }
         } else {
-            acc[0] += a * a;
+            load4_tail(w + i0, n - i0, a);
+            for (int j = 0; j < nv && j < NV; ++j) {
+                double v[4];
+                load4_tail(V + j * ldv + i0, n - i0, v);
+                for (int e = 0; e < 4; ++e) a[e] -= cs[j] * v[e];
+            }
+            for (int e = 0; e < 4; ++e)
+                if (i0 + e < n) w[i0 + e] = a[e];
+            if (mode == 0) {
+                for (int j = 0; j < nv && j < NV; ++j) {
+                    double v[4];
+                    load4_tail(V + j * ldv + i0, n - i0, v);
+                    acc[j] += v[0] * a[0] + v[1] * a[1] + v[2] * a[2] + v[3] * a[3];
+                }
+            }
         }
+        if (mode != 0) acc[0] += a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3];
     }
     block_multi_sum<NV>(acc, mode == 0 ? nv : 1, partial, pstride);
 }
@@ -494,13 +553,14 @@ __global__ void k_finalize(const double* __restrict__ partial, int nb, int nv, i
 }
 
 // w -= sum_j coef[j] V_j (j < nv); coef on the device
-__global__ void k_maxpy(long n, int nv, const double* __restrict__ V, long ldv, const double* __restrict__ coef,
+template <typename VT = double>
+__global__ void k_maxpy(long n, int nv, const VT* __restrict__ V, long ldv, const double* __restrict__ coef,
                         double* __restrict__ w, double sign, const int* __restrict__ active) {
     if (active && !*active) return;
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double a = w[i];
-    for (int j = 0; j < nv; ++j) a -= sign * coef[j] * V[j * ldv + i];
+    for (int j = 0; j < nv; ++j) a -= sign * coef[j] * tod(V[j * ldv + i]);
     w[i] = a;
 }
 
@@ -509,6 +569,15 @@ __global__ void k_scale_inv(long n, double* __restrict__ x, const double* __rest
     if (active && !*active) return;
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] = x[i] / *s;
+}
+
+// v = w / *s stored as a (FP32) basis vector
+template <typename VT>
+__global__ void k_scale_store(long n, const double* __restrict__ w, VT* __restrict__ v, const double* __restrict__ s,
+                              const int* __restrict__ active) {
+    if (active && !*active) return;
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (VT)(w[i] / *s);
 }
 
 // per-component sum |r_c| and the foam normFactor pieces

@@ -17,6 +17,7 @@
 #include <numeric>
 #include <string>
 #include <unordered_map>
+#include <type_traits>
 #include <vector>
 
 #define RDST_API extern "C" __attribute__((visibility("default")))
@@ -135,6 +136,8 @@ struct rdst_ctx {
     Bounds bd{};
     // numbering
     std::vector<int> perm, iperm;       // perm[internal] = original
+    DBuf<int> perm_d;                   // perm on the device
+    DBuf<double> stage;                 // conservative fields in the caller's order (5N)
     std::vector<int> bface_orig;        // active bface -> foam face
     std::vector<double> hV, hC;         // original numbering, for forces
     std::vector<int> hpatch_start, hpatch_size;
@@ -170,6 +173,9 @@ struct rdst_ctx {
     int ilu_ml = 0, ilu_mu = 0;
     // Krylov
     DBuf<double> dx, r, t, Vb, s2, sh, ph, pv, xbar, Ax, pA;
+    DBuf<float> Vf;                 // GMRES basis when it is kept in FP32
+    long ldv = 0;                   // stride between basis vectors (entries)
+    DBuf<double> wv;                // FP64 Arnoldi vector that is orthogonalised before it is stored in Vf
     int limiter_need_grad = 1, venkat_mask = 0;
     bool steady = false;
     bool state_set = false;
@@ -216,6 +222,15 @@ struct rdst_ctx {
             ev_pool.push_back(r.b);
         }
         ev_pending.clear();
+    }
+
+    // drop the captured step graphs (recaptured by the next step)
+    void reset_graphs() {
+        for (Graph* g : {&g_step, &g_pre, &g_cycle, &g_post}) {
+            if (g->exec) cudaGraphExecDestroy(g->exec);
+            for (auto& r : g->events) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+            *g = Graph{};
+        }
     }
 
     ~rdst_ctx() {
@@ -290,6 +305,30 @@ struct CounterScope {
 int flux_code(FluxScheme f) { return (int)f; }
 int lim_code(Limiter l) { return (int)l; }
 
+// Default number of ILU(0) subdomains: about 1536 rows each.  The apply
+// runs one CTA per subdomain and its time is set by the level-to-level
+// chain of each CTA, so once there are more subdomains than CTAs the GPU
+// holds at once the count is rounded to a whole number of such waves (a
+// partial last wave costs a whole extra chain: measured on the 1.2 M-cell
+// wing, 784 parts took 23% longer than 592 or 1184).
+int auto_ilu_parts(int N, Precision prec) {
+    const int p0 = std::max(1, N / 1536);
+    int dev = 0, sms = 0, per_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // the four-slot instance bounds the register use of the ones hex meshes need
+    if (prec == PREC_FP64)
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu_apply<double, 4>, ILU_APPLY_TPB, 0));
+    else if (prec == PREC_FP32)
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu_apply<float, 4>, ILU_APPLY_TPB, 0));
+    else
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu_apply<__nv_bfloat16, 4>, ILU_APPLY_TPB, 0));
+    const long wave = std::max(1L, (long)sms * per_sm);
+    if (p0 <= wave) return std::min(p0, N);
+    const long waves = std::max(1L, std::lround((double)p0 / (double)wave));
+    return (int)std::min<long>(waves * wave, N);
+}
+
 // ---------------------------------------------------------------- set-up
 void build(rdst_ctx& c, const rdst_mesh* mh) {
     cudaStream_t s = c.s;
@@ -338,7 +377,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     std::vector<int> part(N, 0), level(N, 0);
     int nparts = 1;
     if (o.precon == PRECON_ILU0) {
-        nparts = o.ilu_parts > 0 ? o.ilu_parts : std::max(1, N / 1536);
+        nparts = o.ilu_parts > 0 ? o.ilu_parts : auto_ilu_parts(N, o.precision);
         nparts = std::min(nparts, N);
         std::vector<int> idx(N);
         std::iota(idx.begin(), idx.end(), 0);
@@ -565,6 +604,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     m.cf_start = c.cf_start.p; m.cf_list = c.cf_list.p; m.cc_start = c.cc_start.p; m.cc_list = c.cc_list.p;
     m.patches = c.patches.p;
     // ---- fields
+    c.perm_d.upload(c.perm, s); c.stage.alloc(5L * N);
     c.W.alloc(5L * N); c.prim.alloc((size_t)PW * N); c.bs.alloc((size_t)BW * std::max(NB, 1));
     c.q.alloc((size_t)QW * N); c.qb.alloc((size_t)QW * std::max(NB, 1)); c.g.alloc((size_t)GW * N);
     c.psi.alloc((size_t)QW * N); c.fcell.alloc(N); c.fl.alloc(5L * std::max(Fi, 1)); c.bfl.alloc(5L * std::max(NB, 1));
@@ -611,7 +651,10 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     // ---- Krylov
     const long n5 = 5L * N;
     c.dx.alloc(n5); c.r.alloc(n5); c.t.alloc(n5); c.Ax.alloc(n5); c.pA.alloc(n5); c.xbar.alloc(8);
-    if (o.solver == SOLVER_GMRES) c.Vb.alloc((size_t)(o.n_directions + 1) * n5);
+    // basis vectors 64-entry aligned (the orthogonalisation reads 4 entries per 16-byte load)
+    c.ldv = (n5 + 63) / 64 * 64;
+    if (o.solver == SOLVER_GMRES && o.basis32) { c.Vf.alloc((size_t)(o.n_directions + 1) * c.ldv); c.wv.alloc(n5); }
+    else if (o.solver == SOLVER_GMRES) c.Vb.alloc((size_t)(o.n_directions + 1) * c.ldv);
     else { c.s2.alloc(n5); c.sh.alloc(n5); c.ph.alloc(n5); c.pv.alloc(n5); c.Vb.alloc(2 * n5); }
     // limiter needs
     auto vk = [](Limiter l) { return l == LIM_VENKATAKRISHNAN; };
@@ -703,9 +746,10 @@ struct Ops {
             k_copy_identity<MT><<<nblk(c.nvec(), TPB), TPB, 0, c.s>>>((int)c.nvec(), in, out, active);
         CKL();
     }
-    static void spmv(rdst_ctx& c, const double* x, double* y, const double* b, const int* active) {
+    template <typename XT>
+    static void spmv(rdst_ctx& c, const XT* x, double* y, const double* b, const int* active) {
         Timed tm(c, KS_SPMV);
-        k_spmv<MT><<<nblk(c.N, 256), 256, 0, c.s>>>(c.mat<MT>(c.Aval), x, y, b, active);
+        k_spmv<MT, XT><<<nblk(c.N, 256), 256, 0, c.s>>>(c.mat<MT>(c.Aval), x, y, b, active);
         CKL();
     }
     // normFactor + initial residual (dx = 0 -> r = rhs)
@@ -740,74 +784,77 @@ struct Ops {
         k_multidot<<<nb, RED_TPB, 0, c.s>>>(n, 1, a, 0, b, c.partial.p, 8, active); CKL();
         k_finalize<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, 1, 8, out, sq, active); CKL();
     }
-    // V^T w for j <= i (chunks of 8), into out[0..i]
-    static void multidot(rdst_ctx& c, int nv, const double* w, double* out, const int* active) {
-        long n = c.nvec();
-        int nb = red_blocks(n);
-        for (int j0 = 0; j0 < nv; j0 += 8) {
-            int cnt = std::min(8, nv - j0);
-            k_multidot<<<nb, RED_TPB, 0, c.s>>>(n, cnt, c.Vb.p + j0 * n, n, w, c.partial.p, 8, active); CKL();
-            k_finalize<<<cnt, RED_TPB, 0, c.s>>>(c.partial.p, nb, cnt, 8, out + j0, 0, active); CKL();
-        }
-    }
     // V^T w (one pass over w) into out[0..nv)
-    template <int NV>
-    static void vmultidot(rdst_ctx& c, int nv, const double* w, double* out, const int* active) {
+    template <int NV, typename VT>
+    static void vmultidot(rdst_ctx& c, const VT* V, int nv, const double* w, double* out, const int* active) {
         long n = c.nvec();
         int nb = red_blocks(n);
-        k_vmultidot<NV><<<nb, RED_TPB, 0, c.s>>>(n, nv, c.Vb.p, n, w, c.partial.p, 64, active); CKL();
+        k_vmultidot<NV, VT><<<nb, RED_TPB, 0, c.s>>>(n, nv, V, c.ldv, w, c.partial.p, 64, active); CKL();
         k_finalize<<<nv, RED_TPB, 0, c.s>>>(c.partial.p, nb, nv, 64, out, 0, active); CKL();
     }
     // w -= V coef, fused with the next dots (mode 0) or the norm (mode 1)
-    template <int NV>
-    static void maxpy_dot(rdst_ctx& c, int nv, const double* coef, double* w, double* out, int mode,
+    template <int NV, typename VT>
+    static void maxpy_dot(rdst_ctx& c, const VT* V, int nv, const double* coef, double* w, double* out, int mode,
                           const int* active) {
         long n = c.nvec();
         int nb = red_blocks(n);
-        k_maxpy_dot<NV><<<nb, RED_TPB, 0, c.s>>>(n, nv, c.Vb.p, n, coef, w, c.partial.p, 64, mode, active); CKL();
+        k_maxpy_dot<NV, VT><<<nb, RED_TPB, 0, c.s>>>(n, nv, V, c.ldv, coef, w, c.partial.p, 64, mode, active); CKL();
         if (mode == 0) { k_finalize<<<nv, RED_TPB, 0, c.s>>>(c.partial.p, nb, nv, 64, out, 0, active); CKL(); }
         else { k_finalize<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, 1, 64, out, 1, active); CKL(); }
     }
     // CGS2 orthogonalisation of w against V_0..V_i: H[:,i] pieces, beta = |w|
-    template <int NV>
-    static void orth(rdst_ctx& c, int nv, double* w, const int* act) {
+    template <int NV, typename VT>
+    static void orth(rdst_ctx& c, const VT* V, int nv, double* w, const int* act) {
         Scalars* sc = c.sc.p;
-        vmultidot<NV>(c, nv, w, sc->hcol[0], act);
-        maxpy_dot<NV>(c, nv, sc->hcol[0], w, sc->hcol[1], 0, act);
-        maxpy_dot<NV>(c, nv, sc->hcol[1], w, &sc->beta, 1, act);
+        vmultidot<NV, VT>(c, V, nv, w, sc->hcol[0], act);
+        maxpy_dot<NV, VT>(c, V, nv, sc->hcol[0], w, sc->hcol[1], 0, act);
+        maxpy_dot<NV, VT>(c, V, nv, sc->hcol[1], w, &sc->beta, 1, act);
     }
-    // one restart cycle of left-preconditioned GMRES(m) with CGS2
-    static void gmres_cycle(rdst_ctx& c) {
+    // One restart cycle of left-preconditioned GMRES(m) with CGS2.  With an
+    // FP64 basis each Arnoldi vector is built in place in its basis slot;
+    // with an FP32 basis it is built and orthogonalised in the FP64 vector
+    // wv (dots, Hessenberg and Givens stay FP64) and stored normalised.
+    template <typename VT>
+    static void gmres_cycle_t(rdst_ctx& c, VT* Vb) {
+        constexpr bool in_place = std::is_same<VT, double>::value;
         cudaStream_t s = c.s;
         const long n = c.nvec();
         const int m = c.o.n_directions;
         Scalars* sc = c.sc.p;
         int* act = &sc->gm_active;
-        double* V0 = c.Vb.p;
+        double* w0 = in_place ? (double*)Vb : c.wv.p;
         spmv(c, c.dx.p, c.r.p, c.rhs.p, nullptr);            // r = rhs - A dx
-        precond(c, c.r.p, V0, nullptr);                      // w = M^-1 r
-        dot(c, V0, V0, &sc->beta, 1, nullptr);
+        precond(c, c.r.p, w0, nullptr);                      // w = M^-1 r
+        dot(c, w0, w0, &sc->beta, 1, nullptr);
         k_gm_start<<<1, 1, 0, s>>>(sc); CKL();
-        k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, V0, &sc->beta, act); CKL();
+        if (in_place) { k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, w0, &sc->beta, act); CKL(); }
+        else { k_scale_store<VT><<<nblk(n, TPB), TPB, 0, s>>>(n, w0, Vb, &sc->beta, act); CKL(); }
         for (int i = 0; i < m; ++i) {
-            double* Vi = c.Vb.p + i * n;
-            double* w = c.Vb.p + (i + 1) * n;
+            const VT* Vi = Vb + i * c.ldv;
+            double* w = in_place ? (double*)(Vb + (i + 1) * c.ldv) : c.wv.p;
             spmv(c, Vi, c.t.p, nullptr, act);
             precond(c, c.t.p, w, act);
             {
                 Timed tm(c, KS_ORTH);
                 const int nv = i + 1;
-                if (nv <= 8) orth<8>(c, nv, w, act);
-                else if (nv <= 16) orth<16>(c, nv, w, act);
-                else if (nv <= 32) orth<32>(c, nv, w, act);
-                else orth<64>(c, nv, w, act);
+                if (nv <= 8) orth<8, VT>(c, Vb, nv, w, act);
+                else if (nv <= 16) orth<16, VT>(c, Vb, nv, w, act);
+                else if (nv <= 32) orth<32, VT>(c, Vb, nv, w, act);
+                else orth<64, VT>(c, Vb, nv, w, act);
             }
             k_gm_givens<<<1, 1, 0, s>>>(sc, i, m); CKL();
-            if (i < m - 1) { k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, w, &sc->beta, act); CKL(); }
+            if (i < m - 1) {
+                if (in_place) { k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, w, &sc->beta, act); CKL(); }
+                else { k_scale_store<VT><<<nblk(n, TPB), TPB, 0, s>>>(n, w, Vb + (i + 1) * c.ldv, &sc->beta, act); CKL(); }
+            }
         }
         k_gm_backsub<<<1, 1, 0, s>>>(sc, m); CKL();
-        k_maxpy<<<nblk(n, TPB), TPB, 0, s>>>(n, m, c.Vb.p, n, sc->yh, c.dx.p, -1.0, nullptr); CKL();
+        k_maxpy<VT><<<nblk(n, TPB), TPB, 0, s>>>(n, m, Vb, c.ldv, sc->yh, c.dx.p, -1.0, nullptr); CKL();
         finish_iteration(c);
+    }
+    static void gmres_cycle(rdst_ctx& c) {
+        if (c.o.basis32) gmres_cycle_t<float>(c, c.Vf.p);
+        else gmres_cycle_t<double>(c, c.Vb.p);
     }
     static void finish_iteration(rdst_ctx& c) {
         spmv(c, c.dx.p, c.r.p, c.rhs.p, nullptr);
@@ -1201,21 +1248,16 @@ RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const doub
 RDST_API rdst_status rdst_set_conservative(rdst_ctx* c, const double* rho, const double* rhoU, const double* rhoE) {
     if (!c || !rho || !rhoU || !rhoE) return RDST_ERR_ARG;
     return guarded(c, [&] {
-        std::vector<double> W(5L * c->N), prim((size_t)PW * c->N, 0.0);
-        const double Cv = c->o.Cv(), R = c->o.R, Cp = c->o.Cp;
-        for (int r = 0; r < c->N; ++r) {
-            int i = c->perm[r];
-            W[5 * r] = rho[i];
-            for (int k = 0; k < 3; ++k) W[5 * r + 1 + k] = rhoU[3 * i + k];
-            W[5 * r + 4] = rhoE[i];
-            double Ux = rhoU[3 * i] / rho[i], Uy = rhoU[3 * i + 1] / rho[i], Uz = rhoU[3 * i + 2] / rho[i];
-            double e = rhoE[i] / rho[i] - 0.5 * (Ux * Ux + Uy * Uy + Uz * Uz);
-            double T = e / Cv;
-            double* P = &prim[(size_t)PW * r];
-            P[0] = rho[i] * R * T; P[1] = T; P[2] = Cp * T; P[3] = Ux; P[4] = Uy; P[5] = Uz;
-        }
-        CK(cudaMemcpyAsync(c->W.p, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
-        CK(cudaMemcpyAsync(c->prim.p, prim.data(), prim.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
+        const int N = c->N;
+        double* d_rho = c->stage.p;
+        double* d_rhoU = d_rho + N;
+        double* d_rhoE = d_rhoU + 3L * N;
+        CK(cudaMemcpyAsync(d_rho, rho, sizeof(double) * N, cudaMemcpyHostToDevice, c->s));
+        CK(cudaMemcpyAsync(d_rhoU, rhoU, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c->s));
+        CK(cudaMemcpyAsync(d_rhoE, rhoE, sizeof(double) * N, cudaMemcpyHostToDevice, c->s));
+        k_set_conservative<<<nblk(N, TPB), TPB, 0, c->s>>>(N, c->th, c->perm_d.p, d_rho, d_rhoU, d_rhoE, c->W.p,
+                                                           c->prim.p);
+        CKL();
         if (c->state_set) {
             // fields replaced between steps: boundary values from the new
             // internal field, time-control history kept
@@ -1232,15 +1274,16 @@ RDST_API rdst_status rdst_set_conservative(rdst_ctx* c, const double* rho, const
 RDST_API rdst_status rdst_get_conservative(rdst_ctx* c, double* rho, double* rhoU, double* rhoE) {
     if (!c) return RDST_ERR_ARG;
     return guarded(c, [&] {
-        std::vector<double> W(5L * c->N);
-        CK(cudaMemcpyAsync(W.data(), c->W.p, W.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        const int N = c->N;
+        double* d_rho = c->stage.p;
+        double* d_rhoU = d_rho + N;
+        double* d_rhoE = d_rhoU + 3L * N;
+        k_get_conservative<<<nblk(N, TPB), TPB, 0, c->s>>>(N, c->perm_d.p, c->W.p, d_rho, d_rhoU, d_rhoE);
+        CKL();
+        if (rho) CK(cudaMemcpyAsync(rho, d_rho, sizeof(double) * N, cudaMemcpyDeviceToHost, c->s));
+        if (rhoU) CK(cudaMemcpyAsync(rhoU, d_rhoU, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c->s));
+        if (rhoE) CK(cudaMemcpyAsync(rhoE, d_rhoE, sizeof(double) * N, cudaMemcpyDeviceToHost, c->s));
         CK(cudaStreamSynchronize(c->s));
-        for (int r = 0; r < c->N; ++r) {
-            int i = c->perm[r];
-            if (rho) rho[i] = W[5 * r];
-            if (rhoU) for (int k = 0; k < 3; ++k) rhoU[3 * i + k] = W[5 * r + 1 + k];
-            if (rhoE) rhoE[i] = W[5 * r + 4];
-        }
     });
 }
 
@@ -1402,6 +1445,22 @@ RDST_API rdst_status rdst_kernel_stats(rdst_ctx* c, const char* kernel, int64_t*
         }
     c->err = std::string("unknown kernel class ") + kernel;
     return RDST_ERR_ARG;
+}
+
+RDST_API rdst_status rdst_set_profile(rdst_ctx* c, int32_t on) {
+    if (!c) return RDST_ERR_ARG;
+    try {
+        CK(cudaStreamSynchronize(c->s));
+        c->collect_events();
+        if (c->o.profile != (on != 0)) {
+            c->o.profile = on != 0;
+            c->reset_graphs();
+        }
+        return RDST_OK;
+    } catch (const std::exception& e) {
+        c->err = e.what();
+        return RDST_ERR_CUDA;
+    }
 }
 
 RDST_API void rdst_destroy(rdst_ctx* c) { delete c; }

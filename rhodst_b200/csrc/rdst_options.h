@@ -74,6 +74,7 @@ struct Options {
     double start_time = 0.0;
     // B200 additions
     Precision precision = PREC_FP64;
+    int basis32 = -1;                 // GMRES basis vectors in FP32 (-1: when precision is not fp64)
     int ilu_parts = 0;                // 0: choose from the mesh size; 1: exact global ILU(0)
     bool graphs = true;               // capture steps in CUDA graphs
     bool profile = false;             // event-time kernel classes inside steps
@@ -251,12 +252,18 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             else if (t == "bf16") o.precision = PREC_BF16;
             else throw ConfigError("precision must be fp64, fp32 or bf16");
         }
+        else if (k == "krylov.basis") {
+            if (t == "fp64") o.basis32 = 0;
+            else if (t == "fp32") o.basis32 = 1;
+            else throw ConfigError("krylov.basis must be fp64 or fp32");
+        }
         else if (k == "ilu.parts") o.ilu_parts = parse_int(k, v);
         else if (k == "graphs") o.graphs = parse_bool(k, v);
         else if (k == "profile") o.profile = parse_bool(k, v);
         else throw ConfigError("unknown option '" + k + "'");
     }
     if (!o.flux_given) throw ConfigError("keyword fluxScheme is undefined in dictionary rhoDSTDict");
+    if (o.basis32 < 0) o.basis32 = o.precision == PREC_FP64 ? 0 : 1;
     if (o.n_directions < 1 || o.n_directions > 64) throw ConfigError("solvers.W.nDirections must be in [1,64]");
     if (o.max_iter < 0 || o.min_iter < 0) throw ConfigError("solvers.W.maxIter/minIter must be >= 0");
     if (!(o.R > 0) || !(o.Cp > o.R)) throw ConfigError("thermo: need 0 < R < Cp");
