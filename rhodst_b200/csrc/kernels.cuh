@@ -639,13 +639,18 @@ __global__ void k_residual(DevMesh m, const double* __restrict__ fl, const doubl
     }
 }
 
+// one block: each thread sums a fixed stride of the partials, then a
+// fixed-order block reduction (deterministic)
 __global__ void k_residual_finalize(const double* __restrict__ partial, int nb, Scalars* sc) {
-    int c = threadIdx.x;
-    if (c >= 6) return;
-    double s = 0;
-    for (int b = 0; b < nb; ++b) s += partial[b * 6 + c];
-    if (c == 0) sc->res_mag = sqrt(s);
-    else sc->res_l2[c - 1] = sqrt(s);
+    for (int c = 0; c < 6; ++c) {
+        double s = 0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[b * 6 + c];
+        s = block_sum(s);
+        if (threadIdx.x == 0) {
+            if (c == 0) sc->res_mag = sqrt(s);
+            else sc->res_l2[c - 1] = sqrt(s);
+        }
+    }
 }
 
 // ------------------------------------------------------------------ assembly
@@ -878,10 +883,10 @@ __global__ void k_dt_transient(DevMesh m, Thermo th, int neighbouring, const dou
 }
 
 __global__ void k_dt_finalize(const double* partial, int nb, Scalars* sc) {
-    if (threadIdx.x != 0) return;
     double v = 1e300;
-    for (int b = 0; b < nb; ++b) v = fmin(v, partial[b]);
-    sc->deltaT = v;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) v = fmin(v, partial[b]);
+    v = block_min(v);
+    if (threadIdx.x == 0) sc->deltaT = v;
 }
 
 // setSteadyStateDeltaT (timeDST.C:218-273): local 1/dtau per cell
@@ -929,11 +934,11 @@ __global__ void k_dt_steady(DevMesh m, Thermo th, int neighbouring, const double
 }
 
 __global__ void k_rdt_finalize(const double* partial, int nb, Scalars* sc) {
-    if (threadIdx.x != 0) return;
     double lo = 1e300, hi = -1e300;
-    for (int b = 0; b < nb; ++b) { lo = fmin(lo, partial[2 * b]); hi = fmax(hi, partial[2 * b + 1]); }
-    sc->rdt_min = lo;
-    sc->rdt_max = hi;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) { lo = fmin(lo, partial[2 * b]); hi = fmax(hi, partial[2 * b + 1]); }
+    lo = block_min(lo);
+    hi = block_max(hi);
+    if (threadIdx.x == 0) { sc->rdt_min = lo; sc->rdt_max = hi; }
 }
 
 // setCourantDST (timeDST.C:316-443) scalar part: residual-ratio CFL ramp

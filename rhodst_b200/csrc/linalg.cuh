@@ -635,22 +635,26 @@ __global__ void k_nf_finalize(const double* __restrict__ partial, int nb, Scalar
 }
 
 __global__ void k_mean5_finalize(const double* __restrict__ partial, int nb, int N, double* __restrict__ xbar) {
-    int c = threadIdx.x;
-    if (c >= 5) return;
-    double s = 0;
-    for (int b = 0; b < nb; ++b) s += partial[b * 5 + c];
-    xbar[c] = s / N;
+    for (int c = 0; c < 5; ++c) {
+        double s = 0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[b * 5 + c];
+        s = block_sum(s);
+        if (threadIdx.x == 0) xbar[c] = s / N;
+    }
 }
 
 // linear residual per component / normFactor -> initial or final
 __global__ void k_linres_finalize(const double* __restrict__ partial, int nb, Scalars* sc, int initial) {
-    int c = threadIdx.x;
-    if (c >= 5) return;
-    double s = 0;
-    for (int b = 0; b < nb; ++b) s += partial[b * 5 + c];
-    double v = s / sc->nf;
-    if (initial) { sc->lin_initial[c] = v; sc->lin_final[c] = v; }
-    else sc->lin_final[c] = v;
+    for (int c = 0; c < 5; ++c) {
+        double s = 0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[b * 5 + c];
+        s = block_sum(s);
+        if (threadIdx.x == 0) {
+            const double v = s / sc->nf;
+            if (initial) { sc->lin_initial[c] = v; sc->lin_final[c] = v; }
+            else sc->lin_final[c] = v;
+        }
+    }
 }
 
 // BlockSolverPerformance check: converged if every component below the

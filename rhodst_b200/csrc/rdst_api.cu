@@ -115,9 +115,17 @@ __global__ void k_report_dt(const Scalars* sc, rdst_step_report* reps, int cap) 
     if (threadIdx.x == 0 && sc->step_idx < cap) reps[sc->step_idx].deltaT = sc->deltaT;
 }
 
-__global__ void k_mean_courant(const double* __restrict__ cf, int N, const Scalars* sc, rdst_step_report* reps, int cap) {
+// mean of the per-cell Courant numbers: block partials, then one block
+__global__ void k_mean_courant_partial(const double* __restrict__ cf, int N, double* __restrict__ partial) {
     double s = 0;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) s += cf[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) s += cf[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+__global__ void k_mean_courant(const double* __restrict__ partial, int nb, int N, const Scalars* sc,
+                               rdst_step_report* reps, int cap) {
+    double s = 0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[b];
     s = block_sum(s);
     if (threadIdx.x == 0 && sc->step_idx < cap) reps[sc->step_idx].courant = s / N;
 }
@@ -703,7 +711,7 @@ struct Ops {
         k_residual<<<nb, TPB, 0, s>>>(m, c.fl.p, c.bfl.p, visc ? c.vf.p : nullptr, visc ? c.bvf.p : nullptr, c.R.p,
                                       c.rhs.p, c.partial.p);
         CKL();
-        k_residual_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, c.sc.p);
+        k_residual_finalize<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, c.sc.p);
         CKL();
     }
     static void assemble(rdst_ctx& c) {
@@ -760,13 +768,13 @@ struct Ops {
         if (c.o.dependent_W) {
             spmv(c, c.W.p, c.Ax.p, nullptr, nullptr);
             k_sum5<<<nb, RED_TPB, 0, s>>>(N, c.W.p, c.partial.p); CKL();
-            k_mean5_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, N, c.xbar.p); CKL();
+            k_mean5_finalize<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, N, c.xbar.p); CKL();
             k_spmv_const<MT><<<nblk(N, 256), 256, 0, s>>>(c.mat<MT>(c.Aval), c.xbar.p, c.pA.p); CKL();
         }
         k_normfactor<<<nb, RED_TPB, 0, s>>>(N, c.Ax.p, c.rhs.p, c.pA.p, c.o.dependent_W ? 1 : 0, c.partial.p); CKL();
         k_nf_finalize<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, c.sc.p); CKL();
         k_abs5<<<nb, RED_TPB, 0, s>>>(N, c.rhs.p, c.partial.p); CKL();
-        k_linres_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, c.sc.p, 1); CKL();
+        k_linres_finalize<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, c.sc.p, 1); CKL();
         CK(cudaMemsetAsync(c.dx.p, 0, sizeof(double) * c.nvec(), s));
         CK(cudaMemsetAsync(&c.sc.p->lin_iterations, 0, sizeof(int), s));
         k_check<<<1, 1, 0, s>>>(c.sc.p, c.o.tolerance, c.o.rel_tol, c.o.min_iter, c.o.max_iter, 0); CKL();
@@ -860,7 +868,7 @@ struct Ops {
         spmv(c, c.dx.p, c.r.p, c.rhs.p, nullptr);
         int nb = red_blocks(c.N);
         k_abs5<<<nb, RED_TPB, 0, c.s>>>(c.N, c.r.p, c.partial.p); CKL();
-        k_linres_finalize<<<1, 32, 0, c.s>>>(c.partial.p, nb, c.sc.p, 0); CKL();
+        k_linres_finalize<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, c.sc.p, 0); CKL();
         k_check<<<1, 1, 0, c.s>>>(c.sc.p, c.o.tolerance, c.o.rel_tol, c.o.min_iter, c.o.max_iter, 1); CKL();
     }
     // one BiCGStab iteration (van der Vorst, right preconditioned)
@@ -886,7 +894,7 @@ struct Ops {
         k_bi_update<<<nblk(n, TPB), TPB, 0, s>>>(n, c.dx.p, c.r.p, c.ph.p, c.sh.p, c.s2.p, t2, sc); CKL();
         int nb = red_blocks(c.N);
         k_abs5<<<nb, RED_TPB, 0, s>>>(c.N, c.r.p, c.partial.p); CKL();
-        k_linres_finalize<<<1, 32, 0, s>>>(c.partial.p, nb, sc, 0); CKL();
+        k_linres_finalize<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, sc, 0); CKL();
         k_check<<<1, 1, 0, s>>>(sc, c.o.tolerance, c.o.rel_tol, c.o.min_iter, c.o.max_iter, 1); CKL();
     }
     static void iteration(rdst_ctx& c) {
@@ -899,7 +907,7 @@ void set_steady_dt(rdst_ctx& c) {
     int nb = nblk(c.N, TPB);
     k_dt_steady<<<nb, TPB, 0, c.s>>>(c.m, c.th, c.o.neighbouring, c.prim.p, c.dS.p, c.courantF.p, c.rdt.p, c.partial.p);
     CKL();
-    k_rdt_finalize<<<1, 32, 0, c.s>>>(c.partial.p, nb, c.sc.p);
+    k_rdt_finalize<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, c.sc.p);
     CKL();
 }
 
@@ -908,7 +916,7 @@ void set_transient_dt(rdst_ctx& c) {
     int nb = nblk(n, TPB);
     k_dt_transient<<<nb, TPB, 0, c.s>>>(c.m, c.th, c.o.neighbouring, c.prim.p, c.dS.p, c.sc.p, c.partial.p);
     CKL();
-    k_dt_finalize<<<1, 32, 0, c.s>>>(c.partial.p, nb, c.sc.p);
+    k_dt_finalize<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, c.sc.p);
     CKL();
 }
 
@@ -1028,7 +1036,11 @@ void step_head(rdst_ctx& c) {
 
 void step_tail(rdst_ctx& c) {
     post_update(c);
-    if (c.steady) { k_mean_courant<<<1, 256, 0, c.s>>>(c.courantF.p, c.N, c.sc.p, c.reps.p, rdst_ctx::REP_CAP); CKL(); }
+    if (c.steady) {
+        const int nb = red_blocks(c.N);
+        k_mean_courant_partial<<<nb, RED_TPB, 0, c.s>>>(c.courantF.p, c.N, c.partial.p); CKL();
+        k_mean_courant<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, c.N, c.sc.p, c.reps.p, rdst_ctx::REP_CAP); CKL();
+    }
     k_report<<<1, 1, 0, c.s>>>(c.sc.p, c.reps.p, rdst_ctx::REP_CAP);
     CKL();
 }
