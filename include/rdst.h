@@ -182,6 +182,58 @@ rdst_status rdst_forces(rdst_ctx* ctx, int32_t patch, const double lift_dir[3],
 /* Message of the last failing call on this context ("" if none).  With
  * ctx == NULL: the message of the calling thread's last failing
  * context-free call (rdst_residual_norms_noalloc). */
+
+/* ---- discrete adjoint of the steady residual (inviscid) ----
+ * No counterpart in the reference: rhoDST has no adjoint.  R(W) is the
+ * per-unit-volume residual that rdst_residual returns (no pseudo-time
+ * term); it depends on the patch velocity values U_patch (the U_value of
+ * every patch, so far field, inlet and outlet together: the free stream).
+ * In/outflow and sub/supersonic branches of the boundary conditions are
+ * held at the current state's.  Transport and turbulence options are
+ * rejected with RDST_ERR_UNSUPPORTED.
+ *
+ * Objective: the pressure force of one patch along a direction,
+ *   J = scale * sum_{faces b of patch} (p_b - p_ref) S_b . direction
+ * (scale = 1 / (q_ref A_ref) gives a drag or lift coefficient). */
+typedef struct rdst_objective {
+    int32_t patch;
+    double direction[3];
+    double p_ref;
+    double scale;
+} rdst_objective;
+
+typedef struct rdst_adjoint_report {
+    double J;
+    double force[3];       /* scale * sum (p_b - p_ref) S_b = dJ/d(direction) */
+    double dJ_dU[3];       /* total derivative wrt U_patch (all patches together) */
+    double residual0;      /* ||dJ/dW||_2 */
+    double residual;       /* ||dJ/dW - (dR/dW)^T psi||_2 at exit */
+    int32_t iterations;    /* Krylov iterations */
+    int32_t cycles;        /* GMRES restart cycles */
+    double t_ms;           /* device time of the call */
+} rdst_adjoint_report;
+
+/* rdst_objective_gradient: J, the force vector, dJ/dW (N x 5, the state
+ * order of rdst_get_conservative: rho, rhoU xyz, rhoE) and the explicit
+ * dJ/dU_patch at the current state.  Any output may be NULL. */
+rdst_status rdst_objective_gradient(rdst_ctx* ctx, const rdst_objective* obj, double* J, double force[3],
+                                    double* dJdW, double dJdU[3]);
+/* rdst_adjoint_product: u = (dR/dW)^T v (N x 5 each) and
+ * dU = (dR/dU_patch)^T v, matrix-free at the current state. */
+rdst_status rdst_adjoint_product(rdst_ctx* ctx, const double* v, double* u, double dU[3]);
+/* rdst_tangent_product: Ju = (dR/dW) u (N x 5 each), the forward-mode
+ * linearization of the same residual with the same held branches: the
+ * exact counterpart of rdst_adjoint_product (v . Ju = ((dR/dW)^T v) . u). */
+rdst_status rdst_tangent_product(rdst_ctx* ctx, const double* u, double* Ju);
+/* rdst_adjoint: solves (dR/dW)^T psi = dJ/dW by GMRES(n_directions),
+ * right-preconditioned with the transposed step Jacobian (block ILU(0) or
+ * block Jacobi as the solvers.W preconditioner selects), restarted until
+ * the residual falls by rel_tol or after max_cycles cycles; reports J and
+ * dJ/dU_patch = dJ/dU_patch|explicit - psi^T dR/dU_patch.  psi (N x 5)
+ * may be NULL.  Call it at a converged state (R ~ 0). */
+rdst_status rdst_adjoint(rdst_ctx* ctx, const rdst_objective* obj, double rel_tol, int32_t max_cycles,
+                         int32_t n_directions, double* psi, rdst_adjoint_report* report);
+
 const char* rdst_last_error(const rdst_ctx* ctx);
 
 /* Release the context and all its device memory. */

@@ -51,6 +51,15 @@ class RdstMesh(ctypes.Structure):
                 ("patches", POINTER(RdstPatch)), ("wall_distance", POINTER(c_double))]
 
 
+class RdstObjective(ctypes.Structure):
+    _fields_ = [("patch", c_int32), ("direction", c_double * 3), ("p_ref", c_double), ("scale", c_double)]
+
+
+class RdstAdjointReport(ctypes.Structure):
+    _fields_ = [("J", c_double), ("force", c_double * 3), ("dJ_dU", c_double * 3), ("residual0", c_double),
+                ("residual", c_double), ("iterations", c_int32), ("cycles", c_int32), ("t_ms", c_double)]
+
+
 class RdstStepReport(ctypes.Structure):
     _fields_ = [("time", c_double), ("deltaT", c_double), ("courant", c_double),
                 ("res_l2", c_double * 5), ("res_mag", c_double),
@@ -121,6 +130,12 @@ def declare(lib: ctypes.CDLL, prefix: str) -> None:
         f("last_step_ms", c_double, [vp])
         f("kernel_stats", c_int32, [vp, c_char_p, POINTER(ctypes.c_int64), POINTER(c_double)])
         f("set_profile", c_int32, [vp, c_int32])
+    if hasattr(lib, prefix + "adjoint"):
+        f("objective_gradient", c_int32, [vp, POINTER(RdstObjective), dp, dp, dp, dp])
+        f("adjoint_product", c_int32, [vp, dp, dp, dp])
+        f("tangent_product", c_int32, [vp, dp, dp])
+        f("adjoint", c_int32, [vp, POINTER(RdstObjective), c_double, c_int32, c_int32, dp,
+                               POINTER(RdstAdjointReport)])
 
 
 def _dptr(a: Optional[np.ndarray]):
@@ -290,6 +305,54 @@ class Solver:
         d, u, l, s = np.empty((N, 5, 5)), np.empty((Fi, 5, 5)), np.empty((Fi, 5, 5)), np.empty((N, 5))
         self._check(self._fn("assemble")(self._h, _dptr(d), _dptr(u), _dptr(l), _dptr(s)), "assemble")
         return d, u, l, s
+
+    # ---- discrete adjoint
+    def _objective(self, patch: str, direction, p_ref: float, scale: float) -> RdstObjective:
+        ob = RdstObjective()
+        ob.patch = self.mesh.patch_index(patch)
+        for k in range(3):
+            ob.direction[k] = float(direction[k])
+        ob.p_ref = float(p_ref)
+        ob.scale = float(scale)
+        return ob
+
+    def objective_gradient(self, patch: str, direction, p_ref: float = 0.0, scale: float = 1.0):
+        """J = scale * sum over the patch of (p - p_ref) S . direction, its
+        force vector, dJ/dW (N x 5) and the explicit dJ/dU_patch."""
+        ob = self._objective(patch, direction, p_ref, scale)
+        J, force, dU = c_double(), np.empty(3), np.empty(3)
+        dW = np.empty((self.n_cells, 5))
+        self._check(self._fn("objective_gradient")(self._h, ctypes.byref(ob), ctypes.byref(J), _dptr(force),
+                                                   _dptr(dW), _dptr(dU)), "objective_gradient")
+        return float(J.value), force, dW, dU
+
+    def adjoint_product(self, v: np.ndarray):
+        """(dR/dW)^T v (N x 5) and (dR/dU_patch)^T v (3)."""
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(self.n_cells, 5)
+        u, dU = np.empty((self.n_cells, 5)), np.empty(3)
+        self._check(self._fn("adjoint_product")(self._h, _dptr(v), _dptr(u), _dptr(dU)), "adjoint_product")
+        return u, dU
+
+    def tangent_product(self, u: np.ndarray) -> np.ndarray:
+        """(dR/dW) u (N x 5) by forward-mode linearization."""
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.n_cells, 5)
+        Ju = np.empty((self.n_cells, 5))
+        self._check(self._fn("tangent_product")(self._h, _dptr(u), _dptr(Ju)), "tangent_product")
+        return Ju
+
+    def adjoint(self, patch: str, direction, p_ref: float = 0.0, scale: float = 1.0, rel_tol: float = 1e-10,
+                max_cycles: int = 50, n_directions: int = 30, want_psi: bool = False):
+        """Adjoint solve for the pressure-force objective; returns the report
+        as a dict (J, force, dJ_dU, residuals, iterations, t_ms) and psi."""
+        ob = self._objective(patch, direction, p_ref, scale)
+        rep = RdstAdjointReport()
+        psi = np.empty((self.n_cells, 5)) if want_psi else None
+        self._check(self._fn("adjoint")(self._h, ctypes.byref(ob), rel_tol, max_cycles, n_directions,
+                                        _dptr(psi), ctypes.byref(rep)), "adjoint")
+        out = {"J": rep.J, "force": np.array(rep.force[:]), "dJ_dU": np.array(rep.dJ_dU[:]),
+               "residual0": rep.residual0, "residual": rep.residual, "iterations": rep.iterations,
+               "cycles": rep.cycles, "t_ms": rep.t_ms}
+        return out, psi
 
     def forces(self, patch: str, lift_dir, drag_dir, p_ref: float, q_ref_area: float,
                cofr=(0.25, 0.0, 0.0), pitch_axis=(0.0, 0.0, 1.0), l_ref: float = 1.0):

@@ -148,6 +148,95 @@ __global__ void k_init_phib(DevMesh m, const double* __restrict__ W, const doubl
 // of farField*DSTFvPatch*Field.C:144-221) and rho/rhoU/rhoE rebuilt as
 // updateFields.H:84-93.  The valueFractions are stored for the boundary
 // Jacobian (valueInternalCoeffs = 1 - valueFraction).
+// Boundary state of one face from the adjacent cell's rho, p, T, U and the
+// patch values (UInf the patch velocity value): the patch-field updates of
+// fixedValue, zeroGradient, inletOutlet, symmetryPlane/slip and the
+// characteristic far field (farField*DST::updateCoeffs, *.C:144-221).
+// phi_prev (the face's previous mass flux) and mach (the far-field face
+// Mach number from the previous boundary density, temperature and mass
+// flux) only choose branches (in/outflow, sub/supersonic); k_boundary keeps
+// both in the boundary record, so the adjoint differentiates the branches
+// the current states were built with.  Templated so that the adjoint
+// differentiates the same arithmetic.
+template <typename T>
+struct BcOut {
+    T rho, p, Tb;
+    Vec3<T> U;
+    double fp, fU, fT;
+};
+
+__device__ __forceinline__ bool bc_farfield(const DevPatch& P) { return P.bc_p == 5 || P.bc_U == 5 || P.bc_T == 5; }
+
+template <typename T>
+__device__ __forceinline__ BcOut<T> bc_state(const DevPatch& P, const Thermo& th, const Bounds& bd, V3 n, double magS,
+                                             const T& rhoI, const T& pI, const T& TI, const Vec3<T>& Ui,
+                                             const Vec3<T>& UInf, double phi_prev, double mach) {
+    const bool outflow = phi_prev >= 0.0;
+    double supIn = 0, supOut = 0, subIn = 0, subOut = 0;
+    T rho0c0 = T(0.0), cI = T(0.0), pbU = T(0.0);
+    if (bc_farfield(P)) {
+        cI = sqrt(th.gamma * th.R * TI);
+        supIn = dneg0(mach + 1);
+        supOut = dpos0(mach - 1);
+        subIn = dneg(mach) - supIn;
+        subOut = dpos0(mach) - supOut;
+        rho0c0 = rhoI * cI;
+        pbU = 0.5 * (P.p_value + pI - rho0c0 * dot3(n, sub3(UInf, Ui)));
+    }
+    BcOut<T> o;
+    o.fp = 0; o.fU = 0; o.fT = 0;
+    T pb, Tb;
+    Vec3<T> Ub;
+    switch (P.bc_p) {
+        case 0: pb = T(P.p_value); o.fp = 1; break;
+        case 2: o.fp = outflow ? 0.0 : 1.0; pb = outflow ? pI : T(P.p_value); break;
+        case 5: {
+            T pbp = P.p_value - rho0c0 * dot3(n, sub3(UInf, Ui));
+            T ref = supIn * P.p_value + subIn * pbp + subOut * P.p_value;
+            o.fp = 1 - supOut - 0.5 * subIn;
+            pb = o.fp * ref + (1 - o.fp) * pI;
+            break;
+        }
+        default: pb = pI; break;
+    }
+    switch (P.bc_T) {
+        case 0: Tb = T(P.T_value); o.fT = 1; break;
+        case 2: o.fT = outflow ? 0.0 : 1.0; Tb = outflow ? TI : T(P.T_value); break;
+        case 5: {
+            T RI = pI / rhoI / TI;
+            T rhoa = P.p_value / P.T_value / RI;
+            T subsInValue = pbU / (rhoa + (pbU - P.p_value) / sq(cI)) / RI;
+            T sOVF = pbU / (pI + RI * TI * (pbU - pI) / sq(cI));
+            T ref = supIn * P.T_value + subIn * subsInValue;
+            T fT = 1.0 - supOut - sOVF * subOut;
+            o.fT = val(fT);
+            Tb = fT * ref + (1.0 - fT) * TI;
+            break;
+        }
+        default: Tb = TI; break;
+    }
+    switch (P.bc_U) {
+        case 0: Ub = UInf; o.fU = 1; break;
+        case 2: o.fU = outflow ? 0.0 : 1.0; Ub = outflow ? Ui : UInf; break;
+        case 3:
+        case 4: Ub = sub3(Ui, scl3(dot3(n, Ui), n)); break;
+        case 5: {
+            Vec3<T> subsIn = sub3(UInf, scl3((P.p_value - pbU) / rho0c0, n));
+            Vec3<T> subsOut = scl3((pI - pbU) / rho0c0, n);
+            Vec3<T> ref = add3(add3(scl3(supIn, UInf), scl3(subIn, subsIn)), scl3(subOut, subsOut));
+            o.fU = 1 - supOut - subOut;
+            Ub = add3(scl3(o.fU, ref), scl3(1 - o.fU, Ui));
+            break;
+        }
+        default: Ub = Ui; break;
+    }
+    o.p = fmin(fmax(pb, bd.p_min), bd.p_max);
+    o.Tb = Tb;
+    o.U = Ub;
+    o.rho = o.p * (1.0 / (th.R * Tb));
+    return o;
+}
+
 __global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __restrict__ W,
                            const double* __restrict__ prim, double* __restrict__ bs) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,85 +247,29 @@ __global__ void k_boundary(DevMesh m, Thermo th, Bounds bd, const double* __rest
     double magS = m.bmagSf[b];
     V3 n = div3(S, magS);
     const double* Pi = prim + PW * ci;
-    double pI = Pi[0], TI = Pi[1];
-    V3 Ui = mk(Pi[3], Pi[4], Pi[5]);
     double* B = bs + BW * b;
-    bool outflow = B[7] >= 0.0;
-    const V3 UInf = mk(P.U_value[0], P.U_value[1], P.U_value[2]);
-    double supIn = 0, supOut = 0, subIn = 0, subOut = 0, rho0c0 = 0, cI = 0, pbU = 0;
-    if (P.bc_p == 5 || P.bc_U == 5 || P.bc_T == 5) {
-        double cb = sqrt(th.gamma * th.R * B[6]);
-        cI = sqrt(th.gamma * th.R * TI);
-        double mach = B[7] / B[0] / magS / cb;
-        supIn = dneg0(mach + 1);
-        supOut = dpos0(mach - 1);
-        subIn = dneg(mach) - supIn;
-        subOut = dpos0(mach) - supOut;
-        rho0c0 = W[5 * ci] * cI;
-        pbU = 0.5 * (P.p_value + pI - rho0c0 * dot3(n, sub3(UInf, Ui)));
-    }
-    double pb, Tb, fp = 0, fU = 0, fT = 0;
-    V3 Ub;
-    switch (P.bc_p) {
-        case 0: pb = P.p_value; fp = 1; break;
-        case 2: fp = outflow ? 0.0 : 1.0; pb = outflow ? pI : P.p_value; break;
-        case 5: {
-            double pbp = P.p_value - rho0c0 * dot3(n, sub3(UInf, Ui));
-            double ref = supIn * P.p_value + subIn * pbp + subOut * P.p_value;
-            fp = 1 - supOut - 0.5 * subIn;
-            pb = fp * ref + (1 - fp) * pI;
-            break;
-        }
-        default: pb = pI; break;
-    }
-    switch (P.bc_T) {
-        case 0: Tb = P.T_value; fT = 1; break;
-        case 2: fT = outflow ? 0.0 : 1.0; Tb = outflow ? TI : P.T_value; break;
-        case 5: {
-            double rhoI = W[5 * ci];
-            double RI = pI / rhoI / TI;
-            double rhoa = P.p_value / P.T_value / RI;
-            double subsInValue = pbU / (rhoa + (pbU - P.p_value) / sq(cI)) / RI;
-            double sOVF = pbU / (pI + RI * TI * (pbU - pI) / sq(cI));
-            double ref = supIn * P.T_value + subIn * subsInValue;
-            fT = 1 - supOut - sOVF * subOut;
-            Tb = fT * ref + (1 - fT) * TI;
-            break;
-        }
-        default: Tb = TI; break;
-    }
-    switch (P.bc_U) {
-        case 0: Ub = UInf; fU = 1; break;
-        case 2: fU = outflow ? 0.0 : 1.0; Ub = outflow ? Ui : UInf; break;
-        case 3:
-        case 4: Ub = sub3(Ui, scl3(dot3(n, Ui), n)); break;
-        case 5: {
-            V3 subsIn = sub3(UInf, scl3((P.p_value - pbU) / rho0c0, n));
-            V3 subsOut = scl3((pI - pbU) / rho0c0, n);
-            V3 ref = add3(add3(scl3(supIn, UInf), scl3(subIn, subsIn)), scl3(subOut, subsOut));
-            fU = 1 - supOut - subOut;
-            Ub = add3(scl3(fU, ref), scl3(1 - fU, Ui));
-            break;
-        }
-        default: Ub = Ui; break;
-    }
-    pb = fmin(fmax(pb, bd.p_min), bd.p_max);
-    double hb = th.Cp * Tb;
-    double psib = 1.0 / (th.R * Tb);
-    double rhob = pb * psib;
+    // branch inputs from the previous record (kept: B[11] mass flux, B[15] Mach)
+    const double phi_prev = B[7];
+    const double mach = bc_farfield(P) ? B[7] / B[0] / magS / sqrt(th.gamma * th.R * B[6]) : 0.0;
+    const BcOut<double> o = bc_state<double>(P, th, bd, n, magS, W[5 * ci], Pi[0], Pi[1], mk(Pi[3], Pi[4], Pi[5]),
+                                             mk(P.U_value[0], P.U_value[1], P.U_value[2]), phi_prev, mach);
+    B[11] = phi_prev;
+    B[15] = mach;
+    const double hb = th.Cp * o.Tb;
+    const double rhob = o.rho;
     B[0] = rhob;
-    B[1] = rhob * Ub.x;
-    B[2] = rhob * Ub.y;
-    B[3] = rhob * Ub.z;
-    B[4] = rhob * (hb + 0.5 * magSqr3(Ub)) - pb;
-    B[5] = pb;
-    B[6] = Tb;
-    B[8] = fp;
-    B[9] = fU;
-    B[10] = fT;
-    B[12] = Ub.x;
-    B[13] = Ub.y;
-    B[14] = Ub.z;
+    B[1] = rhob * o.U.x;
+    B[2] = rhob * o.U.y;
+    B[3] = rhob * o.U.z;
+    B[4] = rhob * (hb + 0.5 * magSqr3(o.U)) - o.p;
+    B[5] = o.p;
+    B[6] = o.Tb;
+    B[8] = o.fp;
+    B[9] = o.fU;
+    B[10] = o.fT;
+    B[12] = o.U.x;
+    B[13] = o.U.y;
+    B[14] = o.U.z;
 }
 
 // ------------------------------------------------------------------ residual
@@ -408,21 +441,16 @@ __device__ __forceinline__ void recon_scalar(int L, double xP, double xN, V3 gP,
     xn = wn * xP + (1 - wn) * xN;
 }
 
-// Face fluxes of all internal faces (reconstruction + scheme), AoS output.
-__global__ void __launch_bounds__(128) k_face_flux(DevMesh m, Thermo th, int scheme, int lr, int lu, int lt,
-                                                   int lowMach, double Mainf, const double* __restrict__ q,
-                                                   const double* __restrict__ g, const double* __restrict__ psi,
-                                                   const double* __restrict__ fcell, double* __restrict__ fl,
-                                                   double* __restrict__ up) {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= m.Fi) return;
+// Limited reconstruction of the seven recon fields to the owner (so) and
+// neighbour (sn) sides of internal face f (foam limitedSurfaceInterpolation
+// with NVDTVD r, V-limiters for rhoU, or Venkatakrishnan).
+__device__ __forceinline__ void face_recon(const DevMesh& m, int f, int lr, int lu, int lt,
+                                           const double* __restrict__ q, const double* __restrict__ g,
+                                           const double* __restrict__ psi, SideState& so, SideState& sn) {
     const int o = m.own[f], n = m.nei[f];
     const double wf = m.w[f];
-    const V3 S = ldv3(m.Sf, m.Fi, f);
-    const double magS = m.magSf[f];
     const double* qo = q + QW * o;
     const double* qn = q + QW * n;
-    SideState so, sn;
     const int Ls[7] = {lr, lu, lu, lu, lt, lt, lt};
     if (lr == L_VENKAT || lu == L_VENKAT || lt == L_VENKAT) {
         // all fields Venkatakrishnan-limited or linear/upwind (parse enforces a
@@ -470,6 +498,22 @@ __global__ void __launch_bounds__(128) k_face_flux(DevMesh m, Thermo th, int sch
         so.rhoU = add3(scl3(wo, xP), scl3(1 - wo, xN));
         sn.rhoU = add3(scl3(wn, xP), scl3(1 - wn, xN));
     }
+}
+
+// Face fluxes of all internal faces (reconstruction + scheme), AoS output.
+__global__ void __launch_bounds__(128) k_face_flux(DevMesh m, Thermo th, int scheme, int lr, int lu, int lt,
+                                                   int lowMach, double Mainf, const double* __restrict__ q,
+                                                   const double* __restrict__ g, const double* __restrict__ psi,
+                                                   const double* __restrict__ fcell, double* __restrict__ fl,
+                                                   double* __restrict__ up) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.Fi) return;
+    const int o = m.own[f], n = m.nei[f];
+    const double wf = m.w[f];
+    const V3 S = ldv3(m.Sf, m.Fi, f);
+    const double magS = m.magSf[f];
+    SideState so, sn;
+    face_recon(m, f, lr, lu, lt, q, g, psi, so, sn);
     double fs = 1.0;
     if (scheme == F_HLLCP) fs = wf * pow(fcell[o], 3.0) + (1 - wf) * pow(fcell[n], 3.0);
     FFlux F = face_flux(scheme, so, sn, S, magS, th.gamma, fs, lowMach != 0, Mainf);

@@ -8,6 +8,7 @@
 #include "rdst_internal.h"
 #include "linalg.cuh"
 #include "turbulence.cuh"
+#include "adjoint.cuh"
 
 #include <algorithm>
 #include <array>
@@ -130,6 +131,7 @@ __global__ void k_mean_courant(const double* __restrict__ partial, int nb, int N
     if (threadIdx.x == 0 && sc->step_idx < cap) reps[sc->step_idx].courant = s / N;
 }
 
+
 }  // namespace
 
 // ============================================================================
@@ -184,6 +186,13 @@ struct rdst_ctx {
     DBuf<float> Vf;                 // GMRES basis when it is kept in FP32
     long ldv = 0;                   // stride between basis vectors (entries)
     DBuf<double> wv;                // FP64 Arnoldi vector that is orthogonalised before it is stored in Vf
+    // discrete adjoint (allocated on first use)
+    DBuf<double> a_fbar, a_qbbar, a_qbar, a_gbar, a_vval, a_hval, a_wbar, a_wbarb, a_ubarb, a_pbar;
+    DBuf<double> a_r, a_z, a_t, a_psi, a_rhs, a_V, a_tmp, a_u3;
+    DBuf<int> a_vidx, a_hidx;
+    void* a_AT = nullptr;           // transposed Jacobian (storage type of A)
+    DBuf<double> t_buf;             // tangent records (value, derivative)
+    int a_m = 0;
     int limiter_need_grad = 1, venkat_mask = 0;
     bool steady = false;
     bool state_set = false;
@@ -252,6 +261,7 @@ struct rdst_ctx {
         if (Aval) cudaFree(Aval);
         if (LUval) cudaFree(LUval);
         if (dinv) cudaFree(dinv);
+        if (a_AT) cudaFree(a_AT);
         if (s) cudaStreamDestroy(s);
     }
 
@@ -1189,6 +1199,246 @@ void after_state_set(rdst_ctx& c) {
     c.state_set = true;
 }
 
+// ---------------------------------------------------------------- adjoint
+// Buffers of the adjoint pass and of its GMRES(m) (FP64 basis).
+void adj_alloc(rdst_ctx& c, int m) {
+    const long n5 = 5L * c.N;
+    if (!c.a_fbar.p) {
+        c.a_fbar.alloc((size_t)ADJ_FB * std::max(c.Fi, 1));
+        c.a_qbbar.alloc((size_t)ADJ_QB * std::max(c.NB, 1));
+        c.a_qbar.alloc((size_t)ADJ_QB * c.N);
+        c.a_gbar.alloc((size_t)GW * c.N);
+        c.a_vval.alloc(7L * c.N); c.a_vidx.alloc(7L * c.N);
+        c.a_hval.alloc(c.N); c.a_hidx.alloc(c.N);
+        c.a_wbar.alloc(n5);
+        c.a_wbarb.alloc(5L * std::max(c.NB, 1)); c.a_ubarb.alloc(3L * std::max(c.NB, 1));
+        c.a_pbar.alloc(std::max(c.NB, 1));
+        c.a_r.alloc(n5); c.a_z.alloc(n5); c.a_t.alloc(n5); c.a_psi.alloc(n5); c.a_rhs.alloc(n5);
+        c.a_tmp.alloc(n5); c.a_u3.alloc(16);
+        c.a_fbar.zero(c.s); c.a_qbbar.zero(c.s);
+    }
+    if (m > 0 && c.a_m != m) {
+        c.a_V.alloc((size_t)(m + 1) * c.ldv);
+        c.a_m = m;
+    }
+}
+
+int adj_use_c(const rdst_ctx& c) { return (c.o.flux == FLUX_KURGANOV || c.o.flux == FLUX_AUSM) ? 1 : 0; }
+
+// u = (dR/dW)^T v (internal order, device); usum (device, 3) = sum of the
+// patch-velocity shares when given
+void adj_product(rdst_ctx& c, const double* v, double* u, double* usum) {
+    const DevMesh& m = c.m;
+    const Options& o = c.o;
+    cudaStream_t s = c.s;
+    const int use_c = adj_use_c(c);
+    if (m.Fi > 0) {
+        k_adj_faces<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
+                                                   lim_code(o.lim_T), o.low_mach, o.mainf, c.q.p, c.g.p, c.psi.p,
+                                                   c.fcell.p, v, c.a_fbar.p);
+        CKL();
+    }
+    if (m.NB > 0) {
+        k_adj_bfaces<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), o.low_mach, o.mainf, c.qb.p, v,
+                                                     c.a_qbbar.p);
+        CKL();
+    }
+    k_adj_cells<<<nblk(m.N, 128), 128, 0, s>>>(m, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
+                                               lim_code(o.lim_T), c.venkat_mask, o.venkat_K, c.q.p, c.qb.p, c.g.p,
+                                               c.psi.p, c.fcell.p, c.prim.p, c.a_fbar.p, c.a_qbar.p, c.a_gbar.p,
+                                               c.a_vidx.p, c.a_vval.p, c.a_hidx.p, c.a_hval.p);
+    CKL();
+    k_adj_gather<<<nblk(m.N, 128), 128, 0, s>>>(m, c.th, c.bd, use_c, c.W.p, c.a_gbar.p, c.a_qbar.p, c.a_vidx.p,
+                                                c.a_vval.p, c.a_hidx.p, c.a_hval.p, c.a_qbbar.p, c.a_wbar.p);
+    CKL();
+    if (m.NB > 0) {
+        k_adj_bc<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, use_c, c.W.p, c.bs.p, c.a_qbbar.p, nullptr,
+                                                 c.a_wbarb.p, c.a_ubarb.p);
+        CKL();
+    }
+    k_adj_finish<<<nblk(m.N, TPB), TPB, 0, s>>>(m, c.a_wbar.p, c.a_wbarb.p, u);
+    CKL();
+    if (usum) {
+        if (m.NB > 0) {
+            const int nb = red_blocks(m.NB);
+            k_adj_usum<<<nb, RED_TPB, 0, s>>>(m.NB, c.a_ubarb.p, c.partial.p); CKL();
+            k_adj_psum<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, 3, usum); CKL();
+        } else {
+            CK(cudaMemsetAsync(usum, 0, 3 * sizeof(double), s));
+        }
+    }
+}
+
+// dJ/dW (device, internal order) of J = scale sum_patch (p - p_ref) S.d;
+// host out: J, force[3], dJ/dU_patch explicit part [3]
+void adj_objective(rdst_ctx& c, const rdst_objective& ob, double* dJdW, double out[7]) {
+    const DevMesh& m = c.m;
+    cudaStream_t s = c.s;
+    const int nb = red_blocks(std::max(m.NB, 1));
+    V3 dir;
+    dir.x = ob.direction[0]; dir.y = ob.direction[1]; dir.z = ob.direction[2];
+    k_adj_objective<<<nb, RED_TPB, 0, s>>>(m, ob.patch, dir, ob.p_ref,
+                                           ob.scale, c.bs.p, c.a_pbar.p, c.partial.p);
+    CKL();
+    k_adj_psum<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, 4, c.a_u3.p); CKL();
+    if (m.NB > 0) {
+        k_adj_bc<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, adj_use_c(c), c.W.p, c.bs.p, nullptr, c.a_pbar.p,
+                                                 c.a_wbarb.p, c.a_ubarb.p);
+        CKL();
+        const int nbu = red_blocks(m.NB);
+        k_adj_usum<<<nbu, RED_TPB, 0, s>>>(m.NB, c.a_ubarb.p, c.partial.p); CKL();
+        k_adj_psum<<<1, RED_TPB, 0, s>>>(c.partial.p, nbu, 3, c.a_u3.p + 4); CKL();
+    }
+    k_adj_finish<<<nblk(m.N, TPB), TPB, 0, s>>>(m, nullptr, c.a_wbarb.p, dJdW);
+    CKL();
+    CK(cudaMemcpyAsync(out, c.a_u3.p, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+}
+
+// Preconditioner of the transposed system: A is the step's approximate
+// Jacobian (Roe blocks + pseudo-time diagonal, A ~ V dR/dW + V/dtau); the
+// adjoint is right-preconditioned with M^-1 y = V (A^T)^-1 y, (A^T)^-1 by
+// block ILU(0) (or block Jacobi) of the transposed matrix.
+template <typename MT>
+void adj_precond_setup(rdst_ctx& c) {
+    Ops<MT>::assemble(c);
+    const size_t bytes = (size_t)c.n_slots * 32 * 25 * sizeof(MT);
+    if (!c.a_AT) CK(cudaMalloc(&c.a_AT, bytes));
+    k_transpose_blocks<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.a_AT);
+    CKL();
+    if (c.o.precon == PRECON_DIAGONAL) {
+        k_dinv<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.dinv);
+        CKL();
+    } else if (c.o.precon == PRECON_ILU0) {
+        const int n_fid = c.n_slices * c.lu_slots * 32;
+        k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, c.lu_src.p, n_fid);
+        CKL();
+        k_ilu_factor<MT><<<c.n_parts, ILU_TPB, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
+        CKL();
+    }
+}
+
+template <typename MT>
+void adj_precond(rdst_ctx& c, const double* in, double* out) {
+    Ops<MT>::precond(c, in, c.a_tmp.p, nullptr);
+    k_adj_scale_V<<<nblk(5L * c.N, TPB), TPB, 0, c.s>>>(c.N, c.m.V, c.a_tmp.p, out);
+    CKL();
+}
+
+// GMRES(m), right preconditioned, for (dR/dW)^T psi = rhs; returns the
+// number of Krylov iterations; res0 / res the true residual norms.
+template <typename MT>
+int adj_solve(rdst_ctx& c, const double* rhs, double* psi, double rel_tol, int max_cycles, int m, double& res0,
+              double& res, int& cycles) {
+    cudaStream_t s = c.s;
+    const long n = c.nvec();
+    Scalars* sc = c.sc.p;
+    int* act = &sc->gm_active;
+    double* Vb = c.a_V.p;
+    CK(cudaMemsetAsync(psi, 0, sizeof(double) * n, s));
+    int iters = 0;
+    res0 = 0.0;
+    res = 0.0;
+    cycles = 0;
+    double hb[2];
+    for (int cyc = 0; cyc < max_cycles; ++cyc) {
+        // r = rhs - J^T psi (into V_0)
+        adj_product(c, psi, c.a_t.p, nullptr);
+        k_adj_sub<<<nblk(n, TPB), TPB, 0, s>>>(n, rhs, c.a_t.p, Vb); CKL();
+        Ops<MT>::dot(c, Vb, Vb, &sc->beta, 1, nullptr);
+        CK(cudaMemcpyAsync(hb, &sc->beta, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        res = hb[0];
+        if (cyc == 0) res0 = res;
+        if (res <= rel_tol * res0 || res == 0.0) break;
+        ++cycles;
+        k_gm_start<<<1, 1, 0, s>>>(sc); CKL();
+        k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, Vb, &sc->beta, act); CKL();
+        for (int i = 0; i < m; ++i) {
+            const double* Vi = Vb + i * c.ldv;
+            double* w = Vb + (i + 1) * c.ldv;
+            adj_precond<MT>(c, Vi, c.a_z.p);
+            adj_product(c, c.a_z.p, w, nullptr);
+            const int nv = i + 1;
+            if (nv <= 8) Ops<MT>::template orth<8, double>(c, Vb, nv, w, act);
+            else if (nv <= 16) Ops<MT>::template orth<16, double>(c, Vb, nv, w, act);
+            else if (nv <= 32) Ops<MT>::template orth<32, double>(c, Vb, nv, w, act);
+            else Ops<MT>::template orth<64, double>(c, Vb, nv, w, act);
+            k_gm_givens<<<1, 1, 0, s>>>(sc, i, m); CKL();
+            if (i < m - 1) { k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, w, &sc->beta, act); CKL(); }
+            ++iters;
+        }
+        k_gm_backsub<<<1, 1, 0, s>>>(sc, m); CKL();
+        CK(cudaMemsetAsync(c.a_t.p, 0, sizeof(double) * n, s));
+        k_maxpy<double><<<nblk(n, TPB), TPB, 0, s>>>(n, m, Vb, c.ldv, sc->yh, c.a_t.p, -1.0, nullptr); CKL();
+        adj_precond<MT>(c, c.a_t.p, c.a_z.p);
+        k_adj_axpy<<<nblk(n, TPB), TPB, 0, s>>>(n, 1.0, c.a_z.p, psi); CKL();
+    }
+    return iters;
+}
+
+// the cell records (q, gradients, limiters; the boundary states and their
+// branches are those of the last boundary evaluation) at the current W
+template <typename MT>
+void adj_forward(rdst_ctx& c) {
+    if (c.tr.viscous)
+        throw ConfigError("adjoint: only the inviscid residual is differentiated (transport/turbulence set)", true);
+    Ops<MT>::flux(c);
+}
+
+
+// Ju = (dR/dW) u by the forward-mode (tangent) pass (internal order, device)
+void tan_product(rdst_ctx& c, const double* u, double* Ju) {
+    const DevMesh& m = c.m;
+    const Options& o = c.o;
+    cudaStream_t s = c.s;
+    const long N = c.N, NB = std::max(c.NB, 1), Fi = std::max(c.Fi, 1);
+    const size_t need = 2 * (N * QW + N + NB * QW + N * GW + N * QW + N) + 5 * Fi + 5 * NB;
+    if (c.t_buf.n < need) c.t_buf.alloc(need);
+    double* p0 = c.t_buf.p;
+    double* qv = p0;            double* qd = qv + N * QW;
+    double* pv = qd + N * QW;   double* pd = pv + N;
+    double* qbv = pd + N;       double* qbd = qbv + NB * QW;
+    double* gv = qbd + NB * QW; double* gd = gv + N * GW;
+    double* psv = gd + N * GW;  double* psd = psv + N * QW;
+    double* fcv = psd + N * QW; double* fcd = fcv + N;
+    double* fld = fcd + N;      double* bfld = fld + 5 * Fi;
+    const int use_c = adj_use_c(c);
+    k_tan_q<<<nblk(N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, use_c, c.W.p, u, qv, qd, pv, pd); CKL();
+    if (m.NB > 0) { k_tan_qb<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, use_c, c.W.p, u, c.bs.p, qbv, qbd); CKL(); }
+    k_tan_grad<<<nblk(N, 128), 128, 0, s>>>(m, c.venkat_mask, o.venkat_K, o.flux == FLUX_HLLCP, qv, qd, qbv, qbd, pv, pd,
+                                           gv, gd, psv, psd, fcv, fcd);
+    CKL();
+    if (m.Fi > 0) {
+        k_tan_faces<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
+                                                   lim_code(o.lim_T), o.low_mach, o.mainf, qv, qd, gv, gd, psv, psd,
+                                                   fcv, fcd, fld);
+        CKL();
+    }
+    if (m.NB > 0) {
+        k_tan_bfaces<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), o.low_mach, o.mainf, qbv, qbd, bfld);
+        CKL();
+    }
+    k_tan_residual<<<nblk(N, TPB), TPB, 0, s>>>(m, fld, bfld, Ju);
+    CKL();
+}
+
+// internal <-> caller order for N x 5 fields
+void adj_to_internal(rdst_ctx& c, const double* host, double* dev) {
+    std::vector<double> t(5L * c.N);
+    for (int r = 0; r < c.N; ++r)
+        for (int k = 0; k < 5; ++k) t[5L * r + k] = host[5L * c.perm[r] + k];
+    CK(cudaMemcpyAsync(dev, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice, c.s));
+    CK(cudaStreamSynchronize(c.s));
+}
+void adj_to_caller(rdst_ctx& c, const double* dev, double* host) {
+    std::vector<double> t(5L * c.N);
+    CK(cudaMemcpyAsync(t.data(), dev, t.size() * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    for (int r = 0; r < c.N; ++r)
+        for (int k = 0; k < 5; ++k) host[5L * c.perm[r] + k] = t[5L * r + k];
+}
+
 }  // namespace
 
 // ============================================================================ ABI
@@ -1473,6 +1723,97 @@ RDST_API rdst_status rdst_set_profile(rdst_ctx* c, int32_t on) {
         c->err = e.what();
         return RDST_ERR_CUDA;
     }
+}
+
+RDST_API rdst_status rdst_objective_gradient(rdst_ctx* c, const rdst_objective* ob, double* J, double force[3],
+                                             double* dJdW, double dJdU[3]) {
+    if (!c || !ob || !c->state_set) return RDST_ERR_ARG;
+    if (ob->patch < 0 || ob->patch >= c->n_patches) { c->err = "bad patch index"; return RDST_ERR_ARG; }
+    return guarded(c, [&] {
+        dispatch(*c, [&](auto* tag) {
+            using MT = std::remove_pointer_t<decltype(tag)>;
+            adj_forward<MT>(*c);
+        });
+        adj_alloc(*c, 0);
+        double out[7];
+        adj_objective(*c, *ob, c->a_rhs.p, out);
+        if (J) *J = out[0];
+        if (force) for (int k = 0; k < 3; ++k) force[k] = out[1 + k];
+        if (dJdU) for (int k = 0; k < 3; ++k) dJdU[k] = out[4 + k];
+        if (dJdW) adj_to_caller(*c, c->a_rhs.p, dJdW);
+    });
+}
+
+RDST_API rdst_status rdst_tangent_product(rdst_ctx* c, const double* u, double* Ju) {
+    if (!c || !u || !Ju || !c->state_set) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        dispatch(*c, [&](auto* tag) {
+            using MT = std::remove_pointer_t<decltype(tag)>;
+            adj_forward<MT>(*c);
+        });
+        adj_alloc(*c, 0);
+        adj_to_internal(*c, u, c->a_z.p);
+        tan_product(*c, c->a_z.p, c->a_t.p);
+        adj_to_caller(*c, c->a_t.p, Ju);
+    });
+}
+
+RDST_API rdst_status rdst_adjoint_product(rdst_ctx* c, const double* v, double* u, double dU[3]) {
+    if (!c || !v || !u || !c->state_set) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        dispatch(*c, [&](auto* tag) {
+            using MT = std::remove_pointer_t<decltype(tag)>;
+            adj_forward<MT>(*c);
+        });
+        adj_alloc(*c, 0);
+        adj_to_internal(*c, v, c->a_z.p);
+        adj_product(*c, c->a_z.p, c->a_t.p, c->a_u3.p + 8);
+        adj_to_caller(*c, c->a_t.p, u);
+        if (dU) {
+            CK(cudaMemcpyAsync(dU, c->a_u3.p + 8, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+            CK(cudaStreamSynchronize(c->s));
+        }
+    });
+}
+
+RDST_API rdst_status rdst_adjoint(rdst_ctx* c, const rdst_objective* ob, double rel_tol, int32_t max_cycles,
+                                  int32_t n_directions, double* psi, rdst_adjoint_report* rep) {
+    if (!c || !ob || !c->state_set || max_cycles < 1 || n_directions < 1 || n_directions > 64 || !(rel_tol > 0))
+        return RDST_ERR_ARG;
+    if (ob->patch < 0 || ob->patch >= c->n_patches) { c->err = "bad patch index"; return RDST_ERR_ARG; }
+    return guarded(c, [&] {
+        cudaEvent_t e0 = c->get_event(), e1 = c->get_event();
+        CK(cudaEventRecord(e0, c->s));
+        double out[7], usum[3];
+        double res0 = 0, res = 0;
+        int iters = 0, cycles = 0;
+        dispatch(*c, [&](auto* tag) {
+            using MT = std::remove_pointer_t<decltype(tag)>;
+            adj_forward<MT>(*c);
+            adj_alloc(*c, n_directions);
+            adj_objective(*c, *ob, c->a_rhs.p, out);
+            adj_precond_setup<MT>(*c);
+            iters = adj_solve<MT>(*c, c->a_rhs.p, c->a_psi.p, rel_tol, max_cycles, n_directions, res0, res, cycles);
+            adj_product(*c, c->a_psi.p, c->a_t.p, c->a_u3.p + 8);
+        });
+        CK(cudaMemcpyAsync(usum, c->a_u3.p + 8, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaEventRecord(e1, c->s));
+        CK(cudaStreamSynchronize(c->s));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        c->ev_pool.push_back(e0);
+        c->ev_pool.push_back(e1);
+        if (psi) adj_to_caller(*c, c->a_psi.p, psi);
+        if (rep) {
+            rep->J = out[0];
+            for (int k = 0; k < 3; ++k) { rep->force[k] = out[1 + k]; rep->dJ_dU[k] = out[4 + k] - usum[k]; }
+            rep->residual0 = res0;
+            rep->residual = res;
+            rep->iterations = iters;
+            rep->cycles = cycles;
+            rep->t_ms = ms;
+        }
+    });
 }
 
 RDST_API void rdst_destroy(rdst_ctx* c) { delete c; }

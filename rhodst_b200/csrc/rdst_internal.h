@@ -27,7 +27,7 @@ namespace rdst {
 constexpr int QW = 8;     // recon record stride (7 recon fields + muEff)
 constexpr int GW = 24;    // gradient record stride (21 used)
 constexpr int PW = 8;     // prim record stride
-constexpr int BW = 16;    // boundary state stride (rho, rhoU, rhoE, p, T, phi, f_p, f_U, f_T, -, U_b xyz, -)
+constexpr int BW = 16;    // boundary state stride (rho, rhoU, rhoE, p, T, phi, f_p, f_U, f_T, -, phi_prev, U_b xyz, mach_prev)
 constexpr int SELL_C = 32;
 
 struct DevPatch {
