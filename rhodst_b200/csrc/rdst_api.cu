@@ -190,6 +190,8 @@ struct rdst_ctx {
     DBuf<double> a_fbar, a_qbbar, a_qbar, a_gbar, a_vval, a_hval, a_wbar, a_wbarb, a_ubarb, a_pbar;
     DBuf<double> a_r, a_z, a_t, a_psi, a_rhs, a_V, a_tmp, a_u3;
     DBuf<int> a_vidx, a_hidx;
+    DBuf<double> a_Z;               // flexible-GMRES preconditioned directions
+    DBuf<Scalars> a_sc;             // Hessenberg and rotations of the adjoint's outer solve
     void* a_AT = nullptr;           // transposed Jacobian (storage type of A)
     DBuf<double> t_buf;             // tangent records (value, derivative)
     int a_m = 0;
@@ -1219,8 +1221,10 @@ void adj_alloc(rdst_ctx& c, int m) {
     }
     if (m > 0 && c.a_m != m) {
         c.a_V.alloc((size_t)(m + 1) * c.ldv);
+        c.a_Z.alloc((size_t)(m + 1) * c.ldv);
         c.a_m = m;
     }
+    if (!c.a_sc.p) { c.a_sc.alloc(1); c.a_sc.zero(c.s); }
 }
 
 int adj_use_c(const rdst_ctx& c) { return (c.o.flux == FLUX_KURGANOV || c.o.flux == FLUX_AUSM) ? 1 : 0; }
@@ -1325,30 +1329,54 @@ void adj_precond(rdst_ctx& c, const double* in, double* out) {
     CKL();
 }
 
-// GMRES(m), right preconditioned, for (dR/dW)^T psi = rhs; returns the
-// number of Krylov iterations; res0 / res the true residual norms.
+// One application of the adjoint's preconditioner: out ~ V (A^T)^-1 in.
+// With the GMRES step solver it is one restart cycle of that same solver
+// (its directions, basis precision and block ILU(0)/Jacobi) run on A^T, the
+// linear solve the step itself performs on A; otherwise the block
+// preconditioner of A^T alone.
+template <typename MT>
+void adj_prec(rdst_ctx& c, const double* in, double* out) {
+    if (c.o.solver != SOLVER_GMRES) {
+        adj_precond<MT>(c, in, out);
+        return;
+    }
+    const long n = c.nvec();
+    std::swap(c.Aval, c.a_AT);
+    CK(cudaMemcpyAsync(c.rhs.p, in, sizeof(double) * n, cudaMemcpyDeviceToDevice, c.s));
+    CK(cudaMemsetAsync(c.dx.p, 0, sizeof(double) * n, c.s));
+    Ops<MT>::gmres_cycle(c);
+    std::swap(c.Aval, c.a_AT);
+    k_adj_scale_V<<<nblk(n, TPB), TPB, 0, c.s>>>(c.N, c.m.V, c.dx.p, out);
+    CKL();
+}
+
+// Flexible GMRES(m), right preconditioned by adj_prec, for
+// (dR/dW)^T psi = rhs; its Hessenberg lives in its own Scalars (the inner
+// cycles use the step's).  Returns the number of outer iterations; res0 /
+// res are the true residual norms at the start and at exit.
 template <typename MT>
 int adj_solve(rdst_ctx& c, const double* rhs, double* psi, double rel_tol, int max_cycles, int m, double& res0,
               double& res, int& cycles) {
     cudaStream_t s = c.s;
     const long n = c.nvec();
-    Scalars* sc = c.sc.p;
+    Scalars* sc = c.a_sc.p;
     int* act = &sc->gm_active;
     double* Vb = c.a_V.p;
+    double* Zb = c.a_Z.p;
     CK(cudaMemsetAsync(psi, 0, sizeof(double) * n, s));
     int iters = 0;
     res0 = 0.0;
     res = 0.0;
     cycles = 0;
-    double hb[2];
     for (int cyc = 0; cyc < max_cycles; ++cyc) {
         // r = rhs - J^T psi (into V_0)
         adj_product(c, psi, c.a_t.p, nullptr);
         k_adj_sub<<<nblk(n, TPB), TPB, 0, s>>>(n, rhs, c.a_t.p, Vb); CKL();
         Ops<MT>::dot(c, Vb, Vb, &sc->beta, 1, nullptr);
-        CK(cudaMemcpyAsync(hb, &sc->beta, sizeof(double), cudaMemcpyDeviceToHost, s));
+        double beta = 0.0;
+        CK(cudaMemcpyAsync(&beta, &sc->beta, sizeof(double), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        res = hb[0];
+        res = beta;
         if (cyc == 0) res0 = res;
         if (res <= rel_tol * res0 || res == 0.0) break;
         ++cycles;
@@ -1356,23 +1384,29 @@ int adj_solve(rdst_ctx& c, const double* rhs, double* psi, double rel_tol, int m
         k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, Vb, &sc->beta, act); CKL();
         for (int i = 0; i < m; ++i) {
             const double* Vi = Vb + i * c.ldv;
+            double* Zi = Zb + i * c.ldv;
             double* w = Vb + (i + 1) * c.ldv;
-            adj_precond<MT>(c, Vi, c.a_z.p);
-            adj_product(c, c.a_z.p, w, nullptr);
+            adj_prec<MT>(c, Vi, Zi);
+            adj_product(c, Zi, w, nullptr);
             const int nv = i + 1;
-            if (nv <= 8) Ops<MT>::template orth<8, double>(c, Vb, nv, w, act);
-            else if (nv <= 16) Ops<MT>::template orth<16, double>(c, Vb, nv, w, act);
-            else if (nv <= 32) Ops<MT>::template orth<32, double>(c, Vb, nv, w, act);
-            else Ops<MT>::template orth<64, double>(c, Vb, nv, w, act);
+            // CGS2 against V_0..V_i into this solve's own Hessenberg column
+            auto orth = [&](auto nvtag) {
+                constexpr int NV = decltype(nvtag)::value;
+                Ops<MT>::template vmultidot<NV, double>(c, Vb, nv, w, sc->hcol[0], act);
+                Ops<MT>::template maxpy_dot<NV, double>(c, Vb, nv, sc->hcol[0], w, sc->hcol[1], 0, act);
+                Ops<MT>::template maxpy_dot<NV, double>(c, Vb, nv, sc->hcol[1], w, &sc->beta, 1, act);
+            };
+            if (nv <= 8) orth(std::integral_constant<int, 8>());
+            else if (nv <= 16) orth(std::integral_constant<int, 16>());
+            else if (nv <= 32) orth(std::integral_constant<int, 32>());
+            else orth(std::integral_constant<int, 64>());
             k_gm_givens<<<1, 1, 0, s>>>(sc, i, m); CKL();
             if (i < m - 1) { k_scale_inv<<<nblk(n, TPB), TPB, 0, s>>>(n, w, &sc->beta, act); CKL(); }
             ++iters;
         }
         k_gm_backsub<<<1, 1, 0, s>>>(sc, m); CKL();
-        CK(cudaMemsetAsync(c.a_t.p, 0, sizeof(double) * n, s));
-        k_maxpy<double><<<nblk(n, TPB), TPB, 0, s>>>(n, m, Vb, c.ldv, sc->yh, c.a_t.p, -1.0, nullptr); CKL();
-        adj_precond<MT>(c, c.a_t.p, c.a_z.p);
-        k_adj_axpy<<<nblk(n, TPB), TPB, 0, s>>>(n, 1.0, c.a_z.p, psi); CKL();
+        // psi += Z y
+        k_maxpy<double><<<nblk(n, TPB), TPB, 0, s>>>(n, m, Zb, c.ldv, sc->yh, psi, -1.0, nullptr); CKL();
     }
     return iters;
 }
