@@ -121,6 +121,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+def traffic_per_launch(workload: str, kernel: str):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summary (profiles/traffic.json), or None when none was captured."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text()).get(workload, {})
+    return d.get(kernel)
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -248,7 +258,7 @@ def run_ours(args, rank, world):
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
                 "bytes_per_launch": by, "launches": int(n_l), "avg_launch_us": round(ms_l / n_l * 1e3, 3),
-                "traffic": None,
+                "traffic": traffic_per_launch(args.workload, dom),
                 "share_of_step": round(ms_l / max(prof_ms, 1e-9), 4),
                 "note": "working set below L2 (126 MB): L2-resident bandwidth" if
                         (25 * S * (N + 2 * F)) < 100e6 else "HBM-resident"}
@@ -270,12 +280,72 @@ def run_ours(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == "fp64" else (f"f64 residual/dots/Hessenberg, {prec} Jacobian+ILU, "
                                                   f"{'f32' if vb0 == 4 else 'f64'} Krylov basis"),
-            "data": "synthetic (generated mesh, uniform Mach-3 inflow initial state)",
+            "data": "synthetic (generated mesh, uniform free-stream initial state)",
             "config": dict(desc, l2="flushed: 256 MB written between timed steps",
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches), "roofline": roof,
             "kernels": breakdown, "kernels_profiled_ms_per_step": round(prof_ms / max(prof_steps, 1), 3)}
     return line, case
+
+
+def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
+    """Time to a density-residual drop of `drop` in FP64 and in mixed
+    precision (FP32 Jacobian/ILU/basis) on the workload's mesh with
+    first-order HLL reconstruction at CFL 500 (the limited second-order
+    cases stall near 1e-6: limiter switching), then the discrete adjoint of
+    the pressure-drag coefficient at the FP64 converged state, its cost
+    against that forward solve and dJ/dMach, dJ/dalpha."""
+    import math
+    import rhodst_b200
+    first = {"fluxScheme": "HLL", "timeControls": dict(case.options["timeControls"], maxCo=500.0),
+             "interpolationSchemes": {"reconstruct(rho)": "upwind", "reconstruct(U)": "upwind",
+                                      "reconstruct(T)": "upwind"}}
+    g = case.options["thermo"]
+    U0 = np.asarray(case.U[0], dtype=float)
+    c_inf = math.sqrt(g["Cp"] / (g["Cp"] - g["R"]) * g["R"] * 1.0)
+    alpha = math.atan2(U0[1], U0[0])
+    drag = (math.cos(alpha), math.sin(alpha), 0.0)
+    lift = (-math.sin(alpha), math.cos(alpha), 0.0)
+    patch = case.force_patch
+    ref_area = 0.1 if case.name.startswith("naca") else 1.5 * 0.5 * (1.0 + 0.56)
+    qA = 0.5 * (1.0 / (g["R"] * 1.0)) * float(U0 @ U0) * ref_area
+    out = {"drop": drop, "config": "same mesh and free stream, HLL, first-order (upwind) reconstruction, CFL 500",
+           "max_steps": max_steps}
+    solvers = {}
+    for prec in ("fp64", "fp32"):
+        opts = dict(case.options, **first, precision=prec, profile=False)
+        s = rhodst_b200.Solver(case.mesh, case.bcs, opts)
+        s.set_primitive(case.p, case.U, case.T)
+        r0, steps, dev_ms, hit = None, 0, 0.0, None
+        while steps < max_steps and hit is None:
+            reps = s.step(50)
+            dev_ms += s.last_step_ms()
+            for r in reps:
+                steps += 1
+                if r0 is None:
+                    r0 = r["res_l2"][0]
+                if hit is None and r["res_l2"][0] <= drop * r0:
+                    hit = steps
+        f = s.forces(patch, lift, drag, 1.0, qA)
+        out[prec] = {"steps": hit, "steps_run": steps, "device_s": dev_ms * 1e-3,
+                     "final_drop": reps[-1]["res_l2"][0] / r0, "Cl": f["Cl"], "Cd": f["Cd"]}
+        solvers[prec] = s
+    if out["fp64"]["steps"] and out["fp32"]["steps"]:
+        out["speedup_mixed_over_fp64"] = out["fp64"]["device_s"] / out["fp32"]["device_s"]
+    out["Cl_rel_diff"] = abs(out["fp32"]["Cl"] - out["fp64"]["Cl"]) / abs(out["fp64"]["Cl"])
+    out["Cd_rel_diff"] = abs(out["fp32"]["Cd"] - out["fp64"]["Cd"]) / abs(out["fp64"]["Cd"])
+    rep, _ = solvers["fp64"].adjoint(patch, drag, p_ref=1.0, scale=1.0 / qA, rel_tol=1e-8, max_cycles=30,
+                                     n_directions=30)
+    dU_dM = c_inf * U0 / np.linalg.norm(U0)
+    dU_da = np.linalg.norm(U0) * np.array([-math.sin(alpha), math.cos(alpha), 0.0])
+    dJ_dM = float(rep["dJ_dU"] @ dU_dM)
+    dJ_da = float(rep["dJ_dU"] @ dU_da + rep["force"] @ np.array(lift))   # d(drag dir)/dalpha = lift dir
+    out["adjoint"] = {"objective": f"pressure drag coefficient of patch {patch}", "J": rep["J"],
+                      "device_s": rep["t_ms"] * 1e-3, "outer_iterations": rep["iterations"],
+                      "residual_drop": rep["residual"] / rep["residual0"],
+                      "cost_over_forward": rep["t_ms"] * 1e-3 / out["fp64"]["device_s"],
+                      "dJ_dMach": dJ_dM, "dJ_dalpha_per_rad": dJ_da}
+    return out
 
 
 def cpu_baseline(case, budget_s: float, steps_max: int, warmup: int = 1):
@@ -352,6 +422,8 @@ def main():
     ap.add_argument("--converge", type=float, default=0.0,
                     help="run to this density-residual drop instead of timing fixed steps")
     ap.add_argument("--max-steps", type=int, default=5000)
+    ap.add_argument("--no-convergence", dest="convergence", action="store_false",
+                    help="skip the time-to-1e-10 (FP64 vs mixed) and adjoint-cost runs on the same mesh")
     args = ap.parse_args()
     if args.converge > 0:
         run_converge(args)
@@ -376,6 +448,9 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     line, case = run_ours(args, rank, world)
     if rank == 0:
+        inviscid = "transport" not in case.options and case.options.get("RASModel", "laminar") == "laminar"
+        if world == 1 and args.convergence and case.force_patch and inviscid:
+            line["time_to_residual_drop"] = convergence_and_adjoint(case)
         line["cpu_baseline"] = cpu_baseline(case, budget_s=args.cpu_budget, steps_max=1000, warmup=1)
         print(json.dumps(line))
     if world > 1:
