@@ -71,6 +71,16 @@ def workload(name: str):
                 "preconditioner": "subdomain block ILU(0)", "mach": 0.73, "alpha_deg": 2.3, "reynolds": 6.5e6,
                 "precision": precision_desc(c.options)}
         return c, desc
+    if name.startswith("forward_step_3d"):
+        prec = name.split("_")[-1] if name.count("_") >= 3 else "fp32"
+        c = cases.forward_step_3d_hybrid_c5(precision=prec)
+        desc = {"workload": name, "mesh": "3D forward step, hybrid prism/tet from a 240x80x56 lattice, interior nodes "
+                                          "jittered up to 25 % (seed 20240601)",
+                "cells": c.mesh.n_cells, "internal_faces": c.mesh.n_internal_faces, "flux": "HLLC",
+                "reconstruction": "Venkatakrishnan", "ddt": "steadyStateDST local dt, CFL 0.5->5",
+                "solver": "GMRES(20), 1 restart cycle", "preconditioner": "subdomain block ILU(0)",
+                "precision": precision_desc(c.options), "mach": 3.0}
+        return c, desc
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -285,7 +295,7 @@ def run_ours(args, rank, world):
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches), "roofline": roof,
             "kernels": breakdown, "kernels_profiled_ms_per_step": round(prof_ms / max(prof_steps, 1), 3)}
-    return line, case
+    return line, case, s
 
 
 def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
@@ -446,10 +456,10 @@ def main():
     if world > 1:
         import torch
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    line, case = run_ours(args, rank, world)
+    line, case, _ = run_ours(args, rank, world)
     if rank == 0:
         inviscid = "transport" not in case.options and case.options.get("RASModel", "laminar") == "laminar"
-        if world == 1 and args.convergence and case.force_patch and inviscid:
+        if world == 1 and args.convergence and case.force_patch in ("wing", "airfoil") and inviscid:
             line["time_to_residual_drop"] = convergence_and_adjoint(case)
         line["cpu_baseline"] = cpu_baseline(case, budget_s=args.cpu_budget, steps_max=1000, warmup=1)
         print(json.dumps(line))

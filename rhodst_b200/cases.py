@@ -251,3 +251,41 @@ def naca0012_turbulent(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: f
     return Case("naca0012_SA", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N),
                 nuTilda=np.full(N, nut_inf), steps=4000, force_patch="airfoil",
                 force_dirs={"lift": (-math.sin(al), math.cos(al), 0.0), "drag": (math.cos(al), math.sin(al), 0.0)})
+
+
+def forward_step_3d_hybrid_c5(nx: int = 240, ny: int = 80, nz: int = 56, precision: str = "fp32",
+                              limiter: str = "Venkatakrishnan", flux: str = "HLLC", jitter: float = 0.25,
+                              seed: int = 20240601) -> Case:
+    """3D Mach-3 forward-facing step on a hybrid tet/prism mesh (prisms in
+    the lower half, tetrahedra above; interior nodes jittered by up to 25 %
+    of the local spacing from `seed`): 3.96 M cells at the default size.
+    HLLC, limited reconstruction, steady state by local time stepping
+    (steadyStateDST, CFL 0.5 ramping to at most 5: the impulsive Mach-3
+    start is not stable at larger local CFL on the jittered tetrahedra),
+    block-GMRES(20) with subdomain block ILU(0), Jacobian/ILU in
+    `precision` with the FP64 residual.  BCs as the 2D step: fixed inflow,
+    supersonic outflow, slip obstacle, symmetry planes on the channel walls."""
+    m = _mesh.forward_step_3d_hybrid(nx, ny, nz, jitter=jitter, seed=seed)
+    U0 = (3.0, 0.0, 0.0)
+    bcs = {
+        "inlet": {"p": ("fixedValue", 1.0), "U": ("fixedValue", U0), "T": ("fixedValue", 1.0)},
+        "outlet": {"p": "zeroGradient", "U": ("inletOutlet", U0), "T": ("inletOutlet", 1.0)},
+        "obstacle": {"p": "zeroGradient", "U": "slip", "T": "zeroGradient"},
+        "walls": {"p": "symmetryPlane", "U": "symmetryPlane", "T": "symmetryPlane"},
+    }
+    options = {
+        "fluxScheme": flux,
+        "Jacobian": "Roe",
+        "timeControls": {"neighbouring": False, "initialCo": 0.5, "minCo": 0.1, "maxCo": 5.0},
+        "ddtSchemes": {"default": "steadyStateDST"},
+        "interpolationSchemes": {"reconstruct(rho)": limiter, "reconstruct(U)": _vector_limiter(limiter),
+                                 "reconstruct(T)": limiter},
+        "solvers": {"W": {"solver": "GMRES", "preconditioner": "ILUC0", "nDirections": 20,
+                          "tolerance": 1e-12, "relTol": 0.0, "maxIter": 1, "minIter": 1}},
+        "fieldBounds": {"rho": (1e-3, 1e4), "p": (1e-3, 1e4), "T": (1e-3, 1e4)},
+        "thermo": dict(NORMALISED_GAS),
+        "precision": precision,
+    }
+    N = m.n_cells
+    return Case("forwardStep3DHybrid", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N), steps=1000,
+                force_patch="obstacle", force_dirs={"lift": (0.0, 1.0, 0.0), "drag": (1.0, 0.0, 0.0)})

@@ -62,6 +62,9 @@ def smooth_state(case, seed=3):
     U = case.U.copy()
     U[:, 0] *= 1 + amp * modes[2]
     U[:, 1] += amp * np.abs(case.U[:, 0]).max() * modes[3]
+    # a z velocity too: an identically zero field ties every max/min of the
+    # Venkatakrishnan limiter, a point where the limiter has no derivative
+    U[:, 2] += amp * np.abs(case.U[:, 0]).max() * modes[4]
     g = case.options["thermo"]
     rho = p / (g["R"] * T)
     rhoE = rho * ((g["Cp"] - g["R"]) * T + 0.5 * (U ** 2).sum(1))
