@@ -225,6 +225,12 @@ rdst_status rdst_adjoint_product(rdst_ctx* ctx, const double* v, double* u, doub
  * linearization of the same residual with the same held branches: the
  * exact counterpart of rdst_adjoint_product (v . Ju = ((dR/dW)^T v) . u). */
 rdst_status rdst_tangent_product(rdst_ctx* ctx, const double* u, double* Ju);
+/* rdst_boundary_branches: for every boundary face (face - n_internal_faces;
+ * zero on empty patches) the previous mass flux and far-field Mach number
+ * that chose the in/outflow and sub/supersonic branches of the current
+ * boundary states, i.e. the branches the adjoint and tangent linearize.
+ * No counterpart in the reference. */
+rdst_status rdst_boundary_branches(rdst_ctx* ctx, double* phi_prev, double* mach);
 /* rdst_adjoint: solves (dR/dW)^T psi = dJ/dW by GMRES(n_directions),
  * right-preconditioned with the transposed step Jacobian (block ILU(0) or
  * block Jacobi as the solvers.W preconditioner selects), restarted until

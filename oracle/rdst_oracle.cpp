@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <complex>
 #include <string>
 #include <vector>
 
@@ -1971,3 +1972,6 @@ ORACLE_API void rdsto_flux_jacobian(const double* W, const double* n, double gam
 
 // limiter function value (for the limiter unit tests)
 ORACLE_API double rdsto_limiter(int32_t L, double r) { return tvd_limiter((Limiter)L, r); }
+
+// complex-step residual (test reference for the adjoint)
+#include "rdst_cs.inc"

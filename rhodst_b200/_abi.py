@@ -134,6 +134,7 @@ def declare(lib: ctypes.CDLL, prefix: str) -> None:
         f("objective_gradient", c_int32, [vp, POINTER(RdstObjective), dp, dp, dp, dp])
         f("adjoint_product", c_int32, [vp, dp, dp, dp])
         f("tangent_product", c_int32, [vp, dp, dp])
+        f("boundary_branches", c_int32, [vp, dp, dp])
         f("adjoint", c_int32, [vp, POINTER(RdstObjective), c_double, c_int32, c_int32, dp,
                                POINTER(RdstAdjointReport)])
 
@@ -339,6 +340,14 @@ class Solver:
         Ju = np.empty((self.n_cells, 5))
         self._check(self._fn("tangent_product")(self._h, _dptr(u), _dptr(Ju)), "tangent_product")
         return Ju
+
+    def boundary_branches(self):
+        """(previous boundary mass flux, far-field Mach) per boundary face
+        (face - n_internal_faces): the inputs of the current boundary branches."""
+        nb = self.mesh.n_faces - self.mesh.n_internal_faces
+        phi, mach = np.empty(nb), np.empty(nb)
+        self._check(self._fn("boundary_branches")(self._h, _dptr(phi), _dptr(mach)), "boundary_branches")
+        return phi, mach
 
     def adjoint(self, patch: str, direction, p_ref: float = 0.0, scale: float = 1.0, rel_tol: float = 1e-10,
                 max_cycles: int = 50, n_directions: int = 30, want_psi: bool = False):

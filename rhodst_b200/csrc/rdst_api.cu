@@ -1778,6 +1778,24 @@ RDST_API rdst_status rdst_objective_gradient(rdst_ctx* c, const rdst_objective* 
     });
 }
 
+RDST_API rdst_status rdst_boundary_branches(rdst_ctx* c, double* phi_prev, double* mach) {
+    if (!c || !phi_prev || !mach || !c->state_set) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        const int nball = c->NBall;
+        std::fill(phi_prev, phi_prev + nball, 0.0);
+        std::fill(mach, mach + nball, 0.0);
+        if (c->NB == 0) return;
+        std::vector<double> bs((size_t)BW * c->NB);
+        CK(cudaMemcpyAsync(bs.data(), c->bs.p, bs.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        CK(cudaStreamSynchronize(c->s));
+        for (int b = 0; b < c->NB; ++b) {
+            const int k = c->bface_orig[b] - c->Fi;
+            phi_prev[k] = bs[(size_t)BW * b + 11];
+            mach[k] = bs[(size_t)BW * b + 15];
+        }
+    });
+}
+
 RDST_API rdst_status rdst_tangent_product(rdst_ctx* c, const double* u, double* Ju) {
     if (!c || !u || !Ju || !c->state_set) return RDST_ERR_ARG;
     return guarded(c, [&] {

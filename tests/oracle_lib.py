@@ -15,7 +15,7 @@ _lib = None
 
 def build_oracle() -> Path:
     src = ROOT / "oracle" / "rdst_oracle.cpp"
-    deps = [src, ROOT / "include" / "rdst.h", ROOT / "rhodst_b200" / "csrc" / "rdst_options.h"]
+    deps = [src, ROOT / "oracle" / "rdst_cs.inc", ROOT / "include" / "rdst.h", ROOT / "rhodst_b200" / "csrc" / "rdst_options.h"]
     if not ORACLE_SO.exists() or any(p.stat().st_mtime > ORACLE_SO.stat().st_mtime for p in deps):
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
     return ORACLE_SO
@@ -38,6 +38,11 @@ def load_oracle() -> ctypes.CDLL:
         lib.rdsto_set_partition.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
         lib.rdsto_precondition.restype = ctypes.c_int32
         lib.rdsto_precondition.argtypes = [ctypes.c_void_p, d, d]
+        lib.rdsto_cs_residual.restype = ctypes.c_int32
+        lib.rdsto_cs_residual.argtypes = [ctypes.c_void_p, d, d, d, ctypes.c_double, d, d, d, d]
+        lib.rdsto_cs_objective.restype = ctypes.c_int32
+        lib.rdsto_cs_objective.argtypes = [ctypes.c_void_p, d, d, d, ctypes.c_double, d, d, ctypes.c_int32, d,
+                                           ctypes.c_double, ctypes.c_double, d, d, d]
         lib.rdsto_linear_solve.restype = ctypes.c_int32
         lib.rdsto_linear_solve.argtypes = [ctypes.c_void_p, d, ctypes.c_void_p]
         _lib = lib
@@ -68,3 +73,99 @@ class OracleSolver(Solver):
         self._check(self.lib.rdsto_linear_solve(self._h, x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                                 ctypes.byref(rep)), "linear_solve")
         return x, rep.as_dict()
+
+
+def _dp(a):
+    import numpy as np
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a
+
+
+class ComplexStep:
+    """Complex-step derivatives of the oracle's inviscid residual and of the
+    pressure-force objective (rdsto_cs_residual / rdsto_cs_objective):
+    Im f(x + i h v) / h with h = 1e-30, exact to rounding.  W, u are N x 5
+    conservative fields; branches = (phi_prev, mach) per boundary face or
+    None for the oracle's own."""
+    H = 1e-30
+
+    def __init__(self, oracle: "OracleSolver"):
+        self.o = oracle
+
+    def residual(self, W, u=None, dU=None, branches=None):
+        import numpy as np
+        N = self.o.n_cells
+        keep = []
+        def p(a):
+            if a is None:
+                return None
+            q, arr = _dp(a)
+            keep.append(arr)
+            return q
+        R, dR = np.empty((N, 5)), np.empty((N, 5))
+        ph, mc = branches if branches is not None else (None, None)
+        st = self.o.lib.rdsto_cs_residual(self.o._h, p(W), p(u), p(dU), self.H, p(ph), p(mc), p(R), p(dR))
+        self.o._check(st, "cs_residual")
+        return R, dR
+
+    def objective(self, W, patch: str, direction, p_ref=0.0, scale=1.0, u=None, dU=None, branches=None,
+                  per_cell=False):
+        import numpy as np
+        keep = []
+        def p(a):
+            if a is None:
+                return None
+            q, arr = _dp(a)
+            keep.append(arr)
+            return q
+        J, dJ = ctypes.c_double(), ctypes.c_double()
+        ph, mc = branches if branches is not None else (None, None)
+        cells = np.zeros(self.o.n_cells) if per_cell else None
+        st = self.o.lib.rdsto_cs_objective(self.o._h, p(W), p(u), p(dU), self.H, p(ph), p(mc),
+                                           self.o.mesh.patch_index(patch), p(list(direction)), p_ref, scale,
+                                           ctypes.byref(J), ctypes.byref(dJ),
+                                           cells.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if per_cell else None)
+        self.o._check(st, "cs_objective")
+        return (J.value, dJ.value, cells) if per_cell else (J.value, dJ.value)
+
+
+def conservative_array(W):
+    """(rho, rhoU, rhoE) -> N x 5."""
+    import numpy as np
+    rho, rhoU, rhoE = W
+    return np.ascontiguousarray(np.concatenate([rho[:, None], rhoU, rhoE[:, None]], 1))
+
+
+def distance2_colors(mesh, hops: int = 2):
+    """Greedy colouring of the cells such that two cells of one colour are
+    more than `hops` face-hops apart (hops = 2 for a residual whose rows
+    depend on face neighbours only, 4 when they depend on neighbours of
+    neighbours)."""
+    import numpy as np
+    N = mesh.n_cells
+    own = np.asarray(mesh.owner[:mesh.n_internal_faces])
+    nei = np.asarray(mesh.neighbour)
+    adj = [[] for _ in range(N)]
+    for a, b in zip(own, nei):
+        adj[a].append(int(b))
+        adj[b].append(int(a))
+    color = -np.ones(N, dtype=np.int64)
+    for i in range(N):
+        seen = {i}
+        front = [i]
+        for _ in range(hops):
+            nxt = []
+            for x in front:
+                for y in adj[x]:
+                    if y not in seen:
+                        seen.add(y)
+                        nxt.append(y)
+            front = nxt
+        used = {int(color[j]) for j in seen if color[j] >= 0}
+        k = 0
+        while k in used:
+            k += 1
+        color[i] = k
+    return color, adj
