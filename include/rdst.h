@@ -231,6 +231,16 @@ rdst_status rdst_tangent_product(rdst_ctx* ctx, const double* u, double* Ju);
  * boundary states, i.e. the branches the adjoint and tangent linearize.
  * No counterpart in the reference. */
 rdst_status rdst_boundary_branches(rdst_ctx* ctx, double* phi_prev, double* mach);
+/* rdst_set_geometry: replace the mesh metrics of the context (Sf, Cf,
+ * magSf, weights, deltaCoeffs, C, V and the wall distance) with those of a
+ * mesh of the same topology -- equal counts, owner/neighbour lists and patch
+ * ranges, else RDST_ERR_MESH and the context is unchanged.  State, options
+ * and boundary values stay; the next residual, step or adjoint call works on
+ * the new geometry.  Shape derivatives use it: the explicit derivatives of
+ * R and J with respect to a design variable that moves the mesh, at a fixed
+ * state, without building a new context.  No counterpart in the reference
+ * (rhoDST runs on static meshes). */
+rdst_status rdst_set_geometry(rdst_ctx* ctx, const rdst_mesh* mesh);
 /* rdst_adjoint: solves (dR/dW)^T psi = dJ/dW by GMRES(n_directions),
  * right-preconditioned with the transposed step Jacobian (block ILU(0) or
  * block Jacobi as the solvers.W preconditioner selects), restarted until

@@ -14,7 +14,7 @@ import ctypes
 from pathlib import Path
 from typing import Mapping
 
-from . import cases, mesh
+from . import cases, mesh, shape
 from ._abi import RdstError, RdstStepReport, declare, flatten_options
 from ._abi import Solver as _AbiSolver
 

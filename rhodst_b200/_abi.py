@@ -135,6 +135,7 @@ def declare(lib: ctypes.CDLL, prefix: str) -> None:
         f("adjoint_product", c_int32, [vp, dp, dp, dp])
         f("tangent_product", c_int32, [vp, dp, dp])
         f("boundary_branches", c_int32, [vp, dp, dp])
+        f("set_geometry", c_int32, [vp, POINTER(RdstMesh)])
         f("adjoint", c_int32, [vp, POINTER(RdstObjective), c_double, c_int32, c_int32, dp,
                                POINTER(RdstAdjointReport)])
 
@@ -190,22 +191,8 @@ class Solver:
                 P.nuTilda_value = 0.0
             if P.bc_nuTilda == BC_FARFIELD:
                 P.bc_nuTilda = BC_INLET_OUTLET
-        self._arrays = dict(
-            owner=np.ascontiguousarray(m.owner, dtype=np.int32),
-            neighbour=np.ascontiguousarray(m.neighbour, dtype=np.int32),
-            Sf=np.ascontiguousarray(m.Sf, dtype=np.float64), Cf=np.ascontiguousarray(m.Cf, dtype=np.float64),
-            magSf=np.ascontiguousarray(m.magSf, dtype=np.float64),
-            weights=np.ascontiguousarray(m.weights, dtype=np.float64),
-            deltaCoeffs=np.ascontiguousarray(m.deltaCoeffs, dtype=np.float64),
-            C=np.ascontiguousarray(m.C, dtype=np.float64), V=np.ascontiguousarray(m.V, dtype=np.float64))
-        wd = None if m.wall_distance is None else np.ascontiguousarray(m.wall_distance, dtype=np.float64)
-        a = self._arrays
-        cm = RdstMesh(m.n_cells, m.n_internal_faces, m.n_faces, len(m.patches),
-                      a["owner"].ctypes.data_as(POINTER(c_int32)), a["neighbour"].ctypes.data_as(POINTER(c_int32)),
-                      _dptr(a["Sf"]), _dptr(a["Cf"]), _dptr(a["magSf"]), _dptr(a["weights"]),
-                      _dptr(a["deltaCoeffs"]), _dptr(a["C"]), _dptr(a["V"]), patches,
-                      _dptr(wd) if wd is not None else None)
-        self._keep += [patches, cm, wd]
+        self._patches = patches
+        cm = self._c_mesh(m)
         flat = {}
         for k, v in options.items():
             if isinstance(v, Mapping):
@@ -218,6 +205,27 @@ class Solver:
         if st != RDST_OK:
             raise RdstError(st, f"create failed ({flat.get('fluxScheme')})")
         self.options = flat
+
+    def _c_mesh(self, m):
+        """rdst_mesh view of a PolyMesh; the arrays it points to are kept
+        alive with the solver."""
+        a = dict(
+            owner=np.ascontiguousarray(m.owner, dtype=np.int32),
+            neighbour=np.ascontiguousarray(m.neighbour, dtype=np.int32),
+            Sf=np.ascontiguousarray(m.Sf, dtype=np.float64), Cf=np.ascontiguousarray(m.Cf, dtype=np.float64),
+            magSf=np.ascontiguousarray(m.magSf, dtype=np.float64),
+            weights=np.ascontiguousarray(m.weights, dtype=np.float64),
+            deltaCoeffs=np.ascontiguousarray(m.deltaCoeffs, dtype=np.float64),
+            C=np.ascontiguousarray(m.C, dtype=np.float64), V=np.ascontiguousarray(m.V, dtype=np.float64))
+        wd = None if m.wall_distance is None else np.ascontiguousarray(m.wall_distance, dtype=np.float64)
+        cm = RdstMesh(m.n_cells, m.n_internal_faces, m.n_faces, len(m.patches),
+                      a["owner"].ctypes.data_as(POINTER(c_int32)), a["neighbour"].ctypes.data_as(POINTER(c_int32)),
+                      _dptr(a["Sf"]), _dptr(a["Cf"]), _dptr(a["magSf"]), _dptr(a["weights"]),
+                      _dptr(a["deltaCoeffs"]), _dptr(a["C"]), _dptr(a["V"]), self._patches,
+                      _dptr(wd) if wd is not None else None)
+        self._arrays = a
+        self._keep = [self._patches, cm, wd]
+        return cm
 
     # -- plumbing ---------------------------------------------------------
     def _fn(self, name):
@@ -340,6 +348,16 @@ class Solver:
         Ju = np.empty((self.n_cells, 5))
         self._check(self._fn("tangent_product")(self._h, _dptr(u), _dptr(Ju)), "tangent_product")
         return Ju
+
+    def set_geometry(self, mesh):
+        """Move the solver onto `mesh`, which has this solver's topology
+        (rdst_set_geometry); state, options and boundary values stay."""
+        old = [(p.name, p.start, p.size) for p in self.mesh.patches]
+        if [(p.name, p.start, p.size) for p in mesh.patches] != old:
+            raise ValueError("set_geometry: the new mesh's patches differ from the solver's")
+        cm = self._c_mesh(mesh)
+        self._check(self._fn("set_geometry")(self._h, ctypes.byref(cm)), "set_geometry")
+        self.mesh = mesh
 
     def boundary_branches(self):
         """(previous boundary mass flux, far-field Mach) per boundary face

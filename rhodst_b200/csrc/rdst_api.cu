@@ -57,6 +57,11 @@ struct DBuf {
         alloc(v.size());
         if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
     }
+    // copy into the existing allocation: device pointers (and graphs that hold them) stay valid
+    void overwrite(const std::vector<T>& v, cudaStream_t s) {
+        if (v.size() != n) throw std::invalid_argument("buffer size changed");
+        if (n) CK(cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
     void zero(cudaStream_t s) { if (n) CK(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
     void free_() { if (p) cudaFree(p); p = nullptr; n = 0; }
     ~DBuf() { free_(); }
@@ -150,6 +155,7 @@ struct rdst_ctx {
     DBuf<double> stage;                 // conservative fields in the caller's order (5N)
     std::vector<int> bface_orig;        // active bface -> foam face
     std::vector<double> hV, hC;         // original numbering, for forces
+    std::vector<int> hown, hnei;        // foam owner/neighbour lists (topology check of a new geometry)
     std::vector<int> hpatch_start, hpatch_size;
     std::vector<int> bface_of_face;     // foam boundary face -> active bface (or -1)
     // device mesh
@@ -350,6 +356,68 @@ int auto_ilu_parts(int N, Precision prec) {
 }
 
 // ---------------------------------------------------------------- set-up
+// Mesh metrics in the internal row order: face area vectors, centres,
+// interpolation weights and delta coefficients, owner-to-neighbour vectors,
+// cell volumes and centres, the componentwise half face-area sums of the
+// local time step (timeDST.C:117-153) and the wall distance.  With
+// `in_place` the values are copied into the buffers of an existing context
+// whose topology is unchanged, so every device pointer (and the CUDA graphs
+// that hold them) stays valid.
+void load_geometry(rdst_ctx& c, const rdst_mesh* mh, bool in_place) {
+    cudaStream_t s = c.s;
+    const int N = c.N, Fi = c.Fi, F = c.F, NB = c.NB;
+    std::vector<double> Sf(3 * (size_t)Fi), magSf(Fi), w(Fi), dc(Fi), d(3 * (size_t)Fi), Cf(3 * (size_t)Fi);
+    for (int f = 0; f < Fi; ++f) {
+        for (int k = 0; k < 3; ++k) {
+            Sf[k * (size_t)Fi + f] = mh->Sf[3 * f + k];
+            Cf[k * (size_t)Fi + f] = mh->Cf[3 * f + k];
+            d[k * (size_t)Fi + f] = mh->C[3 * mh->neighbour[f] + k] - mh->C[3 * mh->owner[f] + k];
+        }
+        magSf[f] = mh->magSf[f]; w[f] = mh->weights[f]; dc[f] = mh->deltaCoeffs[f];
+    }
+    std::vector<double> bSf(3 * (size_t)NB), bmagSf(NB), bdc(NB), bCf(3 * (size_t)NB);
+    for (int b = 0; b < NB; ++b) {
+        int f = c.bface_orig[b];
+        for (int k = 0; k < 3; ++k) {
+            bSf[k * (size_t)NB + b] = mh->Sf[3 * f + k];
+            bCf[k * (size_t)NB + b] = mh->Cf[3 * f + k];
+        }
+        bmagSf[b] = mh->magSf[f]; bdc[b] = mh->deltaCoeffs[f];
+    }
+    std::vector<double> V(N), C(3 * (size_t)N), dS(3 * (size_t)N, 0.0);
+    c.hV.assign(mh->V, mh->V + N);
+    c.hC.assign(mh->C, mh->C + 3 * (size_t)N);
+    for (int r = 0; r < N; ++r) {
+        int i = c.perm[r];
+        V[r] = mh->V[i];
+        for (int k = 0; k < 3; ++k) C[k * (size_t)N + r] = mh->C[3 * i + k];
+    }
+    // dS = 1/2 sum |Sf| componentwise (timeDST.C:117-153), non-empty faces
+    for (int f = 0; f < F; ++f) {
+        if (f >= Fi && c.bface_of_face[f - Fi] < 0) continue;
+        int ro = c.iperm[mh->owner[f]];
+        for (int k = 0; k < 3; ++k) dS[3 * ro + k] += std::fabs(mh->Sf[3 * f + k]);
+        if (f < Fi) {
+            int rn = c.iperm[mh->neighbour[f]];
+            for (int k = 0; k < 3; ++k) dS[3 * rn + k] += std::fabs(mh->Sf[3 * f + k]);
+        }
+    }
+    for (auto& x : dS) x *= 0.5;
+    std::vector<double> yv;
+    if (c.turb) {
+        yv.resize(N);
+        for (int r = 0; r < N; ++r) yv[r] = mh->wall_distance[c.perm[r]];
+    }
+    auto put = [&](DBuf<double>& b, const std::vector<double>& v) {
+        if (in_place) b.overwrite(v, s); else b.upload(v, s);
+    };
+    put(c.Sf, Sf); put(c.magSf, magSf); put(c.w, w); put(c.dc, dc); put(c.d, d); put(c.Cf, Cf);
+    put(c.bSf, bSf); put(c.bmagSf, bmagSf); put(c.bdc, bdc); put(c.bCf, bCf);
+    put(c.V, V); put(c.C, C); put(c.dS, dS);
+    if (c.turb) put(c.ywall, yv);
+    CK(cudaStreamSynchronize(s));
+}
+
 void build(rdst_ctx& c, const rdst_mesh* mh) {
     cudaStream_t s = c.s;
     const int N = mh->n_cells, Fi = mh->n_internal_faces, F = mh->n_faces;
@@ -424,48 +492,18 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     for (int r = 0; r < N; ++r) c.iperm[c.perm[r]] = r;
     // ---- device mesh
     std::vector<int> own(Fi), nei(Fi);
-    std::vector<double> Sf(3 * (size_t)Fi), magSf(Fi), w(Fi), dc(Fi), d(3 * (size_t)Fi), Cf(3 * (size_t)Fi);
     for (int f = 0; f < Fi; ++f) {
         own[f] = c.iperm[mh->owner[f]];
         nei[f] = c.iperm[mh->neighbour[f]];
-        for (int k = 0; k < 3; ++k) {
-            Sf[k * (size_t)Fi + f] = mh->Sf[3 * f + k];
-            Cf[k * (size_t)Fi + f] = mh->Cf[3 * f + k];
-            d[k * (size_t)Fi + f] = mh->C[3 * mh->neighbour[f] + k] - mh->C[3 * mh->owner[f] + k];
-        }
-        magSf[f] = mh->magSf[f]; w[f] = mh->weights[f]; dc[f] = mh->deltaCoeffs[f];
     }
     std::vector<int> bcell(NB), bpatch(NB);
-    std::vector<double> bSf(3 * (size_t)NB), bmagSf(NB), bdc(NB), bCf(3 * (size_t)NB);
     for (int b = 0; b < NB; ++b) {
         int f = c.bface_orig[b];
         bcell[b] = c.iperm[mh->owner[f]];
         bpatch[b] = fpatch[f - Fi];
-        for (int k = 0; k < 3; ++k) {
-            bSf[k * (size_t)NB + b] = mh->Sf[3 * f + k];
-            bCf[k * (size_t)NB + b] = mh->Cf[3 * f + k];
-        }
-        bmagSf[b] = mh->magSf[f]; bdc[b] = mh->deltaCoeffs[f];
     }
-    std::vector<double> V(N), C(3 * (size_t)N), dS(3 * (size_t)N, 0.0);
-    c.hV.assign(mh->V, mh->V + N);
-    c.hC.assign(mh->C, mh->C + 3 * (size_t)N);
-    for (int r = 0; r < N; ++r) {
-        int i = c.perm[r];
-        V[r] = mh->V[i];
-        for (int k = 0; k < 3; ++k) C[k * (size_t)N + r] = mh->C[3 * i + k];
-    }
-    // dS = 1/2 sum |Sf| componentwise (timeDST.C:117-153), non-empty faces
-    for (int f = 0; f < F; ++f) {
-        if (f >= Fi && c.bface_of_face[f - Fi] < 0) continue;
-        int ro = c.iperm[mh->owner[f]];
-        for (int k = 0; k < 3; ++k) dS[3 * ro + k] += std::fabs(mh->Sf[3 * f + k]);
-        if (f < Fi) {
-            int rn = c.iperm[mh->neighbour[f]];
-            for (int k = 0; k < 3; ++k) dS[3 * rn + k] += std::fabs(mh->Sf[3 * f + k]);
-        }
-    }
-    for (auto& x : dS) x *= 0.5;
+    c.hown.assign(mh->owner, mh->owner + F);
+    c.hnei.assign(mh->neighbour, mh->neighbour + Fi);
     // cell -> face CSR in internal row order (codes: f < Fi internal, Fi+b boundary)
     std::vector<int> cf_start(N + 1, 0), cf_list, cc_start(N + 1, 0), cc_list;
     for (int r = 0; r < N; ++r) {
@@ -604,13 +642,13 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         c.lu_slots = MS;
     }
     // ---- upload
-    c.own.upload(own, s); c.nei.upload(nei, s); c.Sf.upload(Sf, s); c.magSf.upload(magSf, s); c.w.upload(w, s);
-    c.dc.upload(dc, s); c.d.upload(d, s); c.Cf.upload(Cf, s);
+    c.own.upload(own, s); c.nei.upload(nei, s);
     c.bcell.upload(bcell, s); c.bpatch.upload(bpatch, s);
     std::vector<int> bfo(c.bface_orig);
     c.bfaceD.upload(bfo, s);
-    c.bSf.upload(bSf, s); c.bmagSf.upload(bmagSf, s); c.bdc.upload(bdc, s); c.bCf.upload(bCf, s);
-    c.V.upload(V, s); c.C.upload(C, s); c.dS.upload(dS, s);
+    c.turb = (o.turbulence != TURB_LAMINAR);
+    if (c.turb && !mh->wall_distance) throw std::invalid_argument("Spalart-Allmaras needs the wall distance field");
+    load_geometry(c, mh, false);
     c.cf_start.upload(cf_start, s); c.cf_list.upload(cf_list, s); c.cf_slot.upload(cf_slot, s);
     c.cc_start.upload(cc_start, s); c.cc_list.upload(cc_list, s);
     c.patches.upload(dp, s);
@@ -630,12 +668,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     c.psi.alloc((size_t)QW * N); c.fcell.alloc(N); c.fl.alloc(5L * std::max(Fi, 1)); c.bfl.alloc(5L * std::max(NB, 1));
     c.R.alloc(5L * N); c.rhs.alloc(5L * N);
     c.mut.alloc(N); c.mut.zero(s); c.mut_b.alloc(std::max(NB, 1)); c.mut_b.zero(s);
-    c.turb = (o.turbulence != TURB_LAMINAR);
     if (c.turb) {
-        if (!mh->wall_distance) throw std::invalid_argument("Spalart-Allmaras needs the wall distance field");
-        std::vector<double> yv(N);
-        for (int r = 0; r < N; ++r) yv[r] = mh->wall_distance[c.perm[r]];
-        c.ywall.upload(yv, s);
         const size_t nb1 = std::max(NB, 1), fi1 = std::max(Fi, 1);
         c.nut.alloc(N); c.nut.zero(s); c.nut_b.alloc(nb1); c.nut_b.zero(s);
         c.saD.alloc(N); c.safv1.alloc(N); c.sadiag.alloc(N); c.sab.alloc(N); c.sax2.alloc(N); c.sagn.alloc(3L * N);
@@ -1507,6 +1540,25 @@ RDST_API rdst_status rdst_create(const rdst_mesh* mesh, int32_t n_options, const
     }
     *out = c.release();
     return RDST_OK;
+}
+
+RDST_API rdst_status rdst_set_geometry(rdst_ctx* c, const rdst_mesh* mesh) {
+    if (!c || !mesh) return RDST_ERR_ARG;
+    if (!mesh->owner || (c->Fi > 0 && !mesh->neighbour) || !mesh->Sf || !mesh->Cf || !mesh->magSf ||
+        !mesh->weights || !mesh->deltaCoeffs || !mesh->C || !mesh->V || (c->turb && !mesh->wall_distance))
+        return RDST_ERR_MESH;
+    return guarded(c, [&] {
+        if (mesh->n_cells != c->N || mesh->n_internal_faces != c->Fi || mesh->n_faces != c->F ||
+            mesh->n_patches != c->n_patches)
+            throw std::invalid_argument("mesh sizes differ from the context's");
+        if (!std::equal(c->hown.begin(), c->hown.end(), mesh->owner) ||
+            !std::equal(c->hnei.begin(), c->hnei.end(), mesh->neighbour))
+            throw std::invalid_argument("owner/neighbour lists differ from the context's");
+        for (int p = 0; p < c->n_patches; ++p)
+            if (mesh->patches[p].start != c->hpatch_start[p] || mesh->patches[p].size != c->hpatch_size[p])
+                throw std::invalid_argument("patch ranges differ from the context's");
+        load_geometry(*c, mesh, true);
+    });
 }
 
 RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const double* U, const double* T,

@@ -64,6 +64,11 @@ class PolyMesh:
     weights: np.ndarray = None
     deltaCoeffs: np.ndarray = None
     wall_distance: Optional[np.ndarray] = None
+    # airfoil meshes: per point, the chordwise position x_s of the surface
+    # point its grid line starts from, the side (+1 upper, -1 lower, 0 not
+    # on an airfoil grid line) and the weight with which a normal
+    # displacement of that surface point carries over to it
+    surface_map: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
 
     @property
     def n_faces(self) -> int:
@@ -443,8 +448,29 @@ def naca_cmesh(ni: int = 257, nj: int = 65, farfield: float = 20.0, first_cell: 
         out[(out == 1) & (r < 0.6)] = 0
         return out
 
-    return build_polymesh(ptsf, [("hex", cells)], classify,
+    mesh = build_polymesh(ptsf, [("hex", cells)], classify,
                           [("airfoil", WALL), ("farfield", PATCH), ("frontAndBack", EMPTY)])
+    # surface map: every point of grid line i moves with the surface point
+    # i at weight 1 - eta_j (the interpolation above is linear in y0 and the
+    # outer boundary does not depend on the surface's y)
+    i_lat = np.broadcast_to(np.arange(nip)[:, None, None], pts.shape[:3]).reshape(-1)[used]
+    e_lat = np.broadcast_to(eta[None, :, None], pts.shape[:3]).reshape(-1)[used]
+    on_air = (i_lat >= nw + 1) & (i_lat <= nw + nair - 1)
+    si = np.clip(i_lat - nw, 0, nair)
+    side = np.where(on_air, np.where(beta[si] <= math.pi, -1, 1), 0).astype(np.int8)
+    mesh.surface_map = (np.where(on_air, xs[si], 0.0), side, np.where(on_air, 1.0 - e_lat, 0.0))
+    return mesh
+
+
+def moved(mesh: PolyMesh, points: np.ndarray) -> PolyMesh:
+    """The mesh with its points replaced (same faces, cells, patches and
+    numbering) and its geometry recomputed; the wall distance is recomputed
+    from the wall patches when the mesh carries one."""
+    out = dataclasses.replace(mesh, points=np.ascontiguousarray(points, dtype=np.float64))
+    compute_geometry(out)
+    if mesh.wall_distance is not None:
+        out.wall_distance = wall_distance(out, [p.name for p in mesh.patches if p.type == WALL])
+    return out
 
 
 def _two_stage(n: int, first: float, ratio: float) -> np.ndarray:

@@ -50,9 +50,11 @@ def test_tangent_matches_complex_step_far_field(flux, limiter):
     assert err <= 1e-9, (flux, limiter, err)
 
 
-def complex_step_gradient(case, W, branches, patch, direction, p_ref, hops):
-    """dJ/dU_patch by complex step: J assembled by coloured columns, sparse
-    direct solve of J^T psi = dJ/dW, dJ/dU = dJ/dU|explicit - psi^T dR/dU."""
+def complex_step_adjoint(case, W, branches, patch, direction, p_ref, hops):
+    """psi of the complex-step reference: the Jacobian assembled by
+    coloured columns and dJ/dW by complex step, sparse direct solve of
+    J^T psi = dJ/dW.  Returns (ComplexStep on the case's mesh, W as N x 5,
+    psi as N x 5)."""
     o = OracleSolver(case.mesh, case.bcs, case.options)
     o.set_conservative(*W)
     cs = ComplexStep(o)
@@ -91,6 +93,14 @@ def complex_step_gradient(case, W, branches, patch, direction, p_ref, hops):
         u[:, comp] = 1.0
         _, _, cells = cs.objective(Wa, patch, direction, p_ref=p_ref, u=u, branches=branches, per_cell=True)
         dJdW[:, comp] = cells
+    psi = spla.spsolve(Jm.T.tocsc(), dJdW.ravel())
+    return cs, Wa, psi.reshape(N, 5)
+
+
+def complex_step_gradient(case, W, branches, patch, direction, p_ref, hops):
+    """dJ/dU_patch by complex step: dJ/dU = dJ/dU|explicit - psi^T dR/dU."""
+    cs, Wa, psi = complex_step_adjoint(case, W, branches, patch, direction, p_ref, hops)
+    N = case.mesh.n_cells
     dRdU = np.zeros((5 * N, 3))
     dJdU = np.zeros(3)
     for m in range(3):
@@ -99,8 +109,7 @@ def complex_step_gradient(case, W, branches, patch, direction, p_ref, hops):
         _, dR = cs.residual(Wa, None, e, branches=branches)
         dRdU[:, m] = dR.ravel()
         dJdU[m] = cs.objective(Wa, patch, direction, p_ref=p_ref, dU=e, branches=branches)[1]
-    psi = spla.spsolve(Jm.T.tocsc(), dJdW.ravel())
-    return dJdU - dRdU.T @ psi
+    return dJdU - dRdU.T @ psi.ravel()
 
 
 @pytest.mark.parametrize("flux", ["Kurganov", "HLL"])
