@@ -183,14 +183,16 @@ rdst_status rdst_forces(rdst_ctx* ctx, int32_t patch, const double lift_dir[3],
  * ctx == NULL: the message of the calling thread's last failing
  * context-free call (rdst_residual_norms_noalloc). */
 
-/* ---- discrete adjoint of the steady residual (inviscid) ----
+/* ---- discrete adjoint of the steady residual ----
  * No counterpart in the reference: rhoDST has no adjoint.  R(W) is the
  * per-unit-volume residual that rdst_residual returns (no pseudo-time
- * term); it depends on the patch velocity values U_patch (the U_value of
- * every patch, so far field, inlet and outlet together: the free stream).
- * In/outflow and sub/supersonic branches of the boundary conditions are
- * held at the current state's.  Transport and turbulence options are
- * rejected with RDST_ERR_UNSUPPORTED.
+ * term), convective and -- with transport options set -- viscous terms,
+ * muEff = mu(T) + mu_t with mu_t frozen at the last turbulence update
+ * (frozen-turbulence adjoint; the turbulence model is not linearized).  It
+ * depends on the patch velocity values U_patch: the U_value of every patch
+ * that is not a wall, so far field, inlet and outlet together (the free
+ * stream); a wall's velocity is held.  In/outflow and sub/supersonic
+ * branches of the boundary conditions are held at the current state's.
  *
  * Objective: the pressure force of one patch along a direction,
  *   J = scale * sum_{faces b of patch} (p_b - p_ref) S_b . direction

@@ -1,4 +1,6 @@
-// adjoint.cuh -- discrete adjoint of the inviscid residual.
+// adjoint.cuh -- discrete adjoint of the steady residual (convective terms
+// and, with transport options set, the viscous terms of calcFields at frozen
+// turbulent viscosity).
 //
 // u = (dR/dW)^T v for the per-unit-volume residual R(W) of the step
 // (reconstruction, Gauss gradients, Venkatakrishnan/TVD limiters, the seven
@@ -20,6 +22,11 @@
 //                 in/outflow and sub/supersonic branches) -> the adjacent
 //                 cell's W and the patch velocity values;
 //   k_adj_finish  per cell: boundary contributions gathered.
+// With the viscous terms, k_adj_visc_faces / k_adj_visc_bfaces run first (VJP
+// of the face terms wrt the cell velocities, velocity gradients, muEff and
+// the convective face velocity Up, whose bar feeds k_adj_faces/k_adj_bfaces),
+// k_adj_visc_cells gathers the per-cell bars, and k_adj_gather transposes the
+// Gauss gradient of U as well (muEff = mu(T) + frozen mu_t).
 // Every kernel writes only its own face or cell: no atomics, deterministic.
 // The adjoint of the reference's step has no counterpart in the reference.
 #pragma once
@@ -30,6 +37,8 @@ namespace rdst {
 
 constexpr int ADJ_FB = 16;   // per internal face: xbar owner side [7], neighbour side [7], fs bar
 constexpr int ADJ_QB = 8;    // per cell: q bar [7], p bar
+constexpr int ADJ_VF = 32;   // per internal face, viscous input bars: UP[3], UQ[3], gP[9], gQ[9], muP, muQ, Up[3]
+constexpr int ADJ_VBF = 20;  // per boundary face, viscous input bars: Ub[3], UP[3], gP[9], mub, Up[3]
 
 // prim (p, T, h, U) and rho of a cell from W, as the field update computes them
 template <typename T>
@@ -77,14 +86,154 @@ __device__ __forceinline__ double adj_fdot(const FFluxT<Dual<K>>& F, const doubl
            Fb[4] * F.phiEp.d[k];
 }
 
+// sum_j Upbar_j dUp_j (the viscous energy term's use of the face velocity)
+template <int K>
+__device__ __forceinline__ double adj_updot(const FFluxT<Dual<K>>& F, const double* Upb, int k) {
+    return Upb ? Upb[0] * F.Up.x.d[k] + Upb[1] * F.Up.y.d[k] + Upb[2] * F.Up.z.d[k] : 0.0;
+}
+
+// ---------------------------------------------------------------- viscous
+// VJP of visc_face per internal face: bars of its 29 inputs for the output
+// bar of R_P -= (lap + tauS, sig) / V_P, R_Q += (...) / V_Q; forward mode in
+// chunks of 8 inputs.
+__global__ void __launch_bounds__(128) k_adj_visc_faces(DevMesh m, const double* __restrict__ q,
+                                                        const double* __restrict__ prim, const double* __restrict__ gU,
+                                                        const double* __restrict__ up, const double* __restrict__ v,
+                                                        double* __restrict__ vfbar) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.Fi) return;
+    const int P = m.own[f], Q = m.nei[f];
+    const double w = m.w[f], dc = m.dc[f], magS = m.magSf[f];
+    const V3 S = ldv3(m.Sf, m.Fi, f);
+    const V3 kc = sub3(div3(S, magS), scl3(dc, ldv3(m.d, m.Fi, f)));
+    const double VP = m.V[P], VQ = m.V[Q];
+    double bo[7];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) bo[j] = bo[3 + j] = v[5 * Q + 1 + j] / VQ - v[5 * P + 1 + j] / VP;
+    bo[6] = v[5 * Q + 4] / VQ - v[5 * P + 4] / VP;
+    double in[29];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        in[j] = prim[PW * P + 3 + j]; in[3 + j] = prim[PW * Q + 3 + j]; in[26 + j] = up[3 * f + j];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { in[6 + k] = gU[9 * P + k]; in[15 + k] = gU[9 * Q + k]; }
+    in[24] = q[QW * P + 7]; in[25] = q[QW * Q + 7];
+    double* out = vfbar + ADJ_VF * f;
+    using D = Dual<8>;
+    for (int k0 = 0; k0 < 29; k0 += 8) {
+        D UP[3], UQ[3], gP[9], gQ[9], Up[3], o[7];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            UP[j] = D::seed(in[j], j - k0); UQ[j] = D::seed(in[3 + j], 3 + j - k0);
+            Up[j] = D::seed(in[26 + j], 26 + j - k0);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { gP[k] = D::seed(in[6 + k], 6 + k - k0); gQ[k] = D::seed(in[15 + k], 15 + k - k0); }
+        const D muP = D::seed(in[24], 24 - k0), muQ = D::seed(in[25], 25 - k0);
+        visc_face(S, magS, w, dc, kc, UP, UQ, gP, gQ, muP, muQ, Up, o);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k0 + k >= 29) break;
+            double a = 0.0;
+#pragma unroll
+            for (int t = 0; t < 7; ++t) a += bo[t] * o[t].d[k];
+            out[k0 + k] = a;
+        }
+    }
+    out[29] = out[30] = out[31] = 0.0;
+}
+
+// VJP of visc_bface per boundary face (19 inputs)
+__global__ void k_adj_visc_bfaces(DevMesh m, const double* __restrict__ qb, const double* __restrict__ prim,
+                                  const double* __restrict__ gU, const double* __restrict__ bs,
+                                  const double* __restrict__ bup, const double* __restrict__ v,
+                                  double* __restrict__ vbbar) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.NB) return;
+    const int P = m.bcell[b];
+    const double* B = bs + BW * b;
+    const double VP = m.V[P];
+    double bo[7];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) bo[j] = bo[3 + j] = -v[5 * P + 1 + j] / VP;
+    bo[6] = -v[5 * P + 4] / VP;
+    double in[19];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { in[j] = B[12 + j]; in[3 + j] = prim[PW * P + 3 + j]; in[16 + j] = bup[3 * b + j]; }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) in[6 + k] = gU[9 * P + k];
+    in[15] = qb[QW * b + 7];
+    const V3 S = ldv3(m.bSf, m.NB, b);
+    const double magS = m.bmagSf[b], dc = m.bdc[b];
+    double* out = vbbar + ADJ_VBF * b;
+    using D = Dual<8>;
+    for (int k0 = 0; k0 < 19; k0 += 8) {
+        D Ub[3], UP[3], gP[9], Up[3], o[7];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            Ub[j] = D::seed(in[j], j - k0); UP[j] = D::seed(in[3 + j], 3 + j - k0); Up[j] = D::seed(in[16 + j], 16 + j - k0);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) gP[k] = D::seed(in[6 + k], 6 + k - k0);
+        const D mub = D::seed(in[15], 15 - k0);
+        visc_bface(S, magS, dc, Ub, UP, gP, mub, Up, o);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k0 + k >= 19) break;
+            double a = 0.0;
+#pragma unroll
+            for (int t = 0; t < 7; ++t) a += bo[t] * o[t].d[k];
+            out[k0 + k] = a;
+        }
+    }
+    out[19] = 0.0;
+}
+
+// Per cell: the viscous input bars of its faces gathered -- velocity
+// gradient bar gUbar (9) and the direct bars of its velocity and muEff
+// (ucbar: U[3], mu).
+__global__ void k_adj_visc_cells(DevMesh m, const double* __restrict__ vfbar, const double* __restrict__ vbbar,
+                                 double* __restrict__ gUbar, double* __restrict__ ucbar) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m.N) return;
+    double gb[9], ub[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gb[k] = 0.0;
+    for (int kk = m.cf_start[j]; kk < m.cf_start[j + 1]; ++kk) {
+        const int code = m.cf_list[kk];
+        if (code < m.Fi) {
+            const double* r = vfbar + ADJ_VF * code;
+            const bool own = m.own[code] == j;
+            const int u0 = own ? 0 : 3, g0 = own ? 6 : 15;
+#pragma unroll
+            for (int t = 0; t < 3; ++t) ub[t] += r[u0 + t];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) gb[k] += r[g0 + k];
+            ub[3] += r[own ? 24 : 25];
+        } else {
+            const double* r = vbbar + ADJ_VBF * (code - m.Fi);
+#pragma unroll
+            for (int t = 0; t < 3; ++t) ub[t] += r[3 + t];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) gb[k] += r[6 + k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gUbar[9 * j + k] = gb[k];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) ucbar[4 * j + t] = ub[t];
+}
+
 // ---------------------------------------------------------------- faces
 __global__ void __launch_bounds__(128) k_adj_faces(DevMesh m, Thermo th, int scheme, int lr, int lu, int lt,
                                                    int lowMach, double Mainf, const double* __restrict__ q,
                                                    const double* __restrict__ g, const double* __restrict__ psi,
                                                    const double* __restrict__ fcell, const double* __restrict__ v,
-                                                   double* __restrict__ fbar) {
+                                                   const double* __restrict__ vfbar, double* __restrict__ fbar) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.Fi) return;
+    const double* Upb = vfbar ? vfbar + ADJ_VF * f + 26 : nullptr;
     const int o = m.own[f], n = m.nei[f];
     const double wf = m.w[f];
     const V3 S = ldv3(m.Sf, m.Fi, f);
@@ -106,8 +255,8 @@ __global__ void __launch_bounds__(128) k_adj_faces(DevMesh m, Thermo th, int sch
         b.rPsi = D(sn.rPsi); b.e = D(sn.e); b.s = D(sn.s);
         const FFluxT<D> F = face_flux(scheme, a, b, S, magS, th.gamma, D::seed(fs, 7), lowMach != 0, Mainf);
 #pragma unroll
-        for (int k = 0; k < 7; ++k) out[k] = adj_fdot(F, Fb, k);
-        out[14] = adj_fdot(F, Fb, 7);
+        for (int k = 0; k < 7; ++k) out[k] = adj_fdot(F, Fb, k) + adj_updot(F, Upb, k);
+        out[14] = adj_fdot(F, Fb, 7) + adj_updot(F, Upb, 7);
     }
     {   // neighbour side
         using D = Dual<7>;
@@ -117,16 +266,18 @@ __global__ void __launch_bounds__(128) k_adj_faces(DevMesh m, Thermo th, int sch
         const SideStateT<D> b = adj_side<7>(sn, 0);
         const FFluxT<D> F = face_flux(scheme, a, b, S, magS, th.gamma, D(fs), lowMach != 0, Mainf);
 #pragma unroll
-        for (int k = 0; k < 7; ++k) out[7 + k] = adj_fdot(F, Fb, k);
+        for (int k = 0; k < 7; ++k) out[7 + k] = adj_fdot(F, Fb, k) + adj_updot(F, Upb, k);
     }
     out[15] = 0.0;
 }
 
 // boundary faces: F(qb, qb), both sides carry the boundary record
 __global__ void k_adj_bfaces(DevMesh m, Thermo th, int scheme, int lowMach, double Mainf,
-                             const double* __restrict__ qb, const double* __restrict__ v, double* __restrict__ qbbar) {
+                             const double* __restrict__ qb, const double* __restrict__ v,
+                             const double* __restrict__ vbbar, double* __restrict__ qbbar) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.NB) return;
+    const double* Upb = vbbar ? vbbar + ADJ_VBF * b + 16 : nullptr;
     using D = Dual<7>;
     const double* qq = qb + QW * b;
     SideState s;
@@ -139,7 +290,7 @@ __global__ void k_adj_bfaces(DevMesh m, Thermo th, int scheme, int lowMach, doub
     for (int k = 0; k < 5; ++k) Fb[k] = v[5 * c + k] / m.V[c];
     double* out = qbbar + ADJ_QB * b;
 #pragma unroll
-    for (int k = 0; k < 7; ++k) out[k] = adj_fdot(F, Fb, k);
+    for (int k = 0; k < 7; ++k) out[k] = adj_fdot(F, Fb, k) + adj_updot(F, Upb, k);
     out[7] = 0.0;
 }
 
@@ -384,18 +535,25 @@ __global__ void __launch_bounds__(128) k_adj_cells(DevMesh m, int scheme, int lr
 // then the VJP of the recon record q(W_j) (and of p) to W_j.  Boundary faces
 // of j receive their gradient and record shares in qbbar (only cell j
 // writes them).
-__global__ void __launch_bounds__(128) k_adj_gather(DevMesh m, Thermo th, Bounds bd, int use_c,
+__global__ void __launch_bounds__(128) k_adj_gather(DevMesh m, Thermo th, Bounds bd, Transport tr, int use_c,
                                                     const double* __restrict__ W, const double* __restrict__ gbar,
                                                     const double* __restrict__ qbar, const int* __restrict__ vrec_idx,
                                                     const double* __restrict__ vrec_val,
                                                     const int* __restrict__ hrec_idx,
-                                                    const double* __restrict__ hrec_val, double* __restrict__ qbbar,
+                                                    const double* __restrict__ hrec_val,
+                                                    const double* __restrict__ gUbar, const double* __restrict__ ucbar,
+                                                    double* __restrict__ vbbar, double* __restrict__ qbbar,
                                                     double* __restrict__ wbar) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= m.N) return;
     double qa[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) qa[k] = qbar[ADJ_QB * j + k];
+    double ua[4] = {0, 0, 0, 0};      // viscous: velocity bar [3], muEff bar
+    if (gUbar) {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) ua[t] = ucbar[4 * j + t];
+    }
     const double Vj = m.V[j];
     const int k0 = m.cf_start[j], k1 = m.cf_start[j + 1];
     for (int kk = k0; kk < k1; ++kk) {
@@ -413,6 +571,16 @@ __global__ void __launch_bounds__(128) k_adj_gather(DevMesh m, Thermo th, Bounds
                 const double xf = (S.x * go[3 * fld] + S.y * go[3 * fld + 1] + S.z * go[3 * fld + 2]) / Vo -
                                   (S.x * gn[3 * fld] + S.y * gn[3 * fld + 1] + S.z * gn[3 * fld + 2]) / Vn;
                 qa[fld] += coef * xf;
+            }
+            if (gUbar) {    // Gauss gradient of U: (grad U)_dj += S_d U_f,j / V, U_f = w U_o + (1 - w) U_n
+                const double* uo = gUbar + 9 * o;
+                const double* un = gUbar + 9 * n;
+#pragma unroll
+                for (int jc = 0; jc < 3; ++jc) {
+                    const double xf = (S.x * uo[jc] + S.y * uo[3 + jc] + S.z * uo[6 + jc]) / Vo -
+                                      (S.x * un[jc] + S.y * un[3 + jc] + S.z * un[6 + jc]) / Vn;
+                    ua[jc] += coef * xf;
+                }
             }
             // a neighbour's records count once, also when several faces
             // join the pair
@@ -438,6 +606,12 @@ __global__ void __launch_bounds__(128) k_adj_gather(DevMesh m, Thermo th, Bounds
                 if (vrec_idx[7 * j + fld] == -2 - b) add += vrec_val[7 * j + fld];
                 qbb[fld] += add;
             }
+            if (gUbar) {    // the boundary velocity's share of j's velocity gradient
+                const double* uj = gUbar + 9 * j;
+                double* vb = vbbar + ADJ_VBF * b;
+#pragma unroll
+                for (int jc = 0; jc < 3; ++jc) vb[jc] += (S.x * uj[jc] + S.y * uj[3 + jc] + S.z * uj[6 + jc]) / Vj;
+            }
         }
     }
     // q(W_j), p(W_j) VJP
@@ -450,11 +624,13 @@ __global__ void __launch_bounds__(128) k_adj_gather(DevMesh m, Thermo th, Bounds
     adj_prim(th, bd, Wd, rho, p, Tt, h, U);
     D qd[7];
     adj_qrec(th, use_c, Wd[0], mkv(Wd[1], Wd[2], Wd[3]), Wd[4], p, Tt, h, qd);
+    const D mu = gUbar ? tr.mu_of(Tt) : D(0.0);
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
         double s = qa[7] * p.d[k];
 #pragma unroll
         for (int fld = 0; fld < 7; ++fld) s += qa[fld] * qd[fld].d[k];
+        if (gUbar) s += ua[0] * U.x.d[k] + ua[1] * U.y.d[k] + ua[2] * U.z.d[k] + ua[3] * mu.d[k];
         wbar[5 * j + k] = s;
     }
 }
@@ -462,9 +638,10 @@ __global__ void __launch_bounds__(128) k_adj_gather(DevMesh m, Thermo th, Bounds
 // Per boundary face: VJP of qb(bs(W_c, U_patch)) with qbbar (and, for the
 // objective, of the face pressure with pbar) -> W_c share (wbarb) and the
 // patch-velocity share (ubarb), with the branches recorded in bs.
-__global__ void k_adj_bc(DevMesh m, Thermo th, Bounds bd, int use_c, const double* __restrict__ W,
+__global__ void k_adj_bc(DevMesh m, Thermo th, Bounds bd, Transport tr, int use_c, const double* __restrict__ W,
                          const double* __restrict__ bs, const double* __restrict__ qbbar,
-                         const double* __restrict__ pbar, double* __restrict__ wbarb, double* __restrict__ ubarb) {
+                         const double* __restrict__ pbar, const double* __restrict__ vbbar,
+                         double* __restrict__ wbarb, double* __restrict__ ubarb) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.NB) return;
     const DevPatch P = m.patches[m.bpatch[b]];
@@ -477,7 +654,11 @@ __global__ void k_adj_bc(DevMesh m, Thermo th, Bounds bd, int use_c, const doubl
     D Wd[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) Wd[k] = D::seed(W[5 * c + k], k);
-    const Vec3<D> Ud = mkv(D::seed(P.U_value[0], 5), D::seed(P.U_value[1], 6), D::seed(P.U_value[2], 7));
+    // the patch velocity values of the free stream: walls' values are their
+    // own motion and are held
+    const int sU = (P.type == RDST_PATCH_WALL) ? -1 : 5;
+    const Vec3<D> Ud = mkv(D::seed(P.U_value[0], sU), D::seed(P.U_value[1], sU < 0 ? -1 : 6),
+                           D::seed(P.U_value[2], sU < 0 ? -1 : 7));
     D rho, p, Tt, h;
     Vec3<D> U;
     adj_prim(th, bd, Wd, rho, p, Tt, h, U);
@@ -499,6 +680,12 @@ __global__ void k_adj_bc(DevMesh m, Thermo th, Bounds bd, int use_c, const doubl
             for (int fld = 0; fld < 7; ++fld) s += qbb[fld] * qd[fld].d[k];
         }
         acc[k] = s;
+    }
+    if (vbbar) {    // viscous: boundary velocity and muEff_b = mu(T_b) + mu_t,b
+        const double* vb = vbbar + ADJ_VBF * b;
+        const D mub = tr.mu_of(o.Tb);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += vb[0] * o.U.x.d[k] + vb[1] * o.U.y.d[k] + vb[2] * o.U.z.d[k] + vb[15] * mub.d[k];
     }
 #pragma unroll
     for (int k = 0; k < 5; ++k) wbarb[5 * b + k] = acc[k];
@@ -634,9 +821,11 @@ __device__ __forceinline__ Tn tn_ld(const double* v, const double* d, long i) { 
 __device__ __forceinline__ void tn_st(double* v, double* d, long i, const Tn& x) { v[i] = x.v; d[i] = x.d[0]; }
 
 // cells: q record of W + eps u
-__global__ void k_tan_q(int N, Thermo th, Bounds bd, int use_c, const double* __restrict__ W,
-                        const double* __restrict__ u, double* __restrict__ qv, double* __restrict__ qd,
-                        double* __restrict__ pv, double* __restrict__ pd) {
+// (viscous: also the velocity and muEff = mu(T) + mu_t per cell, 4 each)
+__global__ void k_tan_q(int N, Thermo th, Bounds bd, Transport tr, int use_c, const double* __restrict__ W,
+                        const double* __restrict__ u, const double* __restrict__ mut, double* __restrict__ qv,
+                        double* __restrict__ qd, double* __restrict__ pv, double* __restrict__ pd,
+                        double* __restrict__ uv, double* __restrict__ ud) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     Tn Wd[5];
@@ -650,12 +839,18 @@ __global__ void k_tan_q(int N, Thermo th, Bounds bd, int use_c, const double* __
 #pragma unroll
     for (int k = 0; k < 7; ++k) tn_st(qv, qd, (long)QW * i + k, q[k]);
     tn_st(pv, pd, i, p);
+    if (uv) {
+        tn_st(uv, ud, 4L * i, U.x); tn_st(uv, ud, 4L * i + 1, U.y); tn_st(uv, ud, 4L * i + 2, U.z);
+        tn_st(uv, ud, 4L * i + 3, tr.mu_of(Tt) + mut[i]);
+    }
 }
 
 // boundary faces: boundary record of the perturbed state
-__global__ void k_tan_qb(DevMesh m, Thermo th, Bounds bd, int use_c, const double* __restrict__ W,
-                         const double* __restrict__ u, const double* __restrict__ bs, double* __restrict__ qbv,
-                         double* __restrict__ qbd) {
+// (viscous: also the boundary velocity and muEff_b, 4 per face)
+__global__ void k_tan_qb(DevMesh m, Thermo th, Bounds bd, Transport tr, int use_c, const double* __restrict__ W,
+                         const double* __restrict__ u, const double* __restrict__ bs, const double* __restrict__ mut_b,
+                         double* __restrict__ qbv, double* __restrict__ qbd, double* __restrict__ ubv,
+                         double* __restrict__ ubd) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.NB) return;
     const DevPatch P = m.patches[m.bpatch[b]];
@@ -677,6 +872,91 @@ __global__ void k_tan_qb(DevMesh m, Thermo th, Bounds bd, int use_c, const doubl
     adj_qrec(th, use_c, o.rho, scl3(o.rho, o.U), rhoE, o.p, o.Tb, hb, q);
 #pragma unroll
     for (int k = 0; k < 7; ++k) tn_st(qbv, qbd, (long)QW * b + k, q[k]);
+    if (ubv) {
+        tn_st(ubv, ubd, 4L * b, o.U.x); tn_st(ubv, ubd, 4L * b + 1, o.U.y); tn_st(ubv, ubd, 4L * b + 2, o.U.z);
+        tn_st(ubv, ubd, 4L * b + 3, tr.mu_of(o.Tb) + mut_b[b]);
+    }
+}
+
+// cells: Gauss gradient of U (k_grad's aU) from the velocity records
+__global__ void k_tan_gradU(DevMesh m, const double* __restrict__ uv, const double* __restrict__ ud,
+                            const double* __restrict__ ubv, const double* __restrict__ ubd,
+                            double* __restrict__ gUv, double* __restrict__ gUd) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.N) return;
+    Tn a[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = Tn(0.0);
+    for (int kk = m.cf_start[i]; kk < m.cf_start[i + 1]; ++kk) {
+        const int code = m.cf_list[kk];
+        if (code < m.Fi) {
+            const int o = m.own[code], n = m.nei[code];
+            const double wf = m.w[code];
+            const V3 S = ldv3(m.Sf, m.Fi, code);
+            const double sg = (o == i) ? 1.0 : -1.0;
+            const double Sv[3] = {sg * S.x, sg * S.y, sg * S.z};
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const Tn xf = wf * tn_ld(uv, ud, 4L * o + j) + (1 - wf) * tn_ld(uv, ud, 4L * n + j);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) a[3 * d + j] += Sv[d] * xf;
+            }
+        } else {
+            const int b = code - m.Fi;
+            const V3 S = ldv3(m.bSf, m.NB, b);
+            const double Sv[3] = {S.x, S.y, S.z};
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) a[3 * d + j] += Sv[d] * tn_ld(ubv, ubd, 4L * b + j);
+        }
+    }
+    const double Vi = m.V[i];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) tn_st(gUv, gUd, 9L * i + k, a[k] / Vi);
+}
+
+// internal faces: derivative of the viscous terms (8 per face)
+__global__ void k_tan_visc_faces(DevMesh m, const double* __restrict__ uv, const double* __restrict__ ud,
+                                 const double* __restrict__ gUv, const double* __restrict__ gUd,
+                                 const double* __restrict__ upv, const double* __restrict__ upd,
+                                 double* __restrict__ vfd) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.Fi) return;
+    const int P = m.own[f], Q = m.nei[f];
+    const double dc = m.dc[f], magS = m.magSf[f];
+    const V3 S = ldv3(m.Sf, m.Fi, f);
+    const V3 kc = sub3(div3(S, magS), scl3(dc, ldv3(m.d, m.Fi, f)));
+    Tn UP[3], UQ[3], gP[9], gQ[9], Up[3], o[7];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        UP[j] = tn_ld(uv, ud, 4L * P + j); UQ[j] = tn_ld(uv, ud, 4L * Q + j); Up[j] = tn_ld(upv, upd, 3L * f + j);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { gP[k] = tn_ld(gUv, gUd, 9L * P + k); gQ[k] = tn_ld(gUv, gUd, 9L * Q + k); }
+    visc_face(S, magS, m.w[f], dc, kc, UP, UQ, gP, gQ, tn_ld(uv, ud, 4L * P + 3), tn_ld(uv, ud, 4L * Q + 3), Up, o);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) vfd[8L * f + k] = o[k].d[0];
+}
+
+__global__ void k_tan_visc_bfaces(DevMesh m, const double* __restrict__ uv, const double* __restrict__ ud,
+                                  const double* __restrict__ gUv, const double* __restrict__ gUd,
+                                  const double* __restrict__ ubv, const double* __restrict__ ubd,
+                                  const double* __restrict__ bupv, const double* __restrict__ bupd,
+                                  double* __restrict__ bvfd) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.NB) return;
+    const int P = m.bcell[b];
+    Tn Ub[3], UP[3], gP[9], Up[3], o[7];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        Ub[j] = tn_ld(ubv, ubd, 4L * b + j); UP[j] = tn_ld(uv, ud, 4L * P + j); Up[j] = tn_ld(bupv, bupd, 3L * b + j);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gP[k] = tn_ld(gUv, gUd, 9L * P + k);
+    visc_bface(ldv3(m.bSf, m.NB, b), m.bmagSf[b], m.bdc[b], Ub, UP, gP, tn_ld(ubv, ubd, 4L * b + 3), Up, o);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) bvfd[8L * b + k] = o[k].d[0];
 }
 
 // cells: Gauss gradient, Venkatakrishnan limiter and HLLCP sensor (k_grad)
@@ -762,7 +1042,8 @@ __global__ void __launch_bounds__(128) k_tan_faces(DevMesh m, Thermo th, int sch
                                                    const double* __restrict__ qd, const double* __restrict__ gv,
                                                    const double* __restrict__ gd, const double* __restrict__ psv,
                                                    const double* __restrict__ psd, const double* __restrict__ fcv,
-                                                   const double* __restrict__ fcd, double* __restrict__ fld) {
+                                                   const double* __restrict__ fcd, double* __restrict__ fld,
+                                                   double* __restrict__ upv, double* __restrict__ upd) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.Fi) return;
     const int o = m.own[f], n = m.nei[f];
@@ -825,11 +1106,12 @@ __global__ void __launch_bounds__(128) k_tan_faces(DevMesh m, Thermo th, int sch
     const FFluxT<Tn> F = face_flux(scheme, a, b, S, magS, th.gamma, fs, lowMach != 0, Mainf);
     double* out = fld + 5 * f;
     out[0] = F.phi.d[0]; out[1] = F.phiUp.x.d[0]; out[2] = F.phiUp.y.d[0]; out[3] = F.phiUp.z.d[0]; out[4] = F.phiEp.d[0];
+    if (upv) { tn_st(upv, upd, 3L * f, F.Up.x); tn_st(upv, upd, 3L * f + 1, F.Up.y); tn_st(upv, upd, 3L * f + 2, F.Up.z); }
 }
 
 __global__ void k_tan_bfaces(DevMesh m, Thermo th, int scheme, int lowMach, double Mainf,
                              const double* __restrict__ qbv, const double* __restrict__ qbd,
-                             double* __restrict__ bfld) {
+                             double* __restrict__ bfld, double* __restrict__ bupv, double* __restrict__ bupd) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.NB) return;
     SideStateT<Tn> s;
@@ -840,10 +1122,15 @@ __global__ void k_tan_bfaces(DevMesh m, Thermo th, int scheme, int lowMach, doub
     const FFluxT<Tn> F = face_flux(scheme, s, s, ldv3(m.bSf, m.NB, b), m.bmagSf[b], th.gamma, Tn(1.0), lowMach != 0, Mainf);
     double* out = bfld + 5 * b;
     out[0] = F.phi.d[0]; out[1] = F.phiUp.x.d[0]; out[2] = F.phiUp.y.d[0]; out[3] = F.phiUp.z.d[0]; out[4] = F.phiEp.d[0];
+    if (bupv) {
+        tn_st(bupv, bupd, 3L * b, F.Up.x); tn_st(bupv, bupd, 3L * b + 1, F.Up.y); tn_st(bupv, bupd, 3L * b + 2, F.Up.z);
+    }
 }
 
-// cells: Ju_i = (sum_f +-dF_f + sum_b dF_b) / V_i
+// cells: Ju_i = (sum_f +-dF_f + sum_b dF_b) / V_i, less the viscous terms'
+// derivatives when given
 __global__ void k_tan_residual(DevMesh m, const double* __restrict__ fld, const double* __restrict__ bfld,
+                               const double* __restrict__ vfd, const double* __restrict__ bvfd,
                                double* __restrict__ Ju) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.N) return;
@@ -854,9 +1141,21 @@ __global__ void k_tan_residual(DevMesh m, const double* __restrict__ fld, const 
             const double sg = m.own[code] == i ? 1.0 : -1.0;
 #pragma unroll
             for (int k = 0; k < 5; ++k) a[k] += sg * fld[5 * code + k];
+            if (vfd) {
+                const double* t = vfd + 8L * code;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) a[1 + k] -= sg * (t[k] + t[3 + k]);
+                a[4] -= sg * t[6];
+            }
         } else {
 #pragma unroll
             for (int k = 0; k < 5; ++k) a[k] += bfld[5 * (code - m.Fi) + k];
+            if (bvfd) {
+                const double* t = bvfd + 8L * (code - m.Fi);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) a[1 + k] -= t[k] + t[3 + k];
+                a[4] -= t[6];
+            }
         }
     }
     const double Vi = m.V[i];

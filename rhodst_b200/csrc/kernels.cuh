@@ -78,6 +78,12 @@ struct Transport {
     __device__ __forceinline__ double mu_of_T(double T) const {
         return As > 0 ? As * sqrt(T) / (1.0 + Ts / T) : mu;
     }
+    // the same law on any scalar type (the adjoint's dual numbers)
+    template <typename T>
+    __device__ __forceinline__ T mu_of(const T& Tt) const {
+        if (As > 0) return As * sqrt(Tt) / (1.0 + Ts / Tt);
+        return T(mu);
+    }
 };
 
 // initial state from primitives (createFields.H:21-72)
@@ -539,88 +545,119 @@ __global__ void k_bface_flux(DevMesh m, Thermo th, int scheme, int lowMach, doub
 }
 
 // tau = muEff dev2(T(grad U)): t(i,j) = mu (g(j,i) - 2/3 tr(g) d_ij)
-__device__ __forceinline__ void tau_of(const double g[9], double mu, double t[9]) {
-    const double tr = g[0] + g[4] + g[8];
+template <typename T>
+__device__ __forceinline__ void tau_of(const T (&g)[9], const T& mu, T (&t)[9]) {
+    const T tr = g[0] + g[4] + g[8];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) t[3 * i + j] = mu * (g[3 * j + i] - (i == j ? (2.0 / 3.0) * tr : 0.0));
+        for (int j = 0; j < 3; ++j) {
+            T a = g[3 * j + i];
+            if (i == j) a = a - (2.0 / 3.0) * tr;
+            t[3 * i + j] = mu * a;
+        }
 }
 
-// Viscous face terms of calcFields (baseFluxDST.C:229-250) per internal
-// face: lap = muEff_f |Sf| snGrad(U) (corrected: dc (U_N - U_P) +
-// (n - d dc) . (grad U)_f), tauS = Sf . (tau)_f, sig = (lap + tauS) . Up.
+// Viscous terms of one internal face (baseFluxDST.C:229-250): lap = muEff_f
+// |Sf| snGrad(U) (corrected: dc (U_N - U_P) + (n - d dc) . (grad U)_f),
+// tauS = Sf . (tau)_f, sig = (lap + tauS) . Up; out = (lap[3], tauS[3], sig).
+// Inputs: cell velocities, velocity gradients (g_ij = dU_j/dx_i), muEff of
+// both cells and the face velocity Up of the convective flux.
+template <typename T>
+__device__ __forceinline__ void visc_face(const V3& S, double magS, double w, double dc, const V3& kc, const T (&UP)[3],
+                                          const T (&UQ)[3], const T (&gP)[9], const T (&gQ)[9], const T& muP,
+                                          const T& muQ, const T (&Up)[3], T (&out)[7]) {
+    const T muf = w * muP + (1 - w) * muQ;
+    T tP[9], tQ[9];
+    tau_of(gP, muP, tP);
+    tau_of(gQ, muQ, tQ);
+    const double kv[3] = {kc.x, kc.y, kc.z}, Sv[3] = {S.x, S.y, S.z};
+    T lap[3], ts[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        T corr(0.0), a(0.0);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            corr += kv[i] * (w * gP[3 * i + j] + (1 - w) * gQ[3 * i + j]);
+            a += Sv[i] * (w * tP[3 * i + j] + (1 - w) * tQ[3 * i + j]);
+        }
+        const T sn = dc * (UQ[j] - UP[j]) + corr;
+        lap[j] = (muf * magS) * sn;
+        ts[j] = a;
+    }
+    out[6] = (lap[0] + ts[0]) * Up[0] + (lap[1] + ts[1]) * Up[1] + (lap[2] + ts[2]) * Up[2];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { out[j] = lap[j]; out[3 + j] = ts[j]; }
+}
+
+// Viscous terms of one boundary face: snGrad = (U_b - U_P) dc_b, the cell
+// gradient corrected to the patch snGrad (gaussGrad::correctBoundaryConditions),
+// tau_b from muEff_b.  Same outputs as visc_face.
+template <typename T>
+__device__ __forceinline__ void visc_bface(const V3& S, double magS, double dc, const T (&Ub)[3], const T (&UP)[3],
+                                           const T (&gP)[9], const T& mub, const T (&Up)[3], T (&out)[7]) {
+    const double n[3] = {S.x / magS, S.y / magS, S.z / magS}, Sv[3] = {S.x, S.y, S.z};
+    T snb[3], g[9], t[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) snb[j] = dc * (Ub[j] - UP[j]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) g[k] = gP[k];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const T ng = n[0] * g[j] + n[1] * g[3 + j] + n[2] * g[6 + j];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g[3 * i + j] += n[i] * (snb[j] - ng);
+    }
+    tau_of(g, mub, t);
+    T lap[3], ts[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        ts[j] = Sv[0] * t[j] + Sv[1] * t[3 + j] + Sv[2] * t[6 + j];
+        lap[j] = (mub * magS) * snb[j];
+    }
+    out[6] = (lap[0] + ts[0]) * Up[0] + (lap[1] + ts[1]) * Up[1] + (lap[2] + ts[2]) * Up[2];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { out[j] = lap[j]; out[3 + j] = ts[j]; }
+}
+
+// Viscous face terms per internal face (visc_face on the cell records).
 __global__ void __launch_bounds__(128) k_visc_faces(DevMesh m, const double* __restrict__ q, const double* __restrict__ prim,
                                                     const double* __restrict__ gU, const double* __restrict__ up,
                                                     double* __restrict__ vf) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.Fi) return;
     const int P = m.own[f], Q = m.nei[f];
-    const double w = m.w[f], dc = m.dc[f], magS = m.magSf[f];
+    const double dc = m.dc[f], magS = m.magSf[f];
     const V3 S = ldv3(m.Sf, m.Fi, f);
-    const V3 n = div3(S, magS);
-    const V3 d = ldv3(m.d, m.Fi, f);
-    const V3 kc = sub3(n, scl3(dc, d));
-    const double muP = q[QW * P + 7], muQ = q[QW * Q + 7];
-    const double muf = w * muP + (1 - w) * muQ;
-    double gP[9], gQ[9], tP[9], tQ[9];
+    const V3 kc = sub3(div3(S, magS), scl3(dc, ldv3(m.d, m.Fi, f)));
+    double UP[3], UQ[3], gP[9], gQ[9], Up[3], out[7];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { UP[j] = prim[PW * P + 3 + j]; UQ[j] = prim[PW * Q + 3 + j]; Up[j] = up[3 * f + j]; }
 #pragma unroll
     for (int k = 0; k < 9; ++k) { gP[k] = gU[9 * P + k]; gQ[k] = gU[9 * Q + k]; }
-    tau_of(gP, muP, tP);
-    tau_of(gQ, muQ, tQ);
-    const double kv[3] = {kc.x, kc.y, kc.z}, Sv[3] = {S.x, S.y, S.z};
-    double lap[3], ts[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        double corr = 0, a = 0;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            corr += kv[i] * (w * gP[3 * i + j] + (1 - w) * gQ[3 * i + j]);
-            a += Sv[i] * (w * tP[3 * i + j] + (1 - w) * tQ[3 * i + j]);
-        }
-        double sn = dc * (prim[PW * Q + 3 + j] - prim[PW * P + 3 + j]) + corr;
-        lap[j] = (muf * magS) * sn;
-        ts[j] = a;
-    }
-    double sig = (lap[0] + ts[0]) * up[3 * f] + (lap[1] + ts[1]) * up[3 * f + 1] + (lap[2] + ts[2]) * up[3 * f + 2];
+    visc_face(S, magS, m.w[f], dc, kc, UP, UQ, gP, gQ, q[QW * P + 7], q[QW * Q + 7], Up, out);
     double* o = vf + 8 * f;
-    o[0] = lap[0]; o[1] = lap[1]; o[2] = lap[2]; o[3] = ts[0]; o[4] = ts[1]; o[5] = ts[2]; o[6] = sig;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) o[k] = out[k];
 }
 
-// boundary faces: snGrad = (U_b - U_P) dc_b, gradient corrected to the
-// patch snGrad (gaussGrad::correctBoundaryConditions), tau_b from muEff_b
+// boundary faces (visc_bface on the boundary record and the cell's records)
 __global__ void k_visc_bfaces(DevMesh m, const double* __restrict__ qb, const double* __restrict__ prim,
                               const double* __restrict__ gU, const double* __restrict__ bs,
                               const double* __restrict__ bup, double* __restrict__ bvf) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.NB) return;
     const int P = m.bcell[b];
-    const double magS = m.bmagSf[b], dc = m.bdc[b];
-    const V3 S = ldv3(m.bSf, m.NB, b);
-    const double n[3] = {S.x / magS, S.y / magS, S.z / magS}, Sv[3] = {S.x, S.y, S.z};
     const double* B = bs + BW * b;
-    double snb[3], g[9], t[9];
+    double Ub[3], UP[3], gP[9], Up[3], out[7];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) snb[j] = dc * (B[12 + j] - prim[PW * P + 3 + j]);
+    for (int j = 0; j < 3; ++j) { Ub[j] = B[12 + j]; UP[j] = prim[PW * P + 3 + j]; Up[j] = bup[3 * b + j]; }
 #pragma unroll
-    for (int k = 0; k < 9; ++k) g[k] = gU[9 * P + k];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        double ng = n[0] * g[j] + n[1] * g[3 + j] + n[2] * g[6 + j];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) g[3 * i + j] += n[i] * (snb[j] - ng);
-    }
-    const double mub = qb[QW * b + 7];
-    tau_of(g, mub, t);
-    double lap[3], ts[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        ts[j] = Sv[0] * t[j] + Sv[1] * t[3 + j] + Sv[2] * t[6 + j];
-        lap[j] = (mub * magS) * snb[j];
-    }
-    double sig = (lap[0] + ts[0]) * bup[3 * b] + (lap[1] + ts[1]) * bup[3 * b + 1] + (lap[2] + ts[2]) * bup[3 * b + 2];
+    for (int k = 0; k < 9; ++k) gP[k] = gU[9 * P + k];
+    visc_bface(ldv3(m.bSf, m.NB, b), m.bmagSf[b], m.bdc[b], Ub, UP, gP, qb[QW * b + 7], Up, out);
     double* o = bvf + 8 * b;
-    o[0] = lap[0]; o[1] = lap[1]; o[2] = lap[2]; o[3] = ts[0]; o[4] = ts[1]; o[5] = ts[2]; o[6] = sig;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) o[k] = out[k];
 }
 
 // calcFields (baseFluxDST.C:223-255): R = div(face fluxes) per unit volume,

@@ -197,6 +197,7 @@ struct rdst_ctx {
     DBuf<double> a_r, a_z, a_t, a_psi, a_rhs, a_V, a_tmp, a_u3;
     DBuf<int> a_vidx, a_hidx;
     DBuf<double> a_Z;               // flexible-GMRES preconditioned directions
+    DBuf<double> a_vfbar, a_vbbar, a_gUbar, a_ucbar;   // viscous input bars (faces, boundary faces, cells)
     DBuf<Scalars> a_sc;             // Hessenberg and rotations of the adjoint's outer solve
     void* a_AT = nullptr;           // transposed Jacobian (storage type of A)
     DBuf<double> t_buf;             // tangent records (value, derivative)
@@ -1251,6 +1252,11 @@ void adj_alloc(rdst_ctx& c, int m) {
         c.a_r.alloc(n5); c.a_z.alloc(n5); c.a_t.alloc(n5); c.a_psi.alloc(n5); c.a_rhs.alloc(n5);
         c.a_tmp.alloc(n5); c.a_u3.alloc(16);
         c.a_fbar.zero(c.s); c.a_qbbar.zero(c.s);
+        if (c.tr.viscous) {
+            c.a_vfbar.alloc((size_t)ADJ_VF * std::max(c.Fi, 1)); c.a_vbbar.alloc((size_t)ADJ_VBF * std::max(c.NB, 1));
+            c.a_gUbar.alloc(9L * c.N); c.a_ucbar.alloc(4L * c.N);
+            c.a_vfbar.zero(c.s); c.a_vbbar.zero(c.s);
+        }
     }
     if (m > 0 && c.a_m != m) {
         c.a_V.alloc((size_t)(m + 1) * c.ldv);
@@ -1269,15 +1275,28 @@ void adj_product(rdst_ctx& c, const double* v, double* u, double* usum) {
     const Options& o = c.o;
     cudaStream_t s = c.s;
     const int use_c = adj_use_c(c);
+    const bool visc = c.tr.viscous != 0;
+    double* vfbar = visc ? c.a_vfbar.p : nullptr;
+    double* vbbar = visc ? c.a_vbbar.p : nullptr;
+    if (visc) {     // viscous face terms first: their face-velocity bars feed the convective VJP
+        if (m.Fi > 0) {
+            k_adj_visc_faces<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.q.p, c.prim.p, c.gU.p, c.up.p, v, vfbar);
+            CKL();
+        }
+        if (m.NB > 0) {
+            k_adj_visc_bfaces<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.qb.p, c.prim.p, c.gU.p, c.bs.p, c.bup.p, v, vbbar);
+            CKL();
+        }
+    }
     if (m.Fi > 0) {
         k_adj_faces<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
                                                    lim_code(o.lim_T), o.low_mach, o.mainf, c.q.p, c.g.p, c.psi.p,
-                                                   c.fcell.p, v, c.a_fbar.p);
+                                                   c.fcell.p, v, vfbar, c.a_fbar.p);
         CKL();
     }
     if (m.NB > 0) {
         k_adj_bfaces<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), o.low_mach, o.mainf, c.qb.p, v,
-                                                     c.a_qbbar.p);
+                                                     vbbar, c.a_qbbar.p);
         CKL();
     }
     k_adj_cells<<<nblk(m.N, 128), 128, 0, s>>>(m, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
@@ -1285,11 +1304,16 @@ void adj_product(rdst_ctx& c, const double* v, double* u, double* usum) {
                                                c.psi.p, c.fcell.p, c.prim.p, c.a_fbar.p, c.a_qbar.p, c.a_gbar.p,
                                                c.a_vidx.p, c.a_vval.p, c.a_hidx.p, c.a_hval.p);
     CKL();
-    k_adj_gather<<<nblk(m.N, 128), 128, 0, s>>>(m, c.th, c.bd, use_c, c.W.p, c.a_gbar.p, c.a_qbar.p, c.a_vidx.p,
-                                                c.a_vval.p, c.a_hidx.p, c.a_hval.p, c.a_qbbar.p, c.a_wbar.p);
+    if (visc) {
+        k_adj_visc_cells<<<nblk(m.N, 128), 128, 0, s>>>(m, vfbar, vbbar, c.a_gUbar.p, c.a_ucbar.p);
+        CKL();
+    }
+    k_adj_gather<<<nblk(m.N, 128), 128, 0, s>>>(m, c.th, c.bd, c.tr, use_c, c.W.p, c.a_gbar.p, c.a_qbar.p, c.a_vidx.p,
+                                                c.a_vval.p, c.a_hidx.p, c.a_hval.p, visc ? c.a_gUbar.p : nullptr,
+                                                visc ? c.a_ucbar.p : nullptr, vbbar, c.a_qbbar.p, c.a_wbar.p);
     CKL();
     if (m.NB > 0) {
-        k_adj_bc<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, use_c, c.W.p, c.bs.p, c.a_qbbar.p, nullptr,
+        k_adj_bc<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, c.tr, use_c, c.W.p, c.bs.p, c.a_qbbar.p, nullptr, vbbar,
                                                  c.a_wbarb.p, c.a_ubarb.p);
         CKL();
     }
@@ -1319,8 +1343,8 @@ void adj_objective(rdst_ctx& c, const rdst_objective& ob, double* dJdW, double o
     CKL();
     k_adj_psum<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, 4, c.a_u3.p); CKL();
     if (m.NB > 0) {
-        k_adj_bc<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, adj_use_c(c), c.W.p, c.bs.p, nullptr, c.a_pbar.p,
-                                                 c.a_wbarb.p, c.a_ubarb.p);
+        k_adj_bc<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, c.tr, adj_use_c(c), c.W.p, c.bs.p, nullptr, c.a_pbar.p,
+                                                 nullptr, c.a_wbarb.p, c.a_ubarb.p);
         CKL();
         const int nbu = red_blocks(m.NB);
         k_adj_usum<<<nbu, RED_TPB, 0, s>>>(m.NB, c.a_ubarb.p, c.partial.p); CKL();
@@ -1448,8 +1472,6 @@ int adj_solve(rdst_ctx& c, const double* rhs, double* psi, double rel_tol, int m
 // branches are those of the last boundary evaluation) at the current W
 template <typename MT>
 void adj_forward(rdst_ctx& c) {
-    if (c.tr.viscous)
-        throw ConfigError("adjoint: only the inviscid residual is differentiated (transport/turbulence set)", true);
     Ops<MT>::flux(c);
 }
 
@@ -1460,7 +1482,11 @@ void tan_product(rdst_ctx& c, const double* u, double* Ju) {
     const Options& o = c.o;
     cudaStream_t s = c.s;
     const long N = c.N, NB = std::max(c.NB, 1), Fi = std::max(c.Fi, 1);
-    const size_t need = 2 * (N * QW + N + NB * QW + N * GW + N * QW + N) + 5 * Fi + 5 * NB;
+    const bool visc = c.tr.viscous != 0;
+    // viscous records: velocity + muEff (4) per cell and boundary face, grad U
+    // (9) per cell, face velocity (3) per face, viscous terms (8) per face
+    const size_t nvisc = visc ? 2 * (4 * N + 4 * NB + 9 * N + 3 * Fi + 3 * NB) + 8 * Fi + 8 * NB : 0;
+    const size_t need = 2 * (N * QW + N + NB * QW + N * GW + N * QW + N) + 5 * Fi + 5 * NB + nvisc;
     if (c.t_buf.n < need) c.t_buf.alloc(need);
     double* p0 = c.t_buf.p;
     double* qv = p0;            double* qd = qv + N * QW;
@@ -1470,23 +1496,46 @@ void tan_product(rdst_ctx& c, const double* u, double* Ju) {
     double* psv = gd + N * GW;  double* psd = psv + N * QW;
     double* fcv = psd + N * QW; double* fcd = fcv + N;
     double* fld = fcd + N;      double* bfld = fld + 5 * Fi;
+    double *uv = nullptr, *ud = nullptr, *ubv = nullptr, *ubd = nullptr, *gUv = nullptr, *gUd = nullptr;
+    double *upv = nullptr, *upd = nullptr, *bupv = nullptr, *bupd = nullptr, *vfd = nullptr, *bvfd = nullptr;
+    if (visc) {
+        uv = bfld + 5 * NB;  ud = uv + 4 * N;
+        ubv = ud + 4 * N;    ubd = ubv + 4 * NB;
+        gUv = ubd + 4 * NB;  gUd = gUv + 9 * N;
+        upv = gUd + 9 * N;   upd = upv + 3 * Fi;
+        bupv = upd + 3 * Fi; bupd = bupv + 3 * NB;
+        vfd = bupd + 3 * NB; bvfd = vfd + 8 * Fi;
+    }
     const int use_c = adj_use_c(c);
-    k_tan_q<<<nblk(N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, use_c, c.W.p, u, qv, qd, pv, pd); CKL();
-    if (m.NB > 0) { k_tan_qb<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, use_c, c.W.p, u, c.bs.p, qbv, qbd); CKL(); }
+    k_tan_q<<<nblk(N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, c.tr, use_c, c.W.p, u, c.mut.p, qv, qd, pv, pd, uv, ud); CKL();
+    if (m.NB > 0) {
+        k_tan_qb<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, c.bd, c.tr, use_c, c.W.p, u, c.bs.p, c.mut_b.p, qbv, qbd,
+                                                 ubv, ubd);
+        CKL();
+    }
     k_tan_grad<<<nblk(N, 128), 128, 0, s>>>(m, c.venkat_mask, o.venkat_K, o.flux == FLUX_HLLCP, qv, qd, qbv, qbd, pv, pd,
                                            gv, gd, psv, psd, fcv, fcd);
     CKL();
     if (m.Fi > 0) {
         k_tan_faces<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
                                                    lim_code(o.lim_T), o.low_mach, o.mainf, qv, qd, gv, gd, psv, psd,
-                                                   fcv, fcd, fld);
+                                                   fcv, fcd, fld, upv, upd);
         CKL();
     }
     if (m.NB > 0) {
-        k_tan_bfaces<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), o.low_mach, o.mainf, qbv, qbd, bfld);
+        k_tan_bfaces<<<nblk(m.NB, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), o.low_mach, o.mainf, qbv, qbd, bfld,
+                                                     bupv, bupd);
         CKL();
     }
-    k_tan_residual<<<nblk(N, TPB), TPB, 0, s>>>(m, fld, bfld, Ju);
+    if (visc) {
+        k_tan_gradU<<<nblk(N, 128), 128, 0, s>>>(m, uv, ud, ubv, ubd, gUv, gUd); CKL();
+        if (m.Fi > 0) { k_tan_visc_faces<<<nblk(m.Fi, 128), 128, 0, s>>>(m, uv, ud, gUv, gUd, upv, upd, vfd); CKL(); }
+        if (m.NB > 0) {
+            k_tan_visc_bfaces<<<nblk(m.NB, 128), 128, 0, s>>>(m, uv, ud, gUv, gUd, ubv, ubd, bupv, bupd, bvfd);
+            CKL();
+        }
+    }
+    k_tan_residual<<<nblk(N, TPB), TPB, 0, s>>>(m, fld, bfld, vfd, bvfd, Ju);
     CKL();
 }
 
