@@ -300,7 +300,8 @@ def run_ours(args, rank, world):
 
 def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
     """Time to a density-residual drop of `drop` in FP64 and in mixed
-    precision (FP32 Jacobian/ILU/basis) on the workload's mesh with
+    precision (FP32 Jacobian/ILU/basis; and BF16 Jacobian/ILU with the FP32
+    basis) on the workload's mesh with
     first-order HLL reconstruction at CFL 500 (the limited second-order
     cases stall near 1e-6: limiter switching), then the discrete adjoint of
     the pressure-drag coefficient at the FP64 converged state, its cost
@@ -322,7 +323,7 @@ def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
     out = {"drop": drop, "config": "same mesh and free stream, HLL, first-order (upwind) reconstruction, CFL 500",
            "max_steps": max_steps}
     solvers = {}
-    for prec in ("fp64", "fp32"):
+    for prec in ("fp64", "fp32", "bf16"):
         opts = dict(case.options, **first, precision=prec, profile=False)
         s = rhodst_b200.Solver(case.mesh, case.bcs, opts)
         s.set_primitive(case.p, case.U, case.T)
@@ -342,8 +343,12 @@ def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
         solvers[prec] = s
     if out["fp64"]["steps"] and out["fp32"]["steps"]:
         out["speedup_mixed_over_fp64"] = out["fp64"]["device_s"] / out["fp32"]["device_s"]
+    if out["fp64"]["steps"] and out["bf16"]["steps"]:
+        out["speedup_bf16_over_fp64"] = out["fp64"]["device_s"] / out["bf16"]["device_s"]
     out["Cl_rel_diff"] = abs(out["fp32"]["Cl"] - out["fp64"]["Cl"]) / abs(out["fp64"]["Cl"])
     out["Cd_rel_diff"] = abs(out["fp32"]["Cd"] - out["fp64"]["Cd"]) / abs(out["fp64"]["Cd"])
+    out["bf16_Cl_rel_diff"] = abs(out["bf16"]["Cl"] - out["fp64"]["Cl"]) / abs(out["fp64"]["Cl"])
+    out["bf16_Cd_rel_diff"] = abs(out["bf16"]["Cd"] - out["fp64"]["Cd"]) / abs(out["fp64"]["Cd"])
     rep, _ = solvers["fp64"].adjoint(patch, drag, p_ref=1.0, scale=1.0 / qA, rel_tol=1e-8, max_cycles=30,
                                      n_directions=30)
     dU_dM = c_inf * U0 / np.linalg.norm(U0)
@@ -359,21 +364,37 @@ def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
 
 
 def cpu_baseline(case, budget_s: float, steps_max: int, warmup: int = 1):
-    """The oracle (CPU restatement of the reference step, single thread) on
-    a bounded sample of the same workload."""
-    from tests.oracle_lib import OracleSolver
-    o = OracleSolver(case.mesh, case.bcs, case.options)
-    o.set_primitive(case.p, case.U, case.T)
-    o.step(warmup)
-    n = 0
-    t0 = time.perf_counter()
-    while n < steps_max and (time.perf_counter() - t0) < budget_s:
-        o.step(1)
-        n += 1
-    dt = time.perf_counter() - t0
+    """The oracle (CPU FP64 restatement of the reference step) on a bounded
+    sample of the same workload, on all host cores: cells split by RCB into
+    one subdomain per thread with ILU(0) per subdomain -- the reference run
+    on that many processors, whose ILU drops the couplings across processor
+    patches -- and, for scale, one core with one subdomain (exact ILU(0))."""
+    from tests.oracle_lib import OracleSolver, set_threads
     N = case.mesh.n_cells
-    return {"value": N * n / dt, "unit": "cell-iter/s", "cores": 1, "kind": "port",
-            "sample": f"{n} steps of the same workload after {warmup} warm-up step(s), {dt:.2f} s"}
+
+    def timed(threads, parts, budget, w):
+        set_threads(threads)
+        o = OracleSolver(case.mesh, case.bcs, case.options, rcb_parts=parts)
+        o.set_primitive(case.p, case.U, case.T)
+        if w:
+            o.step(w)
+        n = 0
+        t0 = time.perf_counter()
+        while n < steps_max and (n == 0 or (time.perf_counter() - t0) < budget):
+            o.step(1)
+            n += 1
+        return n, time.perf_counter() - t0
+
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    n, dt = timed(cores, cores, budget_s, warmup)
+    out = {"value": N * n / dt, "unit": "cell-iter/s", "cores": cores, "kind": "port",
+           "sample": f"{n} steps of the same workload after {warmup} warm-up step(s), {dt:.2f} s, "
+                     f"{cores} threads, RCB into {cores} subdomains with ILU(0) per subdomain"}
+    n1, dt1 = timed(1, 1, budget_s / 3, 0)
+    out["single_core"] = {"value": N * n1 / dt1, "cores": 1,
+                          "sample": f"{n1} step(s), {dt1:.2f} s, 1 thread, one subdomain (exact ILU(0))"}
+    set_threads(0)
+    return out
 
 
 def run_converge(args):
@@ -448,7 +469,8 @@ def main():
         line = {"impl": "reference", "metric": "cell_iterations_per_s", "value": cb["value"], "unit": "cell-iter/s",
                 "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": dict(desc, note="rhoDST needs foam-extend 4.1 (absent); CPU FP64 restatement timed"),
+                "config": dict(desc, note="rhoDST needs foam-extend 4.1 (absent); CPU FP64 restatement timed "
+                                          "on all host cores"),
                 "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))

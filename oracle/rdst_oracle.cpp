@@ -33,6 +33,13 @@
 
 #ifdef _OPENMP
 #include <omp.h>
+#define OMP_FOR _Pragma("omp parallel for schedule(static)")
+#define OMP_FOR_DYN _Pragma("omp parallel for schedule(dynamic, 1)")
+#define OMP_FOR_REDUCE_OR_ANY _Pragma("omp parallel for schedule(static) reduction(|:any)")
+#else
+#define OMP_FOR_REDUCE_OR_ANY
+#define OMP_FOR
+#define OMP_FOR_DYN
 #endif
 
 #define ORACLE_API extern "C" __attribute__((visibility("default")))
@@ -60,6 +67,27 @@ inline double neg0(double s) { return s <= 0 ? 1.0 : 0.0; }
 // foam sign(): sign(0) = +1
 inline double fsign(double s) { return s >= 0 ? 1.0 : -1.0; }
 inline double sqr(double x) { return x * x; }
+
+// Threading.  Cell loops run in parallel; face loops that scatter into
+// cells are written as per-cell gathers over the cell's faces in ascending
+// order, the order in which a serial face loop adds them, so fields are the
+// same bit for bit for any thread count.  Sums over all cells use fixed
+// blocks of 2048 summed in order: one value for any thread count.
+template <class F>
+double det_sum(int n, F&& term) {
+    const int B = 2048, nb = (n + B - 1) / B;
+    std::vector<double> part(nb, 0.0);
+    OMP_FOR
+    for (int k = 0; k < nb; ++k) {
+        double s = 0;
+        const int e = std::min(n, (k + 1) * B);
+        for (int i = k * B; i < e; ++i) s += term(i);
+        part[k] = s;
+    }
+    double s = 0;
+    for (double v : part) s += v;
+    return s;
+}
 
 struct Patch {
     int start, size, type, bc_p, bc_U, bc_T, bc_nut;
@@ -172,6 +200,7 @@ struct Ctx {
 // 1 - pos(phi), foam pos(0) = 1).
 // ----------------------------------------------------------------------
 void eval_boundary(Ctx& c) {
+    OMP_FOR
     for (int b = 0; b < c.NB; ++b) {
         if (!c.active[b]) continue;
         const int f = c.Fi + b;
@@ -278,38 +307,43 @@ void internal_coeffs(const Ctx& c, int b, double& cp, v3& cu, double& cT) {
 void grad_scalar(const Ctx& c, const std::vector<double>& x, const std::vector<double>& xb,
                  std::vector<v3>& g) {
     g.assign(c.N, v3{0, 0, 0});
-    for (int f = 0; f < c.Fi; ++f) {
-        double xf = c.w[f] * x[c.own[f]] + (1 - c.w[f]) * x[c.nei[f]];
-        v3 s = xf * c.Sf[f];
-        g[c.own[f]] = g[c.own[f]] + s;
-        g[c.nei[f]] = g[c.nei[f]] - s;
+    OMP_FOR
+    for (int i = 0; i < c.N; ++i) {
+        v3 a{0, 0, 0};
+        for (int f : c.cellFaces[i]) {
+            if (f < c.Fi) {
+                double xf = c.w[f] * x[c.own[f]] + (1 - c.w[f]) * x[c.nei[f]];
+                v3 s = xf * c.Sf[f];
+                a = (c.own[f] == i) ? a + s : a - s;
+            } else {
+                a = a + xb[f - c.Fi] * c.Sf[f];
+            }
+        }
+        g[i] = a / c.V[i];
     }
-    for (int b = 0; b < c.NB; ++b) {
-        if (!c.active[b]) continue;
-        int f = c.Fi + b;
-        g[c.own[f]] = g[c.own[f]] + xb[b] * c.Sf[f];
-    }
-    for (int i = 0; i < c.N; ++i) g[i] = g[i] / c.V[i];
 }
 
 // tensor gradient (grad U)_{ij} = d U_j / d x_i, stored row-major [9]
 void grad_vector(const Ctx& c, const std::vector<v3>& x, const std::vector<v3>& xb,
                  std::vector<std::array<double, 9>>& g) {
     g.assign(c.N, std::array<double, 9>{});
-    auto add = [&](int cell, const v3& S, const v3& xf, double sgn) {
-        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) g[cell][3 * i + j] += sgn * S[i] * xf[j];
-    };
-    for (int f = 0; f < c.Fi; ++f) {
-        v3 xf = c.w[f] * x[c.own[f]] + (1 - c.w[f]) * x[c.nei[f]];
-        add(c.own[f], c.Sf[f], xf, 1.0);
-        add(c.nei[f], c.Sf[f], xf, -1.0);
+    OMP_FOR
+    for (int cell = 0; cell < c.N; ++cell) {
+        std::array<double, 9> a{};
+        auto add = [&](const v3& S, const v3& xf, double sgn) {
+            for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) a[3 * i + j] += sgn * S[i] * xf[j];
+        };
+        for (int f : c.cellFaces[cell]) {
+            if (f < c.Fi) {
+                v3 xf = c.w[f] * x[c.own[f]] + (1 - c.w[f]) * x[c.nei[f]];
+                add(c.Sf[f], xf, c.own[f] == cell ? 1.0 : -1.0);
+            } else {
+                add(c.Sf[f], xb[f - c.Fi], 1.0);
+            }
+        }
+        for (int k = 0; k < 9; ++k) a[k] /= c.V[cell];
+        g[cell] = a;
     }
-    for (int b = 0; b < c.NB; ++b) {
-        if (!c.active[b]) continue;
-        int f = c.Fi + b;
-        add(c.own[f], c.Sf[f], xb[b], 1.0);
-    }
-    for (int i = 0; i < c.N; ++i) for (int k = 0; k < 9; ++k) g[i][k] /= c.V[i];
 }
 
 // ----------------------------------------------------------------------
@@ -354,22 +388,17 @@ double side_weight(Limiter L, double faceFlux, double w, double r) {
 // eps^2 = (K h)^3 with h = V^(1/3); reconstruction phi_f = phi_C + psi grad.(Cf-C).
 void venkat_psi(const Ctx& c, const std::vector<double>& x, const std::vector<double>& xb,
                 const std::vector<v3>& g, std::vector<double>& psi) {
-    std::vector<double> mx(x), mn(x);
-    for (int f = 0; f < c.Fi; ++f) {
-        int a = c.own[f], b = c.nei[f];
-        mx[a] = std::max(mx[a], x[b]); mn[a] = std::min(mn[a], x[b]);
-        mx[b] = std::max(mx[b], x[a]); mn[b] = std::min(mn[b], x[a]);
-    }
-    for (int bb = 0; bb < c.NB; ++bb) {
-        if (!c.active[bb]) continue;
-        int a = c.own[c.Fi + bb];
-        mx[a] = std::max(mx[a], xb[bb]); mn[a] = std::min(mn[a], xb[bb]);
-    }
     psi.assign(c.N, 1.0);
+    OMP_FOR
     for (int i = 0; i < c.N; ++i) {
+        double mxi = x[i], mni = x[i];         // max/min over the face neighbours (order-free)
+        for (int f : c.cellFaces[i]) {
+            double xo = f < c.Fi ? x[c.own[f] == i ? c.nei[f] : c.own[f]] : xb[f - c.Fi];
+            mxi = std::max(mxi, xo); mni = std::min(mni, xo);
+        }
         double hh = std::cbrt(c.V[i]);
         double eps2 = std::pow(c.o.venkat_K * hh, 3);
-        double dmax = mx[i] - x[i], dmin = mn[i] - x[i];
+        double dmax = mxi - x[i], dmin = mni - x[i];
         double p = 1.0;
         for (int f : c.cellFaces[i]) {
             double d2 = dot(g[i], c.Cf[f] - c.C[i]);
@@ -393,6 +422,7 @@ void reconstruct_scalar(const Ctx& c, Limiter L, const std::vector<double>& x,
     if (L != LIM_LINEAR && L != LIM_UPWIND) grad_scalar(c, x, xb, g);
     std::vector<double> psi;
     if (L == LIM_VENKATAKRISHNAN) venkat_psi(c, x, xb, g, psi);
+    OMP_FOR
     for (int f = 0; f < c.Fi; ++f) {
         int P = c.own[f], Nn = c.nei[f];
         if (L == LIM_VENKATAKRISHNAN) {
@@ -426,11 +456,13 @@ void reconstruct_vector(const Ctx& c, Limiter L, const std::vector<v3>& x, const
         for (int k = 0; k < 3; ++k) {
             std::vector<double> xk(c.N), xbk(c.NB);
             std::vector<v3> gk(c.N);
+            OMP_FOR
             for (int i = 0; i < c.N; ++i) { xk[i] = x[i][k]; gk[i] = {g[i][k], g[i][3 + k], g[i][6 + k]}; }
             for (int b = 0; b < c.NB; ++b) xbk[b] = xb[b][k];
             venkat_psi(c, xk, xbk, gk, psi[k]);
         }
     }
+    OMP_FOR
     for (int f = 0; f < c.Fi; ++f) {
         int P = c.own[f], Nn = c.nei[f];
         if (L == LIM_VENKATAKRISHNAN) {
@@ -704,6 +736,7 @@ void compute_flux(Ctx& c) {
     const bool kt = (c.o.flux == FLUX_KURGANOV || c.o.flux == FLUX_AUSM);
     // cell fields reconstructed by every scheme (KurganovDST.C:95-132 etc.)
     std::vector<double> rPsi(c.N), e(c.N), s(c.N), rPsi_b(c.NB, 0), e_b(c.NB, 0), s_b(c.NB, 0);
+    OMP_FOR
     for (int i = 0; i < c.N; ++i) {
         rPsi[i] = c.R * c.T[i];                 // 1/psi, psi = 1/(R T)
         e[i] = c.h[i] - c.p[i] / c.rho[i];
@@ -734,8 +767,10 @@ void compute_flux(Ctx& c) {
     std::vector<double> fface(c.F, 1.0);
     if (c.o.flux == FLUX_HLLCP) {
         std::vector<double> fc(c.N, 1.0);
+        OMP_FOR
         for (int i = 0; i < c.N; ++i)
             for (int k : c.cellCells[i]) fc[i] = std::min(fc[i], std::min(c.p[i] / c.p[k], c.p[k] / c.p[i]));
+        OMP_FOR
         for (int f = 0; f < c.Fi; ++f)
             fface[f] = c.w[f] * std::pow(fc[c.own[f]], 3) + (1 - c.w[f]) * std::pow(fc[c.nei[f]], 3);
     }
@@ -743,6 +778,7 @@ void compute_flux(Ctx& c) {
     c.phiEp.assign(c.F, 0.0);
     c.phiUp.assign(c.F, v3{0, 0, 0});
     c.Up.assign(c.F, v3{0, 0, 0});
+    OMP_FOR
     for (int f = 0; f < c.F; ++f) {
         if (f >= c.Fi && !c.active[f - c.Fi]) continue;
         Side so{rho_o[f], rhoU_o[f], rPsi_o[f], e_o[f], s_o[f]};
@@ -767,6 +803,7 @@ void compute_flux(Ctx& c) {
         for (int f : c.cellFaces[i]) r += ((c.own[f] == i) ? 1.0 : -1.0) * val(f);
         return r / c.V[i];
     };
+    OMP_FOR
     for (int i = 0; i < c.N; ++i) {
         c.Rv[i][0] = div(i, [&](int f) { return c.phi[f]; });
         for (int k = 0; k < 3; ++k) c.Rv[i][1 + k] = div(i, [&](int f) { return c.phiUp[f][k]; });
@@ -795,6 +832,7 @@ void viscous_terms(Ctx& c) {
     std::vector<t3> gU;
     grad_vector(c, c.U, c.U_b, gU);
     std::vector<double> muE(c.N), muE_b(c.NB, 0.0);
+    OMP_FOR
     for (int i = 0; i < c.N; ++i) muE[i] = mu_of_T(c, c.T[i]) + c.mut[i];
     for (int b = 0; b < c.NB; ++b) if (c.active[b]) muE_b[b] = mu_of_T(c, c.T_b[b]) + c.mut_b[b];
     auto tau_of = [&](const t3& g, double m) {
@@ -806,9 +844,11 @@ void viscous_terms(Ctx& c) {
         return t;
     };
     std::vector<t3> tau(c.N);
+    OMP_FOR
     for (int i = 0; i < c.N; ++i) tau[i] = tau_of(gU[i], muE[i]);
     std::vector<v3> lap(c.F, v3{0, 0, 0}), tauS(c.F, v3{0, 0, 0});
     std::vector<double> sig(c.F, 0.0);
+    OMP_FOR
     for (int f = 0; f < c.Fi; ++f) {
         int P = c.own[f], Q = c.nei[f];
         double w = c.w[f];
@@ -854,6 +894,7 @@ void viscous_terms(Ctx& c) {
         for (int f : c.cellFaces[i]) r += ((c.own[f] == i) ? 1.0 : -1.0) * val(f);
         return r / c.V[i];
     };
+    OMP_FOR
     for (int i = 0; i < c.N; ++i) {
         for (int k = 0; k < 3; ++k) {
             double l = div(i, [&](int f) { return lap[f][k]; });
@@ -893,6 +934,7 @@ void assemble(Ctx& c, LDU& A) {
     A.l.assign(Fi, t5{});
     A.s.assign(N, v5{0, 0, 0, 0, 0});
     // fvmDST::ddt: d = I * ddt diag; s = ddt source - diag*psi (zero within Single)
+    OMP_FOR
     for (int i = 0; i < N; ++i) {
         double rdt = (c.o.ddt == DDT_EULER) ? 1.0 / c.deltaT : c.rDeltaT[i];
         double dg = rdt * c.V[i];
@@ -901,6 +943,7 @@ void assemble(Ctx& c, LDU& A) {
     // Roe::computeJacobianDST
     std::vector<v3> Uc(N);
     std::vector<double> phiJ(N), a1(N), cc(N);
+    OMP_FOR
     for (int i = 0; i < N; ++i) {
         Uc[i] = c.rhoU[i] / c.rho[i];
         phiJ[i] = 0.5 * (g - 1) * magSqr(Uc[i]);
@@ -908,6 +951,7 @@ void assemble(Ctx& c, LDU& A) {
         cc[i] = std::sqrt(g * c.R * c.T[i]);   // sqrt(Cp/Cv/psi)
     }
     std::vector<double> lambda(Fi);
+    OMP_FOR
     for (int f = 0; f < Fi; ++f) {
         int P = c.own[f], Q = c.nei[f];
         v3 n = c.Sf[f] / c.magSf[f];
@@ -937,13 +981,18 @@ void assemble(Ctx& c, LDU& A) {
         }
     }
     // negSumDiag: d[owner] -= lower, d[neighbour] -= upper
-    for (int f = 0; f < Fi; ++f)
-        for (int k = 0; k < 25; ++k) {
-            A.d[c.own[f]][k] -= A.l[f][k];
-            A.d[c.nei[f]][k] -= A.u[f][k];
+    OMP_FOR
+    for (int i = 0; i < N; ++i)
+        for (int f : c.cellFaces[i]) {
+            if (f >= Fi) break;
+            const t5& M = (c.own[f] == i) ? A.l[f] : A.u[f];
+            for (int k = 0; k < 25; ++k) A.d[i][k] -= M[k];
         }
-    // Boundary Jacobians (Roe::computeBoundaryJacobians, Roe.C:274-379)
+    // Boundary Jacobians (Roe::computeBoundaryJacobians, Roe.C:274-379),
+    // computed per face in parallel and added in face order
     const double Cv = c.Cv;
+    std::vector<t5> pics(c.NB);
+    OMP_FOR
     for (int b = 0; b < c.NB; ++b) {
         if (!c.active[b]) continue;
         const int f = Fi + b, ci = c.own[f];
@@ -989,10 +1038,15 @@ void assemble(Ctx& c, LDU& A) {
         internal_coeffs(c, b, cp, cu, cT);
         t5 dXbdXi{};
         dXbdXi[0] = cp; dXbdXi[6] = cu[0]; dXbdXi[12] = cu[1]; dXbdXi[18] = cu[2]; dXbdXi[24] = cT;
-        t5 pic = mm(mm(dRdXb, dXbdXi), dXidWi);
-        for (int k = 0; k < 25; ++k) A.d[ci][k] += beta * pic[k];
+        pics[b] = mm(mm(dRdXb, dXbdXi), dXidWi);
+    }
+    for (int b = 0; b < c.NB; ++b) {
+        if (!c.active[b]) continue;
+        const int ci = c.own[Fi + b];
+        for (int k = 0; k < 25; ++k) A.d[ci][k] += beta * pics[b][k];
     }
     // source -= R V (fluxDST.C:124)
+    OMP_FOR
     for (int i = 0; i < N; ++i)
         for (int k = 0; k < 5; ++k) A.s[i][k] -= c.Rv[i][k] * c.V[i];
 }
@@ -1007,18 +1061,31 @@ typedef std::vector<v5> Vec;
 
 void Amul(const Ctx& c, const LDU& A, const Vec& x, Vec& y) {
     y.resize(c.N);
-    for (int i = 0; i < c.N; ++i) y[i] = mv(A.d[i], x[i]);
-    for (int f = 0; f < c.Fi; ++f) {
-        v5 a = mv(A.u[f], x[c.nei[f]]);
-        v5 b = mv(A.l[f], x[c.own[f]]);
-        for (int k = 0; k < 5; ++k) { y[c.own[f]][k] += a[k]; y[c.nei[f]][k] += b[k]; }
+    OMP_FOR
+    for (int i = 0; i < c.N; ++i) {
+        v5 yi = mv(A.d[i], x[i]);
+        for (int f : c.cellFaces[i]) {
+            if (f >= c.Fi) break;
+            v5 a = (c.own[f] == i) ? mv(A.u[f], x[c.nei[f]]) : mv(A.l[f], x[c.own[f]]);
+            for (int k = 0; k < 5; ++k) yi[k] += a[k];
+        }
+        y[i] = yi;
     }
 }
 
 double sumProd(const Vec& a, const Vec& b) {
-    double s = 0;
-    for (size_t i = 0; i < a.size(); ++i) for (int k = 0; k < 5; ++k) s += a[i][k] * b[i][k];
-    return s;
+    return det_sum((int)a.size(), [&](int i) {
+        double s = 0;
+        for (int k = 0; k < 5; ++k) s += a[i][k] * b[i][k];
+        return s;
+    });
+}
+
+// y = x (parallel copy of a block vector)
+void vcopy(Vec& y, const Vec& x) {
+    y.resize(x.size());
+    OMP_FOR
+    for (int i = 0; i < (int)x.size(); ++i) y[i] = x[i];
 }
 
 struct PreconData {
@@ -1027,13 +1094,29 @@ struct PreconData {
     // ILU(0) factors in CSR per row (cells in natural order)
     std::vector<int> rowStart, col;       // off-diagonal columns per row, ascending
     std::vector<t5> val;                  // L (k < i) or U (k > i) block
+    std::vector<std::vector<int>> prow;   // rows of each partition part, ascending (independent)
 };
+
+// rows of each part in ascending order (one part: all rows)
+std::vector<std::vector<int>> part_rows(const Ctx& c) {
+    if (c.part.empty()) {
+        std::vector<std::vector<int>> r(1, std::vector<int>(c.N));
+        for (int i = 0; i < c.N; ++i) r[0][i] = i;
+        return r;
+    }
+    int np = 0;
+    for (int i = 0; i < c.N; ++i) np = std::max(np, c.part[i] + 1);
+    std::vector<std::vector<int>> r(np);
+    for (int i = 0; i < c.N; ++i) r[c.part[i]].push_back(i);
+    return r;
+}
 
 void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
     M.kind = c.o.precon;
     const int N = c.N;
     if (M.kind == PRECON_DIAGONAL) {
         M.Dinv.resize(N);
+        OMP_FOR
         for (int i = 0; i < N; ++i) M.Dinv[i] = inv5(A.d[i]);
         return;
     }
@@ -1045,14 +1128,20 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
     // treats processor interfaces).
     std::vector<std::vector<std::pair<int, t5>>> rows(N);
     auto same = [&](int a, int b) { return c.part.empty() || c.part[a] == c.part[b]; };
-    for (int f = 0; f < c.Fi; ++f) {
-        int P = c.own[f], Q = c.nei[f];
-        if (!same(P, Q)) continue;
-        rows[P].push_back({Q, A.u[f]});
-        rows[Q].push_back({P, A.l[f]});
-    }
+    // row entries in face order (owner row: upper, neighbour row: lower)
+    OMP_FOR
+    for (int i = 0; i < N; ++i)
+        for (int f : c.cellFaces[i]) {
+            if (f >= c.Fi) break;
+            int P = c.own[f], Q = c.nei[f];
+            if (!same(P, Q)) continue;
+            if (P == i) rows[i].push_back({Q, A.u[f]});
+            else rows[i].push_back({P, A.l[f]});
+        }
     // one block per cell pair: faces joining the same pair are summed
-    for (auto& r : rows) {
+    OMP_FOR
+    for (int ii = 0; ii < N; ++ii) {
+        auto& r = rows[ii];
         std::sort(r.begin(), r.end(), [](auto& a, auto& b) { return a.first < b.first; });
         std::vector<std::pair<int, t5>> m;
         for (auto& e : r) {
@@ -1066,6 +1155,7 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
     for (int i = 0; i < N; ++i) M.rowStart[i + 1] = M.rowStart[i] + (int)rows[i].size();
     M.col.resize(M.rowStart[N]);
     M.val.resize(M.rowStart[N]);
+    OMP_FOR
     for (int i = 0; i < N; ++i)
         for (size_t k = 0; k < rows[i].size(); ++k) {
             M.col[M.rowStart[i] + k] = rows[i][k].first;
@@ -1073,7 +1163,12 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
         }
     std::vector<t5> D(A.d.begin(), A.d.end());
     M.Dinv.resize(N);
-    for (int i = 0; i < N; ++i) {
+    // parts are independent (no couplings between them): one part per task,
+    // rows of a part in ascending order
+    M.prow = part_rows(c);
+    OMP_FOR_DYN
+    for (int pp = 0; pp < (int)M.prow.size(); ++pp)
+    for (int i : M.prow[pp]) {
         for (int q = M.rowStart[i]; q < M.rowStart[i + 1]; ++q) {
             int k = M.col[q];
             if (k >= i) break;
@@ -1104,53 +1199,55 @@ void precondition(const Ctx& c, const PreconData& M, Vec& x, const Vec& b) {
     x.resize(N);
     if (M.kind == PRECON_NONE) { x = b; return; }
     if (M.kind == PRECON_DIAGONAL) {
+        OMP_FOR
         for (int i = 0; i < N; ++i) x[i] = mv(M.Dinv[i], b[i]);
         return;
     }
-    // forward: y_i = b_i - sum_{k<i} L_ik y_k
-    for (int i = 0; i < N; ++i) {
-        v5 y = b[i];
-        for (int q = M.rowStart[i]; q < M.rowStart[i + 1]; ++q) {
-            int k = M.col[q];
-            if (k >= i) break;
-            v5 t = mv(M.val[q], x[k]);
-            for (int e = 0; e < 5; ++e) y[e] -= t[e];
+    // per part (independent): forward y_i = b_i - sum_{k<i} L_ik y_k, then
+    // backward x_i = inv(U_ii) (y_i - sum_{j>i} U_ij x_j)
+    OMP_FOR_DYN
+    for (int pp = 0; pp < (int)M.prow.size(); ++pp) {
+        const std::vector<int>& rows = M.prow[pp];
+        for (int i : rows) {
+            v5 y = b[i];
+            for (int q = M.rowStart[i]; q < M.rowStart[i + 1]; ++q) {
+                int k = M.col[q];
+                if (k >= i) break;
+                v5 t = mv(M.val[q], x[k]);
+                for (int e = 0; e < 5; ++e) y[e] -= t[e];
+            }
+            x[i] = y;
         }
-        x[i] = y;
-    }
-    // backward: x_i = inv(U_ii) (y_i - sum_{j>i} U_ij x_j)
-    for (int i = N - 1; i >= 0; --i) {
-        v5 y = x[i];
-        for (int q = M.rowStart[i]; q < M.rowStart[i + 1]; ++q) {
-            int j = M.col[q];
-            if (j <= i) continue;
-            v5 t = mv(M.val[q], x[j]);
-            for (int e = 0; e < 5; ++e) y[e] -= t[e];
+        for (int r = (int)rows.size() - 1; r >= 0; --r) {
+            const int i = rows[r];
+            v5 y = x[i];
+            for (int q = M.rowStart[i]; q < M.rowStart[i + 1]; ++q) {
+                int j = M.col[q];
+                if (j <= i) continue;
+                v5 t = mv(M.val[q], x[j]);
+                for (int e = 0; e < 5; ++e) y[e] -= t[e];
+            }
+            x[i] = mv(M.Dinv[i], y);
         }
-        x[i] = mv(M.Dinv[i], y);
     }
 }
 
 // foam normFactor: sum(|A x - A xRef| + |b - A xRef|) + small, xRef = average(x)
 double norm_factor(const Ctx& c, const LDU& A, const Vec& x, const Vec& b, const Vec& Ax) {
     v5 xr{0, 0, 0, 0, 0};
-    for (int i = 0; i < c.N; ++i) for (int k = 0; k < 5; ++k) xr[k] += x[i][k];
-    for (int k = 0; k < 5; ++k) xr[k] /= c.N;
+    for (int k = 0; k < 5; ++k) xr[k] = det_sum(c.N, [&](int i) { return x[i][k]; }) / c.N;
     Vec xref(c.N, xr), pA;
     Amul(c, A, xref, pA);
-    double s = 0;
-    for (int i = 0; i < c.N; ++i) {
+    double s = det_sum(c.N, [&](int i) {
         double a = 0, bb = 0;
         for (int k = 0; k < 5; ++k) { a += sqr(Ax[i][k] - pA[i][k]); bb += sqr(b[i][k] - pA[i][k]); }
-        s += std::sqrt(a) + std::sqrt(bb);
-    }
+        return std::sqrt(a) + std::sqrt(bb);
+    });
     return s + SOLVER_SMALL;
 }
 
 void cmpt_residual(const Vec& r, double nf, double* out) {
-    double s[5] = {0, 0, 0, 0, 0};
-    for (auto& v : r) for (int k = 0; k < 5; ++k) s[k] += std::fabs(v[k]);
-    for (int k = 0; k < 5; ++k) out[k] = s[k] / nf;
+    for (int k = 0; k < 5; ++k) out[k] = det_sum((int)r.size(), [&](int i) { return std::fabs(r[i][k]); }) / nf;
 }
 
 bool converged(const Options& o, const double* ini, const double* fin, int it) {
@@ -1169,10 +1266,12 @@ void linear_solve(Ctx& c, const LDU& A, const PreconData& M, Vec& dx, Report& re
     const int N = c.N;
     const Options& o = c.o;
     Vec x0(N), Ax0, b(N);
+    OMP_FOR
     for (int i = 0; i < N; ++i) x0[i] = {c.rho[i], c.rhoU[i][0], c.rhoU[i][1], c.rhoU[i][2], c.rhoE[i]};
     double nf;
     if (o.dependent_W) {
         Amul(c, A, x0, Ax0);
+        OMP_FOR
         for (int i = 0; i < N; ++i) for (int k = 0; k < 5; ++k) b[i][k] = Ax0[i][k] + A.s[i][k];
         nf = norm_factor(c, A, x0, b, Ax0);
     } else {
@@ -1198,14 +1297,20 @@ void linear_solve(Ctx& c, const LDU& A, const PreconData& M, Vec& dx, Report& re
             int used = 0;
             for (int i = 0; i < m; ++i) {
                 if (beta == 0.0) break;          // lucky breakdown
-                Vk[i] = w;
-                for (auto& v : Vk[i]) for (int k = 0; k < 5; ++k) v[k] /= beta;
+                Vk[i].resize(N);
+                {
+                    Vec& Vi = Vk[i];
+                    OMP_FOR
+                    for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) Vi[q][k] = w[q][k] / beta;
+                }
                 Amul(c, A, Vk[i], t);
                 precondition(c, M, w, t);
                 for (int j = 0; j <= i; ++j) {   // modified Gram-Schmidt
                     double hji = sumProd(w, Vk[j]);
                     H[j * m + i] = hji;
-                    for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) w[q][k] -= hji * Vk[j][q][k];
+                    const Vec& Vj = Vk[j];
+                    OMP_FOR
+                    for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) w[q][k] -= hji * Vj[q][k];
                 }
                 beta = std::sqrt(sumProd(w, w));
                 for (int j = 0; j < i; ++j) {   // previous Givens rotations
@@ -1231,9 +1336,11 @@ void linear_solve(Ctx& c, const LDU& A, const PreconData& M, Vec& dx, Report& re
                 for (int j = i + 1; j < used; ++j) sum -= H[i * m + j] * yh[j];
                 yh[i] = sum / H[i * m + i];
             }
-            for (int i = 0; i < used; ++i)
-                for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) dx[q][k] += yh[i] * Vk[i][q][k];
+            OMP_FOR
+            for (int q = 0; q < N; ++q)
+                for (int i = 0; i < used; ++i) for (int k = 0; k < 5; ++k) dx[q][k] += yh[i] * Vk[i][q][k];
             Amul(c, A, dx, t);
+            OMP_FOR
             for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) r[q][k] = A.s[q][k] - t[q][k];
             cmpt_residual(r, nf, rep.lin_final);
             ++it;
@@ -1246,15 +1353,18 @@ void linear_solve(Ctx& c, const LDU& A, const PreconData& M, Vec& dx, Report& re
             rhoOld = rho;
             rho = sumProd(rw, r);
             beta = rho / rhoOld * (alpha / omega);
+            OMP_FOR
             for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) p[q][k] = r[q][k] + beta * (p[q][k] - omega * v[q][k]);
             precondition(c, M, ph, p);
             Amul(c, A, ph, v);
             alpha = rho / sumProd(rw, v);
+            OMP_FOR
             for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) s[q][k] = r[q][k] - alpha * v[q][k];
             precondition(c, M, sh, s);
             Amul(c, A, sh, t2);
             double tt = sumProd(t2, t2);
             omega = tt > 0 ? sumProd(t2, s) / tt : 0.0;
+            OMP_FOR
             for (int q = 0; q < N; ++q)
                 for (int k = 0; k < 5; ++k) {
                     dx[q][k] += alpha * ph[q][k] + omega * sh[q][k];
@@ -1273,13 +1383,15 @@ void linear_solve(Ctx& c, const LDU& A, const PreconData& M, Vec& dx, Report& re
 // that only differs when a bound is active)
 // ----------------------------------------------------------------------
 void update_fields(Ctx& c, const Vec& dx) {
-    bool bnd = false;
-    auto clampv = [&](double v, double lo, double hi) {
-        if (v < lo) { bnd = true; return lo; }
-        if (v > hi) { bnd = true; return hi; }
-        return v;
-    };
+    int any = 0;
+    OMP_FOR_REDUCE_OR_ANY
     for (int i = 0; i < c.N; ++i) {
+        bool bnd = false;
+        auto clampv = [&](double v, double lo, double hi) {
+            if (v < lo) { bnd = true; return lo; }
+            if (v > hi) { bnd = true; return hi; }
+            return v;
+        };
         c.rho[i] += dx[i][0];
         for (int k = 0; k < 3; ++k) c.rhoU[i][k] += dx[i][1 + k];
         c.rhoE[i] += dx[i][4];
@@ -1289,8 +1401,9 @@ void update_fields(Ctx& c, const Vec& dx) {
         c.h[i] = clampv(hh, c.Cp * c.o.T_min, c.Cp * c.o.T_max);
         c.T[i] = c.h[i] / c.Cp;                       // thermo.correct(): hConstThermo
         c.p[i] = clampv(c.rho[i] * c.R * c.T[i], c.o.p_min, c.o.p_max);   // p = rho/psi
+        if (bnd) any = 1;
     }
-    c.bounded = bnd;
+    c.bounded = any != 0;
     eval_boundary(c);
 }
 
@@ -1301,6 +1414,7 @@ void set_steady_dt(Ctx& c) {           // setSteadyStateDeltaT (timeDST.C:218-27
     const double g = c.gamma;
     c.rDeltaT.assign(c.N, 0.0);
     if (!c.o.neighbouring) {
+        OMP_FOR
         for (int i = 0; i < c.N; ++i) {
             double cs = std::sqrt(g * c.R * c.T[i]);
             double lambdaC = (std::fabs(c.U[i][0]) + cs) * c.dS[i][0] + (std::fabs(c.U[i][1]) + cs) * c.dS[i][1] +
@@ -1309,14 +1423,16 @@ void set_steady_dt(Ctx& c) {           // setSteadyStateDeltaT (timeDST.C:218-27
         }
         return;
     }
-    for (int f = 0; f < c.Fi; ++f) {
-        int P = c.own[f], Q = c.nei[f];
-        v3 Uf = c.w[f] * c.U[P] + (1 - c.w[f]) * c.U[Q];
-        double cf = c.w[f] * std::sqrt(g * c.R * c.T[P]) + (1 - c.w[f]) * std::sqrt(g * c.R * c.T[Q]);
-        double dtSf = (mag(Uf) + cf) * c.dc[f];
-        c.rDeltaT[P] = std::max(c.rDeltaT[P], dtSf);
-        c.rDeltaT[Q] = std::max(c.rDeltaT[Q], dtSf);
-    }
+    OMP_FOR
+    for (int i = 0; i < c.N; ++i)               // max over the cell's faces (order-free)
+        for (int f : c.cellFaces[i]) {
+            if (f >= c.Fi) break;
+            int P = c.own[f], Q = c.nei[f];
+            v3 Uf = c.w[f] * c.U[P] + (1 - c.w[f]) * c.U[Q];
+            double cf = c.w[f] * std::sqrt(g * c.R * c.T[P]) + (1 - c.w[f]) * std::sqrt(g * c.R * c.T[Q]);
+            double dtSf = (mag(Uf) + cf) * c.dc[f];
+            c.rDeltaT[i] = std::max(c.rDeltaT[i], dtSf);
+        }
     for (int b = 0; b < c.NB; ++b) {
         if (!c.active[b]) continue;
         if (c.patches[c.bpatch[b]].type != RDST_PATCH_WALL) continue;
@@ -1351,32 +1467,31 @@ void set_transient_dt(Ctx& c) {        // setTransientDeltaT (timeDST.C:275-314)
 }
 
 void set_courant(Ctx& c, Report& rep) {   // setCourantDST (timeDST.C:316-443), no solverPerf
-    double ss = 0;
-    for (int i = 0; i < c.N; ++i) {
+    double ss = det_sum(c.N, [&](int i) {     // gSumSqr(mag(R))
         double m2 = 0;
         for (int k = 0; k < 5; ++k) m2 += sqr(c.Rv[i][k]);
-        ss += m2;                          // gSumSqr(mag(R))
-    }
+        return m2;
+    });
     double residualR = std::sqrt(ss);
     rep.res_mag = residualR;
     if (c.residual != -1) c.residualRatio = std::min(std::max(c.residual / residualR, 0.1), 2.0);
     c.residual = residualR;
     if (c.o.ddt == DDT_STEADY) {
         std::vector<double> factor(c.N, 1.0), eNew(c.N);
+        OMP_FOR
         for (int i = 0; i < c.N; ++i) eNew[i] = c.rhoE[i] / c.rho[i] - 0.5 * magSqr(c.rhoU[i] / c.rho[i]);
-        for (int f = 0; f < c.Fi; ++f) {
-            int P = c.own[f], Q = c.nei[f];
-            if (c.rho[P] < 0.95 * c.rhoOld[P] || eNew[P] < 0.95 * c.eOld[P] || eNew[P] < SMALL) {
-                factor[P] = std::min(factor[P], 0.5);
-                factor[Q] = std::min(factor[Q], 0.75);
+        auto drop = [&](int k) { return c.rho[k] < 0.95 * c.rhoOld[k] || eNew[k] < 0.95 * c.eOld[k] || eNew[k] < SMALL; };
+        OMP_FOR
+        for (int i = 0; i < c.N; ++i)               // min over the cell's faces (order-free)
+            for (int f : c.cellFaces[i]) {
+                if (f >= c.Fi) break;
+                const int k = c.own[f] == i ? c.nei[f] : c.own[f];
+                if (drop(i)) factor[i] = std::min(factor[i], 0.5);
+                if (drop(k)) factor[i] = std::min(factor[i], 0.75);
             }
-            if (c.rho[Q] < 0.95 * c.rhoOld[Q] || eNew[Q] < 0.95 * c.eOld[Q] || eNew[Q] < SMALL) {
-                factor[Q] = std::min(factor[Q], 0.5);
-                factor[P] = std::min(factor[P], 0.75);
-            }
-        }
         c.rhoOld = c.rho;
         c.eOld = eNew;
+        OMP_FOR
         for (int i = 0; i < c.N; ++i)
             c.courantField[i] = std::min(std::max(c.courantField[i] * c.residualRatio * factor[i], c.o.min_co), c.o.max_co);
         set_steady_dt(c);
@@ -1623,11 +1738,7 @@ void single_iterate(Ctx& c, Report& rep) {
     auto t0 = std::chrono::steady_clock::now();
     compute_flux(c);
     rep.t[0] = seconds_since(t0) * 1e3;
-    for (int k = 0; k < 5; ++k) {
-        double s = 0;
-        for (int i = 0; i < c.N; ++i) s += sqr(c.Rv[i][k] * c.V[i]);
-        rep.res_l2[k] = std::sqrt(s);
-    }
+    for (int k = 0; k < 5; ++k) rep.res_l2[k] = std::sqrt(det_sum(c.N, [&](int i) { return sqr(c.Rv[i][k] * c.V[i]); }));
     t0 = std::chrono::steady_clock::now();
     LDU A;
     assemble(c, A);
@@ -1720,6 +1831,58 @@ ORACLE_API rdst_status rdsto_create(const rdst_mesh* m, int32_t n_opts, const ch
     c.mut.assign(Nn, 0.0); c.mut_b.assign(NB, 0.0); c.nut.assign(Nn, 0.0); c.nut_b.assign(NB, 0.0);
     c.viscous = (c.o.mu > 0 || c.o.As > 0 || c.o.turbulence != TURB_LAMINAR);
     *out = h.release();
+    return RDST_OK;
+}
+
+// Threads of the oracle's parallel loops (n <= 0: the OpenMP default).
+ORACLE_API int32_t rdsto_set_threads(int32_t n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+// Recursive coordinate bisection of the cells into n_parts parts (longest
+// extent, split at the proportional rank; ties by index) and the ILU(0)
+// partition set to it: the subdomains of a run on n_parts processors, whose
+// ILU factors drop the couplings between processors.
+static void rcb_split(const Ctx& c, std::vector<int>& idx, int lo, int hi, int p0, int np, std::vector<int>& part) {
+    if (np <= 1 || hi - lo <= 1) {
+        for (int i = lo; i < hi; ++i) part[idx[i]] = p0;
+        return;
+    }
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int i = lo; i < hi; ++i)
+        for (int k = 0; k < 3; ++k) { mn[k] = std::min(mn[k], c.C[idx[i]][k]); mx[k] = std::max(mx[k], c.C[idx[i]][k]); }
+    int ax = 0;
+    for (int k = 1; k < 3; ++k) if (mx[k] - mn[k] > mx[ax] - mn[ax]) ax = k;
+    const int nl = np / 2;
+    const int mid = lo + (int)((long)(hi - lo) * nl / np);
+    std::nth_element(idx.begin() + lo, idx.begin() + mid, idx.begin() + hi, [&](int a, int b) {
+        return c.C[a][ax] < c.C[b][ax] || (c.C[a][ax] == c.C[b][ax] && a < b);
+    });
+    rcb_split(c, idx, lo, mid, p0, nl, part);
+    rcb_split(c, idx, mid, hi, p0 + nl, np - nl, part);
+}
+
+ORACLE_API rdst_status rdsto_partition_rcb(rdst_ctx* ctx, int32_t n_parts) {
+    if (!ctx || n_parts < 1) return RDST_ERR_ARG;
+    Ctx& c = ctx->c;
+    if (n_parts == 1) { c.part.clear(); return RDST_OK; }
+    std::vector<int> idx(c.N);
+    for (int i = 0; i < c.N; ++i) idx[i] = i;
+    c.part.assign(c.N, 0);
+    rcb_split(c, idx, 0, c.N, 0, n_parts, c.part);
+    return RDST_OK;
+}
+
+ORACLE_API rdst_status rdsto_get_partition(rdst_ctx* ctx, int32_t* part) {
+    if (!ctx || !part) return RDST_ERR_ARG;
+    const Ctx& c = ctx->c;
+    for (int i = 0; i < c.N; ++i) part[i] = c.part.empty() ? 0 : c.part[i];
     return RDST_OK;
 }
 

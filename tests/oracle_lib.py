@@ -45,17 +45,38 @@ def load_oracle() -> ctypes.CDLL:
                                            ctypes.c_double, ctypes.c_double, d, d, d]
         lib.rdsto_linear_solve.restype = ctypes.c_int32
         lib.rdsto_linear_solve.argtypes = [ctypes.c_void_p, d, ctypes.c_void_p]
+        lib.rdsto_set_threads.restype = ctypes.c_int32
+        lib.rdsto_set_threads.argtypes = [ctypes.c_int32]
+        lib.rdsto_partition_rcb.restype = ctypes.c_int32
+        lib.rdsto_partition_rcb.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        lib.rdsto_get_partition.restype = ctypes.c_int32
+        lib.rdsto_get_partition.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
         _lib = lib
     return _lib
 
 
+def set_threads(n: int = 0) -> int:
+    """Threads of the oracle's parallel loops (0: the OpenMP default);
+    returns the count in effect.  Results do not depend on it."""
+    return int(load_oracle().rdsto_set_threads(n))
+
+
 class OracleSolver(Solver):
-    def __init__(self, mesh, bcs, options, partition=None):
+    def __init__(self, mesh, bcs, options, partition=None, rcb_parts=None):
         super().__init__(load_oracle(), "rdsto_", mesh, bcs, options)
+        if rcb_parts is not None:
+            self._check(self.lib.rdsto_partition_rcb(self._h, int(rcb_parts)), "partition_rcb")
         if partition is not None:
             import numpy as np
             self._part = np.ascontiguousarray(partition, dtype=np.int32)
             self.lib.rdsto_set_partition(self._h, self._part.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+
+    def partition(self):
+        import numpy as np
+        out = np.empty(self.n_cells, dtype=np.int32)
+        self._check(self.lib.rdsto_get_partition(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
+                    "get_partition")
+        return out
 
     def precondition(self, b):
         import numpy as np
