@@ -188,6 +188,11 @@ struct Ctx {
     std::vector<double> courantField, rDeltaT, rhoOld, eOld;
     std::vector<v3> dS;
     bool bounded = false;
+    // SARC1: the strain-rate tensor of the last turbulence update (its
+    // old-time value; 6 components, symmetric) and rho before the update
+    std::vector<std::array<double, 6>> S_old;
+    bool S_old_valid = false;
+    std::vector<double> rho0;
 };
 
 // ----------------------------------------------------------------------
@@ -1544,6 +1549,7 @@ void initialize_time(Ctx& c) {           // timeDST::initialize (timeDST.C:67-20
 struct SACoeffs {
     double sigmaNut = 0.66666, kappa = 0.41, Cb1 = 0.1355, Cb2 = 0.622, Cw2 = 0.3, Cw3 = 2.0, Cv1 = 7.1, Cv2 = 5.0;
     double Cn1 = 16.0, Cn2 = 0.7, Cn3 = 0.9, Ct3 = 1.2, Ct4 = 0.5, Cr1 = 1.0, Cr2 = 2.0, Cr3 = 1.0;
+    double Cr2_SARC1 = 12.0;                 // SARC1.C:310-317
     double Cw1() const { return Cb1 / (kappa * kappa) + (1.0 + Cb2) / sigmaNut; }
 };
 inline double fpos(double s) { return s >= 0 ? 1.0 : 0.0; }   // foam pos(): pos(0) = 1
@@ -1588,15 +1594,57 @@ void update_mut(Ctx& c, const std::vector<double>& fv1c) {
     }
 }
 
+// symmetric-tensor slot of (a, q): xx xy xz yy yz zz
+inline int sym6(int a, int q) {
+    static const int T[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    return T[3 * a + q];
+}
+
 void sa_correct(Ctx& c) {
     const SACoeffs K;
     const int N = c.N;
     const bool neg_sa = c.o.turbulence == TURB_SANEG;
+    const bool sarc1 = c.o.turbulence == TURB_SARC1;
     typedef std::array<double, 9> t3;
     std::vector<t3> gU;
     grad_vector(c, c.U, c.U_b, gU);
     std::vector<v3> gn;
     grad_scalar(c, c.nut, c.nut_b, gn);
+    // SARC1 (SARC1.C:125-180, 655-669): S = symm(grad U) per cell; the
+    // material derivative ddt(rho, S_ij) + div(phi, S_ij) with the flow's
+    // ddt scheme (old time: the last update's S; at the first update the
+    // current S, as foam creates an old-time field from the current one),
+    // div by Gauss upwind on the step's mass flux, zeroGradient boundary
+    // values of S_ij
+    std::vector<std::array<double, 6>> Sc;
+    std::vector<std::array<double, 6>> DSDt;
+    if (sarc1) {
+        Sc.resize(N);
+        DSDt.resize(N);
+        for (int i = 0; i < N; ++i) {
+            const t3& g = gU[i];
+            for (int a = 0; a < 3; ++a)
+                for (int q = a; q < 3; ++q) Sc[i][sym6(a, q)] = 0.5 * (g[3 * a + q] + g[3 * q + a]);
+        }
+        if (!c.S_old_valid) c.S_old = Sc;
+        for (int i = 0; i < N; ++i) {
+            double rdt = (c.o.ddt == DDT_EULER) ? 1.0 / c.deltaT : c.rDeltaT[i];
+            std::array<double, 6> dv{};
+            for (int f : c.cellFaces[i]) {
+                if (f < c.Fi) {
+                    const double ph = c.phi[f];
+                    const int up = ph >= 0 ? c.own[f] : c.nei[f];        // upwind, pos(0) = 1
+                    const double sg = (c.own[f] == i) ? 1.0 : -1.0;
+                    for (int k = 0; k < 6; ++k) dv[k] += sg * ph * Sc[up][k];
+                } else {
+                    const double ph = c.phi_b[f - c.Fi];
+                    for (int k = 0; k < 6; ++k) dv[k] += ph * Sc[i][k];
+                }
+            }
+            for (int k = 0; k < 6; ++k)
+                DSDt[i][k] = rdt * (c.rho[i] * Sc[i][k] - c.rho0[i] * c.S_old[i][k]) + dv[k] / c.V[i];
+        }
+    }
     std::vector<double> mu(N), chi(N), fv1(N), D(N), diag(N), b(N, 0.0);
     for (int i = 0; i < N; ++i) {
         mu[i] = mu_of_T(c, c.T[i]);
@@ -1651,9 +1699,25 @@ void sa_correct(Ctx& c) {
                 }
             double sqrS = 2.0 * S2, sqrW = 2.0 * W2b;
             double rStar = std::sqrt(sqrS / std::max(sqrW, SMALL));
-            double rrStar = std::sqrt(sqrW / std::max(sqrS, SMALL));
-            double rTilda = rrStar * (rrStar - 1.0);
-            double fr1 = (1 + K.Cr1) * 2.0 * rStar / (1.0 + rStar) * (1.0 - K.Cr3 * std::atan(K.Cr2 * rTilda)) - K.Cr1;
+            double fr1;
+            if (sarc1) {
+                // rTilda = 2/(rho max(D^2, SMALL)^2) sum_aq (sum_k W_ak S_qk) DS_aq/Dt, D^2 = (S^2 + W^2)/2
+                double sqrD = 0.5 * (sqrS + sqrW);
+                double acc = 0;
+                for (int a = 0; a < 3; ++a)
+                    for (int q = 0; q < 3; ++q) {
+                        double ws = 0;
+                        for (int k = 0; k < 3; ++k)
+                            ws += 0.5 * (g[3 * a + k] - g[3 * k + a]) * Sc[i][sym6(q, k)];
+                        acc += ws * DSDt[i][sym6(a, q)];
+                    }
+                double rTilda = 2.0 / (rho * sqr(std::max(sqrD, SMALL))) * acc;
+                fr1 = (1 + K.Cr1) * 2.0 * rStar / (1.0 + rStar) * (1.0 - K.Cr3 * std::atan(K.Cr2_SARC1 * rTilda)) - K.Cr1;
+            } else {
+                double rrStar = std::sqrt(sqrW / std::max(sqrS, SMALL));
+                double rTilda = rrStar * (rrStar - 1.0);
+                fr1 = (1 + K.Cr1) * 2.0 * rStar / (1.0 + rStar) * (1.0 - K.Cr3 * std::atan(K.Cr2 * rTilda)) - K.Cr1;
+            }
             b[i] += K.Cb1 * rho * Stilda * nt * fr1 * V;
             diag[i] += K.Cw1() * fw * nt * rho / sqr(c.y[i]) * V;
             D[i] = rho * nt / K.sigmaNut + mu[i];
@@ -1727,6 +1791,10 @@ void sa_correct(Ctx& c) {
     if (!neg_sa) for (auto& v : c.nut) v = std::max(v, 0.0);
     eval_nut_boundary(c);
     update_mut(c, fv1);
+    if (sarc1) {                // this update's S is the next one's old time
+        c.S_old = Sc;
+        c.S_old_valid = true;
+    }
 }
 
 double seconds_since(std::chrono::steady_clock::time_point t0) {
@@ -1752,6 +1820,7 @@ void single_iterate(Ctx& c, Report& rep) {
     linear_solve(c, A, M, dx, rep);
     rep.t[3] = seconds_since(t0) * 1e3;
     t0 = std::chrono::steady_clock::now();
+    if (c.o.turbulence == TURB_SARC1) c.rho0 = c.rho;     // rho.oldTime() of the turbulence update
     update_fields(c, dx);
     rep.flags = c.bounded ? 1 : 0;
     if (c.o.turbulence != TURB_LAMINAR) sa_correct(c);      // turbulence_.correct()
@@ -1894,6 +1963,7 @@ ORACLE_API rdst_status rdsto_set_partition(rdst_ctx* ctx, const int32_t* part) {
 }
 
 static void init_from_primitive(Ctx& c) {
+    c.S_old_valid = false;          // a new state: SARC1's old-time S restarts from the current one
     for (int i = 0; i < c.N; ++i) {
         c.h[i] = c.Cp * c.T[i];
         c.rho[i] = c.p[i] / (c.R * c.T[i]);

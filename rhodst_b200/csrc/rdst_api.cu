@@ -171,6 +171,8 @@ struct rdst_ctx {
     Transport tr{};
     // Spalart-Allmaras
     DBuf<double> nut, nut_b, ywall, saD, safv1, sadiag, sab, sax2, sagn, safup, saflo, safdP, safdQ, safcorr, sabd, sabb;
+    DBuf<double> saSold, saRho0;        // SARC1: old-time strain rate, pre-update rho
+    DBuf<int> saSoldValid;
     SAFields sa{};
     bool turb = false;
     DBuf<Scalars> sc;
@@ -675,11 +677,14 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         c.saD.alloc(N); c.safv1.alloc(N); c.sadiag.alloc(N); c.sab.alloc(N); c.sax2.alloc(N); c.sagn.alloc(3L * N);
         c.safup.alloc(fi1); c.saflo.alloc(fi1); c.safdP.alloc(fi1); c.safdQ.alloc(fi1); c.safcorr.alloc(fi1);
         c.sabd.alloc(nb1); c.sabb.alloc(nb1);
+        c.saSold.alloc(6L * N); c.saSold.zero(s); c.saRho0.alloc(N); c.saRho0.zero(s);
+        c.saSoldValid.alloc(1); c.saSoldValid.zero(s);
         SAFields& F = c.sa;
         F.nut = c.nut.p; F.nut_b = c.nut_b.p; F.mut = c.mut.p; F.mut_b = c.mut_b.p; F.y = c.ywall.p;
         F.D = c.saD.p; F.fv1 = c.safv1.p; F.diag = c.sadiag.p; F.b = c.sab.p; F.x2 = c.sax2.p; F.gn = c.sagn.p;
         F.fup = c.safup.p; F.flo = c.saflo.p; F.fdP = c.safdP.p; F.fdQ = c.safdQ.p; F.fcorr = c.safcorr.p;
         F.bd = c.sabd.p; F.bb = c.sabb.p;
+        F.S_old = c.saSold.p; F.rho0 = c.saRho0.p; F.S_old_valid = c.saSoldValid.p;
     }
     if (c.tr.viscous) {
         c.gU.alloc(9L * N); c.up.alloc(3L * std::max(Fi, 1)); c.bup.alloc(3L * std::max(NB, 1));
@@ -973,8 +978,10 @@ void sa_correct(rdst_ctx& c) {
     const int neg_sa = c.o.turbulence == TURB_SANEG;
     SAFields F = c.sa;
     k_sa_grad<<<nblk(c.N, 128), 128, 0, s>>>(m, c.prim.p, c.bs.p, F, c.gU.p); CKL();
-    k_sa_cell<<<nblk(c.N, 128), 128, 0, s>>>(m, c.tr, neg_sa, c.steady ? 1 : 0, c.W.p, c.prim.p, c.gU.p, c.rdt.p,
-                                            c.sc.p, F); CKL();
+    const int sarc1 = c.o.turbulence == TURB_SARC1;
+    k_sa_cell<<<nblk(c.N, 128), 128, 0, s>>>(m, c.tr, neg_sa, sarc1, c.steady ? 1 : 0, c.W.p, c.prim.p, c.gU.p, c.rdt.p,
+                                            c.sc.p, c.fl.p, c.bs.p, F); CKL();
+    if (sarc1) { k_sarc1_valid<<<1, 1, 0, s>>>(F.S_old_valid); CKL(); }
     if (m.Fi > 0) { k_sa_faces<<<nblk(m.Fi, TPB), TPB, 0, s>>>(m, c.fl.p, F); CKL(); }
     if (m.NB > 0) { k_sa_bfaces<<<nblk(m.NB, TPB), TPB, 0, s>>>(m, c.tr, neg_sa, c.bs.p, F); CKL(); }
     k_sa_assemble<<<nblk(c.N, TPB), TPB, 0, s>>>(m, c.o.nut_relax, F); CKL();
@@ -997,6 +1004,9 @@ void post_update(rdst_ctx& c) {
     cudaStream_t s = c.s;
     {
         Timed tm(c, KS_UPDATE);
+        if (c.turb && c.o.turbulence == TURB_SARC1) {      // rho.oldTime() of the turbulence update
+            k_sarc1_rho0<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.W.p, c.saRho0.p); CKL();
+        }
         k_update<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, c.dx.p, c.W.p, c.prim.p, c.sc.p); CKL();
     }
     k_boundary<<<nblk(c.NB, TPB), TPB, 0, s>>>(c.m, c.th, c.bd, c.W.p, c.prim.p, c.bs.p); CKL();
@@ -1627,6 +1637,8 @@ RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const doub
         CKL();
         CK(cudaStreamSynchronize(c->s));
         after_state_set(*c);
+        // a new state: SARC1's old-time strain rate restarts from the current one
+        if (c->saSoldValid.p) CK(cudaMemsetAsync(c->saSoldValid.p, 0, sizeof(int), c->s));
         if (c->turb) {
             std::vector<double> nv(c->N);
             for (int r = 0; r < c->N; ++r) nv[r] = nut[c->perm[r]];
@@ -1655,6 +1667,7 @@ RDST_API rdst_status rdst_set_conservative(rdst_ctx* c, const double* rho, const
         k_set_conservative<<<nblk(N, TPB), TPB, 0, c->s>>>(N, c->th, c->perm_d.p, d_rho, d_rhoU, d_rhoE, c->W.p,
                                                            c->prim.p);
         CKL();
+        if (c->saSoldValid.p) CK(cudaMemsetAsync(c->saSoldValid.p, 0, sizeof(int), c->s));
         if (c->state_set) {
             // fields replaced between steps: boundary values from the new
             // internal field, time-control history kept

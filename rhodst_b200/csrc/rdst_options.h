@@ -237,8 +237,7 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
         else if (k == "RASModel" || k == "turbulence") {
             if (t == "laminar") o.turbulence = TURB_LAMINAR;
             else if (t == "SAneg") o.turbulence = TURB_SANEG;
-            else if (t == "SARC1")
-                throw ConfigError("RASModel SARC1 (Spalart-Shur rotation/curvature) is not on this path yet", true);
+            else if (t == "SARC1") o.turbulence = TURB_SARC1;
             else if (t == "SARC2") o.turbulence = TURB_SARC2;
             else throw ConfigError("Unknown RASModel " + t + "\nValid models are: (laminar SAneg SARC1 SARC2)");
         }

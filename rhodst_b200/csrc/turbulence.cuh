@@ -1,7 +1,9 @@
 // turbulence.cuh -- Spalart-Allmaras transport of nuTilda on the device,
 // segregated after the coupled update (turbulence_.correct(),
 // Single.C:101): SAneg (SAneg.C:490-605, negative nuTilda and the modified
-// Stilda) and SARC2 (SARC2.C:121-155, 425-488).  The scalar system is
+// Stilda), SARC1 (SARC1.C:125-180, 619-697: the Spalart-Shur
+// rotation/curvature multiplier with the material derivative of the strain
+// rate) and SARC2 (SARC2.C:121-155, 425-488).  The scalar system is
 // built per face (upwind convection with the step's mass flux, Gauss linear
 // corrected diffusion) and per cell (ddt, Cb2 term, production /
 // destruction with implicit Sp parts), relaxed as fvMatrix::relax and
@@ -15,6 +17,7 @@ namespace rdst {
 struct SAConst {
     double sigmaNut = 0.66666, kappa = 0.41, Cb1 = 0.1355, Cb2 = 0.622, Cw2 = 0.3, Cw3 = 2.0, Cv1 = 7.1, Cv2 = 5.0;
     double Cn1 = 16.0, Cn2 = 0.7, Cn3 = 0.9, Ct3 = 1.2, Ct4 = 0.5, Cr1 = 1.0, Cr2 = 2.0, Cr3 = 1.0;
+    double Cr2_SARC1 = 12.0;     // SARC1.C:310-317
     __device__ double Cw1() const { return Cb1 / (kappa * kappa) + (1.0 + Cb2) / sigmaNut; }
 };
 
@@ -40,7 +43,21 @@ struct SAFields {
     double* fcorr;    // [Fi] explicit non-orthogonal correction
     double* bd;       // [NB] boundary diagonal contribution
     double* bb;       // [NB] boundary source contribution
+    double* S_old;    // [6N] SARC1: strain rate of the last update (old time)
+    double* rho0;     // [N]  SARC1: rho before the coupled update (rho.oldTime())
+    int* S_old_valid; // [1]  SARC1: 0 until the first update after a new state
 };
+
+// symmetric-tensor slot of (a, q): xx xy xz yy yz zz
+__device__ __forceinline__ int sym6(int a, int q) { return a <= q ? (a == 0 ? q : a + q + 1) : (q == 0 ? a : a + q + 1); }
+
+// S = symm(grad U) (6), g_ij = dU_j/dx_i
+__device__ __forceinline__ void strain6(const double* g, double S[6]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int q = a; q < 3; ++q) S[sym6(a, q)] = 0.5 * (g[3 * a + q] + g[3 * q + a]);
+}
 
 // nuTilda boundary value: fixedValue, inletOutlet on phi, else zeroGradient
 __device__ __forceinline__ double nut_vf(const DevPatch& P, double phi) {
@@ -97,9 +114,10 @@ __global__ void __launch_bounds__(128) k_sa_grad(DevMesh m, const double* __rest
 }
 
 // per cell: ddt, Cb2 term, sources with implicit parts, DnuTildaEff, fv1
-__global__ void k_sa_cell(DevMesh m, Transport tr, int neg_sa, int steady, const double* __restrict__ W,
+__global__ void k_sa_cell(DevMesh m, Transport tr, int neg_sa, int sarc1, int steady, const double* __restrict__ W,
                           const double* __restrict__ prim, const double* __restrict__ gU,
-                          const double* __restrict__ rdtc, const Scalars* __restrict__ sc, SAFields F) {
+                          const double* __restrict__ rdtc, const Scalars* __restrict__ sc,
+                          const double* __restrict__ fl, const double* __restrict__ bs, SAFields F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.N) return;
     const SAConst K;
@@ -152,9 +170,59 @@ __global__ void k_sa_cell(DevMesh m, Transport tr, int neg_sa, int steady, const
     } else {
         const double sqrS = 2.0 * S2, sqrW = 2.0 * W2;
         const double rStar = sqrt(sqrS / fmax(sqrW, D_SMALL));
-        const double rrStar = sqrt(sqrW / fmax(sqrS, D_SMALL));
-        const double rTilda = rrStar * (rrStar - 1.0);
-        const double fr1 = (1 + K.Cr1) * 2.0 * rStar / (1.0 + rStar) * (1.0 - K.Cr3 * atan(K.Cr2 * rTilda)) - K.Cr1;
+        double fr1;
+        if (sarc1) {
+            // DS/Dt = ddt(rho, S) + div(phi, S): the flow's ddt scheme with
+            // the last update's S as old time (the current S at the first
+            // update), Gauss upwind on the step's mass flux, zeroGradient S_b
+            double Si[6], So[6], dv[6] = {0, 0, 0, 0, 0, 0};
+            strain6(g, Si);
+            const int valid = *F.S_old_valid;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) So[k] = valid ? F.S_old[6 * i + k] : Si[k];
+            for (int kk = m.cf_start[i]; kk < m.cf_start[i + 1]; ++kk) {
+                const int code = m.cf_list[kk];
+                if (code < m.Fi) {
+                    const double ph = fl[5 * code];
+                    const int up = ph >= 0 ? m.own[code] : m.nei[code];      // upwind, pos(0) = 1
+                    const double sg = (m.own[code] == i) ? 1.0 : -1.0;
+                    double Su[6];
+                    strain6(gU + 9 * up, Su);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) dv[k] += sg * ph * Su[k];
+                } else {
+                    const double ph = bs[BW * (code - m.Fi) + 7];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) dv[k] += ph * Si[k];
+                }
+            }
+            const double rdt0 = steady ? rdtc[i] : 1.0 / sc->deltaT;
+            double DS[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) DS[k] = rdt0 * (rho * Si[k] - F.rho0[i] * So[k]) + dv[k] / V;
+            // rTilda = 2/(rho max(D^2, SMALL)^2) sum_aq (sum_k W_ak S_qk) DS_aq/Dt
+            const double sqrD = 0.5 * (sqrS + sqrW);
+            double acc = 0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    double ws = 0;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) ws += 0.5 * (g[3 * a + k] - g[3 * k + a]) * Si[sym6(q, k)];
+                    acc += ws * DS[sym6(a, q)];
+                }
+            const double mD = fmax(sqrD, D_SMALL);
+            const double rTilda = 2.0 / (rho * (mD * mD)) * acc;
+            fr1 = (1 + K.Cr1) * 2.0 * rStar / (1.0 + rStar) * (1.0 - K.Cr3 * atan(K.Cr2_SARC1 * rTilda)) - K.Cr1;
+            // this update's S is the next one's old time (only cell i reads slot i)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) F.S_old[6 * i + k] = Si[k];
+        } else {
+            const double rrStar = sqrt(sqrW / fmax(sqrS, D_SMALL));
+            const double rTilda = rrStar * (rrStar - 1.0);
+            fr1 = (1 + K.Cr1) * 2.0 * rStar / (1.0 + rStar) * (1.0 - K.Cr3 * atan(K.Cr2 * rTilda)) - K.Cr1;
+        }
         b += K.Cb1 * rho * Stilda * nt * fr1 * V;
         diag += K.Cw1() * fw * nt * rho / (yy * yy) * V;
         F.D[i] = rho * nt / K.sigmaNut + mu;
@@ -163,6 +231,13 @@ __global__ void k_sa_cell(DevMesh m, Transport tr, int neg_sa, int steady, const
     F.b[i] = b;
     F.fv1[i] = fv1;
 }
+
+// SARC1 bookkeeping: rho before the coupled update; old-time S now valid
+__global__ void k_sarc1_rho0(int N, const double* __restrict__ W, double* __restrict__ rho0) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) rho0[i] = W[5 * i];
+}
+__global__ void k_sarc1_valid(int* __restrict__ flag) { *flag = 1; }
 
 // per internal face: upwind convection + corrected diffusion coefficients
 __global__ void k_sa_faces(DevMesh m, const double* __restrict__ fl, SAFields F) {

@@ -242,7 +242,7 @@ def small_turbulent(model="SAneg"):
     return c.with_options(**{"ilu.parts": 4})
 
 
-@pytest.mark.parametrize("model", ["SAneg", "SARC2"])
+@pytest.mark.parametrize("model", ["SAneg", "SARC1", "SARC2"])
 def test_sa_steps(model):
     case = small_turbulent(model)
     part = rhodst_b200.partition_cells(case.mesh.C, 4)
@@ -255,7 +255,12 @@ def test_sa_steps(model):
     pg, Ug, Tg, ng = gpu.primitive()
     po, Uo, To, no = ora.primitive()
     assert rel(pg, po) < 1e-9 and rel(Ug, Uo) < 1e-9 and rel(Tg, To) < 1e-9
-    assert rel(ng, no) < 1e-9
+    # SARC1's rTilda divides by (S^2 + W^2)^2/4: where the strain rate is at
+    # rounding level (the uniform far field) it is amplified rounding, and
+    # nuTilda moves by ~1e-7 between two valid evaluation orders (the oracle
+    # alone, built with and without FMA contraction: 6.3e-8 after these 6
+    # steps; SARC2 1.5e-10)
+    assert rel(ng, no) < (1e-6 if model == "SARC1" else 1e-9)
 
 
 def test_sa_residual_with_mut():
