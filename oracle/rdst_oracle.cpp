@@ -1419,12 +1419,15 @@ void set_steady_dt(Ctx& c) {           // setSteadyStateDeltaT (timeDST.C:218-27
     const double g = c.gamma;
     c.rDeltaT.assign(c.N, 0.0);
     if (!c.o.neighbouring) {
+        // the cell-centre definition divides by the scalar courant
+        // (timeDST.C:221-227), not the per-cell field that setCourantDST
+        // ramps: with neighbouring false a steady run keeps initialCo
         OMP_FOR
         for (int i = 0; i < c.N; ++i) {
             double cs = std::sqrt(g * c.R * c.T[i]);
             double lambdaC = (std::fabs(c.U[i][0]) + cs) * c.dS[i][0] + (std::fabs(c.U[i][1]) + cs) * c.dS[i][1] +
                              (std::fabs(c.U[i][2]) + cs) * c.dS[i][2];
-            c.rDeltaT[i] = lambdaC / (c.courantField[i] * c.V[i]);
+            c.rDeltaT[i] = lambdaC / (c.courant * c.V[i]);
         }
         return;
     }

@@ -124,7 +124,7 @@ def naca0012_inviscid(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: fl
     options = {
         "fluxScheme": flux,
         "Jacobian": "Roe",
-        "timeControls": {"neighbouring": False, "initialCo": 2.0, "minCo": 0.1, "maxCo": 50.0},
+        "timeControls": {"neighbouring": True, "initialCo": 2.0, "minCo": 0.1, "maxCo": 50.0},
         "ddtSchemes": {"default": "steadyStateDST"},
         "interpolationSchemes": {"reconstruct(rho)": limiter, "reconstruct(U)": vlim,
                                  "reconstruct(T)": limiter},
@@ -161,7 +161,7 @@ def swept_wing_c3(n_around: int = 192, n_normal: int = 64, n_span: int = 64, n_t
     options = {
         "fluxScheme": flux,
         "Jacobian": "Roe",
-        "timeControls": {"neighbouring": False, "initialCo": 5.0, "minCo": 0.1, "maxCo": 50.0},
+        "timeControls": {"neighbouring": True, "initialCo": 5.0, "minCo": 0.1, "maxCo": 50.0},
         "ddtSchemes": {"default": "steadyStateDST"},
         "interpolationSchemes": {"reconstruct(rho)": "OSPRE", "reconstruct(U)": "OSPREV",
                                  "reconstruct(T)": "OSPRE"},
@@ -232,7 +232,7 @@ def naca0012_turbulent(ni: int = 257, nj: int = 65, mach: float = 0.73, alpha: f
     options = {
         "fluxScheme": flux,
         "Jacobian": "Roe",
-        "timeControls": {"neighbouring": False, "initialCo": 2.0, "minCo": 0.1, "maxCo": 50.0},
+        "timeControls": {"neighbouring": True, "initialCo": 2.0, "minCo": 0.1, "maxCo": 50.0},
         "ddtSchemes": {"default": "steadyStateDST"},
         "interpolationSchemes": {"reconstruct(rho)": limiter, "reconstruct(U)": vlim,
                                  "reconstruct(T)": limiter},
@@ -276,7 +276,7 @@ def forward_step_3d_hybrid_c5(nx: int = 240, ny: int = 80, nz: int = 56, precisi
     options = {
         "fluxScheme": flux,
         "Jacobian": "Roe",
-        "timeControls": {"neighbouring": False, "initialCo": 0.5, "minCo": 0.1, "maxCo": 5.0},
+        "timeControls": {"neighbouring": True, "initialCo": 0.5, "minCo": 0.1, "maxCo": 5.0},
         "ddtSchemes": {"default": "steadyStateDST"},
         "interpolationSchemes": {"reconstruct(rho)": limiter, "reconstruct(U)": _vector_limiter(limiter),
                                  "reconstruct(T)": limiter},

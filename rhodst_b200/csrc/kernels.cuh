@@ -973,7 +973,7 @@ __global__ void k_dt_finalize(const double* partial, int nb, Scalars* sc) {
 // setSteadyStateDeltaT (timeDST.C:218-273): local 1/dtau per cell
 __global__ void k_dt_steady(DevMesh m, Thermo th, int neighbouring, const double* __restrict__ prim,
                             const double* __restrict__ dS, const double* __restrict__ courantF,
-                            double* __restrict__ rdt, double* partial) {
+                            const Scalars* __restrict__ sc, double* __restrict__ rdt, double* partial) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double g = th.gamma;
     double v = 0;
@@ -983,7 +983,8 @@ __global__ void k_dt_steady(DevMesh m, Thermo th, int neighbouring, const double
             double cs = sqrt(g * th.R * prim[PW * i + 1]);
             double lambdaC = (fabs(prim[PW * i + 3]) + cs) * dS[3 * i] + (fabs(prim[PW * i + 4]) + cs) * dS[3 * i + 1] +
                              (fabs(prim[PW * i + 5]) + cs) * dS[3 * i + 2];
-            v = lambdaC / (courantF[i] * m.V[i]);
+            // the scalar courant (timeDST.C:221-227), not the ramped per-cell field
+            v = lambdaC / (sc->courant * m.V[i]);
         } else {
             for (int k = m.cf_start[i]; k < m.cf_start[i + 1]; ++k) {
                 int code = m.cf_list[k];

@@ -956,7 +956,8 @@ struct Ops {
 
 void set_steady_dt(rdst_ctx& c) {
     int nb = nblk(c.N, TPB);
-    k_dt_steady<<<nb, TPB, 0, c.s>>>(c.m, c.th, c.o.neighbouring, c.prim.p, c.dS.p, c.courantF.p, c.rdt.p, c.partial.p);
+    k_dt_steady<<<nb, TPB, 0, c.s>>>(c.m, c.th, c.o.neighbouring, c.prim.p, c.dS.p, c.courantF.p, c.sc.p, c.rdt.p,
+                                     c.partial.p);
     CKL();
     k_rdt_finalize<<<1, RED_TPB, 0, c.s>>>(c.partial.p, nb, c.sc.p);
     CKL();

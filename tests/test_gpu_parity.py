@@ -172,6 +172,17 @@ def test_farfield_airfoil_steps():
     _run_pair(case, 10, partition=rhodst_b200.partition_cells(case.mesh.C, 4), tol=1e-9)
 
 
+@pytest.mark.parametrize("neighbouring", [True, False])
+def test_local_time_step_definitions(neighbouring):
+    """Both local pseudo-time steps of setSteadyStateDeltaT: the face-based
+    one with the per-cell ramped courant, the cell-centre one with the scalar
+    courant (timeDST.C:218-273)."""
+    case = small_airfoil().with_options(**{"timeControls.neighbouring": neighbouring})
+    rg, ro = _run_pair(case, 8, partition=rhodst_b200.partition_cells(case.mesh.C, 4), tol=1e-9)
+    for a, b in zip(rg, ro):
+        assert abs(a["rdt_max"] - b["rdt_max"]) <= 1e-9 * abs(b["rdt_max"])
+
+
 def test_wing_small_steps():
     case = cases.swept_wing_c3(n_around=48, n_normal=16, n_span=8, n_tip=4, ilu_parts=6)
     _run_pair(case, 4, partition=rhodst_b200.partition_cells(case.mesh.C, 6), tol=1e-9)

@@ -317,3 +317,26 @@ def test_viscous_linear_field_interior():
     assert interior.sum() >= 15
     dR = R[0.01][interior, 1:4] - R[0.0][interior, 1:4]
     assert np.abs(dR).max() < 1e-11
+
+
+def test_cell_centre_local_time_step_keeps_the_initial_courant():
+    """setSteadyStateDeltaT with neighbouring false divides by the scalar
+    courant (timeDST.C:221-227), which a steady run never changes: maxCo has
+    no effect there, while the face-based definition ramps per cell."""
+    from rhodst_b200 import cases
+    from tests.oracle_lib import OracleSolver
+
+    def run(nb, max_co):
+        c = cases.naca0012_inviscid(ni=97, nj=25, flux="HLL", limiter="upwind", first_cell=5e-3)
+        c = c.with_options(**{"timeControls.neighbouring": nb, "timeControls.maxCo": max_co})
+        o = OracleSolver(c.mesh, c.bcs, c.options)
+        o.set_primitive(c.p, c.U, c.T)
+        reps = o.step(12)
+        return [r["rdt_max"] for r in reps], o.conservative()[0]
+
+    a, Wa = run(False, 50.0)
+    b, Wb = run(False, 500.0)
+    assert a == b and np.array_equal(Wa, Wb)
+    c, _ = run(True, 50.0)
+    d, _ = run(True, 500.0)
+    assert c != d
