@@ -266,12 +266,19 @@ def test_sa_steps(model):
     pg, Ug, Tg, ng = gpu.primitive()
     po, Uo, To, no = ora.primitive()
     assert rel(pg, po) < 1e-9 and rel(Ug, Uo) < 1e-9 and rel(Tg, To) < 1e-9
-    # SARC1's rTilda divides by (S^2 + W^2)^2/4: where the strain rate is at
-    # rounding level (the uniform far field) it is amplified rounding, and
-    # nuTilda moves by ~1e-7 between two valid evaluation orders (the oracle
-    # alone, built with and without FMA contraction: 6.3e-8 after these 6
-    # steps; SARC2 1.5e-10)
-    assert rel(ng, no) < (1e-6 if model == "SARC1" else 1e-9)
+    if model != "SARC1":
+        assert rel(ng, no) < 1e-9
+        return
+    # SARC1's material derivative takes ddt(rho, S) = rDeltaT (rho S - rho0 S0)
+    # with the local pseudo-time step: in the wall layer's tiny cells a huge
+    # rDeltaT times a difference of nearly equal strain rates amplifies
+    # rounding.  The oracle alone, built with and without FMA contraction,
+    # differs there by 3.9e-5 after these six steps (2e-9 from 0.1 to 1 chord,
+    # 7e-13 beyond); SARC2 by 6e-10 everywhere
+    y = case.mesh.wall_distance
+    away = y >= 0.1
+    assert np.abs(ng - no)[away].max() <= 1e-7 * np.abs(no).max()
+    assert rel(ng, no) < 1e-4
 
 
 def test_sa_residual_with_mut():
