@@ -193,6 +193,11 @@ struct Ctx {
     std::vector<std::array<double, 6>> S_old;
     bool S_old_valid = false;
     std::vector<double> rho0;
+    // dual-time stepping: W at the two previous time levels, foam Time's
+    // deltaTSave (deltaT0 of the next step), the step's BDF2 coefficients
+    std::vector<std::array<double, 5>> Wn, Wnm1;
+    bool dual_started = false;
+    double dt_save = 1.0, dual_a = 0, dual_b = 0, dual_c = 0;
 };
 
 // ----------------------------------------------------------------------
@@ -939,11 +944,19 @@ void assemble(Ctx& c, LDU& A) {
     A.l.assign(Fi, t5{});
     A.s.assign(N, v5{0, 0, 0, 0, 0});
     // fvmDST::ddt: d = I * ddt diag; s = ddt source - diag*psi (zero within Single)
+    // dual2ndDST::fvmDdt (dual2ndDST.C:375-412): diag (rDeltaTau + a) V,
+    // source V (rDeltaTau W - b W^n - c W^n-1) less diag W (fvmDST.C:98-125)
+    const bool dual = c.o.ddt == DDT_DUAL2ND;
     OMP_FOR
     for (int i = 0; i < N; ++i) {
         double rdt = (c.o.ddt == DDT_EULER) ? 1.0 / c.deltaT : c.rDeltaT[i];
-        double dg = rdt * c.V[i];
+        double dg = dual ? (rdt + c.dual_a) * c.V[i] : rdt * c.V[i];
         for (int k = 0; k < 5; ++k) A.d[i][6 * k] = dg;
+        if (dual) {
+            const double Wi[5] = {c.rho[i], c.rhoU[i][0], c.rhoU[i][1], c.rhoU[i][2], c.rhoE[i]};
+            for (int k = 0; k < 5; ++k)
+                A.s[i][k] = c.V[i] * (rdt * Wi[k] - c.dual_b * c.Wn[i][k] - c.dual_c * c.Wnm1[i][k]) - dg * Wi[k];
+        }
     }
     // Roe::computeJacobianDST
     std::vector<v3> Uc(N);
@@ -1474,6 +1487,8 @@ void set_transient_dt(Ctx& c) {        // setTransientDeltaT (timeDST.C:275-314)
     c.deltaT = m;
 }
 
+void courant_update(Ctx& c, double residualR, bool pseudo);
+
 void set_courant(Ctx& c, Report& rep) {   // setCourantDST (timeDST.C:316-443), no solverPerf
     double ss = det_sum(c.N, [&](int i) {     // gSumSqr(mag(R))
         double m2 = 0;
@@ -1482,9 +1497,17 @@ void set_courant(Ctx& c, Report& rep) {   // setCourantDST (timeDST.C:316-443), 
     });
     double residualR = std::sqrt(ss);
     rep.res_mag = residualR;
+    courant_update(c, residualR, c.o.ddt == DDT_STEADY);
+}
+
+// setCourantDST after residualR is known: the residual ratio, then the
+// per-cell ramp and local time step (steady state, or a dual-time inner
+// iteration before its convergence) or the scalar courant and the global
+// time step (adjustTimeStep)
+void courant_update(Ctx& c, double residualR, bool pseudo) {
     if (c.residual != -1) c.residualRatio = std::min(std::max(c.residual / residualR, 0.1), 2.0);
     c.residual = residualR;
-    if (c.o.ddt == DDT_STEADY) {
+    if (pseudo) {
         std::vector<double> factor(c.N, 1.0), eNew(c.N);
         OMP_FOR
         for (int i = 0; i < c.N; ++i) eNew[i] = c.rhoE[i] / c.rho[i] - 0.5 * magSqr(c.rhoU[i] / c.rho[i]);
@@ -1533,7 +1556,7 @@ void initialize_time(Ctx& c) {           // timeDST::initialize (timeDST.C:67-20
     c.deltaT = c.o.delta_t;
     if (c.o.ddt == DDT_STEADY) set_steady_dt(c);
     else {
-        if (c.o.adjust_time_step) set_transient_dt(c);
+        set_transient_dt(c);          // unconditional in timeDST::initialize (timeDST.C:196-205)
         set_steady_dt(c);
     }
 }
@@ -1831,6 +1854,94 @@ void single_iterate(Ctx& c, Report& rep) {
     rep.t[4] = seconds_since(t0) * 1e3;
 }
 
+// residualControls + steadyCheck (residualControls.C:70-82,
+// steadyCheck.C:69-98): the mean of the five normalised initial residuals of
+// each inner solve, converged after maxInnerIter iterations, below
+// minResudual, or when the scaled slope of log(residual) over the last 20 %
+// of the history falls under magConvergedSlope (from iterationStart on)
+struct SteadyCheck {
+    std::vector<double> residuals;
+    int count = 0;
+    double residual = 1, slope = 1;
+    const Options& o;
+    explicit SteadyCheck(const Options& opt) : o(opt) {}
+    void add(const double ir[5]) {
+        double mean = 0;
+        for (int k = 0; k < 5; ++k) mean += ir[k];
+        mean /= 5;
+        ++count;
+        residual = mean;
+        residuals.push_back(mean);
+    }
+    bool converged_now() const {
+        return count > o.max_inner_iter || residual < o.min_residual || slope < o.mag_converged_slope;
+    }
+    bool converged() {
+        if (count >= o.iteration_start) {
+            double sumXi = 0, sumYi = 0, sumXiSqr = 0, sumYiXi = 0;
+            const int N = (int)(0.2 * residuals.size());
+            const double maxY = std::log(*std::max_element(residuals.begin(), residuals.end()));
+            const double minY = std::log(*std::min_element(residuals.begin(), residuals.end()));
+            const double deltaY = maxY - minY;
+            for (int i = 0; i < N; ++i) {
+                const int xi = (int)residuals.size() - 1 - i;
+                const double yi = std::log(residuals[xi]);
+                sumXi += xi;
+                sumXiSqr += std::pow(xi, 2);
+                sumYi += yi;
+                sumYiXi += yi * xi;
+            }
+            slope = (residuals.size() - 1) / deltaY *
+                    std::fabs((sumYiXi - sumXi * sumYi / N) / (sumXiSqr - std::pow(sumXi, 2) / N));
+        }
+        return converged_now();
+    }
+};
+
+// Dual::iterate (Dual.C:80-124) for one physical time step: inner
+// pseudo-time iterations of the coupled system with the dual2ndDST ddt until
+// the steadyCheck converges, then the physical time-step control
+void dual_iterate(Ctx& c, Report& rep, double dt, double dt0) {
+    // old time levels (foam creates them from the current field at first use)
+    if (!c.dual_started) {
+        c.Wn.resize(c.N);
+        for (int i = 0; i < c.N; ++i) c.Wn[i] = {c.rho[i], c.rhoU[i][0], c.rhoU[i][1], c.rhoU[i][2], c.rhoE[i]};
+        c.Wnm1 = c.Wn;
+        c.dual_started = true;
+    } else {
+        c.Wnm1.swap(c.Wn);
+        for (int i = 0; i < c.N; ++i) c.Wn[i] = {c.rho[i], c.rhoU[i][0], c.rhoU[i][1], c.rhoU[i][2], c.rhoE[i]};
+    }
+    // dual2ndDST::fvmDdt coefficients (dual2ndDST.C:391-395)
+    c.dual_a = 1.0 / dt + 1.0 / (dt + dt0);
+    c.dual_c = dt / (dt0 * (dt + dt0));
+    c.dual_b = -(c.dual_a + c.dual_c);
+    SteadyCheck rc(c.o);
+    int inner = 0;
+    do {
+        compute_flux(c);
+        for (int k = 0; k < 5; ++k) rep.res_l2[k] = std::sqrt(det_sum(c.N, [&](int i) { return sqr(c.Rv[i][k] * c.V[i]); }));
+        LDU A;
+        assemble(c, A);
+        PreconData M;
+        build_precon(c, A, M);
+        Vec dx;
+        linear_solve(c, A, M, dx, rep);
+        update_fields(c, dx);
+        rc.add(rep.lin_initial);
+        // setCourantDST(&solverPerf): |initialResidual|, pseudo-time branch
+        // while the steadyCheck (its last slope) is not converged
+        double ir2 = 0;
+        for (int k = 0; k < 5; ++k) ir2 += sqr(rep.lin_initial[k]);
+        courant_update(c, std::sqrt(ir2), !rc.converged_now());
+        ++inner;
+    } while (!rc.converged());
+    set_courant(c, rep);             // setCourantDST(): residual of R_, converged: physical time step
+    rep.flags = c.bounded ? 1 : 0;
+    rep.lin_iterations = inner;
+    c.dual_a = c.dual_b = c.dual_c = 0;
+}
+
 }  // namespace
 
 struct rdst_ctx { Ctx c; };
@@ -1967,6 +2078,8 @@ ORACLE_API rdst_status rdsto_set_partition(rdst_ctx* ctx, const int32_t* part) {
 
 static void init_from_primitive(Ctx& c) {
     c.S_old_valid = false;          // a new state: SARC1's old-time S restarts from the current one
+    c.dual_started = false;         // and the time levels of dual-time stepping from it
+    c.dt_save = c.o.delta_t;        // foam Time: deltaT0 of the first step = controlDict deltaT
     for (int i = 0; i < c.N; ++i) {
         c.h[i] = c.Cp * c.T[i];
         c.rho[i] = c.p[i] / (c.R * c.T[i]);
@@ -2053,9 +2166,12 @@ ORACLE_API rdst_status rdsto_step(rdst_ctx* ctx, int32_t n, rdst_step_report* re
     Ctx& c = ctx->c;
     for (int s = 0; s < n; ++s) {
         double dt = c.deltaT;
+        const double dt0 = c.dt_save;       // Time::operator++: deltaT0 = deltaTSave, deltaTSave = deltaT
+        c.dt_save = dt;
         c.time += dt;                       // runTime++ (rhoDST.C:73)
         Report rep;
-        single_iterate(c, rep);
+        if (c.o.dual) dual_iterate(c, rep, dt, dt0);
+        else single_iterate(c, rep);
         for (int i = 0; i < c.N; ++i)
             if (!(c.rho[i] > 0) || !(c.p[i] > 0) || !std::isfinite(c.rhoE[i]))
                 return fail(ctx, RDST_ERR_DIVERGED, "non-physical state after step");

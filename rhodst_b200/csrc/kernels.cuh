@@ -751,14 +751,16 @@ __global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, Transpor
                                                   const double* __restrict__ W, const double* __restrict__ prim,
                                                   const double* __restrict__ bs, const double* __restrict__ rdtc,
                                                   const double* __restrict__ mut,
-                                                  const Scalars* __restrict__ sc, int steady, double beta) {
+                                                  const Scalars* __restrict__ sc, int steady, double beta,
+                                                  double dual_a) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= m.N) return;
     const double g = th.gamma;
     double D[25];
     {
-        double rdt = steady ? rdtc[r] : 1.0 / sc->deltaT;
-        double dg = rdt * m.V[r];
+        // local pseudo-time (steady, dual: + a of dual2ndDST, dual2ndDST.C:397)
+        // or the global physical step
+        double dg = (steady ? rdtc[r] + dual_a : 1.0 / sc->deltaT) * m.V[r];
 #pragma unroll
         for (int e = 0; e < 25; ++e) D[e] = (e % 6 == 0) ? dg : 0.0;
     }
@@ -1066,6 +1068,33 @@ __global__ void k_store_old(int N, const double* __restrict__ W, const double* _
     if (i >= N) return;
     rhoOld[i] = W[5 * i];
     eOld[i] = eNewBuf[i];
+}
+
+// dual2ndDST source less diag W per component (dual2ndDST.C:399-405,
+// fvmDST.C:98-125), added to rhs = -R V
+__global__ void k_dual_source(int N, const double* __restrict__ V, const double* __restrict__ W,
+                              const double* __restrict__ rdtc, const double* __restrict__ Wn,
+                              const double* __restrict__ Wnm1, double a, double b, double c,
+                              double* __restrict__ rhs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double rdt = rdtc[i], Vi = V[i];
+    const double dg = (rdt + a) * Vi;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const double w = W[5 * i + k];
+        const double s = Vi * (rdt * w - b * Wn[5 * i + k] - c * Wnm1[5 * i + k]) - dg * w;
+        rhs[5 * i + k] = s + rhs[5 * i + k];
+    }
+}
+
+// setCourantDST's residual ratio with a given residualR (|initialResidual| of
+// a dual-time inner solve), and the scalar courant when adjusting
+__global__ void k_courant_scalar_r(Scalars* sc, double residualR, int transient_adjust, double min_co, double max_co) {
+    if (threadIdx.x != 0) return;
+    if (sc->residual != -1) sc->residualRatio = fmin(fmax(sc->residual / residualR, 0.1), 2.0);
+    sc->residual = residualR;
+    if (transient_adjust) sc->courant = fmin(fmax(sc->courant * sc->residualRatio, min_co), max_co);
 }
 
 __global__ void k_time_advance(Scalars* sc) {

@@ -11,6 +11,7 @@
 #include "adjoint.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <array>
 #include <cstdio>
 #include <cstring>
@@ -200,6 +201,11 @@ struct rdst_ctx {
     DBuf<int> a_vidx, a_hidx;
     DBuf<double> a_Z;               // flexible-GMRES preconditioned directions
     DBuf<double> a_vfbar, a_vbbar, a_gUbar, a_ucbar;   // viscous input bars (faces, boundary faces, cells)
+    // dual-time stepping: W at the previous two time levels, foam Time's
+    // deltaTSave, the step's a of dual2ndDST (0 outside a dual step)
+    DBuf<double> dWn, dWnm1;
+    bool dual_started = false;
+    double dt_save = 1.0, dual_a = 0.0;
     DBuf<Scalars> a_sc;             // Hessenberg and rotations of the adjoint's outer solve
     void* a_AT = nullptr;           // transposed Jacobian (storage type of A)
     DBuf<double> t_buf;             // tangent records (value, derivative)
@@ -769,7 +775,8 @@ struct Ops {
         SellMat<MT> A = c.mat<MT>(c.Aval);
         Timed tm(c, KS_ASSEMBLE);
         k_assemble<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.m, c.th, c.tr, A, c.cf_slot.p, c.W.p, c.prim.p, c.bs.p,
-                                                        c.rdt.p, c.mut.p, c.sc.p, c.steady ? 1 : 0, c.o.beta);
+                                                        c.rdt.p, c.mut.p, c.sc.p, (c.steady || c.o.dual) ? 1 : 0,
+                                                        c.o.beta, c.dual_a);
         CKL();
     }
     static void precond_setup(rdst_ctx& c) {
@@ -1050,7 +1057,7 @@ void initialize_time(rdst_ctx& c) {
     CKL();
     if (c.steady) set_steady_dt(c);
     else {
-        if (c.o.adjust_time_step) set_transient_dt(c);
+        set_transient_dt(c);          // unconditional in timeDST::initialize (timeDST.C:196-205)
         set_steady_dt(c);
     }
 }
@@ -1193,6 +1200,157 @@ void run_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
         total_ms += ms;
         done += chunk;
     }
+    c.last_step_ms = total_ms;
+    int flags = 0;
+    CK(cudaMemcpyAsync(&flags, &c.sc.p->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    c.collect_events();
+    if (flags & 2) throw std::domain_error("non-physical state (NaN or non-positive rho/p) after the update");
+}
+
+// residualControls + steadyCheck (residualControls.C:70-82,
+// steadyCheck.C:69-98): mean of the five normalised initial residuals of
+// each inner solve; converged after maxInnerIter iterations, below
+// minResudual, or when the scaled slope of log(residual) over the last 20 %
+// of the history falls under magConvergedSlope (from iterationStart on)
+struct SteadyCheck {
+    std::vector<double> residuals;
+    int count = 0;
+    double residual = 1, slope = 1;
+    const Options& o;
+    explicit SteadyCheck(const Options& opt) : o(opt) {}
+    void add(const double ir[5]) {
+        double mean = 0;
+        for (int k = 0; k < 5; ++k) mean += ir[k];
+        mean /= 5;
+        ++count;
+        residual = mean;
+        residuals.push_back(mean);
+    }
+    bool converged_now() const {
+        return count > o.max_inner_iter || residual < o.min_residual || slope < o.mag_converged_slope;
+    }
+    bool converged() {
+        if (count >= o.iteration_start) {
+            double sumXi = 0, sumYi = 0, sumXiSqr = 0, sumYiXi = 0;
+            const int N = (int)(0.2 * residuals.size());
+            const double maxY = std::log(*std::max_element(residuals.begin(), residuals.end()));
+            const double minY = std::log(*std::min_element(residuals.begin(), residuals.end()));
+            const double deltaY = maxY - minY;
+            for (int i = 0; i < N; ++i) {
+                const int xi = (int)residuals.size() - 1 - i;
+                const double yi = std::log(residuals[xi]);
+                sumXi += xi;
+                sumXiSqr += std::pow(xi, 2);
+                sumYi += yi;
+                sumYiXi += yi * xi;
+            }
+            slope = (residuals.size() - 1) / deltaY *
+                    std::fabs((sumYiXi - sumXi * sumYi / N) / (sumXiSqr - std::pow(sumXi, 2) / N));
+        }
+        return converged_now();
+    }
+};
+
+// Dual::iterate (Dual.C:80-124), one physical time step per report: inner
+// pseudo-time iterations of the coupled system with the dual2ndDST ddt until
+// the steadyCheck converges, then the physical time-step control.  The
+// inner-loop decisions are the host's, so the launches are direct.
+template <typename MT>
+void run_dual_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
+    cudaStream_t s = c.s;
+    const Options& o = c.o;
+    const long n5 = 5L * c.N;
+    if (!c.dWn.p) { c.dWn.alloc(n5); c.dWnm1.alloc(n5); }
+    if (!c.step_ev[0]) { CK(cudaEventCreate(&c.step_ev[0])); CK(cudaEventCreate(&c.step_ev[1])); }
+    std::vector<int> inner_counts;
+    int done = 0;
+    double total_ms = 0;
+    while (done < n) {
+        const int chunk = std::min(n - done, rdst_ctx::REP_CAP);
+        CK(cudaMemsetAsync(&c.sc.p->step_idx, 0, sizeof(int), s));
+        CK(cudaEventRecord(c.step_ev[0], s));
+        for (int st = 0; st < chunk; ++st) {
+            // runTime++: deltaT0 = deltaTSave, deltaTSave = deltaT
+            double dt = 0;
+            CK(cudaMemcpyAsync(&dt, &c.sc.p->deltaT, sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            const double dt0 = c.dt_save;
+            c.dt_save = dt;
+            // old time levels (created from the current field at first use)
+            if (!c.dual_started) {
+                CK(cudaMemcpyAsync(c.dWn.p, c.W.p, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                CK(cudaMemcpyAsync(c.dWnm1.p, c.W.p, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                c.dual_started = true;
+            } else {
+                std::swap(c.dWn.p, c.dWnm1.p);
+                CK(cudaMemcpyAsync(c.dWn.p, c.W.p, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            }
+            // dual2ndDST::fvmDdt coefficients (dual2ndDST.C:391-395)
+            const double a = 1.0 / dt + 1.0 / (dt + dt0);
+            const double cc = dt / (dt0 * (dt + dt0));
+            const double b = -(a + cc);
+            c.dual_a = a;
+            k_report_dt<<<1, 1, 0, s>>>(c.sc.p, c.reps.p, rdst_ctx::REP_CAP); CKL();
+            k_time_advance<<<1, 1, 0, s>>>(c.sc.p); CKL();
+            SteadyCheck rc(o);
+            int inner = 0;
+            do {
+                Ops<MT>::flux(c);
+                Ops<MT>::assemble(c);
+                k_dual_source<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.V.p, c.W.p, c.rdt.p, c.dWn.p, c.dWnm1.p, a, b, cc,
+                                                             c.rhs.p);
+                CKL();
+                Ops<MT>::precond_setup(c);
+                Ops<MT>::solve_init(c);
+                iterations_direct<MT>(c);
+                {
+                    Timed tm(c, KS_UPDATE);
+                    k_update<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, c.dx.p, c.W.p, c.prim.p, c.sc.p); CKL();
+                }
+                k_boundary<<<nblk(c.NB, TPB), TPB, 0, s>>>(c.m, c.th, c.bd, c.W.p, c.prim.p, c.bs.p); CKL();
+                double ir[5];
+                CK(cudaMemcpyAsync(ir, c.sc.p->lin_initial, sizeof(ir), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                rc.add(ir);
+                // setCourantDST(&solverPerf): |initialResidual|; the pseudo-time
+                // branch while the steadyCheck (its last slope) is not converged
+                double ir2 = 0;
+                for (int k = 0; k < 5; ++k) ir2 += ir[k] * ir[k];
+                const bool pseudo = !rc.converged_now();
+                k_courant_scalar_r<<<1, 1, 0, s>>>(c.sc.p, std::sqrt(ir2), (!pseudo && o.adjust_time_step) ? 1 : 0,
+                                                   o.min_co, o.max_co);
+                CKL();
+                if (pseudo) {
+                    k_courant_cells<<<nblk(c.N, TPB), TPB, 0, s>>>(c.m, c.W.p, c.rhoOld.p, c.eOld.p, c.courantF.p,
+                                                                  c.sc.p, o.min_co, o.max_co, c.eNew.p);
+                    CKL();
+                    k_store_old<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.W.p, c.eNew.p, c.rhoOld.p, c.eOld.p); CKL();
+                    set_steady_dt(c);
+                } else if (o.adjust_time_step) {
+                    set_transient_dt(c);
+                }
+                ++inner;
+            } while (!rc.converged());
+            // setCourantDST(): residual of R, the converged branch
+            k_courant_scalar<<<1, 1, 0, s>>>(c.sc.p, o.adjust_time_step ? 1 : 0, o.min_co, o.max_co); CKL();
+            if (o.adjust_time_step) set_transient_dt(c);
+            k_report<<<1, 1, 0, s>>>(c.sc.p, c.reps.p, rdst_ctx::REP_CAP); CKL();
+            c.dual_a = 0.0;
+            inner_counts.push_back(inner);
+        }
+        CK(cudaEventRecord(c.step_ev[1], s));
+        if (host_reps)
+            CK(cudaMemcpyAsync(host_reps + done, c.reps.p, sizeof(rdst_step_report) * chunk, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, c.step_ev[0], c.step_ev[1]));
+        total_ms += ms;
+        done += chunk;
+    }
+    // the report's iteration count of a dual step: its inner iterations
+    if (host_reps)
+        for (int k = 0; k < n; ++k) host_reps[k].lin_iterations = inner_counts[k];
     c.last_step_ms = total_ms;
     int flags = 0;
     CK(cudaMemcpyAsync(&flags, &c.sc.p->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1638,8 +1796,12 @@ RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const doub
         CKL();
         CK(cudaStreamSynchronize(c->s));
         after_state_set(*c);
-        // a new state: SARC1's old-time strain rate restarts from the current one
+        // a new state: SARC1's old-time strain rate and the dual-time levels
+        // restart from the current one; deltaT0 of the first step is
+        // controlDict's deltaT (foam Time)
         if (c->saSoldValid.p) CK(cudaMemsetAsync(c->saSoldValid.p, 0, sizeof(int), c->s));
+        c->dual_started = false;
+        c->dt_save = c->o.delta_t;
         if (c->turb) {
             std::vector<double> nv(c->N);
             for (int r = 0; r < c->N; ++r) nv[r] = nut[c->perm[r]];
@@ -1669,6 +1831,8 @@ RDST_API rdst_status rdst_set_conservative(rdst_ctx* c, const double* rho, const
                                                            c->prim.p);
         CKL();
         if (c->saSoldValid.p) CK(cudaMemsetAsync(c->saSoldValid.p, 0, sizeof(int), c->s));
+        c->dual_started = false;
+        c->dt_save = c->o.delta_t;
         if (c->state_set) {
             // fields replaced between steps: boundary values from the new
             // internal field, time-control history kept
@@ -1723,7 +1887,8 @@ RDST_API rdst_status rdst_step(rdst_ctx* c, int32_t n, rdst_step_report* reps) {
         if (n == 0) return;
         dispatch(*c, [&](auto* tag) {
             using MT = std::remove_pointer_t<decltype(tag)>;
-            run_steps<MT>(*c, n, reps);
+            if (c->o.dual) run_dual_steps<MT>(*c, n, reps);
+            else run_steps<MT>(*c, n, reps);
         });
     });
 }

@@ -26,7 +26,7 @@ enum Limiter { LIM_LINEAR = 0, LIM_UPWIND, LIM_OSPRE, LIM_VANLEER, LIM_MINMOD, L
                LIM_SUPERBEE, LIM_MUSCL, LIM_VENKATAKRISHNAN };
 enum Solver { SOLVER_GMRES = 0, SOLVER_BICGSTAB };
 enum Precon { PRECON_NONE = 0, PRECON_DIAGONAL, PRECON_ILU0 };
-enum Ddt { DDT_EULER = 0, DDT_STEADY };
+enum Ddt { DDT_EULER = 0, DDT_STEADY, DDT_DUAL2ND };
 enum Precision { PREC_FP64 = 0, PREC_FP32, PREC_BF16 };
 enum Turbulence { TURB_LAMINAR = 0, TURB_SANEG, TURB_SARC1, TURB_SARC2 };
 
@@ -43,6 +43,12 @@ struct Options {
     std::string jacobian = "Roe";
     bool dependent_W = true;          // dependentVariable W | deltaW
     double beta = 1.0;                // timeIntegration.beta
+    bool dual = false;                // timeIntegration Dual (Dual.C:80-124)
+    int max_inner_iter = 20;          // timeIntegration.maxInnerIter (IOdictDST.C:222-225)
+    bool inner_correct_turbulence = false;   // timeIntegration.innerCorrectTurbulence
+    int iteration_start = -1;         // residualControls.iterationStart (-1: 500 steady, 10 unsteady)
+    double mag_converged_slope = 0.1; // residualControls.magConvergedSlope
+    double min_residual = 1e-5;       // residualControls.minResudual
     bool adjust_time_step = true;     // timeControls.adjustTimeStep
     bool neighbouring = false;        // timeControls.neighbouring
     double initial_co = 1.0, min_co = 0.1, max_co = 50.0;
@@ -174,17 +180,21 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             else throw ConfigError("dependentVariable must be W or deltaW");
         }
         else if (k == "timeIntegration.timeIntegration") {
-            if (t == "Dual") throw ConfigError("timeIntegration Dual (dual-time stepping) is not on this path", true);
-            if (t != "Single" && t != "GPU")
+            if (t == "Dual") o.dual = true;
+            else if (t != "Single" && t != "GPU")
                 throw ConfigError("Unknown timeIntegration type " + t + "\nValid timeIntegration types are: (Dual Single)");
         }
         else if (k == "timeIntegration.beta") o.beta = parse_double(k, v);
-        else if (k == "timeIntegration.innerCorrectTurbulence" || k == "timeIntegration.maxInnerIter") {}
+        else if (k == "timeIntegration.innerCorrectTurbulence") o.inner_correct_turbulence = parse_bool(k, v);
+        else if (k == "timeIntegration.maxInnerIter") o.max_inner_iter = parse_int(k, v);
         else if (k == "timeControls.adjustTimeStep") o.adjust_time_step = parse_bool(k, v);
         else if (k == "timeControls.neighbouring") o.neighbouring = parse_bool(k, v);
         else if (k == "timeControls.initialCo") o.initial_co = parse_double(k, v);
         else if (k == "timeControls.minCo") o.min_co = parse_double(k, v);
         else if (k == "timeControls.maxCo") o.max_co = parse_double(k, v);
+        else if (k == "residualControls.iterationStart") o.iteration_start = parse_int(k, v);
+        else if (k == "residualControls.magConvergedSlope") o.mag_converged_slope = parse_double(k, v);
+        else if (k == "residualControls.minResudual") o.min_residual = parse_double(k, v);
         else if (k.rfind("residualControls.", 0) == 0) {}
         else if (k == "directWaveSpeed") {
             o.direct_wave_speed = parse_bool(k, v);
@@ -198,7 +208,7 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
         else if (k == "ddtSchemes.default") {
             if (t == "Euler") o.ddt = DDT_EULER;
             else if (t == "steadyStateDST") o.ddt = DDT_STEADY;
-            else if (t == "dual2ndDST") throw ConfigError("ddt dual2ndDST belongs to dual-time stepping, not on this path", true);
+            else if (t == "dual2ndDST") o.ddt = DDT_DUAL2ND;
             else throw ConfigError("Unknown ddtScheme " + t + "\nValid ddt schemes are: (Euler steadyStateDST dual2ndDST)");
         }
         else if (k == "interpolationSchemes.reconstruct(rho)") o.lim_rho = parse_limiter(k, v, false);
@@ -267,6 +277,15 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
     if (o.max_iter < 0 || o.min_iter < 0) throw ConfigError("solvers.W.maxIter/minIter must be >= 0");
     if (!(o.R > 0) || !(o.Cp > o.R)) throw ConfigError("thermo: need 0 < R < Cp");
     if (o.lim_U == LIM_VENKATAKRISHNAN) {}
+    // dual-time stepping: the Dual iteration with the dual2ndDST ddt (the
+    // pairing of the reference's dual-time tutorial); laminar and inviscid
+    // flows (the SA equation's own dual2ndDST ddt is not restated)
+    if (o.dual != (o.ddt == DDT_DUAL2ND))
+        throw ConfigError("timeIntegration Dual is restated with ddtSchemes dual2ndDST (and dual2ndDST with Dual)", true);
+    if (o.dual && o.turbulence != TURB_LAMINAR)
+        throw ConfigError("dual-time stepping with a turbulence model is not on this path", true);
+    if (o.iteration_start < 0) o.iteration_start = (o.ddt == DDT_STEADY) ? 500 : 10;
+    if (o.max_inner_iter < 0) throw ConfigError("timeIntegration.maxInnerIter must be >= 0");
     return o;
 }
 

@@ -183,6 +183,27 @@ def test_local_time_step_definitions(neighbouring):
         assert abs(a["rdt_max"] - b["rdt_max"]) <= 1e-9 * abs(b["rdt_max"])
 
 
+@pytest.mark.parametrize("adjust", [False, True])
+def test_dual_time_steps(adjust):
+    """Dual-time stepping (Dual::iterate + dual2ndDST + steadyCheck): the
+    same inner-iteration counts, physical time steps, residuals and fields
+    as the oracle over three physical steps."""
+    case = cases.forward_step_c1().with_options(**{
+        "timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST",
+        "timeControls.adjustTimeStep": adjust, "controlDict.deltaT": 0.02})
+    gpu, ora = pair(case)
+    for s in (gpu, ora):
+        s.set_primitive(case.p, case.U, case.T)
+    rg, ro = gpu.step(3), ora.step(3)
+    for a, b in zip(rg, ro):
+        assert a["lin_iterations"] == b["lin_iterations"], (a["lin_iterations"], b["lin_iterations"])
+        assert abs(a["deltaT"] - b["deltaT"]) <= 1e-10 * abs(b["deltaT"])
+        assert abs(a["res_mag"] - b["res_mag"]) <= 1e-8 * abs(b["res_mag"]), (a["res_mag"], b["res_mag"])
+    Wg, Wo = gpu.conservative(), ora.conservative()
+    for a, b in zip(Wg, Wo):
+        assert rel(a, b) < 1e-9
+
+
 def test_wing_small_steps():
     case = cases.swept_wing_c3(n_around=48, n_normal=16, n_span=8, n_tip=4, ilu_parts=6)
     _run_pair(case, 4, partition=rhodst_b200.partition_cells(case.mesh.C, 6), tol=1e-9)

@@ -1,0 +1,109 @@
+"""Dual-time stepping in the oracle (Dual::iterate, Dual.C:80-124, with the
+dual2ndDST ddt, dual2ndDST.C:375-412, and the steadyCheck inner-loop test,
+steadyCheck.C:69-98).
+
+(1) Converged inner iterations solve the BDF2 equations: R(W^n+1) +
+    a W^n+1 + b W^n + c W^n-1 = 0 with a = 1/dt + 1/(dt + dt0),
+    c = dt/(dt0 (dt + dt0)), b = -(a + c); at the first step W^n-1 = W^n
+    and dt0 is controlDict's deltaT (foam Time's deltaT0), afterwards the
+    previous step's.
+(2) The inner loop stops after maxInnerIter + 1 iterations when neither the
+    residual level nor the slope test is met.
+(3) The physical time step comes from initialCo at initialisation
+    (timeDST::initialize calls setTransientDeltaT unconditionally) and stays
+    with adjustTimeStep false.
+(4) Dual needs dual2ndDST and the reverse; turbulence models are rejected.
+"""
+import numpy as np
+import pytest
+
+from rhodst_b200 import cases
+from rhodst_b200._abi import RdstError
+from tests.oracle_lib import OracleSolver
+
+
+def dual_case(**opts):
+    base = {"timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST",
+            "timeControls.adjustTimeStep": False, "controlDict.deltaT": 0.02}
+    base.update(opts)
+    return cases.forward_step_c1().with_options(**base)
+
+
+def state(o):
+    r, ru, re = o.conservative()
+    return np.concatenate([r[:, None], ru, re[:, None]], 1)
+
+
+def coeffs(dt, dt0):
+    a = 1 / dt + 1 / (dt + dt0)
+    c = dt / (dt0 * (dt + dt0))
+    return a, -(a + c), c
+
+
+def test_converged_inner_iterations_solve_bdf2():
+    c = dual_case(**{"timeIntegration.maxInnerIter": 200, "residualControls.minResudual": 1e-12,
+                     "residualControls.magConvergedSlope": 0.0})
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T)
+    W0 = state(o)
+    r1 = o.step(1)[0]
+    W1 = state(o)
+    R1 = o.residual()
+    r2 = o.step(1)[0]
+    W2 = state(o)
+    R2 = o.residual()
+    assert r1["lin_iterations"] < 201 and r2["lin_iterations"] < 201
+    a, b, cc = coeffs(r1["deltaT"], 0.02)                 # first step: W^n-1 = W^n, dt0 = controlDict deltaT
+    res1 = R1 + a * W1 + b * W0 + cc * W0
+    a, b, cc = coeffs(r2["deltaT"], r1["deltaT"])
+    res2 = R2 + a * W2 + b * W1 + cc * W0
+    for res, Wn1, Wn in ((res1, W1, W0), (res2, W2, W1)):
+        scale = np.abs(a * (Wn1 - Wn)).max()
+        assert np.abs(res).max() <= 1e-9 * scale, (np.abs(res).max(), scale)
+
+
+def test_physical_time_step_from_initial_courant():
+    c = dual_case()
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T)
+    reps = o.step(3)
+    dts = [r["deltaT"] for r in reps]
+    assert dts[0] != 0.02 and dts[0] == dts[1] == dts[2]
+    assert reps[-1]["time"] == pytest.approx(sum(dts))
+
+
+def test_inner_loop_stops_after_max_inner_iter():
+    c = dual_case(**{"timeIntegration.maxInnerIter": 7, "residualControls.minResudual": 0.0,
+                     "residualControls.magConvergedSlope": 0.0})
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T)
+    assert [r["lin_iterations"] for r in o.step(2)] == [8, 8]
+
+
+def test_slope_test_ends_the_inner_loop():
+    """With no residual level the inner loop runs until log(residual)
+    flattens (the rounding floor): the scaled slope test ends it before
+    maxInnerIter."""
+    c = dual_case(**{"timeIntegration.maxInnerIter": 400, "residualControls.minResudual": 0.0})
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T)
+    for r in o.step(2):
+        assert 10 <= r["lin_iterations"] < 401
+        assert np.mean(r["lin_initial"]) < 1e-12
+
+
+@pytest.mark.parametrize("opts", [
+    {"timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "Euler"},
+    {"timeIntegration.timeIntegration": "Single", "ddtSchemes.default": "dual2ndDST"},
+])
+def test_dual_needs_dual2nd(opts):
+    c = cases.forward_step_c1().with_options(**opts)
+    with pytest.raises(RdstError):
+        OracleSolver(c.mesh, c.bcs, c.options)
+
+
+def test_dual_with_turbulence_is_rejected():
+    c = cases.naca0012_turbulent(ni=97, nj=25, first_cell=5e-3).with_options(**{
+        "timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST"})
+    with pytest.raises(RdstError):
+        OracleSolver(c.mesh, c.bcs, c.options)
