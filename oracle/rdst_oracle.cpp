@@ -1564,8 +1564,9 @@ void initialize_time(Ctx& c) {           // timeDST::initialize (timeDST.C:67-20
 // ----------------------------------------------------------------------
 // Spalart-Allmaras, segregated nuTilda equation after the coupled update
 // (turbulence_.correct(), Single.C:101): SAneg (SAneg.C:490-605, negative
-// nuTilda and the modified Stilda of Allmaras et al. 2012) and SARC2
-// (SARC2.C:121-155, 425-488).  Discretisation of the foam-extend fvMatrix
+// nuTilda and the modified Stilda of Allmaras et al. 2012), SARC1
+// (SARC1.C:125-180, 619-697) and SARC2 (SARC2.C:121-155, 425-488).
+// Discretisation of the foam-extend fvMatrix
 // (restated, not vendored): ddt with the flow's ddt scheme; upwind
 // convection with the flow's face mass flux phi; Gauss linear corrected
 // diffusion; explicit Cb2 |grad nuTilda|^2; implicit Sp parts of the

@@ -979,7 +979,7 @@ void set_transient_dt(rdst_ctx& c) {
     CKL();
 }
 
-// Spalart-Allmaras transport (SAneg / SARC2), segregated
+// Spalart-Allmaras transport (SAneg / SARC1 / SARC2), segregated
 void sa_correct(rdst_ctx& c) {
     cudaStream_t s = c.s;
     const DevMesh& m = c.m;

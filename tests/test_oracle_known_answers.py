@@ -340,3 +340,20 @@ def test_cell_centre_local_time_step_keeps_the_initial_courant():
     c, _ = run(True, 50.0)
     d, _ = run(True, 500.0)
     assert c != d
+
+
+def test_transient_initial_time_step_comes_from_initial_courant():
+    """timeDST::initialize calls setTransientDeltaT for every unsteady run
+    (timeDST.C:196-205): with adjustTimeStep false the physical time step is
+    the initialCo one, not controlDict's deltaT, and it stays."""
+    from rhodst_b200 import cases
+    from tests.oracle_lib import OracleSolver
+    c = cases.forward_step_c1().with_options(**{"timeControls.adjustTimeStep": False, "controlDict.deltaT": 0.5})
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T)
+    dts = [r["deltaT"] for r in o.step(3)]
+    assert dts[0] < 0.5 and dts[0] == dts[1] == dts[2]
+    c2 = c.with_options(**{"timeControls.initialCo": 2 * c.options["timeControls"]["initialCo"]})
+    o2 = OracleSolver(c2.mesh, c2.bcs, c2.options)
+    o2.set_primitive(c2.p, c2.U, c2.T)
+    assert o2.step(1)[0]["deltaT"] == pytest.approx(2 * dts[0], rel=1e-12)
