@@ -1727,7 +1727,9 @@ void sa_correct(Ctx& c) {
             double sqrS = 2.0 * S2, sqrW = 2.0 * W2b;
             double rStar = std::sqrt(sqrS / std::max(sqrW, SMALL));
             double fr1;
-            if (sarc1) {
+            if (c.o.turbulence == TURB_SA) {
+                fr1 = 1.0;                  // no rotation/curvature multiplier
+            } else if (sarc1) {
                 // rTilda = 2/(rho max(D^2, SMALL)^2) sum_aq (sum_k W_ak S_qk) DS_aq/Dt, D^2 = (S^2 + W^2)/2
                 double sqrD = 0.5 * (sqrS + sqrW);
                 double acc = 0;

@@ -20,9 +20,13 @@ from . import mesh as _mesh
 # "normalisedGas 1 11640.3 2.5 0 0 1" -> molWeight 11640.3, Cp 2.5, mu 0, Pr 1
 R_UNIVERSAL = 8314.47
 NORMALISED_GAS = {"R": R_UNIVERSAL / 11640.3, "Cp": 2.5}
-# air (RAE2822 tutorial thermophysicalProperties: molWeight 28.9, Cp 1005,
-# Sutherland As 1.458e-6, Ts 110.4, Pr 0.72)
-AIR = {"R": R_UNIVERSAL / 28.9, "Cp": 1005.0}
+# air of the RAE2822 tutorial (constant/thermophysicalProperties:
+# "specie 1 28.966 1005 0 1.4584e-6 110.33": molWeight, Cp, Hf, As, Ts)
+AIR = {"R": R_UNIVERSAL / 28.966, "Cp": 1005.0}
+AIR_SUTHERLAND = {"As": 1.4584e-6, "Ts": 110.33}
+# foam's sutherlandTransport conducts heat by the modified Eucken relation,
+# kappa = mu Cv (1.32 + 1.77 R/Cv): alpha = kappa/Cp = mu/Pr with this Pr
+AIR_PR = AIR["Cp"] / (1.32 * (AIR["Cp"] - AIR["R"]) + 1.77 * AIR["R"])
 
 
 @dataclasses.dataclass
@@ -289,3 +293,51 @@ def forward_step_3d_hybrid_c5(nx: int = 240, ny: int = 80, nz: int = 56, precisi
     N = m.n_cells
     return Case("forwardStep3DHybrid", m, bcs, options, np.ones(N), np.tile(U0, (N, 1)), np.ones(N), steps=1000,
                 force_patch="obstacle", force_dirs={"lift": (0.0, 1.0, 0.0), "drag": (1.0, 0.0, 0.0)})
+
+
+def rae2822(model: str = "SpalartAllmaras", flux: str = "Kurganov", limiter: str = "OSPRE") -> Case:
+    """The reference's RAE2822 tutorial (tutorials/RAE2822): its own mesh
+    (constant/polyMesh, 23,552 cells, read by rhodst_b200.foam and stored in
+    tests/golden/rae2822_mesh.npz), its free stream (0/include/
+    freestreamConditions: p 108987.773, U (233.44 9.417 0), T 255.556; nuTilda
+    4.4e-5), boundary conditions (far-field p/U/T, no-slip adiabatic airfoil,
+    nuTilda inletOutlet / fixedValue 0), Sutherland air, SpalartAllmaras,
+    Kurganov with OSPRE/OSPREV, steadyStateDST with the face-based local time
+    step at CFL 1 -> 500, BiCGStab + ILUC0 (maxIter 100, tolerance and relTol
+    1e-10), nuTilda relaxation 0.5 and the tutorial's field bounds
+    (system/*).  This path's discretisation differs from the tutorial's
+    schemes in two places: grad(U) is Gauss linear (the tutorial asks for
+    cellLimited) and nuTilda is convected upwind (linearUpwind there)."""
+    from pathlib import Path
+    from . import foam
+    fixture = Path(__file__).resolve().parents[1] / "tests" / "golden" / "rae2822_mesh.npz"
+    m = foam.load_npz(fixture)
+    m.wall_distance = _mesh.wall_distance(m, ["airfoil"])
+    p_inf, T_inf, U_inf, nut_inf = 108987.773, 255.556, (233.44, 9.417, 0.0), 4.4e-5
+    bcs = {
+        "airfoil": {"p": "zeroGradient", "U": ("fixedValue", (0.0, 0.0, 0.0)), "T": "zeroGradient",
+                    "nuTilda": ("fixedValue", 0.0)},
+        "freestreamBC": {"p": ("farField", p_inf), "U": ("farField", U_inf), "T": ("farField", T_inf),
+                         "nuTilda": ("inletOutlet", nut_inf)},
+    }
+    options = {
+        "fluxScheme": flux,
+        "Jacobian": "Roe",
+        "dependentVariable": "W",
+        "timeControls": {"neighbouring": True, "initialCo": 1.0, "minCo": 1.0, "maxCo": 500.0},
+        "ddtSchemes": {"default": "steadyStateDST"},
+        "interpolationSchemes": {"reconstruct(rho)": limiter, "reconstruct(U)": _vector_limiter(limiter),
+                                 "reconstruct(T)": limiter},
+        "solvers": {"W": {"solver": "BiCGStab", "preconditioner": "ILUC0", "minIter": 1, "maxIter": 100,
+                          "tolerance": 1e-10, "relTol": 1e-10}},
+        "relaxationFactors": {"nuTilda": 0.5},
+        "fieldBounds": {"rho": (0.01, 10.0), "p": (100.0, 1e6), "T": (10.0, 800.0)},
+        "thermo": dict(AIR),
+        "transport": dict(AIR_SUTHERLAND, Pr=AIR_PR),
+        "RASModel": model,
+    }
+    N = m.n_cells
+    al = math.atan2(U_inf[1], U_inf[0])
+    return Case("rae2822", m, bcs, options, np.full(N, p_inf), np.tile(np.array(U_inf), (N, 1)),
+                np.full(N, T_inf), nuTilda=np.full(N, nut_inf), steps=1000, force_patch="airfoil",
+                force_dirs={"lift": (-math.sin(al), math.cos(al), 0.0), "drag": (math.cos(al), math.sin(al), 0.0)})

@@ -986,10 +986,10 @@ void sa_correct(rdst_ctx& c) {
     const int neg_sa = c.o.turbulence == TURB_SANEG;
     SAFields F = c.sa;
     k_sa_grad<<<nblk(c.N, 128), 128, 0, s>>>(m, c.prim.p, c.bs.p, F, c.gU.p); CKL();
-    const int sarc1 = c.o.turbulence == TURB_SARC1;
+    const int sarc1 = c.o.turbulence == TURB_SARC1 ? 1 : (c.o.turbulence == TURB_SA ? 2 : 0);
     k_sa_cell<<<nblk(c.N, 128), 128, 0, s>>>(m, c.tr, neg_sa, sarc1, c.steady ? 1 : 0, c.W.p, c.prim.p, c.gU.p, c.rdt.p,
                                             c.sc.p, c.fl.p, c.bs.p, F); CKL();
-    if (sarc1) { k_sarc1_valid<<<1, 1, 0, s>>>(F.S_old_valid); CKL(); }
+    if (sarc1 == 1) { k_sarc1_valid<<<1, 1, 0, s>>>(F.S_old_valid); CKL(); }
     if (m.Fi > 0) { k_sa_faces<<<nblk(m.Fi, TPB), TPB, 0, s>>>(m, c.fl.p, F); CKL(); }
     if (m.NB > 0) { k_sa_bfaces<<<nblk(m.NB, TPB), TPB, 0, s>>>(m, c.tr, neg_sa, c.bs.p, F); CKL(); }
     k_sa_assemble<<<nblk(c.N, TPB), TPB, 0, s>>>(m, c.o.nut_relax, F); CKL();

@@ -28,7 +28,7 @@ enum Solver { SOLVER_GMRES = 0, SOLVER_BICGSTAB };
 enum Precon { PRECON_NONE = 0, PRECON_DIAGONAL, PRECON_ILU0 };
 enum Ddt { DDT_EULER = 0, DDT_STEADY, DDT_DUAL2ND };
 enum Precision { PREC_FP64 = 0, PREC_FP32, PREC_BF16 };
-enum Turbulence { TURB_LAMINAR = 0, TURB_SANEG, TURB_SARC1, TURB_SARC2 };
+enum Turbulence { TURB_LAMINAR = 0, TURB_SANEG, TURB_SARC1, TURB_SARC2, TURB_SA };
 
 // Thrown by the parser; mapped to RDST_ERR_CONFIG / RDST_ERR_UNSUPPORTED.
 struct ConfigError : std::runtime_error {
@@ -249,7 +249,13 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             else if (t == "SAneg") o.turbulence = TURB_SANEG;
             else if (t == "SARC1") o.turbulence = TURB_SARC1;
             else if (t == "SARC2") o.turbulence = TURB_SARC2;
-            else throw ConfigError("Unknown RASModel " + t + "\nValid models are: (laminar SAneg SARC1 SARC2)");
+            // foam-extend's compressible SpalartAllmaras (the RAE2822 and
+            // oneraM6Turb tutorials): the SARC equations without the
+            // rotation/curvature multiplier (SARC1.C with
+            // spalartShurCorrection false, SARC1.C:183-199)
+            else if (t == "SpalartAllmaras") o.turbulence = TURB_SA;
+            else throw ConfigError("Unknown RASModel " + t +
+                                   "\nValid models are: (laminar SAneg SARC1 SARC2 SpalartAllmaras)");
         }
         else if (k == "relaxationFactors.nuTilda") o.nut_relax = parse_double(k, v);
         else if (k == "solvers.nuTilda.nSweeps") o.nut_sweeps = parse_int(k, v);

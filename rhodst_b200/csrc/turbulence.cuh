@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(128) k_sa_grad(DevMesh m, const double* __rest
 }
 
 // per cell: ddt, Cb2 term, sources with implicit parts, DnuTildaEff, fv1
+// sarc1: 0 SARC2 multiplier, 1 SARC1 multiplier, 2 none (SpalartAllmaras)
 __global__ void k_sa_cell(DevMesh m, Transport tr, int neg_sa, int sarc1, int steady, const double* __restrict__ W,
                           const double* __restrict__ prim, const double* __restrict__ gU,
                           const double* __restrict__ rdtc, const Scalars* __restrict__ sc,
@@ -171,7 +172,9 @@ __global__ void k_sa_cell(DevMesh m, Transport tr, int neg_sa, int sarc1, int st
         const double sqrS = 2.0 * S2, sqrW = 2.0 * W2;
         const double rStar = sqrt(sqrS / fmax(sqrW, D_SMALL));
         double fr1;
-        if (sarc1) {
+        if (sarc1 == 2) {
+            fr1 = 1.0;                      // SpalartAllmaras: no rotation/curvature multiplier
+        } else if (sarc1) {
             // DS/Dt = ddt(rho, S) + div(phi, S): the flow's ddt scheme with
             // the last update's S as old time (the current S at the first
             // update), Gauss upwind on the step's mass flux, zeroGradient S_b

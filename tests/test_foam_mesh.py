@@ -1,0 +1,98 @@
+"""foam polyMesh input (rhodst_b200.foam) and the reference's RAE2822
+tutorial case: the reader against the tutorial's own files (when the
+reference tree is present), the stored mesh's geometry, foam's ordering
+checks, and the oracle running the case."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from rhodst_b200 import cases, foam
+from rhodst_b200 import mesh as M
+
+FIXTURE = Path(__file__).resolve().parent / "golden" / "rae2822_mesh.npz"
+TUTORIAL = Path("/root/reference/tutorials/RAE2822/constant/polyMesh")
+
+
+@pytest.mark.skipif(not TUTORIAL.exists(), reason="reference tree not present")
+def test_reader_matches_the_stored_tutorial_mesh():
+    a = foam.read_polymesh(TUTORIAL)
+    b = foam.load_npz(FIXTURE)
+    assert np.array_equal(a.points, b.points) and np.array_equal(a.faces, b.faces)
+    assert np.array_equal(a.owner, b.owner) and np.array_equal(a.neighbour, b.neighbour)
+    assert [(p.name, p.type, p.start, p.size) for p in a.patches] == \
+           [(p.name, p.type, p.start, p.size) for p in b.patches]
+
+
+def test_tutorial_mesh_geometry():
+    m = foam.load_npz(FIXTURE)
+    assert (m.n_cells, m.n_faces, m.n_internal_faces) == (23552, 94608, 46704)
+    assert [(p.name, p.type) for p in m.patches] == [("frontAndBackPlanes", M.EMPTY), ("freestreamBC", M.PATCH),
+                                                     ("airfoil", M.WALL)]
+    assert m.V.min() > 0
+    S = np.zeros((m.n_cells, 3))
+    Fi = m.n_internal_faces
+    np.add.at(S, m.owner, m.Sf)
+    np.add.at(S, m.neighbour, -m.Sf[:Fi])
+    assert np.abs(S).max() <= 1e-12 * np.abs(m.Sf).max()          # closed cells
+    d = m.C[m.neighbour] - m.C[m.owner[:Fi]]
+    assert np.all(np.einsum("ij,ij->i", d, m.Sf[:Fi]) > 0)        # owner -> neighbour normals
+    air = m.patch("airfoil")
+    x = m.Cf[air.start:air.start + air.size, 0]
+    assert 0 < x.min() and x.max() < 1                             # unit chord
+
+
+def _write(d: Path, name: str, cls: str, body: str):
+    (d / name).write_text("FoamFile\n{\n    version 2.0;\n    format ascii;\n    class " + cls +
+                          ";\n    object " + name + ";\n}\n// comment\n" + body)
+
+
+def _two_cells(d: Path, owner_first=True):
+    pts = [(0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 1, 0), (1, 1, 0), (2, 1, 0),
+           (0, 0, 1), (1, 0, 1), (2, 0, 1), (0, 1, 1), (1, 1, 1), (2, 1, 1)]
+    _write(d, "points", "vectorField", f"{len(pts)}\n(\n" + "\n".join(f"({a} {b} {c})" for a, b, c in pts) + "\n)\n")
+    faces = [(1, 4, 10, 7),                                      # internal x = 1, normal +x
+             (0, 6, 9, 3), (2, 5, 11, 8),                        # x = 0, x = 2
+             (0, 1, 7, 6), (1, 2, 8, 7), (3, 9, 10, 4), (4, 10, 11, 5),
+             (0, 3, 4, 1), (1, 4, 5, 2), (6, 7, 10, 9), (7, 8, 11, 10)]
+    _write(d, "faces", "faceList", f"{len(faces)}\n(\n" + "\n".join("4(%d %d %d %d)" % f for f in faces) + "\n)\n")
+    own = [0, 0, 1, 0, 1, 0, 1, 0, 1, 0, 1]
+    nei = [1] if owner_first else [0]
+    if not owner_first:
+        own[0] = 1
+    _write(d, "owner", "labelList", f"{len(own)}\n(\n" + "\n".join(map(str, own)) + "\n)\n")
+    _write(d, "neighbour", "labelList", f"{len(nei)}\n(\n" + "\n".join(map(str, nei)) + "\n)\n")
+    _write(d, "boundary", "polyBoundaryMesh", """3
+(
+    inlet { type patch; nFaces 1; startFace 1; }
+    outlet { type patch; nFaces 1; startFace 2; }
+    walls { type wall; inGroups 1(wall); nFaces 8; startFace 3; }
+)
+""")
+
+
+def test_reader_on_a_two_cell_mesh(tmp_path):
+    _two_cells(tmp_path)
+    m = foam.read_polymesh(tmp_path)
+    assert m.n_cells == 2 and m.n_internal_faces == 1
+    assert np.allclose(m.V, 1.0) and np.allclose(m.Sf[0], (1, 0, 0))
+    assert np.allclose(m.C, [(0.5, 0.5, 0.5), (1.5, 0.5, 0.5)])
+    assert [p.name for p in m.patches] == ["inlet", "outlet", "walls"] and m.patches[2].type == M.WALL
+
+
+def test_reader_checks_foam_ordering(tmp_path):
+    _two_cells(tmp_path, owner_first=False)
+    with pytest.raises(ValueError):
+        foam.read_polymesh(tmp_path)
+
+
+def test_tutorial_case_runs_on_the_oracle():
+    from tests.oracle_lib import OracleSolver
+    c = cases.rae2822()
+    o = OracleSolver(c.mesh, c.bcs, c.options, rcb_parts=4)
+    o.set_primitive(c.p, c.U, c.T, c.nuTilda)
+    reps = o.step(20)
+    r = [x["res_l2"][0] for x in reps]
+    assert np.all(np.isfinite(r)) and r[-1] < 0.5 * r[0]
+    nut = o.primitive()[3]
+    assert nut.min() >= 0 and np.isfinite(nut).all()

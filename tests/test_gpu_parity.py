@@ -274,7 +274,7 @@ def small_turbulent(model="SAneg"):
     return c.with_options(**{"ilu.parts": 4})
 
 
-@pytest.mark.parametrize("model", ["SAneg", "SARC1", "SARC2"])
+@pytest.mark.parametrize("model", ["SAneg", "SARC1", "SARC2", "SpalartAllmaras"])
 def test_sa_steps(model):
     case = small_turbulent(model)
     part = rhodst_b200.partition_cells(case.mesh.C, 4)
@@ -300,6 +300,22 @@ def test_sa_steps(model):
     away = y >= 0.1
     assert np.abs(ng - no)[away].max() <= 1e-7 * np.abs(no).max()
     assert rel(ng, no) < 1e-4
+
+
+def test_rae2822_tutorial_steps():
+    """The reference's RAE2822 tutorial (its own mesh, conditions and solver
+    settings; SpalartAllmaras, BiCGStab + ILUC0 to 1e-10): five steps."""
+    case = cases.rae2822().with_options(**{"ilu.parts": 8})
+    part = rhodst_b200.partition_cells(case.mesh.C, 8)
+    gpu, ora = pair(case, partition=part)
+    for s in (gpu, ora):
+        s.set_primitive(case.p, case.U, case.T, case.nuTilda)
+    rg, ro = gpu.step(5), ora.step(5)
+    for a, b in zip(rg, ro):
+        assert abs(a["res_mag"] - b["res_mag"]) <= 1e-8 * abs(b["res_mag"])
+    pg, Ug, Tg, ng = gpu.primitive()
+    po, Uo, To, no = ora.primitive()
+    assert rel(pg, po) < 1e-8 and rel(Ug, Uo) < 1e-8 and rel(Tg, To) < 1e-8 and rel(ng, no) < 1e-8
 
 
 def test_sa_residual_with_mut():
