@@ -189,6 +189,19 @@ def basis_bytes(options: dict) -> int:
     return 8 if b == "fp64" else 4
 
 
+def max_over_ranks(x: float) -> float:
+    """The maximum of x over the ranks of the default process group (the
+    job's time is its slowest rank's); x itself without one."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world):
     import torch
     import rhodst_b200
@@ -221,10 +234,7 @@ def run_ours(args, rank, world):
         torch.distributed.barrier()
     launches = s.launch_count() - launches0
     total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms)
     value = world * N * args.steps / (total_ms * 1e-3)
     # kernel classes and the roofline of the dominant one: CUDA events around
     # each launch (on the library's stream) over a separate run of the same
@@ -281,7 +291,7 @@ def run_ours(args, rank, world):
         s.set_conservative(rho, rhoU, rhoE)
         s.step(1)
         rho, rhoU, rhoE = s.conservative()
-    e2e_t = time.perf_counter() - t0
+    e2e_t = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * N * e2e_steps / e2e_t, "unit": "cell-iter/s",
            "h2d_bytes_per_step": int(rho.nbytes + rhoU.nbytes + rhoE.nbytes + 8 * 8 * N),
            "d2h_bytes_per_step": int(rho.nbytes + rhoU.nbytes + rhoE.nbytes)}
