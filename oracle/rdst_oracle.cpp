@@ -1852,7 +1852,7 @@ void single_iterate(Ctx& c, Report& rep) {
     if (c.o.turbulence == TURB_SARC1) c.rho0 = c.rho;     // rho.oldTime() of the turbulence update
     update_fields(c, dx);
     rep.flags = c.bounded ? 1 : 0;
-    if (c.o.turbulence != TURB_LAMINAR) sa_correct(c);      // turbulence_.correct()
+    if (c.o.turbulence != TURB_LAMINAR && !c.o.frozen_turbulence) sa_correct(c);   // turbulence_.correct()
     set_courant(c, rep);
     rep.t[4] = seconds_since(t0) * 1e3;
 }

@@ -1018,7 +1018,7 @@ void post_update(rdst_ctx& c) {
         k_update<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, c.dx.p, c.W.p, c.prim.p, c.sc.p); CKL();
     }
     k_boundary<<<nblk(c.NB, TPB), TPB, 0, s>>>(c.m, c.th, c.bd, c.W.p, c.prim.p, c.bs.p); CKL();
-    if (c.turb) sa_correct(c);          // turbulence_.correct()
+    if (c.turb && !c.o.frozen_turbulence) sa_correct(c);   // turbulence_.correct(); frozen: mu_t held
     k_courant_scalar<<<1, 1, 0, s>>>(c.sc.p, (!c.steady && c.o.adjust_time_step) ? 1 : 0, c.o.min_co, c.o.max_co); CKL();
     if (c.steady) {
         k_courant_cells<<<nblk(c.N, TPB), TPB, 0, s>>>(c.m, c.W.p, c.rhoOld.p, c.eOld.p, c.courantF.p, c.sc.p,

@@ -56,6 +56,7 @@ struct Options {
     bool low_mach = false;            // AUSM+up
     double mainf = 0.5;               // AUSM+up
     double venkat_K = 5.0;            // Venkatakrishnan constant (not in the reference)
+    bool frozen_turbulence = false;   // skip the turbulence update: mu_t held (not in the reference)
     // fvSchemes
     Ddt ddt = DDT_EULER;
     Limiter lim_rho = LIM_OSPRE, lim_U = LIM_OSPRE, lim_T = LIM_OSPRE;
@@ -205,6 +206,7 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
         else if (k == "Mainf") o.mainf = parse_double(k, v);
         else if (k == "addSpectralRadiusToPhysicalBoundaries") parse_bool(k, v);
         else if (k == "venkatakrishnanK") o.venkat_K = parse_double(k, v);
+        else if (k == "frozenTurbulence") o.frozen_turbulence = parse_bool(k, v);
         else if (k == "ddtSchemes.default") {
             if (t == "Euler") o.ddt = DDT_EULER;
             else if (t == "steadyStateDST") o.ddt = DDT_STEADY;

@@ -44,3 +44,13 @@ def test_new_state_restarts_the_old_time_strain_rate():
     assert np.array_equal(ra["res_l2"], rb["res_l2"])
     assert np.array_equal(a.primitive()[3], b.primitive()[3])
     assert W[0].shape[0] == case.mesh.n_cells
+
+
+def test_frozen_turbulence_holds_nu_tilda():
+    """frozenTurbulence skips the turbulence update: nuTilda stays while the
+    mean flow moves."""
+    case = airfoil("SAneg").with_options(frozenTurbulence=True)
+    o, _ = run(case, 3)
+    p, U, T, nut = o.primitive()
+    assert np.array_equal(nut, case.nuTilda)
+    assert np.abs(p - case.p).max() > 0
