@@ -1,4 +1,4 @@
-"""foam polyMesh input: the mesh of an existing rhoDST case.
+"""foam case input and output: the mesh and fields of an existing rhoDST case.
 
 `read_polymesh(dir)` reads an ASCII `constant/polyMesh` (points, faces,
 owner, neighbour, boundary) into a PolyMesh with the library's geometry
@@ -10,6 +10,11 @@ patch, wall, symmetryPlane/symmetry and empty.
 
 `save_npz` / `load_npz` store the topology compactly (a mesh read once can
 travel without the case directory).
+
+`read_field` reads an ASCII vol field (uniform or nonuniform internal
+field, per-patch entries, '#include' and '$' macros as the tutorials use
+them); `write_state` / `read_state` write and read p, U, T and nuTilda as a
+time directory a foam case restarts from.
 """
 from __future__ import annotations
 
@@ -161,3 +166,145 @@ def load_npz(path) -> _mesh.PolyMesh:
            zip(z["patch_names"], z["patch_types"], z["patch_start"], z["patch_size"])]
     return assemble(z["points"], z["faces"].astype(np.int64), z["owner"].astype(np.int64),
                     z["neighbour"].astype(np.int64), bnd)
+
+
+# ---------------------------------------------------------------- fields
+# ASCII volScalarField / volVectorField files: read the internal field
+# (uniform or nonuniform), the boundary patches' types and values, with
+# '#include' files and '$name' substitutions resolved the way the tutorials
+# use them; write the state as fields a foam case restarts from.
+
+def _resolve(path: Path, chain=()) -> str:
+    """File text with '#include "f"' replaced by the included text
+    (relative to the including file) and comments removed."""
+    path = Path(path)
+    if path in chain:
+        raise ValueError(f"#include loop at {path}")
+    text = path.read_text()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", " ", text)
+
+    def inc(m):
+        return _resolve(path.parent / m.group(1), chain + (path,))
+    return re.sub(r'#include\s+"([^"]+)"', inc, text)
+
+
+def _top_entries(text: str) -> dict:
+    """Top-level 'name value;' entries (values as strings)."""
+    out = {}
+    depth = 0
+    for m in re.finditer(r"[{}]|(\w+)\s+([^;{}]+);", text):
+        if m.group(0) == "{":
+            depth += 1
+        elif m.group(0) == "}":
+            depth -= 1
+        elif depth == 0 and m.group(1):
+            out[m.group(1)] = m.group(2).strip()
+    return out
+
+
+def _value(s: str, macros: dict):
+    """'uniform x' | 'uniform (a b c)' | 'nonuniform List<...> n (...)' |
+    '$name' -> float, tuple or array."""
+    s = s.strip()
+    for _ in range(8):
+        m = re.search(r"\$(\w+)", s)
+        if not m:
+            break
+        s = s[:m.start()] + macros[m.group(1)] + s[m.end():]
+    if s.startswith("uniform"):
+        s = s[len("uniform"):].strip()
+    if s.startswith("nonuniform"):
+        m = re.match(r"nonuniform\s+List<(\w+)>\s+(\d+)\s*\((.*)\)\s*$", s, flags=re.S)
+        if not m:
+            raise ValueError("nonuniform list not understood")
+        kind, n = m.group(1), int(m.group(2))
+        nums = np.array(re.findall(r"[-+0-9.eE]+", m.group(3)), dtype=float)
+        return nums.reshape(n, 3) if kind == "vector" else nums.reshape(n)
+    if s.startswith("("):
+        return tuple(float(x) for x in s.strip("()").split())
+    return float(s)
+
+
+def read_field(path):
+    """(internal, boundary): the internal field (float, 3-tuple or array)
+    and per patch a dict of its entries (type, value, ... as parsed)."""
+    text = _resolve(Path(path))
+    hdr = re.search(r"FoamFile\s*\{.*?\}", text, flags=re.S)
+    body = text[hdr.end():] if hdr else text
+    macros = {k: v for k, v in _top_entries(body).items()}
+    m = re.search(r"internalField\s+(.*?);\s*\n", body, flags=re.S)
+    internal = _value(m.group(1), macros)
+    bm = re.search(r"boundaryField\s*\{(.*)\}", body, flags=re.S)
+    boundary = {}
+    if bm:
+        for name, block in re.findall(r"(\w+)\s*\{(.*?)\}", bm.group(1), flags=re.S):
+            entries = {k: v.strip() for k, v in re.findall(r"(\w+)\s+([^;]+);", block)}
+            for k in ("value", "inletValue", "freestreamValue"):
+                if k in entries:
+                    entries[k] = _value(entries[k], macros)
+            boundary[name] = entries
+    return internal, boundary
+
+
+def _fmt_list(values: np.ndarray) -> str:
+    if values.ndim == 1:
+        kind = "scalar"
+        rows = "\n".join(repr(float(x)) for x in values)
+    else:
+        kind = "vector"
+        rows = "\n".join("(%r %r %r)" % (float(a), float(b), float(c)) for a, b, c in values)
+    return f"nonuniform List<{kind}> {values.shape[0]}\n(\n{rows}\n)"
+
+
+def write_field(path, name: str, values, mesh: _mesh.PolyMesh, boundary_values=None, dimensions="[0 0 0 0 0 0 0]"):
+    """An ASCII vol field with the cell values and, per non-empty patch,
+    'calculated' boundary values (boundary_values[patch] arrays, or the
+    adjacent cells' values)."""
+    values = np.asarray(values, dtype=float)
+    cls = "volScalarField" if values.ndim == 1 else "volVectorField"
+    own = np.asarray(mesh.owner)
+    lines = ["FoamFile", "{", "    version     2.0;", "    format      ascii;", f"    class       {cls};",
+             f"    object      {name};", "}", "", f"dimensions      {dimensions};", "",
+             f"internalField   {_fmt_list(values)};", "", "boundaryField", "{"]
+    for p in mesh.patches:
+        lines.append(f"    {p.name}")
+        lines.append("    {")
+        if p.type == _mesh.EMPTY:
+            lines.append("        type            empty;")
+        else:
+            bv = None if boundary_values is None else boundary_values.get(p.name)
+            if bv is None:
+                bv = values[own[p.start:p.start + p.size]]
+            lines.append("        type            calculated;")
+            lines.append(f"        value           {_fmt_list(np.asarray(bv, dtype=float))};")
+        lines.append("    }")
+    lines += ["}", ""]
+    Path(path).write_text("\n".join(lines))
+
+
+def write_state(directory, mesh: _mesh.PolyMesh, p, U, T, nuTilda=None):
+    """p, U, T (and nuTilda) of a solver state as a foam time directory."""
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    write_field(d / "p", "p", p, mesh, dimensions="[1 -1 -2 0 0 0 0]")
+    write_field(d / "U", "U", U, mesh, dimensions="[0 1 -1 0 0 0 0]")
+    write_field(d / "T", "T", T, mesh, dimensions="[0 0 0 1 0 0 0]")
+    if nuTilda is not None:
+        write_field(d / "nuTilda", "nuTilda", nuTilda, mesh, dimensions="[0 2 -1 0 0 0 0]")
+
+
+def read_state(directory, mesh: _mesh.PolyMesh):
+    """p, U, T, nuTilda (None when absent) as cell arrays from a time
+    directory (uniform fields expanded)."""
+    d = Path(directory)
+    N = mesh.n_cells
+
+    def cells(name, vec):
+        if not (d / name).exists():
+            return None
+        v, _ = read_field(d / name)
+        if isinstance(v, np.ndarray):
+            return v
+        return np.tile(np.asarray(v, dtype=float), (N, 1)) if vec else np.full(N, float(v))
+    return cells("p", False), cells("U", True), cells("T", False), cells("nuTilda", False)
