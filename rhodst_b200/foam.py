@@ -15,6 +15,11 @@ travel without the case directory).
 field, per-patch entries, '#include' and '$' macros as the tutorials use
 them); `write_state` / `read_state` write and read p, U, T and nuTilda as a
 time directory a foam case restarts from.
+
+`read_case(dir)` turns a whole rhoDST case directory into a Case: mesh,
+fields and boundary conditions, and the options of rhoDSTDict, fvSchemes,
+fvSolution, controlDict, thermophysicalProperties and RASProperties under
+their own names; `case.notes` lists the entries this path does not take.
 """
 from __future__ import annotations
 
@@ -308,3 +313,175 @@ def read_state(directory, mesh: _mesh.PolyMesh):
             return v
         return np.tile(np.asarray(v, dtype=float), (N, 1)) if vec else np.full(N, float(v))
     return cells("p", False), cells("U", True), cells("T", False), cells("nuTilda", False)
+
+
+# ---------------------------------------------------------------- case
+# A whole rhoDST case directory as a Case: the mesh, the 0/ fields and their
+# boundary conditions, and the options this path takes from system/ and
+# constant/ (rhoDSTDict, fvSchemes, fvSolution, controlDict,
+# thermophysicalProperties, RASProperties), with foam's own key names.
+
+def parse_dict(text: str) -> dict:
+    """A foam dictionary as nested dicts of strings (comments removed,
+    '#include' already resolved by the caller)."""
+    tokens = re.findall(r'"[^"]*"|[{};]|[^\s{};]+', text)
+    pos = 0
+
+    def block():
+        nonlocal pos
+        out = {}
+        while pos < len(tokens):
+            t = tokens[pos]
+            if t == "}":
+                pos += 1
+                return out
+            if t == ";":
+                pos += 1
+                continue
+            key = t
+            pos += 1
+            if pos < len(tokens) and tokens[pos] == "{":
+                pos += 1
+                out[key] = block()
+                continue
+            vals = []
+            depth = 0
+            while pos < len(tokens) and not (tokens[pos] == ";" and depth == 0):
+                if tokens[pos] == "{":
+                    depth += 1
+                elif tokens[pos] == "}":
+                    if depth == 0:
+                        break
+                    depth -= 1
+                vals.append(tokens[pos])
+                pos += 1
+            if pos < len(tokens) and tokens[pos] == ";":
+                pos += 1
+            out[key] = " ".join(vals)
+        return out
+    return block()
+
+
+def read_dict(path) -> dict:
+    text = _resolve(Path(path))
+    d = parse_dict(text)
+    d.pop("FoamFile", None)
+    return d
+
+
+def _bool(v: str) -> bool:
+    return v.strip().lower() in ("true", "yes", "on", "1")
+
+
+def _thermo(d: dict):
+    """(thermo, transport) options from thermophysicalProperties."""
+    ttype = d["thermoType"]
+    mix = d["mixture"].split()
+    # specie: name nMoles molWeight; hConstThermo: Cp Hf; transport: As Ts | mu Pr
+    mol_w, Cp = float(mix[2]), float(mix[3])
+    R = 8314.47 / mol_w
+    thermo = {"R": R, "Cp": Cp}
+    if "sutherlandTransport" in ttype:
+        As, Ts = float(mix[5]), float(mix[6])
+        Cv = Cp - R
+        return thermo, {"As": As, "Ts": Ts, "Pr": Cp / (1.32 * Cv + 1.77 * R)}   # Eucken conductivity
+    if "constTransport" in ttype:
+        mu, Pr = float(mix[5]), float(mix[6])
+        return thermo, ({"mu": mu, "Pr": Pr} if mu > 0 else None)
+    raise ValueError(f"thermoType {ttype} is not read")
+
+
+_FARFIELD_KEY = {"p": "pInf", "U": "UInf", "T": "TInf"}
+
+
+def _bc_spec(field: str, e: dict):
+    t = e["type"]
+    if t.startswith("farField"):
+        v = e[_FARFIELD_KEY[field]]
+        return ("farField", _value(v, {}) if not isinstance(v, (float, tuple)) else v)
+    if t == "fixedValue":
+        return ("fixedValue", e["value"])
+    if t == "inletOutlet":
+        return ("inletOutlet", e["inletValue"])
+    if t in ("zeroGradient", "slip", "symmetryPlane", "symmetry", "calculated"):
+        return t
+    raise ValueError(f"boundary condition {t} of {field} is not read")
+
+
+def read_case(directory, time: str = "0"):
+    """The case at `directory` (mesh, `time` fields, options) as a Case;
+    `case.notes` lists the entries this path does not take."""
+    from .cases import Case, _vector_limiter  # noqa: F401  (Case type)
+    d = Path(directory)
+    m = read_polymesh(d / "constant" / "polyMesh")
+    notes = []
+    rho = read_dict(d / "system" / "rhoDSTDict")
+    schemes = read_dict(d / "system" / "fvSchemes")
+    sol = read_dict(d / "system" / "fvSolution")
+    ctrl = read_dict(d / "system" / "controlDict")
+    thermo, transport = _thermo(read_dict(d / "constant" / "thermophysicalProperties"))
+    ras_path = d / "constant" / "RASProperties"
+    model = "laminar"
+    if ras_path.exists():
+        ras = read_dict(ras_path)
+        if _bool(ras.get("turbulence", "off")):
+            model = ras["RASModel"]
+    opts = {}
+    for k in ("fluxScheme", "Jacobian", "dependentVariable", "lowMach", "Mainf", "directWaveSpeed"):
+        if k in rho:
+            opts[k] = rho[k]
+    for sub in ("timeIntegration", "timeControls", "residualControls"):
+        if sub in rho:
+            opts[sub] = dict(rho[sub])
+    opts["ddtSchemes"] = {"default": schemes["ddtSchemes"]["default"]}
+    interp = schemes.get("interpolationSchemes", {})
+    opts["interpolationSchemes"] = {k: v for k, v in interp.items() if k.startswith("reconstruct(")}
+    for k, v in schemes.get("gradSchemes", {}).items():
+        if v.strip() != "Gauss linear":
+            notes.append(f"gradSchemes {k} {v}: Gauss linear here")
+    for k, v in schemes.get("divSchemes", {}).items():
+        if k.startswith("div(phi,nuTilda)") and "upwind" != v.split()[-1]:
+            notes.append(f"divSchemes {k} {v}: upwind here")
+    dep = opts.get("dependentVariable", "W")
+    W = sol["solvers"].get(dep, sol["solvers"].get("W"))
+    opts["solvers"] = {"W": {k: W[k] for k in ("solver", "preconditioner", "nDirections", "tolerance", "relTol",
+                                                "maxIter", "minIter") if k in W}}
+    if "relaxationFactors" in sol and "nuTilda" in sol["relaxationFactors"]:
+        opts["relaxationFactors"] = {"nuTilda": sol["relaxationFactors"]["nuTilda"]}
+    if "fieldBounds" in sol:
+        opts["fieldBounds"] = dict(sol["fieldBounds"])
+    opts["controlDict"] = {"deltaT": ctrl["deltaT"]}
+    if "startTime" in ctrl:
+        opts["controlDict"]["startTime"] = ctrl["startTime"]
+    opts["thermo"] = thermo
+    if transport:
+        opts["transport"] = transport
+    if model != "laminar":
+        opts["RASModel"] = model
+    # fields and boundary conditions
+    td = d / time
+    N = m.n_cells
+    fields, bfields = {}, {}
+    for f in ("p", "U", "T", "nuTilda"):
+        if (td / f).exists():
+            fields[f], bfields[f] = read_field(td / f)
+    bcs = {}
+    for p in m.patches:
+        if p.type == _mesh.EMPTY:
+            continue
+        spec = {}
+        for f in ("p", "U", "T", "nuTilda"):
+            if f in bfields and p.name in bfields[f]:
+                spec[f] = _bc_spec(f, bfields[f][p.name])
+        bcs[p.name] = spec
+
+    def cells(v, vec):
+        if isinstance(v, np.ndarray):
+            return v
+        return np.tile(np.asarray(v, dtype=float), (N, 1)) if vec else np.full(N, float(v))
+    if model != "laminar":
+        m.wall_distance = _mesh.wall_distance(m, [p.name for p in m.patches if p.type == _mesh.WALL])
+    case = Case(d.name, m, bcs, opts, cells(fields["p"], False), cells(fields["U"], True), cells(fields["T"], False),
+                nuTilda=cells(fields["nuTilda"], False) if "nuTilda" in fields else None)
+    case.notes = notes
+    return case

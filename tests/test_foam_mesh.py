@@ -139,3 +139,49 @@ def test_state_round_trip_through_foam_fields(tmp_path):
     # uniform fields expand to every cell
     q, _, _, _ = foam.read_state(tmp_path / "missing", c.mesh)
     assert q is None
+
+
+CASE = Path("/root/reference/tutorials/RAE2822")
+
+
+@pytest.mark.skipif(not CASE.exists(), reason="reference tree not present")
+def test_case_reader_gives_the_tutorial_case():
+    """read_case on the tutorial directory yields the options, boundary
+    conditions and initial fields cases.rae2822 sets (numerically), names
+    what this path does not take, and runs the same steps."""
+    from rhodst_b200._abi import flatten_options
+    from tests.oracle_lib import OracleSolver
+    a = foam.read_case(CASE)
+    b = cases.rae2822()
+    fa, fb = flatten_options(a.options), flatten_options(b.options)
+    fa.pop("controlDict.deltaT"); fa.pop("controlDict.startTime"); fa.pop("dependentVariable"); fb.pop("dependentVariable")
+    fa.pop("timeIntegration.timeIntegration")
+    assert fa.keys() == fb.keys()
+    for k in fa:
+        try:
+            va = [float(x) for x in fa[k].split()]
+            vb = [float(x) for x in fb[k].split()]
+            assert va == pytest.approx(vb, rel=1e-15), k
+        except ValueError:
+            assert fa[k].lower() == fb[k].lower(), k
+    assert a.bcs == b.bcs
+    assert np.array_equal(a.p, b.p) and np.array_equal(a.U, b.U) and np.array_equal(a.T, b.T)
+    assert np.array_equal(a.nuTilda, b.nuTilda)
+    assert any("cellLimited" in n for n in a.notes) and any("linearUpwind" in n for n in a.notes)
+    ra, rb = [], []
+    for c, out in ((a, ra), (b, rb)):
+        o = OracleSolver(c.mesh, c.bcs, c.options, rcb_parts=4)
+        o.set_primitive(c.p, c.U, c.T, c.nuTilda)
+        out += [r["res_l2"][0] for r in o.step(2)]
+    assert ra == rb
+
+
+def test_dictionary_parser():
+    d = foam.parse_dict("""
+        a 1;   b  (1 2 3);
+        sub { x yes; y "q w"; inner { z 1e-5; } }
+        c uniform (0 0 0);
+    """)
+    assert d["a"] == "1" and d["c"].split() == ["uniform", "(0", "0", "0)"]
+    assert d["b"].split() == ["(1", "2", "3)"]
+    assert d["sub"] == {"x": "yes", "y": '"q w"', "inner": {"z": "1e-5"}}
