@@ -16,6 +16,9 @@ field, per-patch entries, '#include' and '$' macros as the tutorials use
 them); `write_state` / `read_state` write and read p, U, T and nuTilda as a
 time directory a foam case restarts from.
 
+`block_mesh(dict)` builds the meshes tutorials define by blockMeshDict
+(hex blocks, simpleGrading, straight edges).
+
 `read_case(dir)` turns a whole rhoDST case directory into a Case: mesh,
 fields and boundary conditions, and the options of rhoDSTDict, fvSchemes,
 fvSolution, controlDict, thermophysicalProperties and RASProperties under
@@ -413,7 +416,13 @@ def read_case(directory, time: str = "0"):
     `case.notes` lists the entries this path does not take."""
     from .cases import Case, _vector_limiter  # noqa: F401  (Case type)
     d = Path(directory)
-    m = read_polymesh(d / "constant" / "polyMesh")
+    poly = d / "constant" / "polyMesh"
+    if (poly / "points").exists():
+        m = read_polymesh(poly)
+    elif (poly / "blockMeshDict").exists():
+        m = block_mesh(read_dict(poly / "blockMeshDict"))
+    else:
+        raise FileNotFoundError(f"{poly}: no polyMesh and no blockMeshDict")
     notes = []
     rho = read_dict(d / "system" / "rhoDSTDict")
     schemes = read_dict(d / "system" / "fvSchemes")
@@ -485,3 +494,100 @@ def read_case(directory, time: str = "0"):
                 nuTilda=cells(fields["nuTilda"], False) if "nuTilda" in fields else None)
     case.notes = notes
     return case
+
+
+# ---------------------------------------------------------------- blockMesh
+# Meshes that tutorials define by constant/polyMesh/blockMeshDict: hex
+# blocks with simpleGrading, straight edges, patches by block faces and the
+# unlisted boundary faces in 'defaultFaces' (empty), as blockMesh builds
+# them.  Cells are numbered block by block, the block's first direction
+# fastest; coincident points of neighbouring blocks are merged.
+
+def _graded(n: int, ratio: float) -> np.ndarray:
+    """n+1 coordinates in [0,1], last cell / first cell = ratio."""
+    if n < 1:
+        raise ValueError("a block needs at least one cell per direction")
+    if abs(ratio - 1.0) < 1e-14:
+        return np.linspace(0.0, 1.0, n + 1)
+    r = ratio ** (1.0 / (n - 1)) if n > 1 else 1.0
+    if n == 1 or abs(r - 1.0) < 1e-14:
+        return np.linspace(0.0, 1.0, n + 1)
+    x = (r ** np.arange(n + 1) - 1.0) / (r ** n - 1.0)
+    return x
+
+
+def _tuples(s: str):
+    return [tuple(float(x) for x in t.split()) for t in re.findall(r"\(([^()]*)\)", s)]
+
+
+def block_mesh(d: dict) -> _mesh.PolyMesh:
+    scale = float(d.get("convertToMeters", d.get("scale", "1")))
+    verts = np.array(_tuples(d["vertices"]), dtype=float) * scale
+    if re.search(r"\w", d.get("edges", "()").strip("() ")):
+        raise ValueError("curved block edges are not generated")
+    if re.search(r"\w", d.get("mergePatchPairs", "()").strip("() ")):
+        raise ValueError("mergePatchPairs is not generated")
+    blocks = re.findall(r"hex\s*\(([^)]*)\)\s*\(([^)]*)\)\s*simpleGrading\s*\(([^)]*)\)", d["blocks"])
+    if not blocks:
+        raise ValueError("no hex blocks")
+    corner = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+    pts_all, cells_all = [], []
+    base = 0
+    for vs, ns, gs in blocks:
+        v = verts[[int(x) for x in vs.split()]]
+        n = [int(x) for x in ns.split()]
+        g = [float(x) for x in gs.split()]
+        if len(g) != 3:
+            raise ValueError("simpleGrading with three ratios is generated")
+        s, t, u = (_graded(n[k], g[k]) for k in range(3))
+        S, T, Uu = np.meshgrid(s, t, u, indexing="ij")          # (nx+1, ny+1, nz+1)
+        w = [(1 - S) * (1 - T) * (1 - Uu), S * (1 - T) * (1 - Uu), S * T * (1 - Uu), (1 - S) * T * (1 - Uu),
+             (1 - S) * (1 - T) * Uu, S * (1 - T) * Uu, S * T * Uu, (1 - S) * T * Uu]
+        P = sum(w[k][..., None] * v[k] for k in range(8))       # trilinear in the block's corners
+        pid = base + np.arange(P[..., 0].size).reshape(P.shape[:3])
+        pts_all.append(P.reshape(-1, 3, order="C"))
+        # cells: i fastest, then j, then k; hex vertex order as foam's
+        k_, j_, i_ = np.meshgrid(np.arange(n[2]), np.arange(n[1]), np.arange(n[0]), indexing="ij")
+        i_, j_, k_ = i_.ravel(), j_.ravel(), k_.ravel()
+        c = np.stack([pid[i_, j_, k_], pid[i_ + 1, j_, k_], pid[i_ + 1, j_ + 1, k_], pid[i_, j_ + 1, k_],
+                      pid[i_, j_, k_ + 1], pid[i_ + 1, j_, k_ + 1], pid[i_ + 1, j_ + 1, k_ + 1],
+                      pid[i_, j_ + 1, k_ + 1]], axis=1)
+        cells_all.append(c)
+        base += P[..., 0].size
+    pts = np.concatenate(pts_all)
+    cells = np.concatenate(cells_all)
+    # merge coincident points (neighbouring blocks share their face points)
+    tol = 1e-9 * max(1.0, float(np.abs(pts).max()))
+    key = np.round(pts / tol).astype(np.int64)
+    _, first, inv = np.unique(key, axis=0, return_index=True, return_inverse=True)
+    order = np.argsort(first)
+    rank = np.empty_like(order)
+    rank[order] = np.arange(order.size)
+    pts = pts[first[order]]
+    cells = rank[inv.ravel()][cells]
+    # patches from block faces
+    bnd = d.get("boundary", {})
+    if isinstance(bnd, str):            # boundary ( name { type ..; faces (..); } ... )
+        body = bnd.strip()
+        if not (body.startswith("(") and body.endswith(")")):
+            raise ValueError("boundary must be a list of named patch dictionaries")
+        bnd = parse_dict(body[1:-1])
+    defs, quads = [], []
+    for name, pd in bnd.items():
+        defs.append((name, _PATCH_TYPES[pd["type"].strip()]))
+        quads.append([verts[[int(x) for x in q]] for q in
+                      [t.split() for t in re.findall(r"\(([^()]*)\)", pd.get("faces", ""))]])
+    defs.append(("defaultFaces", _mesh.EMPTY))
+
+    def classify(centres, normals):
+        out = np.full(centres.shape[0], len(defs) - 1)
+        for pi, qs in enumerate(quads):
+            for q in qs:
+                nq = np.cross(q[2] - q[0], q[3] - q[1])
+                nq /= np.linalg.norm(nq)
+                on = np.abs((centres - q[0]) @ nq) < 1e-9 * max(1.0, np.abs(q).max())
+                lo, hi = q.min(0) - 1e-12, q.max(0) + 1e-12
+                inside = np.all((centres >= lo) & (centres <= hi), axis=1)
+                out[on & inside] = pi
+        return out
+    return _mesh.build_polymesh(pts, [("hex", cells)], classify, defs)

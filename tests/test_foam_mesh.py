@@ -185,3 +185,60 @@ def test_dictionary_parser():
     assert d["a"] == "1" and d["c"].split() == ["uniform", "(0", "0", "0)"]
     assert d["b"].split() == ["(1", "2", "3)"]
     assert d["sub"] == {"x": "yes", "y": '"q w"', "inner": {"z": "1e-5"}}
+
+
+STEP = Path("/root/reference/tutorials/forwardStep")
+STEP_DUAL = Path("/root/reference/tutorials/forwardStepDual")
+
+
+@pytest.mark.skipif(not STEP.exists(), reason="reference tree not present")
+def test_block_mesh_tutorial_is_the_forward_step():
+    """The forwardStep tutorial's blockMeshDict gives the built-in generator's
+    mesh at full resolution (same cells, numbering and patches)."""
+    c = foam.read_case(STEP)
+    r = M.forward_step_2d(3)
+    assert np.abs(c.mesh.C - r.C).max() < 1e-12
+    assert np.array_equal(c.mesh.owner, r.owner) and np.array_equal(c.mesh.neighbour, r.neighbour)
+    assert [(p.name, p.type, p.start, p.size) for p in c.mesh.patches] == \
+           [(p.name, p.type, p.start, p.size) for p in r.patches]
+    assert c.bcs["obstacle"] == {"p": "zeroGradient", "U": "slip", "T": "zeroGradient"}
+    assert c.bcs["inlet"]["U"] == ("fixedValue", (3.0, 0.0, 0.0))
+    assert c.options["ddtSchemes"]["default"] == "Euler" and "transport" not in c.options
+    from tests.oracle_lib import OracleSolver
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T)
+    assert np.isfinite(o.step(1)[0]["res_mag"])
+
+
+@pytest.mark.skipif(not STEP_DUAL.exists(), reason="reference tree not present")
+def test_dual_time_tutorial_reads_and_runs():
+    from tests.oracle_lib import OracleSolver
+    c = foam.read_case(STEP_DUAL)
+    assert c.options["timeIntegration"]["timeIntegration"] == "Dual"
+    assert c.options["ddtSchemes"]["default"] == "dual2ndDST"
+    c = c.with_options(**{"timeIntegration.maxInnerIter": 2})
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T)
+    r = o.step(1)[0]
+    assert r["lin_iterations"] == 3 and np.isfinite(r["res_mag"])
+
+
+def test_block_mesh_grading_and_merging():
+    d = foam.parse_dict("""
+        vertices ((0 0 0) (1 0 0) (2 0 0) (0 1 0) (1 1 0) (2 1 0)
+                  (0 0 1) (1 0 1) (2 0 1) (0 1 1) (1 1 1) (2 1 1));
+        blocks (hex (0 1 4 3 6 7 10 9) (4 2 1) simpleGrading (2 1 1)
+                hex (1 2 5 4 7 8 11 10) (3 2 1) simpleGrading (1 1 1));
+        edges ();
+        boundary ( left { type patch; faces ((0 6 9 3)); }
+                   walls { type wall; faces ((0 1 7 6) (1 2 8 7) (3 9 10 4) (4 10 11 5)); } );
+    """)
+    m = foam.block_mesh(d)
+    assert m.n_cells == 14 and m.points.shape[0] == (5 + 3) * 3 * 2    # the shared x = 1 points merged
+    assert m.n_internal_faces == (3 * 2 + 4 * 1) + (2 * 2 + 3 * 1) + 2  # block 0, block 1, shared faces
+    xs = np.unique(np.round(m.points[:, 0], 12))
+    dx = np.diff(xs[xs <= 1 + 1e-12])
+    assert dx[-1] / dx[0] == pytest.approx(2.0)                         # last/first cell of block 0
+    names = [(p.name, p.type, p.size) for p in m.patches]
+    assert names == [("left", M.PATCH, 2), ("walls", M.WALL, 14), ("defaultFaces", M.EMPTY, 28 + 2)]
+    assert np.isclose(m.V.sum(), 2.0)
