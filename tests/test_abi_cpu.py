@@ -50,6 +50,8 @@ def test_partition_host_only():
     ("timeIntegration.timeIntegration", "Dual", 6),
     ("interpolationSchemes.reconstruct(U)", "OSPRE", 6),
     ("solvers.W.nDirections", "0", 1),
+    ("RASModel", "kEpsilon", 1),
+    ("timeIntegration.maxInnerIter", "-1", 1),
 ])
 def test_config_errors(key, value, status):
     case = cases.forward_step_c1().with_options(**{key: value})
@@ -70,3 +72,31 @@ def test_missing_flux_scheme():
 def test_flatten_options():
     f = _abi.flatten_options({"a": {"b": True, "c": (1.0, 2)}, "d": 1e-3})
     assert f == {"a.b": "true", "a.c": "1.0 2", "d": "0.001"}
+
+
+def test_dual_time_with_turbulence_is_rejected_before_device_work():
+    case = cases.naca0012_turbulent(ni=97, nj=25, first_cell=5e-3).with_options(**{
+        "timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST"})
+    with pytest.raises(_abi.RdstError) as e:
+        rhodst_b200.Solver(case.mesh, case.bcs, case.options)
+    assert e.value.status == 6
+
+
+def test_valid_options_reach_the_device_check():
+    """Options this path takes pass parsing; without a GPU the context
+    then fails at the CUDA device check, not earlier."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    for case in (cases.forward_step_c1().with_options(**{"timeIntegration.timeIntegration": "Dual",
+                                                         "ddtSchemes.default": "dual2ndDST"}),
+                 cases.rae2822(), cases.naca0012_turbulent(ni=97, nj=25, model="SARC1", first_cell=5e-3)):
+        with pytest.raises(_abi.RdstError) as e:
+            rhodst_b200.Solver(case.mesh, case.bcs, case.options)
+        assert e.value.status == 3, case.name
+
+
+def test_set_geometry_checks_its_arguments(gpulib):
+    gpulib.rdst_set_geometry.restype = ctypes.c_int32
+    gpulib.rdst_set_geometry.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    assert gpulib.rdst_set_geometry(None, None) == 7
