@@ -181,7 +181,8 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             else throw ConfigError("dependentVariable must be W or deltaW");
         }
         else if (k == "timeIntegration.timeIntegration") {
-            if (t == "Dual") o.dual = true;
+            // GPU / GPUDual: the foam adapter's selector names for Single / Dual
+            if (t == "Dual" || t == "GPUDual") o.dual = true;
             else if (t != "Single" && t != "GPU")
                 throw ConfigError("Unknown timeIntegration type " + t + "\nValid timeIntegration types are: (Dual Single)");
         }

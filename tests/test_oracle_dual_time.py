@@ -107,3 +107,14 @@ def test_dual_with_turbulence_is_rejected():
         "timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST"})
     with pytest.raises(RdstError):
         OracleSolver(c.mesh, c.bcs, c.options)
+
+
+def test_adapter_selector_name_selects_dual_time():
+    a = dual_case(**{"timeIntegration.maxInnerIter": 3})
+    b = a.with_options(**{"timeIntegration.timeIntegration": "GPUDual"})
+    ra = OracleSolver(a.mesh, a.bcs, a.options)
+    rb = OracleSolver(b.mesh, b.bcs, b.options)
+    for o, c in ((ra, a), (rb, b)):
+        o.set_primitive(c.p, c.U, c.T)
+    x, y = ra.step(1)[0], rb.step(1)[0]
+    assert x["lin_iterations"] == y["lin_iterations"] == 4 and x["res_mag"] == y["res_mag"]
