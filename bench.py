@@ -361,10 +361,8 @@ def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
     out["bf16_Cd_rel_diff"] = abs(out["bf16"]["Cd"] - out["fp64"]["Cd"]) / abs(out["fp64"]["Cd"])
     rep, _ = solvers["fp64"].adjoint(patch, drag, p_ref=1.0, scale=1.0 / qA, rel_tol=1e-8, max_cycles=30,
                                      n_directions=30)
-    dU_dM = c_inf * U0 / np.linalg.norm(U0)
-    dU_da = np.linalg.norm(U0) * np.array([-math.sin(alpha), math.cos(alpha), 0.0])
-    dJ_dM = float(rep["dJ_dU"] @ dU_dM)
-    dJ_da = float(rep["dJ_dU"] @ dU_da + rep["force"] @ np.array(lift))   # d(drag dir)/dalpha = lift dir
+    from rhodst_b200.shape import freestream_derivatives
+    dJ_dM, dJ_da = freestream_derivatives(rep["dJ_dU"], rep["force"], U0, c_inf, lift)
     out["adjoint"] = {"objective": f"pressure drag coefficient of patch {patch}", "J": rep["J"],
                       "device_s": rep["t_ms"] * 1e-3, "outer_iterations": rep["iterations"],
                       "residual_drop": rep["residual"] / rep["residual0"],

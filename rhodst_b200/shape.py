@@ -128,3 +128,22 @@ def shape_gradient(solver, param: HicksHenne, a: np.ndarray, patch: str, directi
                               max_cycles=max_cycles, n_directions=n_directions, want_psi=True)
     psi_dR, dJ = explicit_derivatives(solver, param, a, patch, direction, p_ref, scale, h, variables, psi=psi)
     return dJ - psi_dR, rep, psi
+
+
+def freestream_derivatives(dJ_dU, force, U_inf, c_inf: float, lift_dir=None):
+    """dJ/dMach and dJ/dalpha (per radian) from the adjoint's derivative
+    with respect to the free-stream velocity value (rdst_adjoint's dJ_dU)
+    and the objective's force vector, for a pressure-force objective whose
+    direction turns with the flow angle (drag: d(direction)/dalpha is the
+    lift direction).  The free stream U = Mach c (cos alpha, sin alpha, 0)."""
+    dJ_dU = np.asarray(dJ_dU, dtype=float)
+    U = np.asarray(U_inf, dtype=float)
+    speed = float(np.linalg.norm(U))
+    alpha = math.atan2(U[1], U[0])
+    dU_dM = c_inf * U / speed
+    dU_da = speed * np.array([-math.sin(alpha), math.cos(alpha), 0.0])
+    if lift_dir is None:
+        lift_dir = (-math.sin(alpha), math.cos(alpha), 0.0)
+    dJ_dM = float(dJ_dU @ dU_dM)
+    dJ_da = float(dJ_dU @ dU_da + np.asarray(force, dtype=float) @ np.asarray(lift_dir, dtype=float))
+    return dJ_dM, dJ_da

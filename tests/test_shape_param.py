@@ -72,3 +72,23 @@ def test_moved_mesh_keeps_topology_and_recomputes_geometry(base):
         assert np.array_equal(getattr(m, name), getattr(ref, name)), name
     # the volume change is of the order of the displacement
     assert 0 < np.abs(m.V - base.V).max() < 1e-2 * base.V.max()
+
+
+def test_freestream_derivatives_chain_rule():
+    """For J = a . U(M, alpha) + b . d(alpha), d = (cos, sin, 0) the drag
+    direction, the adjoint quantities dJ/dU = a and force = b give dJ/dMach
+    and dJ/dalpha; checked against central differences of J."""
+    import math
+    from rhodst_b200.shape import freestream_derivatives
+    a = np.array([0.3, -1.2, 0.7])
+    b = np.array([2.0, 0.5, -0.4])
+    c_inf, M0, al0 = 1.3, 0.73, math.radians(2.3)
+
+    def J(M, al):
+        U = M * c_inf * np.array([math.cos(al), math.sin(al), 0.0])
+        return a @ U + b @ np.array([math.cos(al), math.sin(al), 0.0])
+    U0 = M0 * c_inf * np.array([math.cos(al0), math.sin(al0), 0.0])
+    dM, da = freestream_derivatives(a, b, U0, c_inf)
+    h = 1e-6
+    assert dM == pytest.approx((J(M0 + h, al0) - J(M0 - h, al0)) / (2 * h), rel=1e-8)
+    assert da == pytest.approx((J(M0, al0 + h) - J(M0, al0 - h)) / (2 * h), rel=1e-8)
