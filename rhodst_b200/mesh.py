@@ -586,8 +586,9 @@ def forward_step_3d_hybrid(nx: int = 240, ny: int = 80, nz: int = 40, jitter: fl
 
     Channel 3.0 x 1.0 x 0.5, step 0.2 high at x = 0.6.  The structured
     lattice (nx, ny, nz) minus the step is split into prisms (two per hex,
-    z-extruded triangles) for y < prism_fraction and tetrahedra (six per
-    hex, Kuhn split) above.  Interior nodes are jittered by up to
+    y-extruded triangles) for y < prism_fraction and tetrahedra (six per
+    hex, Kuhn split) above; the prisms' triangles use the tetrahedra's face
+    diagonal, so the two layers are conforming.  Interior nodes are jittered by up to
     `jitter` x the local spacing, uniformly, from `seed`.
     Patches: inlet, outlet, obstacle (patch), walls (symmetryPlane: bottom,
     top, sides).
@@ -606,8 +607,7 @@ def forward_step_3d_hybrid(nx: int = 240, ny: int = 80, nz: int = 40, jitter: fl
     interior[:, 0, :] = interior[:, -1, :] = False
     interior[:, :, 0] = interior[:, :, -1] = False
     interior[sx:, :sy + 1, :] = False        # step surface and inside
-    jit = rng.uniform(-jitter, jitter, size=pts.shape) * np.array([hx, hy, hz])
-    pts = pts + jit * interior[..., None]
+    jit = rng.uniform(-jitter, jitter, size=pts.shape) * np.array([hx, hy, hz]) * interior[..., None]
     idx = np.arange(pts.shape[0] * pts.shape[1] * pts.shape[2]).reshape(pts.shape[:3])
     ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
     keep = ~((ii >= sx) & (jj < sy))
@@ -618,19 +618,40 @@ def forward_step_3d_hybrid(nx: int = 240, ny: int = 80, nz: int = 40, jitter: fl
     pr = (jj * hy) < prism_fraction * Ly
     hp = hexes[pr]
     ht = hexes[~pr]
-    # prisms: split the x-y quad along the 0-2 diagonal, extrude in z
-    p1 = np.stack([hp[:, 0], hp[:, 1], hp[:, 2], hp[:, 4], hp[:, 5], hp[:, 6]], axis=1)
-    p2 = np.stack([hp[:, 0], hp[:, 2], hp[:, 3], hp[:, 4], hp[:, 6], hp[:, 7]], axis=1)
+    # prisms: the x-z quad split along its (i,k)-(i+1,k+1) diagonal and
+    # extruded in y, the diagonal the Kuhn tetrahedra below use on their
+    # y-faces, so prism and tetrahedron layers share their triangles
+    p1 = np.stack([hp[:, 0], hp[:, 1], hp[:, 5], hp[:, 3], hp[:, 2], hp[:, 6]], axis=1)
+    p2 = np.stack([hp[:, 0], hp[:, 5], hp[:, 4], hp[:, 3], hp[:, 6], hp[:, 7]], axis=1)
     prisms = np.stack([p1, p2], axis=1).reshape(-1, 6)
     # Kuhn split of a hex into 6 tets along the 0-6 diagonal
     kuhn = [[0, 1, 2, 6], [0, 2, 3, 6], [0, 3, 7, 6], [0, 7, 4, 6], [0, 4, 5, 6], [0, 5, 1, 6]]
     tets = np.stack([ht[:, k] for k in kuhn], axis=1).reshape(-1, 4)
     ptsf = pts.reshape(-1, 3)
-    # orient tets positively
-    p = ptsf[tets]
-    v = np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), p[:, 3] - p[:, 0])
-    neg = v < 0
+
+    def tet_vol(P, t):
+        p = P[t]
+        return np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), p[:, 3] - p[:, 0])
+    # orient on the lattice: tets positively, prisms with the first triangle
+    # counter-clockwise seen along the extrusion
+    neg = tet_vol(ptsf, tets) < 0
     tets[neg] = tets[neg][:, [0, 2, 1, 3]]
+    neg = tet_vol(ptsf, prisms[:, :4]) < 0
+    prisms[neg] = prisms[neg][:, [0, 2, 1, 3, 5, 4]]
+    # jitter, halved at the corners of any cell it would flatten below a
+    # fifth of its lattice volume (a Kuhn tetrahedron is a sixth of a cube:
+    # a quarter-spacing move of its corners can invert it); prisms checked
+    # by their three tetrahedra
+    pr_tets = np.concatenate([prisms[:, [0, 1, 2, 3]], prisms[:, [1, 2, 3, 4]], prisms[:, [2, 3, 4, 5]]])
+    checks = np.concatenate([tets, pr_tets])
+    v0 = np.abs(tet_vol(ptsf, checks))
+    jf = jit.reshape(-1, 3).copy()
+    for _ in range(40):
+        bad = tet_vol(ptsf + jf, checks) < 0.2 * v0
+        if not np.any(bad):
+            break
+        jf[np.unique(checks[bad])] *= 0.5
+    ptsf = ptsf + jf
     used = np.unique(np.concatenate([prisms.ravel(), tets.ravel()]))
     remap = -np.ones(ptsf.shape[0], dtype=np.int64)
     remap[used] = np.arange(used.size)
