@@ -122,14 +122,19 @@ typedef struct rdst_ctx rdst_ctx;
  *   "Jacobian" "Roe"                 (rhoDSTDict; JacobianDST.C:72-91)
  *   "timeIntegration.timeIntegration" "Single"
  *   "timeControls.neighbouring" "true" ...
- *   "ddtSchemes.default" "Euler" | "steadyStateDST"
+ *   "ddtSchemes.default" "Euler" | "steadyStateDST" | "dual2ndDST"
  *   "interpolationSchemes.reconstruct(rho)" "OSPRE"
- *   "solvers.W.solver" "GMRES" | "BiCGStab"
- *   "solvers.W.preconditioner" "ILUC0" | "diagonal" | "none"
+ *   "solvers.W.solver" "GMRES" | "BiCGStab" | "GaussSeidel" | "ILU"
+ *   "solvers.W.preconditioner" "ILUC0" | "Cholesky" | "GaussSeidel" |
+ *                              "ILUCp" | "diagonal" | "none"
+ *   "solvers.W.nSweeps" "1"  "solvers.W.fillInLevel" "0"
  *   "fieldBounds.p" "0.001 10000"
  *   "thermo.R" / "thermo.Cp" / "transport.mu" / "transport.Pr" ...
- * Unknown selector values return RDST_ERR_CONFIG; reference options this
- * path rejects (directWaveSpeed false, AMG, dual2ndDST) RDST_ERR_UNSUPPORTED.
+ * (solver/preconditioner names as foam-extend registers them for the 5x5
+ * block matrix, Vector5typedefs.C:1602-1708).  Unknown selector values
+ * return RDST_ERR_CONFIG; reference options this path rejects
+ * (directWaveSpeed false, AMG, dual time with a turbulence model)
+ * RDST_ERR_UNSUPPORTED.
  * Replaces createFields.H:115-152 (flux, Jacobian and iteration selection)
  * and timeDST::initialize (timeDST.C:67-208). */
 rdst_status rdst_create(const rdst_mesh* mesh, int32_t n_options,

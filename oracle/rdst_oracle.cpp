@@ -1070,10 +1070,13 @@ void assemble(Ctx& c, LDU& A) {
 }
 
 // ----------------------------------------------------------------------
-// Block linear algebra: Amul, preconditioners, GMRES, BiCGStab (foam-extend
-// BlockLduMatrix::Amul, BlockDiagonalPrecon, BlockILUC0Precon,
-// BlockGMRESSolver, BlockBiCGStabSolver; restated from the published
-// algorithms, foam-extend 4.1 is not vendored)
+// Block linear algebra: Amul, preconditioners, GMRES, BiCGStab and the
+// stationary solvers (foam-extend BlockLduMatrix::Amul, BlockDiagonalPrecon,
+// BlockILUC0Precon, BlockCholeskyPrecon, BlockGaussSeidelPrecon,
+// BlockILUCpPrecon, BlockGMRESSolver, BlockBiCGStabSolver,
+// BlockGaussSeidelSolver, BlockILUSolver as instantiated at
+// libraries/vector5/Vector5typedefs/Vector5typedefs.C:1602-1708; restated
+// from the published algorithms, foam-extend 4.1 is not vendored)
 // ----------------------------------------------------------------------
 typedef std::vector<v5> Vec;
 
@@ -1108,10 +1111,12 @@ void vcopy(Vec& y, const Vec& x) {
 
 struct PreconData {
     int kind = PRECON_NONE;
-    std::vector<t5> Dinv;                 // diagonal: inv(D); ILU: inv(pivot)
-    // ILU(0) factors in CSR per row (cells in natural order)
+    int sweeps = 1;                       // Gauss-Seidel sweeps per application
+    const LDU* A = nullptr;               // the matrix (Gauss-Seidel residual sweeps)
+    std::vector<t5> Dinv;                 // diagonal: inv(D); factored: inv(pivot)
+    // factors in CSR per row (cells in natural order)
     std::vector<int> rowStart, col;       // off-diagonal columns per row, ascending
-    std::vector<t5> val;                  // L (k < i) or U (k > i) block
+    std::vector<t5> val;                  // L D~^-1 (k < i) or U (k > i) block
     std::vector<std::vector<int>> prow;   // rows of each partition part, ascending (independent)
 };
 
@@ -1138,12 +1143,19 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
         for (int i = 0; i < N; ++i) M.Dinv[i] = inv5(A.d[i]);
         return;
     }
-    if (M.kind != PRECON_ILU0) return;
-    // Exact block ILU(0) in cell order (IKJ form): for row i, for each k < i
+    if (!lu_factored((Precon)M.kind)) return;
+    M.A = &A;
+    M.sweeps = c.o.n_sweeps;
+    // Incomplete block LU in cell order (IKJ form): for row i, for each k < i
     // in the pattern: L_ik = A_ik inv(U_kk); A_ij -= L_ik U_kj for j > k in
-    // the pattern of row i.  Couplings between cells of different partition
-    // parts are dropped (block-Jacobi across parts, as foam-extend's ILUC0
-    // treats processor interfaces).
+    // the pattern of row i (j == i: the pivot).  ILUC0 keeps every update on
+    // the matrix pattern; ILUCp on the pattern extended to the cells within
+    // fillInLevel + 1 faces (foam-extend extendedLduAddressing: neighbours
+    // of neighbours, level by level); Cholesky keeps only the pivot updates
+    // (the diagonal-based factorisation (D~ + L) D~^-1 (D~ + U)); Gauss-Seidel
+    // keeps none (pivots = diagonal blocks).  Couplings between cells of
+    // different partition parts are dropped (block-Jacobi across parts, as
+    // foam-extend's preconditioners treat processor interfaces).
     std::vector<std::vector<std::pair<int, t5>>> rows(N);
     auto same = [&](int a, int b) { return c.part.empty() || c.part[a] == c.part[b]; };
     // row entries in face order (owner row: upper, neighbour row: lower)
@@ -1156,6 +1168,31 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
             if (P == i) rows[i].push_back({Q, A.u[f]});
             else rows[i].push_back({P, A.l[f]});
         }
+    if (M.kind == PRECON_ILUCP && c.o.fill_in > 0) {
+        // cells within fill_in + 1 faces (inside the part), zero blocks
+        std::vector<std::vector<int>> adj(N);
+        for (int i = 0; i < N; ++i)
+            for (auto& e : rows[i]) adj[i].push_back(e.first);
+        const t5 zero{};
+        OMP_FOR
+        for (int i = 0; i < N; ++i) {
+            std::vector<int> front = adj[i], seen = adj[i];
+            seen.push_back(i);
+            for (int lev = 0; lev < c.o.fill_in; ++lev) {
+                std::vector<int> next;
+                for (int a : front)
+                    for (int b2 : adj[a])
+                        if (std::find(seen.begin(), seen.end(), b2) == seen.end()) {
+                            seen.push_back(b2);
+                            next.push_back(b2);
+                        }
+                for (int b2 : next) rows[i].push_back({b2, zero});
+                front.swap(next);
+            }
+        }
+    }
+    const bool upd_off = M.kind == PRECON_ILU0 || M.kind == PRECON_ILUCP;
+    const bool upd_diag = upd_off || M.kind == PRECON_CHOLESKY;
     // one block per cell pair: faces joining the same pair are summed
     OMP_FOR
     for (int ii = 0; ii < N; ++ii) {
@@ -1196,9 +1233,11 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
                 int j = M.col[r];
                 if (j <= k) continue;
                 if (j == i) {
+                    if (!upd_diag) continue;
                     t5 t = mm(M.val[q], M.val[r]);
                     for (int e = 0; e < 25; ++e) D[i][e] -= t[e];
                 } else {
+                    if (!upd_off) continue;
                     for (int s = M.rowStart[i]; s < M.rowStart[i + 1]; ++s)
                         if (M.col[s] == j) {
                             t5 t = mm(M.val[q], M.val[r]);
@@ -1212,6 +1251,8 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
     }
 }
 
+void lu_apply(const Ctx& c, const PreconData& M, Vec& x, const Vec& b, bool upper);
+
 void precondition(const Ctx& c, const PreconData& M, Vec& x, const Vec& b) {
     const int N = c.N;
     x.resize(N);
@@ -1221,8 +1262,30 @@ void precondition(const Ctx& c, const PreconData& M, Vec& x, const Vec& b) {
         for (int i = 0; i < N; ++i) x[i] = mv(M.Dinv[i], b[i]);
         return;
     }
-    // per part (independent): forward y_i = b_i - sum_{k<i} L_ik y_k, then
-    // backward x_i = inv(U_ii) (y_i - sum_{j>i} U_ij x_j)
+    if (M.kind == PRECON_GAUSS_SEIDEL) {
+        // forward sweeps x += (D + L)^-1 (b - A x) from x = 0, L the
+        // same-part strict lower blocks (BlockGaussSeidelPrecon)
+        Vec r, z, t;
+        lu_apply(c, M, x, b, false);
+        for (int sw = 1; sw < M.sweeps; ++sw) {
+            Amul(c, *M.A, x, t);
+            r.resize(N);
+            OMP_FOR
+            for (int i = 0; i < N; ++i) for (int k = 0; k < 5; ++k) r[i][k] = b[i][k] - t[i][k];
+            lu_apply(c, M, z, r, false);
+            OMP_FOR
+            for (int i = 0; i < N; ++i) for (int k = 0; k < 5; ++k) x[i][k] += z[i][k];
+        }
+        return;
+    }
+    lu_apply(c, M, x, b, true);
+}
+
+// x = (L U)^-1 b with the stored factors, per part (independent): forward
+// y_i = b_i - sum_{k<i} L_ik y_k, then backward x_i = inv(U_ii) (y_i -
+// sum_{j>i} U_ij x_j) (without the U terms when `upper` is false)
+void lu_apply(const Ctx& c, const PreconData& M, Vec& x, const Vec& b, bool upper) {
+    x.resize(c.N);
     OMP_FOR_DYN
     for (int pp = 0; pp < (int)M.prow.size(); ++pp) {
         const std::vector<int>& rows = M.prow[pp];
@@ -1239,7 +1302,7 @@ void precondition(const Ctx& c, const PreconData& M, Vec& x, const Vec& b) {
         for (int r = (int)rows.size() - 1; r >= 0; --r) {
             const int i = rows[r];
             v5 y = x[i];
-            for (int q = M.rowStart[i]; q < M.rowStart[i + 1]; ++q) {
+            for (int q = M.rowStart[i]; q < M.rowStart[i + 1] && upper; ++q) {
                 int j = M.col[q];
                 if (j <= i) continue;
                 v5 t = mv(M.val[q], x[j]);
@@ -1357,6 +1420,21 @@ void linear_solve(Ctx& c, const LDU& A, const PreconData& M, Vec& dx, Report& re
             OMP_FOR
             for (int q = 0; q < N; ++q)
                 for (int i = 0; i < used; ++i) for (int k = 0; k < 5; ++k) dx[q][k] += yh[i] * Vk[i][q][k];
+            Amul(c, A, dx, t);
+            OMP_FOR
+            for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) r[q][k] = A.s[q][k] - t[q][k];
+            cmpt_residual(r, nf, rep.lin_final);
+            ++it;
+        }
+    } else if (o.solver == SOLVER_GAUSS_SEIDEL || o.solver == SOLVER_ILU) {
+        // stationary iteration dx += M^-1 (b - A dx) with Gauss-Seidel sweeps
+        // or the Cholesky-type factorisation (BlockGaussSeidelSolver,
+        // BlockILUSolver), the residual checked after every application
+        Vec z, t;
+        while (!converged(o, rep.lin_initial, rep.lin_final, it)) {
+            precondition(c, M, z, r);
+            OMP_FOR
+            for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) dx[q][k] += z[q][k];
             Amul(c, A, dx, t);
             OMP_FOR
             for (int q = 0; q < N; ++q) for (int k = 0; k < 5; ++k) r[q][k] = A.s[q][k] - t[q][k];

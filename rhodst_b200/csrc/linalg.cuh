@@ -123,6 +123,13 @@ __global__ void k_jacobi(int N, const MT* __restrict__ dinv, const double* __res
     }
 }
 
+// y += x (skipped when *active is 0)
+__global__ void k_vadd(long n, const double* __restrict__ x, double* __restrict__ y, const int* __restrict__ active) {
+    if (active && !*active) return;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += x[i];
+}
+
 template <typename MT>
 __global__ void k_copy_identity(int n, const double* __restrict__ x, double* __restrict__ y, const int* __restrict__ active) {
     if (active && !*active) return;
@@ -148,6 +155,7 @@ struct IluDev {
     const int* tr_kj;       // factor id of U_kj
     const int* tr_rj;       // factor id of A_rj (-1: diagonal)
     int ml, mu;             // factor slots per row
+    int mu_use;             // U slots the backward sweep applies (0: (D + L)^-1 of Gauss-Seidel)
     const int* lu_col;      // [fid] column of each factor slot (-1: empty)
     const int* lu_src;      // [fid] SELL flat slot of the same block in A
 };
@@ -157,13 +165,19 @@ __device__ __forceinline__ int lu_fid(int r, int s, int ms) { return ((r >> 5) *
 constexpr int ILU_TPB = 128;
 
 // same-subdomain blocks of A -> factor storage (fully parallel, before the
-// level-scheduled factorisation); empty slots stay zero
+// level-scheduled factorisation); fill slots outside the matrix pattern
+// (lu_src -2) restart from zero, empty slots (-1) stay zero
 template <typename MT>
 __global__ void k_ilu_gather(SellMat<MT> A, MT* __restrict__ lu, const int* __restrict__ lu_src, int n_fid) {
     const int fid = blockIdx.x * blockDim.x + threadIdx.x;
     if (fid >= n_fid) return;
     const int src = lu_src[fid];
-    if (src < 0) return;
+    if (src == -1) return;
+    if (src < 0) {
+#pragma unroll
+        for (int e = 0; e < 25; ++e) lu[flat_e(fid, e)] = mt_zero<MT>();
+        return;
+    }
 #pragma unroll
     for (int e = 0; e < 25; ++e) lu[flat_e(fid, e)] = A.val[flat_e(src, e)];
 }
@@ -311,7 +325,7 @@ __global__ void __launch_bounds__(ILU_APPLY_TPB, ILU_APPLY_MINB)
     for (int sweep = 0; sweep < 2; ++sweep) {
         const bool back = sweep == 1;
         const int dir = back ? -1 : 1;
-        const int s0 = back ? ml : 0, ns = back ? mu : ml;
+        const int s0 = back ? ml : 0, ns = back ? P.mu_use : ml;
         const double* ysrc = back ? x : b;
         IluCursor cur{back ? l1 - 1 : l0, 0};
         auto in_range = [&](int l) { return back ? l >= l0 : l < l1; };

@@ -189,9 +189,10 @@ struct rdst_ctx {
     int n_parts = 1;
     DBuf<int> part_lvl0, lvl_off, low_start, nlu, tr_start, tr_kj, tr_rj, lu_col, lu_src;
     int lu_slots = 0;
-    int ilu_ml = 0, ilu_mu = 0;
+    int ilu_ml = 0, ilu_mu = 0, ilu_mu_use = 0;
     // Krylov
     DBuf<double> dx, r, t, Vb, s2, sh, ph, pv, xbar, Ax, pA;
+    DBuf<double> gs_r, gs_z;        // residual and correction of Gauss-Seidel sweeps after the first
     DBuf<float> Vf;                 // GMRES basis when it is kept in FP32
     long ldv = 0;                   // stride between basis vectors (entries)
     DBuf<double> wv;                // FP64 Arnoldi vector that is orthogonalised before it is stored in Vf
@@ -292,7 +293,7 @@ struct rdst_ctx {
     IluDev ilu() const {
         IluDev P;
         P.n_parts = n_parts; P.part_lvl0 = part_lvl0.p; P.lvl_off = lvl_off.p;
-        P.nlu = nlu.p; P.low_start = low_start.p; P.ml = ilu_ml; P.mu = ilu_mu; P.lu_col = lu_col.p; P.lu_src = lu_src.p;
+        P.nlu = nlu.p; P.low_start = low_start.p; P.ml = ilu_ml; P.mu = ilu_mu; P.mu_use = ilu_mu_use; P.lu_col = lu_col.p; P.lu_src = lu_src.p;
         P.tr_start = tr_start.p; P.tr_kj = tr_kj.p; P.tr_rj = tr_rj.p;
         return P;
     }
@@ -470,29 +471,59 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     for (int f = 0; f < Fi; ++f) { cfaces[mh->owner[f]].push_back(f); cfaces[mh->neighbour[f]].push_back(f); }
     for (int b = 0; b < NB; ++b) cfaces[mh->owner[c.bface_orig[b]]].push_back(Fi + b);
     for (auto& v : cfaces) std::sort(v.begin(), v.end());
-    // partition + wavefront levels for the subdomain ILU(0)
+    // partition + wavefront levels for the subdomain factorisations.  The
+    // factor pattern of a row (original numbering) is its same-part face
+    // neighbours, or for ILUCp the same-part cells within fill_in + 1 faces
+    // (neighbours of neighbours, level by level, as foam-extend's
+    // extendedLduAddressing builds them).
     std::vector<int> part(N, 0), level(N, 0);
+    std::vector<std::vector<int>> lupat;
     int nparts = 1;
-    if (o.precon == PRECON_ILU0) {
+    const bool factored = lu_factored(o.precon);
+    if (factored) {
         nparts = o.ilu_parts > 0 ? o.ilu_parts : auto_ilu_parts(N, o.precision);
         nparts = std::min(nparts, N);
         std::vector<int> idx(N);
         std::iota(idx.begin(), idx.end(), 0);
         rcb(mh->C, idx, 0, N, 0, nparts, part.data());
-        for (int i = 0; i < N; ++i) {
-            int lv = 0;
+        lupat.resize(N);
+        for (int i = 0; i < N; ++i)
             for (int f : cfaces[i]) {
                 if (f >= Fi) continue;
                 int k = mh->owner[f] == i ? mh->neighbour[f] : mh->owner[f];
-                if (k < i && part[k] == part[i]) lv = std::max(lv, level[k] + 1);
+                if (part[k] == part[i]) lupat[i].push_back(k);
             }
+        for (auto& v : lupat) { std::sort(v.begin(), v.end()); v.erase(std::unique(v.begin(), v.end()), v.end()); }
+        if (o.precon == PRECON_ILUCP && o.fill_in > 0) {
+            std::vector<std::vector<int>> ext(N);
+            std::vector<int> mark(N, -1);
+            for (int i = 0; i < N; ++i) {
+                std::vector<int> front = lupat[i], seen = lupat[i];
+                mark[i] = i;
+                for (int k : front) mark[k] = i;
+                for (int lev = 0; lev < o.fill_in; ++lev) {
+                    std::vector<int> next;
+                    for (int a : front)
+                        for (int b2 : lupat[a])
+                            if (mark[b2] != i) { mark[b2] = i; next.push_back(b2); seen.push_back(b2); }
+                    front.swap(next);
+                }
+                std::sort(seen.begin(), seen.end());
+                ext[i].swap(seen);
+            }
+            lupat.swap(ext);
+        }
+        for (int i = 0; i < N; ++i) {
+            int lv = 0;
+            for (int k : lupat[i])
+                if (k < i) lv = std::max(lv, level[k] + 1);
             level[i] = lv;
         }
     }
     c.n_parts = nparts;
     c.perm.resize(N);
     std::iota(c.perm.begin(), c.perm.end(), 0);
-    if (o.precon == PRECON_ILU0)
+    if (factored)
         std::stable_sort(c.perm.begin(), c.perm.end(), [&](int a, int b) {
             if (part[a] != part[b]) return part[a] < part[b];
             return level[a] < level[b];
@@ -571,42 +602,51 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
             seen[pos] = 1;
         }
     }
-    // ---- ILU plan.  The factors live in their own ELL layout, factor slot s
-    // x cell: L_q (same-subdomain lower, by column) at s = q < ML, U_q at
-    // s = ML + q; entries interleaved by cell, lu_val[(s*25 + e)*N + r].
-    // Wavefront levels are contiguous row ranges per subdomain.
-    if (o.precon == PRECON_ILU0) {
+    // ---- factorisation plan.  The factors live in their own ELL layout,
+    // factor slot s x cell: L_q (same-subdomain lower, by column) at
+    // s = q < ML, U_q at s = ML + q; entries interleaved by cell,
+    // lu_val[(s*25 + e)*N + r].  Wavefront levels are contiguous row ranges
+    // per subdomain.  Slots outside the matrix pattern (ILUCp fill) start
+    // from zero blocks.
+    if (factored) {
+        std::vector<std::vector<int>> lurows(N);     // factor pattern in row order, ascending
+        for (int r = 0; r < N; ++r) {
+            for (int k : lupat[c.perm[r]]) lurows[r].push_back(c.iperm[k]);
+            std::sort(lurows[r].begin(), lurows[r].end());
+        }
         std::vector<int> nl(N, 0), nu(N, 0);
         for (int r = 0; r < N; ++r)
-            for (int cc : rowcols[r])
-                if (ipart[cc] == ipart[r]) { if (cc < r) ++nl[r]; else ++nu[r]; }
+            for (int cc : lurows[r]) { if (cc < r) ++nl[r]; else ++nu[r]; }
         const int ML = *std::max_element(nl.begin(), nl.end());
         const int MU = *std::max_element(nu.begin(), nu.end());
-        if (ML > 8 || MU > 8) throw std::invalid_argument("a cell has more than 8 lower/upper neighbours");
+        if (ML > 8 || MU > 8) {
+            if (o.precon == PRECON_ILUCP && o.fill_in > 0)
+                throw ConfigError("ILUCp fillInLevel " + std::to_string(o.fill_in) +
+                                  " gives a cell more than 8 lower/upper factor blocks on this mesh", true);
+            throw std::invalid_argument("a cell has more than 8 lower/upper neighbours");
+        }
         c.ilu_ml = ML;
         c.ilu_mu = MU;
+        // Gauss-Seidel applies (D + L)^-1: the backward sweep uses no U blocks
+        c.ilu_mu_use = o.precon == PRECON_GAUSS_SEIDEL ? 0 : MU;
         const int MS = std::max(ML + MU, 1);
         // factor id of slot s of row r: slices of 32 rows, MS slots each,
         // entries interleaved by lane (the SELL addressing with width MS)
         auto lfid = [&](int r, int sl) { return ((r >> 5) * MS + sl) * 32 + (r & 31); };
         std::vector<int> lu_col((size_t)c.n_slices * MS * 32, -1), lu_src((size_t)c.n_slices * MS * 32, -1);
         auto fid_of = [&](int r, int cc) {     // factor id of coupling (r, cc), or -1
-            int q = 0;
-            if (cc < r) {
-                for (int x : rowcols[r]) { if (x == cc) return lfid(r, q); if (x < r && ipart[x] == ipart[r]) ++q; }
-            } else {
-                for (int x : rowcols[r]) { if (x == cc) return lfid(r, ML + q); if (x > r && ipart[x] == ipart[r]) ++q; }
-            }
-            return -1;
+            auto it = std::lower_bound(lurows[r].begin(), lurows[r].end(), cc);
+            if (it == lurows[r].end() || *it != cc) return -1;
+            const int k = (int)(it - lurows[r].begin());
+            return cc < r ? lfid(r, k) : lfid(r, ML + k - nl[r]);
         };
         for (int r = 0; r < N; ++r) {
             int ql = 0, qu = 0;
-            for (size_t k = 0; k < rowcols[r].size(); ++k) {
-                int cc = rowcols[r][k];
-                if (ipart[cc] != ipart[r]) continue;
+            for (int cc : lurows[r]) {
                 int sidx = cc < r ? ql++ : ML + qu++;
                 lu_col[lfid(r, sidx)] = cc;
-                lu_src[lfid(r, sidx)] = flat(r, 1 + (int)k);
+                const int pos = pos_of(r, cc);
+                lu_src[lfid(r, sidx)] = pos >= 0 ? flat(r, 1 + pos) : -2;   // -2: fill, zeroed per factorisation
             }
         }
         std::vector<int> lvl_off, part_lvl0(nparts + 1, 0);
@@ -624,7 +664,10 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         }
         // IKJ update triples: for each L_rk (row order, then q), the pairs
         // (U_kj, A_rj) with j > k in row k's upper factor and in row r's
-        // pattern (j == r: the diagonal, encoded -1)
+        // pattern (j == r: the diagonal, encoded -1).  Cholesky keeps only
+        // the diagonal ones, Gauss-Seidel none.
+        const bool upd_off = o.precon == PRECON_ILU0 || o.precon == PRECON_ILUCP;
+        const bool upd_diag = upd_off || o.precon == PRECON_CHOLESKY;
         std::vector<int> nlu(N), low_start(N + 1, 0), tr_start(1, 0), tr_kj, tr_rj;
         for (int r = 0; r < N; ++r) {
             nlu[r] = nl[r] | (nu[r] << 8);
@@ -636,8 +679,11 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
                 for (int u = 0; u < nu[k]; ++u) {
                     int j = lu_col[lfid(k, ML + u)];
                     int kj = lfid(k, ML + u);
-                    if (j == r) { tr_kj.push_back(kj); tr_rj.push_back(-1); continue; }
-                    if (ipart[j] != ipart[r]) continue;
+                    if (j == r) {
+                        if (upd_diag) { tr_kj.push_back(kj); tr_rj.push_back(-1); }
+                        continue;
+                    }
+                    if (!upd_off || ipart[j] != ipart[r]) continue;
                     int rj = fid_of(r, j);
                     if (rj >= 0) { tr_kj.push_back(kj); tr_rj.push_back(rj); }
                 }
@@ -707,12 +753,13 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     size_t mbytes = (size_t)c.n_slots * 32 * 25 * c.mt_size;
     CK(cudaMalloc(&c.Aval, mbytes));
     CK(cudaMemsetAsync(c.Aval, 0, mbytes, s));
-    if (o.precon == PRECON_ILU0) {
+    if (factored) {
         size_t lbytes = (size_t)c.n_slices * c.lu_slots * 32 * 25 * c.mt_size;
         CK(cudaMalloc(&c.LUval, lbytes));
         CK(cudaMemsetAsync(c.LUval, 0, lbytes, s));
     }
     if (o.precon != PRECON_NONE) CK(cudaMalloc(&c.dinv, (size_t)c.n_slices * 32 * 25 * c.mt_size));
+    if (o.precon == PRECON_GAUSS_SEIDEL && o.n_sweeps > 1) { c.gs_r.alloc(5L * N); c.gs_z.alloc(5L * N); }
     // ---- Krylov
     const long n5 = 5L * N;
     c.dx.alloc(n5); c.r.alloc(n5); c.t.alloc(n5); c.Ax.alloc(n5); c.pA.alloc(n5); c.xbar.alloc(8);
@@ -783,7 +830,7 @@ struct Ops {
         if (c.o.precon == PRECON_DIAGONAL) {
             k_dinv<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.dinv);
             CKL();
-        } else if (c.o.precon == PRECON_ILU0) {
+        } else if (lu_factored(c.o.precon)) {
             Timed tm(c, KS_FACTOR);
             const int n_fid = c.n_slices * c.lu_slots * 32;
             k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, c.lu_src.p, n_fid);
@@ -792,25 +839,39 @@ struct Ops {
             CKL();
         }
     }
+    // out = (L U)^-1 in with the stored factors
+    static void lu_apply(rdst_ctx& c, const double* in, double* out, const int* active) {
+        const int nb = std::max(c.ilu_ml, c.ilu_mu);
+        const MT* LU = (const MT*)c.LUval;
+        auto P = c.ilu();
+        const MT* di = (const MT*)c.dinv;
+        const int N = c.N;
+        if (nb <= 2) k_ilu_apply<MT, 2><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        else if (nb <= 3) k_ilu_apply<MT, 3><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        else if (nb <= 4) k_ilu_apply<MT, 4><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        else if (nb <= 6) k_ilu_apply<MT, 6><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        else k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        CKL();
+    }
     static void precond(rdst_ctx& c, const double* in, double* out, const int* active) {
         Timed tm(c, KS_PRECOND);
-        if (c.o.precon == PRECON_DIAGONAL)
+        if (c.o.precon == PRECON_DIAGONAL) {
             k_jacobi<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.N, (const MT*)c.dinv, in, out, active);
-        else if (c.o.precon == PRECON_ILU0) {
-            const int nb = std::max(c.ilu_ml, c.ilu_mu);
-            const MT* LU = (const MT*)c.LUval;
-            auto P = c.ilu();
-            const MT* di = (const MT*)c.dinv;
-            const int N = c.N;
-            if (nb <= 2) k_ilu_apply<MT, 2><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-            else if (nb <= 3) k_ilu_apply<MT, 3><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-            else if (nb <= 4) k_ilu_apply<MT, 4><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-            else if (nb <= 6) k_ilu_apply<MT, 6><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-            else k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-        }
-        else
+            CKL();
+        } else if (lu_factored(c.o.precon)) {
+            lu_apply(c, in, out, active);
+            // further Gauss-Seidel sweeps: out += (D + L)^-1 (in - A out)
+            for (int sw = 1; c.o.precon == PRECON_GAUSS_SEIDEL && sw < c.o.n_sweeps; ++sw) {
+                k_spmv<MT, double><<<nblk(c.N, 256), 256, 0, c.s>>>(c.mat<MT>(c.Aval), out, c.gs_r.p, in, active);
+                CKL();
+                lu_apply(c, c.gs_r.p, c.gs_z.p, active);
+                k_vadd<<<nblk(c.nvec(), TPB), TPB, 0, c.s>>>(c.nvec(), c.gs_z.p, out, active);
+                CKL();
+            }
+        } else {
             k_copy_identity<MT><<<nblk(c.nvec(), TPB), TPB, 0, c.s>>>((int)c.nvec(), in, out, active);
-        CKL();
+            CKL();
+        }
     }
     template <typename XT>
     static void spmv(rdst_ctx& c, const XT* x, double* y, const double* b, const int* active) {
@@ -842,6 +903,8 @@ struct Ops {
             c.pv.zero(s);
             CK(cudaMemsetAsync(c.ph.p, 0, sizeof(double) * c.nvec(), s));
             k_bi_init<<<1, 1, 0, s>>>(c.sc.p); CKL();
+        } else if (c.o.solver != SOLVER_GMRES) {
+            CK(cudaMemcpyAsync(c.r.p, c.rhs.p, sizeof(double) * c.nvec(), cudaMemcpyDeviceToDevice, s));
         }
     }
     static void dot(rdst_ctx& c, const double* a, const double* b, double* out, int sq, const int* active) {
@@ -955,9 +1018,18 @@ struct Ops {
         k_linres_finalize<<<1, RED_TPB, 0, s>>>(c.partial.p, nb, sc, 0); CKL();
         k_check<<<1, 1, 0, s>>>(sc, c.o.tolerance, c.o.rel_tol, c.o.min_iter, c.o.max_iter, 1); CKL();
     }
+    // one stationary iteration dx += M^-1 (rhs - A dx) (Gauss-Seidel sweeps
+    // or the Cholesky-type factorisation), then the residual check
+    static void stationary_iter(rdst_ctx& c) {
+        precond(c, c.r.p, c.t.p, nullptr);
+        k_vadd<<<nblk(c.nvec(), TPB), TPB, 0, c.s>>>(c.nvec(), c.t.p, c.dx.p, nullptr);
+        CKL();
+        finish_iteration(c);
+    }
     static void iteration(rdst_ctx& c) {
         if (c.o.solver == SOLVER_GMRES) gmres_cycle(c);
-        else bicgstab_iter(c);
+        else if (c.o.solver == SOLVER_BICGSTAB) bicgstab_iter(c);
+        else stationary_iter(c);
     }
 };
 
@@ -1539,7 +1611,7 @@ void adj_precond_setup(rdst_ctx& c) {
     if (c.o.precon == PRECON_DIAGONAL) {
         k_dinv<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.dinv);
         CKL();
-    } else if (c.o.precon == PRECON_ILU0) {
+    } else if (lu_factored(c.o.precon)) {
         const int n_fid = c.n_slices * c.lu_slots * 32;
         k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, c.lu_src.p, n_fid);
         CKL();
@@ -1550,7 +1622,10 @@ void adj_precond_setup(rdst_ctx& c) {
 
 template <typename MT>
 void adj_precond(rdst_ctx& c, const double* in, double* out) {
+    // Gauss-Seidel sweeps after the first take their residual with A^T
+    std::swap(c.Aval, c.a_AT);
     Ops<MT>::precond(c, in, c.a_tmp.p, nullptr);
+    std::swap(c.Aval, c.a_AT);
     k_adj_scale_V<<<nblk(5L * c.N, TPB), TPB, 0, c.s>>>(c.N, c.m.V, c.a_tmp.p, out);
     CKL();
 }

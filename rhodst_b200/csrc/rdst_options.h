@@ -24,11 +24,21 @@ enum FluxScheme { FLUX_KURGANOV = 0, FLUX_HLL, FLUX_HLLC, FLUX_HLLCP, FLUX_AUSMP
                   FLUX_AUSMPLUSUP, FLUX_AUSM };
 enum Limiter { LIM_LINEAR = 0, LIM_UPWIND, LIM_OSPRE, LIM_VANLEER, LIM_MINMOD, LIM_VANALBADA,
                LIM_SUPERBEE, LIM_MUSCL, LIM_VENKATAKRISHNAN };
-enum Solver { SOLVER_GMRES = 0, SOLVER_BICGSTAB };
-enum Precon { PRECON_NONE = 0, PRECON_DIAGONAL, PRECON_ILU0 };
+enum Solver { SOLVER_GMRES = 0, SOLVER_BICGSTAB, SOLVER_GAUSS_SEIDEL, SOLVER_ILU };
+// ILU0: ILUC0 (exact ILU on the matrix pattern); CHOLESKY: the diagonal-only
+// incomplete factorisation (D~ + L) D~^-1 (D~ + U); GAUSS_SEIDEL: forward
+// block Gauss-Seidel sweeps (D + L)^-1; ILUCP: ILU on the pattern extended
+// to cells within fillInLevel + 1 faces
+enum Precon { PRECON_NONE = 0, PRECON_DIAGONAL, PRECON_ILU0, PRECON_CHOLESKY, PRECON_GAUSS_SEIDEL, PRECON_ILUCP };
 enum Ddt { DDT_EULER = 0, DDT_STEADY, DDT_DUAL2ND };
 enum Precision { PREC_FP64 = 0, PREC_FP32, PREC_BF16 };
 enum Turbulence { TURB_LAMINAR = 0, TURB_SANEG, TURB_SARC1, TURB_SARC2, TURB_SA };
+
+// preconditioners stored as incomplete block-LU factors (pivot inverses and
+// L D~^-1 / U blocks on a row pattern)
+inline bool lu_factored(Precon p) {
+    return p == PRECON_ILU0 || p == PRECON_CHOLESKY || p == PRECON_GAUSS_SEIDEL || p == PRECON_ILUCP;
+}
 
 // Thrown by the parser; mapped to RDST_ERR_CONFIG / RDST_ERR_UNSUPPORTED.
 struct ConfigError : std::runtime_error {
@@ -66,6 +76,8 @@ struct Options {
     int n_directions = 8;
     double tolerance = 1e-6, rel_tol = 0.0;
     int max_iter = 1000, min_iter = 0;
+    int n_sweeps = 1;                 // Gauss-Seidel sweeps per application (nSweeps)
+    int fill_in = 0;                  // ILUCp extension level (fillInLevel)
     // fvSolution: fieldBounds (updateFields.H:44-62)
     double rho_min = 1e-15, rho_max = 1e10, p_min = 1e-15, p_max = 1e10, T_min = 1e-15, T_max = 1e10;
     // thermophysicalProperties (perfectGas, hConstThermo, const/Sutherland transport)
@@ -218,20 +230,32 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
         else if (k == "interpolationSchemes.reconstruct(U)") o.lim_U = parse_limiter(k, v, true);
         else if (k == "interpolationSchemes.reconstruct(T)") o.lim_T = parse_limiter(k, v, false);
         else if (k == "solvers.W.solver") {
+            // the asymmetric block-matrix solvers of Vector5typedefs.C:1655-1708
             if (t == "GMRES") o.solver = SOLVER_GMRES;
             else if (t == "BiCGStab") o.solver = SOLVER_BICGSTAB;
-            else if (t == "AMG" || t == "CG" || t == "GaussSeidel" || t == "ILU" || t == "Cholesky" || t == "SAMG")
-                throw ConfigError("block solver " + t + " is not on this path (GMRES, BiCGStab)", true);
-            else throw ConfigError("Unknown block solver " + t + "\nValid solvers are: (BiCGStab GMRES)");
+            else if (t == "GaussSeidel") o.solver = SOLVER_GAUSS_SEIDEL;
+            else if (t == "ILU") o.solver = SOLVER_ILU;
+            else if (t == "AMG")
+                throw ConfigError("block solver AMG is not on this path (BiCGStab GMRES GaussSeidel ILU)", true);
+            else if (t == "CG")
+                throw ConfigError("Unknown asymmetric matrix solver CG\n"
+                                  "Valid asymmetric matrix solvers are: (AMG BiCGStab GMRES GaussSeidel ILU)");
+            else throw ConfigError("Unknown block solver " + t + "\nValid solvers are: (AMG BiCGStab GMRES GaussSeidel ILU)");
         }
-        else if (k == "solvers.W.preconditioner") {
-            if (t == "ILUC0" || t == "ILU0" || t == "Cholesky") o.precon = PRECON_ILU0;
+        else if (k == "solvers.W.preconditioner" || k == "solvers.W.preconditioner.preconditioner") {
+            if (t == "ILUC0" || t == "ILU0") o.precon = PRECON_ILU0;
+            else if (t == "Cholesky") o.precon = PRECON_CHOLESKY;
+            else if (t == "GaussSeidel") o.precon = PRECON_GAUSS_SEIDEL;
+            else if (t == "ILUCp") o.precon = PRECON_ILUCP;
             else if (t == "diagonal" || t == "Jacobi") o.precon = PRECON_DIAGONAL;
             else if (t == "none") o.precon = PRECON_NONE;
-            else if (t == "AMG" || t == "ILUCp" || t == "GaussSeidel" || t == "SAMG")
-                throw ConfigError("preconditioner " + t + " is not on this path (ILUC0, diagonal, none)", true);
+            else if (t == "AMG" || t == "SAMG")
+                throw ConfigError("preconditioner " + t +
+                                  " is not on this path (Cholesky GaussSeidel ILUC0 ILUCp diagonal none)", true);
             else throw ConfigError("Unknown block preconditioner " + t);
         }
+        else if (k == "solvers.W.nSweeps" || k == "solvers.W.preconditioner.nSweeps") o.n_sweeps = parse_int(k, v);
+        else if (k == "solvers.W.fillInLevel" || k == "solvers.W.preconditioner.fillInLevel") o.fill_in = parse_int(k, v);
         else if (k == "solvers.W.nDirections") o.n_directions = parse_int(k, v);
         else if (k == "solvers.W.tolerance") o.tolerance = parse_double(k, v);
         else if (k == "solvers.W.relTol") o.rel_tol = parse_double(k, v);
@@ -284,6 +308,12 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
     if (o.basis32 < 0) o.basis32 = o.precision == PREC_FP64 ? 0 : 1;
     if (o.n_directions < 1 || o.n_directions > 64) throw ConfigError("solvers.W.nDirections must be in [1,64]");
     if (o.max_iter < 0 || o.min_iter < 0) throw ConfigError("solvers.W.maxIter/minIter must be >= 0");
+    if (o.n_sweeps < 1 || o.n_sweeps > 64) throw ConfigError("solvers.W.nSweeps must be in [1,64]");
+    if (o.fill_in < 0 || o.fill_in > 3) throw ConfigError("solvers.W.fillInLevel must be in [0,3]");
+    // the stationary solvers iterate their own factorisation: Gauss-Seidel
+    // sweeps, or (BlockILUSolver) the Cholesky-type incomplete factorisation
+    if (o.solver == SOLVER_GAUSS_SEIDEL) o.precon = PRECON_GAUSS_SEIDEL;
+    if (o.solver == SOLVER_ILU) o.precon = PRECON_CHOLESKY;
     if (!(o.R > 0) || !(o.Cp > o.R)) throw ConfigError("thermo: need 0 < R < Cp");
     if (o.lim_U == LIM_VENKATAKRISHNAN) {}
     // dual-time stepping: the Dual iteration with the dual2ndDST ddt (the

@@ -454,7 +454,7 @@ def read_case(directory, time: str = "0"):
     dep = opts.get("dependentVariable", "W")
     W = sol["solvers"].get(dep, sol["solvers"].get("W"))
     opts["solvers"] = {"W": {k: W[k] for k in ("solver", "preconditioner", "nDirections", "tolerance", "relTol",
-                                                "maxIter", "minIter") if k in W}}
+                                                "maxIter", "minIter", "nSweeps", "fillInLevel") if k in W}}
     if "relaxationFactors" in sol and "nuTilda" in sol["relaxationFactors"]:
         opts["relaxationFactors"] = {"nuTilda": sol["relaxationFactors"]["nuTilda"]}
     if "fieldBounds" in sol:

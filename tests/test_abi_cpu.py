@@ -52,6 +52,11 @@ def test_partition_host_only():
     ("solvers.W.nDirections", "0", 1),
     ("RASModel", "kEpsilon", 1),
     ("timeIntegration.maxInnerIter", "-1", 1),
+    ("solvers.W.solver", "CG", 1),                 # symmetric matrices only in foam-extend
+    ("solvers.W.preconditioner", "AMG", 6),
+    ("solvers.W.preconditioner", "ILUCq", 1),
+    ("solvers.W.nSweeps", "0", 1),
+    ("solvers.W.fillInLevel", "4", 1),
 ])
 def test_config_errors(key, value, status):
     case = cases.forward_step_c1().with_options(**{key: value})
@@ -90,7 +95,13 @@ def test_valid_options_reach_the_device_check():
         pytest.skip("a GPU is present")
     for case in (cases.forward_step_c1().with_options(**{"timeIntegration.timeIntegration": "Dual",
                                                          "ddtSchemes.default": "dual2ndDST"}),
-                 cases.rae2822(), cases.naca0012_turbulent(ni=97, nj=25, model="SARC1", first_cell=5e-3)):
+                 cases.rae2822(), cases.naca0012_turbulent(ni=97, nj=25, model="SARC1", first_cell=5e-3),
+                 *[cases.forward_step_c1().with_options(**o) for o in (
+                     {"solvers.W.solver": "GaussSeidel", "solvers.W.nSweeps": 2},
+                     {"solvers.W.solver": "ILU"},
+                     {"solvers.W.preconditioner": "Cholesky"},
+                     {"solvers.W.preconditioner": {"preconditioner": "GaussSeidel", "nSweeps": 3}},
+                     {"solvers.W.preconditioner": "ILUCp", "solvers.W.fillInLevel": 1})]):
         with pytest.raises(_abi.RdstError) as e:
             rhodst_b200.Solver(case.mesh, case.bcs, case.options)
         assert e.value.status == 3, case.name
