@@ -312,8 +312,7 @@ def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
     """Time to a density-residual drop of `drop` in FP64 and in mixed
     precision (FP32 Jacobian/ILU/basis; and BF16 Jacobian/ILU with the FP32
     basis) on the workload's mesh with
-    first-order HLL reconstruction at CFL 500 (the limited second-order
-    cases stall near 1e-6: limiter switching), then the discrete adjoint of
+    first-order HLL reconstruction at CFL 500, then the discrete adjoint of
     the pressure-drag coefficient at the FP64 converged state, its cost
     against that forward solve and dJ/dMach, dJ/dalpha."""
     import math

@@ -24,7 +24,19 @@ def _gpu_available() -> bool:
         return False
 
 
+# Modules that run after the step, adjoint and shape parity suites (the
+# selectable-solver rows and the frozen-turbulence gradient), so that those
+# suites report first; the allocation-free module stays last.
+_LATE = ("test_gpu_block_solvers.py", "test_gpu_adjoint_frozen_sa.py")
+
+
+def _order(item):
+    name = Path(str(item.fspath)).name
+    return 2 if name.startswith("test_zz") else (1 if name in _LATE else 0)
+
+
 def pytest_collection_modifyitems(config, items):
+    items.sort(key=_order)
     if _gpu_available():
         return
     skip = pytest.mark.skip(reason="no GPU in this environment")
