@@ -269,6 +269,15 @@ void rdst_destroy(rdst_ctx* ctx);
 rdst_status rdst_partition_cells(int32_t n_cells, const double* C,
                                  int32_t n_parts, int32_t* out_part);
 
+/* Host-only helper (no GPU needed): recursive bisection of the cell graph
+ * (internal faces owner/neighbour) by breadth-first distance from a
+ * pseudo-peripheral cell, n_parts parts; the partition the library uses
+ * with the option "ilu.partition" "graph" (foam-extend's decomposePar
+ * methods, scotch or hierarchical, cut processors the same two ways). */
+rdst_status rdst_partition_graph(int32_t n_cells, int32_t n_internal_faces,
+                                 const int32_t* owner, const int32_t* neighbour,
+                                 int32_t n_parts, int32_t* out_part);
+
 /* Instrumentation (no reference counterpart).
  * rdst_stream: the CUDA stream (cudaStream_t) all of the context's kernels
  * run on, so a caller can record its own events around rdst_step.

@@ -34,6 +34,9 @@ def load_library() -> ctypes.CDLL:
         lib.rdst_partition_cells.restype = ctypes.c_int32
         lib.rdst_partition_cells.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
                                              ctypes.POINTER(ctypes.c_int32)]
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        lib.rdst_partition_graph.restype = ctypes.c_int32
+        lib.rdst_partition_graph.argtypes = [ctypes.c_int32, ctypes.c_int32, i32p, i32p, ctypes.c_int32, i32p]
         _lib = lib
     return _lib
 
@@ -70,5 +73,22 @@ def partition_cells(C, n_parts: int):
     return out
 
 
-__all__ = ["Solver", "solver_for", "RdstError", "RdstStepReport", "load_library", "partition_cells",
+def partition_graph(mesh, n_parts: int):
+    """Recursive graph bisection of the cell graph (the partition of the
+    option "ilu.partition" "graph")."""
+    import numpy as np
+    lib = load_library()
+    Fi = int(mesh.n_internal_faces)
+    own = np.ascontiguousarray(np.asarray(mesh.owner)[:Fi], dtype=np.int32)
+    nei = np.ascontiguousarray(np.asarray(mesh.neighbour)[:Fi], dtype=np.int32)
+    out = np.empty(int(mesh.n_cells), dtype=np.int32)
+    p = ctypes.POINTER(ctypes.c_int32)
+    st = lib.rdst_partition_graph(int(mesh.n_cells), Fi, own.ctypes.data_as(p), nei.ctypes.data_as(p), n_parts,
+                                  out.ctypes.data_as(p))
+    if st != 0:
+        raise RdstError(st, "partition_graph")
+    return out
+
+
+__all__ = ["Solver", "solver_for", "RdstError", "RdstStepReport", "load_library", "partition_cells", "partition_graph",
            "mesh", "cases", "flatten_options"]

@@ -94,6 +94,73 @@ void rcb(const double* C, std::vector<int>& idx, int lo, int hi, int part0, int 
     rcb(C, idx, mid, hi, part0 + n1, nparts - n1, out);
 }
 
+// Recursive graph bisection of the cell graph (internal faces): each set is
+// ordered by breadth-first distance from a pseudo-peripheral cell (the cell
+// farthest from the set's first cell; ties by position), then by cell
+// index, and cut at the proportional rank; cells the search does not reach
+// (another component) go last.  Subdomains cut this way are graph slabs,
+// whose wavefront level chains are shorter than those of coordinate boxes
+// on stretched body-fitted meshes.
+struct CellGraph {
+    std::vector<int> start, adj;            // CSR, neighbours ascending
+    CellGraph(int N, int Fi, const int32_t* own, const int32_t* nei) : start(N + 1, 0) {
+        for (int f = 0; f < Fi; ++f) { ++start[own[f] + 1]; ++start[nei[f] + 1]; }
+        for (int i = 0; i < N; ++i) start[i + 1] += start[i];
+        adj.resize(start[N]);
+        std::vector<int> pos(start.begin(), start.end() - 1);
+        for (int f = 0; f < Fi; ++f) { adj[pos[own[f]]++] = nei[f]; adj[pos[nei[f]]++] = own[f]; }
+        for (int i = 0; i < N; ++i) std::sort(adj.begin() + start[i], adj.begin() + start[i + 1]);
+    }
+};
+
+void graph_bisect(const CellGraph& g, std::vector<int>& idx, int lo, int hi, int part0, int nparts, int32_t* out,
+                  std::vector<int>& dist, std::vector<int>& stamp, int& tick) {
+    if (nparts <= 1 || hi - lo <= 1) {
+        for (int i = lo; i < hi; ++i) out[idx[i]] = part0;
+        return;
+    }
+    // distances inside the set idx[lo, hi): -1 = not reached
+    auto bfs = [&](int src) {
+        ++tick;
+        for (int i = lo; i < hi; ++i) { stamp[idx[i]] = tick; dist[idx[i]] = -1; }
+        std::vector<int> q;
+        q.reserve(hi - lo);
+        q.push_back(src);
+        dist[src] = 0;
+        for (size_t h = 0; h < q.size(); ++h) {
+            const int v = q[h];
+            for (int k = g.start[v]; k < g.start[v + 1]; ++k) {
+                const int w = g.adj[k];
+                if (stamp[w] == tick && dist[w] < 0) { dist[w] = dist[v] + 1; q.push_back(w); }
+            }
+        }
+        int far = idx[lo];
+        for (int i = lo; i < hi; ++i)
+            if (dist[idx[i]] > dist[far]) far = idx[i];
+        return far;
+    };
+    bfs(bfs(idx[lo]));
+    int dmax = 0;
+    for (int i = lo; i < hi; ++i) dmax = std::max(dmax, dist[idx[i]]);
+    for (int i = lo; i < hi; ++i)
+        if (dist[idx[i]] < 0) dist[idx[i]] = dmax + 1;
+    std::sort(idx.begin() + lo, idx.begin() + hi, [&](int a, int b) {
+        return dist[a] < dist[b] || (dist[a] == dist[b] && a < b);
+    });
+    const int n1 = nparts / 2;
+    const int mid = lo + (int)((long)(hi - lo) * n1 / nparts);
+    graph_bisect(g, idx, lo, mid, part0, n1, out, dist, stamp, tick);
+    graph_bisect(g, idx, mid, hi, part0 + n1, nparts - n1, out, dist, stamp, tick);
+}
+
+void graph_partition(int N, int Fi, const int32_t* own, const int32_t* nei, int nparts, int32_t* out) {
+    CellGraph g(N, Fi, own, nei);
+    std::vector<int> idx(N), dist(N, -1), stamp(N, 0);
+    std::iota(idx.begin(), idx.end(), 0);
+    int tick = 0;
+    graph_bisect(g, idx, 0, N, 0, nparts, out, dist, stamp, tick);
+}
+
 struct Report5 { rdst_step_report r; };
 
 // report of the current step into reps[sc->step_idx]; advances the slot
@@ -483,9 +550,13 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     if (factored) {
         nparts = o.ilu_parts > 0 ? o.ilu_parts : auto_ilu_parts(N, o.precision);
         nparts = std::min(nparts, N);
-        std::vector<int> idx(N);
-        std::iota(idx.begin(), idx.end(), 0);
-        rcb(mh->C, idx, 0, N, 0, nparts, part.data());
+        if (o.ilu_graph) {
+            graph_partition(N, Fi, mh->owner, mh->neighbour, nparts, part.data());
+        } else {
+            std::vector<int> idx(N);
+            std::iota(idx.begin(), idx.end(), 0);
+            rcb(mh->C, idx, 0, N, 0, nparts, part.data());
+        }
         lupat.resize(N);
         for (int i = 0; i < N; ++i)
             for (int f : cfaces[i]) {
@@ -2230,5 +2301,18 @@ RDST_API rdst_status rdst_partition_cells(int32_t n_cells, const double* C, int3
     std::vector<int> idx(n_cells);
     std::iota(idx.begin(), idx.end(), 0);
     rcb(C, idx, 0, n_cells, 0, std::min(n_parts, n_cells), out);
+    return RDST_OK;
+}
+
+RDST_API rdst_status rdst_partition_graph(int32_t n_cells, int32_t n_internal_faces, const int32_t* owner,
+                                          const int32_t* neighbour, int32_t n_parts, int32_t* out) {
+    if (n_cells <= 0 || n_internal_faces < 0 || !out || n_parts <= 0 ||
+        (n_internal_faces > 0 && (!owner || !neighbour)))
+        return RDST_ERR_ARG;
+    for (int f = 0; f < n_internal_faces; ++f)
+        if (owner[f] < 0 || owner[f] >= n_cells || neighbour[f] < 0 || neighbour[f] >= n_cells ||
+            owner[f] == neighbour[f])
+            return RDST_ERR_MESH;
+    graph_partition(n_cells, n_internal_faces, owner, neighbour, std::min(n_parts, n_cells), out);
     return RDST_OK;
 }

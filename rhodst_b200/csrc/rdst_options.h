@@ -95,6 +95,7 @@ struct Options {
     Precision precision = PREC_FP64;
     int basis32 = -1;                 // GMRES basis vectors in FP32 (-1: when precision is not fp64)
     int ilu_parts = 0;                // 0: choose from the mesh size; 1: exact global ILU(0)
+    bool ilu_graph = false;           // subdomains by graph bisection (true) or coordinate bisection
     bool graphs = true;               // capture steps in CUDA graphs
     bool profile = false;             // event-time kernel classes inside steps
 
@@ -300,6 +301,11 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             else throw ConfigError("krylov.basis must be fp64 or fp32");
         }
         else if (k == "ilu.parts") o.ilu_parts = parse_int(k, v);
+        else if (k == "ilu.partition") {
+            if (t == "rcb") o.ilu_graph = false;
+            else if (t == "graph") o.ilu_graph = true;
+            else throw ConfigError("ilu.partition must be rcb or graph");
+        }
         else if (k == "graphs") o.graphs = parse_bool(k, v);
         else if (k == "profile") o.profile = parse_bool(k, v);
         else throw ConfigError("unknown option '" + k + "'");

@@ -57,6 +57,7 @@ def test_partition_host_only():
     ("solvers.W.preconditioner", "ILUCq", 1),
     ("solvers.W.nSweeps", "0", 1),
     ("solvers.W.fillInLevel", "4", 1),
+    ("ilu.partition", "scotch", 1),
 ])
 def test_config_errors(key, value, status):
     case = cases.forward_step_c1().with_options(**{key: value})
@@ -111,3 +112,72 @@ def test_set_geometry_checks_its_arguments(gpulib):
     gpulib.rdst_set_geometry.restype = ctypes.c_int32
     gpulib.rdst_set_geometry.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     assert gpulib.rdst_set_geometry(None, None) == 7
+
+
+def _graph_bisection_reference(m, n_parts):
+    """Restatement with scipy: order each set by breadth-first distance from
+    the cell farthest from its first cell (then by index), cut at the
+    proportional rank, unreached cells last."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import breadth_first_order
+    N, Fi = m.n_cells, m.n_internal_faces
+    own = np.asarray(m.owner)[:Fi].astype(np.int64)
+    nei = np.asarray(m.neighbour)[:Fi].astype(np.int64)
+    A = sp.coo_matrix((np.ones(Fi), (own, nei)), shape=(N, N)).tocsr()
+    A = (A + A.T).tocsr()
+
+    def dist(G, src):
+        order, pred = breadth_first_order(G, src, directed=False, return_predecessors=True)
+        d = np.full(G.shape[0], -1, dtype=np.int64)
+        d[src] = 0
+        for v in order[1:]:
+            d[v] = d[pred[v]] + 1
+        return d
+
+    out = np.zeros(N, dtype=np.int64)
+
+    def rec(cells, n, p0):
+        if n <= 1 or cells.size <= 1:
+            out[cells] = p0
+            return
+        G = A[cells][:, cells]
+        d = dist(G, int(np.argmax(dist(G, 0))))
+        d[d < 0] = d.max() + 1
+        order = np.lexsort((cells, d))
+        k = cells.size * (n // 2) // n
+        rec(cells[order[:k]], n // 2, p0)
+        rec(cells[order[k:]], n - n // 2, p0 + n // 2)
+
+    rec(np.arange(N), n_parts, 0)
+    return out
+
+
+def _level_chains(m, part):
+    """Longest wavefront chain (levels) of each part in cell order."""
+    Fi = m.n_internal_faces
+    own = np.asarray(m.owner)[:Fi]
+    nei = np.asarray(m.neighbour)[:Fi]
+    level = np.zeros(m.n_cells, dtype=np.int64)
+    same = part[own] == part[nei]
+    lower = [[] for _ in range(m.n_cells)]
+    for a, b in zip(own[same], nei[same]):
+        lower[b].append(a)
+    for i in range(m.n_cells):
+        if lower[i]:
+            level[i] = 1 + max(level[k] for k in lower[i])
+    mx = np.zeros(part.max() + 1, dtype=np.int64)
+    np.maximum.at(mx, part, level)
+    return mx + 1
+
+
+def test_graph_partition_host_only():
+    m = cases.naca0012_inviscid(ni=129, nj=33, first_cell=2e-3).mesh
+    part = rhodst_b200.partition_graph(m, 16)
+    sizes = np.bincount(part, minlength=16)
+    assert sizes.sum() == m.n_cells and sizes.max() - sizes.min() <= 1
+    assert np.array_equal(part, rhodst_b200.partition_graph(m, 16))
+    assert np.array_equal(part, _graph_bisection_reference(m, 16))
+    # graph slabs have shorter level chains than coordinate boxes here
+    lg = _level_chains(m, part)
+    lr = _level_chains(m, rhodst_b200.partition_cells(m.C, 16))
+    assert lg.max() <= lr.max() and lg.mean() < lr.mean(), (lg.max(), lr.max(), lg.mean(), lr.mean())

@@ -1,6 +1,7 @@
 """B200 library vs. CPU oracle for the other selectable block preconditioners
 and solvers: Cholesky (diagonal-based incomplete factorisation), Gauss-Seidel
-sweeps, ILUCp with fill-in, and the stationary GaussSeidel / ILU solvers.
+sweeps, ILUCp with fill-in, and the stationary GaussSeidel / ILU solvers;
+and the subdomain ILU(0) on graph-bisection subdomains.
 
 Both sides run the same subdomain partition (the GPU's RCB parts, passed to
 the oracle), FP64 throughout.  Step trajectories agree to 1e-9 relative (the
@@ -25,9 +26,9 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-def run_pair(case, steps, parts, tol=1e-9):
-    case = case.with_options(**{"ilu.parts": parts})
-    part = rhodst_b200.partition_cells(case.mesh.C, parts)
+def run_pair(case, steps, parts, tol=1e-9, graph=False):
+    case = case.with_options(**{"ilu.parts": parts, "ilu.partition": "graph" if graph else "rcb"})
+    part = rhodst_b200.partition_graph(case.mesh, parts) if graph else rhodst_b200.partition_cells(case.mesh.C, parts)
     gpu = rhodst_b200.Solver(case.mesh, case.bcs, case.options)
     ora = OracleSolver(case.mesh, case.bcs, case.options, partition=part)
     for s in (gpu, ora):
@@ -92,3 +93,11 @@ def test_too_wide_fill_is_refused():
     with pytest.raises(_abi.RdstError) as e:
         rhodst_b200.Solver(c.mesh, c.bcs, c.options)
     assert e.value.status == 6
+
+
+@pytest.mark.parametrize("case_fn", [
+    lambda: step_case("GMRES", "ILUC0"),
+    lambda: cases.naca0012_inviscid(ni=129, nj=33, first_cell=2e-3, n_directions=10),
+], ids=["C1", "airfoil"])
+def test_graph_bisection_subdomains(case_fn):
+    run_pair(case_fn(), 5, parts=16, graph=True)
