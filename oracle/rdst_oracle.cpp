@@ -356,6 +356,51 @@ void grad_vector(const Ctx& c, const std::vector<v3>& x, const std::vector<v3>& 
     }
 }
 
+// cellLimited Gauss linear k for grad(U) (foam-extend cellLimitedGrad for a
+// vector field, as the RAE2822 tutorial selects it): per velocity component
+// j the spread maxD/minD of U_j over the face neighbours and boundary values
+// (widened by (1/k - 1)(maxD - minD) for k < 1); the limiter is the minimum
+// over the cell's faces of maxD/d (d > maxD + VSMALL) or minD/d
+// (d < minD - VSMALL), d = (Cf - C) . grad U_j; grad U_j is scaled by it.
+void limit_grad_U(const Ctx& c, std::vector<std::array<double, 9>>& g) {
+    const double k = c.o.grad_U_limit;
+    if (!(k > 0)) return;
+    OMP_FOR
+    for (int i = 0; i < c.N; ++i) {
+        v3 mx = c.U[i], mn = c.U[i];
+        for (int f : c.cellFaces[i]) {
+            if (f < c.Fi) {
+                const v3& o = c.U[c.own[f] == i ? c.nei[f] : c.own[f]];
+                for (int j = 0; j < 3; ++j) { mx[j] = std::max(mx[j], o[j]); mn[j] = std::min(mn[j], o[j]); }
+            } else if (c.active[f - c.Fi]) {
+                const v3& o = c.U_b[f - c.Fi];
+                for (int j = 0; j < 3; ++j) { mx[j] = std::max(mx[j], o[j]); mn[j] = std::min(mn[j], o[j]); }
+            }
+        }
+        for (int j = 0; j < 3; ++j) {
+            mx[j] -= c.U[i][j];
+            mn[j] -= c.U[i][j];
+            if (k < 1.0) {
+                const double w = (1.0 / k - 1.0) * (mx[j] - mn[j]);
+                mx[j] += w;
+                mn[j] -= w;
+            }
+        }
+        v3 lim{1.0, 1.0, 1.0};
+        for (int f : c.cellFaces[i]) {
+            if (f >= c.Fi && !c.active[f - c.Fi]) continue;
+            const v3 d = c.Cf[f] - c.C[i];
+            for (int j = 0; j < 3; ++j) {
+                const double e = d[0] * g[i][j] + d[1] * g[i][3 + j] + d[2] * g[i][6 + j];
+                if (e > mx[j] + VSMALL) lim[j] = std::min(lim[j], mx[j] / e);
+                else if (e < mn[j] - VSMALL) lim[j] = std::min(lim[j], mn[j] / e);
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < 3; ++j) g[i][3 * a + j] *= lim[j];
+    }
+}
+
 // ----------------------------------------------------------------------
 // Limited reconstruction (foam-extend limitedSurfaceInterpolationScheme with
 // a TVD limiter, as selected by "reconstruct(X)" and called with the +-1
@@ -841,6 +886,7 @@ void viscous_terms(Ctx& c) {
     typedef std::array<double, 9> t3;
     std::vector<t3> gU;
     grad_vector(c, c.U, c.U_b, gU);
+    limit_grad_U(c, gU);
     std::vector<double> muE(c.N), muE_b(c.NB, 0.0);
     OMP_FOR
     for (int i = 0; i < c.N; ++i) muE[i] = mu_of_T(c, c.T[i]) + c.mut[i];
@@ -1713,6 +1759,7 @@ void sa_correct(Ctx& c) {
     typedef std::array<double, 9> t3;
     std::vector<t3> gU;
     grad_vector(c, c.U, c.U_b, gU);
+    limit_grad_U(c, gU);
     std::vector<v3> gn;
     grad_scalar(c, c.nut, c.nut_b, gn);
     // SARC1 (SARC1.C:125-180, 655-669): S = symm(grad U) per cell; the
@@ -1850,6 +1897,13 @@ void sa_correct(Ctx& c) {
         v3 n = c.Sf[f] / c.magSf[f];
         v3 kc = n - c.dc[f] * (c.C[Q] - c.C[P]);
         double corr = Df * c.magSf[f] * dot(kc, c.w[f] * gn[P] + (1 - c.w[f]) * gn[Q]);
+        // linearUpwind grad(nuTilda): the explicit part of the face value
+        // nuTilda_C + (Cf - C) . grad nuTilda_C of the upwind cell C
+        // (fvm::div's faceFluxCorrection phi * correction, moved to the source)
+        if (c.o.nut_linear_upwind) {
+            const int C = ph >= 0 ? P : Q;
+            corr -= ph * dot(c.Cf[f] - c.C[C], gn[C]);
+        }
         b[P] += corr;
         b[Q] -= corr;
     }
@@ -2319,6 +2373,19 @@ ORACLE_API rdst_status rdsto_precondition(rdst_ctx* ctx, const double* b, double
     for (int i = 0; i < c.N; ++i) for (int k = 0; k < 5; ++k) bb[i][k] = b[5 * i + k];
     precondition(c, M, xx, bb);
     for (int i = 0; i < c.N; ++i) for (int k = 0; k < 5; ++k) x[5 * i + k] = xx[i][k];
+    return RDST_OK;
+}
+
+// grad(U) at the current state as the viscous terms use it (test hook:
+// Gauss linear, cellLimited when selected), row-major d U_j / d x_i, N x 9.
+ORACLE_API rdst_status rdsto_grad_U(rdst_ctx* ctx, double* out) {
+    if (!ctx || !out) return RDST_ERR_ARG;
+    Ctx& c = ctx->c;
+    compute_flux(c);
+    std::vector<std::array<double, 9>> g;
+    grad_vector(c, c.U, c.U_b, g);
+    limit_grad_U(c, g);
+    for (int i = 0; i < c.N; ++i) for (int k = 0; k < 9; ++k) out[9 * i + k] = g[i][k];
     return RDST_OK;
 }
 

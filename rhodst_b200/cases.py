@@ -298,7 +298,8 @@ def forward_step_3d_hybrid_c5(nx: int = 240, ny: int = 80, nz: int = 56, precisi
                 force_patch="obstacle", force_dirs={"lift": (0.0, 1.0, 0.0), "drag": (1.0, 0.0, 0.0)})
 
 
-def rae2822(model: str = "SpalartAllmaras", flux: str = "Kurganov", limiter: str = "OSPRE") -> Case:
+def rae2822(model: str = "SpalartAllmaras", flux: str = "Kurganov", limiter: str = "OSPRE",
+            tutorial_schemes: bool = False) -> Case:
     """The reference's RAE2822 tutorial (tutorials/RAE2822): its own mesh
     (constant/polyMesh, 23,552 cells, read by rhodst_b200.foam and stored in
     tests/golden/rae2822_mesh.npz), its free stream (0/include/
@@ -308,9 +309,10 @@ def rae2822(model: str = "SpalartAllmaras", flux: str = "Kurganov", limiter: str
     Kurganov with OSPRE/OSPREV, steadyStateDST with the face-based local time
     step at CFL 1 -> 500, BiCGStab + ILUC0 (maxIter 100, tolerance and relTol
     1e-10), nuTilda relaxation 0.5 and the tutorial's field bounds
-    (system/*).  This path's discretisation differs from the tutorial's
-    schemes in two places: grad(U) is Gauss linear (the tutorial asks for
-    cellLimited) and nuTilda is convected upwind (linearUpwind there)."""
+    (system/*).  With `tutorial_schemes` the tutorial's gradient and
+    convection schemes too (system/fvSchemes: grad(U) cellLimited Gauss
+    linear 1, div(phi,nuTilda) Gauss linearUpwind grad(nuTilda)); without,
+    Gauss linear and upwind."""
     from pathlib import Path
     from . import foam
     fixture = Path(__file__).resolve().parents[1] / "tests" / "golden" / "rae2822_mesh.npz"
@@ -339,6 +341,10 @@ def rae2822(model: str = "SpalartAllmaras", flux: str = "Kurganov", limiter: str
         "transport": dict(AIR_SUTHERLAND, Pr=AIR_PR),
         "RASModel": model,
     }
+    if tutorial_schemes:
+        options["gradSchemes"] = {"grad(U)": "cellLimited Gauss linear 1"}
+        if model != "laminar":
+            options["divSchemes"] = {"div(phi,nuTilda)": "Gauss linearUpwind grad(nuTilda)"}
     N = m.n_cells
     al = math.atan2(U_inf[1], U_inf[0])
     return Case("rae2822", m, bcs, options, np.full(N, p_inf), np.tile(np.array(U_inf), (N, 1)),

@@ -433,6 +433,60 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, int venkat_mask, double
     }
 }
 
+// cellLimited Gauss linear k for grad(U) (foam-extend cellLimitedGrad of a
+// vector field): per velocity component j, the spread maxD/minD of U_j over
+// the cell's face neighbours and boundary values (widened by
+// (1/k - 1)(maxD - minD) for k < 1), the limiter min over the cell's faces
+// of maxD/d (d > maxD + VSMALL) or minD/d (d < minD - VSMALL) with
+// d = (Cf - C) . grad U_j, and grad U_j scaled by it, in place (each thread
+// reads its neighbours' velocities, not their gradients).
+__global__ void __launch_bounds__(128) k_limit_gradU(DevMesh m, double k_lim, const double* __restrict__ prim,
+                                                     const double* __restrict__ bs, double* __restrict__ gU) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.N) return;
+    const int k0 = m.cf_start[i], k1 = m.cf_start[i + 1];
+    double Ui[3], mx[3], mn[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { Ui[j] = prim[PW * i + 3 + j]; mx[j] = Ui[j]; mn[j] = Ui[j]; }
+    for (int k = k0; k < k1; ++k) {
+        const int code = m.cf_list[k];
+        const double* xo;
+        if (code < m.Fi) { const int o = m.own[code]; xo = prim + PW * (o == i ? m.nei[code] : o) + 3; }
+        else xo = bs + BW * (code - m.Fi) + 12;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) { mx[j] = fmax(mx[j], xo[j]); mn[j] = fmin(mn[j], xo[j]); }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        mx[j] -= Ui[j];
+        mn[j] -= Ui[j];
+        if (k_lim < 1.0) {
+            const double w = (1.0 / k_lim - 1.0) * (mx[j] - mn[j]);
+            mx[j] += w;
+            mn[j] -= w;
+        }
+    }
+    double g[9], lim[3] = {1.0, 1.0, 1.0};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) g[k] = gU[9 * i + k];
+    const V3 Ci = ldv3(m.C, m.N, i);
+    for (int k = k0; k < k1; ++k) {
+        const int code = m.cf_list[k];
+        const V3 Cf = code < m.Fi ? ldv3(m.Cf, m.Fi, code) : ldv3(m.bCf, m.NB, code - m.Fi);
+        const V3 d = sub3(Cf, Ci);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double e = d.x * g[j] + d.y * g[3 + j] + d.z * g[6 + j];
+            if (e > mx[j] + D_VSMALL) lim[j] = fmin(lim[j], mx[j] / e);
+            else if (e < mn[j] - D_VSMALL) lim[j] = fmin(lim[j], mn[j] / e);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) gU[9 * i + 3 * a + j] = g[3 * a + j] * lim[j];
+}
+
 // scalar limited reconstruction to the owner (xo) and neighbour (xn) sides
 __device__ __forceinline__ void recon_scalar(int L, double xP, double xN, V3 gP, V3 gN, V3 d, double w,
                                              double& xo, double& xn) {

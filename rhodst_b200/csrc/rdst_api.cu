@@ -860,6 +860,10 @@ struct Ops {
         k_grad<<<nblk(m.N, 128), 128, 0, s>>>(m, c.venkat_mask, o.venkat_K, c.q.p, c.qb.p, c.prim.p, c.g.p, c.psi.p,
                                              c.fcell.p, o.flux == FLUX_HLLCP, c.bs.p, visc ? c.gU.p : nullptr);
         CKL();
+        if (visc && o.grad_U_limit > 0) {
+            k_limit_gradU<<<nblk(m.N, 128), 128, 0, s>>>(m, o.grad_U_limit, c.prim.p, c.bs.p, c.gU.p);
+            CKL();
+        }
         if (m.Fi > 0) {
             Timed tm(c, KS_FLUX);
             k_face_flux<<<nblk(m.Fi, 128), 128, 0, s>>>(m, c.th, flux_code(o.flux), lim_code(o.lim_rho), lim_code(o.lim_U),
@@ -1129,11 +1133,14 @@ void sa_correct(rdst_ctx& c) {
     const int neg_sa = c.o.turbulence == TURB_SANEG;
     SAFields F = c.sa;
     k_sa_grad<<<nblk(c.N, 128), 128, 0, s>>>(m, c.prim.p, c.bs.p, F, c.gU.p); CKL();
+    if (c.o.grad_U_limit > 0) {
+        k_limit_gradU<<<nblk(c.N, 128), 128, 0, s>>>(m, c.o.grad_U_limit, c.prim.p, c.bs.p, c.gU.p); CKL();
+    }
     const int sarc1 = c.o.turbulence == TURB_SARC1 ? 1 : (c.o.turbulence == TURB_SA ? 2 : 0);
     k_sa_cell<<<nblk(c.N, 128), 128, 0, s>>>(m, c.tr, neg_sa, sarc1, c.steady ? 1 : 0, c.W.p, c.prim.p, c.gU.p, c.rdt.p,
                                             c.sc.p, c.fl.p, c.bs.p, F); CKL();
     if (sarc1 == 1) { k_sarc1_valid<<<1, 1, 0, s>>>(F.S_old_valid); CKL(); }
-    if (m.Fi > 0) { k_sa_faces<<<nblk(m.Fi, TPB), TPB, 0, s>>>(m, c.fl.p, F); CKL(); }
+    if (m.Fi > 0) { k_sa_faces<<<nblk(m.Fi, TPB), TPB, 0, s>>>(m, c.fl.p, F, c.o.nut_linear_upwind ? 1 : 0); CKL(); }
     if (m.NB > 0) { k_sa_bfaces<<<nblk(m.NB, TPB), TPB, 0, s>>>(m, c.tr, neg_sa, c.bs.p, F); CKL(); }
     k_sa_assemble<<<nblk(c.N, TPB), TPB, 0, s>>>(m, c.o.nut_relax, F); CKL();
     // Jacobi sweeps from the current nuTilda, ping-pong nut <-> x2
@@ -1787,6 +1794,8 @@ int adj_solve(rdst_ctx& c, const double* rhs, double* psi, double rel_tol, int m
 // branches are those of the last boundary evaluation) at the current W
 template <typename MT>
 void adj_forward(rdst_ctx& c) {
+    if (c.tr.viscous && c.o.grad_U_limit > 0)
+        throw ConfigError("the linearization of cellLimited grad(U) is not on this path", true);
     Ops<MT>::flux(c);
 }
 

@@ -70,6 +70,8 @@ struct Options {
     // fvSchemes
     Ddt ddt = DDT_EULER;
     Limiter lim_rho = LIM_OSPRE, lim_U = LIM_OSPRE, lim_T = LIM_OSPRE;
+    double grad_U_limit = 0.0;        // gradSchemes grad(U): 0 Gauss linear, k cellLimited Gauss linear k
+    bool nut_linear_upwind = false;   // divSchemes div(phi,nuTilda): Gauss upwind | Gauss linearUpwind grad(nuTilda)
     // fvSolution: solvers.W
     Solver solver = SOLVER_BICGSTAB;
     Precon precon = PRECON_ILU0;
@@ -106,6 +108,19 @@ struct Options {
 inline std::string trim(const std::string& s) {
     size_t a = s.find_first_not_of(" \t\n;"), b = s.find_last_not_of(" \t\n;");
     return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+// runs of blanks -> one space (dictionary entries such as "Gauss  linear")
+inline std::string collapse_ws(const std::string& s) {
+    std::string out;
+    bool sp = false;
+    for (char ch : trim(s)) {
+        if (ch == ' ' || ch == '\t' || ch == '\n') { sp = true; continue; }
+        if (sp && !out.empty()) out += ' ';
+        sp = false;
+        out += ch;
+    }
+    return out;
 }
 
 inline bool parse_bool(const std::string& k, const std::string& v) {
@@ -299,6 +314,32 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             if (t == "fp64") o.basis32 = 0;
             else if (t == "fp32") o.basis32 = 1;
             else throw ConfigError("krylov.basis must be fp64 or fp32");
+        }
+        else if (k == "gradSchemes.default") {
+            if (collapse_ws(t) != "Gauss linear")
+                throw ConfigError("gradSchemes default " + t + " is not on this path (Gauss linear)", true);
+        }
+        else if (k == "gradSchemes.grad(U)") {
+            // fvSchemes gradSchemes: Gauss linear, or cellLimited Gauss linear k
+            const std::string g = collapse_ws(t);
+            if (g == "Gauss linear") o.grad_U_limit = 0.0;
+            else if (g.rfind("cellLimited Gauss linear ", 0) == 0) {
+                o.grad_U_limit = parse_double(k, g.substr(25));
+                if (!(o.grad_U_limit > 0.0 && o.grad_U_limit <= 1.0))
+                    throw ConfigError("cellLimited coefficient must be in (0, 1]");
+            } else throw ConfigError("gradSchemes grad(U) " + t + " is not on this path "
+                                     "(Gauss linear, cellLimited Gauss linear k)", true);
+        }
+        else if (k == "divSchemes.div(phi,nuTilda)") {
+            const std::string d = collapse_ws(t);
+            if (d == "Gauss upwind") o.nut_linear_upwind = false;
+            else if (d == "Gauss linearUpwind grad(nuTilda)") o.nut_linear_upwind = true;
+            else throw ConfigError("divSchemes div(phi,nuTilda) " + t + " is not on this path "
+                                   "(Gauss upwind, Gauss linearUpwind grad(nuTilda))", true);
+        }
+        else if (k == "divSchemes.div(tauMC)") {
+            if (collapse_ws(t) != "Gauss linear")
+                throw ConfigError("divSchemes div(tauMC) " + t + " is not on this path (Gauss linear)", true);
         }
         else if (k == "ilu.parts") o.ilu_parts = parse_int(k, v);
         else if (k == "ilu.partition") {

@@ -243,7 +243,7 @@ __global__ void k_sarc1_rho0(int N, const double* __restrict__ W, double* __rest
 __global__ void k_sarc1_valid(int* __restrict__ flag) { *flag = 1; }
 
 // per internal face: upwind convection + corrected diffusion coefficients
-__global__ void k_sa_faces(DevMesh m, const double* __restrict__ fl, SAFields F) {
+__global__ void k_sa_faces(DevMesh m, const double* __restrict__ fl, SAFields F, int lin_upwind) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.Fi) return;
     const int P = m.own[f], Q = m.nei[f];
@@ -260,7 +260,15 @@ __global__ void k_sa_faces(DevMesh m, const double* __restrict__ fl, SAFields F)
     const V3 kc = sub3(n, scl3(dc, ldv3(m.d, m.Fi, f)));
     const V3 gf = add3(scl3(w, mk(F.gn[3 * P], F.gn[3 * P + 1], F.gn[3 * P + 2])),
                        scl3(1 - w, mk(F.gn[3 * Q], F.gn[3 * Q + 1], F.gn[3 * Q + 2])));
-    F.fcorr[f] = Df * magS * dot3(kc, gf);
+    double corr = Df * magS * dot3(kc, gf);
+    if (lin_upwind) {
+        // linearUpwind grad(nuTilda): explicit part phi (Cf - C) . grad nuTilda_C
+        // of the upwind cell C, moved to the source
+        const int C = ph >= 0 ? P : Q;
+        const V3 dC = sub3(ldv3(m.Cf, m.Fi, f), ldv3(m.C, m.N, C));
+        corr -= ph * dot3(dC, mk(F.gn[3 * C], F.gn[3 * C + 1], F.gn[3 * C + 2]));
+    }
+    F.fcorr[f] = corr;
 }
 
 // per boundary face: convection through f ref + (1-f) nu_P, diffusion with

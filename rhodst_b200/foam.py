@@ -445,12 +445,23 @@ def read_case(directory, time: str = "0"):
     opts["ddtSchemes"] = {"default": schemes["ddtSchemes"]["default"]}
     interp = schemes.get("interpolationSchemes", {})
     opts["interpolationSchemes"] = {k: v for k, v in interp.items() if k.startswith("reconstruct(")}
-    for k, v in schemes.get("gradSchemes", {}).items():
-        if v.strip() != "Gauss linear":
+    # the gradient and convection schemes this path selects by name: grad(U)
+    # (Gauss linear or cellLimited) and div(phi,nuTilda) (upwind or
+    # linearUpwind); the entries of equations this path does not solve
+    # (k, epsilon, e) are not read
+    grads = {k: " ".join(v.split()) for k, v in schemes.get("gradSchemes", {}).items()}
+    divs = {k: " ".join(v.split()) for k, v in schemes.get("divSchemes", {}).items()}
+    taken = {}
+    if grads.get("grad(U)", "Gauss linear") != "Gauss linear":
+        taken.setdefault("gradSchemes", {})["grad(U)"] = grads["grad(U)"]
+    for k, v in grads.items():
+        if k not in ("default", "grad(U)") and v != "Gauss linear":
             notes.append(f"gradSchemes {k} {v}: Gauss linear here")
-    for k, v in schemes.get("divSchemes", {}).items():
-        if k.startswith("div(phi,nuTilda)") and "upwind" != v.split()[-1]:
-            notes.append(f"divSchemes {k} {v}: upwind here")
+    if grads.get("default", "Gauss linear") != "Gauss linear":
+        notes.append(f"gradSchemes default {grads['default']}: Gauss linear here")
+    if model != "laminar" and "div(phi,nuTilda)" in divs and divs["div(phi,nuTilda)"] != "Gauss upwind":
+        taken.setdefault("divSchemes", {})["div(phi,nuTilda)"] = divs["div(phi,nuTilda)"]
+    opts.update(taken)
     dep = opts.get("dependentVariable", "W")
     W = sol["solvers"].get(dep, sol["solvers"].get("W"))
     opts["solvers"] = {"W": {k: W[k] for k in ("solver", "preconditioner", "nDirections", "tolerance", "relTol",

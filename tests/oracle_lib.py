@@ -36,6 +36,8 @@ def load_oracle() -> ctypes.CDLL:
         lib.rdsto_limiter.argtypes = [ctypes.c_int32, ctypes.c_double]
         lib.rdsto_set_partition.restype = ctypes.c_int32
         lib.rdsto_set_partition.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
+        lib.rdsto_grad_U.restype = ctypes.c_int32
+        lib.rdsto_grad_U.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         lib.rdsto_precondition.restype = ctypes.c_int32
         lib.rdsto_precondition.argtypes = [ctypes.c_void_p, d, d]
         lib.rdsto_cs_residual.restype = ctypes.c_int32
@@ -77,6 +79,14 @@ class OracleSolver(Solver):
         self._check(self.lib.rdsto_get_partition(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
                     "get_partition")
         return out
+
+    def grad_U(self):
+        """grad(U) (N x 3 x 3, [i, a, j] = d U_j / d x_a) as the viscous terms
+        use it at the current state (cellLimited when selected)."""
+        import numpy as np
+        out = np.empty((self.n_cells, 9))
+        self._check(self.lib.rdsto_grad_U(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "grad_U")
+        return out.reshape(-1, 3, 3)
 
     def precondition(self, b):
         import numpy as np

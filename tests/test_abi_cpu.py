@@ -58,6 +58,9 @@ def test_partition_host_only():
     ("solvers.W.nSweeps", "0", 1),
     ("solvers.W.fillInLevel", "4", 1),
     ("ilu.partition", "scotch", 1),
+    ("gradSchemes.grad(U)", "cellLimited Gauss linear 2", 1),
+    ("gradSchemes.grad(U)", "leastSquares", 6),
+    ("divSchemes.div(phi,nuTilda)", "Gauss QUICK", 6),
 ])
 def test_config_errors(key, value, status):
     case = cases.forward_step_c1().with_options(**{key: value})
@@ -96,7 +99,8 @@ def test_valid_options_reach_the_device_check():
         pytest.skip("a GPU is present")
     for case in (cases.forward_step_c1().with_options(**{"timeIntegration.timeIntegration": "Dual",
                                                          "ddtSchemes.default": "dual2ndDST"}),
-                 cases.rae2822(), cases.naca0012_turbulent(ni=97, nj=25, model="SARC1", first_cell=5e-3),
+                 cases.rae2822(), cases.rae2822(tutorial_schemes=True),
+                 cases.naca0012_turbulent(ni=97, nj=25, model="SARC1", first_cell=5e-3),
                  *[cases.forward_step_c1().with_options(**o) for o in (
                      {"solvers.W.solver": "GaussSeidel", "solvers.W.nSweeps": 2},
                      {"solvers.W.solver": "ILU"},
