@@ -124,16 +124,16 @@ typedef struct rdst_ctx rdst_ctx;
  *   "timeControls.neighbouring" "true" ...
  *   "ddtSchemes.default" "Euler" | "steadyStateDST" | "dual2ndDST"
  *   "interpolationSchemes.reconstruct(rho)" "OSPRE"
- *   "solvers.W.solver" "GMRES" | "BiCGStab" | "GaussSeidel" | "ILU"
+ *   "solvers.W.solver" "GMRES" | "BiCGStab" | "GaussSeidel" | "ILU" | "AMG"
  *   "solvers.W.preconditioner" "ILUC0" | "Cholesky" | "GaussSeidel" |
- *                              "ILUCp" | "diagonal" | "none"
+ *                              "ILUCp" | "AMG" | "diagonal" | "none"
  *   "solvers.W.nSweeps" "1"  "solvers.W.fillInLevel" "0"
  *   "fieldBounds.p" "0.001 10000"
  *   "thermo.R" / "thermo.Cp" / "transport.mu" / "transport.Pr" ...
  * (solver/preconditioner names as foam-extend registers them for the 5x5
  * block matrix, Vector5typedefs.C:1602-1708).  Unknown selector values
  * return RDST_ERR_CONFIG; reference options this path rejects
- * (directWaveSpeed false, AMG, dual time with a turbulence model)
+ * (directWaveSpeed false, SAMG, dual time with a turbulence model)
  * RDST_ERR_UNSUPPORTED.
  * Replaces createFields.H:115-152 (flux, Jacobian and iteration selection)
  * and timeDST::initialize (timeDST.C:67-208). */

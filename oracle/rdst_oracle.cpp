@@ -19,6 +19,7 @@
 // libraries can be loaded side by side.
 #include "../include/rdst.h"
 #include "../rhodst_b200/csrc/rdst_options.h"
+#include "../rhodst_b200/csrc/rdst_amg.h"
 
 #include <algorithm>
 #include <array>
@@ -1155,8 +1156,19 @@ void vcopy(Vec& y, const Vec& x) {
     for (int i = 0; i < (int)x.size(); ++i) y[i] = x[i];
 }
 
+// one coarse level of the AMG hierarchy: block CSR (rows ascending, columns
+// ascending, the diagonal among them), its diagonal inverses, and the map of
+// the finer level's nodes onto it
+struct AmgLevel {
+    int n = 0;
+    std::vector<int> start, col, dslot;
+    std::vector<t5> val, dinv;
+    std::vector<int> agg;                 // finer node -> node of this level
+};
+
 struct PreconData {
     int kind = PRECON_NONE;
+    std::vector<AmgLevel> amg;            // levels 1.. (level 0 is the matrix itself)
     int sweeps = 1;                       // Gauss-Seidel sweeps per application
     const LDU* A = nullptr;               // the matrix (Gauss-Seidel residual sweeps)
     std::vector<t5> Dinv;                 // diagonal: inv(D); factored: inv(pivot)
@@ -1180,6 +1192,68 @@ std::vector<std::vector<int>> part_rows(const Ctx& c) {
     return r;
 }
 
+// AMG set-up: the aggregation plan of the cell graph, then per coarse
+// level the Galerkin blocks (sums of the finer blocks between two
+// aggregates, finer rows ascending, then the finer row's blocks in column
+// order) and their diagonal inverses
+void build_amg(const Ctx& c, const LDU& A, PreconData& M) {
+    const int N = c.N;
+    M.A = &A;
+    M.Dinv.resize(N);
+    for (int i = 0; i < N; ++i) M.Dinv[i] = inv5(A.d[i]);
+    std::vector<std::vector<int>> adj(N);
+    for (int f = 0; f < c.Fi; ++f) { adj[c.own[f]].push_back(c.nei[f]); adj[c.nei[f]].push_back(c.own[f]); }
+    const AmgPlan P = amg_plan(adj, c.o.amg_min_coarse, c.o.amg_max_levels);
+    M.amg.clear();
+    // finer level as row lists of (column, block); level 0 from the LDU faces
+    std::vector<std::vector<std::pair<int, t5>>> rows(N);
+    for (int i = 0; i < N; ++i) {
+        rows[i].push_back({i, A.d[i]});
+        for (int f : c.cellFaces[i]) {
+            if (f >= c.Fi) break;
+            if (c.own[f] == i) rows[i].push_back({c.nei[f], A.u[f]});
+            else rows[i].push_back({c.own[f], A.l[f]});
+        }
+        std::stable_sort(rows[i].begin(), rows[i].end(), [](auto& a, auto& b) { return a.first < b.first; });
+    }
+    for (size_t l = 0; l < P.agg.size(); ++l) {
+        AmgLevel L;
+        L.n = P.n[l + 1];
+        L.agg = P.agg[l];
+        const auto& cadj = P.adj[l + 1];
+        L.start.assign(L.n + 1, 0);
+        for (int I = 0; I < L.n; ++I) L.start[I + 1] = L.start[I] + (int)cadj[I].size() + 1;
+        L.col.resize(L.start[L.n]);
+        L.dslot.resize(L.n);
+        for (int I = 0; I < L.n; ++I) {
+            std::vector<int> cols(cadj[I]);
+            cols.push_back(I);
+            std::sort(cols.begin(), cols.end());
+            for (size_t q = 0; q < cols.size(); ++q) {
+                L.col[L.start[I] + q] = cols[q];
+                if (cols[q] == I) L.dslot[I] = L.start[I] + (int)q;
+            }
+        }
+        L.val.assign(L.col.size(), t5{});
+        for (int i = 0; i < (int)rows.size(); ++i) {
+            const int I = L.agg[i];
+            for (auto& e : rows[i]) {
+                const int J = L.agg[e.first];
+                auto b = L.col.begin() + L.start[I], en = L.col.begin() + L.start[I + 1];
+                const int slot = (int)(std::lower_bound(b, en, J) - L.col.begin());
+                for (int k = 0; k < 25; ++k) L.val[slot][k] += e.second[k];
+            }
+        }
+        L.dinv.resize(L.n);
+        for (int I = 0; I < L.n; ++I) L.dinv[I] = inv5(L.val[L.dslot[I]]);
+        std::vector<std::vector<std::pair<int, t5>>> next(L.n);
+        for (int I = 0; I < L.n; ++I)
+            for (int q = L.start[I]; q < L.start[I + 1]; ++q) next[I].push_back({L.col[q], L.val[q]});
+        rows.swap(next);
+        M.amg.push_back(std::move(L));
+    }
+}
+
 void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
     M.kind = c.o.precon;
     const int N = c.N;
@@ -1187,6 +1261,10 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
         M.Dinv.resize(N);
         OMP_FOR
         for (int i = 0; i < N; ++i) M.Dinv[i] = inv5(A.d[i]);
+        return;
+    }
+    if (M.kind == PRECON_AMG) {
+        build_amg(c, A, M);
         return;
     }
     if (!lu_factored((Precon)M.kind)) return;
@@ -1299,6 +1377,70 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
 
 void lu_apply(const Ctx& c, const PreconData& M, Vec& x, const Vec& b, bool upper);
 
+// r = b - A x on AMG level l (0: the step's matrix)
+void amg_residual(const Ctx& c, const PreconData& M, int l, const Vec& x, const Vec& b, Vec& r) {
+    if (l == 0) {
+        Vec t;
+        Amul(c, *M.A, x, t);
+        r.resize(b.size());
+        for (size_t i = 0; i < b.size(); ++i) for (int k = 0; k < 5; ++k) r[i][k] = b[i][k] - t[i][k];
+        return;
+    }
+    const AmgLevel& L = M.amg[l - 1];
+    r.resize(L.n);
+    for (int I = 0; I < L.n; ++I) {
+        v5 a = b[I];
+        for (int q = L.start[I]; q < L.start[I + 1]; ++q) {
+            v5 t = mv(L.val[q], x[L.col[q]]);
+            for (int k = 0; k < 5; ++k) a[k] -= t[k];
+        }
+        r[I] = a;
+    }
+}
+
+// damped block-Jacobi sweep x += omega D^-1 (b - A x); from x = 0 when `zero`
+void amg_smooth(const Ctx& c, const PreconData& M, int l, Vec& x, const Vec& b, bool zero) {
+    const std::vector<t5>& Di = l == 0 ? M.Dinv : M.amg[l - 1].dinv;
+    const double w = c.o.amg_omega;
+    if (zero) {
+        x.resize(b.size());
+        for (size_t i = 0; i < b.size(); ++i) {
+            v5 t = mv(Di[i], b[i]);
+            for (int k = 0; k < 5; ++k) x[i][k] = w * t[k];
+        }
+        return;
+    }
+    Vec r;
+    amg_residual(c, M, l, x, b, r);
+    for (size_t i = 0; i < b.size(); ++i) {
+        v5 t = mv(Di[i], r[i]);
+        for (int k = 0; k < 5; ++k) x[i][k] += w * t[k];
+    }
+}
+
+// x = V-cycle on level l from x = 0: nPreSweeps sweeps, the residual
+// summed over the aggregates, the coarse correction injected back, then
+// nPostSweeps sweeps; the coarsest level takes amg.coarsestSweeps sweeps
+void amg_vcycle(const Ctx& c, const PreconData& M, int l, Vec& x, const Vec& b) {
+    const int nl = (int)M.amg.size() + 1;
+    if (l == nl - 1) {
+        amg_smooth(c, M, l, x, b, true);
+        for (int s = 1; s < c.o.amg_coarsest_sweeps; ++s) amg_smooth(c, M, l, x, b, false);
+        return;
+    }
+    bool zero = true;
+    for (int s = 0; s < c.o.amg_pre; ++s) { amg_smooth(c, M, l, x, b, zero); zero = false; }
+    if (zero) x.assign(b.size(), v5{0, 0, 0, 0, 0});
+    Vec r;
+    amg_residual(c, M, l, x, b, r);
+    const AmgLevel& L = M.amg[l];
+    Vec bc(L.n, v5{0, 0, 0, 0, 0}), xc;
+    for (size_t i = 0; i < r.size(); ++i) for (int k = 0; k < 5; ++k) bc[L.agg[i]][k] += r[i][k];
+    amg_vcycle(c, M, l + 1, xc, bc);
+    for (size_t i = 0; i < x.size(); ++i) for (int k = 0; k < 5; ++k) x[i][k] += xc[L.agg[i]][k];
+    for (int s = 0; s < c.o.amg_post; ++s) amg_smooth(c, M, l, x, b, false);
+}
+
 void precondition(const Ctx& c, const PreconData& M, Vec& x, const Vec& b) {
     const int N = c.N;
     x.resize(N);
@@ -1306,6 +1448,10 @@ void precondition(const Ctx& c, const PreconData& M, Vec& x, const Vec& b) {
     if (M.kind == PRECON_DIAGONAL) {
         OMP_FOR
         for (int i = 0; i < N; ++i) x[i] = mv(M.Dinv[i], b[i]);
+        return;
+    }
+    if (M.kind == PRECON_AMG) {
+        amg_vcycle(c, M, 0, x, b);
         return;
     }
     if (M.kind == PRECON_GAUSS_SEIDEL) {
@@ -1472,7 +1618,7 @@ void linear_solve(Ctx& c, const LDU& A, const PreconData& M, Vec& dx, Report& re
             cmpt_residual(r, nf, rep.lin_final);
             ++it;
         }
-    } else if (o.solver == SOLVER_GAUSS_SEIDEL || o.solver == SOLVER_ILU) {
+    } else if (o.solver == SOLVER_GAUSS_SEIDEL || o.solver == SOLVER_ILU || o.solver == SOLVER_AMG) {
         // stationary iteration dx += M^-1 (b - A dx) with Gauss-Seidel sweeps
         // or the Cholesky-type factorisation (BlockGaussSeidelSolver,
         // BlockILUSolver), the residual checked after every application

@@ -9,6 +9,8 @@
 #include "linalg.cuh"
 #include "turbulence.cuh"
 #include "adjoint.cuh"
+#include "amg.cuh"
+#include "rdst_amg.h"
 
 #include <algorithm>
 #include <cmath>
@@ -260,6 +262,18 @@ struct rdst_ctx {
     // Krylov
     DBuf<double> dx, r, t, Vb, s2, sh, ph, pv, xbar, Ax, pA;
     DBuf<double> gs_r, gs_z;        // residual and correction of Gauss-Seidel sweeps after the first
+    // block AMG: coarse levels 1.. (level 0 is the step's matrix)
+    struct AmgDev {
+        int n = 0, nnz = 0;
+        DBuf<int> start, col, dslot;   // block CSR, columns ascending
+        DBuf<int> gstart, gsrc;        // Galerkin gather: coarse slot -> finer slots
+        DBuf<int> mstart, mem;         // members (finer nodes) of each node, ascending
+        DBuf<int> agg;                 // finer node -> node of this level
+        DBuf<double> val, dinv;        // 25 nnz, 25 n
+        DBuf<double> x, b, r;          // 5 n
+    };
+    std::vector<std::unique_ptr<AmgDev>> amg;
+    DBuf<double> amg_r0;            // level-0 residual
     DBuf<float> Vf;                 // GMRES basis when it is kept in FP32
     long ldv = 0;                   // stride between basis vectors (entries)
     DBuf<double> wv;                // FP64 Arnoldi vector that is orthogonalised before it is stored in Vf
@@ -767,6 +781,82 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         c.lu_col.upload(lu_col, s); c.lu_src.upload(lu_src, s);
         c.lu_slots = MS;
     }
+    // ---- AMG hierarchy: plan on the cell graph (original numbering), level
+    // 0 in the internal row order; the Galerkin gather lists sum the finer
+    // blocks in finer-row order, then by slot
+    if (o.precon == PRECON_AMG) {
+        std::vector<std::vector<int>> adj0(N);
+        for (int f = 0; f < Fi; ++f) { adj0[mh->owner[f]].push_back(mh->neighbour[f]); adj0[mh->neighbour[f]].push_back(mh->owner[f]); }
+        const AmgPlan P = amg_plan(adj0, o.amg_min_coarse, o.amg_max_levels);
+        // finer-level slots per row: (column, slot id) with slot ids of the
+        // SELL store on level 0, CSR positions on coarse levels
+        std::vector<std::vector<std::pair<int, int>>> fine(N);
+        for (int r = 0; r < N; ++r) {
+            fine[r].push_back({r, flat(r, 0)});
+            for (size_t k = 0; k < rowcols[r].size(); ++k) fine[r].push_back({rowcols[r][k], flat(r, 1 + (int)k)});
+        }
+        // level-0 node ids are internal rows; the plan's are original cells
+        std::vector<int> node_of_row(c.perm);
+        for (size_t l = 0; l < P.agg.size(); ++l) {
+            auto L = std::make_unique<rdst_ctx::AmgDev>();
+            const int nf = (int)fine.size(), nc = P.n[l + 1];
+            const std::vector<int>& aggp = P.agg[l];          // plan node of level l -> level l+1
+            std::vector<int> agg(nf);                         // this context's finer ids -> coarse
+            for (int i = 0; i < nf; ++i) agg[i] = aggp[l == 0 ? node_of_row[i] : i];
+            const auto& cadj = P.adj[l + 1];
+            std::vector<int> start(nc + 1, 0), col, dslot(nc);
+            for (int I = 0; I < nc; ++I) {
+                std::vector<int> cols(cadj[I]);
+                cols.push_back(I);
+                std::sort(cols.begin(), cols.end());
+                for (int cc : cols) {
+                    if (cc == I) dslot[I] = (int)col.size();
+                    col.push_back(cc);
+                }
+                start[I + 1] = (int)col.size();
+            }
+            const int nnz = (int)col.size();
+            std::vector<std::vector<int>> lists(nnz);
+            // finer rows in plan order (original cell order on level 0)
+            std::vector<int> order(nf);
+            for (int i = 0; i < nf; ++i) order[i] = i;
+            if (l == 0) for (int i = 0; i < nf; ++i) order[i] = c.iperm[i];
+            for (int i : order)
+                for (auto& e : fine[i]) {
+                    const int I = agg[i], J = agg[e.first];
+                    const int sl = (int)(std::lower_bound(col.begin() + start[I], col.begin() + start[I + 1], J) -
+                                         col.begin());
+                    lists[sl].push_back(e.second);
+                }
+            std::vector<int> gstart(nnz + 1, 0), gsrc;
+            for (int q = 0; q < nnz; ++q) {
+                gsrc.insert(gsrc.end(), lists[q].begin(), lists[q].end());
+                gstart[q + 1] = (int)gsrc.size();
+            }
+            std::vector<std::vector<int>> members(nc);
+            for (int i : order) members[agg[i]].push_back(i);
+            std::vector<int> mstart(nc + 1, 0), mem;
+            for (int I = 0; I < nc; ++I) {
+                mem.insert(mem.end(), members[I].begin(), members[I].end());
+                mstart[I + 1] = (int)mem.size();
+            }
+            L->n = nc; L->nnz = nnz;
+            L->start.upload(start, s); L->col.upload(col, s); L->dslot.upload(dslot, s);
+            L->gstart.upload(gstart, s); L->gsrc.upload(gsrc, s);
+            L->mstart.upload(mstart, s); L->mem.upload(mem, s); L->agg.upload(agg, s);
+            L->val.alloc(25L * nnz); L->dinv.alloc(25L * nc);
+            L->x.alloc(5L * nc); L->b.alloc(5L * nc); L->r.alloc(5L * nc);
+            L->x.zero(s);
+            c.amg.push_back(std::move(L));
+            // this level's rows for the next: (column, CSR position)
+            std::vector<std::vector<std::pair<int, int>>> next(nc);
+            for (int I = 0; I < nc; ++I)
+                for (int q = start[I]; q < start[I + 1]; ++q) next[I].push_back({col[q], q});
+            fine.swap(next);
+            CK(cudaStreamSynchronize(s));     // the host vectors of this level go out of scope
+        }
+        c.amg_r0.alloc(5L * N);
+    }
     // ---- upload
     c.own.upload(own, s); c.nei.upload(nei, s);
     c.bcell.upload(bcell, s); c.bpatch.upload(bpatch, s);
@@ -901,10 +991,82 @@ struct Ops {
                                                         c.o.beta, c.dual_a);
         CKL();
     }
+    // AMG coarse levels of the matrix in Aval (the step's A, or A^T for the adjoint)
+    static void amg_setup(rdst_ctx& c) {
+        k_dinv<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.dinv);
+        CKL();
+        for (size_t l = 0; l < c.amg.size(); ++l) {
+            auto& L = *c.amg[l];
+            const long t = 25L * L.nnz;
+            if (l == 0)
+                k_amg_gather_sell<MT><<<nblk(t, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.Aval), L.gstart.p, L.gsrc.p, L.val.p,
+                                                                     L.nnz);
+            else
+                k_amg_gather_csr<<<nblk(t, TPB), TPB, 0, c.s>>>(c.amg[l - 1]->val.p, L.gstart.p, L.gsrc.p, L.val.p,
+                                                                L.nnz);
+            CKL();
+            k_amg_dinv<<<nblk(L.n, 128), 128, 0, c.s>>>(L.n, L.dslot.p, L.val.p, L.dinv.p);
+            CKL();
+        }
+    }
+    // r = b - A x and the damped block-Jacobi update on level l
+    static void amg_resid(rdst_ctx& c, int l, const double* x, const double* b, double* r, const int* act) {
+        if (l == 0) {
+            k_spmv<MT, double><<<nblk(c.N, 256), 256, 0, c.s>>>(c.mat<MT>(c.Aval), x, r, b, act);
+        } else {
+            auto& L = *c.amg[l - 1];
+            k_amg_resid<<<nblk(L.n, 128), 128, 0, c.s>>>(L.n, L.start.p, L.col.p, L.val.p, x, b, r, act);
+        }
+        CKL();
+    }
+    static void amg_jacobi(rdst_ctx& c, int l, const double* r, double* x, int zero, const int* act) {
+        if (l == 0)
+            k_amg_jacobi0<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.N, (const MT*)c.dinv, r, x, c.o.amg_omega, zero, act);
+        else {
+            auto& L = *c.amg[l - 1];
+            k_amg_jacobi<<<nblk(L.n, 128), 128, 0, c.s>>>(L.n, L.dinv.p, r, x, c.o.amg_omega, zero, act);
+        }
+        CKL();
+    }
+    // x = one V-cycle on level l from x = 0 (level 0: b = in, x = out)
+    static void amg_vcycle(rdst_ctx& c, int l, const double* b, double* x, const int* act) {
+        const int nl = (int)c.amg.size() + 1;
+        const long n = l == 0 ? c.N : c.amg[l - 1]->n;
+        double* r = l == 0 ? c.amg_r0.p : c.amg[l - 1]->r.p;
+        if (l == nl - 1) {
+            amg_jacobi(c, l, b, x, 1, act);
+            for (int sw = 1; sw < c.o.amg_coarsest_sweeps; ++sw) {
+                amg_resid(c, l, x, b, r, act);
+                amg_jacobi(c, l, r, x, 0, act);
+            }
+            return;
+        }
+        bool zero = true;
+        for (int sw = 0; sw < c.o.amg_pre; ++sw) {
+            if (zero) amg_jacobi(c, l, b, x, 1, act);
+            else { amg_resid(c, l, x, b, r, act); amg_jacobi(c, l, r, x, 0, act); }
+            zero = false;
+        }
+        if (zero) { k_amg_zero<<<nblk(5 * n, TPB), TPB, 0, c.s>>>(5 * n, x, act); CKL(); }
+        amg_resid(c, l, x, b, r, act);
+        auto& C = *c.amg[l];
+        k_amg_restrict<<<nblk(C.n, 128), 128, 0, c.s>>>(C.n, C.mstart.p, C.mem.p, r, C.b.p, act);
+        CKL();
+        amg_vcycle(c, l + 1, C.b.p, C.x.p, act);
+        k_amg_prolong<<<nblk(n, 128), 128, 0, c.s>>>((int)n, C.agg.p, C.x.p, x, act);
+        CKL();
+        for (int sw = 0; sw < c.o.amg_post; ++sw) {
+            amg_resid(c, l, x, b, r, act);
+            amg_jacobi(c, l, r, x, 0, act);
+        }
+    }
     static void precond_setup(rdst_ctx& c) {
         if (c.o.precon == PRECON_DIAGONAL) {
             k_dinv<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.dinv);
             CKL();
+        } else if (c.o.precon == PRECON_AMG) {
+            Timed tm(c, KS_FACTOR);
+            amg_setup(c);
         } else if (lu_factored(c.o.precon)) {
             Timed tm(c, KS_FACTOR);
             const int n_fid = c.n_slices * c.lu_slots * 32;
@@ -933,6 +1095,8 @@ struct Ops {
         if (c.o.precon == PRECON_DIAGONAL) {
             k_jacobi<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.N, (const MT*)c.dinv, in, out, active);
             CKL();
+        } else if (c.o.precon == PRECON_AMG) {
+            amg_vcycle(c, 0, in, out, active);
         } else if (lu_factored(c.o.precon)) {
             lu_apply(c, in, out, active);
             // further Gauss-Seidel sweeps: out += (D + L)^-1 (in - A out)
@@ -1689,6 +1853,10 @@ void adj_precond_setup(rdst_ctx& c) {
     if (c.o.precon == PRECON_DIAGONAL) {
         k_dinv<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.dinv);
         CKL();
+    } else if (c.o.precon == PRECON_AMG) {
+        std::swap(c.Aval, c.a_AT);
+        Ops<MT>::amg_setup(c);
+        std::swap(c.Aval, c.a_AT);
     } else if (lu_factored(c.o.precon)) {
         const int n_fid = c.n_slices * c.lu_slots * 32;
         k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, c.lu_src.p, n_fid);

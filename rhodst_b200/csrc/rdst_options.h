@@ -24,12 +24,14 @@ enum FluxScheme { FLUX_KURGANOV = 0, FLUX_HLL, FLUX_HLLC, FLUX_HLLCP, FLUX_AUSMP
                   FLUX_AUSMPLUSUP, FLUX_AUSM };
 enum Limiter { LIM_LINEAR = 0, LIM_UPWIND, LIM_OSPRE, LIM_VANLEER, LIM_MINMOD, LIM_VANALBADA,
                LIM_SUPERBEE, LIM_MUSCL, LIM_VENKATAKRISHNAN };
-enum Solver { SOLVER_GMRES = 0, SOLVER_BICGSTAB, SOLVER_GAUSS_SEIDEL, SOLVER_ILU };
+enum Solver { SOLVER_GMRES = 0, SOLVER_BICGSTAB, SOLVER_GAUSS_SEIDEL, SOLVER_ILU, SOLVER_AMG };
 // ILU0: ILUC0 (exact ILU on the matrix pattern); CHOLESKY: the diagonal-only
 // incomplete factorisation (D~ + L) D~^-1 (D~ + U); GAUSS_SEIDEL: forward
 // block Gauss-Seidel sweeps (D + L)^-1; ILUCP: ILU on the pattern extended
-// to cells within fillInLevel + 1 faces
-enum Precon { PRECON_NONE = 0, PRECON_DIAGONAL, PRECON_ILU0, PRECON_CHOLESKY, PRECON_GAUSS_SEIDEL, PRECON_ILUCP };
+// to cells within fillInLevel + 1 faces; AMG: one V-cycle of aggregation
+// AMG with damped block-Jacobi smoothing
+enum Precon { PRECON_NONE = 0, PRECON_DIAGONAL, PRECON_ILU0, PRECON_CHOLESKY, PRECON_GAUSS_SEIDEL, PRECON_ILUCP,
+              PRECON_AMG };
 enum Ddt { DDT_EULER = 0, DDT_STEADY, DDT_DUAL2ND };
 enum Precision { PREC_FP64 = 0, PREC_FP32, PREC_BF16 };
 enum Turbulence { TURB_LAMINAR = 0, TURB_SANEG, TURB_SARC1, TURB_SARC2, TURB_SA };
@@ -80,6 +82,11 @@ struct Options {
     int max_iter = 1000, min_iter = 0;
     int n_sweeps = 1;                 // Gauss-Seidel sweeps per application (nSweeps)
     int fill_in = 0;                  // ILUCp extension level (fillInLevel)
+    int amg_pre = 0, amg_post = 2;    // AMG nPreSweeps / nPostSweeps (block-Jacobi sweeps per level)
+    int amg_max_levels = 100;         // AMG nMaxLevels
+    int amg_min_coarse = 4;           // AMG minCoarseEqns (cells on the coarsest level)
+    int amg_coarsest_sweeps = 10;     // block-Jacobi sweeps on the coarsest level
+    double amg_omega = 0.6;           // block-Jacobi damping of the AMG smoother
     // fvSolution: fieldBounds (updateFields.H:44-62)
     double rho_min = 1e-15, rho_max = 1e10, p_min = 1e-15, p_max = 1e10, T_min = 1e-15, T_max = 1e10;
     // thermophysicalProperties (perfectGas, hConstThermo, const/Sutherland transport)
@@ -251,8 +258,7 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             else if (t == "BiCGStab") o.solver = SOLVER_BICGSTAB;
             else if (t == "GaussSeidel") o.solver = SOLVER_GAUSS_SEIDEL;
             else if (t == "ILU") o.solver = SOLVER_ILU;
-            else if (t == "AMG")
-                throw ConfigError("block solver AMG is not on this path (BiCGStab GMRES GaussSeidel ILU)", true);
+            else if (t == "AMG") o.solver = SOLVER_AMG;
             else if (t == "CG")
                 throw ConfigError("Unknown asymmetric matrix solver CG\n"
                                   "Valid asymmetric matrix solvers are: (AMG BiCGStab GMRES GaussSeidel ILU)");
@@ -263,13 +269,26 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             else if (t == "Cholesky") o.precon = PRECON_CHOLESKY;
             else if (t == "GaussSeidel") o.precon = PRECON_GAUSS_SEIDEL;
             else if (t == "ILUCp") o.precon = PRECON_ILUCP;
+            else if (t == "AMG") o.precon = PRECON_AMG;
             else if (t == "diagonal" || t == "Jacobi") o.precon = PRECON_DIAGONAL;
             else if (t == "none") o.precon = PRECON_NONE;
-            else if (t == "AMG" || t == "SAMG")
+            else if (t == "SAMG")
                 throw ConfigError("preconditioner " + t +
-                                  " is not on this path (Cholesky GaussSeidel ILUC0 ILUCp diagonal none)", true);
+                                  " is not on this path (AMG Cholesky GaussSeidel ILUC0 ILUCp diagonal none)", true);
             else throw ConfigError("Unknown block preconditioner " + t);
         }
+        else if (k == "solvers.W.nPreSweeps" || k == "solvers.W.preconditioner.nPreSweeps") o.amg_pre = parse_int(k, v);
+        else if (k == "solvers.W.nPostSweeps" || k == "solvers.W.preconditioner.nPostSweeps") o.amg_post = parse_int(k, v);
+        else if (k == "solvers.W.nMaxLevels" || k == "solvers.W.preconditioner.nMaxLevels")
+            o.amg_max_levels = parse_int(k, v);
+        else if (k == "solvers.W.minCoarseEqns" || k == "solvers.W.preconditioner.minCoarseEqns")
+            o.amg_min_coarse = parse_int(k, v);
+        else if (k == "solvers.W.smoother" || k == "solvers.W.preconditioner.smoother") {
+            if (t != "Jacobi" && t != "diagonal")
+                throw ConfigError("AMG smoother " + t + " is not on this path (Jacobi)", true);
+        }
+        else if (k == "amg.omega") o.amg_omega = parse_double(k, v);
+        else if (k == "amg.coarsestSweeps") o.amg_coarsest_sweeps = parse_int(k, v);
         else if (k == "solvers.W.nSweeps" || k == "solvers.W.preconditioner.nSweeps") o.n_sweeps = parse_int(k, v);
         else if (k == "solvers.W.fillInLevel" || k == "solvers.W.preconditioner.fillInLevel") o.fill_in = parse_int(k, v);
         else if (k == "solvers.W.nDirections") o.n_directions = parse_int(k, v);
@@ -361,6 +380,12 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
     // sweeps, or (BlockILUSolver) the Cholesky-type incomplete factorisation
     if (o.solver == SOLVER_GAUSS_SEIDEL) o.precon = PRECON_GAUSS_SEIDEL;
     if (o.solver == SOLVER_ILU) o.precon = PRECON_CHOLESKY;
+    if (o.solver == SOLVER_AMG) o.precon = PRECON_AMG;
+    if (o.amg_pre < 0 || o.amg_post < 0 || o.amg_pre + o.amg_post < 1 || o.amg_pre > 16 || o.amg_post > 16)
+        throw ConfigError("AMG nPreSweeps/nPostSweeps must be in [0,16] with at least one sweep");
+    if (o.amg_max_levels < 2 || o.amg_min_coarse < 1 || o.amg_coarsest_sweeps < 1 || o.amg_coarsest_sweeps > 200)
+        throw ConfigError("AMG needs nMaxLevels >= 2, minCoarseEqns >= 1, coarsestSweeps in [1,200]");
+    if (!(o.amg_omega > 0.0 && o.amg_omega <= 1.0)) throw ConfigError("amg.omega must be in (0,1]");
     if (!(o.R > 0) || !(o.Cp > o.R)) throw ConfigError("thermo: need 0 < R < Cp");
     if (o.lim_U == LIM_VENKATAKRISHNAN) {}
     // dual-time stepping: the Dual iteration with the dual2ndDST ddt (the

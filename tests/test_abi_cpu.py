@@ -44,7 +44,10 @@ def test_partition_host_only():
 @pytest.mark.parametrize("key,value,status", [
     ("fluxScheme", "Roe", 1),                      # unknown selector -> FatalError analogue
     ("Jacobian", "Steger", 1),
-    ("solvers.W.solver", "AMG", 6),                # selectable in foam, not on this path
+    ("solvers.W.preconditioner", "SAMG", 6),       # selectable in foam, not on this path
+    ("solvers.W.smoother", "GaussSeidel", 6),       # AMG smoothing is block Jacobi here
+    ("amg.omega", "1.5", 1),
+    ("solvers.W.nPostSweeps", "-1", 1),
     ("directWaveSpeed", "false", 6),               # latent reference bug rejected
     ("ddtSchemes.default", "dual2ndDST", 6),
     ("timeIntegration.timeIntegration", "Dual", 6),
@@ -53,7 +56,6 @@ def test_partition_host_only():
     ("RASModel", "kEpsilon", 1),
     ("timeIntegration.maxInnerIter", "-1", 1),
     ("solvers.W.solver", "CG", 1),                 # symmetric matrices only in foam-extend
-    ("solvers.W.preconditioner", "AMG", 6),
     ("solvers.W.preconditioner", "ILUCq", 1),
     ("solvers.W.nSweeps", "0", 1),
     ("solvers.W.fillInLevel", "4", 1),
@@ -106,7 +108,9 @@ def test_valid_options_reach_the_device_check():
                      {"solvers.W.solver": "ILU"},
                      {"solvers.W.preconditioner": "Cholesky"},
                      {"solvers.W.preconditioner": {"preconditioner": "GaussSeidel", "nSweeps": 3}},
-                     {"solvers.W.preconditioner": "ILUCp", "solvers.W.fillInLevel": 1})]):
+                     {"solvers.W.preconditioner": "ILUCp", "solvers.W.fillInLevel": 1},
+                     {"solvers.W.preconditioner": "AMG", "solvers.W.nPreSweeps": 1},
+                     {"solvers.W.solver": "AMG", "solvers.W.smoother": "Jacobi"})]):
         with pytest.raises(_abi.RdstError) as e:
             rhodst_b200.Solver(case.mesh, case.bcs, case.options)
         assert e.value.status == 3, case.name

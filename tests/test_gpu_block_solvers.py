@@ -1,7 +1,8 @@
 """B200 library vs. CPU oracle for the other selectable block preconditioners
 and solvers: Cholesky (diagonal-based incomplete factorisation), Gauss-Seidel
 sweeps, ILUCp with fill-in, and the stationary GaussSeidel / ILU solvers;
-and the subdomain ILU(0) on graph-bisection subdomains.
+block AMG (preconditioner and solver); and the subdomain ILU(0) on
+graph-bisection subdomains.
 
 Both sides run the same subdomain partition (the GPU's RCB parts, passed to
 the oracle), FP64 throughout.  Step trajectories agree to 1e-9 relative (the
@@ -62,8 +63,19 @@ def test_preconditioned_steps(solver, precon, extra):
     run_pair(step_case(solver, precon, iters=2 if solver == "BiCGStab" else 1, **extra), 4, parts=8)
 
 
+@pytest.mark.parametrize("solver,extra", [
+    ("GMRES", {}),
+    ("BiCGStab", {"solvers.W.nPreSweeps": 1, "solvers.W.nPostSweeps": 1, "amg.omega": 0.8}),
+    ("GMRES", {"solvers.W.minCoarseEqns": 200, "amg.coarsestSweeps": 4}),
+])
+def test_amg_preconditioned_steps(solver, extra):
+    """Block AMG (aggregation of the cell graph, Galerkin coarse blocks
+    gathered on the device every step, damped block-Jacobi V-cycle)."""
+    run_pair(step_case(solver, "AMG", iters=2 if solver == "BiCGStab" else 1, **extra), 4, parts=1)
+
+
 @pytest.mark.parametrize("solver,extra", [("GaussSeidel", {}), ("GaussSeidel", {"solvers.W.nSweeps": 2}),
-                                          ("ILU", {})])
+                                          ("ILU", {}), ("AMG", {})])
 def test_stationary_solver_steps(solver, extra):
     rg, _ = run_pair(step_case(solver, "none", iters=6, **extra), 4, parts=8)
     assert all(r["lin_iterations"] == 6 for r in rg)
