@@ -27,7 +27,8 @@ def _gpu_available() -> bool:
 # Modules that run after the step, adjoint and shape parity suites (the
 # selectable-solver rows and the frozen-turbulence gradient), so that those
 # suites report first; the allocation-free module stays last.
-_LATE = ("test_gpu_block_solvers.py", "test_gpu_adjoint_frozen_sa.py", "test_gpu_tutorial_schemes.py")
+_LATE = ("test_gpu_block_solvers.py", "test_gpu_adjoint_frozen_sa.py", "test_gpu_tutorial_schemes.py",
+         "test_gpu_adjoint_c5.py")
 
 
 def _order(item):
