@@ -262,6 +262,16 @@ const char* rdst_last_error(const rdst_ctx* ctx);
 /* Release the context and all its device memory. */
 void rdst_destroy(rdst_ctx* ctx);
 
+/* Held cells (no reference counterpart: the halo cells of an overlapping
+ * domain decomposition, where the reference has processor patches): cells
+ * with mask[i] != 0 (original numbering, n_cells entries) keep their state
+ * in the steps -- their residual is zero (so they enter neither the
+ * residual norms nor the CFL ramp) and their rows of the implicit system
+ * are identity rows with no right-hand side.  Their states still enter the
+ * neighbours' fluxes, as Dirichlet data set with rdst_set_conservative.
+ * NULL clears the mask. */
+rdst_status rdst_set_held_cells(rdst_ctx* ctx, const uint8_t* mask);
+
 /* Host-only helper (no GPU needed): recursive coordinate bisection of the
  * cell centres into n_parts parts, out_part[n_cells].  The GPU library uses
  * the same partition for its subdomain ILU(0) (block-Jacobi across parts,

@@ -182,6 +182,7 @@ struct Ctx {
     bool viscous = false;
     // residual R_ (baseFluxDST R_, per unit volume) and face fluxes
     std::vector<v5> Rv;
+    std::vector<unsigned char> rmask;  // held cells: zero residual, identity rows (empty: none)
     std::vector<double> phi, phiEp;
     std::vector<v3> phiUp, Up;
     // time control (timeDST)
@@ -193,6 +194,7 @@ struct Ctx {
     // old-time value; 6 components, symmetric) and rho before the update
     std::vector<std::array<double, 6>> S_old;
     bool S_old_valid = false;
+    bool state_set = false;           // a state has been set (later sets keep the time-control history)
     std::vector<double> rho0;
     // dual-time stepping: W at the two previous time levels, foam Time's
     // deltaTSave (deltaT0 of the next step), the step's BDF2 coefficients
@@ -866,6 +868,9 @@ void compute_flux(Ctx& c) {
         c.Rv[i][4] = div(i, [&](int f) { return c.phiEp[f]; });
     }
     if (c.viscous) viscous_terms(c);
+    if (!c.rmask.empty())
+        for (int i = 0; i < c.N; ++i)
+            if (c.rmask[i]) c.Rv[i] = v5{0, 0, 0, 0, 0};
 }
 
 // Laminar viscosity: constTransport mu, or Sutherland As sqrt(T)/(1 + Ts/T)
@@ -1114,6 +1119,19 @@ void assemble(Ctx& c, LDU& A) {
     OMP_FOR
     for (int i = 0; i < N; ++i)
         for (int k = 0; k < 5; ++k) A.s[i][k] -= c.Rv[i][k] * c.V[i];
+    // held (halo) cells: identity rows, no source, so their update is zero
+    if (!c.rmask.empty()) {
+        for (int i = 0; i < N; ++i) {
+            if (!c.rmask[i]) continue;
+            A.d[i] = t5{};
+            for (int k = 0; k < 5; ++k) A.d[i][6 * k] = 1.0;
+            A.s[i] = v5{0, 0, 0, 0, 0};
+        }
+        for (int f = 0; f < Fi; ++f) {
+            if (c.rmask[c.own[f]]) A.u[f] = t5{};      // row owner, column neighbour
+            if (c.rmask[c.nei[f]]) A.l[f] = t5{};      // row neighbour, column owner
+        }
+    }
 }
 
 // ----------------------------------------------------------------------
@@ -2376,6 +2394,7 @@ static void init_from_primitive(Ctx& c) {
     }
     eval_boundary(c);
     initialize_time(c);
+    c.state_set = true;
 }
 
 ORACLE_API rdst_status rdsto_set_primitive(rdst_ctx* ctx, const double* p, const double* U, const double* T,
@@ -2400,6 +2419,14 @@ ORACLE_API rdst_status rdsto_set_primitive(rdst_ctx* ctx, const double* p, const
     return RDST_OK;
 }
 
+ORACLE_API rdst_status rdsto_set_held_cells(rdst_ctx* ctx, const uint8_t* mask) {
+    if (!ctx) return RDST_ERR_ARG;
+    Ctx& c = ctx->c;
+    if (!mask) c.rmask.clear();
+    else c.rmask.assign(mask, mask + c.N);
+    return RDST_OK;
+}
+
 ORACLE_API rdst_status rdsto_set_conservative(rdst_ctx* ctx, const double* rho, const double* rhoU,
                                               const double* rhoE) {
     if (!ctx || !rho || !rhoU || !rhoE) return RDST_ERR_ARG;
@@ -2409,6 +2436,22 @@ ORACLE_API rdst_status rdsto_set_conservative(rdst_ctx* ctx, const double* rho, 
         double e = rhoE[i] / rho[i] - 0.5 * magSqr(c.U[i]);
         c.T[i] = e / c.Cv;
         c.p[i] = rho[i] * c.R * c.T[i];
+    }
+    if (c.state_set) {
+        // fields replaced between steps: boundary values from the new
+        // internal field (with the boundary branches of the last
+        // evaluation), time-control history kept
+        c.S_old_valid = false;
+        c.dual_started = false;
+        c.dt_save = c.o.delta_t;
+        for (int i = 0; i < c.N; ++i) {
+            c.h[i] = c.Cp * c.T[i];
+            c.rho[i] = rho[i];
+            c.rhoU[i] = {rhoU[3 * i], rhoU[3 * i + 1], rhoU[3 * i + 2]};
+            c.rhoE[i] = rhoE[i];
+        }
+        eval_boundary(c);
+        return RDST_OK;
     }
     init_from_primitive(c);
     for (int i = 0; i < c.N; ++i) {           // keep the given W exactly

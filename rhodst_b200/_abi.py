@@ -115,6 +115,7 @@ def declare(lib: ctypes.CDLL, prefix: str) -> None:
     f("create", c_int32, [POINTER(RdstMesh), c_int32, POINTER(c_char_p), POINTER(c_char_p), POINTER(vp)])
     f("set_primitive", c_int32, [vp, dp, dp, dp, dp])
     f("set_conservative", c_int32, [vp, dp, dp, dp])
+    f("set_held_cells", c_int32, [vp, POINTER(ctypes.c_uint8)])
     f("get_conservative", c_int32, [vp, dp, dp, dp])
     f("get_primitive", c_int32, [vp, dp, dp, dp, dp])
     f("step", c_int32, [vp, c_int32, POINTER(RdstStepReport)])
@@ -259,6 +260,18 @@ class Solver:
         T = np.ascontiguousarray(np.broadcast_to(T, (N,)), dtype=np.float64)
         nt = None if nuTilda is None else np.ascontiguousarray(np.broadcast_to(nuTilda, (N,)), dtype=np.float64)
         self._check(self._fn("set_primitive")(self._h, _dptr(p), _dptr(U), _dptr(T), _dptr(nt)), "set_primitive")
+
+    def set_held_cells(self, mask=None):
+        """Cells held at their state in the steps (the halo cells of a
+        decomposed run: zero residual, identity rows), or None for none."""
+        if mask is None:
+            self._check(self._fn("set_held_cells")(self._h, None), "set_held_cells")
+            return
+        mk = np.ascontiguousarray(np.asarray(mask, dtype=bool), dtype=np.uint8)
+        if mk.shape != (self.n_cells,):
+            raise ValueError("mask needs one entry per cell")
+        self._check(self._fn("set_held_cells")(self._h, mk.ctypes.data_as(POINTER(ctypes.c_uint8))),
+                    "set_held_cells")
 
     def set_conservative(self, rho, rhoU, rhoE):
         N = self.n_cells

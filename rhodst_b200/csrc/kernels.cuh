@@ -755,6 +755,10 @@ __global__ void k_residual(DevMesh m, const double* __restrict__ fl, const doubl
             for (int k = 0; k < 3; ++k) Rv[1 + k] -= vs[k] / Vi + vs[3 + k] / Vi;
             Rv[4] -= vs[6] / Vi;
         }
+        if (m.rmask && m.rmask[i]) {
+#pragma unroll
+            for (int c = 0; c < 5; ++c) Rv[c] = 0.0;
+        }
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             double Rc = Rv[c];

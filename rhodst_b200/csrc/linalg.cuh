@@ -123,6 +123,20 @@ __global__ void k_jacobi(int N, const MT* __restrict__ dinv, const double* __res
     }
 }
 
+// held cells' rows of the block matrix -> identity (their update is zero;
+// the right-hand side of those rows is zero through the residual mask)
+template <typename MT>
+__global__ void k_hold_rows(SellMat<MT> A, const unsigned char* __restrict__ mask) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.N || !mask[r]) return;
+    const int sl = r >> 5, w = A.slice_w[sl];
+    for (int k = 0; k < w; ++k) {
+        const int fid = (A.slice_off[sl] + k) * 32 + (r & 31);
+#pragma unroll
+        for (int e = 0; e < 25; ++e) st(A.val + flat_e(fid, e), (k == 0 && e % 6 == 0) ? 1.0 : 0.0);
+    }
+}
+
 // y += x (skipped when *active is 0)
 __global__ void k_vadd(long n, const double* __restrict__ x, double* __restrict__ y, const int* __restrict__ active) {
     if (active && !*active) return;

@@ -274,6 +274,7 @@ struct rdst_ctx {
     };
     std::vector<std::unique_ptr<AmgDev>> amg;
     DBuf<double> amg_r0;            // level-0 residual
+    DBuf<unsigned char> rmask;      // held cells (internal order): zero residual, identity rows; empty: none
     DBuf<float> Vf;                 // GMRES basis when it is kept in FP32
     long ldv = 0;                   // stride between basis vectors (entries)
     DBuf<double> wv;                // FP64 Arnoldi vector that is orthogonalised before it is stored in Vf
@@ -990,6 +991,10 @@ struct Ops {
                                                         c.rdt.p, c.mut.p, c.sc.p, (c.steady || c.o.dual) ? 1 : 0,
                                                         c.o.beta, c.dual_a);
         CKL();
+        if (c.m.rmask) {
+            k_hold_rows<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(A, c.m.rmask);
+            CKL();
+        }
     }
     // AMG coarse levels of the matrix in Aval (the step's A, or A^T for the adjoint)
     static void amg_setup(rdst_ctx& c) {
@@ -2137,6 +2142,24 @@ RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const doub
             if (m.NB > 0) { k_sa_mutb<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->tr, c->bs.p, c->sa); CKL(); }
             CK(cudaStreamSynchronize(c->s));
         }
+    });
+}
+
+RDST_API rdst_status rdst_set_held_cells(rdst_ctx* c, const uint8_t* mask) {
+    if (!c) return RDST_ERR_ARG;
+    return guarded(c, [&] {
+        if (!mask) {
+            c->rmask.free_();
+            c->m.rmask = nullptr;
+        } else {
+            std::vector<unsigned char> mk(c->N);
+            for (int r = 0; r < c->N; ++r) mk[r] = mask[c->perm[r]] ? 1 : 0;
+            c->rmask.upload(mk, c->s);
+            c->m.rmask = c->rmask.p;
+            CK(cudaStreamSynchronize(c->s));
+        }
+        // the captured step graphs hold the mesh record: capture them again
+        c->reset_graphs();
     });
 }
 

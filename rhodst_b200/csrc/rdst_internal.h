@@ -63,6 +63,7 @@ struct DevMesh {
     const int* cc_start;   // [N+1] cell->cell (internal faces), for HLLCP
     const int* cc_list;
     const DevPatch* patches;
+    const unsigned char* rmask = nullptr;   // cells whose residual is held at zero (halo cells), or none
 };
 
 struct Thermo {

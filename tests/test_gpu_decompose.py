@@ -1,0 +1,94 @@
+"""The decomposed steady solve on the B200 library.
+
+* Held cells (the halo of a subdomain): GPU steps match the oracle's with
+  the same held cells on a subdomain mesh, 1e-9.
+* Two ranks, each a process with its own context on this GPU, exchange
+  halos through gloo between steps (no kernel waits on the other rank) and
+  reach the single-context steady state: owned states agree to 1e-8.
+"""
+import os
+import socket
+import tempfile
+
+import numpy as np
+import pytest
+
+import rhodst_b200
+from rhodst_b200 import decompose
+from tests.oracle_lib import OracleSolver
+from tests.test_decompose import steady_case
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+def test_held_cells_steps_parity():
+    c = steady_case().with_options(**{"ilu.parts": 2})
+    sub = decompose.decompose(c.mesh, 3)[1]
+    bcs = dict(c.bcs)
+    bcs[decompose.HALO_PATCH] = {"p": "zeroGradient", "U": "zeroGradient", "T": "zeroGradient"}
+    part = rhodst_b200.partition_cells(sub.mesh.C, 2)
+    gpu = rhodst_b200.Solver(sub.mesh, bcs, c.options)
+    ora = OracleSolver(sub.mesh, bcs, c.options, partition=part)
+    for s in (gpu, ora):
+        s.set_primitive(c.p[sub.cells], c.U[sub.cells], c.T[sub.cells])
+        s.set_held_cells(~sub.owned)
+    W0 = gpu.conservative()
+    rg, ro = gpu.step(5), ora.step(5)
+    for a, b in zip(rg, ro):
+        assert abs(a["res_mag"] - b["res_mag"]) <= 1e-9 * abs(b["res_mag"])
+    Wg, Wo = gpu.conservative(), ora.conservative()
+    for a, b, a0 in zip(Wg, Wo, W0):
+        assert rel(a, b) < 1e-9
+        assert np.array_equal(a[~sub.owned], a0[~sub.owned])          # held cells keep their state
+    assert np.abs(gpu.residual()[~sub.owned]).max() == 0.0
+
+
+def _rank(rank, world, port, out):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import torch.distributed as dist
+    from rhodst_b200.distributed import DecomposedSolver
+    from tests.test_decompose import steady_case as sc
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        d = DecomposedSolver(sc())
+        hist = [d.residual_l2()[0]]
+        for _ in range(8):
+            d.step(50)
+            hist.append(d.residual_l2()[0])
+            if hist[-1] < 1e-12 * hist[0]:
+                break
+        ids, rho, rhoU, rhoE = d.owned_state()
+        np.savez(f"{out}_{rank}.npz", ids=ids, rho=rho, rhoU=rhoU, rhoE=rhoE, hist=np.array(hist))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_on_one_gpu_reach_the_single_context_steady_state():
+    import torch.multiprocessing as mp
+    c = steady_case()
+    s = rhodst_b200.solver_for(c)
+    r0 = None
+    for _ in range(12):
+        reps = s.step(50)
+        r0 = reps[0]["res_l2"][0] if r0 is None else r0
+        if reps[-1]["res_l2"][0] < 1e-12 * r0:
+            break
+    W = s.conservative()
+    s.close()
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "rank")
+        mp.start_processes(_rank, args=(2, port, out), nprocs=2, start_method="spawn", join=True)
+        got = [np.load(f"{out}_{r}.npz") for r in range(2)]
+    for g in got:
+        assert g["hist"][-1] < 1e-10 * g["hist"][0], g["hist"]
+    for k, name in enumerate(("rho", "rhoU", "rhoE")):
+        for g in got:
+            assert np.abs(g[name] - W[k][g["ids"]]).max() <= 1e-8 * np.abs(W[k]).max(), name
