@@ -76,7 +76,9 @@ def _rank(rank, world, port, out):
     from tests.oracle_lib import OracleSolver as OS
     from tests.oracle_lib import set_threads
     set_threads(2)
-    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    import datetime
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=300))
     try:
         d = DecomposedSolver(steady_case(), make_solver=OS)
         hist = [d.residual_l2()[0]]

@@ -53,7 +53,9 @@ def _rank(rank, world, port, out):
     import torch.distributed as dist
     from rhodst_b200.distributed import DecomposedSolver
     from tests.test_decompose import steady_case as sc
-    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    import datetime
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=300))
     try:
         d = DecomposedSolver(sc())
         hist = [d.residual_l2()[0]]
