@@ -272,6 +272,13 @@ void rdst_destroy(rdst_ctx* ctx);
  * NULL clears the mask. */
 rdst_status rdst_set_held_cells(rdst_ctx* ctx, const uint8_t* mask);
 
+/* Replace nuTilda between steps (n_cells values, original numbering): its
+ * boundary values and mu_t follow; the mean flow and the time-control
+ * history are kept (the turbulence counterpart of rdst_set_conservative
+ * after a first state, used for the halo cells of a decomposed run).
+ * Held cells keep their nuTilda in the segregated nuTilda solve too. */
+rdst_status rdst_set_nu_tilda(rdst_ctx* ctx, const double* nut);
+
 /* Host-only helper (no GPU needed): recursive coordinate bisection of the
  * cell centres into n_parts parts, out_part[n_cells].  The GPU library uses
  * the same partition for its subdomain ILU(0) (block-Jacobi across parts,

@@ -2110,7 +2110,8 @@ void sa_correct(Ctx& c) {
     for (int it = 0; it < c.o.nut_sweeps; ++it) {
         for (int i = 0; i < N; ++i) xn[i] = b[i];
         for (int f = 0; f < c.Fi; ++f) { xn[c.own[f]] -= up[f] * x[c.nei[f]]; xn[c.nei[f]] -= lo[f] * x[c.own[f]]; }
-        for (int i = 0; i < N; ++i) x[i] = xn[i] / diag[i];
+        for (int i = 0; i < N; ++i)
+            if (c.rmask.empty() || !c.rmask[i]) x[i] = xn[i] / diag[i];   // held cells keep their nuTilda
     }
     c.nut = x;
     if (!neg_sa) for (auto& v : c.nut) v = std::max(v, 0.0);
@@ -2416,6 +2417,21 @@ ORACLE_API rdst_status rdsto_set_primitive(rdst_ctx* ctx, const double* p, const
         }
         update_mut(c, fv1);
     }
+    return RDST_OK;
+}
+
+ORACLE_API rdst_status rdsto_set_nu_tilda(rdst_ctx* ctx, const double* nut) {
+    if (!ctx || !nut) return RDST_ERR_ARG;
+    Ctx& c = ctx->c;
+    if (c.o.turbulence == TURB_LAMINAR || !c.state_set) return RDST_ERR_ARG;
+    for (int i = 0; i < c.N; ++i) c.nut[i] = nut[i];
+    eval_nut_boundary(c);
+    std::vector<double> fv1(c.N);
+    for (int i = 0; i < c.N; ++i) {
+        double chi = c.rho[i] * c.nut[i] / mu_of_T(c, c.T[i]);
+        fv1[i] = chi * chi * chi / (chi * chi * chi + std::pow(7.1, 3));
+    }
+    update_mut(c, fv1);
     return RDST_OK;
 }
 

@@ -116,6 +116,7 @@ def declare(lib: ctypes.CDLL, prefix: str) -> None:
     f("set_primitive", c_int32, [vp, dp, dp, dp, dp])
     f("set_conservative", c_int32, [vp, dp, dp, dp])
     f("set_held_cells", c_int32, [vp, POINTER(ctypes.c_uint8)])
+    f("set_nu_tilda", c_int32, [vp, dp])
     f("get_conservative", c_int32, [vp, dp, dp, dp])
     f("get_primitive", c_int32, [vp, dp, dp, dp, dp])
     f("step", c_int32, [vp, c_int32, POINTER(RdstStepReport)])
@@ -272,6 +273,14 @@ class Solver:
             raise ValueError("mask needs one entry per cell")
         self._check(self._fn("set_held_cells")(self._h, mk.ctypes.data_as(POINTER(ctypes.c_uint8))),
                     "set_held_cells")
+
+    def set_nu_tilda(self, nut):
+        """Replace nuTilda between steps (mu_t follows; mean flow and time
+        control kept)."""
+        nt = np.ascontiguousarray(nut, dtype=np.float64)
+        if nt.shape != (self.n_cells,):
+            raise ValueError("nuTilda needs one value per cell")
+        self._check(self._fn("set_nu_tilda")(self._h, _dptr(nt)), "set_nu_tilda")
 
     def set_conservative(self, rho, rhoU, rhoE):
         N = self.n_cells

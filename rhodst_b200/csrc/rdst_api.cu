@@ -2145,6 +2145,25 @@ RDST_API rdst_status rdst_set_primitive(rdst_ctx* c, const double* p, const doub
     });
 }
 
+RDST_API rdst_status rdst_set_nu_tilda(rdst_ctx* c, const double* nut) {
+    if (!c || !nut) return RDST_ERR_ARG;
+    if (!c->turb || !c->state_set) { c->err = "set_nu_tilda needs a turbulence model and a state"; return RDST_ERR_ARG; }
+    return guarded(c, [&] {
+        // nuTilda replaced between steps: boundary values and mu_t from it,
+        // with the mean flow and the time-control history kept
+        std::vector<double> nv(c->N);
+        for (int r = 0; r < c->N; ++r) nv[r] = nut[c->perm[r]];
+        CK(cudaMemcpyAsync(c->nut.p, nv.data(), nv.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
+        const DevMesh& m = c->m;
+        if (m.NB > 0) { k_sa_bc<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->bs.p, c->sa); CKL(); }
+        k_sa_init_mut<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->tr, c->W.p, c->prim.p, c->sa); CKL();
+        k_sa_finish<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->o.turbulence == TURB_SANEG, c->W.p, c->nut.p, c->sa);
+        CKL();
+        if (m.NB > 0) { k_sa_mutb<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->tr, c->bs.p, c->sa); CKL(); }
+        CK(cudaStreamSynchronize(c->s));
+    });
+}
+
 RDST_API rdst_status rdst_set_held_cells(rdst_ctx* c, const uint8_t* mask) {
     if (!c) return RDST_ERR_ARG;
     return guarded(c, [&] {

@@ -322,6 +322,7 @@ __global__ void k_sa_assemble(DevMesh m, double alpha, SAFields F) {
 __global__ void k_sa_jacobi(DevMesh m, SAFields F, const double* __restrict__ xin, double* __restrict__ xout) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.N) return;
+    if (m.rmask && m.rmask[i]) { xout[i] = xin[i]; return; }      // held cell keeps its nuTilda
     double s = F.b[i];
     for (int k = m.cf_start[i]; k < m.cf_start[i + 1]; ++k) {
         int code = m.cf_list[k];

@@ -4,7 +4,9 @@ layers, `decompose.py`) with its own context, and after every step the
 ranks exchange the states of the halo cells with the owners (point-to-point
 through torch.distributed: NCCL between GPUs, gloo on the CPU).
 
-Within a step the subdomains are independent (their halos are held at the
+With a Spalart-Allmaras model nuTilda travels with the mean flow and the
+halo cells keep it in the segregated nuTilda solve as well.  Within a step
+the subdomains are independent (their halos are held at the
 values of the last exchange: an overlapping Schwarz iteration in
 pseudo-time with Dirichlet data on the halo), so the converged state is
 the single-mesh steady state, R = 0 on every owned cell: the owned cells'
@@ -35,8 +37,7 @@ class DecomposedSolver:
         self.group = group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
-        if case.options.get("RASModel", "laminar") != "laminar":
-            raise ValueError("the decomposed solver exchanges the mean flow only (no turbulence model)")
+        self.turb = case.options.get("RASModel", "laminar") != "laminar"
         td = case.options.get("ddtSchemes", {}).get("default", "Euler")
         if td != "steadyStateDST":
             raise ValueError("the decomposed solver iterates steady states (ddt steadyStateDST)")
@@ -44,12 +45,14 @@ class DecomposedSolver:
         self.sub = subs[self.rank]
         bcs = dict(case.bcs)
         bcs[_dec.HALO_PATCH] = {"p": "zeroGradient", "U": "zeroGradient", "T": "zeroGradient"}
+        if self.turb:
+            bcs[_dec.HALO_PATCH]["nuTilda"] = "zeroGradient"
         if make_solver is None:
             from . import Solver
             make_solver = Solver
         self.solver = make_solver(self.sub.mesh, bcs, case.options)
         c = self.sub.cells
-        self.solver.set_primitive(case.p[c], case.U[c], case.T[c])
+        self.solver.set_primitive(case.p[c], case.U[c], case.T[c], case.nuTilda[c] if self.turb else None)
         # halo cells are held in the steps (zero residual, identity rows):
         # each step solves the owned cells with the halo as Dirichlet data,
         # and the residual norms and the CFL ramp see the owned cells only
@@ -59,13 +62,18 @@ class DecomposedSolver:
 
     # -- halo exchange ------------------------------------------------------
     def exchange(self):
-        """Owned states -> the peers' halo cells (rho, rhoU, rhoE per cell)."""
+        """Owned states -> the peers' halo cells (rho, rhoU, rhoE, and
+        nuTilda with a turbulence model, per cell)."""
         import torch
         rho, rhoU, rhoE = self.solver.conservative()
-        W = np.concatenate([rho[:, None], rhoU, rhoE[:, None]], axis=1)
+        cols = [rho[:, None], rhoU, rhoE[:, None]]
+        if self.turb:
+            cols.append(self.solver.primitive()[3][:, None])
+        W = np.concatenate(cols, axis=1)
+        nc = W.shape[1]
         reqs, inbox = [], {}
         for q in sorted(self.sub.recv):
-            buf = torch.empty((self.sub.recv[q].size, 5), dtype=torch.float64, device=self._device)
+            buf = torch.empty((self.sub.recv[q].size, nc), dtype=torch.float64, device=self._device)
             inbox[q] = buf
             reqs.append(self.dist.irecv(buf, src=q, group=self.group))
         for q in sorted(self.sub.send):
@@ -76,6 +84,8 @@ class DecomposedSolver:
         for q, buf in inbox.items():
             W[self.sub.recv[q]] = buf.cpu().numpy()
         self.solver.set_conservative(W[:, 0].copy(), np.ascontiguousarray(W[:, 1:4]), W[:, 4].copy())
+        if self.turb:
+            self.solver.set_nu_tilda(W[:, 5].copy())
 
     def step(self, n: int = 1):
         """n steps, each followed by the halo exchange; this rank's reports."""

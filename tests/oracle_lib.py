@@ -36,6 +36,8 @@ def load_oracle() -> ctypes.CDLL:
         lib.rdsto_limiter.argtypes = [ctypes.c_int32, ctypes.c_double]
         lib.rdsto_set_partition.restype = ctypes.c_int32
         lib.rdsto_set_partition.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
+        lib.rdsto_set_nu_tilda.restype = ctypes.c_int32
+        lib.rdsto_set_nu_tilda.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         lib.rdsto_set_held_cells.restype = ctypes.c_int32
         lib.rdsto_set_held_cells.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint8)]
         lib.rdsto_grad_U.restype = ctypes.c_int32

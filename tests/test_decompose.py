@@ -122,3 +122,39 @@ def test_two_ranks_reach_the_single_mesh_steady_state():
         ref = W[k]
         for g in got:
             assert np.abs(g[name] - ref[g["ids"]]).max() <= 1e-8 * np.abs(ref).max(), name
+
+
+def test_sa_steady_state_is_a_fixed_point_of_the_subdomain_steps():
+    """With the Spalart-Allmaras model the halo carries nuTilda too
+    (rdst_set_nu_tilda) and held cells keep it in the nuTilda solve: the
+    single-mesh steady state (W, nuTilda) loaded into the subdomains is left
+    where it is by a step (owned cells, to round-off)."""
+    c = cases.naca0012_turbulent(ni=65, nj=17, first_cell=1e-2, reynolds=1e5, flux="HLL",
+                                 limiter="upwind").with_options(**{"timeControls.maxCo": 500.0})
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T, c.nuTilda)
+    r0 = None
+    for _ in range(20):
+        reps = o.step(50)
+        r0 = reps[0]["res_l2"][0] if r0 is None else r0
+        if reps[-1]["res_l2"][0] < 1e-12 * r0:
+            break
+    assert reps[-1]["res_l2"][0] < 1e-10 * r0
+    W, prim = o.conservative(), o.primitive()
+    bcs = dict(c.bcs)
+    bcs[decompose.HALO_PATCH] = {"p": "zeroGradient", "U": "zeroGradient", "T": "zeroGradient",
+                                 "nuTilda": "zeroGradient"}
+    for s in decompose.decompose(c.mesh, 3):
+        cs, own = s.cells, s.owned
+        os_ = OracleSolver(s.mesh, bcs, c.options)
+        os_.set_primitive(prim[0][cs], prim[1][cs], prim[2][cs], prim[3][cs])
+        os_.set_held_cells(~own)
+        os_.set_conservative(W[0][cs], W[1][cs], W[2][cs])
+        os_.set_nu_tilda(prim[3][cs])
+        os_.step(1)
+        W2, p2 = os_.conservative(), os_.primitive()
+        for a, b in zip(W2, W):
+            assert np.abs(a[own] - b[cs][own]).max() <= 1e-12 * np.abs(b).max()
+        assert np.abs(p2[3][own] - prim[3][cs][own]).max() <= 1e-12 * np.abs(prim[3]).max()
+        # held cells keep their state and nuTilda
+        assert np.array_equal(p2[3][~own], prim[3][cs][~own])
