@@ -25,25 +25,43 @@ def rel(a, b):
     return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
 
 
-def test_held_cells_steps_parity():
-    c = steady_case().with_options(**{"ilu.parts": 2})
+def sa_case():
+    from rhodst_b200 import cases
+    return cases.naca0012_turbulent(ni=65, nj=17, first_cell=1e-2, reynolds=1e5, flux="HLL",
+                                    limiter="upwind").with_options(**{"timeControls.maxCo": 500.0})
+
+
+@pytest.mark.parametrize("turb", [False, True], ids=["inviscid", "SA"])
+def test_held_cells_steps_parity(turb):
+    c = (sa_case() if turb else steady_case()).with_options(**{"ilu.parts": 2})
     sub = decompose.decompose(c.mesh, 3)[1]
     bcs = dict(c.bcs)
     bcs[decompose.HALO_PATCH] = {"p": "zeroGradient", "U": "zeroGradient", "T": "zeroGradient"}
+    if turb:
+        bcs[decompose.HALO_PATCH]["nuTilda"] = "zeroGradient"
     part = rhodst_b200.partition_cells(sub.mesh.C, 2)
     gpu = rhodst_b200.Solver(sub.mesh, bcs, c.options)
     ora = OracleSolver(sub.mesh, bcs, c.options, partition=part)
+    cs = sub.cells
+    nut = c.nuTilda[cs] * (1.0 + 0.3 * np.sin(3.0 * c.mesh.C[cs, 0]) ** 2) if turb else None
     for s in (gpu, ora):
-        s.set_primitive(c.p[sub.cells], c.U[sub.cells], c.T[sub.cells])
+        s.set_primitive(c.p[cs], c.U[cs], c.T[cs], nut)
         s.set_held_cells(~sub.owned)
+        if turb:
+            s.set_nu_tilda(nut)
     W0 = gpu.conservative()
     rg, ro = gpu.step(5), ora.step(5)
+    tol = 1e-8 if turb else 1e-9
     for a, b in zip(rg, ro):
-        assert abs(a["res_mag"] - b["res_mag"]) <= 1e-9 * abs(b["res_mag"])
+        assert abs(a["res_mag"] - b["res_mag"]) <= tol * abs(b["res_mag"])
     Wg, Wo = gpu.conservative(), ora.conservative()
     for a, b, a0 in zip(Wg, Wo, W0):
-        assert rel(a, b) < 1e-9
+        assert rel(a, b) < tol
         assert np.array_equal(a[~sub.owned], a0[~sub.owned])          # held cells keep their state
+    if turb:
+        ng, no = gpu.primitive()[3], ora.primitive()[3]
+        assert rel(ng, no) < tol
+        assert np.array_equal(ng[~sub.owned], nut[~sub.owned])
     assert np.abs(gpu.residual()[~sub.owned]).max() == 0.0
 
 
