@@ -195,6 +195,7 @@ struct Ctx {
     std::vector<std::array<double, 6>> S_old;
     bool S_old_valid = false;
     bool state_set = false;           // a state has been set (later sets keep the time-control history)
+    std::vector<double> nutN, nutNm1;  // nuTilda old time levels of dual-time stepping
     std::vector<double> rho0;
     // dual-time stepping: W at the two previous time levels, foam Time's
     // deltaTSave (deltaT0 of the next step), the step's BDF2 coefficients
@@ -1993,6 +1994,13 @@ void sa_correct(Ctx& c) {
         // fvm::ddt(rho, nuTilda): diag rdt rho V, source rdt rho nuTilda_old V
         diag[i] = rdt * rho * V;
         b[i] = rdt * rho * nt * V;
+        if (c.dual_a != 0.0) {
+            // dual2ndDST::fvmDdt(rho, vf) (dual2ndDST.C:456-488): diag
+            // (rDeltaTau + a) rho V, source V (rDeltaTau rho nuTilda
+            // - b rho^n nuTilda^n - c rho^n-1 nuTilda^n-1)
+            diag[i] += c.dual_a * rho * V;
+            b[i] -= V * (c.dual_b * c.Wn[i][0] * c.nutN[i] + c.dual_c * c.Wnm1[i][0] * c.nutNm1[i]);
+        }
         // + Cb2/sigma rho |grad nuTilda|^2 (explicit, moved to the right)
         b[i] += K.Cb2 / K.sigmaNut * rho * magSqr(gn[i]) * V;
         if (neg_sa) {
@@ -2207,11 +2215,16 @@ void dual_iterate(Ctx& c, Report& rep, double dt, double dt0) {
         c.Wn.resize(c.N);
         for (int i = 0; i < c.N; ++i) c.Wn[i] = {c.rho[i], c.rhoU[i][0], c.rhoU[i][1], c.rhoU[i][2], c.rhoE[i]};
         c.Wnm1 = c.Wn;
+        c.nutN = c.nut;
+        c.nutNm1 = c.nut;
         c.dual_started = true;
     } else {
         c.Wnm1.swap(c.Wn);
         for (int i = 0; i < c.N; ++i) c.Wn[i] = {c.rho[i], c.rhoU[i][0], c.rhoU[i][1], c.rhoU[i][2], c.rhoE[i]};
+        c.nutNm1.swap(c.nutN);
+        c.nutN = c.nut;
     }
+    const bool turb = c.o.turbulence != TURB_LAMINAR;
     // dual2ndDST::fvmDdt coefficients (dual2ndDST.C:391-395)
     c.dual_a = 1.0 / dt + 1.0 / (dt + dt0);
     c.dual_c = dt / (dt0 * (dt + dt0));
@@ -2228,6 +2241,9 @@ void dual_iterate(Ctx& c, Report& rep, double dt, double dt0) {
         Vec dx;
         linear_solve(c, A, M, dx, rep);
         update_fields(c, dx);
+        // turbulence inside the loop when innerCorrectTurbulence
+        // (timeDST::correctTurbulence, timeDST.C:460-463; Dual.C:111-112)
+        if (turb && c.o.inner_correct_turbulence && !c.o.frozen_turbulence) sa_correct(c);
         rc.add(rep.lin_initial);
         // setCourantDST(&solverPerf): |initialResidual|, pseudo-time branch
         // while the steadyCheck (its last slope) is not converged
@@ -2236,6 +2252,8 @@ void dual_iterate(Ctx& c, Report& rep, double dt, double dt0) {
         courant_update(c, std::sqrt(ir2), !rc.converged_now());
         ++inner;
     } while (!rc.converged());
+    // and once after it otherwise (Dual.C:120-121)
+    if (turb && !c.o.inner_correct_turbulence && !c.o.frozen_turbulence) sa_correct(c);
     set_courant(c, rep);             // setCourantDST(): residual of R_, converged: physical time step
     rep.flags = c.bounded ? 1 : 0;
     rep.lin_iterations = inner;

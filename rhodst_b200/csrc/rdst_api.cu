@@ -287,8 +287,9 @@ struct rdst_ctx {
     // dual-time stepping: W at the previous two time levels, foam Time's
     // deltaTSave, the step's a of dual2ndDST (0 outside a dual step)
     DBuf<double> dWn, dWnm1;
+    DBuf<double> nutN, nutNm1;      // nuTilda old time levels of dual-time stepping
     bool dual_started = false;
-    double dt_save = 1.0, dual_a = 0.0;
+    double dt_save = 1.0, dual_a = 0.0, dual_b = 0.0, dual_c = 0.0;
     DBuf<Scalars> a_sc;             // Hessenberg and rotations of the adjoint's outer solve
     void* a_AT = nullptr;           // transposed Jacobian (storage type of A)
     DBuf<double> t_buf;             // tangent records (value, derivative)
@@ -1306,8 +1307,12 @@ void sa_correct(rdst_ctx& c) {
         k_limit_gradU<<<nblk(c.N, 128), 128, 0, s>>>(m, c.o.grad_U_limit, c.prim.p, c.bs.p, c.gU.p); CKL();
     }
     const int sarc1 = c.o.turbulence == TURB_SARC1 ? 1 : (c.o.turbulence == TURB_SA ? 2 : 0);
-    k_sa_cell<<<nblk(c.N, 128), 128, 0, s>>>(m, c.tr, neg_sa, sarc1, c.steady ? 1 : 0, c.W.p, c.prim.p, c.gU.p, c.rdt.p,
-                                            c.sc.p, c.fl.p, c.bs.p, F); CKL();
+    k_sa_cell<<<nblk(c.N, 128), 128, 0, s>>>(m, c.tr, neg_sa, sarc1, (c.steady || c.o.dual) ? 1 : 0, c.W.p, c.prim.p,
+                                            c.gU.p, c.rdt.p, c.sc.p, c.fl.p, c.bs.p, F); CKL();
+    if (c.o.dual && c.dual_a != 0.0) {
+        k_sa_dual<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.V.p, c.W.p, c.dWn.p, c.dWnm1.p, c.nutN.p, c.nutNm1.p,
+                                                 c.dual_a, c.dual_b, c.dual_c, F); CKL();
+    }
     if (sarc1 == 1) { k_sarc1_valid<<<1, 1, 0, s>>>(F.S_old_valid); CKL(); }
     if (m.Fi > 0) { k_sa_faces<<<nblk(m.Fi, TPB), TPB, 0, s>>>(m, c.fl.p, F, c.o.nut_linear_upwind ? 1 : 0); CKL(); }
     if (m.NB > 0) { k_sa_bfaces<<<nblk(m.NB, TPB), TPB, 0, s>>>(m, c.tr, neg_sa, c.bs.p, F); CKL(); }
@@ -1581,6 +1586,7 @@ void run_dual_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
     const Options& o = c.o;
     const long n5 = 5L * c.N;
     if (!c.dWn.p) { c.dWn.alloc(n5); c.dWnm1.alloc(n5); }
+    if (c.turb && !c.nutN.p) { c.nutN.alloc(c.N); c.nutNm1.alloc(c.N); }
     if (!c.step_ev[0]) { CK(cudaEventCreate(&c.step_ev[0])); CK(cudaEventCreate(&c.step_ev[1])); }
     std::vector<int> inner_counts;
     int done = 0;
@@ -1600,16 +1606,27 @@ void run_dual_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
             if (!c.dual_started) {
                 CK(cudaMemcpyAsync(c.dWn.p, c.W.p, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
                 CK(cudaMemcpyAsync(c.dWnm1.p, c.W.p, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                if (c.turb) {
+                    CK(cudaMemcpyAsync(c.nutN.p, c.nut.p, c.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                    CK(cudaMemcpyAsync(c.nutNm1.p, c.nut.p, c.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                }
                 c.dual_started = true;
             } else {
                 std::swap(c.dWn.p, c.dWnm1.p);
                 CK(cudaMemcpyAsync(c.dWn.p, c.W.p, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                if (c.turb) {
+                    std::swap(c.nutN.p, c.nutNm1.p);
+                    CK(cudaMemcpyAsync(c.nutN.p, c.nut.p, c.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                }
             }
             // dual2ndDST::fvmDdt coefficients (dual2ndDST.C:391-395)
             const double a = 1.0 / dt + 1.0 / (dt + dt0);
             const double cc = dt / (dt0 * (dt + dt0));
             const double b = -(a + cc);
             c.dual_a = a;
+            c.dual_b = b;
+            c.dual_c = cc;
+            const bool sa = c.turb && !o.frozen_turbulence;
             k_report_dt<<<1, 1, 0, s>>>(c.sc.p, c.reps.p, rdst_ctx::REP_CAP); CKL();
             k_time_advance<<<1, 1, 0, s>>>(c.sc.p); CKL();
             SteadyCheck rc(o);
@@ -1628,6 +1645,9 @@ void run_dual_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
                     k_update<<<nblk(c.N, TPB), TPB, 0, s>>>(c.N, c.th, c.bd, c.dx.p, c.W.p, c.prim.p, c.sc.p); CKL();
                 }
                 k_boundary<<<nblk(c.NB, TPB), TPB, 0, s>>>(c.m, c.th, c.bd, c.W.p, c.prim.p, c.bs.p); CKL();
+                // turbulence inside the loop when innerCorrectTurbulence
+                // (timeDST::correctTurbulence, timeDST.C:460-463; Dual.C:111-112)
+                if (sa && o.inner_correct_turbulence) sa_correct(c);
                 double ir[5];
                 CK(cudaMemcpyAsync(ir, c.sc.p->lin_initial, sizeof(ir), cudaMemcpyDeviceToHost, s));
                 CK(cudaStreamSynchronize(s));
@@ -1651,11 +1671,13 @@ void run_dual_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
                 }
                 ++inner;
             } while (!rc.converged());
+            // and once after it otherwise (Dual.C:120-121)
+            if (sa && !o.inner_correct_turbulence) sa_correct(c);
             // setCourantDST(): residual of R, the converged branch
             k_courant_scalar<<<1, 1, 0, s>>>(c.sc.p, o.adjust_time_step ? 1 : 0, o.min_co, o.max_co); CKL();
             if (o.adjust_time_step) set_transient_dt(c);
             k_report<<<1, 1, 0, s>>>(c.sc.p, c.reps.p, rdst_ctx::REP_CAP); CKL();
-            c.dual_a = 0.0;
+            c.dual_a = c.dual_b = c.dual_c = 0.0;
             inner_counts.push_back(inner);
         }
         CK(cudaEventRecord(c.step_ev[1], s));

@@ -389,12 +389,13 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
     if (!(o.R > 0) || !(o.Cp > o.R)) throw ConfigError("thermo: need 0 < R < Cp");
     if (o.lim_U == LIM_VENKATAKRISHNAN) {}
     // dual-time stepping: the Dual iteration with the dual2ndDST ddt (the
-    // pairing of the reference's dual-time tutorial); laminar and inviscid
-    // flows (the SA equation's own dual2ndDST ddt is not restated)
+    // pairing of the reference's dual-time tutorial), for the mean flow and
+    // the nuTilda equation of SAneg, SARC2 and SpalartAllmaras
     if (o.dual != (o.ddt == DDT_DUAL2ND))
         throw ConfigError("timeIntegration Dual is restated with ddtSchemes dual2ndDST (and dual2ndDST with Dual)", true);
-    if (o.dual && o.turbulence != TURB_LAMINAR)
-        throw ConfigError("dual-time stepping with a turbulence model is not on this path", true);
+    if (o.dual && o.turbulence == TURB_SARC1)
+        throw ConfigError("dual-time stepping with SARC1 (the dual-time ddt of its strain-rate transport) "
+                          "is not on this path", true);
     if (o.iteration_start < 0) o.iteration_start = (o.ddt == DDT_STEADY) ? 500 : 10;
     if (o.max_inner_iter < 0) throw ConfigError("timeIntegration.maxInnerIter must be >= 0");
     return o;

@@ -318,6 +318,20 @@ __global__ void k_sa_assemble(DevMesh m, double alpha, SAFields F) {
     F.diag[i] = Dn;
 }
 
+// dual2ndDST::fvmDdt(rho, nuTilda) (dual2ndDST.C:456-488) on top of the
+// pseudo-time part rDeltaTau rho V of k_sa_cell: diag += a rho V, source
+// -= V (b rho^n nuTilda^n + c rho^n-1 nuTilda^n-1)
+__global__ void k_sa_dual(int N, const double* __restrict__ V, const double* __restrict__ W,
+                          const double* __restrict__ Wn, const double* __restrict__ Wnm1,
+                          const double* __restrict__ nutN, const double* __restrict__ nutNm1, double a, double b,
+                          double c, SAFields F) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double Vi = V[i];
+    F.diag[i] += a * W[5L * i] * Vi;
+    F.b[i] -= Vi * (b * Wn[5L * i] * nutN[i] + c * Wnm1[5L * i] * nutNm1[i]);
+}
+
 // one point-Jacobi sweep x_out = (b - offdiag x_in) / D
 __global__ void k_sa_jacobi(DevMesh m, SAFields F, const double* __restrict__ xin, double* __restrict__ xout) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;

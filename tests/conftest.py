@@ -28,7 +28,7 @@ def _gpu_available() -> bool:
 # selectable-solver rows and the frozen-turbulence gradient), so that those
 # suites report first; the allocation-free module stays last.
 _LATE = ("test_gpu_block_solvers.py", "test_gpu_adjoint_frozen_sa.py", "test_gpu_tutorial_schemes.py",
-         "test_gpu_adjoint_c5.py", "test_gpu_decompose.py")
+         "test_gpu_adjoint_c5.py", "test_gpu_decompose.py", "test_gpu_dual_sa.py")
 
 
 def _order(item):

@@ -85,8 +85,8 @@ def test_flatten_options():
     assert f == {"a.b": "true", "a.c": "1.0 2", "d": "0.001"}
 
 
-def test_dual_time_with_turbulence_is_rejected_before_device_work():
-    case = cases.naca0012_turbulent(ni=97, nj=25, first_cell=5e-3).with_options(**{
+def test_dual_time_with_sarc1_is_rejected_before_device_work():
+    case = cases.naca0012_turbulent(ni=97, nj=25, first_cell=5e-3, model="SARC1").with_options(**{
         "timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST"})
     with pytest.raises(_abi.RdstError) as e:
         rhodst_b200.Solver(case.mesh, case.bcs, case.options)

@@ -12,7 +12,10 @@ steadyCheck.C:69-98).
 (3) The physical time step comes from initialCo at initialisation
     (timeDST::initialize calls setTransientDeltaT unconditionally) and stays
     with adjustTimeStep false.
-(4) Dual needs dual2ndDST and the reverse; turbulence models are rejected.
+(4) Dual needs dual2ndDST and the reverse; SARC1 is rejected.
+(5) With Spalart-Allmaras the nuTilda equation takes its own dual2ndDST ddt:
+    a steady state is a fixed point of dual steps (either placement of the
+    turbulence update), a disturbed nuTilda moves.
 """
 import numpy as np
 import pytest
@@ -102,11 +105,65 @@ def test_dual_needs_dual2nd(opts):
         OracleSolver(c.mesh, c.bcs, c.options)
 
 
-def test_dual_with_turbulence_is_rejected():
-    c = cases.naca0012_turbulent(ni=97, nj=25, first_cell=5e-3).with_options(**{
+def test_dual_with_sarc1_is_rejected():
+    c = cases.naca0012_turbulent(ni=97, nj=25, first_cell=5e-3, model="SARC1").with_options(**{
         "timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST"})
     with pytest.raises(RdstError):
         OracleSolver(c.mesh, c.bcs, c.options)
+
+
+def sa_steady():
+    """A converged first-order SA airfoil state (p, U, T, nuTilda)."""
+    c = cases.naca0012_turbulent(ni=65, nj=17, first_cell=1e-2, reynolds=1e5, flux="HLL",
+                                 limiter="upwind").with_options(**{"timeControls.maxCo": 500.0})
+    o = OracleSolver(c.mesh, c.bcs, c.options)
+    o.set_primitive(c.p, c.U, c.T, c.nuTilda)
+    r0 = None
+    for _ in range(20):
+        reps = o.step(50)
+        r0 = reps[0]["res_l2"][0] if r0 is None else r0
+        if reps[-1]["res_l2"][0] < 1e-12 * r0:
+            break
+    assert reps[-1]["res_l2"][0] < 1e-10 * r0
+    return c, o.primitive()
+
+
+@pytest.mark.parametrize("inner", [False, True])
+def test_dual_sa_keeps_a_steady_state(inner):
+    """The SA equation with its own dual2ndDST ddt (dual2ndDST.C:456-488,
+    turbulence corrected inside the inner loop with innerCorrectTurbulence,
+    once after it otherwise): a steady state (W, nuTilda) is a fixed point
+    of dual-time steps, since its BDF2 terms vanish and its residuals are
+    zero."""
+    c, prim = sa_steady()
+    d = c.with_options(**{"timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST",
+                          "timeControls.adjustTimeStep": False, "controlDict.deltaT": 0.05,
+                          "timeIntegration.innerCorrectTurbulence": inner, "timeControls.maxCo": 50.0})
+    o = OracleSolver(d.mesh, d.bcs, d.options)
+    o.set_primitive(*prim)
+    reps = o.step(2)
+    p2 = o.primitive()
+    for a, b in zip(p2, prim):
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+    assert all(r["lin_iterations"] >= 1 for r in reps)
+
+
+@pytest.mark.parametrize("inner", [False, True])
+def test_dual_sa_moves_nu_tilda_in_time(inner):
+    """From a disturbed nuTilda the dual steps change nuTilda, finite, and
+    the two placements of the turbulence update give different paths."""
+    c, prim = sa_steady()
+    d = c.with_options(**{"timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST",
+                          "timeControls.adjustTimeStep": False, "controlDict.deltaT": 0.05,
+                          "timeIntegration.innerCorrectTurbulence": inner, "timeControls.maxCo": 50.0,
+                          "timeIntegration.maxInnerIter": 10})
+    nut = prim[3] * (1.0 + 0.5 * np.sin(2.0 * c.mesh.C[:, 0]) ** 2)
+    o = OracleSolver(d.mesh, d.bcs, d.options)
+    o.set_primitive(prim[0], prim[1], prim[2], nut)
+    o.step(2)
+    n2 = o.primitive()[3]
+    assert np.all(np.isfinite(n2))
+    assert np.abs(n2 - nut).max() > 1e-6 * np.abs(nut).max()
 
 
 def test_adapter_selector_name_selects_dual_time():
