@@ -279,6 +279,14 @@ rdst_status rdst_set_held_cells(rdst_ctx* ctx, const uint8_t* mask);
  * Held cells keep their nuTilda in the segregated nuTilda solve too. */
 rdst_status rdst_set_nu_tilda(rdst_ctx* ctx, const double* nut);
 
+/* The states of n listed cells (original numbering): six values per cell,
+ * rho, rhoU (3), rhoE, nuTilda (0 without a turbulence model).  get reads
+ * them; set writes them between steps with rdst_set_conservative's
+ * semantics (boundary values and mu_t follow, time-control history kept),
+ * so a decomposed run moves only its halo cells. */
+rdst_status rdst_get_cells(rdst_ctx* ctx, int32_t n, const int32_t* cells, double* out);
+rdst_status rdst_set_cells(rdst_ctx* ctx, int32_t n, const int32_t* cells, const double* in);
+
 /* Host-only helper (no GPU needed): recursive coordinate bisection of the
  * cell centres into n_parts parts, out_part[n_cells].  The GPU library uses
  * the same partition for its subdomain ILU(0) (block-Jacobi across parts,

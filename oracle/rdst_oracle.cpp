@@ -2453,6 +2453,57 @@ ORACLE_API rdst_status rdsto_set_nu_tilda(rdst_ctx* ctx, const double* nut) {
     return RDST_OK;
 }
 
+ORACLE_API rdst_status rdsto_get_cells(rdst_ctx* ctx, int32_t n, const int32_t* cells, double* out) {
+    if (!ctx || n < 0 || (n > 0 && (!cells || !out))) return RDST_ERR_ARG;
+    Ctx& c = ctx->c;
+    for (int j = 0; j < n; ++j) {
+        const int i = cells[j];
+        if (i < 0 || i >= c.N) return RDST_ERR_ARG;
+        double* o = out + 6L * j;
+        o[0] = c.rho[i]; o[1] = c.rhoU[i][0]; o[2] = c.rhoU[i][1]; o[3] = c.rhoU[i][2]; o[4] = c.rhoE[i];
+        o[5] = c.o.turbulence != TURB_LAMINAR ? c.nut[i] : 0.0;
+    }
+    return RDST_OK;
+}
+
+// the listed cells' states between steps, as set_conservative after a first
+// state (boundary values from the new internal field, time control kept)
+// with mu_t from nuTilda
+ORACLE_API rdst_status rdsto_set_cells(rdst_ctx* ctx, int32_t n, const int32_t* cells, const double* in) {
+    if (!ctx || n < 0 || (n > 0 && (!cells || !in))) return RDST_ERR_ARG;
+    Ctx& c = ctx->c;
+    if (!c.state_set) return RDST_ERR_ARG;
+    const bool turb = c.o.turbulence != TURB_LAMINAR;
+    for (int j = 0; j < n; ++j) {
+        const int i = cells[j];
+        if (i < 0 || i >= c.N) return RDST_ERR_ARG;
+        const double* v = in + 6L * j;
+        c.rho[i] = v[0];
+        c.rhoU[i] = {v[1], v[2], v[3]};
+        c.rhoE[i] = v[4];
+        c.U[i] = c.rhoU[i] / c.rho[i];
+        double e = c.rhoE[i] / c.rho[i] - 0.5 * magSqr(c.U[i]);
+        c.T[i] = e / c.Cv;
+        c.p[i] = c.rho[i] * c.R * c.T[i];
+        c.h[i] = c.Cp * c.T[i];
+        if (turb) c.nut[i] = v[5];
+    }
+    c.S_old_valid = false;
+    c.dual_started = false;
+    c.dt_save = c.o.delta_t;
+    eval_boundary(c);
+    if (turb) {
+        eval_nut_boundary(c);
+        std::vector<double> fv1(c.N);
+        for (int i = 0; i < c.N; ++i) {
+            double chi = c.rho[i] * c.nut[i] / mu_of_T(c, c.T[i]);
+            fv1[i] = chi * chi * chi / (chi * chi * chi + std::pow(7.1, 3));
+        }
+        update_mut(c, fv1);
+    }
+    return RDST_OK;
+}
+
 ORACLE_API rdst_status rdsto_set_held_cells(rdst_ctx* ctx, const uint8_t* mask) {
     if (!ctx) return RDST_ERR_ARG;
     Ctx& c = ctx->c;

@@ -117,6 +117,8 @@ def declare(lib: ctypes.CDLL, prefix: str) -> None:
     f("set_conservative", c_int32, [vp, dp, dp, dp])
     f("set_held_cells", c_int32, [vp, POINTER(ctypes.c_uint8)])
     f("set_nu_tilda", c_int32, [vp, dp])
+    f("get_cells", c_int32, [vp, c_int32, POINTER(c_int32), dp])
+    f("set_cells", c_int32, [vp, c_int32, POINTER(c_int32), dp])
     f("get_conservative", c_int32, [vp, dp, dp, dp])
     f("get_primitive", c_int32, [vp, dp, dp, dp, dp])
     f("step", c_int32, [vp, c_int32, POINTER(RdstStepReport)])
@@ -273,6 +275,21 @@ class Solver:
             raise ValueError("mask needs one entry per cell")
         self._check(self._fn("set_held_cells")(self._h, mk.ctypes.data_as(POINTER(ctypes.c_uint8))),
                     "set_held_cells")
+
+    def get_cells(self, cells):
+        """States of the listed cells: n x 6 (rho, rhoU, rhoE, nuTilda)."""
+        ids = np.ascontiguousarray(cells, dtype=np.int32)
+        out = np.empty((ids.size, 6))
+        self._check(self._fn("get_cells")(self._h, ids.size, ids.ctypes.data_as(POINTER(c_int32)), _dptr(out)),
+                    "get_cells")
+        return out
+
+    def set_cells(self, cells, values):
+        """Write n x 6 states into the listed cells between steps."""
+        ids = np.ascontiguousarray(cells, dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(ids.size, 6)
+        self._check(self._fn("set_cells")(self._h, ids.size, ids.ctypes.data_as(POINTER(c_int32)), _dptr(v)),
+                    "set_cells")
 
     def set_nu_tilda(self, nut):
         """Replace nuTilda between steps (mu_t follows; mean flow and time

@@ -123,6 +123,38 @@ __global__ void k_set_conservative(int N, Thermo th, const int* __restrict__ per
     P[3] = Ux; P[4] = Uy; P[5] = Uz;
 }
 
+// the states of a list of cells (internal rows): rho, rhoU, rhoE, nuTilda
+// (0 without a turbulence model), six values per cell
+__global__ void k_get_cells(int n, const int* __restrict__ rows, const double* __restrict__ W,
+                            const double* __restrict__ nut, double* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int r = rows[j];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[6L * j + k] = W[5L * r + k];
+    out[6L * j + 5] = nut ? nut[r] : 0.0;
+}
+
+// the same six values into a list of cells; W and the primitive record as
+// k_set_conservative makes them (same operations, so the same bits)
+__global__ void k_set_cells(int n, Thermo th, const int* __restrict__ rows, const double* __restrict__ in,
+                            double* __restrict__ W, double* __restrict__ prim, double* __restrict__ nut) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int r = rows[j];
+    const double* v = in + 6L * j;
+    const double rh = v[0], mx = v[1], my = v[2], mz = v[3], E = v[4];
+    W[5 * r] = rh; W[5 * r + 1] = mx; W[5 * r + 2] = my; W[5 * r + 3] = mz; W[5 * r + 4] = E;
+    const double Ux = __ddiv_rn(mx, rh), Uy = __ddiv_rn(my, rh), Uz = __ddiv_rn(mz, rh);
+    const double k2 = __dadd_rn(__dadd_rn(__dmul_rn(Ux, Ux), __dmul_rn(Uy, Uy)), __dmul_rn(Uz, Uz));
+    const double e = __dsub_rn(__ddiv_rn(E, rh), __dmul_rn(0.5, k2));
+    const double T = __ddiv_rn(e, th.Cv);
+    double* P = prim + PW * r;
+    P[0] = __dmul_rn(__dmul_rn(rh, th.R), T); P[1] = T; P[2] = __dmul_rn(th.Cp, T);
+    P[3] = Ux; P[4] = Uy; P[5] = Uz;
+    if (nut) nut[r] = v[5];
+}
+
 // W (internal order) -> rho, rhoU, rhoE in the caller's cell order
 __global__ void k_get_conservative(int N, const int* __restrict__ perm, const double* __restrict__ W,
                                    double* __restrict__ rho, double* __restrict__ rhoU, double* __restrict__ rhoE) {

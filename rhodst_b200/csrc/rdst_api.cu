@@ -2186,6 +2186,65 @@ RDST_API rdst_status rdst_set_nu_tilda(rdst_ctx* c, const double* nut) {
     });
 }
 
+// cell ids (original numbering) -> internal rows on the device
+static void upload_rows(rdst_ctx& c, int32_t n, const int32_t* cells, DBuf<int>& rows) {
+    std::vector<int> r(n);
+    for (int j = 0; j < n; ++j) {
+        if (cells[j] < 0 || cells[j] >= c.N) throw std::invalid_argument("cell id out of range");
+        r[j] = c.iperm[cells[j]];
+    }
+    rows.upload(r, c.s);
+}
+
+RDST_API rdst_status rdst_get_cells(rdst_ctx* c, int32_t n, const int32_t* cells, double* out) {
+    if (!c || n < 0 || (n > 0 && (!cells || !out))) return RDST_ERR_ARG;
+    if (n == 0) return RDST_OK;
+    return guarded(c, [&] {
+        DBuf<int> rows;
+        DBuf<double> buf;
+        upload_rows(*c, n, cells, rows);
+        buf.alloc(6L * n);
+        k_get_cells<<<nblk(n, TPB), TPB, 0, c->s>>>(n, rows.p, c->W.p, c->turb ? c->nut.p : nullptr, buf.p);
+        CKL();
+        CK(cudaMemcpyAsync(out, buf.p, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, c->s));
+        CK(cudaStreamSynchronize(c->s));
+    });
+}
+
+RDST_API rdst_status rdst_set_cells(rdst_ctx* c, int32_t n, const int32_t* cells, const double* in) {
+    if (!c || n < 0 || (n > 0 && (!cells || !in))) return RDST_ERR_ARG;
+    if (!c->state_set) { c->err = "set_cells needs a state"; return RDST_ERR_ARG; }
+    return guarded(c, [&] {
+        DBuf<int> rows;
+        DBuf<double> buf;
+        if (n > 0) {
+            upload_rows(*c, n, cells, rows);
+            std::vector<double> v(in, in + 6L * n);
+            buf.upload(v, c->s);
+            k_set_cells<<<nblk(n, TPB), TPB, 0, c->s>>>(n, c->th, rows.p, buf.p, c->W.p, c->prim.p,
+                                                        c->turb ? c->nut.p : nullptr);
+            CKL();
+        }
+        // as rdst_set_conservative between steps: boundary values from the
+        // new internal field, time-control history kept; and mu_t from nuTilda
+        if (c->saSoldValid.p) CK(cudaMemsetAsync(c->saSoldValid.p, 0, sizeof(int), c->s));
+        c->dual_started = false;
+        c->dt_save = c->o.delta_t;
+        const DevMesh& m = c->m;
+        k_boundary<<<nblk(c->NB, TPB), TPB, 0, c->s>>>(m, c->th, c->bd, c->W.p, c->prim.p, c->bs.p);
+        CKL();
+        if (c->turb) {
+            if (m.NB > 0) { k_sa_bc<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->bs.p, c->sa); CKL(); }
+            k_sa_init_mut<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->tr, c->W.p, c->prim.p, c->sa); CKL();
+            k_sa_finish<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->o.turbulence == TURB_SANEG, c->W.p, c->nut.p,
+                                                           c->sa);
+            CKL();
+            if (m.NB > 0) { k_sa_mutb<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->tr, c->bs.p, c->sa); CKL(); }
+        }
+        CK(cudaStreamSynchronize(c->s));
+    });
+}
+
 RDST_API rdst_status rdst_set_held_cells(rdst_ctx* c, const uint8_t* mask) {
     if (!c) return RDST_ERR_ARG;
     return guarded(c, [&] {

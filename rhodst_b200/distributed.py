@@ -62,30 +62,24 @@ class DecomposedSolver:
 
     # -- halo exchange ------------------------------------------------------
     def exchange(self):
-        """Owned states -> the peers' halo cells (rho, rhoU, rhoE, and
-        nuTilda with a turbulence model, per cell)."""
+        """Owned states -> the peers' halo cells: six values per cell (rho,
+        rhoU, rhoE, nuTilda), read and written for the send and halo cells
+        only (rdst_get_cells / rdst_set_cells)."""
         import torch
-        rho, rhoU, rhoE = self.solver.conservative()
-        cols = [rho[:, None], rhoU, rhoE[:, None]]
-        if self.turb:
-            cols.append(self.solver.primitive()[3][:, None])
-        W = np.concatenate(cols, axis=1)
-        nc = W.shape[1]
         reqs, inbox = [], {}
         for q in sorted(self.sub.recv):
-            buf = torch.empty((self.sub.recv[q].size, nc), dtype=torch.float64, device=self._device)
+            buf = torch.empty((self.sub.recv[q].size, 6), dtype=torch.float64, device=self._device)
             inbox[q] = buf
             reqs.append(self.dist.irecv(buf, src=q, group=self.group))
         for q in sorted(self.sub.send):
-            t = torch.from_numpy(np.ascontiguousarray(W[self.sub.send[q]])).to(self._device)
+            t = torch.from_numpy(self.solver.get_cells(self.sub.send[q])).to(self._device)
             reqs.append(self.dist.isend(t, dst=q, group=self.group))
         for r in reqs:
             r.wait()
-        for q, buf in inbox.items():
-            W[self.sub.recv[q]] = buf.cpu().numpy()
-        self.solver.set_conservative(W[:, 0].copy(), np.ascontiguousarray(W[:, 1:4]), W[:, 4].copy())
-        if self.turb:
-            self.solver.set_nu_tilda(W[:, 5].copy())
+        if inbox:
+            ids = np.concatenate([self.sub.recv[q] for q in sorted(inbox)])
+            vals = np.concatenate([inbox[q].cpu().numpy() for q in sorted(inbox)])
+            self.solver.set_cells(ids, vals)
 
     def step(self, n: int = 1):
         """n steps, each followed by the halo exchange; this rank's reports."""

@@ -158,3 +158,44 @@ def test_sa_steady_state_is_a_fixed_point_of_the_subdomain_steps():
         assert np.abs(p2[3][own] - prim[3][cs][own]).max() <= 1e-12 * np.abs(prim[3]).max()
         # held cells keep their state and nuTilda
         assert np.array_equal(p2[3][~own], prim[3][cs][~own])
+
+
+@pytest.mark.parametrize("turb", [False, True])
+def test_set_cells_is_set_conservative_for_those_cells(turb):
+    """Writing a subset of cells with set_cells gives the state that
+    set_conservative of the whole field gives (the residual to round-off);
+    get_cells reads the six values back."""
+    c = (cases.naca0012_turbulent(ni=65, nj=17, first_cell=1e-2, reynolds=1e5) if turb
+         else cases.naca0012_inviscid(ni=65, nj=17, first_cell=1e-2))
+    N = c.mesh.n_cells
+    rng = np.random.default_rng(4)
+    nut0 = c.nuTilda if turb else None
+    a = OracleSolver(c.mesh, c.bcs, c.options)
+    b = OracleSolver(c.mesh, c.bcs, c.options)
+    for s in (a, b):
+        s.set_primitive(c.p, c.U, c.T, nut0)
+        s.step(2)
+    W = a.conservative()
+    ids = np.sort(rng.choice(N, size=N // 5, replace=False)).astype(np.int32)
+    vals = b.get_cells(ids)
+    assert np.array_equal(vals[:, 0], W[0][ids]) and np.array_equal(vals[:, 1:4], W[1][ids])
+    vals[:, 0] *= 1.01
+    vals[:, 4] *= 1.02
+    if turb:
+        vals[:, 5] *= 1.3
+    b.set_cells(ids, vals)
+    rho, rhoU, rhoE = (x.copy() for x in W)
+    rho[ids], rhoU[ids], rhoE[ids] = vals[:, 0], vals[:, 1:4], vals[:, 4]
+    a.set_conservative(rho, rhoU, rhoE)
+    if turb:
+        nut = a.primitive()[3].copy()
+        nut[ids] = vals[:, 5]
+        a.set_nu_tilda(nut)
+    for x, y in zip(a.conservative(), b.conservative()):
+        assert np.array_equal(x, y)
+    # set_conservative re-derives p and T of every cell from W (the last
+    # update derived them through the bounded h), set_cells only those it
+    # writes: the residuals agree to round-off
+    Ra, Rb = a.residual(), b.residual()
+    assert np.abs(Ra - Rb).max() <= 1e-12 * np.abs(Ra).max()
+    assert np.array_equal(a.primitive()[3], b.primitive()[3])
