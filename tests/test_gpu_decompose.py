@@ -127,7 +127,7 @@ def test_get_and_set_cells_match_the_oracle(turb):
         s.set_primitive(c.p, c.U, c.T, c.nuTilda if turb else None)
     ids = np.arange(0, N, 7, dtype=np.int32)
     vg, vo = gpu.get_cells(ids), ora.get_cells(ids)
-    assert np.array_equal(vg, vo)
+    assert rel(vg, vo) < 1e-14                     # the initial states, each side's own arithmetic
     vals = vo.copy()
     vals[:, 0] *= 1.02
     vals[:, 4] *= 1.03
