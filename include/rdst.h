@@ -133,7 +133,7 @@ typedef struct rdst_ctx rdst_ctx;
  * (solver/preconditioner names as foam-extend registers them for the 5x5
  * block matrix, Vector5typedefs.C:1602-1708).  Unknown selector values
  * return RDST_ERR_CONFIG; reference options this path rejects
- * (directWaveSpeed false, SAMG, dual time with a turbulence model)
+ * (directWaveSpeed false, SAMG, dual time with SARC1)
  * RDST_ERR_UNSUPPORTED.
  * Replaces createFields.H:115-152 (flux, Jacobian and iteration selection)
  * and timeDST::initialize (timeDST.C:67-208). */
