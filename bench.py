@@ -210,6 +210,7 @@ def run_ours(args, rank, world):
     case, desc = workload(args.workload)
     opts = dict(case.options)
     opts["profile"] = False          # timed steps run without per-kernel events
+    opts["device"] = dev             # the library's own CUDA runtime: name this rank's GPU
     s = rhodst_b200.Solver(case.mesh, case.bcs, opts)
     s.set_primitive(case.p, case.U, case.T)
     N, F = case.mesh.n_cells, case.mesh.n_internal_faces

@@ -214,7 +214,7 @@ struct rdst_ctx {
     Options o;
     std::string err;
     cudaStream_t s = nullptr;
-    int dev = 0;
+    int dev = -1;                   // the context's GPU (set at creation)
     // sizes
     int N = 0, Fi = 0, F = 0, NBall = 0, NB = 0, n_patches = 0;
     Thermo th{};
@@ -1706,6 +1706,9 @@ rdst_status guarded(rdst_ctx* c, F&& fn) {
     CounterScope cs(*c);
     try {
         c->err.clear();
+        // this library's CUDA runtime keeps its own current device: every
+        // call runs on the context's GPU, whatever the caller's runtime set
+        if (c->dev >= 0) CK(cudaSetDevice(c->dev));
         fn();
         return RDST_OK;
     } catch (const ConfigError& e) {
@@ -2098,6 +2101,10 @@ RDST_API rdst_status rdst_create(const rdst_mesh* mesh, int32_t n_options, const
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RDST_ERR_CUDA;
     rdst_status st = guarded(c.get(), [&] {
+        if (c->o.device >= 0) {
+            if (c->o.device >= ndev) throw ConfigError("option device: no such GPU");
+            CK(cudaSetDevice(c->o.device));
+        }
         CK(cudaGetDevice(&c->dev));
         CK(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
         build(*c, mesh);

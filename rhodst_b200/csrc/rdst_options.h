@@ -106,6 +106,7 @@ struct Options {
     int ilu_parts = 0;                // 0: choose from the mesh size; 1: exact global ILU(0)
     bool ilu_graph = false;           // subdomains by graph bisection (true) or coordinate bisection
     bool graphs = true;               // capture steps in CUDA graphs
+    int device = -1;                  // GPU ordinal of the context (-1: the calling thread's current one)
     bool profile = false;             // event-time kernel classes inside steps
 
     double gamma() const { return Cp / (Cp - R); }
@@ -367,6 +368,7 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
             else throw ConfigError("ilu.partition must be rcb or graph");
         }
         else if (k == "graphs") o.graphs = parse_bool(k, v);
+        else if (k == "device") o.device = parse_int(k, v);
         else if (k == "profile") o.profile = parse_bool(k, v);
         else throw ConfigError("unknown option '" + k + "'");
     }

@@ -41,6 +41,7 @@ class DecomposedSolver:
         td = case.options.get("ddtSchemes", {}).get("default", "Euler")
         if td != "steadyStateDST":
             raise ValueError("the decomposed solver iterates steady states (ddt steadyStateDST)")
+        backend = dist.get_backend(group)
         subs = _dec.decompose(case.mesh, self.world, layers=layers, method=method)
         self.sub = subs[self.rank]
         bcs = dict(case.bcs)
@@ -50,14 +51,18 @@ class DecomposedSolver:
         if make_solver is None:
             from . import Solver
             make_solver = Solver
-        self.solver = make_solver(self.sub.mesh, bcs, case.options)
+        options = dict(case.options)
+        if backend == "nccl":
+            # one GPU per rank: the library's context on this rank's device
+            import os
+            options.setdefault("device", int(os.environ.get("LOCAL_RANK", self.rank)))
+        self.solver = make_solver(self.sub.mesh, bcs, options)
         c = self.sub.cells
         self.solver.set_primitive(case.p[c], case.U[c], case.T[c], case.nuTilda[c] if self.turb else None)
         # halo cells are held in the steps (zero residual, identity rows):
         # each step solves the owned cells with the halo as Dirichlet data,
         # and the residual norms and the CFL ramp see the owned cells only
         self.solver.set_held_cells(~self.sub.owned)
-        backend = dist.get_backend(group)
         self._device = "cuda" if backend == "nccl" else "cpu"
 
     # -- halo exchange ------------------------------------------------------

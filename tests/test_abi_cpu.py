@@ -60,6 +60,7 @@ def test_partition_host_only():
     ("solvers.W.nSweeps", "0", 1),
     ("solvers.W.fillInLevel", "4", 1),
     ("ilu.partition", "scotch", 1),
+    ("device", "gpu0", 1),
     ("gradSchemes.grad(U)", "cellLimited Gauss linear 2", 1),
     ("gradSchemes.grad(U)", "leastSquares", 6),
     ("divSchemes.div(phi,nuTilda)", "Gauss QUICK", 6),
