@@ -53,9 +53,12 @@ class DecomposedSolver:
             make_solver = Solver
         options = dict(case.options)
         if backend == "nccl":
-            # one GPU per rank: the library's context on this rank's device
+            # one GPU per rank: the library's context and torch's halo
+            # buffers on this rank's device
             import os
+            import torch
             options.setdefault("device", int(os.environ.get("LOCAL_RANK", self.rank)))
+            torch.cuda.set_device(int(options["device"]))
         self.solver = make_solver(self.sub.mesh, bcs, options)
         c = self.sub.cells
         self.solver.set_primitive(case.p[c], case.U[c], case.T[c], case.nuTilda[c] if self.turb else None)
