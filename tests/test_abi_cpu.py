@@ -111,7 +111,9 @@ def test_valid_options_reach_the_device_check():
                      {"solvers.W.preconditioner": {"preconditioner": "GaussSeidel", "nSweeps": 3}},
                      {"solvers.W.preconditioner": "ILUCp", "solvers.W.fillInLevel": 1},
                      {"solvers.W.preconditioner": "AMG", "solvers.W.nPreSweeps": 1},
-                     {"solvers.W.solver": "AMG", "solvers.W.smoother": "Jacobi"})]):
+                     {"solvers.W.solver": "AMG", "solvers.W.smoother": "Jacobi"},
+                     {"device": 0, "ilu.partition": "graph"},
+                     {"gradSchemes.grad(U)": "cellLimited Gauss linear 0.5"})]):
         with pytest.raises(_abi.RdstError) as e:
             rhodst_b200.Solver(case.mesh, case.bcs, case.options)
         assert e.value.status == 3, case.name
