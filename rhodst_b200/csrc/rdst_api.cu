@@ -706,11 +706,15 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
             for (int cc : lurows[r]) { if (cc < r) ++nl[r]; else ++nu[r]; }
         const int ML = *std::max_element(nl.begin(), nl.end());
         const int MU = *std::max_element(nu.begin(), nu.end());
+        // the mesh's own pattern: up to 8 lower/upper neighbours; ILUCp fill
+        // up to 16 (the wider apply keeps its factor rows partly in local
+        // memory)
         if (ML > 8 || MU > 8) {
-            if (o.precon == PRECON_ILUCP && o.fill_in > 0)
+            if (!(o.precon == PRECON_ILUCP && o.fill_in > 0))
+                throw std::invalid_argument("a cell has more than 8 lower/upper neighbours");
+            if (ML > 16 || MU > 16)
                 throw ConfigError("ILUCp fillInLevel " + std::to_string(o.fill_in) +
-                                  " gives a cell more than 8 lower/upper factor blocks on this mesh", true);
-            throw std::invalid_argument("a cell has more than 8 lower/upper neighbours");
+                                  " gives a cell more than 16 lower/upper factor blocks on this mesh", true);
         }
         c.ilu_ml = ML;
         c.ilu_mu = MU;
@@ -1093,7 +1097,8 @@ struct Ops {
         else if (nb <= 3) k_ilu_apply<MT, 3><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
         else if (nb <= 4) k_ilu_apply<MT, 4><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
         else if (nb <= 6) k_ilu_apply<MT, 6><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-        else k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        else if (nb <= 8) k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        else k_ilu_apply<MT, 16><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
         CKL();
     }
     static void precond(rdst_ctx& c, const double* in, double* out, const int* active) {

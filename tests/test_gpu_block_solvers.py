@@ -99,9 +99,20 @@ def test_cell_triangles(precon):
     run_pair(c.with_options(**opts), 4, parts=2)
 
 
+def test_ilucp_wide_fill_steps():
+    """fillInLevel 2 on the split channel: 10 lower / 9 upper factor blocks
+    a cell, the sixteen-slot apply."""
+    c = split_channel_case(8, 5)
+    x, y = c.mesh.C[:, 0], c.mesh.C[:, 1]
+    c.p = 1.0 + 0.2 * np.sin(2.1 * x + 0.3) * np.cos(2.7 * y)
+    opts = {"fluxScheme": "HLL", "solvers.W.solver": "GMRES", "solvers.W.preconditioner": "ILUCp",
+            "solvers.W.fillInLevel": 2, "solvers.W.nDirections": 4, "solvers.W.maxIter": 1,
+            "solvers.W.minIter": 1, "solvers.W.tolerance": 0.0}
+    run_pair(c.with_options(**opts), 4, parts=1)
+
+
 def test_too_wide_fill_is_refused():
-    c = split_channel_case(8, 5).with_options(**{"solvers.W.preconditioner": "ILUCp", "solvers.W.fillInLevel": 2,
-                                                 "ilu.parts": 1})
+    c = step_case("GMRES", "ILUCp", **{"solvers.W.fillInLevel": 3, "ilu.parts": 1})
     with pytest.raises(_abi.RdstError) as e:
         rhodst_b200.Solver(c.mesh, c.bcs, c.options)
     assert e.value.status == 6
