@@ -331,7 +331,11 @@ rdst_status rdst_set_profile(rdst_ctx* ctx, int32_t on);
  * R (n_cells x 5, per unit volume), V (n_cells) and out (6) are DEVICE
  * pointers owned by the caller; out[0] = sqrt(sum_i |R_i|^2) (res_mag of
  * rdst_step_report), out[1+k] = ||R_k V||_2 (res_l2).  Runs asynchronously
- * on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * on `stream` (a cudaStream_t; NULL = legacy default stream) on the GPU
+ * that holds R: V and out must live on the same GPU and `stream` must
+ * belong to it; host pointers and buffers on different GPUs are rejected
+ * with RDST_ERR_ARG before anything is launched.  The calling thread's
+ * current device is left as it was.
  * Scratch is a fixed 192 KiB array in the library's device image, present
  * on every GPU that loads the library until the process exits; n_cells
  * above 1,048,576 is rejected with RDST_ERR_ARG.  Calls share that array:

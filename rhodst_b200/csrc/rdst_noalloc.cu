@@ -17,6 +17,12 @@
 // streams, no ordering between them) race on it and must be serialised by
 // the caller.  Each call overwrites exactly the partials it later reads, so
 // no clearing is needed between calls.
+//
+// The GPU a call runs on is the one that holds R (V and out must be on the
+// same one; host memory is rejected): the library carries its own CUDA
+// runtime, whose current device is not the caller's, so the call selects
+// that device for its set-up and launches and restores the thread's
+// previous device afterwards.  `stream` must belong to that device.
 #include "../../include/rdst.h"
 
 #include <cuda_runtime.h>
@@ -94,12 +100,23 @@ __global__ void k_na_norm_final(const double* __restrict__ partial, int nb, doub
     out[c] = sqrt(s);
 }
 
+// Device of a caller buffer: device memory (or managed memory) only, taken
+// from the pointer itself, since the library's own CUDA runtime does not
+// follow the caller's current device.
+bool device_of(const void* p, int& dev) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return false;
+    dev = a.device;
+    return true;
+}
+
 // Set-up on the first call per device (with that device current): the
 // device address of the scratch array.
-double* scratch_for_current_device(cudaError_t& err) {
-    int dev = 0;
-    err = cudaGetDevice(&dev);
-    if (err != cudaSuccess) return nullptr;
+double* scratch_for_device(int dev, cudaError_t& err) {
     if (dev < 0 || dev >= NA_MAX_DEVICES) {
         err = cudaErrorInvalidDevice;
         return nullptr;
@@ -113,6 +130,21 @@ double* scratch_for_current_device(cudaError_t& err) {
     }
     return g_scratch[dev];
 }
+
+// Makes `dev` current on this thread for the lifetime of the guard and
+// restores the previous device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
 
 }  // namespace
 
@@ -131,8 +163,25 @@ RDST_API rdst_status rdst_residual_norms_noalloc(int32_t n_cells, const double* 
                 " exceeds the fixed scratch capacity of " + std::to_string(NA_MAX_CELLS) + " cells";
         return RDST_ERR_ARG;
     }
+    // the GPU is the one holding the buffers, checked before any launch
+    int dev = -1, dev_v = -1, dev_o = -1;
+    if (!device_of(R, dev) || !device_of(V, dev_v) || !device_of(out, dev_o)) {
+        g_err = "rdst_residual_norms_noalloc: R, V and out must be device memory";
+        return RDST_ERR_ARG;
+    }
+    if (dev_v != dev || dev_o != dev) {
+        g_err = "rdst_residual_norms_noalloc: R, V and out are on different devices (" + std::to_string(dev) +
+                ", " + std::to_string(dev_v) + ", " + std::to_string(dev_o) + ")";
+        return RDST_ERR_ARG;
+    }
+    DeviceGuard guard(dev);
+    if (guard.err != cudaSuccess) {
+        g_err = std::string("rdst_residual_norms_noalloc: cannot select device ") + std::to_string(dev) + ": " +
+                cudaGetErrorString(guard.err);
+        return RDST_ERR_CUDA;
+    }
     cudaError_t e = cudaSuccess;
-    double* partial = scratch_for_current_device(e);
+    double* partial = scratch_for_device(dev, e);
     if (!partial) {
         g_err = std::string("rdst_residual_norms_noalloc: scratch set-up failed: ") + cudaGetErrorString(e);
         return RDST_ERR_CUDA;

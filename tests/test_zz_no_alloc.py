@@ -60,3 +60,44 @@ def test_residual_norms_noalloc_rejects_oversize():
     st = fn(1_048_577, buf.data_ptr(), buf.data_ptr(), buf.data_ptr(), None)
     assert st == 7                       # RDST_ERR_ARG, nothing launched
     assert b"exceeds the fixed scratch capacity" in lib.rdst_last_error(None)
+
+
+def test_residual_norms_noalloc_rejects_host_memory():
+    """Host buffers are refused on the host, before anything is launched."""
+    lib, fn = _fn()
+    host = np.zeros(64, dtype=np.float64)
+    p = host.ctypes.data
+    st = fn(4, p, p, p, None)
+    assert st == 7                       # RDST_ERR_ARG
+    assert b"must be device memory" in lib.rdst_last_error(None)
+
+
+def test_residual_norms_noalloc_follows_the_buffers_device():
+    """A context created on another GPU first leaves the library's runtime
+    on that GPU; the call must still run on the GPU holding the buffers
+    (device 0 here) and give the same norms as the step report."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    lib, fn = _fn()
+    case = cases.forward_step_c1()
+    other = rhodst_b200.Solver(case.mesh, case.bcs, dict(case.options, device=1))
+    other.set_primitive(case.p, case.U, case.T)
+    s = rhodst_b200.solver_for(case)
+    R = s.residual()
+    rep = s.step(1)[0]
+    expect = np.array([rep["res_mag"]] + list(rep["res_l2"]))
+    dev = torch.device("cuda", 0)
+    Rd = torch.tensor(R, dtype=torch.float64, device=dev).contiguous()
+    Vd = torch.tensor(case.mesh.V, dtype=torch.float64, device=dev).contiguous()
+    out = torch.zeros(6, dtype=torch.float64, device=dev)
+    other.residual()                     # the library's runtime is now on device 1
+    st = fn(case.mesh.n_cells, Rd.data_ptr(), Vd.data_ptr(), out.data_ptr(),
+            torch.cuda.current_stream(dev).cuda_stream)
+    assert st == 0, lib.rdst_last_error(None)
+    torch.cuda.synchronize(dev)
+    assert np.allclose(out.cpu().numpy(), expect, rtol=1e-12, atol=0.0)
+    # buffers split across two GPUs are refused before any launch
+    V1 = Vd.to(torch.device("cuda", 1))
+    st = fn(case.mesh.n_cells, Rd.data_ptr(), V1.data_ptr(), out.data_ptr(), None)
+    assert st == 7 and b"different devices" in lib.rdst_last_error(None)
