@@ -20,6 +20,7 @@
 #include "../include/rdst.h"
 #include "../rhodst_b200/csrc/rdst_options.h"
 #include "../rhodst_b200/csrc/rdst_amg.h"
+#include "../rhodst_b200/csrc/rdst_order.h"
 
 #include <algorithm>
 #include <array>
@@ -1191,10 +1192,13 @@ struct PreconData {
     int sweeps = 1;                       // Gauss-Seidel sweeps per application
     const LDU* A = nullptr;               // the matrix (Gauss-Seidel residual sweeps)
     std::vector<t5> Dinv;                 // diagonal: inv(D); factored: inv(pivot)
-    // factors in CSR per row (cells in natural order)
-    std::vector<int> rowStart, col;       // off-diagonal columns per row, ascending
-    std::vector<t5> val;                  // L D~^-1 (k < i) or U (k > i) block
-    std::vector<std::vector<int>> prow;   // rows of each partition part, ascending (independent)
+    // factors in CSR per row; rows factorised in the order of key(i): the
+    // cell number (mesh order) or the breadth-first rank of rdst_order.h
+    std::vector<int> rowStart, col;       // off-diagonal columns per row, by key
+    std::vector<t5> val;                  // L D~^-1 (key k < key i) or U (key k > key i) block
+    std::vector<std::vector<int>> prow;   // rows of each partition part, by key (independent)
+    std::vector<int> rank;                // breadth-first ranks (empty: mesh order)
+    int key(int i) const { return rank.empty() ? i : rank[i]; }
 };
 
 // rows of each part in ascending order (one part: all rows)
@@ -1289,9 +1293,24 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
     if (!lu_factored((Precon)M.kind)) return;
     M.A = &A;
     M.sweeps = c.o.n_sweeps;
-    // Incomplete block LU in cell order (IKJ form): for row i, for each k < i
-    // in the pattern: L_ik = A_ik inv(U_kk); A_ij -= L_ik U_kj for j > k in
-    // the pattern of row i (j == i: the pivot).  ILUC0 keeps every update on
+    // factorisation order inside the parts: mesh order, or breadth first
+    // (rdst_order.h; the default with more than one part)
+    {
+        int np = 1;
+        for (int i = 0; i < (int)c.part.size(); ++i) np = std::max(np, c.part[i] + 1);
+        M.rank.clear();
+        if (c.o.ilu_order == 1 || (c.o.ilu_order < 0 && np > 1)) {
+            std::vector<std::vector<int>> adj(N);
+            for (int f = 0; f < c.Fi; ++f) { adj[c.own[f]].push_back(c.nei[f]); adj[c.nei[f]].push_back(c.own[f]); }
+            std::vector<int> part = c.part.empty() ? std::vector<int>(N, 0) : c.part;
+            M.rank = subdomain_bfs_rank(adj, part);
+        }
+    }
+    // Incomplete block LU in factorisation order (IKJ form; order = key(i),
+    // the cell number, or the breadth-first rank inside the parts): for row
+    // i, for each k before i in the pattern: L_ik = A_ik inv(U_kk);
+    // A_ij -= L_ik U_kj for j after k in the pattern of row i (j == i: the
+    // pivot).  ILUC0 keeps every update on
     // the matrix pattern; ILUCp on the pattern extended to the cells within
     // fillInLevel + 1 faces (foam-extend extendedLduAddressing: neighbours
     // of neighbours, level by level); Cholesky keeps only the pivot updates
@@ -1347,6 +1366,8 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
                 for (int k = 0; k < 25; ++k) m.back().second[k] += e.second[k];
             else m.push_back(e);
         }
+        if (!M.rank.empty())
+            std::sort(m.begin(), m.end(), [&](auto& a, auto& b) { return M.rank[a.first] < M.rank[b.first]; });
         r.swap(m);
     }
     M.rowStart.assign(N + 1, 0);
@@ -1364,17 +1385,20 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
     // parts are independent (no couplings between them): one part per task,
     // rows of a part in ascending order
     M.prow = part_rows(c);
+    if (!M.rank.empty())
+        for (auto& rows_p : M.prow)
+            std::sort(rows_p.begin(), rows_p.end(), [&](int a, int b) { return M.rank[a] < M.rank[b]; });
     OMP_FOR_DYN
     for (int pp = 0; pp < (int)M.prow.size(); ++pp)
     for (int i : M.prow[pp]) {
         for (int q = M.rowStart[i]; q < M.rowStart[i + 1]; ++q) {
             int k = M.col[q];
-            if (k >= i) break;
+            if (M.key(k) >= M.key(i)) break;
             M.val[q] = mm(M.val[q], M.Dinv[k]);          // L_ik
-            // for j > k in row k's upper part and in row i's pattern (or j = i)
+            // for j after k in row k's upper part and in row i's pattern (or j = i)
             for (int r = M.rowStart[k]; r < M.rowStart[k + 1]; ++r) {
                 int j = M.col[r];
-                if (j <= k) continue;
+                if (M.key(j) <= M.key(k)) continue;
                 if (j == i) {
                     if (!upd_diag) continue;
                     t5 t = mm(M.val[q], M.val[r]);
@@ -1504,7 +1528,7 @@ void lu_apply(const Ctx& c, const PreconData& M, Vec& x, const Vec& b, bool uppe
             v5 y = b[i];
             for (int q = M.rowStart[i]; q < M.rowStart[i + 1]; ++q) {
                 int k = M.col[q];
-                if (k >= i) break;
+                if (M.key(k) >= M.key(i)) break;
                 v5 t = mv(M.val[q], x[k]);
                 for (int e = 0; e < 5; ++e) y[e] -= t[e];
             }
@@ -1515,7 +1539,7 @@ void lu_apply(const Ctx& c, const PreconData& M, Vec& x, const Vec& b, bool uppe
             v5 y = x[i];
             for (int q = M.rowStart[i]; q < M.rowStart[i + 1] && upper; ++q) {
                 int j = M.col[q];
-                if (j <= i) continue;
+                if (M.key(j) <= M.key(i)) continue;
                 v5 t = mv(M.val[q], x[j]);
                 for (int e = 0; e < 5; ++e) y[e] -= t[e];
             }

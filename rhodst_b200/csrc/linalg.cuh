@@ -172,6 +172,25 @@ struct IluDev {
     int mu_use;             // U slots the backward sweep applies (0: (D + L)^-1 of Gauss-Seidel)
     const int* lu_col;      // [fid] column of each factor slot (-1: empty)
     const int* lu_src;      // [fid] SELL flat slot of the same block in A
+    // task records of the bulk apply (null: not kept).  Each sweep's tasks
+    // (24 rows of one level, in the order the sweep takes them) are laid
+    // out one after the other in rec_f (forward) / rec_b (backward): a
+    // 96-byte header of 24 words (byte offset of the row's record from the
+    // task start | slot count << 24), then the row records: the columns of
+    // the row's L (U) slots, padded to 16 bytes, the blocks (entry 5i+j),
+    // and backward the pivot inverse, each record padded to 16 bytes.
+    // task_f/task_b: (offset in 16-byte units, bytes) per task; part_tf /
+    // part_tb: first task of each part.  The headers and columns are set
+    // once; k_ilu_pack writes the blocks at val_f/val_b (16-byte units) of
+    // every row after each factorisation.
+    unsigned char* rec_f;
+    unsigned char* rec_b;
+    const uint2* task_f;
+    const uint2* task_b;
+    const int* part_tf;
+    const int* part_tb;
+    const unsigned* val_f;
+    const unsigned* val_b;
 };
 
 __device__ __forceinline__ int lu_fid(int r, int s, int ms) { return ((r >> 5) * ms + s) * 32 + (r & 31); }
@@ -268,6 +287,7 @@ __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> A, MT* __res
 constexpr int ILU_APPLY_TPB = 128;
 constexpr int ILU_APPLY_MINB = 4;      // resident CTAs per SM the register budget is sized for
 constexpr int ILU_MAX_LV = 1023;       // level offsets staged in shared memory up to this many
+constexpr int ILU_LB_MAX = 1024;       // widest level the bulk apply's level buffers hold (2 x 40 KB)
 
 // One row task of a sweep: the factor row's columns, this lane's entries
 // of each slot, its pivot-inverse row (backward sweep) and the starting
@@ -394,6 +414,340 @@ __global__ void __launch_bounds__(ILU_APPLY_TPB, ILU_APPLY_MINB)
                 q[d] = q[d + 1]; rq[d] = rq[d + 1]; aq[d] = aq[d + 1]; eq[d] = eq[d + 1]; vq[d] = vq[d + 1];
             }
         }
+    }
+}
+
+// ---- ILU apply with the factor rows of each task brought in by bulk copies
+//
+// Same subdomains, levels and tasks as k_ilu_apply.  What differs is how a
+// task's data reaches the lanes, and the arithmetic (below): the task records
+// (IluDev::rec_f / rec_b, one contiguous byte range per task) are brought
+// in by a single cp.async.bulk (TMA) copy, issued by one thread, into a
+// shared-memory stage whose mbarrier counts the bytes; NS stages keep
+// NS - 1 tasks in flight ahead of the one being computed.  The copies run
+// in the async proxy (no register of the lanes waits on them), the lanes
+// read 16-byte-aligned records from shared memory, and the memory system
+// sees large contiguous requests.  The starting values y0 (b forward, the
+// forward result backward) come by per-lane cp.async.  With LB, the x
+// values of each level also go to one of two shared-memory level buffers
+// (level l to buffer l & 1, row r at r - first row of l, padded to 16
+// bytes for vector loads): the dependencies
+// of a row in the level the sweep took just before are read from there,
+// older ones from global memory.  In breadth-first order (rdst_order.h)
+// nearly all couplings join consecutive levels.
+//
+// A stage is refilled only after the barrier that ends the task that read
+// it.  Each mbarrier wait is bounded (2 s of globaltimer): on expiry the
+// CTA raises bit 2 of *flags (reported as a timeout by the host), waits,
+// again bounded, for its copies in flight and returns.
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy completing on an mbarrier (no multicast)
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+// true once the phase of parity `parity` has completed; false after 2 s
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+    unsigned long long t0 = 0;
+    for (unsigned it = 0;; ++it) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        if (ok) return true;
+        if ((it & 63) == 0) {
+            const unsigned long long now = globaltimer_ns();
+            if (it == 0) t0 = now;
+            else if (now - t0 > 2000000000ull) return false;
+        }
+    }
+}
+__device__ __forceinline__ void cpa8(unsigned dst, const void* src, bool ok) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(ok ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Four warps a subdomain, five lanes a row (one per component), six rows a
+// warp: a task is up to 24 rows of one level.  The lanes multiply in CT,
+// the arithmetic of the factors' storage type: double for 8-byte factors,
+// float for 4- and 2-byte ones (the reduced-precision preconditioner
+// applies its FP32/BF16 factors in FP32; its input b and output x stay
+// FP64 vectors).  Each factor block's product with x_k is summed first
+// (the block-times-vector of the oracle's apply), then subtracted from y,
+// block by block in column order.
+constexpr int ILU_BULK_TPB = 128;
+constexpr int ILU_BULK_RPT = (ILU_BULK_TPB / 32) * 6;   // rows per task (24)
+constexpr int ILU_BULK_HDR = ILU_BULK_RPT * 4;           // task header bytes (96)
+
+template <typename MT> struct IluCT { using T = float; };
+template <> struct IluCT<double> { using T = double; };
+__device__ __forceinline__ double to_ct(double v, double) { return v; }
+__device__ __forceinline__ float to_ct(float v, float) { return v; }
+__device__ __forceinline__ float to_ct(__nv_bfloat16 v, float) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_ct(double v, float) { return (float)v; }
+// level-buffer row: five values padded to 16 bytes (6 doubles / 8 floats)
+template <typename CT> constexpr int lb_row() { return sizeof(CT) == 8 ? 6 : 8; }
+__device__ __forceinline__ void lb_load(const double* p, double (&o)[5]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a0 = q[0], a1 = q[1], a2 = q[2];
+    o[0] = a0.x; o[1] = a0.y; o[2] = a1.x; o[3] = a1.y; o[4] = a2.x;
+}
+__device__ __forceinline__ void lb_load(const float* p, float (&o)[5]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a0 = q[0], a1 = q[1];
+    o[0] = a0.x; o[1] = a0.y; o[2] = a0.z; o[3] = a0.w; o[4] = a1.x;
+}
+
+// stages the bulk apply keeps (NS - 1 tasks in flight)
+template <typename MT>
+constexpr int ilu_bulk_stages() { return 3; }
+
+// factor blocks -> task records (after each factorisation): one CTA per 32
+// rows, each factor slot staged through shared memory so both the sliced
+// loads and the record stores are contiguous
+template <typename MT>
+__global__ void __launch_bounds__(256) k_ilu_pack(int N, const MT* __restrict__ lu, const MT* __restrict__ dinv,
+                                                  IluDev P) {
+    __shared__ MT tile[25][33];
+    __shared__ int s_nmax[2];
+    const int chunk = blockIdx.x, r0 = chunk * 32;
+    const int ms = P.ml + P.mu;
+    // slots any row of the chunk uses (the rest of the sliced store is empty)
+    if (threadIdx.x < 32) {
+        const int r = r0 + threadIdx.x;
+        const int nlu = r < N ? P.nlu[r] : 0;
+        int a = nlu & 255, u = P.mu_use ? (nlu >> 8) & 255 : 0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a = max(a, __shfl_xor_sync(0xffffffffu, a, o));
+            u = max(u, __shfl_xor_sync(0xffffffffu, u, o));
+        }
+        if (threadIdx.x == 0) { s_nmax[0] = a; s_nmax[1] = u; }
+    }
+    __syncthreads();
+    const int lmax = s_nmax[0], umax = s_nmax[1];
+    for (int sl = 0; sl <= ms; ++sl) {            // sl == ms: the pivot inverses
+        if (sl < P.ml ? sl >= lmax : (sl < ms && sl - P.ml >= umax)) continue;
+        const MT* src = sl < ms ? lu + (size_t)(chunk * ms + sl) * 800 : dinv + (size_t)chunk * 800;
+        __syncthreads();
+        for (int i = threadIdx.x; i < 800; i += blockDim.x) tile[i >> 5][i & 31] = src[i];
+        __syncthreads();
+        for (int i = threadIdx.x; i < 800; i += blockDim.x) {
+            const int row = i / 25, e = i - 25 * (i / 25), r = r0 + row;
+            if (r >= N) continue;
+            const int nl = P.nlu[r] & 255, nu = P.mu_use ? (P.nlu[r] >> 8) & 255 : 0;
+            if (sl < P.ml) {
+                if (sl < nl) reinterpret_cast<MT*>(P.rec_f + (size_t)P.val_f[r] * 16)[25 * sl + e] = tile[e][row];
+            } else if (sl < ms) {
+                const int q = sl - P.ml;
+                if (q < nu) reinterpret_cast<MT*>(P.rec_b + (size_t)P.val_b[r] * 16)[25 * q + e] = tile[e][row];
+            } else {
+                reinterpret_cast<MT*>(P.rec_b + (size_t)P.val_b[r] * 16)[25 * nu + e] = tile[e][row];
+            }
+        }
+    }
+}
+
+template <typename MT, int NS, bool LB>
+__global__ void __launch_bounds__(ILU_BULK_TPB, 8)
+    k_ilu_apply_bulk(IluDev P, const double* __restrict__ b, double* x, const int* __restrict__ active,
+                     int lb_rows, int stage_bytes, int off_slots, int task_slots, int* flags) {
+    using CT = typename IluCT<MT>::T;
+    constexpr int T = ILU_BULK_TPB;
+    constexpr int RPT = ILU_BULK_RPT;
+    constexpr int LR = lb_row<CT>();
+    if (active && !*active) return;
+    __shared__ __align__(8) unsigned long long s_bar[NS];
+    __shared__ int s_abort;
+    extern __shared__ __align__(128) unsigned char s_dyn[];
+    unsigned char* s_stage = s_dyn;                                                   // [NS][stage_bytes]
+    double* s_y0 = reinterpret_cast<double*>(s_dyn + (size_t)NS * stage_bytes);       // [NS][T]
+    CT* s_lvx = reinterpret_cast<CT*>(s_y0 + NS * T);                                 // [2][lb_rows][LR]
+    uint2* s_task = reinterpret_cast<uint2*>(s_lvx + 2 * LR * lb_rows);               // [task_slots] f then b
+    int* s_off = reinterpret_cast<int*>(s_task + task_slots);                         // [off_slots]
+    const int part = blockIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int rsub = lane / 5, comp = lane - 5 * (lane / 5);
+    const bool lane_ok = lane < 30;
+    const int i_row = warp * 6 + rsub;
+    const int l0 = P.part_lvl0[part], l1 = P.part_lvl0[part + 1];
+    const bool staged = l1 - l0 < off_slots;
+    if (staged)
+        for (int i = tid; i <= l1 - l0; i += T) s_off[i] = P.lvl_off[l0 + i];
+    const int tf0 = P.part_tf[part], ntf = P.part_tf[part + 1] - tf0;
+    const int tb0 = P.part_tb[part], ntb = P.part_tb[part + 1] - tb0;
+    const bool tstaged = ntf + ntb <= task_slots;
+    if (tstaged) {
+        for (int i = tid; i < ntf; i += T) s_task[i] = P.task_f[tf0 + i];
+        for (int i = tid; i < ntb; i += T) s_task[ntf + i] = P.task_b[tb0 + i];
+    }
+    const unsigned bar0 = (unsigned)__cvta_generic_to_shared(&s_bar[0]);
+    const unsigned stage0 = (unsigned)__cvta_generic_to_shared(s_stage);
+    const unsigned y0a = (unsigned)__cvta_generic_to_shared(s_y0 + tid);
+    if (tid == 0) {
+        for (int k = 0; k < NS; ++k) mbar_init(bar0 + 8 * k, 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto off = [&](int l) { return staged ? s_off[l - l0] : P.lvl_off[l]; };
+    unsigned par = 0;          // bit k: parity of stage k's next completion
+    unsigned pending = 0;      // bit k: a copy into stage k not yet waited for
+
+#pragma unroll 1
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        const bool back = sweep == 1;
+        const int dir = back ? -1 : 1;
+        const unsigned char* rec = back ? P.rec_b : P.rec_f;
+        const double* ysrc = back ? x : b;
+        IluCursor cur{back ? l1 - 1 : l0, 0};
+        int tcount = 0;        // tasks of this sweep issued so far
+        auto in_range = [&](int l) { return back ? l >= l0 : l < l1; };
+        // per queued task: first row, rows, its level's first row and buffer,
+        // the previous level's first row and width
+        int qr0[NS], qn[NS], qa[NS], qbuf[NS], qpa[NS], qpw[NS];
+        bool qv[NS];
+        // advance the cursor and start task d's copies into stage d
+        auto next = [&](int d) {
+            qv[d] = in_range(cur.l);
+            qr0[d] = 0; qn[d] = 0; qa[d] = 0; qbuf[d] = 0; qpa[d] = 0; qpw[d] = 0;
+            if (qv[d]) {
+                const int r0 = off(cur.l), r1 = off(cur.l + 1), n = r1 - r0;
+                qr0[d] = r0 + cur.base;
+                qn[d] = min(RPT, n - cur.base);
+                if (LB) {
+                    qa[d] = r0;
+                    qbuf[d] = (cur.l & 1) * lb_rows * LR;
+                    const int lp = cur.l - dir;          // the level taken just before
+                    if (in_range(lp)) { qpa[d] = off(lp); qpw[d] = off(lp + 1) - qpa[d]; }
+                }
+                cur.base += RPT;
+                if (cur.base >= n) { cur.l += dir; cur.base = 0; }
+                if (tid == 0) {
+                    const uint2 tk = tstaged ? s_task[(back ? ntf : 0) + tcount]
+                                             : (back ? P.task_b[tb0 + tcount] : P.task_f[tf0 + tcount]);
+                    mbar_expect_tx(bar0 + 8 * d, tk.y);
+                    bulk_g2s(stage0 + (unsigned)(d * stage_bytes), rec + (size_t)tk.x * 16, tk.y, bar0 + 8 * d);
+                }
+                ++tcount;
+                pending |= 1u << d;
+            }
+            const bool act = qv[d] && lane_ok && i_row < qn[d];
+            cpa8(y0a + (unsigned)(d * T * 8), ysrc + (act ? 5 * (size_t)(qr0[d] + i_row) + comp : 0), act);
+            cpa_commit();
+        };
+        // task d: wait for its stage, y = y0 - sum_k (L_rk x_k) (backward
+        // x_r = inv(U_rr) y), then the barrier that ends the task
+        auto run = [&](int d) {
+            if (!mbar_wait(bar0 + 8 * d, (par >> d) & 1u)) {
+                atomicOr(flags, 4);
+                s_abort = 1;
+            }
+            par ^= 1u << d;
+            pending &= ~(1u << d);
+            cpa_wait<NS - 1>();
+            const bool act = lane_ok && i_row < qn[d] && !s_abort;
+            const int r = qr0[d] + i_row;
+            const unsigned char* st0 = s_stage + (size_t)d * stage_bytes;
+            const unsigned hdr = act ? reinterpret_cast<const unsigned*>(st0)[i_row] : 0u;
+            const int cnt = (int)(hdr >> 24);
+            const int* cols = reinterpret_cast<const int*>(st0 + (hdr & 0xffffffu));
+            const MT* vals = reinterpret_cast<const MT*>(st0 + (hdr & 0xffffffu) + 16 * ((cnt + 3) >> 2));
+            CT y = to_ct(s_y0[d * T + tid], CT());
+            if (act) {
+                // the first four blocks side by side (their products are
+                // independent), then subtracted in column order; a block
+                // past the row's count loads nothing and contributes 0
+                const CT* pbuf = s_lvx + (lb_rows * LR - qbuf[d]);   // the other level buffer
+                CT part4[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    CT t = CT(0);
+                    if (k < cnt) {
+                        const int ck = cols[k];
+                        const unsigned rel = (unsigned)(ck - qpa[d]);
+                        CT xk[5];
+                        if (LB && rel < (unsigned)qpw[d]) {
+                            lb_load(pbuf + LR * rel, xk);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 5; ++j) xk[j] = to_ct(x[5 * ck + j], CT());
+                        }
+                        t = to_ct(vals[25 * k + 5 * comp], CT()) * xk[0];
+#pragma unroll
+                        for (int j = 1; j < 5; ++j) t += to_ct(vals[25 * k + 5 * comp + j], CT()) * xk[j];
+                    }
+                    part4[k] = t;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) y -= part4[k];
+                for (int k = 4; k < cnt; ++k) {
+                    const int ck = cols[k];
+                    const unsigned rel = (unsigned)(ck - qpa[d]);
+                    CT xk[5];
+                    if (LB && rel < (unsigned)qpw[d]) {
+                        lb_load(pbuf + LR * rel, xk);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 5; ++j) xk[j] = to_ct(x[5 * ck + j], CT());
+                    }
+                    CT t = to_ct(vals[25 * k + 5 * comp], CT()) * xk[0];
+#pragma unroll
+                    for (int j = 1; j < 5; ++j) t += to_ct(vals[25 * k + 5 * comp + j], CT()) * xk[j];
+                    y -= t;
+                }
+            }
+            if (back) {
+                CT a = CT(0);
+#pragma unroll
+                for (int j = 0; j < 5; ++j) {
+                    const CT yj = __shfl_sync(0xffffffffu, y, (lane_ok ? 5 * rsub : 0) + j);
+                    a += (act ? to_ct(vals[25 * cnt + 5 * comp + j], CT()) : CT(0)) * yj;
+                }
+                y = a;
+            }
+            if (act) {
+                x[5 * (size_t)r + comp] = (double)y;
+                if (LB) s_lvx[qbuf[d] + LR * (r - qa[d]) + comp] = y;
+            }
+            __syncthreads();
+        };
+        // stage slots rotate with compile-time indices (the body is
+        // unrolled NS times), so the queue stays in registers
+#pragma unroll
+        for (int d = 0; d < NS - 1; ++d) next(d);
+        bool go = qv[0];
+        while (go) {
+#pragma unroll
+            for (int u = 0; u < NS; ++u) {
+                if (go) {
+                    next((u + NS - 1) % NS);
+                    run(u);
+                    go = qv[(u + 1) % NS] && !s_abort;
+                }
+            }
+        }
+        cpa_wait<0>();
+        if (s_abort) {
+            // copies still in flight land before the CTA's shared memory goes
+            for (int d = 0; d < NS; ++d)
+                if ((pending >> d) & 1u) mbar_wait(bar0 + 8 * d, (par >> d) & 1u);
+            return;
+        }
+        // the next sweep issues its first tasks into stages 0..NS-2 again:
+        // the queue rotation restarts, parities carry on
+        __syncthreads();
     }
 }
 

@@ -11,6 +11,7 @@
 #include "adjoint.cuh"
 #include "amg.cuh"
 #include "rdst_amg.h"
+#include "rdst_order.h"
 
 #include <algorithm>
 #include <cmath>
@@ -33,6 +34,11 @@ namespace {
 struct CudaError : std::runtime_error {
     explicit CudaError(const std::string& m) : std::runtime_error(m) {}
 };
+// a bounded device wait gave up (a kernel raised bit 2 of the step flags)
+struct TimeoutError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
 
 inline void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
@@ -259,6 +265,16 @@ struct rdst_ctx {
     DBuf<int> part_lvl0, lvl_off, low_start, nlu, tr_start, tr_kj, tr_rj, lu_col, lu_src;
     int lu_slots = 0;
     int ilu_ml = 0, ilu_mu = 0, ilu_mu_use = 0;
+    // task records of the bulk ILU apply (empty: the register apply runs)
+    DBuf<unsigned char> rec_f, rec_b;
+    DBuf<uint2> task_f, task_b;
+    DBuf<int> part_tf, part_tb;
+    DBuf<unsigned> val_f, val_b;
+    int ilu_stage_bytes = 0;         // largest task record, rounded to 128 bytes
+    int ilu_stages = 0;              // stages of the bulk apply (2 or 3)
+    int ilu_lb_rows = 0;             // rows of each level buffer (0: none)
+    int ilu_off_slots = 0;           // level offsets staged in shared memory (max levels + 1, even)
+    int ilu_task_slots = 0;          // task table entries staged (max forward + backward tasks, even)
     // Krylov
     DBuf<double> dx, r, t, Vb, s2, sh, ph, pv, xbar, Ax, pA;
     DBuf<double> gs_r, gs_z;        // residual and correction of Gauss-Seidel sweeps after the first
@@ -378,6 +394,8 @@ struct rdst_ctx {
         P.n_parts = n_parts; P.part_lvl0 = part_lvl0.p; P.lvl_off = lvl_off.p;
         P.nlu = nlu.p; P.low_start = low_start.p; P.ml = ilu_ml; P.mu = ilu_mu; P.mu_use = ilu_mu_use; P.lu_col = lu_col.p; P.lu_src = lu_src.p;
         P.tr_start = tr_start.p; P.tr_kj = tr_kj.p; P.tr_rj = tr_rj.p;
+        P.rec_f = rec_f.p; P.rec_b = rec_b.p; P.task_f = task_f.p; P.task_b = task_b.p;
+        P.part_tf = part_tf.p; P.part_tb = part_tb.p; P.val_f = val_f.p; P.val_b = val_b.p;
         return P;
     }
     long nvec() const { return 5L * N; }
@@ -429,14 +447,18 @@ int lim_code(Limiter l) { return (int)l; }
 // chain of each CTA, so once there are more subdomains than CTAs the GPU
 // holds at once the count is rounded to a whole number of such waves (a
 // partial last wave costs a whole extra chain: measured on the 1.2 M-cell
-// wing, 784 parts took 23% longer than 592 or 1184).
-int auto_ilu_parts(int N, Precision prec) {
+// wing with the register apply, 784 parts took 23% longer than 592 or
+// 1184).  The bulk apply holds eight CTAs an SM (64 registers a thread, its
+// shared memory sized for that), the register apply four.
+int auto_ilu_parts(int N, Precision prec, bool bulk) {
     const int p0 = std::max(1, N / 1536);
     int dev = 0, sms = 0, per_sm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // the four-slot instance bounds the register use of the ones hex meshes need
-    if (prec == PREC_FP64)
+    if (bulk)
+        per_sm = 8;
+    else if (prec == PREC_FP64)
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu_apply<double, 4>, ILU_APPLY_TPB, 0));
     else if (prec == PREC_FP32)
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu_apply<float, 4>, ILU_APPLY_TPB, 0));
@@ -511,6 +533,121 @@ void load_geometry(rdst_ctx& c, const rdst_mesh* mh, bool in_place) {
     CK(cudaStreamSynchronize(s));
 }
 
+// The bulk apply's task records (IluDev::rec_f / rec_b): the tasks of each
+// part in the order the apply's cursor takes them (forward: levels
+// ascending; backward: levels descending; 24-row chunks of a level in
+// ascending rows), their headers and columns written here, the blocks by
+// k_ilu_pack after each factorisation.  Three stages when the CTAs every
+// subdomain needs at once (up to eight an SM) still fit with them, else
+// two; a task too large for one CTA's shared memory leaves the register
+// apply in place.
+void build_task_records(rdst_ctx& c, const Options& o, int nparts, const std::vector<int>& part_lvl0,
+                        const std::vector<int>& lvl_off, const std::vector<int>& lu_col, const std::vector<int>& nl,
+                        const std::vector<int>& nu, int ML, int MS) {
+    const int N = c.N;
+    const size_t S = o.precision == PREC_FP64 ? 8 : (o.precision == PREC_FP32 ? 4 : 2);
+    auto lfid = [&](int r, int sl) { return ((r >> 5) * MS + sl) * 32 + (r & 31); };
+    auto r16 = [](size_t v) { return (v + 15) / 16 * 16; };
+    auto cnt_of = [&](int r, bool back) { return back ? (c.ilu_mu_use ? nu[r] : 0) : nl[r]; };
+    auto rec_bytes = [&](int r, bool back) {
+        const int n = cnt_of(r, back);
+        return r16(16 * (size_t)((n + 3) / 4) + (size_t)(n + (back ? 1 : 0)) * 25 * S);
+    };
+    struct Tk { int r0, n; };
+    std::vector<Tk> tf, tb;
+    std::vector<int> ptf(nparts + 1, 0), ptb(nparts + 1, 0);
+    int maxw = 0, maxlv = 0, maxtasks = 0;
+    for (int p = 0; p < nparts; ++p) {
+        ptf[p] = (int)tf.size();
+        ptb[p] = (int)tb.size();
+        const int a = part_lvl0[p], e = part_lvl0[p + 1];
+        maxlv = std::max(maxlv, e - a);
+        for (int li = a; li < e; ++li) {
+            const int r0 = lvl_off[li], n = lvl_off[li + 1] - r0;
+            maxw = std::max(maxw, n);
+            for (int b = 0; b < n; b += ILU_BULK_RPT) tf.push_back({r0 + b, std::min(ILU_BULK_RPT, n - b)});
+        }
+        for (int li = e - 1; li >= a; --li) {
+            const int r0 = lvl_off[li], n = lvl_off[li + 1] - r0;
+            for (int b = 0; b < n; b += ILU_BULK_RPT) tb.push_back({r0 + b, std::min(ILU_BULK_RPT, n - b)});
+        }
+        maxtasks = std::max(maxtasks, (int)(tf.size() - ptf[p] + tb.size() - ptb[p]));
+    }
+    ptf[nparts] = (int)tf.size();
+    ptb[nparts] = (int)tb.size();
+    size_t max_task = 0;
+    auto layout = [&](const std::vector<Tk>& tasks, bool back, std::vector<uint2>& tab) {
+        tab.resize(tasks.size());
+        size_t pos = 0;
+        for (size_t t = 0; t < tasks.size(); ++t) {
+            size_t bytes = ILU_BULK_HDR;
+            for (int i = 0; i < tasks[t].n; ++i) bytes += rec_bytes(tasks[t].r0 + i, back);
+            tab[t] = make_uint2((unsigned)(pos / 16), (unsigned)bytes);
+            pos += bytes;
+            max_task = std::max(max_task, bytes);
+        }
+        return pos;
+    };
+    std::vector<uint2> tabf, tabb;
+    const size_t totf = layout(tf, false, tabf), totb = layout(tb, true, tabb);
+    // shared memory: stages, y0 slots, level buffers, task table, level offsets
+    const int stage = (int)((max_task + 127) / 128 * 128);
+    const int lb = maxw <= ILU_LB_MAX ? maxw : 0;
+    const int task_slots = (maxtasks + 1) / 2 * 2;
+    const int off_slots = (maxlv + 2) / 2 * 2;
+    auto smem = [&](int ns) {
+        return (size_t)ns * stage + (size_t)ns * ILU_BULK_TPB * 8 + (size_t)lb * (S == 8 ? 96 : 64) +
+               (size_t)task_slots * 8 + (size_t)off_slots * 4 + 64;
+    };
+    int dev = 0, per_sm = 0, per_block = 0, reserved = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    CK(cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    CK(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    // CTAs an SM must hold for all subdomains to run at once (up to 8)
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t want = (size_t)std::min(8, std::max(1, (nparts + sms - 1) / std::max(sms, 1)));
+    int ns = 3;
+    if ((smem(3) + reserved) * want > (size_t)per_sm) ns = 2;
+    if (smem(ns) > (size_t)per_block) return;
+    std::vector<unsigned char> bf(totf, 0), bb(totb, 0);
+    std::vector<unsigned> vf(N, 0), vb(N, 0);
+    auto fill = [&](const std::vector<Tk>& tasks, const std::vector<uint2>& tab, bool back,
+                    std::vector<unsigned char>& buf, std::vector<unsigned>& val) {
+        for (size_t t = 0; t < tasks.size(); ++t) {
+            const size_t start = (size_t)tab[t].x * 16;
+            unsigned* hdr = reinterpret_cast<unsigned*>(buf.data() + start);
+            size_t pos = start + ILU_BULK_HDR;
+            for (int i = 0; i < tasks[t].n; ++i) {
+                const int r = tasks[t].r0 + i, n = cnt_of(r, back);
+                hdr[i] = (unsigned)(pos - start) | ((unsigned)n << 24);
+                int* cols = reinterpret_cast<int*>(buf.data() + pos);
+                const int ncol = 4 * ((n + 3) / 4);
+                for (int q = 0; q < ncol; ++q) cols[q] = q < n ? lu_col[lfid(r, back ? ML + q : q)] : -1;
+                val[r] = (unsigned)((pos + 16 * (size_t)((n + 3) / 4)) / 16);
+                pos += rec_bytes(r, back);
+            }
+        }
+    };
+    fill(tf, tabf, false, bf, vf);
+    fill(tb, tabb, true, bb, vb);
+    cudaStream_t s = c.s;
+    c.rec_f.upload(bf, s); c.rec_b.upload(bb, s);
+    c.task_f.upload(tabf, s); c.task_b.upload(tabb, s);
+    c.part_tf.upload(ptf, s); c.part_tb.upload(ptb, s);
+    c.val_f.upload(vf, s); c.val_b.upload(vb, s);
+    c.ilu_stage_bytes = stage;
+    c.ilu_stages = ns;
+    c.ilu_lb_rows = lb;
+    c.ilu_task_slots = task_slots;
+    c.ilu_off_slots = off_slots;
+    CK(cudaStreamSynchronize(s));
+}
+
+template <typename MT>
+static void ilu_bulk_attr(rdst_ctx& c);
+
 void build(rdst_ctx& c, const rdst_mesh* mh) {
     cudaStream_t s = c.s;
     const int N = mh->n_cells, Fi = mh->n_internal_faces, F = mh->n_faces;
@@ -559,12 +696,13 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     // neighbours, or for ILUCp the same-part cells within fill_in + 1 faces
     // (neighbours of neighbours, level by level, as foam-extend's
     // extendedLduAddressing builds them).
-    std::vector<int> part(N, 0), level(N, 0);
+    std::vector<int> part(N, 0), level(N, 0), rank;
+    bool bfs_order = false;
     std::vector<std::vector<int>> lupat;
     int nparts = 1;
     const bool factored = lu_factored(o.precon);
     if (factored) {
-        nparts = o.ilu_parts > 0 ? o.ilu_parts : auto_ilu_parts(N, o.precision);
+        nparts = o.ilu_parts > 0 ? o.ilu_parts : auto_ilu_parts(N, o.precision, o.ilu_bulk);
         nparts = std::min(nparts, N);
         if (o.ilu_graph) {
             graph_partition(N, Fi, mh->owner, mh->neighbour, nparts, part.data());
@@ -600,10 +738,28 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
             }
             lupat.swap(ext);
         }
-        for (int i = 0; i < N; ++i) {
+        // factorisation order of each subdomain: mesh order, or breadth
+        // first (rdst_order.h); a row's wavefront level is one past the
+        // deepest of its pattern cells that come before it
+        bfs_order = o.ilu_order == 1 || (o.ilu_order < 0 && nparts > 1);
+        rank.resize(N);
+        if (bfs_order) {
+            std::vector<std::vector<int>> adj(N);
+            for (int f = 0; f < Fi; ++f) { adj[mh->owner[f]].push_back(mh->neighbour[f]); adj[mh->neighbour[f]].push_back(mh->owner[f]); }
+            rank = subdomain_bfs_rank(adj, part);
+        } else {
+            std::iota(rank.begin(), rank.end(), 0);
+        }
+        std::vector<int> byrank(N);
+        std::iota(byrank.begin(), byrank.end(), 0);
+        if (bfs_order)
+            std::sort(byrank.begin(), byrank.end(), [&](int a, int b) {
+                return part[a] != part[b] ? part[a] < part[b] : rank[a] < rank[b];
+            });
+        for (int i : byrank) {
             int lv = 0;
             for (int k : lupat[i])
-                if (k < i) lv = std::max(lv, level[k] + 1);
+                if (rank[k] < rank[i]) lv = std::max(lv, level[k] + 1);
             level[i] = lv;
         }
     }
@@ -613,7 +769,8 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     if (factored)
         std::stable_sort(c.perm.begin(), c.perm.end(), [&](int a, int b) {
             if (part[a] != part[b]) return part[a] < part[b];
-            return level[a] < level[b];
+            if (level[a] != level[b]) return level[a] < level[b];
+            return rank[a] < rank[b];
         });
     c.iperm.resize(N);
     for (int r = 0; r < N; ++r) c.iperm[c.perm[r]] = r;
@@ -786,6 +943,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         c.tr_start.upload(tr_start, s); c.tr_kj.upload(tr_kj, s); c.tr_rj.upload(tr_rj, s);
         c.lu_col.upload(lu_col, s); c.lu_src.upload(lu_src, s);
         c.lu_slots = MS;
+        if (o.ilu_bulk) build_task_records(c, o, nparts, part_lvl0, lvl_off, lu_col, nl, nu, ML, MS);
     }
     // ---- AMG hierarchy: plan on the cell graph (original numbering), level
     // 0 in the internal row order; the Galerkin gather lists sum the finer
@@ -926,6 +1084,11 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         CK(cudaMemsetAsync(c.LUval, 0, lbytes, s));
     }
     if (o.precon != PRECON_NONE) CK(cudaMalloc(&c.dinv, (size_t)c.n_slices * 32 * 25 * c.mt_size));
+    if (c.rec_f.p) {
+        if (o.precision == PREC_FP64) ilu_bulk_attr<double>(c);
+        else if (o.precision == PREC_FP32) ilu_bulk_attr<float>(c);
+        else ilu_bulk_attr<__nv_bfloat16>(c);
+    }
     if (o.precon == PRECON_GAUSS_SEIDEL && o.n_sweeps > 1) { c.gs_r.alloc(5L * N); c.gs_z.alloc(5L * N); }
     // ---- Krylov
     const long n5 = 5L * N;
@@ -942,6 +1105,57 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
 }
 
 // ---------------------------------------------------------------- step pieces
+// The bulk-copy apply (factor rows as records, one TMA copy per task):
+// its dynamic shared memory is the stages, the lanes' y0 slots and the x
+// ring when the context has one.
+template <typename MT>
+static size_t ilu_bulk_smem(const rdst_ctx& c) {
+    return (size_t)c.ilu_stages * c.ilu_stage_bytes + (size_t)c.ilu_stages * ILU_BULK_TPB * 8 +
+           (size_t)c.ilu_lb_rows * (sizeof(MT) == 8 ? 96 : 64) + (size_t)c.ilu_task_slots * 8 +
+           (size_t)c.ilu_off_slots * 4;
+}
+template <typename MT, int NS, bool LB>
+static void ilu_bulk_launch(rdst_ctx& c, bool attr_only, const IluDev& P, const double* in, double* out,
+                            const int* active) {
+    const size_t sm = ilu_bulk_smem<MT>(c);
+    if (attr_only) {
+        CK(cudaFuncSetAttribute(k_ilu_apply_bulk<MT, NS, LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        return;
+    }
+    k_ilu_apply_bulk<MT, NS, LB><<<c.n_parts, ILU_BULK_TPB, sm, c.s>>>(P, in, out, active, c.ilu_lb_rows,
+                                                                        c.ilu_stage_bytes, c.ilu_off_slots,
+                                                                        c.ilu_task_slots, &c.sc.p->flags);
+}
+template <typename MT>
+static void ilu_bulk_dispatch(rdst_ctx& c, bool attr_only, const IluDev& P, const double* in, double* out,
+                              const int* active) {
+    const bool lb = c.ilu_lb_rows > 0;
+    if (c.ilu_stages == 3) {
+        if (lb) ilu_bulk_launch<MT, 3, true>(c, attr_only, P, in, out, active);
+        else ilu_bulk_launch<MT, 3, false>(c, attr_only, P, in, out, active);
+    } else {
+        if (lb) ilu_bulk_launch<MT, 2, true>(c, attr_only, P, in, out, active);
+        else ilu_bulk_launch<MT, 2, false>(c, attr_only, P, in, out, active);
+    }
+}
+// dynamic shared memory above the default 48 KB: set once when the
+// context is built (not while a step is being captured)
+template <typename MT>
+static void ilu_bulk_attr(rdst_ctx& c) {
+    ilu_bulk_dispatch<MT>(c, true, c.ilu(), nullptr, nullptr, nullptr);
+}
+template <typename MT>
+static void ilu_apply_bulk(rdst_ctx& c, const IluDev& P, const double* in, double* out, const int* active) {
+    ilu_bulk_dispatch<MT>(c, false, P, in, out, active);
+}
+// blocks of the fresh factors -> the task records
+template <typename MT>
+static void ilu_pack(rdst_ctx& c) {
+    if (!c.rec_f.p) return;
+    k_ilu_pack<MT><<<c.n_slices, 256, 0, c.s>>>(c.N, (const MT*)c.LUval, (const MT*)c.dinv, c.ilu());
+    CKL();
+}
+
 template <typename MT>
 struct Ops {
     static void flux(rdst_ctx& c) {
@@ -1084,6 +1298,7 @@ struct Ops {
             CKL();
             k_ilu_factor<MT><<<c.n_parts, ILU_TPB, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
             CKL();
+            ilu_pack<MT>(c);
         }
     }
     // out = (L U)^-1 in with the stored factors
@@ -1093,12 +1308,16 @@ struct Ops {
         auto P = c.ilu();
         const MT* di = (const MT*)c.dinv;
         const int N = c.N;
-        if (nb <= 2) k_ilu_apply<MT, 2><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-        else if (nb <= 3) k_ilu_apply<MT, 3><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-        else if (nb <= 4) k_ilu_apply<MT, 4><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-        else if (nb <= 6) k_ilu_apply<MT, 6><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-        else if (nb <= 8) k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
-        else k_ilu_apply<MT, 16><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        if (c.rec_f.p) {
+            ilu_apply_bulk<MT>(c, P, in, out, active);
+        } else {
+            if (nb <= 2) k_ilu_apply<MT, 2><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else if (nb <= 3) k_ilu_apply<MT, 3><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else if (nb <= 4) k_ilu_apply<MT, 4><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else if (nb <= 6) k_ilu_apply<MT, 6><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else if (nb <= 8) k_ilu_apply<MT, 8><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+            else k_ilu_apply<MT, 16><<<c.n_parts, ILU_APPLY_TPB, 0, c.s>>>(N, LU, di, P, in, out, active);
+        }
         CKL();
     }
     static void precond(rdst_ctx& c, const double* in, double* out, const int* active) {
@@ -1534,6 +1753,7 @@ void run_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
     CK(cudaMemcpyAsync(&flags, &c.sc.p->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     c.collect_events();
+    if (flags & 4) throw TimeoutError("a bounded wait of the ILU apply expired (bulk copy not completed)");
     if (flags & 2) throw std::domain_error("non-physical state (NaN or non-positive rho/p) after the update");
 }
 
@@ -1702,6 +1922,7 @@ void run_dual_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
     CK(cudaMemcpyAsync(&flags, &c.sc.p->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     c.collect_events();
+    if (flags & 4) throw TimeoutError("a bounded wait of the ILU apply expired (bulk copy not completed)");
     if (flags & 2) throw std::domain_error("non-physical state (NaN or non-positive rho/p) after the update");
 }
 
@@ -1722,6 +1943,9 @@ rdst_status guarded(rdst_ctx* c, F&& fn) {
     } catch (const CudaError& e) {
         c->err = e.what();
         return RDST_ERR_CUDA;
+    } catch (const TimeoutError& e) {
+        c->err = e.what();
+        return RDST_ERR_TIMEOUT;
     } catch (const std::invalid_argument& e) {
         c->err = e.what();
         return RDST_ERR_MESH;
@@ -1898,6 +2122,7 @@ void adj_precond_setup(rdst_ctx& c) {
         CKL();
         k_ilu_factor<MT><<<c.n_parts, ILU_TPB, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
         CKL();
+        ilu_pack<MT>(c);
     }
 }
 

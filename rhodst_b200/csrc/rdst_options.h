@@ -105,6 +105,9 @@ struct Options {
     int basis32 = -1;                 // GMRES basis vectors in FP32 (-1: when precision is not fp64)
     int ilu_parts = 0;                // 0: choose from the mesh size; 1: exact global ILU(0)
     bool ilu_graph = false;           // subdomains by graph bisection (true) or coordinate bisection
+    int ilu_order = -1;               // rows of a subdomain: 0 mesh order, 1 breadth-first (rdst_order.h),
+                                      // -1 breadth-first with more than one subdomain, else mesh order
+    bool ilu_bulk = true;             // ILU apply: task records, one bulk copy per task (same results)
     bool graphs = true;               // capture steps in CUDA graphs
     int device = -1;                  // GPU ordinal of the context (-1: the calling thread's current one)
     bool profile = false;             // event-time kernel classes inside steps
@@ -362,6 +365,13 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
                 throw ConfigError("divSchemes div(tauMC) " + t + " is not on this path (Gauss linear)", true);
         }
         else if (k == "ilu.parts") o.ilu_parts = parse_int(k, v);
+        else if (k == "ilu.bulk") o.ilu_bulk = parse_bool(k, v);
+        else if (k == "ilu.order") {
+            if (t == "natural") o.ilu_order = 0;
+            else if (t == "bfs") o.ilu_order = 1;
+            else if (t == "auto") o.ilu_order = -1;
+            else throw ConfigError("ilu.order must be natural, bfs or auto");
+        }
         else if (k == "ilu.partition") {
             if (t == "rcb") o.ilu_graph = false;
             else if (t == "graph") o.ilu_graph = true;

@@ -139,9 +139,53 @@ def test_cholesky_is_the_diagonal_factorisation_with_cell_triangles():
     assert np.abs(x2 - x).max() > 1e-8 * np.abs(x).max()
 
 
-@pytest.mark.parametrize("parts", [None, 3])
-def test_gauss_seidel_sweeps(parts):
-    c = channel_case("HLL", nx=8, ny=4)
+def bfs_rank(mesh, part):
+    """Breadth-first factorisation order inside each part, restated from
+    its definition: per connected component (by lowest cell), start at a
+    pseudo-peripheral cell (two sweeps from the lowest cell, each taking the
+    lowest cell of the deepest level), then cells by (level, number)."""
+    N, Fi = mesh.n_cells, mesh.n_internal_faces
+    adj = [[] for _ in range(N)]
+    for f in range(Fi):
+        a, b2 = int(mesh.owner[f]), int(mesh.neighbour[f])
+        if part[a] == part[b2]:
+            adj[a].append(b2)
+            adj[b2].append(a)
+
+    def levels(s):
+        d = {s: 0}
+        front = [s]
+        while front:
+            nxt = []
+            for u in front:
+                for v in adj[u]:
+                    if v not in d:
+                        d[v] = d[u] + 1
+                        nxt.append(v)
+            front = nxt
+        return d
+
+    rank = np.full(N, -1)
+    seen = np.zeros(N, bool)
+    count = {}
+    for s0 in range(N):
+        if seen[s0]:
+            continue
+        comp = sorted(levels(s0))
+        seen[comp] = True
+        far = lambda d: min(comp, key=lambda i: (-d[i], i))
+        start = far(levels(far(levels(comp[0]))))
+        d = levels(start)
+        p = int(part[s0])
+        for i in sorted(comp, key=lambda i: (d[i], i)):
+            rank[i] = count.get(p, 0)
+            count[p] = rank[i] + 1
+    return rank
+
+
+@pytest.mark.parametrize("parts,order", [(None, "natural"), (3, "natural"), (3, "bfs")])
+def test_gauss_seidel_sweeps(parts, order):
+    c = channel_case("HLL", nx=8, ny=4).with_options(**{"ilu.order": order})
     N = c.mesh.n_cells
     part = None
     if parts:
@@ -151,7 +195,8 @@ def test_gauss_seidel_sweeps(parts):
     o1 = oracle_for(c.with_options(**{"solvers.W.preconditioner": "GaussSeidel"}), 5, partition=part)
     A, _ = dense_system(o1, c.mesh)
     same = np.ones((N, N), bool) if part is None else (part[:, None] == part[None, :])
-    lowmask = np.kron(np.tril(same, -1), np.ones((5, 5), bool))
+    key = np.arange(N) if order == "natural" else bfs_rank(c.mesh, np.zeros(N, int) if part is None else part)
+    lowmask = np.kron(same & (key[None, :] < key[:, None]), np.ones((5, 5), bool))
     dmask = np.kron(np.eye(N, dtype=bool), np.ones((5, 5), bool))
     DL = np.where(lowmask | dmask, A, 0.0)
     x1 = o1.precondition(b).ravel()
