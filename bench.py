@@ -477,8 +477,9 @@ def main():
         line = {"impl": "reference", "metric": "cell_iterations_per_s", "value": cb["value"], "unit": "cell-iter/s",
                 "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": dict(desc, note="rhoDST needs foam-extend 4.1 (absent); CPU FP64 restatement timed "
-                                          "on all host cores"),
+                "config": dict(desc, precision="fp64 throughout (the oracle has no reduced-precision storage)",
+                               note="rhoDST needs foam-extend 4.1 (absent); CPU FP64 restatement timed "
+                                    "on all host cores"),
                 "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))

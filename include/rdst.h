@@ -109,7 +109,10 @@ typedef struct rdst_step_report {
     double lin_initial[5];     /* linear solver initial residual (normalised)*/
     double lin_final[5];       /* linear solver final residual               */
     int32_t lin_iterations;    /* GMRES restarts / BiCGStab iterations       */
-    int32_t flags;             /* bit0: field bounding was active            */
+    int32_t flags;             /* bit0: field bounding was active;
+                                  bit3: the (last) linear solve stopped at
+                                  maxIter with neither tolerance nor relTol
+                                  reached (foam's converged() false)        */
     double rdt_min, rdt_max;   /* min/max of the local 1/dtau                */
     double t_flux_ms, t_jacobian_ms, t_precond_ms, t_krylov_ms, t_update_ms;
 } rdst_step_report;

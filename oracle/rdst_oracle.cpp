@@ -1566,6 +1566,17 @@ void cmpt_residual(const Vec& r, double nf, double* out) {
     for (int k = 0; k < 5; ++k) out[k] = det_sum((int)r.size(), [&](int i) { return std::fabs(r[i][k]); }) / nf;
 }
 
+// the solver performance's converged(): every component below the
+// tolerance or below relTol x initial (maxIter aside)
+bool tolerances_reached(const Options& o, const double* ini, const double* fin) {
+    bool tol = true, rel = o.rel_tol > 0;
+    for (int k = 0; k < 5; ++k) {
+        if (!(fin[k] < o.tolerance)) tol = false;
+        if (!(fin[k] < o.rel_tol * ini[k])) rel = false;
+    }
+    return tol || rel;
+}
+
 bool converged(const Options& o, const double* ini, const double* fin, int it) {
     if (it < o.min_iter) return false;
     bool tol = true, rel = o.rel_tol > 0;
@@ -2180,7 +2191,7 @@ void single_iterate(Ctx& c, Report& rep) {
     t0 = std::chrono::steady_clock::now();
     if (c.o.turbulence == TURB_SARC1) c.rho0 = c.rho;     // rho.oldTime() of the turbulence update
     update_fields(c, dx);
-    rep.flags = c.bounded ? 1 : 0;
+    rep.flags = (c.bounded ? 1 : 0) | (tolerances_reached(c.o, rep.lin_initial, rep.lin_final) ? 0 : 8);
     if (c.o.turbulence != TURB_LAMINAR && !c.o.frozen_turbulence) sa_correct(c);   // turbulence_.correct()
     set_courant(c, rep);
     rep.t[4] = seconds_since(t0) * 1e3;
@@ -2279,7 +2290,7 @@ void dual_iterate(Ctx& c, Report& rep, double dt, double dt0) {
     // and once after it otherwise (Dual.C:120-121)
     if (turb && !c.o.inner_correct_turbulence && !c.o.frozen_turbulence) sa_correct(c);
     set_courant(c, rep);             // setCourantDST(): residual of R_, converged: physical time step
-    rep.flags = c.bounded ? 1 : 0;
+    rep.flags = (c.bounded ? 1 : 0) | (tolerances_reached(c.o, rep.lin_initial, rep.lin_final) ? 0 : 8);
     rep.lin_iterations = inner;
     c.dual_a = c.dual_b = c.dual_c = 0;
 }

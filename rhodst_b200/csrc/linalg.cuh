@@ -1040,7 +1040,10 @@ __global__ void k_linres_finalize(const double* __restrict__ partial, int nb, Sc
 }
 
 // BlockSolverPerformance check: converged if every component below the
-// tolerance, or below relTol x initial, or maxIter reached (after minIter)
+// tolerance, or below relTol x initial, or maxIter reached (after minIter).
+// A solve that stops on maxIter alone raises bit 3 of the step flags (the
+// solver performance's converged() is false); one that stops on the
+// tolerances clears it.
 __global__ void k_check(Scalars* sc, double tol, double relTol, int minIter, int maxIter, int count) {
     if (threadIdx.x != 0) return;
     if (count) sc->lin_iterations += 1;
@@ -1051,6 +1054,7 @@ __global__ void k_check(Scalars* sc, double tol, double relTol, int minIter, int
         if (!(sc->lin_final[c] < relTol * sc->lin_initial[c])) r = false;
     }
     sc->converged = (it >= minIter) && (t || r || it >= maxIter);
+    if (sc->converged) sc->flags = (t || r) ? (sc->flags & ~8) : (sc->flags | 8);
 }
 
 // ---------------------------------------------------------------- GMRES

@@ -1,7 +1,9 @@
 """foam polyMesh input (rhodst_b200.foam) and the reference's RAE2822
 tutorial case: the reader against the tutorial's own files (when the
-reference tree is present), the stored mesh's geometry, foam's ordering
-checks, and the oracle running the case."""
+reference tree is given by RHODST_REFERENCE, the root of a rhoDST checkout),
+the stored mesh's geometry, foam's ordering checks, and the oracle running
+the case."""
+import os
 from pathlib import Path
 
 import numpy as np
@@ -11,10 +13,13 @@ from rhodst_b200 import cases, foam
 from rhodst_b200 import mesh as M
 
 FIXTURE = Path(__file__).resolve().parent / "golden" / "rae2822_mesh.npz"
-TUTORIAL = Path("/root/reference/tutorials/RAE2822/constant/polyMesh")
+# the reference tree (a rhoDST checkout) when RHODST_REFERENCE names one;
+# the tests that read its tutorial files skip without it
+_REF = Path(os.environ["RHODST_REFERENCE"]) if os.environ.get("RHODST_REFERENCE") else Path("/nonexistent")
+TUTORIAL = _REF / "tutorials/RAE2822/constant/polyMesh"
 
 
-@pytest.mark.skipif(not TUTORIAL.exists(), reason="reference tree not present")
+@pytest.mark.skipif(not TUTORIAL.exists(), reason="RHODST_REFERENCE does not name a reference tree")
 def test_reader_matches_the_stored_tutorial_mesh():
     a = foam.read_polymesh(TUTORIAL)
     b = foam.load_npz(FIXTURE)
@@ -98,10 +103,10 @@ def test_tutorial_case_runs_on_the_oracle():
     assert nut.min() >= 0 and np.isfinite(nut).all()
 
 
-FIELDS = Path("/root/reference/tutorials/RAE2822/0")
+FIELDS = _REF / "tutorials/RAE2822/0"
 
 
-@pytest.mark.skipif(not FIELDS.exists(), reason="reference tree not present")
+@pytest.mark.skipif(not FIELDS.exists(), reason="RHODST_REFERENCE does not name a reference tree")
 def test_tutorial_fields_match_the_case():
     """The tutorial's 0/ fields (with their #include and $ macros) give the
     free stream and boundary conditions cases.rae2822 sets."""
@@ -141,10 +146,10 @@ def test_state_round_trip_through_foam_fields(tmp_path):
     assert q is None
 
 
-CASE = Path("/root/reference/tutorials/RAE2822")
+CASE = _REF / "tutorials/RAE2822"
 
 
-@pytest.mark.skipif(not CASE.exists(), reason="reference tree not present")
+@pytest.mark.skipif(not CASE.exists(), reason="RHODST_REFERENCE does not name a reference tree")
 def test_case_reader_gives_the_tutorial_case():
     """read_case on the tutorial directory yields the options, boundary
     conditions and initial fields cases.rae2822 sets (numerically), names
@@ -188,11 +193,11 @@ def test_dictionary_parser():
     assert d["sub"] == {"x": "yes", "y": '"q w"', "inner": {"z": "1e-5"}}
 
 
-STEP = Path("/root/reference/tutorials/forwardStep")
-STEP_DUAL = Path("/root/reference/tutorials/forwardStepDual")
+STEP = _REF / "tutorials/forwardStep"
+STEP_DUAL = _REF / "tutorials/forwardStepDual"
 
 
-@pytest.mark.skipif(not STEP.exists(), reason="reference tree not present")
+@pytest.mark.skipif(not STEP.exists(), reason="RHODST_REFERENCE does not name a reference tree")
 def test_block_mesh_tutorial_is_the_forward_step():
     """The forwardStep tutorial's blockMeshDict gives the built-in generator's
     mesh at full resolution (same cells, numbering and patches)."""
@@ -211,7 +216,7 @@ def test_block_mesh_tutorial_is_the_forward_step():
     assert np.isfinite(o.step(1)[0]["res_mag"])
 
 
-@pytest.mark.skipif(not STEP_DUAL.exists(), reason="reference tree not present")
+@pytest.mark.skipif(not STEP_DUAL.exists(), reason="RHODST_REFERENCE does not name a reference tree")
 def test_dual_time_tutorial_reads_and_runs():
     from tests.oracle_lib import OracleSolver
     c = foam.read_case(STEP_DUAL)
