@@ -309,18 +309,46 @@ def run_ours(args, rank, world):
     return line, case, s
 
 
-def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
-    """Time to a density-residual drop of `drop` in FP64 and in mixed
-    precision (FP32 Jacobian/ILU/basis; and BF16 Jacobian/ILU with the FP32
-    basis) on the workload's mesh with
-    first-order HLL reconstruction at CFL 500, then the discrete adjoint of
-    the pressure-drag coefficient at the FP64 converged state, its cost
-    against that forward solve and dJ/dMach, dJ/dalpha."""
-    import math
+def _run_to_drop(case, opts, drop, max_steps, chunk=50):
+    """Steps of a fresh context until ||R_rho V||_2 falls by `drop` from the
+    first step's value (or max_steps): steps to the drop, device seconds,
+    the drop history every `chunk` steps, the context."""
     import rhodst_b200
-    first = {"fluxScheme": "HLL", "timeControls": dict(case.options["timeControls"], maxCo=500.0),
-             "interpolationSchemes": {"reconstruct(rho)": "upwind", "reconstruct(U)": "upwind",
-                                      "reconstruct(T)": "upwind"}}
+    s = rhodst_b200.Solver(case.mesh, case.bcs, dict(opts, profile=False))
+    s.set_primitive(case.p, case.U, case.T, case.nuTilda)
+    r0, steps, dev_ms, hit, hist = None, 0, 0.0, None, []
+    while steps < max_steps and hit is None:
+        reps = s.step(chunk)
+        dev_ms += s.last_step_ms()
+        for r in reps:
+            steps += 1
+            if r0 is None:
+                r0 = r["res_l2"][0]
+            if hit is None and r["res_l2"][0] <= drop * r0:
+                hit = steps
+        hist.append(float("%.3g" % (reps[-1]["res_l2"][0] / r0)))
+    return {"steps": hit, "steps_run": steps, "device_s": dev_ms * 1e-3, "final_drop": hist[-1],
+            "history_every_%d" % chunk: hist}, s
+
+
+def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
+    """Time to a density-residual drop of `drop`, FP64 against reduced
+    precision, on three configurations:
+
+    * wing, its own scheme (HLLC, OSPRE/OSPREV, local time step ramped to
+      CFL 50), FP64 and FP32, up to 600 steps: where it stalls, the stall
+      level and the history;
+    * wing, first-order HLL at CFL 500 (a proxy that converges: the
+      speed-up figures of mixed precision), FP64 / FP32 / BF16, with C_l
+      and C_d of each;
+    * C2, the 257x65 turbulent NACA0012 (SAneg, AUSM+up + Venkatakrishnan,
+      CFL 50), FP64, up to 3000 steps;
+
+    then the discrete adjoint of the pressure-drag coefficient at the proxy's
+    FP64 converged state, solved to the same `drop`, its cost against that
+    forward solve, and dJ/dMach, dJ/dalpha."""
+    import math
+    from rhodst_b200 import cases
     g = case.options["thermo"]
     U0 = np.asarray(case.U[0], dtype=float)
     c_inf = math.sqrt(g["Cp"] / (g["Cp"] - g["R"]) * g["R"] * 1.0)
@@ -330,44 +358,54 @@ def convergence_and_adjoint(case, drop: float = 1e-10, max_steps: int = 1500):
     patch = case.force_patch
     ref_area = 0.1 if case.name.startswith("naca") else 1.5 * 0.5 * (1.0 + 0.56)
     qA = 0.5 * (1.0 / (g["R"] * 1.0)) * float(U0 @ U0) * ref_area
-    out = {"drop": drop, "config": "same mesh and free stream, HLL, first-order (upwind) reconstruction, CFL 500",
-           "max_steps": max_steps}
+    out = {"drop": drop}
+    # the configuration's own scheme
+    own = {"config": "the workload's own scheme: HLLC, OSPRE/OSPREV, local time step ramped to CFL 50",
+           "max_steps": 600}
+    for prec in ("fp64", "fp32"):
+        r, s = _run_to_drop(case, dict(case.options, precision=prec), drop, 600)
+        own[prec] = r
+        s.close()
+    out["own_scheme"] = own
+    # first-order proxy
+    first = {"fluxScheme": "HLL", "timeControls": dict(case.options["timeControls"], maxCo=500.0),
+             "interpolationSchemes": {"reconstruct(rho)": "upwind", "reconstruct(U)": "upwind",
+                                      "reconstruct(T)": "upwind"}}
+    prox = {"config": "proxy: same mesh and free stream, HLL, first-order (upwind) reconstruction, CFL 500",
+            "max_steps": max_steps}
     solvers = {}
     for prec in ("fp64", "fp32", "bf16"):
-        opts = dict(case.options, **first, precision=prec, profile=False)
-        s = rhodst_b200.Solver(case.mesh, case.bcs, opts)
-        s.set_primitive(case.p, case.U, case.T)
-        r0, steps, dev_ms, hit = None, 0, 0.0, None
-        while steps < max_steps and hit is None:
-            reps = s.step(50)
-            dev_ms += s.last_step_ms()
-            for r in reps:
-                steps += 1
-                if r0 is None:
-                    r0 = r["res_l2"][0]
-                if hit is None and r["res_l2"][0] <= drop * r0:
-                    hit = steps
+        r, s = _run_to_drop(case, dict(case.options, **first, precision=prec), drop, max_steps)
         f = s.forces(patch, lift, drag, 1.0, qA)
-        out[prec] = {"steps": hit, "steps_run": steps, "device_s": dev_ms * 1e-3,
-                     "final_drop": reps[-1]["res_l2"][0] / r0, "Cl": f["Cl"], "Cd": f["Cd"]}
+        r.update(Cl=f["Cl"], Cd=f["Cd"])
+        prox[prec] = r
         solvers[prec] = s
-    if out["fp64"]["steps"] and out["fp32"]["steps"]:
-        out["speedup_mixed_over_fp64"] = out["fp64"]["device_s"] / out["fp32"]["device_s"]
-    if out["fp64"]["steps"] and out["bf16"]["steps"]:
-        out["speedup_bf16_over_fp64"] = out["fp64"]["device_s"] / out["bf16"]["device_s"]
-    out["Cl_rel_diff"] = abs(out["fp32"]["Cl"] - out["fp64"]["Cl"]) / abs(out["fp64"]["Cl"])
-    out["Cd_rel_diff"] = abs(out["fp32"]["Cd"] - out["fp64"]["Cd"]) / abs(out["fp64"]["Cd"])
-    out["bf16_Cl_rel_diff"] = abs(out["bf16"]["Cl"] - out["fp64"]["Cl"]) / abs(out["fp64"]["Cl"])
-    out["bf16_Cd_rel_diff"] = abs(out["bf16"]["Cd"] - out["fp64"]["Cd"]) / abs(out["fp64"]["Cd"])
-    rep, _ = solvers["fp64"].adjoint(patch, drag, p_ref=1.0, scale=1.0 / qA, rel_tol=1e-8, max_cycles=30,
+    if prox["fp64"]["steps"] and prox["fp32"]["steps"]:
+        prox["speedup_mixed_over_fp64"] = prox["fp64"]["device_s"] / prox["fp32"]["device_s"]
+    if prox["fp64"]["steps"] and prox["bf16"]["steps"]:
+        prox["speedup_bf16_over_fp64"] = prox["fp64"]["device_s"] / prox["bf16"]["device_s"]
+    for p in ("fp32", "bf16"):
+        prox[p + "_Cl_rel_diff"] = abs(prox[p]["Cl"] - prox["fp64"]["Cl"]) / abs(prox["fp64"]["Cl"])
+        prox[p + "_Cd_rel_diff"] = abs(prox[p]["Cd"] - prox["fp64"]["Cd"]) / abs(prox["fp64"]["Cd"])
+    out["first_order_proxy"] = prox
+    # C2 as configured
+    c2 = cases.naca0012_turbulent()
+    r, s = _run_to_drop(c2, c2.options, drop, 3000)
+    r["config"] = "C2: NACA0012 257x65, Re 6.5e6, SAneg, AUSM+up + Venkatakrishnan, CFL 50, GMRES(30) + ILU(0)"
+    out["c2_airfoil_fp64"] = r
+    s.close()
+    # adjoint at the proxy's FP64 state, to the same drop
+    rep, _ = solvers["fp64"].adjoint(patch, drag, p_ref=1.0, scale=1.0 / qA, rel_tol=drop, max_cycles=60,
                                      n_directions=30)
     from rhodst_b200.shape import freestream_derivatives
     dJ_dM, dJ_da = freestream_derivatives(rep["dJ_dU"], rep["force"], U0, c_inf, lift)
     out["adjoint"] = {"objective": f"pressure drag coefficient of patch {patch}", "J": rep["J"],
                       "device_s": rep["t_ms"] * 1e-3, "outer_iterations": rep["iterations"],
                       "residual_drop": rep["residual"] / rep["residual0"],
-                      "cost_over_forward": rep["t_ms"] * 1e-3 / out["fp64"]["device_s"],
+                      "cost_over_forward": rep["t_ms"] * 1e-3 / prox["fp64"]["device_s"],
                       "dJ_dMach": dJ_dM, "dJ_dalpha_per_rad": dJ_da}
+    for s in solvers.values():
+        s.close()
     return out
 
 

@@ -167,6 +167,8 @@ struct Ctx {
     std::vector<std::vector<int>> cellFaces;   // all non-empty faces of each cell
     std::vector<std::vector<int>> cellCells;   // internal-face neighbours
     std::vector<int> part;            // ILU partition (empty: one part)
+    // breadth-first factorisation ranks of the partition they were made for
+    mutable std::vector<int> bfs_rank, bfs_part;
     // thermo
     double R, Cp, Cv, gamma;
     // state: conservative + thermo fields (createFields.H / updateFields.H)
@@ -1300,10 +1302,14 @@ void build_precon(const Ctx& c, const LDU& A, PreconData& M) {
         for (int i = 0; i < (int)c.part.size(); ++i) np = std::max(np, c.part[i] + 1);
         M.rank.clear();
         if (c.o.ilu_order == 1 || (c.o.ilu_order < 0 && np > 1)) {
-            std::vector<std::vector<int>> adj(N);
-            for (int f = 0; f < c.Fi; ++f) { adj[c.own[f]].push_back(c.nei[f]); adj[c.nei[f]].push_back(c.own[f]); }
             std::vector<int> part = c.part.empty() ? std::vector<int>(N, 0) : c.part;
-            M.rank = subdomain_bfs_rank(adj, part);
+            if (c.bfs_rank.empty() || c.bfs_part != part) {      // once per partition
+                std::vector<std::vector<int>> adj(N);
+                for (int f = 0; f < c.Fi; ++f) { adj[c.own[f]].push_back(c.nei[f]); adj[c.nei[f]].push_back(c.own[f]); }
+                c.bfs_rank = subdomain_bfs_rank(adj, part);
+                c.bfs_part = part;
+            }
+            M.rank = c.bfs_rank;
         }
     }
     // Incomplete block LU in factorisation order (IKJ form; order = key(i),
