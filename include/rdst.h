@@ -289,6 +289,13 @@ rdst_status rdst_set_nu_tilda(rdst_ctx* ctx, const double* nut);
  * so a decomposed run moves only its halo cells. */
 rdst_status rdst_get_cells(rdst_ctx* ctx, int32_t n, const int32_t* cells, double* out);
 rdst_status rdst_set_cells(rdst_ctx* ctx, int32_t n, const int32_t* cells, const double* in);
+/* The same with the values in DEVICE memory of the context's GPU (cells
+ * stays a host array): the halo of a decomposed run goes to and from NCCL
+ * without a host copy.  get returns once the values are in out_dev; set
+ * reads in_dev, which must be ready when it is called.  (No counterpart in
+ * the reference, whose processor patches exchange inside foam-extend.) */
+rdst_status rdst_get_cells_device(rdst_ctx* ctx, int32_t n, const int32_t* cells, double* out_dev);
+rdst_status rdst_set_cells_device(rdst_ctx* ctx, int32_t n, const int32_t* cells, const double* in_dev);
 
 /* Host-only helper (no GPU needed): recursive coordinate bisection of the
  * cell centres into n_parts parts, out_part[n_cells].  The GPU library uses

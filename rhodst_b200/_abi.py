@@ -134,6 +134,8 @@ def declare(lib: ctypes.CDLL, prefix: str) -> None:
         f("last_step_ms", c_double, [vp])
         f("kernel_stats", c_int32, [vp, c_char_p, POINTER(ctypes.c_int64), POINTER(c_double)])
         f("set_profile", c_int32, [vp, c_int32])
+        f("get_cells_device", c_int32, [vp, c_int32, POINTER(c_int32), c_void_p])
+        f("set_cells_device", c_int32, [vp, c_int32, POINTER(c_int32), c_void_p])
     if hasattr(lib, prefix + "adjoint"):
         f("objective_gradient", c_int32, [vp, POINTER(RdstObjective), dp, dp, dp, dp])
         f("adjoint_product", c_int32, [vp, dp, dp, dp])
@@ -290,6 +292,19 @@ class Solver:
         v = np.ascontiguousarray(values, dtype=np.float64).reshape(ids.size, 6)
         self._check(self._fn("set_cells")(self._h, ids.size, ids.ctypes.data_as(POINTER(c_int32)), _dptr(v)),
                     "set_cells")
+
+    def get_cells_device(self, cells, out_ptr: int):
+        """States of the listed cells into a device buffer of the context's
+        GPU (n x 6 doubles at out_ptr; B200 library only)."""
+        ids = np.ascontiguousarray(cells, dtype=np.int32)
+        self._check(self._fn("get_cells_device")(self._h, ids.size, ids.ctypes.data_as(POINTER(c_int32)),
+                                                 c_void_p(out_ptr)), "get_cells_device")
+
+    def set_cells_device(self, cells, in_ptr: int):
+        """set_cells from a device buffer (n x 6 doubles at in_ptr, ready)."""
+        ids = np.ascontiguousarray(cells, dtype=np.int32)
+        self._check(self._fn("set_cells_device")(self._h, ids.size, ids.ctypes.data_as(POINTER(c_int32)),
+                                                 c_void_p(in_ptr)), "set_cells_device")
 
     def set_nu_tilda(self, nut):
         """Replace nuTilda between steps (mu_t follows; mean flow and time

@@ -2482,6 +2482,54 @@ RDST_API rdst_status rdst_set_cells(rdst_ctx* c, int32_t n, const int32_t* cells
     });
 }
 
+// the same gather into a DEVICE buffer of the context's GPU (6 doubles per
+// cell), for a halo handed to NCCL without a host copy; returns once the
+// values are in the buffer
+RDST_API rdst_status rdst_get_cells_device(rdst_ctx* c, int32_t n, const int32_t* cells, double* out_dev) {
+    if (!c || n < 0 || (n > 0 && (!cells || !out_dev))) return RDST_ERR_ARG;
+    if (n == 0) return RDST_OK;
+    return guarded(c, [&] {
+        DBuf<int> rows;
+        upload_rows(*c, n, cells, rows);
+        k_get_cells<<<nblk(n, TPB), TPB, 0, c->s>>>(n, rows.p, c->W.p, c->turb ? c->nut.p : nullptr, out_dev);
+        CKL();
+        CK(cudaStreamSynchronize(c->s));
+    });
+}
+
+// rdst_set_cells from a DEVICE buffer of the context's GPU (6 doubles per
+// cell, ready when the call is made)
+RDST_API rdst_status rdst_set_cells_device(rdst_ctx* c, int32_t n, const int32_t* cells, const double* in_dev) {
+    if (!c || n < 0 || (n > 0 && (!cells || !in_dev))) return RDST_ERR_ARG;
+    if (!c->state_set) { c->err = "set_cells needs a state"; return RDST_ERR_ARG; }
+    return guarded(c, [&] {
+        DBuf<int> rows;
+        if (n > 0) {
+            upload_rows(*c, n, cells, rows);
+            k_set_cells<<<nblk(n, TPB), TPB, 0, c->s>>>(n, c->th, rows.p, in_dev, c->W.p, c->prim.p,
+                                                        c->turb ? c->nut.p : nullptr);
+            CKL();
+        }
+        // as rdst_set_conservative between steps: boundary values from the
+        // new internal field, time-control history kept; and mu_t from nuTilda
+        if (c->saSoldValid.p) CK(cudaMemsetAsync(c->saSoldValid.p, 0, sizeof(int), c->s));
+        c->dual_started = false;
+        c->dt_save = c->o.delta_t;
+        const DevMesh& m = c->m;
+        k_boundary<<<nblk(c->NB, TPB), TPB, 0, c->s>>>(m, c->th, c->bd, c->W.p, c->prim.p, c->bs.p);
+        CKL();
+        if (c->turb) {
+            if (m.NB > 0) { k_sa_bc<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->bs.p, c->sa); CKL(); }
+            k_sa_init_mut<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->tr, c->W.p, c->prim.p, c->sa); CKL();
+            k_sa_finish<<<nblk(c->N, TPB), TPB, 0, c->s>>>(c->N, c->o.turbulence == TURB_SANEG, c->W.p, c->nut.p,
+                                                           c->sa);
+            CKL();
+            if (m.NB > 0) { k_sa_mutb<<<nblk(m.NB, TPB), TPB, 0, c->s>>>(m, c->tr, c->bs.p, c->sa); CKL(); }
+        }
+        CK(cudaStreamSynchronize(c->s));
+    });
+}
+
 RDST_API rdst_status rdst_set_held_cells(rdst_ctx* c, const uint8_t* mask) {
     if (!c) return RDST_ERR_ARG;
     return guarded(c, [&] {

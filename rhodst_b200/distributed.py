@@ -72,22 +72,37 @@ class DecomposedSolver:
     def exchange(self):
         """Owned states -> the peers' halo cells: six values per cell (rho,
         rhoU, rhoE, nuTilda), read and written for the send and halo cells
-        only (rdst_get_cells / rdst_set_cells)."""
+        only.  Under NCCL the values stay on the GPU: gathered into torch
+        device buffers by rdst_get_cells_device, sent and received by NCCL,
+        scattered by rdst_set_cells_device; on gloo they go through host
+        arrays (rdst_get_cells / rdst_set_cells)."""
         import torch
+        device_path = self._device == "cuda" and hasattr(self.solver, "get_cells_device")
         reqs, inbox = [], {}
         for q in sorted(self.sub.recv):
             buf = torch.empty((self.sub.recv[q].size, 6), dtype=torch.float64, device=self._device)
             inbox[q] = buf
             reqs.append(self.dist.irecv(buf, src=q, group=self.group))
+        outbox = []
         for q in sorted(self.sub.send):
-            t = torch.from_numpy(self.solver.get_cells(self.sub.send[q])).to(self._device)
+            if device_path:
+                t = torch.empty((self.sub.send[q].size, 6), dtype=torch.float64, device="cuda")
+                self.solver.get_cells_device(self.sub.send[q], t.data_ptr())
+            else:
+                t = torch.from_numpy(self.solver.get_cells(self.sub.send[q])).to(self._device)
+            outbox.append(t)
             reqs.append(self.dist.isend(t, dst=q, group=self.group))
         for r in reqs:
             r.wait()
         if inbox:
             ids = np.concatenate([self.sub.recv[q] for q in sorted(inbox)])
-            vals = np.concatenate([inbox[q].cpu().numpy() for q in sorted(inbox)])
-            self.solver.set_cells(ids, vals)
+            if device_path:
+                vals = torch.cat([inbox[q] for q in sorted(inbox)]).contiguous()
+                torch.cuda.current_stream().synchronize()
+                self.solver.set_cells_device(ids, vals.data_ptr())
+            else:
+                vals = np.concatenate([inbox[q].cpu().numpy() for q in sorted(inbox)])
+                self.solver.set_cells(ids, vals)
 
     def step(self, n: int = 1):
         """n steps, each followed by the halo exchange; this rank's reports."""
