@@ -16,23 +16,45 @@ __device__ __forceinline__ size_t flat_e(int flat, int e) {
     return (size_t)(flat >> 5) * (32 * 25) + (size_t)e * 32 + (flat & 31);
 }
 
-// inverse of a 5x5 block (Gauss-Jordan, partial pivoting), in registers
+// inverse of a 5x5 block (Gauss-Jordan, partial pivoting: the first row
+// with the largest |a[r][c]| below the diagonal), fully unrolled so that the
+// row swaps are selects on registers, not indexed local memory
 __device__ __forceinline__ void inv5(const double A[25], double X[25]) {
     double a[5][10];
 #pragma unroll
     for (int i = 0; i < 5; ++i)
 #pragma unroll
         for (int j = 0; j < 5; ++j) { a[i][j] = A[5 * i + j]; a[i][j + 5] = (i == j) ? 1.0 : 0.0; }
+#pragma unroll
     for (int c = 0; c < 5; ++c) {
         int p = c;
-        for (int r = c + 1; r < 5; ++r) if (fabs(a[r][c]) > fabs(a[p][c])) p = r;
-        if (p != c) for (int j = 0; j < 10; ++j) { double t = a[p][j]; a[p][j] = a[c][j]; a[c][j] = t; }
-        double piv = 1.0 / a[c][c];
+        double best = fabs(a[c][c]);
+#pragma unroll
+        for (int r = c + 1; r < 5; ++r) {
+            const double v = fabs(a[r][c]);
+            if (v > best) { best = v; p = r; }
+        }
+#pragma unroll
+        for (int r = c + 1; r < 5; ++r) {
+            const bool sw = r == p;
+#pragma unroll
+            for (int j = 0; j < 10; ++j) {
+                const double t = a[r][j], u = a[c][j];
+                a[r][j] = sw ? u : t;
+                a[c][j] = sw ? t : u;
+            }
+        }
+        const double piv = 1.0 / a[c][c];
+#pragma unroll
         for (int j = 0; j < 10; ++j) a[c][j] *= piv;
+#pragma unroll
         for (int r = 0; r < 5; ++r) {
             if (r == c) continue;
-            double f = a[r][c];
-            if (f != 0.0) for (int j = 0; j < 10; ++j) a[r][j] -= f * a[c][j];
+            const double f = a[r][c];
+            if (f != 0.0) {
+#pragma unroll
+                for (int j = 0; j < 10; ++j) a[r][j] -= f * a[c][j];
+            }
         }
     }
 #pragma unroll
@@ -265,9 +287,12 @@ __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> A, MT* __res
                                 D[5 * i + j] -= a;
                             }
                     } else {
+#pragma unroll
                         for (int i = 0; i < 5; ++i)
+#pragma unroll
                             for (int j = 0; j < 5; ++j) {
                                 double a = 0;
+#pragma unroll
                                 for (int t2 = 0; t2 < 5; ++t2) a += Lrk[5 * i + t2] * U[5 * t2 + j];
                                 MT* p = lu + flat_e(rj, 5 * i + j);
                                 st(p, ld(p) - a);
@@ -515,47 +540,58 @@ template <typename MT>
 constexpr int ilu_bulk_stages() { return 3; }
 
 // factor blocks -> task records (after each factorisation): one CTA per 32
-// rows, each factor slot staged through shared memory so both the sliced
-// loads and the record stores are contiguous
+// rows.  The slots the chunk's rows use are staged through shared memory
+// (sliced loads contiguous), then each row's values are written as one
+// contiguous run (its record's value area, complete 16-byte sectors): the
+// L blocks forward; the U blocks and the pivot inverse backward.
+template <typename MT>
+__host__ __device__ constexpr int ilu_pack_tile() { return 25 * 33; }
+
 template <typename MT>
 __global__ void __launch_bounds__(256) k_ilu_pack(int N, const MT* __restrict__ lu, const MT* __restrict__ dinv,
                                                   IluDev P) {
-    __shared__ MT tile[25][33];
-    __shared__ int s_nmax[2];
+    extern __shared__ __align__(16) unsigned char s_pack[];
+    MT* tiles = reinterpret_cast<MT*>(s_pack);        // [slots][25][33]
+    __shared__ int s_n[2][32], s_max[2];
+    constexpr int TL = ilu_pack_tile<MT>();
     const int chunk = blockIdx.x, r0 = chunk * 32;
     const int ms = P.ml + P.mu;
-    // slots any row of the chunk uses (the rest of the sliced store is empty)
     if (threadIdx.x < 32) {
         const int r = r0 + threadIdx.x;
         const int nlu = r < N ? P.nlu[r] : 0;
-        int a = nlu & 255, u = P.mu_use ? (nlu >> 8) & 255 : 0;
+        int nl = nlu & 255, nu = P.mu_use ? (nlu >> 8) & 255 : 0;
+        s_n[0][threadIdx.x] = r < N ? nl : -1;
+        s_n[1][threadIdx.x] = r < N ? nu : -1;
         for (int o = 16; o > 0; o >>= 1) {
-            a = max(a, __shfl_xor_sync(0xffffffffu, a, o));
-            u = max(u, __shfl_xor_sync(0xffffffffu, u, o));
+            nl = max(nl, __shfl_xor_sync(0xffffffffu, nl, o));
+            nu = max(nu, __shfl_xor_sync(0xffffffffu, nu, o));
         }
-        if (threadIdx.x == 0) { s_nmax[0] = a; s_nmax[1] = u; }
+        if (threadIdx.x == 0) { s_max[0] = nl; s_max[1] = nu; }
     }
     __syncthreads();
-    const int lmax = s_nmax[0], umax = s_nmax[1];
-    for (int sl = 0; sl <= ms; ++sl) {            // sl == ms: the pivot inverses
-        if (sl < P.ml ? sl >= lmax : (sl < ms && sl - P.ml >= umax)) continue;
-        const MT* src = sl < ms ? lu + (size_t)(chunk * ms + sl) * 800 : dinv + (size_t)chunk * 800;
+    for (int side = 0; side < 2; ++side) {
+        const int nmax = s_max[side];
+        const int ntile = side == 0 ? nmax : nmax + 1;     // backward: U slots, then the pivot inverses
+        for (int t = 0; t < ntile; ++t) {
+            const MT* src = side == 0 ? lu + (size_t)(chunk * ms + t) * 800
+                                      : (t < nmax ? lu + (size_t)(chunk * ms + P.ml + t) * 800
+                                                  : dinv + (size_t)chunk * 800);
+            for (int i = threadIdx.x; i < 800; i += blockDim.x) tiles[t * TL + (i >> 5) * 33 + (i & 31)] = src[i];
+        }
         __syncthreads();
-        for (int i = threadIdx.x; i < 800; i += blockDim.x) tile[i >> 5][i & 31] = src[i];
-        __syncthreads();
-        for (int i = threadIdx.x; i < 800; i += blockDim.x) {
-            const int row = i / 25, e = i - 25 * (i / 25), r = r0 + row;
-            if (r >= N) continue;
-            const int nl = P.nlu[r] & 255, nu = P.mu_use ? (P.nlu[r] >> 8) & 255 : 0;
-            if (sl < P.ml) {
-                if (sl < nl) reinterpret_cast<MT*>(P.rec_f + (size_t)P.val_f[r] * 16)[25 * sl + e] = tile[e][row];
-            } else if (sl < ms) {
-                const int q = sl - P.ml;
-                if (q < nu) reinterpret_cast<MT*>(P.rec_b + (size_t)P.val_b[r] * 16)[25 * q + e] = tile[e][row];
-            } else {
-                reinterpret_cast<MT*>(P.rec_b + (size_t)P.val_b[r] * 16)[25 * nu + e] = tile[e][row];
+        for (int row = 0; row < 32; ++row) {
+            const int n = s_n[side][row];
+            if (n < 0) break;
+            const int words = 25 * (side == 0 ? n : n + 1);
+            MT* dst = reinterpret_cast<MT*>((side == 0 ? P.rec_f + (size_t)P.val_f[r0 + row] * 16
+                                                       : P.rec_b + (size_t)P.val_b[r0 + row] * 16));
+            for (int w = threadIdx.x; w < words; w += blockDim.x) {
+                const int q = w / 25, e = w - 25 * q;
+                const int t = (side == 1 && q == n) ? nmax : q;
+                dst[w] = tiles[t * TL + e * 33 + row];
             }
         }
+        __syncthreads();
     }
 }
 

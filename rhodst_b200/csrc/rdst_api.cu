@@ -611,6 +611,7 @@ void build_task_records(rdst_ctx& c, const Options& o, int nparts, const std::ve
     int ns = 3;
     if ((smem(3) + reserved) * want > (size_t)per_sm) ns = 2;
     if (smem(ns) > (size_t)per_block) return;
+    if ((size_t)(std::max(ML, MS - ML) + 1) * 25 * 33 * S > (size_t)per_block) return;   // the pack's tiles
     std::vector<unsigned char> bf(totf, 0), bb(totb, 0);
     std::vector<unsigned> vf(N, 0), vb(N, 0);
     auto fill = [&](const std::vector<Tk>& tasks, const std::vector<uint2>& tab, bool back,
@@ -1108,6 +1109,11 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
 // The bulk-copy apply (factor rows as records, one TMA copy per task):
 // its dynamic shared memory is the stages, the lanes' y0 slots and the x
 // ring when the context has one.
+// the pack's shared memory: the widest side's slots (L, or U + pivot inverse)
+template <typename MT>
+static size_t ilu_pack_smem(const rdst_ctx& c) {
+    return (size_t)(std::max(c.ilu_ml, c.ilu_mu) + 1) * ilu_pack_tile<MT>() * sizeof(MT);
+}
 template <typename MT>
 static size_t ilu_bulk_smem(const rdst_ctx& c) {
     return (size_t)c.ilu_stages * c.ilu_stage_bytes + (size_t)c.ilu_stages * ILU_BULK_TPB * 8 +
@@ -1143,6 +1149,7 @@ static void ilu_bulk_dispatch(rdst_ctx& c, bool attr_only, const IluDev& P, cons
 template <typename MT>
 static void ilu_bulk_attr(rdst_ctx& c) {
     ilu_bulk_dispatch<MT>(c, true, c.ilu(), nullptr, nullptr, nullptr);
+    CK(cudaFuncSetAttribute(k_ilu_pack<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ilu_pack_smem<MT>(c)));
 }
 template <typename MT>
 static void ilu_apply_bulk(rdst_ctx& c, const IluDev& P, const double* in, double* out, const int* active) {
@@ -1152,7 +1159,8 @@ static void ilu_apply_bulk(rdst_ctx& c, const IluDev& P, const double* in, doubl
 template <typename MT>
 static void ilu_pack(rdst_ctx& c) {
     if (!c.rec_f.p) return;
-    k_ilu_pack<MT><<<c.n_slices, 256, 0, c.s>>>(c.N, (const MT*)c.LUval, (const MT*)c.dinv, c.ilu());
+    k_ilu_pack<MT><<<c.n_slices, 256, ilu_pack_smem<MT>(c), c.s>>>(c.N, (const MT*)c.LUval, (const MT*)c.dinv,
+                                                                   c.ilu());
     CKL();
 }
 
