@@ -451,10 +451,14 @@ int lim_code(Limiter l) { return (int)l; }
 // 1184).  The bulk apply holds eight CTAs an SM (64 registers a thread, its
 // shared memory sized for that), the register apply four.
 int auto_ilu_parts(int N, Precision prec, bool bulk) {
-    const int p0 = std::max(1, N / 1536);
     int dev = 0, sms = 0, per_sm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // a small mesh still gets one subdomain per SM, down to 128 rows each:
+    // with a few large subdomains the apply is one long level chain on a few
+    // SMs (257x65 C-mesh: 10 subdomains 259 us per apply, 130 subdomains
+    // 104 us, and 280 steps to a 1e-10 drop instead of 284)
+    const int p0 = std::max({1, N / 1536, std::min(sms, N / 128)});
     // the four-slot instance bounds the register use of the ones hex meshes need
     if (bulk)
         per_sm = 8;

@@ -166,7 +166,7 @@ def test_c4_frozen_turbulence_gradient_vs_central_differences(problem):
     J.backward()
     g_a, g_M, g_al = a.grad.numpy(), float(mach.grad), float(alpha.grad)
     assert g_a.shape == (64,) and np.all(np.isfinite(g_a))
-    J0 = problem.solver.objective_gradient("airfoil", problem.drag(float(alpha)), p_ref=1.0,
+    J0 = problem.solver.objective_gradient("airfoil", problem.drag(alpha.item()), p_ref=1.0,
                                            scale=1.0 / problem.q_area)[0]
     assert J.item() == pytest.approx(J0, rel=1e-14)
     h = 1e-6
