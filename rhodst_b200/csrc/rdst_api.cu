@@ -1308,7 +1308,7 @@ struct Ops {
             const int n_fid = c.n_slices * c.lu_slots * 32;
             k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, c.lu_src.p, n_fid);
             CKL();
-            k_ilu_factor<MT><<<c.n_parts, ILU_TPB, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
+            k_ilu_factor<MT><<<c.n_parts, c.o.ilu_factor_threads, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
             CKL();
             ilu_pack<MT>(c);
         }
@@ -2132,7 +2132,7 @@ void adj_precond_setup(rdst_ctx& c) {
         const int n_fid = c.n_slices * c.lu_slots * 32;
         k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, c.lu_src.p, n_fid);
         CKL();
-        k_ilu_factor<MT><<<c.n_parts, ILU_TPB, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
+        k_ilu_factor<MT><<<c.n_parts, c.o.ilu_factor_threads, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
         CKL();
         ilu_pack<MT>(c);
     }

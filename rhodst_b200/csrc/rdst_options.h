@@ -108,6 +108,7 @@ struct Options {
     int ilu_order = -1;               // rows of a subdomain: 0 mesh order, 1 breadth-first (rdst_order.h),
                                       // -1 breadth-first with more than one subdomain, else mesh order
     bool ilu_bulk = true;             // ILU apply: task records, one bulk copy per task (same results)
+    int ilu_factor_threads = 32;      // threads of the factorisation's CTA (one CTA per subdomain): 32, 64 or 128
     bool graphs = true;               // capture steps in CUDA graphs
     int device = -1;                  // GPU ordinal of the context (-1: the calling thread's current one)
     bool profile = false;             // event-time kernel classes inside steps
@@ -366,6 +367,11 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
         }
         else if (k == "ilu.parts") o.ilu_parts = parse_int(k, v);
         else if (k == "ilu.bulk") o.ilu_bulk = parse_bool(k, v);
+        else if (k == "ilu.factorThreads") {
+            o.ilu_factor_threads = parse_int(k, v);
+            if (o.ilu_factor_threads != 32 && o.ilu_factor_threads != 64 && o.ilu_factor_threads != 128)
+                throw ConfigError("ilu.factorThreads must be 32, 64 or 128");
+        }
         else if (k == "ilu.order") {
             if (t == "natural") o.ilu_order = 0;
             else if (t == "bfs") o.ilu_order = 1;
