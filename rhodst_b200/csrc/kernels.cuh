@@ -593,7 +593,7 @@ __device__ __forceinline__ void face_recon(const DevMesh& m, int f, int lr, int 
 }
 
 // Face fluxes of all internal faces (reconstruction + scheme), AoS output.
-__global__ void __launch_bounds__(128) k_face_flux(DevMesh m, Thermo th, int scheme, int lr, int lu, int lt,
+__global__ void __launch_bounds__(128, 4) k_face_flux(DevMesh m, Thermo th, int scheme, int lr, int lu, int lt,
                                                    int lowMach, double Mainf, const double* __restrict__ q,
                                                    const double* __restrict__ g, const double* __restrict__ psi,
                                                    const double* __restrict__ fcell, double* __restrict__ fl,
@@ -830,19 +830,113 @@ __device__ __forceinline__ size_t sidx(const int* slice_off, int r, int k, int e
     return slot * (32 * 25) + (size_t)e * 32 + (r & 31);
 }
 
+// Entry e of the convective flux Jacobian calcJ (physics.cuh) with the same
+// operations, for a loop that needs one entry at a time (e a constant after
+// unrolling): no 25-entry array stays live.
+__device__ __forceinline__ double calcJ_entry(int e, const V3& Uf, double gammaf, double phiJf, double a1f,
+                                              const V3& n, double Un) {
+    const double U[3] = {Uf.x, Uf.y, Uf.z};
+    const double N[3] = {n.x, n.y, n.z};
+    const int i = e / 5, c = e % 5;
+    if (i == 0) return (c >= 1 && c <= 3) ? N[c - 1] : 0.0;
+    if (i == 4) {
+        if (c == 0) return Un * (phiJf - a1f);
+        if (c == 4) return gammaf * Un;
+        return a1f * N[c - 1] - Un * (gammaf - 1) * U[c - 1];
+    }
+    const int k = i - 1;
+    if (c == 0) return phiJf * N[k] - U[k] * Un;
+    if (c == 4) return (gammaf - 1) * N[k];
+    const int l = c - 1;
+    return U[k] * N[l] + (k == l ? Un : 0.0) - (gammaf - 1) * (N[k] * U[l]);
+}
+
+// Roe::computeBoundaryJacobians (Roe.C:274-379), one thread per active
+// boundary face: the block (dR/dX) diag(valueInternalCoeffs) (dX/dW) that
+// k_assemble adds to the diagonal of the face's cell.
+__global__ void k_bjac(DevMesh m, Thermo th, const double* __restrict__ W, const double* __restrict__ prim,
+                       const double* __restrict__ bs, double* __restrict__ bjac) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.NB) return;
+    const int r = m.bcell[b];
+    const DevPatch P = m.patches[m.bpatch[b]];
+    const double* B = bs + BW * b;
+    const V3 pSf = ldv3(m.bSf, m.NB, b);
+    const V3 nrm = div3(pSf, m.bmagSf[b]);
+    V3 UB = div3(mk(B[1], B[2], B[3]), B[0]);
+    double pB = B[5], TB = B[6], rhoB = B[0], EB = B[4] / B[0];
+    double rRT = rhoB / pB;
+    double UBS = dot3(UB, pSf);
+    const double Sv[3] = {pSf.x, pSf.y, pSf.z}, Uv[3] = {UB.x, UB.y, UB.z};
+    double dR[25];
+    dR[0] = UBS * rRT;
+    for (int k2 = 0; k2 < 3; ++k2) dR[1 + k2] = rhoB * Sv[k2];
+    dR[4] = -rhoB / TB * UBS;
+    for (int k2 = 0; k2 < 3; ++k2) {
+        dR[(1 + k2) * 5 + 0] = rRT * UBS * Uv[k2] + Sv[k2];
+        for (int l = 0; l < 3; ++l) dR[(1 + k2) * 5 + 1 + l] = rhoB * Uv[k2] * Sv[l] + (k2 == l ? rhoB * UBS : 0.0);
+        dR[(1 + k2) * 5 + 4] = -rhoB / TB * UBS * Uv[k2];
+    }
+    dR[20] = (EB * rRT + 1) * UBS;
+    for (int l = 0; l < 3; ++l) dR[21 + l] = rhoB * UBS * Uv[l] + Sv[l] * (rhoB * EB + pB);
+    dR[24] = rhoB * th.Cv * UBS;
+    // dX/dW at the internal cell
+    const double* w5 = W + 5 * r;
+    const V3 UI = div3(mk(w5[1], w5[2], w5[3]), w5[0]);
+    const double UIv[3] = {UI.x, UI.y, UI.z};
+    double rhoEI = w5[4], pI = prim[PW * r], rRho = 1.0 / w5[0];
+    double rRhoCv = rRho / th.Cv;
+    double e = rhoEI * rRho - 0.5 * magSqr3(UI);
+    double RT = pI * rRho;
+    double RCv = RT / e;
+    double dX[25];
+#pragma unroll
+    for (int q2 = 0; q2 < 25; ++q2) dX[q2] = 0.0;
+    dX[0] = RT - RCv * (e - 0.5 * magSqr3(UI));
+    for (int l = 0; l < 3; ++l) dX[1 + l] = -RCv * UIv[l];
+    dX[4] = RCv;
+    for (int k2 = 0; k2 < 3; ++k2) { dX[(1 + k2) * 5] = -rRho * UIv[k2]; dX[(1 + k2) * 5 + 1 + k2] = rRho; }
+    dX[20] = rRhoCv * (0.5 * magSqr3(UI) - e);
+    for (int l = 0; l < 3; ++l) dX[21 + l] = -rRhoCv * UIv[l];
+    dX[24] = rRhoCv;
+    // valueInternalCoeffs: 1 - valueFraction (mixed types), basicSymmetry
+    double cdiag[5];
+    cdiag[0] = 1.0 - B[8];
+    cdiag[4] = 1.0 - B[10];
+    if (P.bc_U == 3 || P.bc_U == 4) {
+        cdiag[1] = 1 - fabs(nrm.x); cdiag[2] = 1 - fabs(nrm.y); cdiag[3] = 1 - fabs(nrm.z);
+    } else { cdiag[1] = cdiag[2] = cdiag[3] = 1.0 - B[9]; }
+    // pic = (dR . diag(cdiag)) . dX
+    for (int a = 0; a < 5; ++a) {
+        double t1[5];
+        for (int c2 = 0; c2 < 5; ++c2) {
+            double acc2 = 0;
+            for (int k2 = 0; k2 < 5; ++k2) acc2 += dR[5 * a + k2] * (k2 == c2 ? cdiag[k2] : 0.0);
+            t1[c2] = acc2;
+        }
+        for (int c2 = 0; c2 < 5; ++c2) {
+            double acc2 = 0;
+            for (int k2 = 0; k2 < 5; ++k2) acc2 += t1[k2] * dX[5 * k2 + c2];
+            bjac[25 * (size_t)b + 5 * a + c2] = acc2;
+        }
+    }
+}
+
 // Roe Jacobian blocks (Roe.C:152-214) assembled straight into the SELL
 // matrix, one row (cell) per thread: off-diagonal (row, column) blocks from
 // the face's upper (row = owner) / lower (row = neighbour) coefficient,
-// the diagonal as ddt + negSumDiag + boundary Jacobians (fluxDST.C:98-112),
-// accumulated in foam face order.
+// the diagonal as ddt + negSumDiag + boundary Jacobians (fluxDST.C:98-112,
+// the latter from k_bjac), accumulated in foam face order.  The flux
+// Jacobians of the two cells are formed entry by entry inside the block
+// loop, which keeps a thread's registers to about the diagonal block.
 template <typename MT>
-__global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, Transport tr, SellMat<MT> A,
-                                                  const int* __restrict__ cf_slot,
-                                                  const double* __restrict__ W, const double* __restrict__ prim,
-                                                  const double* __restrict__ bs, const double* __restrict__ rdtc,
-                                                  const double* __restrict__ mut,
-                                                  const Scalars* __restrict__ sc, int steady, double beta,
-                                                  double dual_a) {
+__global__ void __launch_bounds__(128, 4) k_assemble(DevMesh m, Thermo th, Transport tr, SellMat<MT> A,
+                                                     const int* __restrict__ cf_slot,
+                                                     const double* __restrict__ W, const double* __restrict__ prim,
+                                                     const double* __restrict__ bjac, const double* __restrict__ rdtc,
+                                                     const double* __restrict__ mut,
+                                                     const Scalars* __restrict__ sc, int steady, double beta,
+                                                     double dual_a) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= m.N) return;
     const double g = th.gamma;
@@ -864,7 +958,6 @@ __global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, Transpor
     V3 Ur;
     double phiJr, a1r, cr;
     cellJ(r, Ur, phiJr, a1r, cr);
-    double J[25], Jc[25];
     for (int k = m.cf_start[r]; k < m.cf_start[r + 1]; ++k) {
         int code = m.cf_list[k];
         if (code < m.Fi) {
@@ -896,96 +989,35 @@ __global__ void __launch_bounds__(128) k_assemble(DevMesh m, Thermo th, Transpor
             } else {
                 lambda = 0.5 * amaxSf;
             }
-            calcJ(Ur, g, phiJr, a1r, nn, J);
-            calcJ(Uc, g, phiJc, a1c, nn, Jc);
+            const double Unr = dot3(Ur, nn), Unc = dot3(Uc, nn);
             const int cs = cf_slot[k];
             const bool accum = cs < 0;          // further face of an already written cell pair
             const int slot = accum ? -cs - 1 : cs;
-            if (isOwner) {
+            MT* p0 = &A.val[sidx(A.slice_off, r, slot, 0)];
+            // owner row: D -= lower(J_r), A_rc = upper(J_c); neighbour row:
+            // D -= upper(J_r), A_rc = lower(J_c)
+            const double wr = isOwner ? wf : 1 - wf, wc = isOwner ? 1 - wf : wf;
 #pragma unroll
-                for (int e = 0; e < 25; ++e) {
-                    double I = (e % 6 == 0) ? 1.0 : 0.0;
-                    double lower = -beta * ((J[e] * wf) * magS + I * lambda);
-                    D[e] -= lower;
-                    double upper = beta * ((Jc[e] * (1 - wf)) * magS - I * lambda);
-                    MT* p = &A.val[sidx(A.slice_off, r, slot, e)];
-                    st(p, accum ? ld(p) + upper : upper);
+            for (int e = 0; e < 25; ++e) {
+                const double I = (e % 6 == 0) ? 1.0 : 0.0;
+                const double J = calcJ_entry(e, Ur, g, phiJr, a1r, nn, Unr);
+                const double Jc = calcJ_entry(e, Uc, g, phiJc, a1c, nn, Unc);
+                double dsub, offd;
+                if (isOwner) {
+                    dsub = -beta * ((J * wr) * magS + I * lambda);
+                    offd = beta * ((Jc * wc) * magS - I * lambda);
+                } else {
+                    dsub = beta * ((J * wr) * magS - I * lambda);
+                    offd = -beta * ((Jc * wc) * magS + I * lambda);
                 }
-            } else {
-#pragma unroll
-                for (int e = 0; e < 25; ++e) {
-                    double I = (e % 6 == 0) ? 1.0 : 0.0;
-                    double upper = beta * ((J[e] * (1 - wf)) * magS - I * lambda);
-                    D[e] -= upper;
-                    double lower = -beta * ((Jc[e] * wf) * magS + I * lambda);
-                    MT* p = &A.val[sidx(A.slice_off, r, slot, e)];
-                    st(p, accum ? ld(p) + lower : lower);
-                }
+                D[e] -= dsub;
+                MT* p = p0 + e * 32;
+                st(p, accum ? ld(p) + offd : offd);
             }
         } else {
-            // Roe::computeBoundaryJacobians (Roe.C:274-379)
-            const int b = code - m.Fi;
-            const DevPatch P = m.patches[m.bpatch[b]];
-            const double* B = bs + BW * b;
-            const V3 pSf = ldv3(m.bSf, m.NB, b);
-            const V3 nrm = div3(pSf, m.bmagSf[b]);
-            V3 UB = div3(mk(B[1], B[2], B[3]), B[0]);
-            double pB = B[5], TB = B[6], rhoB = B[0], EB = B[4] / B[0];
-            double rRT = rhoB / pB;
-            double UBS = dot3(UB, pSf);
-            const double Sv[3] = {pSf.x, pSf.y, pSf.z}, Uv[3] = {UB.x, UB.y, UB.z};
-            double dR[25];
-            dR[0] = UBS * rRT;
-            for (int k2 = 0; k2 < 3; ++k2) dR[1 + k2] = rhoB * Sv[k2];
-            dR[4] = -rhoB / TB * UBS;
-            for (int k2 = 0; k2 < 3; ++k2) {
-                dR[(1 + k2) * 5 + 0] = rRT * UBS * Uv[k2] + Sv[k2];
-                for (int l = 0; l < 3; ++l) dR[(1 + k2) * 5 + 1 + l] = rhoB * Uv[k2] * Sv[l] + (k2 == l ? rhoB * UBS : 0.0);
-                dR[(1 + k2) * 5 + 4] = -rhoB / TB * UBS * Uv[k2];
-            }
-            dR[20] = (EB * rRT + 1) * UBS;
-            for (int l = 0; l < 3; ++l) dR[21 + l] = rhoB * UBS * Uv[l] + Sv[l] * (rhoB * EB + pB);
-            dR[24] = rhoB * th.Cv * UBS;
-            // dX/dW at the internal cell
-            const double* w5 = W + 5 * r;
-            V3 UI = Ur;
-            const double UIv[3] = {UI.x, UI.y, UI.z};
-            double rhoEI = w5[4], pI = prim[PW * r], rRho = 1.0 / w5[0];
-            double rRhoCv = rRho / th.Cv;
-            double e = rhoEI * rRho - 0.5 * magSqr3(UI);
-            double RT = pI * rRho;
-            double RCv = RT / e;
-            double dX[25];
+            const double* pj = bjac + 25 * (size_t)(code - m.Fi);
 #pragma unroll
-            for (int q2 = 0; q2 < 25; ++q2) dX[q2] = 0.0;
-            dX[0] = RT - RCv * (e - 0.5 * magSqr3(UI));
-            for (int l = 0; l < 3; ++l) dX[1 + l] = -RCv * UIv[l];
-            dX[4] = RCv;
-            for (int k2 = 0; k2 < 3; ++k2) { dX[(1 + k2) * 5] = -rRho * UIv[k2]; dX[(1 + k2) * 5 + 1 + k2] = rRho; }
-            dX[20] = rRhoCv * (0.5 * magSqr3(UI) - e);
-            for (int l = 0; l < 3; ++l) dX[21 + l] = -rRhoCv * UIv[l];
-            dX[24] = rRhoCv;
-            // valueInternalCoeffs: 1 - valueFraction (mixed types), basicSymmetry
-            double cdiag[5];
-            cdiag[0] = 1.0 - B[8];
-            cdiag[4] = 1.0 - B[10];
-            if (P.bc_U == 3 || P.bc_U == 4) {
-                cdiag[1] = 1 - fabs(nrm.x); cdiag[2] = 1 - fabs(nrm.y); cdiag[3] = 1 - fabs(nrm.z);
-            } else { cdiag[1] = cdiag[2] = cdiag[3] = 1.0 - B[9]; }
-            // pic = (dR . diag(cdiag)) . dX
-            for (int a = 0; a < 5; ++a) {
-                double t1[5];
-                for (int c2 = 0; c2 < 5; ++c2) {
-                    double acc2 = 0;
-                    for (int k2 = 0; k2 < 5; ++k2) acc2 += dR[5 * a + k2] * (k2 == c2 ? cdiag[k2] : 0.0);
-                    t1[c2] = acc2;
-                }
-                for (int c2 = 0; c2 < 5; ++c2) {
-                    double acc2 = 0;
-                    for (int k2 = 0; k2 < 5; ++k2) acc2 += t1[k2] * dX[5 * k2 + c2];
-                    D[5 * a + c2] += beta * acc2;
-                }
-            }
+            for (int e = 0; e < 25; ++e) D[e] += beta * pj[e];
         }
     }
 #pragma unroll

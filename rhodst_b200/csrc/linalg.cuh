@@ -5,6 +5,8 @@
 // double, float or bf16; vectors, dot products, Hessenberg and norms are FP64.
 #pragma once
 
+#include <climits>
+
 #include "kernels.cuh"
 
 namespace rdst {
@@ -16,22 +18,28 @@ __device__ __forceinline__ size_t flat_e(int flat, int e) {
     return (size_t)(flat >> 5) * (32 * 25) + (size_t)e * 32 + (flat & 31);
 }
 
+// compute type of the block factorisations for storage type MT: FP64
+// storage in double, FP32 and BF16 storage in float
+template <typename MT> struct IluCT { using T = float; };
+template <> struct IluCT<double> { using T = double; };
+
 // inverse of a 5x5 block (Gauss-Jordan, partial pivoting: the first row
 // with the largest |a[r][c]| below the diagonal), fully unrolled so that the
 // row swaps are selects on registers, not indexed local memory
-__device__ __forceinline__ void inv5(const double A[25], double X[25]) {
-    double a[5][10];
+template <typename T>
+__device__ __forceinline__ void inv5(const T A[25], T X[25]) {
+    T a[5][10];
 #pragma unroll
     for (int i = 0; i < 5; ++i)
 #pragma unroll
-        for (int j = 0; j < 5; ++j) { a[i][j] = A[5 * i + j]; a[i][j + 5] = (i == j) ? 1.0 : 0.0; }
+        for (int j = 0; j < 5; ++j) { a[i][j] = A[5 * i + j]; a[i][j + 5] = (i == j) ? T(1) : T(0); }
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
         int p = c;
-        double best = fabs(a[c][c]);
+        T best = fabs(a[c][c]);
 #pragma unroll
         for (int r = c + 1; r < 5; ++r) {
-            const double v = fabs(a[r][c]);
+            const T v = fabs(a[r][c]);
             if (v > best) { best = v; p = r; }
         }
 #pragma unroll
@@ -39,19 +47,19 @@ __device__ __forceinline__ void inv5(const double A[25], double X[25]) {
             const bool sw = r == p;
 #pragma unroll
             for (int j = 0; j < 10; ++j) {
-                const double t = a[r][j], u = a[c][j];
+                const T t = a[r][j], u = a[c][j];
                 a[r][j] = sw ? u : t;
                 a[c][j] = sw ? t : u;
             }
         }
-        const double piv = 1.0 / a[c][c];
+        const T piv = T(1) / a[c][c];
 #pragma unroll
         for (int j = 0; j < 10; ++j) a[c][j] *= piv;
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
             if (r == c) continue;
-            const double f = a[r][c];
-            if (f != 0.0) {
+            const T f = a[r][c];
+            if (f != T(0)) {
 #pragma unroll
                 for (int j = 0; j < 10; ++j) a[r][j] -= f * a[c][j];
             }
@@ -213,6 +221,19 @@ struct IluDev {
     const int* part_tb;
     const unsigned* val_f;
     const unsigned* val_b;
+    // the factorisation written straight into the records (null: gather,
+    // factor and pack instead).  Per update triple (tr_start ranges):
+    // fr_trk: where U_kj is read, the flat SELL slot of A_kj (>= 0), factor
+    // id fid of the sliced store as -fid - 1 (row k takes updates of its
+    // own), or INT_MIN (a fill block of a row without updates: zero);
+    // fr_trt: -1 the diagonal, else the slot of row r that takes it.
+    // fr_desc[low_start[r] + q]: (column k of L_q, flat SELL slot of A_rk or
+    // -2 for a fill, fr_trk of the slot's first triple, its fr_trt + 2 or 0
+    // for none, | 1 << 20 when more triples follow).
+    // nlu bit 16: the row updates one of its own off-diagonal slots.
+    const int* fr_trk;
+    const int* fr_trt;
+    const int4* fr_desc;
 };
 
 __device__ __forceinline__ int lu_fid(int r, int s, int ms) { return ((r >> 5) * ms + s) * 32 + (r & 31); }
@@ -237,51 +258,54 @@ __global__ void k_ilu_gather(SellMat<MT> A, MT* __restrict__ lu, const int* __re
     for (int e = 0; e < 25; ++e) lu[flat_e(fid, e)] = A.val[flat_e(src, e)];
 }
 
+// Level-scheduled subdomain factorisation into the factor store: one CTA
+// per subdomain, a thread per row of the current level, in the compute
+// type of the storage (IluCT).
 template <typename MT>
 __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> A, MT* __restrict__ lu, MT* __restrict__ dinv,
                                                         IluDev P) {
+    using CT = typename IluCT<MT>::T;
     const int part = blockIdx.x;
-    const int N = A.N;
     const int ms = P.ml + P.mu;
     for (int l = P.part_lvl0[part]; l < P.part_lvl0[part + 1]; ++l) {
         for (int r = P.lvl_off[l] + threadIdx.x; r < P.lvl_off[l + 1]; r += blockDim.x) {
             const int nl = P.nlu[r] & 255;
             const MT* dv = A.val + (size_t)A.slice_off[r >> 5] * (32 * 25) + (r & 31);
-            double D[25];
+            CT D[25];
 #pragma unroll
-            for (int e = 0; e < 25; ++e) D[e] = ld(dv + e * 32);
+            for (int e = 0; e < 25; ++e) D[e] = ct_ld(dv + e * 32);
             const int q0 = P.low_start[r];
             for (int q = 0; q < nl; ++q) {
                 const int fq = lu_fid(r, q, ms);
                 const int k = P.lu_col[fq];
-                double Ark[25], Dk[25], Lrk[25];
+                CT Ark[25], Dk[25], Lrk[25];
 #pragma unroll
                 for (int e = 0; e < 25; ++e) {
-                    Ark[e] = ld(lu + flat_e(fq, e));
-                    Dk[e] = ld(dinv + flat_e(k, e));
+                    Ark[e] = ct_ld(lu + flat_e(fq, e));
+                    Dk[e] = ct_ld(dinv + flat_e(k, e));
                 }
 #pragma unroll
                 for (int i = 0; i < 5; ++i)
 #pragma unroll
                     for (int j = 0; j < 5; ++j) {
-                        double a = 0;
+                        CT a = 0;
 #pragma unroll
                         for (int t = 0; t < 5; ++t) a += Ark[5 * i + t] * Dk[5 * t + j];
                         Lrk[5 * i + j] = a;
                     }
 #pragma unroll
-                for (int e = 0; e < 25; ++e) st(lu + flat_e(fq, e), Lrk[e]);
+                for (int e = 0; e < 25; ++e) ct_st(lu + flat_e(fq, e), Lrk[e]);
                 for (int t = P.tr_start[q0 + q]; t < P.tr_start[q0 + q + 1]; ++t) {
                     const int kj = P.tr_kj[t], rj = P.tr_rj[t];
-                    double U[25];
+                    CT U[25];
 #pragma unroll
-                    for (int e = 0; e < 25; ++e) U[e] = ld(lu + flat_e(kj, e));
+                    for (int e = 0; e < 25; ++e) U[e] = ct_ld(lu + flat_e(kj, e));
                     if (rj < 0) {
 #pragma unroll
                         for (int i = 0; i < 5; ++i)
 #pragma unroll
                             for (int j = 0; j < 5; ++j) {
-                                double a = 0;
+                                CT a = 0;
 #pragma unroll
                                 for (int t2 = 0; t2 < 5; ++t2) a += Lrk[5 * i + t2] * U[5 * t2 + j];
                                 D[5 * i + j] -= a;
@@ -291,19 +315,19 @@ __global__ void __launch_bounds__(ILU_TPB) k_ilu_factor(SellMat<MT> A, MT* __res
                         for (int i = 0; i < 5; ++i)
 #pragma unroll
                             for (int j = 0; j < 5; ++j) {
-                                double a = 0;
+                                CT a = 0;
 #pragma unroll
                                 for (int t2 = 0; t2 < 5; ++t2) a += Lrk[5 * i + t2] * U[5 * t2 + j];
                                 MT* p = lu + flat_e(rj, 5 * i + j);
-                                st(p, ld(p) - a);
+                                ct_st(p, ct_ld(p) - a);
                             }
                     }
                 }
             }
-            double X[25];
+            CT X[25];
             inv5(D, X);
 #pragma unroll
-            for (int e = 0; e < 25; ++e) st(dinv + flat_e(r, e), X[e]);
+            for (int e = 0; e < 25; ++e) ct_st(dinv + flat_e(r, e), X[e]);
         }
         __syncthreads();
     }
@@ -516,8 +540,6 @@ constexpr int ILU_BULK_TPB = 128;
 constexpr int ILU_BULK_RPT = (ILU_BULK_TPB / 32) * 6;   // rows per task (24)
 constexpr int ILU_BULK_HDR = ILU_BULK_RPT * 4;           // task header bytes (96)
 
-template <typename MT> struct IluCT { using T = float; };
-template <> struct IluCT<double> { using T = double; };
 __device__ __forceinline__ double to_ct(double v, double) { return v; }
 __device__ __forceinline__ float to_ct(float v, float) { return v; }
 __device__ __forceinline__ float to_ct(__nv_bfloat16 v, float) { return __bfloat162float(v); }
@@ -538,22 +560,27 @@ __device__ __forceinline__ void lb_load(const float* p, float (&o)[5]) {
 // stages the bulk apply keeps (NS - 1 tasks in flight)
 template <typename MT>
 constexpr int ilu_bulk_stages() { return 3; }
+constexpr int ILU_FR_MAXQ = 8;      // lower slots per row the direct factorisation takes
 
 // factor blocks -> task records (after each factorisation): one CTA per 32
-// rows.  The slots the chunk's rows use are staged through shared memory
-// (sliced loads contiguous), then each row's values are written as one
-// contiguous run (its record's value area, complete 16-byte sectors): the
-// L blocks forward; the U blocks and the pivot inverse backward.
+// rows.  The blocks the chunk's rows use are staged through shared memory
+// (loads of the sliced stores contiguous over the rows): the L blocks of the
+// factor store, the U blocks of A (of the factor store for rows whose own
+// blocks take updates), the pivot inverses; then the rows' value areas are
+// written as whole 16-byte chunks, the threads on consecutive chunks of
+// consecutive rows.
 template <typename MT>
 __host__ __device__ constexpr int ilu_pack_tile() { return 25 * 33; }
 
 template <typename MT>
-__global__ void __launch_bounds__(256) k_ilu_pack(int N, const MT* __restrict__ lu, const MT* __restrict__ dinv,
-                                                  IluDev P) {
+__global__ void __launch_bounds__(256) k_ilu_pack(int N, SellMat<MT> A, const MT* __restrict__ lu,
+                                                  const MT* __restrict__ dinv, IluDev P) {
     extern __shared__ __align__(16) unsigned char s_pack[];
     MT* tiles = reinterpret_cast<MT*>(s_pack);        // [slots][25][33]
-    __shared__ int s_n[2][32], s_max[2];
+    __shared__ int s_n[2][32], s_pre[33], s_max[2], s_upd[32];
+    __shared__ int s_src[ILU_FR_MAXQ * 2][32];
     constexpr int TL = ilu_pack_tile<MT>();
+    constexpr int EPC = 16 / (int)sizeof(MT);
     const int chunk = blockIdx.x, r0 = chunk * 32;
     const int ms = P.ml + P.mu;
     if (threadIdx.x < 32) {
@@ -562,6 +589,7 @@ __global__ void __launch_bounds__(256) k_ilu_pack(int N, const MT* __restrict__ 
         int nl = nlu & 255, nu = P.mu_use ? (nlu >> 8) & 255 : 0;
         s_n[0][threadIdx.x] = r < N ? nl : -1;
         s_n[1][threadIdx.x] = r < N ? nu : -1;
+        s_upd[threadIdx.x] = (nlu >> 16) & 1;
         for (int o = 16; o > 0; o >>= 1) {
             nl = max(nl, __shfl_xor_sync(0xffffffffu, nl, o));
             nu = max(nu, __shfl_xor_sync(0xffffffffu, nu, o));
@@ -569,29 +597,207 @@ __global__ void __launch_bounds__(256) k_ilu_pack(int N, const MT* __restrict__ 
         if (threadIdx.x == 0) { s_max[0] = nl; s_max[1] = nu; }
     }
     __syncthreads();
+    // sources of the U blocks: flat SELL slot of A, -1 - fid of the factor
+    // store (rows whose own blocks take updates), or -2 (zero)
+    for (int i = threadIdx.x; i < s_max[1] * 32; i += blockDim.x) {
+        const int u = i >> 5, j = i & 31;
+        const int f = (chunk * ms + P.ml + u) * 32 + j;
+        const int src = r0 + j < N ? P.lu_src[f] : -2;
+        s_src[u][j] = s_upd[j] ? -1 - f : (src >= 0 ? src : -2);     // -2: empty slot or fill, zero
+    }
     for (int side = 0; side < 2; ++side) {
         const int nmax = s_max[side];
         const int ntile = side == 0 ? nmax : nmax + 1;     // backward: U slots, then the pivot inverses
-        for (int t = 0; t < ntile; ++t) {
-            const MT* src = side == 0 ? lu + (size_t)(chunk * ms + t) * 800
-                                      : (t < nmax ? lu + (size_t)(chunk * ms + P.ml + t) * 800
-                                                  : dinv + (size_t)chunk * 800);
-            for (int i = threadIdx.x; i < 800; i += blockDim.x) tiles[t * TL + (i >> 5) * 33 + (i & 31)] = src[i];
-        }
         __syncthreads();
-        for (int row = 0; row < 32; ++row) {
-            const int n = s_n[side][row];
-            if (n < 0) break;
-            const int words = 25 * (side == 0 ? n : n + 1);
-            MT* dst = reinterpret_cast<MT*>((side == 0 ? P.rec_f + (size_t)P.val_f[r0 + row] * 16
-                                                       : P.rec_b + (size_t)P.val_b[r0 + row] * 16));
-            for (int w = threadIdx.x; w < words; w += blockDim.x) {
-                const int q = w / 25, e = w - 25 * q;
-                const int t = (side == 1 && q == n) ? nmax : q;
-                dst[w] = tiles[t * TL + e * 33 + row];
+        for (int t = 0; t < ntile; ++t) {
+            for (int i = threadIdx.x; i < 800; i += blockDim.x) {
+                const int e = i >> 5, j = i & 31;
+                MT v;
+                if (side == 0) v = lu[(size_t)(chunk * ms + t) * 800 + i];
+                else if (t == nmax) v = dinv[(size_t)chunk * 800 + i];
+                else {
+                    const int src = s_src[t][j];
+                    v = src >= 0 ? A.val[flat_e(src, e)] : (src == -2 ? mt_zero<MT>() : lu[flat_e(-1 - src, e)]);
+                }
+                tiles[t * TL + e * 33 + j] = v;
             }
         }
+        // chunks per row, prefix
+        if (threadIdx.x < 32) {
+            const int n = s_n[side][threadIdx.x];
+            const int nel = n < 0 ? 0 : 25 * (side == 0 ? n : n + 1);
+            int c = (nel + EPC - 1) / EPC, x = c;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if ((int)threadIdx.x >= o) x += y;
+            }
+            s_pre[threadIdx.x + 1] = x;
+            if (threadIdx.x == 0) s_pre[0] = 0;
+        }
         __syncthreads();
+        const int total = s_pre[32];
+        for (int g = threadIdx.x; g < total; g += blockDim.x) {
+            int j = 0;
+#pragma unroll
+            for (int st = 16; st > 0; st >>= 1)
+                if (s_pre[j + st] <= g) j += st;
+            const int ch = g - s_pre[j];
+            const int n = s_n[side][j];
+            const int nel = 25 * (side == 0 ? n : n + 1);
+            alignas(16) MT v[EPC];
+#pragma unroll
+            for (int k = 0; k < EPC; ++k) {
+                const int e = ch * EPC + k;
+                const int q = e / 25, ee = e - 25 * q;
+                const int t = (side == 1 && q == n) ? nmax : q;
+                v[k] = e < nel ? tiles[t * TL + ee * 33 + j] : mt_zero<MT>();
+            }
+            uint4* dst = reinterpret_cast<uint4*>(side == 0 ? P.rec_f + (size_t)P.val_f[r0 + j] * 16
+                                                            : P.rec_b + (size_t)P.val_b[r0 + j] * 16);
+            dst[ch] = *reinterpret_cast<const uint4*>(v);
+        }
+    }
+}
+
+// one IKJ update triple of row r: U_kj read from A (us >= 0), the sliced
+// factor store (fid -us - 1) or zero (INT_MIN); L_rk U_kj taken from the
+// diagonal (tgt < 0) or from slot tgt of the row in the factor store
+template <typename MT, typename CT>
+__device__ __forceinline__ void ilu_fr_update(const SellMat<MT>& A, MT* __restrict__ lu, int r, int ms,
+                                              const CT (&Lrk)[25], CT (&D)[25], int us, int tgt) {
+    CT U[25];
+    if (us >= 0) {
+#pragma unroll
+        for (int e = 0; e < 25; ++e) U[e] = ct_ld(A.val + flat_e(us, e));
+    } else if (us != INT_MIN) {
+#pragma unroll
+        for (int e = 0; e < 25; ++e) U[e] = ct_ld(lu + flat_e(-us - 1, e));
+    } else {
+#pragma unroll
+        for (int e = 0; e < 25; ++e) U[e] = CT(0);
+    }
+    if (tgt < 0) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                CT a = 0;
+#pragma unroll
+                for (int t2 = 0; t2 < 5; ++t2) a += Lrk[5 * i + t2] * U[5 * t2 + j];
+                D[5 * i + j] -= a;
+            }
+    } else {
+        const int ft = lu_fid(r, tgt, ms);
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                CT a = 0;
+#pragma unroll
+                for (int t2 = 0; t2 < 5; ++t2) a += Lrk[5 * i + t2] * U[5 * t2 + j];
+                MT* pe = lu + flat_e(ft, 5 * i + j);
+                ct_st(pe, ct_ld(pe) - a);
+            }
+    }
+}
+
+// The subdomain factorisations with the blocks of A read where they lie
+// (no gather; the bulk apply's records are written by k_ilu_pack after it):
+// one CTA (one warp) per subdomain, a thread per row of the current
+// wavefront level, in the compute type of the storage (IluCT: FP32 for FP32
+// and BF16 factors).  Row r forms L_rk = A_rk D_k^-1 and the IKJ updates
+// from its blocks of A and, of earlier rows, the pivot inverses (dinv) and
+// U blocks (A itself, or the factor store for rows whose own blocks take
+// updates: those rows first copy their blocks of A there), and stores L and
+// its pivot inverse in the sliced factor store, lanes side by side.  The
+// addressing of each lower slot is one 16-byte descriptor (fr_desc), all
+// read at the row's start.  Same operations, order and roundings as
+// k_ilu_gather + k_ilu_factor.
+template <typename MT>
+__global__ void __launch_bounds__(32) k_ilu_factor_direct(SellMat<MT> A, MT* __restrict__ lu,
+                                                          MT* __restrict__ dinv, IluDev P) {
+    using CT = typename IluCT<MT>::T;
+    __shared__ int s_off[ILU_MAX_LV + 1];
+    const int ln = threadIdx.x;
+    const int ms = P.ml + P.mu;
+    const int part = blockIdx.x;
+    const int l0 = P.part_lvl0[part], l1 = P.part_lvl0[part + 1];
+    const bool staged = l1 - l0 <= ILU_MAX_LV;
+    if (staged)
+        for (int i = ln; i <= l1 - l0; i += 32) s_off[i] = P.lvl_off[l0 + i];
+    __syncwarp();
+    auto off = [&](int l) { return staged ? s_off[l - l0] : P.lvl_off[l]; };
+    for (int l = l0; l < l1; ++l) {
+        const int end = off(l + 1);
+        for (int base = off(l); base < end; base += 32) {
+            const int r = base + ln;
+            if (r < end) {
+                const int nlu = P.nlu[r];
+                const int q0 = P.low_start[r];
+                const int nl = nlu & 255;
+                const int nu = P.mu_use ? (nlu >> 8) & 255 : 0;
+                const bool upd = (nlu >> 16) & 1;
+                int4 dsc[ILU_FR_MAXQ];
+#pragma unroll
+                for (int q = 0; q < ILU_FR_MAXQ; ++q)
+                    if (q < nl) dsc[q] = P.fr_desc[q0 + q];
+                const MT* dv = A.val + (size_t)A.slice_off[r >> 5] * (32 * 25) + (r & 31);
+                CT D[25];
+#pragma unroll
+                for (int e = 0; e < 25; ++e) D[e] = ct_ld(dv + e * 32);
+                // a row that updates its own blocks takes them from A into
+                // the factor store first (zero where ILU(p) fills)
+                if (upd) {
+                    for (int sl = 0; sl < nl + nu; ++sl) {
+                        const int f = lu_fid(r, sl < nl ? sl : P.ml + sl - nl, ms);
+                        const int src = P.lu_src[f];
+#pragma unroll
+                        for (int e = 0; e < 25; ++e) lu[flat_e(f, e)] = src >= 0 ? A.val[flat_e(src, e)] : mt_zero<MT>();
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < ILU_FR_MAXQ; ++q) {
+                    if (q < nl) {
+                        const int k = dsc[q].x, sl = dsc[q].y, us0 = dsc[q].z, tw = dsc[q].w;
+                        const int fq = lu_fid(r, q, ms);
+                        CT Ark[25], Dk[25], Lrk[25];
+                        if (upd) {
+#pragma unroll
+                            for (int e = 0; e < 25; ++e) Ark[e] = ct_ld(lu + flat_e(fq, e));
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 25; ++e) Ark[e] = sl >= 0 ? ct_ld(A.val + flat_e(sl, e)) : CT(0);
+                        }
+#pragma unroll
+                        for (int e = 0; e < 25; ++e) Dk[e] = ct_ld(dinv + flat_e(k, e));
+#pragma unroll
+                        for (int i = 0; i < 5; ++i)
+#pragma unroll
+                            for (int j = 0; j < 5; ++j) {
+                                CT a = 0;
+#pragma unroll
+                                for (int t = 0; t < 5; ++t) a += Ark[5 * i + t] * Dk[5 * t + j];
+                                Lrk[5 * i + j] = a;
+                            }
+#pragma unroll
+                        for (int e = 0; e < 25; ++e) ct_st(lu + flat_e(fq, e), Lrk[e]);
+                        // update triples: the first rides in the descriptor (w:
+                        // its target slot + 2, 0 none; bit 20: more follow)
+                        const int tfirst = (tw & 0xfffff) - 2;
+                        if (tfirst >= -1) ilu_fr_update(A, lu, r, ms, Lrk, D, us0, tfirst);
+                        if (tw >> 20) {
+                            for (int t = P.tr_start[q0 + q] + 1; t < P.tr_start[q0 + q + 1]; ++t)
+                                ilu_fr_update(A, lu, r, ms, Lrk, D, P.fr_trk[t], P.fr_trt[t]);
+                        }
+                    }
+                }
+                CT X[25];
+                inv5(D, X);
+#pragma unroll
+                for (int e = 0; e < 25; ++e) ct_st(dinv + flat_e(r, e), X[e]);
+            }
+            __syncwarp();
+        }
     }
 }
 

@@ -241,6 +241,7 @@ struct rdst_ctx {
     DevMesh m{};
     // fields
     DBuf<double> W, prim, bs, q, qb, g, psi, fcell, fl, bfl, R, rhs, partial;
+    DBuf<double> bjac;             // boundary Jacobian blocks of the active boundary faces
     DBuf<double> rdt, courantF, rhoOld, eOld, eNew;
     // viscous: grad U, face Up, viscous face terms, turbulent viscosity
     DBuf<double> gU, up, bup, vf, bvf, mut, mut_b;
@@ -270,6 +271,11 @@ struct rdst_ctx {
     DBuf<uint2> task_f, task_b;
     DBuf<int> part_tf, part_tb;
     DBuf<unsigned> val_f, val_b;
+    // addressing of the factorisation that reads A directly (else gather +
+    // factor), both followed by the record pack
+    DBuf<int> fr_trk, fr_trt;
+    DBuf<int4> fr_desc;
+    bool ilu_fused = false;
     int ilu_stage_bytes = 0;         // largest task record, rounded to 128 bytes
     int ilu_stages = 0;              // stages of the bulk apply (2 or 3)
     int ilu_lb_rows = 0;             // rows of each level buffer (0: none)
@@ -396,6 +402,7 @@ struct rdst_ctx {
         P.tr_start = tr_start.p; P.tr_kj = tr_kj.p; P.tr_rj = tr_rj.p;
         P.rec_f = rec_f.p; P.rec_b = rec_b.p; P.task_f = task_f.p; P.task_b = task_b.p;
         P.part_tf = part_tf.p; P.part_tb = part_tb.p; P.val_f = val_f.p; P.val_b = val_b.p;
+        P.fr_trk = fr_trk.p; P.fr_trt = fr_trt.p; P.fr_desc = fr_desc.p;
         return P;
     }
     long nvec() const { return 5L * N; }
@@ -546,7 +553,10 @@ void load_geometry(rdst_ctx& c, const rdst_mesh* mh, bool in_place) {
 // two; a task too large for one CTA's shared memory leaves the register
 // apply in place.
 void build_task_records(rdst_ctx& c, const Options& o, int nparts, const std::vector<int>& part_lvl0,
-                        const std::vector<int>& lvl_off, const std::vector<int>& lu_col, const std::vector<int>& nl,
+                        const std::vector<int>& lvl_off, const std::vector<int>& lu_col,
+                        const std::vector<int>& lu_src, const std::vector<int>& nlu,
+                        const std::vector<int>& low_start, const std::vector<int>& tr_start,
+                        const std::vector<int>& tr_kj, const std::vector<int>& tr_rj, const std::vector<int>& nl,
                         const std::vector<int>& nu, int ML, int MS) {
     const int N = c.N;
     const size_t S = o.precision == PREC_FP64 ? 8 : (o.precision == PREC_FP32 ? 4 : 2);
@@ -642,6 +652,34 @@ void build_task_records(rdst_ctx& c, const Options& o, int nparts, const std::ve
     c.task_f.upload(tabf, s); c.task_b.upload(tabb, s);
     c.part_tf.upload(ptf, s); c.part_tb.upload(ptb, s);
     c.val_f.upload(vf, s); c.val_b.upload(vb, s);
+    // the factorisation reading A directly: where each update triple reads
+    // U_kj and which slot of row r takes it, and one descriptor per L slot
+    {
+        std::vector<int> trk(tr_kj.size()), trt(tr_rj.size());
+        for (size_t t = 0; t < tr_kj.size(); ++t) {
+            const int kj = tr_kj[t];
+            const int k = ((kj >> 5) / MS) * 32 + (kj & 31);
+            trk[t] = (nlu[k] >> 16) & 1 ? -kj - 1 : (lu_src[kj] >= 0 ? lu_src[kj] : INT_MIN);
+            trt[t] = tr_rj[t] < 0 ? -1 : (tr_rj[t] >> 5) % MS;
+        }
+        std::vector<int4> desc(low_start[N]);
+        for (int r = 0; r < N; ++r)
+            for (int q = 0; q < nl[r]; ++q) {
+                const int i = low_start[r] + q, t0 = tr_start[i], t1 = tr_start[i + 1];
+                int4 d;
+                d.x = lu_col[lfid(r, q)];
+                d.y = lu_src[lfid(r, q)];
+                d.z = t1 > t0 ? trk[t0] : 0;
+                d.w = (t1 > t0 ? trt[t0] + 2 : 0) | (t1 - t0 > 1 ? 1 << 20 : 0);
+                desc[i] = d;
+            }
+        if (ML <= ILU_FR_MAXQ) {
+            c.fr_trk.upload(trk, s);
+            c.fr_trt.upload(trt, s);
+            c.fr_desc.upload(desc, s);
+            c.ilu_fused = true;
+        }
+    }
     c.ilu_stage_bytes = stage;
     c.ilu_stages = ns;
     c.ilu_lb_rows = lb;
@@ -938,7 +976,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
                     }
                     if (!upd_off || ipart[j] != ipart[r]) continue;
                     int rj = fid_of(r, j);
-                    if (rj >= 0) { tr_kj.push_back(kj); tr_rj.push_back(rj); }
+                    if (rj >= 0) { tr_kj.push_back(kj); tr_rj.push_back(rj); nlu[r] |= 1 << 16; }
                 }
                 tr_start.push_back((int)tr_kj.size());
             }
@@ -948,7 +986,9 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
         c.tr_start.upload(tr_start, s); c.tr_kj.upload(tr_kj, s); c.tr_rj.upload(tr_rj, s);
         c.lu_col.upload(lu_col, s); c.lu_src.upload(lu_src, s);
         c.lu_slots = MS;
-        if (o.ilu_bulk) build_task_records(c, o, nparts, part_lvl0, lvl_off, lu_col, nl, nu, ML, MS);
+        if (o.ilu_bulk)
+            build_task_records(c, o, nparts, part_lvl0, lvl_off, lu_col, lu_src, nlu, low_start, tr_start, tr_kj, tr_rj,
+                               nl, nu, ML, MS);
     }
     // ---- AMG hierarchy: plan on the cell graph (original numbering), level
     // 0 in the internal row order; the Galerkin gather lists sum the finer
@@ -1049,6 +1089,7 @@ void build(rdst_ctx& c, const rdst_mesh* mh) {
     // ---- fields
     c.perm_d.upload(c.perm, s); c.stage.alloc(5L * N);
     c.W.alloc(5L * N); c.prim.alloc((size_t)PW * N); c.bs.alloc((size_t)BW * std::max(NB, 1));
+    c.bjac.alloc((size_t)25 * std::max(NB, 1));
     c.q.alloc((size_t)QW * N); c.qb.alloc((size_t)QW * std::max(NB, 1)); c.g.alloc((size_t)GW * N);
     c.psi.alloc((size_t)QW * N); c.fcell.alloc(N); c.fl.alloc(5L * std::max(Fi, 1)); c.bfl.alloc(5L * std::max(NB, 1));
     c.R.alloc(5L * N); c.rhs.alloc(5L * N);
@@ -1161,11 +1202,30 @@ static void ilu_apply_bulk(rdst_ctx& c, const IluDev& P, const double* in, doubl
 }
 // blocks of the fresh factors -> the task records
 template <typename MT>
-static void ilu_pack(rdst_ctx& c) {
+static void ilu_pack(rdst_ctx& c, void* val) {
     if (!c.rec_f.p) return;
-    k_ilu_pack<MT><<<c.n_slices, 256, ilu_pack_smem<MT>(c), c.s>>>(c.N, (const MT*)c.LUval, (const MT*)c.dinv,
-                                                                   c.ilu());
+    k_ilu_pack<MT><<<c.n_slices, 256, ilu_pack_smem<MT>(c), c.s>>>(c.N, c.mat<MT>(val), (const MT*)c.LUval,
+                                                                   (const MT*)c.dinv, c.ilu());
     CKL();
+}
+
+// block ILU factorisation of the matrix at val into the factor store:
+// reading A directly when the descriptors were built, else gather + factor;
+// then packed into the bulk apply's records when there are records
+template <typename MT>
+static void ilu_factorise(rdst_ctx& c, void* val) {
+    if (c.ilu_fused) {
+        k_ilu_factor_direct<MT><<<c.n_parts, 32, 0, c.s>>>(c.mat<MT>(val), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
+        CKL();
+    } else {
+        const int n_fid = c.n_slices * c.lu_slots * 32;
+        k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(val), (MT*)c.LUval, c.lu_src.p, n_fid);
+        CKL();
+        k_ilu_factor<MT><<<c.n_parts, c.o.ilu_factor_threads, 0, c.s>>>(c.mat<MT>(val), (MT*)c.LUval,
+                                                                       (MT*)c.dinv, c.ilu());
+        CKL();
+    }
+    ilu_pack<MT>(c, val);
 }
 
 template <typename MT>
@@ -1218,7 +1278,11 @@ struct Ops {
     static void assemble(rdst_ctx& c) {
         SellMat<MT> A = c.mat<MT>(c.Aval);
         Timed tm(c, KS_ASSEMBLE);
-        k_assemble<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.m, c.th, c.tr, A, c.cf_slot.p, c.W.p, c.prim.p, c.bs.p,
+        if (c.m.NB > 0) {
+            k_bjac<<<nblk(c.m.NB, 128), 128, 0, c.s>>>(c.m, c.th, c.W.p, c.prim.p, c.bs.p, c.bjac.p);
+            CKL();
+        }
+        k_assemble<MT><<<nblk(c.N, 128), 128, 0, c.s>>>(c.m, c.th, c.tr, A, c.cf_slot.p, c.W.p, c.prim.p, c.bjac.p,
                                                         c.rdt.p, c.mut.p, c.sc.p, (c.steady || c.o.dual) ? 1 : 0,
                                                         c.o.beta, c.dual_a);
         CKL();
@@ -1305,12 +1369,7 @@ struct Ops {
             amg_setup(c);
         } else if (lu_factored(c.o.precon)) {
             Timed tm(c, KS_FACTOR);
-            const int n_fid = c.n_slices * c.lu_slots * 32;
-            k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, c.lu_src.p, n_fid);
-            CKL();
-            k_ilu_factor<MT><<<c.n_parts, c.o.ilu_factor_threads, 0, c.s>>>(c.mat<MT>(c.Aval), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
-            CKL();
-            ilu_pack<MT>(c);
+            ilu_factorise<MT>(c, c.Aval);
         }
     }
     // out = (L U)^-1 in with the stored factors
@@ -2129,12 +2188,7 @@ void adj_precond_setup(rdst_ctx& c) {
         Ops<MT>::amg_setup(c);
         std::swap(c.Aval, c.a_AT);
     } else if (lu_factored(c.o.precon)) {
-        const int n_fid = c.n_slices * c.lu_slots * 32;
-        k_ilu_gather<MT><<<nblk(n_fid, TPB), TPB, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, c.lu_src.p, n_fid);
-        CKL();
-        k_ilu_factor<MT><<<c.n_parts, c.o.ilu_factor_threads, 0, c.s>>>(c.mat<MT>(c.a_AT), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
-        CKL();
-        ilu_pack<MT>(c);
+        ilu_factorise<MT>(c, c.a_AT);
     }
 }
 

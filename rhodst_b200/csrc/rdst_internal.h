@@ -109,6 +109,15 @@ __device__ __forceinline__ double tod(double v) { return v; }
 __device__ __forceinline__ double tod(float v) { return (double)v; }
 __device__ __forceinline__ double tod(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
 template <typename T> __device__ __forceinline__ T mt_zero() { return T(0); }
+// storage type <-> the compute type of the block factorisations (FP64
+// storage: double; FP32 and BF16 storage: float), without a detour
+// through double
+__device__ __forceinline__ double ct_ld(const double* p) { return *p; }
+__device__ __forceinline__ float ct_ld(const float* p) { return *p; }
+__device__ __forceinline__ float ct_ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ void ct_st(double* p, double v) { *p = v; }
+__device__ __forceinline__ void ct_st(float* p, float v) { *p = v; }
+__device__ __forceinline__ void ct_st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 mt_zero<__nv_bfloat16>() { return __float2bfloat16_rn(0.0f); }
 
 }  // namespace rdst
