@@ -438,6 +438,8 @@ __global__ void __launch_bounds__(128) k_grad(DevMesh m, int venkat_mask, double
         const double* qi = q + QW * i;
         double eps2 = pow(venkat_K * cbrt(Vi), 3.0);
         V3 Ci = ldv3(m.C, m.N, i);
+        // unrolled: acc stays in registers (indexed by constants only)
+#pragma unroll
         for (int j = 0; j < 7; ++j) {
             if (!((venkat_mask >> j) & 1)) { psi[QW * i + j] = 1.0; continue; }
             double x = qi[j], mx = x, mn = x;

@@ -48,7 +48,10 @@ inline void ck(cudaError_t e, const char* what) {
 thread_local long* g_launch_counter = nullptr;
 inline void count_launch() { if (g_launch_counter) ++*g_launch_counter; }
 #define CK(x) ck((x), #x)
-#define CKL() (count_launch(), ck(cudaGetLastError(), "kernel launch"))
+#define RDST_STR2(x) #x
+#define RDST_STR(x) RDST_STR2(x)
+// the launch's source line goes into the message
+#define CKL() (count_launch(), ck(cudaGetLastError(), "kernel launch at rdst_api.cu:" RDST_STR(__LINE__)))
 
 enum { KS_SPMV = 0, KS_PRECOND, KS_FLUX, KS_ASSEMBLE, KS_FACTOR, KS_ORTH, KS_UPDATE, KS_N };
 const char* const KS_NAMES[KS_N] = {"spmv", "precond", "flux", "assemble", "factor", "orth", "update"};
@@ -1165,12 +1168,26 @@ static size_t ilu_bulk_smem(const rdst_ctx& c) {
            (size_t)c.ilu_lb_rows * (sizeof(MT) == 8 ? 96 : 64) + (size_t)c.ilu_task_slots * 8 +
            (size_t)c.ilu_off_slots * 4;
 }
+// A kernel's dynamic shared memory limit is a property of the function on
+// the device, shared by every context of the process: it is raised to the
+// device's per-block maximum less the kernel's static shared memory (never
+// lowered to one context's need, which would fail the launches of a context
+// built earlier with larger tasks).
+template <typename K>
+static void set_max_dyn_smem(K* kernel) {
+    int dev = 0, per_block = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, kernel));
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, per_block - (int)fa.sharedSizeBytes));
+}
 template <typename MT, int NS, bool LB>
 static void ilu_bulk_launch(rdst_ctx& c, bool attr_only, const IluDev& P, const double* in, double* out,
                             const int* active) {
     const size_t sm = ilu_bulk_smem<MT>(c);
     if (attr_only) {
-        CK(cudaFuncSetAttribute(k_ilu_apply_bulk<MT, NS, LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        set_max_dyn_smem(k_ilu_apply_bulk<MT, NS, LB>);
         return;
     }
     k_ilu_apply_bulk<MT, NS, LB><<<c.n_parts, ILU_BULK_TPB, sm, c.s>>>(P, in, out, active, c.ilu_lb_rows,
@@ -1189,12 +1206,12 @@ static void ilu_bulk_dispatch(rdst_ctx& c, bool attr_only, const IluDev& P, cons
         else ilu_bulk_launch<MT, 2, false>(c, attr_only, P, in, out, active);
     }
 }
-// dynamic shared memory above the default 48 KB: set once when the
-// context is built (not while a step is being captured)
+// dynamic shared memory above the default 48 KB: set when a context is
+// built (not while a step is being captured)
 template <typename MT>
 static void ilu_bulk_attr(rdst_ctx& c) {
     ilu_bulk_dispatch<MT>(c, true, c.ilu(), nullptr, nullptr, nullptr);
-    CK(cudaFuncSetAttribute(k_ilu_pack<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ilu_pack_smem<MT>(c)));
+    set_max_dyn_smem(k_ilu_pack<MT>);
 }
 template <typename MT>
 static void ilu_apply_bulk(rdst_ctx& c, const IluDev& P, const double* in, double* out, const int* active) {

@@ -124,3 +124,24 @@ def test_too_wide_fill_is_refused():
 ], ids=["C1", "airfoil"])
 def test_graph_bisection_subdomains(case_fn):
     run_pair(case_fn(), 5, parts=16, graph=True)
+
+
+def test_contexts_with_different_ilu_shapes_coexist():
+    """The dynamic shared-memory limits of the record pack and the bulk
+    apply belong to the kernels, not to a context: a context built later on
+    a mesh with fewer factor blocks per row (2D quads: two lower and two
+    upper) must not shrink them under an earlier context whose rows carry
+    more (3D hexahedra: three and three)."""
+    wing = cases.swept_wing_c3(n_around=32, n_normal=8, n_span=8, n_tip=4, precision="fp64").with_options(
+        **{"ilu.parts": 4})
+    s3 = rhodst_b200.Solver(wing.mesh, wing.bcs, wing.options)
+    s3.set_primitive(wing.p, wing.U, wing.T)
+    r_before = s3.step(1)[-1]["res_mag"]
+    foil = cases.naca0012_inviscid(ni=65, nj=17).with_options(precision="fp64", **{"ilu.parts": 4})
+    s2 = rhodst_b200.Solver(foil.mesh, foil.bcs, foil.options)
+    s2.set_primitive(foil.p, foil.U, foil.T)
+    s2.step(1)
+    r_after = s3.step(1)[-1]["res_mag"]
+    assert np.isfinite(r_before) and np.isfinite(r_after)
+    s2.close()
+    s3.close()
