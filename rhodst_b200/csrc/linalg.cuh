@@ -801,8 +801,17 @@ __global__ void __launch_bounds__(32) k_ilu_factor_direct(SellMat<MT> A, MT* __r
     }
 }
 
+// The apply is specialised by warp: warps 0-3 compute (five lanes a row,
+// six rows a warp), a fifth warp produces.  For each task the producer
+// walks the cursor, publishes the task's rows and level buffers in s_q,
+// starts the bulk copy of its record into a stage and the copies of its y0
+// into the y0 slot, and waits for the latter before the barrier that ends
+// the task being computed; the compute warps only wait for the stage,
+// multiply and store.  All 160 threads take the same barriers.
+constexpr int ILU_BULK_THREADS = ILU_BULK_TPB + 32;
+
 template <typename MT, int NS, bool LB>
-__global__ void __launch_bounds__(ILU_BULK_TPB, 8)
+__global__ void __launch_bounds__(ILU_BULK_THREADS, 6)
     k_ilu_apply_bulk(IluDev P, const double* __restrict__ b, double* x, const int* __restrict__ active,
                      int lb_rows, int stage_bytes, int off_slots, int task_slots, int* flags) {
     using CT = typename IluCT<MT>::T;
@@ -812,6 +821,9 @@ __global__ void __launch_bounds__(ILU_BULK_TPB, 8)
     if (active && !*active) return;
     __shared__ __align__(8) unsigned long long s_bar[NS];
     __shared__ int s_abort;
+    // per stage: valid, first row, rows, the level's first row, its buffer,
+    // the previous level's first row and width
+    __shared__ int s_q[NS][8];
     extern __shared__ __align__(128) unsigned char s_dyn[];
     unsigned char* s_stage = s_dyn;                                                   // [NS][stage_bytes]
     double* s_y0 = reinterpret_cast<double*>(s_dyn + (size_t)NS * stage_bytes);       // [NS][T]
@@ -820,23 +832,24 @@ __global__ void __launch_bounds__(ILU_BULK_TPB, 8)
     int* s_off = reinterpret_cast<int*>(s_task + task_slots);                         // [off_slots]
     const int part = blockIdx.x;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp == T / 32;
     const int rsub = lane / 5, comp = lane - 5 * (lane / 5);
-    const bool lane_ok = lane < 30;
+    const bool lane_ok = !producer && lane < 30;
     const int i_row = warp * 6 + rsub;
     const int l0 = P.part_lvl0[part], l1 = P.part_lvl0[part + 1];
     const bool staged = l1 - l0 < off_slots;
     if (staged)
-        for (int i = tid; i <= l1 - l0; i += T) s_off[i] = P.lvl_off[l0 + i];
+        for (int i = tid; i <= l1 - l0; i += ILU_BULK_THREADS) s_off[i] = P.lvl_off[l0 + i];
     const int tf0 = P.part_tf[part], ntf = P.part_tf[part + 1] - tf0;
     const int tb0 = P.part_tb[part], ntb = P.part_tb[part + 1] - tb0;
     const bool tstaged = ntf + ntb <= task_slots;
     if (tstaged) {
-        for (int i = tid; i < ntf; i += T) s_task[i] = P.task_f[tf0 + i];
-        for (int i = tid; i < ntb; i += T) s_task[ntf + i] = P.task_b[tb0 + i];
+        for (int i = tid; i < ntf; i += ILU_BULK_THREADS) s_task[i] = P.task_f[tf0 + i];
+        for (int i = tid; i < ntb; i += ILU_BULK_THREADS) s_task[ntf + i] = P.task_b[tb0 + i];
     }
     const unsigned bar0 = (unsigned)__cvta_generic_to_shared(&s_bar[0]);
     const unsigned stage0 = (unsigned)__cvta_generic_to_shared(s_stage);
-    const unsigned y0a = (unsigned)__cvta_generic_to_shared(s_y0 + tid);
+    const unsigned y0s = (unsigned)__cvta_generic_to_shared(s_y0);
     if (tid == 0) {
         for (int k = 0; k < NS; ++k) mbar_init(bar0 + 8 * k, 1);
         s_abort = 0;
@@ -844,8 +857,10 @@ __global__ void __launch_bounds__(ILU_BULK_TPB, 8)
     }
     __syncthreads();
     auto off = [&](int l) { return staged ? s_off[l - l0] : P.lvl_off[l]; };
-    unsigned par = 0;          // bit k: parity of stage k's next completion
-    unsigned pending = 0;      // bit k: a copy into stage k not yet waited for
+    unsigned par = 0;          // compute warps: bit k, parity of stage k's next completion
+    unsigned ipar = 0;         // producer: bit k, parity of the next copy issued into stage k
+    unsigned lastp = 0;        // producer: bit k, parity of the last copy issued into stage k
+    unsigned issued = 0;       // producer: bit k, stage k has taken a copy
 
 #pragma unroll 1
     for (int sweep = 0; sweep < 2; ++sweep) {
@@ -854,53 +869,61 @@ __global__ void __launch_bounds__(ILU_BULK_TPB, 8)
         const unsigned char* rec = back ? P.rec_b : P.rec_f;
         const double* ysrc = back ? x : b;
         IluCursor cur{back ? l1 - 1 : l0, 0};
-        int tcount = 0;        // tasks of this sweep issued so far
+        int tcount = 0;        // tasks of this sweep issued so far (producer)
         auto in_range = [&](int l) { return back ? l >= l0 : l < l1; };
-        // per queued task: first row, rows, its level's first row and buffer,
-        // the previous level's first row and width
-        int qr0[NS], qn[NS], qa[NS], qbuf[NS], qpa[NS], qpw[NS];
-        bool qv[NS];
-        // advance the cursor and start task d's copies into stage d
-        auto next = [&](int d) {
-            qv[d] = in_range(cur.l);
-            qr0[d] = 0; qn[d] = 0; qa[d] = 0; qbuf[d] = 0; qpa[d] = 0; qpw[d] = 0;
-            if (qv[d]) {
+        // producer: the next task into stage d (cursor, s_q, record copy,
+        // y0 copies of the compute lanes: thread 32k + lane, row 6k + lane/5)
+        auto prepare = [&](int d) {
+            const bool v = in_range(cur.l);
+            int r0q = 0, nq = 0, aq = 0, bufq = 0, paq = 0, pwq = 0;
+            if (v) {
                 const int r0 = off(cur.l), r1 = off(cur.l + 1), n = r1 - r0;
-                qr0[d] = r0 + cur.base;
-                qn[d] = min(RPT, n - cur.base);
+                r0q = r0 + cur.base;
+                nq = min(RPT, n - cur.base);
                 if (LB) {
-                    qa[d] = r0;
-                    qbuf[d] = (cur.l & 1) * lb_rows * LR;
+                    aq = r0;
+                    bufq = (cur.l & 1) * lb_rows * LR;
                     const int lp = cur.l - dir;          // the level taken just before
-                    if (in_range(lp)) { qpa[d] = off(lp); qpw[d] = off(lp + 1) - qpa[d]; }
+                    if (in_range(lp)) { paq = off(lp); pwq = off(lp + 1) - paq; }
                 }
                 cur.base += RPT;
                 if (cur.base >= n) { cur.l += dir; cur.base = 0; }
-                if (tid == 0) {
+                if (lane == 0) {
                     const uint2 tk = tstaged ? s_task[(back ? ntf : 0) + tcount]
                                              : (back ? P.task_b[tb0 + tcount] : P.task_f[tf0 + tcount]);
                     mbar_expect_tx(bar0 + 8 * d, tk.y);
                     bulk_g2s(stage0 + (unsigned)(d * stage_bytes), rec + (size_t)tk.x * 16, tk.y, bar0 + 8 * d);
                 }
                 ++tcount;
-                pending |= 1u << d;
+                lastp = (lastp & ~(1u << d)) | (ipar & (1u << d));
+                ipar ^= 1u << d;
+                issued |= 1u << d;
             }
-            const bool act = qv[d] && lane_ok && i_row < qn[d];
-            cpa8(y0a + (unsigned)(d * T * 8), ysrc + (act ? 5 * (size_t)(qr0[d] + i_row) + comp : 0), act);
+            if (lane == 0) {
+                s_q[d][0] = v; s_q[d][1] = r0q; s_q[d][2] = nq; s_q[d][3] = aq;
+                s_q[d][4] = bufq; s_q[d][5] = paq; s_q[d][6] = pwq;
+            }
+#pragma unroll
+            for (int k = 0; k < T / 32; ++k) {
+                const int row = 6 * k + rsub;
+                const bool ok = v && lane < 30 && row < nq;
+                cpa8(y0s + (unsigned)((d * T + 32 * k + lane) * 8), ysrc + (ok ? 5 * (size_t)(r0q + row) + comp : 0),
+                     ok);
+            }
             cpa_commit();
         };
-        // task d: wait for its stage, y = y0 - sum_k (L_rk x_k) (backward
-        // x_r = inv(U_rr) y), then the barrier that ends the task
+        // compute warps: task d, after its stage has landed: y = y0 -
+        // sum_k (L_rk x_k) (backward x_r = inv(U_rr) y)
         auto run = [&](int d) {
             if (!mbar_wait(bar0 + 8 * d, (par >> d) & 1u)) {
                 atomicOr(flags, 4);
                 s_abort = 1;
             }
             par ^= 1u << d;
-            pending &= ~(1u << d);
-            cpa_wait<NS - 1>();
-            const bool act = lane_ok && i_row < qn[d] && !s_abort;
-            const int r = qr0[d] + i_row;
+            const int qr0 = s_q[d][1], qn = s_q[d][2], qa = s_q[d][3], qbuf = s_q[d][4];
+            const int qpa = s_q[d][5], qpw = s_q[d][6];
+            const bool act = lane_ok && i_row < qn && !s_abort;
+            const int r = qr0 + i_row;
             const unsigned char* st0 = s_stage + (size_t)d * stage_bytes;
             const unsigned hdr = act ? reinterpret_cast<const unsigned*>(st0)[i_row] : 0u;
             const int cnt = (int)(hdr >> 24);
@@ -911,16 +934,16 @@ __global__ void __launch_bounds__(ILU_BULK_TPB, 8)
                 // the first four blocks side by side (their products are
                 // independent), then subtracted in column order; a block
                 // past the row's count loads nothing and contributes 0
-                const CT* pbuf = s_lvx + (lb_rows * LR - qbuf[d]);   // the other level buffer
+                const CT* pbuf = s_lvx + (lb_rows * LR - qbuf);   // the other level buffer
                 CT part4[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     CT t = CT(0);
                     if (k < cnt) {
                         const int ck = cols[k];
-                        const unsigned rel = (unsigned)(ck - qpa[d]);
+                        const unsigned rel = (unsigned)(ck - qpa);
                         CT xk[5];
-                        if (LB && rel < (unsigned)qpw[d]) {
+                        if (LB && rel < (unsigned)qpw) {
                             lb_load(pbuf + LR * rel, xk);
                         } else {
 #pragma unroll
@@ -936,9 +959,9 @@ __global__ void __launch_bounds__(ILU_BULK_TPB, 8)
                 for (int k = 0; k < 4; ++k) y -= part4[k];
                 for (int k = 4; k < cnt; ++k) {
                     const int ck = cols[k];
-                    const unsigned rel = (unsigned)(ck - qpa[d]);
+                    const unsigned rel = (unsigned)(ck - qpa);
                     CT xk[5];
-                    if (LB && rel < (unsigned)qpw[d]) {
+                    if (LB && rel < (unsigned)qpw) {
                         lb_load(pbuf + LR * rel, xk);
                     } else {
 #pragma unroll
@@ -961,34 +984,42 @@ __global__ void __launch_bounds__(ILU_BULK_TPB, 8)
             }
             if (act) {
                 x[5 * (size_t)r + comp] = (double)y;
-                if (LB) s_lvx[qbuf[d] + LR * (r - qa[d]) + comp] = y;
+                if (LB) s_lvx[qbuf + LR * (r - qa) + comp] = y;
             }
-            __syncthreads();
         };
-        // stage slots rotate with compile-time indices (the body is
-        // unrolled NS times), so the queue stays in registers
+        if (producer) {
 #pragma unroll
-        for (int d = 0; d < NS - 1; ++d) next(d);
-        bool go = qv[0];
+            for (int d = 0; d < NS - 1; ++d) prepare(d);
+            cpa_wait<0>();
+        }
+        __syncthreads();
+        bool go = s_q[0][0] != 0;
         while (go) {
+            // stage slots rotate with compile-time indices (the body is
+            // unrolled NS times), so the queue stays in registers
 #pragma unroll
             for (int u = 0; u < NS; ++u) {
                 if (go) {
-                    next((u + NS - 1) % NS);
-                    run(u);
-                    go = qv[(u + 1) % NS] && !s_abort;
+                    if (producer) {
+                        prepare((u + NS - 1) % NS);
+                        cpa_wait<0>();
+                    } else {
+                        run(u);
+                    }
+                    __syncthreads();
+                    go = s_q[(u + 1) % NS][0] != 0 && !s_abort;
                 }
             }
         }
-        cpa_wait<0>();
         if (s_abort) {
             // copies still in flight land before the CTA's shared memory goes
-            for (int d = 0; d < NS; ++d)
-                if ((pending >> d) & 1u) mbar_wait(bar0 + 8 * d, (par >> d) & 1u);
+            if (producer && lane == 0)
+                for (int d = 0; d < NS; ++d)
+                    if ((issued >> d) & 1u) mbar_wait(bar0 + 8 * d, (lastp >> d) & 1u);
             return;
         }
-        // the next sweep issues its first tasks into stages 0..NS-2 again:
-        // the queue rotation restarts, parities carry on
+        // the next sweep prepares its first tasks into stages 0..NS-2 again:
+        // the rotation restarts, parities carry on
         __syncthreads();
     }
 }

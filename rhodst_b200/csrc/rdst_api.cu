@@ -1190,7 +1190,7 @@ static void ilu_bulk_launch(rdst_ctx& c, bool attr_only, const IluDev& P, const 
         set_max_dyn_smem(k_ilu_apply_bulk<MT, NS, LB>);
         return;
     }
-    k_ilu_apply_bulk<MT, NS, LB><<<c.n_parts, ILU_BULK_TPB, sm, c.s>>>(P, in, out, active, c.ilu_lb_rows,
+    k_ilu_apply_bulk<MT, NS, LB><<<c.n_parts, ILU_BULK_THREADS, sm, c.s>>>(P, in, out, active, c.ilu_lb_rows,
                                                                         c.ilu_stage_bytes, c.ilu_off_slots,
                                                                         c.ilu_task_slots, &c.sc.p->flags);
 }
