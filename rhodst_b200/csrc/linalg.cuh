@@ -221,8 +221,8 @@ struct IluDev {
     const int* part_tb;
     const unsigned* val_f;
     const unsigned* val_b;
-    // the factorisation written straight into the records (null: gather,
-    // factor and pack instead).  Per update triple (tr_start ranges):
+    // the direct factorisation's addressing (null: gather + factor
+    // instead).  Per update triple (tr_start ranges):
     // fr_trk: where U_kj is read, the flat SELL slot of A_kj (>= 0), factor
     // id fid of the sliced store as -fid - 1 (row k takes updates of its
     // own), or INT_MIN (a fill block of a row without updates: zero);

@@ -278,7 +278,7 @@ struct rdst_ctx {
     // factor), both followed by the record pack
     DBuf<int> fr_trk, fr_trt;
     DBuf<int4> fr_desc;
-    bool ilu_fused = false;
+    bool ilu_direct = false;
     int ilu_stage_bytes = 0;         // largest task record, rounded to 128 bytes
     int ilu_stages = 0;              // stages of the bulk apply (2 or 3)
     int ilu_lb_rows = 0;             // rows of each level buffer (0: none)
@@ -680,7 +680,7 @@ void build_task_records(rdst_ctx& c, const Options& o, int nparts, const std::ve
             c.fr_trk.upload(trk, s);
             c.fr_trt.upload(trt, s);
             c.fr_desc.upload(desc, s);
-            c.ilu_fused = true;
+            c.ilu_direct = true;
         }
     }
     c.ilu_stage_bytes = stage;
@@ -1231,7 +1231,7 @@ static void ilu_pack(rdst_ctx& c, void* val) {
 // then packed into the bulk apply's records when there are records
 template <typename MT>
 static void ilu_factorise(rdst_ctx& c, void* val) {
-    if (c.ilu_fused) {
+    if (c.ilu_direct) {
         k_ilu_factor_direct<MT><<<c.n_parts, 32, 0, c.s>>>(c.mat<MT>(val), (MT*)c.LUval, (MT*)c.dinv, c.ilu());
         CKL();
     } else {
