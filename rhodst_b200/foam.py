@@ -1,14 +1,17 @@
 """foam case input and output: the mesh and fields of an existing rhoDST case.
 
-`read_polymesh(dir)` reads an ASCII `constant/polyMesh` (points, faces,
-owner, neighbour, boundary) into a PolyMesh with the library's geometry
+`read_polymesh(dir)` reads a `constant/polyMesh` (points, faces, owner,
+neighbour, boundary) in foam's ascii or binary format, gzipped (`name.gz`)
+or not, faces as a faceList or a binary faceCompactList, into a PolyMesh with the library's geometry
 (face centres and area vectors, cell centres and volumes, weights, delta
 coefficients), keeping foam's face numbering: internal faces in upper
 triangular order, then the patches by startFace.  Faces of three or four
 vertices (the hex, prism and tet meshes this path runs); patch types
 patch, wall, symmetryPlane/symmetry and empty.
 
-`save_npz` / `load_npz` store the topology compactly (a mesh read once can
+`write_polymesh` writes a mesh back in either format (the meshes the
+library generates become foam cases); `save_npz` / `load_npz` store the
+topology compactly (a mesh read once can
 travel without the case directory).
 
 `read_field` reads an ASCII vol field (uniform or nonuniform internal
@@ -26,6 +29,7 @@ their own names; `case.notes` lists the entries this path does not take.
 """
 from __future__ import annotations
 
+import gzip
 import re
 from pathlib import Path
 from typing import List, Tuple
@@ -52,7 +56,7 @@ def _header(text: str) -> dict:
     m = re.search(r"FoamFile\s*\{(.*?)\}", text, flags=re.S)
     out = {}
     if m:
-        for k, v in re.findall(r"(\w+)\s+([^;]+);", m.group(1)):
+        for k, v in re.findall(r'(\w+)\s+("[^"]*"|[^;]+);', m.group(1)):   # arch is quoted and holds ';'
             out[k] = v.strip().strip('"')
     return out
 
@@ -68,16 +72,104 @@ def _list_body(text: str) -> Tuple[int, str]:
     return n, text[start:end]
 
 
-def _read(path: Path) -> Tuple[dict, str]:
-    raw = path.read_text()
-    hdr = _header(raw)
+def _load(path: Path) -> bytes:
+    """The file's bytes; `name.gz` (foam's writeCompression) when `name`
+    itself is absent, gzip content decompressed either way."""
+    path = Path(path)
+    if not path.exists() and path.with_name(path.name + ".gz").exists():
+        path = path.with_name(path.name + ".gz")
+    data = path.read_bytes()
+    if data[:2] == b"\x1f\x8b":
+        data = gzip.decompress(data)
+    return data
+
+
+class _Binary:
+    """Reader of foam's binary list files.  A binary file keeps the text
+    FoamFile header; each list is its count in text, then '(' and the raw
+    items, then ')' (foam writes no parentheses for an empty list).  The
+    header's arch entry gives the byte order and the label and scalar
+    widths ("LSB;label=32;scalar=64" when absent)."""
+
+    def __init__(self, path: Path, data: bytes, hdr: dict):
+        self.path, self.data = path, data
+        arch = hdr.get("arch", "")
+        order = ">" if "MSB" in arch else "<"
+        lw = re.search(r"label\s*=\s*(\d+)", arch)
+        sw = re.search(r"scalar\s*=\s*(\d+)", arch)
+        self.label = np.dtype(f"{order}i{int(lw.group(1)) // 8 if lw else 4}")
+        self.scalar = np.dtype(f"{order}f{int(sw.group(1)) // 8 if sw else 8}")
+        m = re.search(rb"FoamFile\s*\{.*?\}", data, flags=re.S)
+        self.pos = m.end() if m else 0
+
+    def _skip(self):
+        d, n = self.data, len(self.data)
+        while self.pos < n:
+            c = d[self.pos:self.pos + 1]
+            if c.isspace():
+                self.pos += 1
+            elif d.startswith(b"//", self.pos):
+                e = d.find(b"\n", self.pos)
+                self.pos = n if e < 0 else e + 1
+            elif d.startswith(b"/*", self.pos):
+                e = d.find(b"*/", self.pos + 2)
+                if e < 0:
+                    raise ValueError(f"{self.path}: unterminated comment")
+                self.pos = e + 2
+            else:
+                return
+
+    def count(self) -> int:
+        self._skip()
+        m = re.compile(rb"\d+").match(self.data, self.pos)
+        if not m:
+            raise ValueError(f"{self.path}: expected a list count at byte {self.pos}")
+        self.pos = m.end()
+        return int(m.group(0))
+
+    def _expect(self, ch: bytes):
+        if self.data[self.pos:self.pos + 1] != ch:
+            raise ValueError(f"{self.path}: expected {ch!r} at byte {self.pos}")
+        self.pos += 1
+
+    def items(self, n: int, dtype: np.dtype, per: int = 1) -> np.ndarray:
+        """The raw block of a list whose count n was just read (`per`
+        components an item: 3 for a vector)."""
+        self._skip()
+        if n == 0:
+            if self.data.startswith(b"()", self.pos):
+                self.pos += 2
+            return np.zeros(0, dtype=dtype.newbyteorder("="))
+        self._expect(b"(")
+        end = self.pos + n * per * dtype.itemsize
+        if end + 1 > len(self.data):
+            raise ValueError(f"{self.path}: list of {n} items runs past the end of the file")
+        out = np.frombuffer(self.data, dtype=dtype, count=n * per, offset=self.pos)
+        self.pos = end
+        self._expect(b")")
+        return out.astype(dtype.newbyteorder("="))
+
+    def list(self, dtype: np.dtype) -> np.ndarray:
+        return self.items(self.count(), dtype)
+
+
+def _open(path: Path):
+    """(header, text) of an ascii file or (header, _Binary) of a binary one."""
+    data = _load(path)
+    head = data[:4096].decode("latin-1")
+    hdr = _header(head)
+    if hdr.get("format", "ascii") == "binary":
+        return hdr, _Binary(path, data, hdr)
     if hdr.get("format", "ascii") != "ascii":
-        raise ValueError(f"{path}: only ascii polyMesh files are read")
-    return hdr, _strip(raw)
+        raise ValueError(f"{path}: format {hdr.get('format')} is neither ascii nor binary")
+    return hdr, _strip(data.decode("latin-1"))
 
 
 def read_points(path: Path) -> np.ndarray:
-    _, t = _read(path)
+    _, t = _open(path)
+    if isinstance(t, _Binary):
+        n = t.count()
+        return t.items(n, t.scalar, per=3).astype(np.float64).reshape(n, 3)
     n, body = _list_body(t)
     vals = np.array(re.findall(r"[-+0-9.eE]+", body), dtype=float)
     if vals.size != 3 * n:
@@ -86,7 +178,9 @@ def read_points(path: Path) -> np.ndarray:
 
 
 def read_labels(path: Path) -> np.ndarray:
-    _, t = _read(path)
+    _, t = _open(path)
+    if isinstance(t, _Binary):
+        return t.list(t.label).astype(np.int64)
     n, body = _list_body(t)
     vals = np.array(body.split(), dtype=np.int64)
     if vals.size != n:
@@ -94,9 +188,45 @@ def read_labels(path: Path) -> np.ndarray:
     return vals
 
 
+def _pad_faces(path, sizes: np.ndarray, flat: np.ndarray) -> np.ndarray:
+    """(F, 4) vertex table, -1 padded for triangles, from per-face sizes and
+    the faces' vertices back to back."""
+    bad = np.flatnonzero((sizes < 3) | (sizes > 4))
+    if bad.size:
+        raise ValueError(f"{path}: face {bad[0]} has {sizes[bad[0]]} vertices (3 or 4 are read)")
+    out = np.full((sizes.size, 4), -1, dtype=np.int64)
+    start = np.concatenate(([0], np.cumsum(sizes)[:-1]))
+    for k in range(4):
+        has = sizes > k
+        out[has, k] = flat[start[has] + k]
+    return out
+
+
 def read_faces(path: Path) -> np.ndarray:
-    """faceList 'k(v0 .. vk-1)' per face -> (F, 4), -1 padded for triangles."""
-    _, t = _read(path)
+    """faceList 'k(v0 .. vk-1)' per face, or a binary faceList or
+    faceCompactList (offsets, then the vertices back to back) -> (F, 4),
+    -1 padded for triangles."""
+    hdr, t = _open(path)
+    if isinstance(t, _Binary):
+        if hdr.get("class") == "faceCompactList":
+            offsets = t.list(t.label).astype(np.int64)
+            flat = t.list(t.label).astype(np.int64)
+            if offsets.size == 0 or offsets[0] != 0 or offsets[-1] != flat.size or np.any(np.diff(offsets) < 0):
+                raise ValueError(f"{path}: compact face offsets do not cover the vertex list")
+            return _pad_faces(path, np.diff(offsets), flat)
+        n = t.count()
+        t._skip()
+        t._expect(b"(")
+        sizes = np.zeros(n, dtype=np.int64)
+        parts = []
+        for i in range(n):
+            v = t.list(t.label)
+            sizes[i] = v.size
+            parts.append(v)
+        t._skip()
+        t._expect(b")")
+        flat = np.concatenate(parts).astype(np.int64) if parts else np.zeros(0, np.int64)
+        return _pad_faces(path, sizes, flat)
     n, body = _list_body(t)
     items = re.findall(r"(\d+)\s*\(([^)]*)\)", body)
     if len(items) != n:
@@ -111,8 +241,9 @@ def read_faces(path: Path) -> np.ndarray:
 
 
 def read_boundary(path: Path) -> List[Tuple[str, str, int, int]]:
-    """(name, type, startFace, nFaces) per patch, in file order."""
-    _, t = _read(path)
+    """(name, type, startFace, nFaces) per patch, in file order (the
+    boundary file is text in a binary case too)."""
+    t = _strip(_load(path).decode("latin-1"))
     n, body = _list_body(t)
     out = []
     for name, block in re.findall(r"(\w+)\s*\{(.*?)\}", body, flags=re.S):
@@ -156,6 +287,70 @@ def assemble(points, faces, owner, neighbour, bnd) -> _mesh.PolyMesh:
                        n_cells=int(owner.max()) + 1)
     _mesh.compute_geometry(m)
     return m
+
+
+def write_polymesh(directory, m: _mesh.PolyMesh, fmt: str = "ascii", compact: bool = False,
+                   compress: bool = False, label_bits: int = 32) -> None:
+    """Writes m as a foam `constant/polyMesh` (points, faces, owner,
+    neighbour, boundary) in foam's ascii or binary format: faces as a
+    faceList, or with `compact` (binary only) as a faceCompactList of
+    offsets and vertices back to back, the form foam's binary output uses;
+    `compress` writes each list file gzipped as `name.gz`, as foam does
+    under writeCompression.  The boundary file stays text."""
+    if fmt not in ("ascii", "binary"):
+        raise ValueError("fmt is ascii or binary")
+    if compact and fmt != "binary":
+        raise ValueError("faceCompactList is written in binary only")
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    lab = np.dtype(f"<i{label_bits // 8}")
+    arch = f"LSB;label={label_bits};scalar=64"
+
+    def head(cls, obj, binary):
+        return ("FoamFile\n{\n    version     2.0;\n    format      " + ("binary" if binary else "ascii") +
+                ";\n" + (f'    arch        "{arch}";\n' if binary else "") +
+                f"    class       {cls};\n    location    \"constant/polyMesh\";\n    object      {obj};\n}}\n\n")
+
+    def blist(values: np.ndarray) -> bytes:
+        n = values.shape[0]
+        if n == 0:
+            return b"\n0\n"
+        return f"\n{n}\n(".encode() + np.ascontiguousarray(values).tobytes() + b")"
+
+    def put(name, payload: bytes):
+        if compress:
+            (d / (name + ".gz")).write_bytes(gzip.compress(payload))
+        else:
+            (d / name).write_bytes(payload)
+
+    binary = fmt == "binary"
+    sizes = (m.faces >= 0).sum(axis=1)
+    if binary:
+        put("points", head("vectorField", "points", True).encode() +
+            blist(np.asarray(m.points, dtype="<f8").reshape(-1, 3)) + b"\n")
+        if compact:
+            offsets = np.concatenate(([0], np.cumsum(sizes))).astype(lab)
+            flat = m.faces[m.faces >= 0].astype(lab)
+            put("faces", head("faceCompactList", "faces", True).encode() + blist(offsets) + blist(flat) + b"\n")
+        else:
+            body = b"".join(blist(f[:k].astype(lab)) for f, k in zip(m.faces, sizes))
+            put("faces", head("faceList", "faces", True).encode() + f"\n{len(sizes)}\n(".encode() + body +
+                b"\n)\n")
+        put("owner", head("labelList", "owner", True).encode() + blist(m.owner.astype(lab)) + b"\n")
+        put("neighbour", head("labelList", "neighbour", True).encode() + blist(m.neighbour.astype(lab)) + b"\n")
+    else:
+        pts = "\n".join("(%.17g %.17g %.17g)" % tuple(p) for p in m.points)
+        put("points", (head("vectorField", "points", False) + f"{len(m.points)}\n(\n{pts}\n)\n").encode())
+        fcs = "\n".join(f"{k}(" + " ".join(str(int(v)) for v in f[:k]) + ")" for f, k in zip(m.faces, sizes))
+        put("faces", (head("faceList", "faces", False) + f"{len(sizes)}\n(\n{fcs}\n)\n").encode())
+        for name, arr in (("owner", m.owner), ("neighbour", m.neighbour)):
+            body = "\n".join(str(int(v)) for v in arr)
+            put(name, (head("labelList", name, False) + f"{len(arr)}\n(\n{body}\n)\n").encode())
+    names = {v: k for k, v in _PATCH_TYPES.items() if k != "symmetry"}
+    ents = "".join(f"    {p.name}\n    {{\n        type            {names[p.type]};\n"
+                   f"        nFaces          {p.size};\n        startFace       {p.start};\n    }}\n"
+                   for p in m.patches)
+    (d / "boundary").write_text(head("polyBoundaryMesh", "boundary", binary) + f"{len(m.patches)}\n(\n{ents})\n")
 
 
 def save_npz(m: _mesh.PolyMesh, path) -> None:

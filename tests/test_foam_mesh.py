@@ -248,3 +248,86 @@ def test_block_mesh_grading_and_merging():
     names = [(p.name, p.type, p.size) for p in m.patches]
     assert names == [("left", M.PATCH, 2), ("walls", M.WALL, 14), ("defaultFaces", M.EMPTY, 28 + 2)]
     assert np.isclose(m.V.sum(), 2.0)
+
+
+def _same_mesh(a, b):
+    assert np.array_equal(a.points, b.points) and np.array_equal(a.faces, b.faces)
+    assert np.array_equal(a.owner, b.owner) and np.array_equal(a.neighbour, b.neighbour)
+    assert [(p.name, p.type, p.start, p.size) for p in a.patches] == \
+           [(p.name, p.type, p.start, p.size) for p in b.patches]
+    assert np.array_equal(a.V, b.V) and np.array_equal(a.Sf, b.Sf)
+
+
+@pytest.mark.parametrize("fmt,compact,compress", [("ascii", False, False), ("binary", False, False),
+                                                   ("binary", True, False), ("binary", True, True),
+                                                   ("ascii", False, True)])
+def test_polymesh_round_trip(tmp_path, fmt, compact, compress):
+    """A hybrid tet/prism mesh (triangles and quads) written in each of
+    foam's forms and read back: topology, points and geometry bit for bit."""
+    m = M.forward_step_3d_hybrid(nx=12, ny=4, nz=3, jitter=0.25)
+    assert set((m.faces >= 0).sum(axis=1)) == {3, 4}
+    foam.write_polymesh(tmp_path, m, fmt=fmt, compact=compact, compress=compress)
+    if compress:
+        assert (tmp_path / "points.gz").exists() and not (tmp_path / "points").exists()
+    _same_mesh(foam.read_polymesh(tmp_path), m)
+
+
+def test_binary_rae2822_tutorial_mesh(tmp_path):
+    """The tutorial's mesh as a binary faceCompactList case reads back as
+    the stored ascii one."""
+    m = foam.load_npz(FIXTURE)
+    foam.write_polymesh(tmp_path, m, fmt="binary", compact=True)
+    assert b"faceCompactList" in (tmp_path / "faces").read_bytes()[:400]
+    _same_mesh(foam.read_polymesh(tmp_path), m)
+
+
+def _binary_file(path, cls, arch, payload: bytes):
+    path.write_bytes(("FoamFile\n{\n    version 2.0;\n    format binary;\n" +
+                      (f'    arch "{arch}";\n' if arch else "") +
+                      f"    class {cls};\n    object {path.name};\n}}\n// a comment\n/* and a block one */\n")
+                     .encode() + payload)
+
+
+def test_binary_arch_widths_and_byte_order(tmp_path):
+    """The header's arch names the byte order and the label and scalar widths."""
+    lab = np.array([3, 0, 7, 2**33], dtype=">i8")
+    _binary_file(tmp_path / "owner", "labelList", "MSB;label=64;scalar=64",
+                 b"\n4\n(" + lab.tobytes() + b")\n")
+    assert foam.read_labels(tmp_path / "owner").tolist() == [3, 0, 7, 2**33]
+    pts = np.array([[0.5, -1.25, 3.0], [1e-300, 2.0, -0.0]], dtype="<f4")
+    _binary_file(tmp_path / "points", "vectorField", "LSB;label=32;scalar=32",
+                 b"\n2\n(" + pts.tobytes() + b")\n")
+    assert np.array_equal(foam.read_points(tmp_path / "points"), pts.astype(np.float64))
+    # no arch entry: 32-bit little-endian labels
+    _binary_file(tmp_path / "neighbour", "labelList", None, b"\n3\n(" + np.array([1, 2, 5], "<i4").tobytes() + b")")
+    assert foam.read_labels(tmp_path / "neighbour").tolist() == [1, 2, 5]
+
+
+def test_binary_empty_lists(tmp_path):
+    """foam writes an empty binary list as its count alone; '0()' reads too."""
+    _binary_file(tmp_path / "a", "labelList", "LSB;label=32;scalar=64", b"\n0\n")
+    _binary_file(tmp_path / "b", "labelList", "LSB;label=32;scalar=64", b"\n0()\n")
+    assert foam.read_labels(tmp_path / "a").size == 0 and foam.read_labels(tmp_path / "b").size == 0
+
+
+def test_binary_malformed_files_are_rejected(tmp_path):
+    vals = np.arange(5, dtype="<i4")
+    _binary_file(tmp_path / "short", "labelList", "LSB;label=32;scalar=64", b"\n6\n(" + vals.tobytes() + b")")
+    with pytest.raises(ValueError, match="past the end"):
+        foam.read_labels(tmp_path / "short")
+    _binary_file(tmp_path / "noparen", "labelList", "LSB;label=32;scalar=64", b"\n5\n" + vals.tobytes())
+    with pytest.raises(ValueError, match="expected"):
+        foam.read_labels(tmp_path / "noparen")
+    # compact faces whose offsets do not reach the end of the vertex list
+    off = np.array([0, 3, 6], "<i4")
+    flat = np.arange(7, dtype="<i4")
+    _binary_file(tmp_path / "faces", "faceCompactList", "LSB;label=32;scalar=64",
+                 b"\n3\n(" + off.tobytes() + b")\n7\n(" + flat.tobytes() + b")")
+    with pytest.raises(ValueError, match="offsets"):
+        foam.read_faces(tmp_path / "faces")
+    # a pentagon is refused as in ascii
+    off = np.array([0, 5], "<i4")
+    _binary_file(tmp_path / "faces", "faceCompactList", "LSB;label=32;scalar=64",
+                 b"\n2\n(" + off.tobytes() + b")\n5\n(" + np.arange(5, dtype="<i4").tobytes() + b")")
+    with pytest.raises(ValueError, match="5 vertices"):
+        foam.read_faces(tmp_path / "faces")
