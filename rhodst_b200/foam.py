@@ -156,8 +156,8 @@ class _Binary:
 def _open(path: Path):
     """(header, text) of an ascii file or (header, _Binary) of a binary one."""
     data = _load(path)
-    head = data[:4096].decode("latin-1")
-    hdr = _header(head)
+    m = re.search(rb"FoamFile\s*\{.*?\}", data, flags=re.S)     # the header precedes any binary data
+    hdr = _header(m.group(0).decode("latin-1")) if m else {}
     if hdr.get("format", "ascii") == "binary":
         return hdr, _Binary(path, data, hdr)
     if hdr.get("format", "ascii") != "ascii":
