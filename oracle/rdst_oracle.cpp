@@ -205,6 +205,12 @@ struct Ctx {
     std::vector<std::array<double, 5>> Wn, Wnm1;
     bool dual_started = false;
     double dt_save = 1.0, dual_a = 0, dual_b = 0, dual_c = 0;
+    // SARC1 under dual-time stepping: S.oldTime() and its oldTime(), the
+    // time indices foam gives S and each of them (-1: not created), the
+    // physical step's index, deltaT and deltaT0
+    std::vector<std::array<double, 6>> S_o, S_oo;
+    int S_idx = -1, S_o_idx = -1, S_oo_idx = -1, dual_tidx = 0;
+    double dual_dt = 1.0, dual_dt0 = 1.0;
 };
 
 // ----------------------------------------------------------------------
@@ -1984,7 +1990,42 @@ void sa_correct(Ctx& c) {
             for (int a = 0; a < 3; ++a)
                 for (int q = a; q < 3; ++q) Sc[i][sym6(a, q)] = 0.5 * (g[3 * a + q] + g[3 * q + a]);
         }
-        if (!c.S_old_valid) c.S_old = Sc;
+        // under dual-time stepping, dual2ndDST::fvcDdt(rho, S)
+        // (dual2ndDST.C:231-372) with the physical step's old times
+        const bool dual_ddt = c.o.dual && c.dual_a != 0.0;
+        double d_c = 0, d_c0 = 0, d_c00 = 0;
+        if (dual_ddt) {
+            // Sxx_ = S.component(..) (SARC1.C:655-669) at a new time index
+            // stores the old times first (GeometricField::storeOldTimes):
+            // S.oo <- S.o, S.o <- S (the last update's S)
+            if (c.S_o_idx >= 0 && c.S_idx != c.dual_tidx) {
+                if (c.S_oo_idx >= 0) {
+                    c.S_oo = c.S_o;
+                    c.S_oo_idx = c.S_o_idx;
+                }
+                c.S_o = c.S_old;
+                c.S_o_idx = c.S_idx;
+            }
+            c.S_idx = c.dual_tidx;
+            // fvc::ddt creates S.oldTime() from S, and its oldTime() from
+            // that, at first use (with their time indices)
+            if (c.S_o_idx < 0) {
+                c.S_o = Sc;
+                c.S_o_idx = c.S_idx;
+            }
+            if (c.S_oo_idx < 0) {
+                c.S_oo = c.S_o;
+                c.S_oo_idx = c.S_o_idx;
+            }
+            // deltaT0_(vf) (dual2ndDST.C:76-90): GREAT while both old times
+            // carry one time index
+            const double dt = c.dual_dt, dt0 = (c.S_o_idx == c.S_oo_idx) ? 1.0e15 : c.dual_dt0;
+            d_c = 1 + dt / (dt + dt0);
+            d_c00 = dt * dt / (dt0 * (dt + dt0));
+            d_c0 = d_c + d_c00;
+        } else if (!c.S_old_valid) {
+            c.S_old = Sc;
+        }
         for (int i = 0; i < N; ++i) {
             double rdt = (c.o.ddt == DDT_EULER) ? 1.0 / c.deltaT : c.rDeltaT[i];
             std::array<double, 6> dv{};
@@ -1999,8 +2040,15 @@ void sa_correct(Ctx& c) {
                     for (int k = 0; k < 6; ++k) dv[k] += ph * Sc[i][k];
                 }
             }
-            for (int k = 0; k < 6; ++k)
-                DSDt[i][k] = rdt * (c.rho[i] * Sc[i][k] - c.rho0[i] * c.S_old[i][k]) + dv[k] / c.V[i];
+            if (dual_ddt) {
+                const double rdtp = 1.0 / c.dual_dt, ro = c.Wn[i][0], roo = c.Wnm1[i][0];
+                for (int k = 0; k < 6; ++k)
+                    DSDt[i][k] = rdtp * (d_c * c.rho[i] * Sc[i][k] - d_c0 * ro * c.S_o[i][k] +
+                                         d_c00 * roo * c.S_oo[i][k]) + dv[k] / c.V[i];
+            } else {
+                for (int k = 0; k < 6; ++k)
+                    DSDt[i][k] = rdt * (c.rho[i] * Sc[i][k] - c.rho0[i] * c.S_old[i][k]) + dv[k] / c.V[i];
+            }
         }
     }
     std::vector<double> mu(N), chi(N), fv1(N), D(N), diag(N), b(N, 0.0);
@@ -2259,12 +2307,16 @@ void dual_iterate(Ctx& c, Report& rep, double dt, double dt0) {
         c.nutN = c.nut;
         c.nutNm1 = c.nut;
         c.dual_started = true;
+        c.S_idx = c.S_o_idx = c.S_oo_idx = -1;   // SARC1's S history restarts too
     } else {
         c.Wnm1.swap(c.Wn);
         for (int i = 0; i < c.N; ++i) c.Wn[i] = {c.rho[i], c.rhoU[i][0], c.rhoU[i][1], c.rhoU[i][2], c.rhoE[i]};
         c.nutNm1.swap(c.nutN);
         c.nutN = c.nut;
     }
+    c.dual_dt = dt;
+    c.dual_dt0 = dt0;
+    ++c.dual_tidx;
     const bool turb = c.o.turbulence != TURB_LAMINAR;
     // dual2ndDST::fvmDdt coefficients (dual2ndDST.C:391-395)
     c.dual_a = 1.0 / dt + 1.0 / (dt + dt0);

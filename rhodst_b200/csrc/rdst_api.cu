@@ -315,6 +315,12 @@ struct rdst_ctx {
     DBuf<double> nutN, nutNm1;      // nuTilda old time levels of dual-time stepping
     bool dual_started = false;
     double dt_save = 1.0, dual_a = 0.0, dual_b = 0.0, dual_c = 0.0;
+    // SARC1 under dual-time stepping: S.oldTime() and its oldTime(), the
+    // time indices foam gives S and each of them (-1: not created), the
+    // physical step's index and its deltaT / deltaT0
+    DBuf<double> saSo, saSoo;
+    int sa_S_idx = -1, sa_o_idx = -1, sa_oo_idx = -1, dual_tidx = 0;
+    double dual_dt = 1.0, dual_dt0 = 1.0;
     DBuf<Scalars> a_sc;             // Hessenberg and rotations of the adjoint's outer solve
     void* a_AT = nullptr;           // transposed Jacobian (storage type of A)
     DBuf<double> t_buf;             // tangent records (value, derivative)
@@ -1619,6 +1625,39 @@ void sa_correct(rdst_ctx& c) {
         k_limit_gradU<<<nblk(c.N, 128), 128, 0, s>>>(m, c.o.grad_U_limit, c.prim.p, c.bs.p, c.gU.p); CKL();
     }
     const int sarc1 = c.o.turbulence == TURB_SARC1 ? 1 : (c.o.turbulence == TURB_SA ? 2 : 0);
+    F.S_o = nullptr;
+    if (sarc1 == 1 && c.o.dual && c.dual_a != 0.0) {
+        // Sxx_ = S.component(..) (SARC1.C:655-669) at a new time index stores
+        // the old times first (GeometricField::storeOldTimes): S_oo <- S_o,
+        // S_o <- S (the last update's S, in saSold)
+        const size_t n6 = 6 * (size_t)c.N * sizeof(double);
+        if (!c.saSo.p) { c.saSo.alloc(6L * c.N); c.saSoo.alloc(6L * c.N); }
+        if (c.sa_o_idx >= 0 && c.sa_S_idx != c.dual_tidx) {
+            if (c.sa_oo_idx >= 0) {
+                CK(cudaMemcpyAsync(c.saSoo.p, c.saSo.p, n6, cudaMemcpyDeviceToDevice, s));
+                c.sa_oo_idx = c.sa_o_idx;
+            }
+            CK(cudaMemcpyAsync(c.saSo.p, c.saSold.p, n6, cudaMemcpyDeviceToDevice, s));
+            c.sa_o_idx = c.sa_S_idx;
+        }
+        c.sa_S_idx = c.dual_tidx;
+        // fvc::ddt creates S.oldTime() from S and its oldTime() from that at first use
+        F.o_new = c.sa_o_idx < 0;
+        if (F.o_new) c.sa_o_idx = c.sa_S_idx;
+        F.oo_new = c.sa_oo_idx < 0;
+        if (F.oo_new) c.sa_oo_idx = c.sa_o_idx;
+        // dual2ndDST::fvcDdt(rho, vf) (dual2ndDST.C:231-372); deltaT0_(vf)
+        // (:76-90) is GREAT while both old times carry one time index
+        const double dt = c.dual_dt, dt0 = (c.sa_o_idx == c.sa_oo_idx) ? 1.0e15 : c.dual_dt0;
+        F.d_rdt = 1.0 / dt;
+        F.d_c = 1 + dt / (dt + dt0);
+        F.d_c00 = dt * dt / (dt0 * (dt + dt0));
+        F.d_c0 = F.d_c + F.d_c00;
+        F.S_o = c.saSo.p;
+        F.S_oo = c.saSoo.p;
+        F.W_o = c.dWn.p;
+        F.W_oo = c.dWnm1.p;
+    }
     k_sa_cell<<<nblk(c.N, 128), 128, 0, s>>>(m, c.tr, neg_sa, sarc1, (c.steady || c.o.dual) ? 1 : 0, c.W.p, c.prim.p,
                                             c.gU.p, c.rdt.p, c.sc.p, c.fl.p, c.bs.p, F); CKL();
     if (c.o.dual && c.dual_a != 0.0) {
@@ -1915,6 +1954,9 @@ void run_dual_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
             CK(cudaStreamSynchronize(s));
             const double dt0 = c.dt_save;
             c.dt_save = dt;
+            c.dual_dt = dt;
+            c.dual_dt0 = dt0;
+            ++c.dual_tidx;
             // old time levels (created from the current field at first use)
             if (!c.dual_started) {
                 CK(cudaMemcpyAsync(c.dWn.p, c.W.p, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -1923,6 +1965,7 @@ void run_dual_steps(rdst_ctx& c, int n, rdst_step_report* host_reps) {
                     CK(cudaMemcpyAsync(c.nutN.p, c.nut.p, c.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
                     CK(cudaMemcpyAsync(c.nutNm1.p, c.nut.p, c.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
                 }
+                c.sa_S_idx = c.sa_o_idx = c.sa_oo_idx = -1;   // SARC1's S history restarts too
                 c.dual_started = true;
             } else {
                 std::swap(c.dWn.p, c.dWnm1.p);

@@ -408,12 +408,10 @@ inline Options parse_options(int n, const char* const* keys, const char* const* 
     if (o.lim_U == LIM_VENKATAKRISHNAN) {}
     // dual-time stepping: the Dual iteration with the dual2ndDST ddt (the
     // pairing of the reference's dual-time tutorial), for the mean flow and
-    // the nuTilda equation of SAneg, SARC2 and SpalartAllmaras
+    // the nuTilda equation of every SA model (SARC1's strain-rate material
+    // derivative with dual2ndDST's second-order ddt over the physical steps)
     if (o.dual != (o.ddt == DDT_DUAL2ND))
         throw ConfigError("timeIntegration Dual is restated with ddtSchemes dual2ndDST (and dual2ndDST with Dual)", true);
-    if (o.dual && o.turbulence == TURB_SARC1)
-        throw ConfigError("dual-time stepping with SARC1 (the dual-time ddt of its strain-rate transport) "
-                          "is not on this path", true);
     if (o.iteration_start < 0) o.iteration_start = (o.ddt == DDT_STEADY) ? 500 : 10;
     if (o.max_inner_iter < 0) throw ConfigError("timeIntegration.maxInnerIter must be >= 0");
     return o;

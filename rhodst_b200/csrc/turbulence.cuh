@@ -46,6 +46,14 @@ struct SAFields {
     double* S_old;    // [6N] SARC1: strain rate of the last update (old time)
     double* rho0;     // [N]  SARC1: rho before the coupled update (rho.oldTime())
     int* S_old_valid; // [1]  SARC1: 0 until the first update after a new state
+    // SARC1 under dual-time stepping (S_o null: the single-step form):
+    // dual2ndDST::fvcDdt(rho, S) = d_rdt (d_c rho S - d_c0 rho_o S_o + d_c00 rho_oo S_oo)
+    double* S_o;        // [6N] S.oldTime(): S of the last update of the previous physical step
+    double* S_oo;       // [6N] S.oldTime().oldTime()
+    const double* W_o;  // [5N] W of the previous physical step (rho.oldTime() = W_o[5i])
+    const double* W_oo; // [5N] W two physical steps back
+    double d_rdt, d_c, d_c0, d_c00;
+    int o_new, oo_new;  // S_o (S_oo) created in this update as a copy of S (of S_o)
 };
 
 // symmetric-tensor slot of (a, q): xx xy xz yy yz zz
@@ -178,11 +186,27 @@ __global__ void k_sa_cell(DevMesh m, Transport tr, int neg_sa, int sarc1, int st
             // DS/Dt = ddt(rho, S) + div(phi, S): the flow's ddt scheme with
             // the last update's S as old time (the current S at the first
             // update), Gauss upwind on the step's mass flux, zeroGradient S_b
-            double Si[6], So[6], dv[6] = {0, 0, 0, 0, 0, 0};
+            double Si[6], So[6], Soo[6], dv[6] = {0, 0, 0, 0, 0, 0};
             strain6(g, Si);
-            const int valid = *F.S_old_valid;
+            if (F.S_o) {
+                // dual-time: the old times of the physical step, created
+                // from the current S (S_o) and from S_o (S_oo) at first use
 #pragma unroll
-            for (int k = 0; k < 6; ++k) So[k] = valid ? F.S_old[6 * i + k] : Si[k];
+                for (int k = 0; k < 6; ++k) {
+                    So[k] = F.o_new ? Si[k] : F.S_o[6 * i + k];
+                    Soo[k] = F.oo_new ? So[k] : F.S_oo[6 * i + k];
+                }
+                if (F.o_new)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) F.S_o[6 * i + k] = So[k];
+                if (F.oo_new)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) F.S_oo[6 * i + k] = Soo[k];
+            } else {
+                const int valid = *F.S_old_valid;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) So[k] = valid ? F.S_old[6 * i + k] : Si[k];
+            }
             for (int kk = m.cf_start[i]; kk < m.cf_start[i + 1]; ++kk) {
                 const int code = m.cf_list[kk];
                 if (code < m.Fi) {
@@ -199,10 +223,17 @@ __global__ void k_sa_cell(DevMesh m, Transport tr, int neg_sa, int sarc1, int st
                     for (int k = 0; k < 6; ++k) dv[k] += ph * Si[k];
                 }
             }
-            const double rdt0 = steady ? rdtc[i] : 1.0 / sc->deltaT;
             double DS[6];
+            if (F.S_o) {
+                const double ro = F.W_o[5 * i], roo = F.W_oo[5 * i];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) DS[k] = rdt0 * (rho * Si[k] - F.rho0[i] * So[k]) + dv[k] / V;
+                for (int k = 0; k < 6; ++k)
+                    DS[k] = F.d_rdt * (F.d_c * rho * Si[k] - F.d_c0 * ro * So[k] + F.d_c00 * roo * Soo[k]) + dv[k] / V;
+            } else {
+                const double rdt0 = steady ? rdtc[i] : 1.0 / sc->deltaT;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) DS[k] = rdt0 * (rho * Si[k] - F.rho0[i] * So[k]) + dv[k] / V;
+            }
             // rTilda = 2/(rho max(D^2, SMALL)^2) sum_aq (sum_k W_ak S_qk) DS_aq/Dt
             const double sqrD = 0.5 * (sqrS + sqrW);
             double acc = 0;

@@ -12,10 +12,15 @@ steadyCheck.C:69-98).
 (3) The physical time step comes from initialCo at initialisation
     (timeDST::initialize calls setTransientDeltaT unconditionally) and stays
     with adjustTimeStep false.
-(4) Dual needs dual2ndDST and the reverse; SARC1 is rejected.
+(4) Dual needs dual2ndDST and the reverse.
 (5) With Spalart-Allmaras the nuTilda equation takes its own dual2ndDST ddt:
     a steady state is a fixed point of dual steps (either placement of the
     turbulence update), a disturbed nuTilda moves.
+(6) SARC1's material derivative of the strain rate takes dual2ndDST's
+    fvcDdt(rho, S) over the physical steps (dual2ndDST.C:231-372): its
+    coefficients sum to zero (coefft0 = coefft + coefft00), so a steady
+    SARC1 state stays a fixed point over the steps where the old times are
+    copies (deltaT0 GREAT) and the step where they are distinct.
 """
 import numpy as np
 import pytest
@@ -105,17 +110,10 @@ def test_dual_needs_dual2nd(opts):
         OracleSolver(c.mesh, c.bcs, c.options)
 
 
-def test_dual_with_sarc1_is_rejected():
-    c = cases.naca0012_turbulent(ni=97, nj=25, first_cell=5e-3, model="SARC1").with_options(**{
-        "timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST"})
-    with pytest.raises(RdstError):
-        OracleSolver(c.mesh, c.bcs, c.options)
-
-
-def sa_steady():
+def sa_steady(model="SAneg"):
     """A converged first-order SA airfoil state (p, U, T, nuTilda)."""
-    c = cases.naca0012_turbulent(ni=65, nj=17, first_cell=1e-2, reynolds=1e5, flux="HLL",
-                                 limiter="upwind").with_options(**{"timeControls.maxCo": 500.0})
+    c = cases.naca0012_turbulent(ni=65, nj=17, first_cell=1e-2, reynolds=1e5, flux="HLL", limiter="upwind",
+                                 model=model).with_options(**{"timeControls.maxCo": 500.0})
     o = OracleSolver(c.mesh, c.bcs, c.options)
     o.set_primitive(c.p, c.U, c.T, c.nuTilda)
     r0 = None
@@ -175,3 +173,42 @@ def test_adapter_selector_name_selects_dual_time():
         o.set_primitive(c.p, c.U, c.T)
     x, y = ra.step(1)[0], rb.step(1)[0]
     assert x["lin_iterations"] == y["lin_iterations"] == 4 and x["res_mag"] == y["res_mag"]
+
+
+@pytest.mark.parametrize("inner", [False, True])
+def test_dual_sarc1_keeps_a_steady_state(inner):
+    """SARC1 under dual-time stepping: the ddt(rho, S) of its strain-rate
+    material derivative vanishes on a steady state at every step: the first
+    two, where S.oldTime() and its oldTime() carry one time index (deltaT0
+    GREAT, the Euler-like coefficients), and the third, the full BDF2 form."""
+    c, prim = sa_steady("SARC1")
+    d = c.with_options(**{"timeIntegration.timeIntegration": "Dual", "ddtSchemes.default": "dual2ndDST",
+                          "timeControls.adjustTimeStep": False, "controlDict.deltaT": 0.05,
+                          "timeIntegration.innerCorrectTurbulence": inner, "timeControls.maxCo": 50.0})
+    o = OracleSolver(d.mesh, d.bcs, d.options)
+    o.set_primitive(*prim)
+    o.step(3)
+    for a, b in zip(o.primitive(), prim):
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+
+
+def test_dual_sarc1_differs_from_the_model_without_the_multiplier():
+    """From a disturbed nuTilda, SARC1's dual steps move nuTilda, finite, and
+    away from those of SpalartAllmaras (the same equations without the
+    rotation/curvature multiplier)."""
+    c, prim = sa_steady("SARC1")
+    nut = prim[3] * (1.0 + 0.5 * np.sin(2.0 * c.mesh.C[:, 0]) ** 2)
+    out = {}
+    for model in ("SARC1", "SpalartAllmaras"):
+        d = cases.naca0012_turbulent(ni=65, nj=17, first_cell=1e-2, reynolds=1e5, flux="HLL", limiter="upwind",
+                                     model=model).with_options(**{
+            "timeControls.maxCo": 50.0, "timeIntegration.timeIntegration": "Dual",
+            "ddtSchemes.default": "dual2ndDST", "timeControls.adjustTimeStep": False, "controlDict.deltaT": 0.05,
+            "timeIntegration.maxInnerIter": 6})
+        o = OracleSolver(d.mesh, d.bcs, d.options)
+        o.set_primitive(prim[0], prim[1], prim[2], nut)
+        o.step(3)
+        out[model] = o.primitive()[3]
+    n = out["SARC1"]
+    assert np.all(np.isfinite(n)) and np.abs(n - nut).max() > 1e-6 * np.abs(nut).max()
+    assert np.abs(n - out["SpalartAllmaras"]).max() > 1e-8 * np.abs(n).max()
