@@ -14,10 +14,11 @@ library generates become foam cases); `save_npz` / `load_npz` store the
 topology compactly (a mesh read once can
 travel without the case directory).
 
-`read_field` reads an ASCII vol field (uniform or nonuniform internal
-field, per-patch entries, '#include' and '$' macros as the tutorials use
-them); `write_state` / `read_state` write and read p, U, T and nuTilda as a
-time directory a foam case restarts from.
+`read_field` reads a vol field, ascii or binary (uniform or nonuniform
+internal field, per-patch entries, '#include' and '$' macros as the
+tutorials use them); `write_state` / `read_state` write (in either format)
+and read p, U, T and nuTilda as a time directory a foam case restarts
+from.
 
 `block_mesh(dict)` builds the meshes tutorials define by blockMeshDict
 (hex blocks, simpleGrading, straight edges).
@@ -377,18 +378,52 @@ def load_npz(path) -> _mesh.PolyMesh:
 # '#include' files and '$name' substitutions resolved the way the tutorials
 # use them; write the state as fields a foam case restarts from.
 
-def _resolve(path: Path, chain=()) -> str:
+_LIST_WIDTH = {"scalar": 1, "vector": 3, "symmTensor": 6, "tensor": 9}
+
+
+def _binary_lists(path: Path, blocks: list) -> str:
+    """The file as text.  In a binary file each 'nonuniform List<T> n (raw)'
+    is replaced by a placeholder '@@BINk@@' whose values go to blocks[k]
+    (the raw items can hold any byte, so the text parser never sees them);
+    the header's arch gives the scalar width and byte order."""
+    data = _load(path)
+    m = re.search(rb"FoamFile\s*\{.*?\}", data, flags=re.S)
+    hdr = _header(m.group(0).decode("latin-1")) if m else {}
+    if hdr.get("format", "ascii") != "binary":
+        return data.decode("latin-1")
+    b = _Binary(path, data, hdr)
+    pat = re.compile(rb"nonuniform\s+List<(\w+)>\s*(\d+)")
+    out, pos = [], 0
+    while True:
+        m = pat.search(data, pos)
+        if not m:
+            break
+        kind = m.group(1).decode()
+        if kind not in _LIST_WIDTH:
+            raise ValueError(f"{path}: List<{kind}> is not read")
+        n, per = int(m.group(2)), _LIST_WIDTH[kind]
+        b.pos = m.end()
+        vals = b.items(n, b.scalar, per=per).astype(np.float64)
+        blocks.append(vals.reshape(n, per) if per > 1 else vals)
+        out.append(data[pos:m.start()].decode("latin-1") + f"@@BIN{len(blocks) - 1}@@")
+        pos = b.pos
+    out.append(data[pos:].decode("latin-1"))
+    return "".join(out)
+
+
+def _resolve(path: Path, chain=(), blocks=None) -> str:
     """File text with '#include "f"' replaced by the included text
-    (relative to the including file) and comments removed."""
+    (relative to the including file) and comments removed; binary lists
+    of a binary file go to `blocks` (placeholders in the text)."""
     path = Path(path)
     if path in chain:
         raise ValueError(f"#include loop at {path}")
-    text = path.read_text()
+    text = _binary_lists(path, [] if blocks is None else blocks)
     text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
     text = re.sub(r"//[^\n]*", " ", text)
 
     def inc(m):
-        return _resolve(path.parent / m.group(1), chain + (path,))
+        return _resolve(path.parent / m.group(1), chain + (path,), blocks)
     return re.sub(r'#include\s+"([^"]+)"', inc, text)
 
 
@@ -406,15 +441,18 @@ def _top_entries(text: str) -> dict:
     return out
 
 
-def _value(s: str, macros: dict):
+def _value(s: str, macros: dict, blocks=()):
     """'uniform x' | 'uniform (a b c)' | 'nonuniform List<...> n (...)' |
-    '$name' -> float, tuple or array."""
+    '$name' | a binary list's placeholder -> float, tuple or array."""
     s = s.strip()
     for _ in range(8):
         m = re.search(r"\$(\w+)", s)
         if not m:
             break
         s = s[:m.start()] + macros[m.group(1)] + s[m.end():]
+    m = re.fullmatch(r"@@BIN(\d+)@@", s)
+    if m:
+        return blocks[int(m.group(1))]
     if s.startswith("uniform"):
         s = s[len("uniform"):].strip()
     if s.startswith("nonuniform"):
@@ -432,12 +470,13 @@ def _value(s: str, macros: dict):
 def read_field(path):
     """(internal, boundary): the internal field (float, 3-tuple or array)
     and per patch a dict of its entries (type, value, ... as parsed)."""
-    text = _resolve(Path(path))
+    blocks = []
+    text = _resolve(Path(path), blocks=blocks)
     hdr = re.search(r"FoamFile\s*\{.*?\}", text, flags=re.S)
     body = text[hdr.end():] if hdr else text
     macros = {k: v for k, v in _top_entries(body).items()}
     m = re.search(r"internalField\s+(.*?);\s*\n", body, flags=re.S)
-    internal = _value(m.group(1), macros)
+    internal = _value(m.group(1), macros, blocks)
     bm = re.search(r"boundaryField\s*\{(.*)\}", body, flags=re.S)
     boundary = {}
     if bm:
@@ -445,7 +484,7 @@ def read_field(path):
             entries = {k: v.strip() for k, v in re.findall(r"(\w+)\s+([^;]+);", block)}
             for k in ("value", "inletValue", "freestreamValue"):
                 if k in entries:
-                    entries[k] = _value(entries[k], macros)
+                    entries[k] = _value(entries[k], macros, blocks)
             boundary[name] = entries
     return internal, boundary
 
@@ -460,16 +499,36 @@ def _fmt_list(values: np.ndarray) -> str:
     return f"nonuniform List<{kind}> {values.shape[0]}\n(\n{rows}\n)"
 
 
-def write_field(path, name: str, values, mesh: _mesh.PolyMesh, boundary_values=None, dimensions="[0 0 0 0 0 0 0]"):
-    """An ASCII vol field with the cell values and, per non-empty patch,
-    'calculated' boundary values (boundary_values[patch] arrays, or the
-    adjacent cells' values)."""
+def _fmt_list_binary(values: np.ndarray) -> bytes:
+    kind = "scalar" if values.ndim == 1 else "vector"
+    n = values.shape[0]
+    head = f"nonuniform List<{kind}> {n}\n".encode()
+    return head + (b"(" + np.ascontiguousarray(values, dtype="<f8").tobytes() + b")" if n else b"")
+
+
+def write_field(path, name: str, values, mesh: _mesh.PolyMesh, boundary_values=None, dimensions="[0 0 0 0 0 0 0]",
+                fmt: str = "ascii"):
+    """A vol field in foam's ascii or binary format with the cell values
+    and, per non-empty patch, 'calculated' boundary values
+    (boundary_values[patch] arrays, or the adjacent cells' values)."""
+    if fmt not in ("ascii", "binary"):
+        raise ValueError("fmt is ascii or binary")
+    binary = fmt == "binary"
+    lists: List[bytes] = []
+
+    def fmt_list(v):
+        if not binary:
+            return _fmt_list(v)
+        lists.append(_fmt_list_binary(v))
+        return f"@@BIN{len(lists) - 1}@@"
+
     values = np.asarray(values, dtype=float)
     cls = "volScalarField" if values.ndim == 1 else "volVectorField"
     own = np.asarray(mesh.owner)
-    lines = ["FoamFile", "{", "    version     2.0;", "    format      ascii;", f"    class       {cls};",
+    lines = ["FoamFile", "{", "    version     2.0;", f"    format      {fmt};",
+             *(['    arch        "LSB;label=32;scalar=64";'] if binary else []), f"    class       {cls};",
              f"    object      {name};", "}", "", f"dimensions      {dimensions};", "",
-             f"internalField   {_fmt_list(values)};", "", "boundaryField", "{"]
+             f"internalField   {fmt_list(values)};", "", "boundaryField", "{"]
     for p in mesh.patches:
         lines.append(f"    {p.name}")
         lines.append("    {")
@@ -480,21 +539,25 @@ def write_field(path, name: str, values, mesh: _mesh.PolyMesh, boundary_values=N
             if bv is None:
                 bv = values[own[p.start:p.start + p.size]]
             lines.append("        type            calculated;")
-            lines.append(f"        value           {_fmt_list(np.asarray(bv, dtype=float))};")
+            lines.append(f"        value           {fmt_list(np.asarray(bv, dtype=float))};")
         lines.append("    }")
     lines += ["}", ""]
-    Path(path).write_text("\n".join(lines))
+    text = "\n".join(lines).encode()
+    for k, raw in enumerate(lists):
+        text = text.replace(f"@@BIN{k}@@".encode(), raw, 1)
+    Path(path).write_bytes(text)
 
 
-def write_state(directory, mesh: _mesh.PolyMesh, p, U, T, nuTilda=None):
-    """p, U, T (and nuTilda) of a solver state as a foam time directory."""
+def write_state(directory, mesh: _mesh.PolyMesh, p, U, T, nuTilda=None, fmt: str = "ascii"):
+    """p, U, T (and nuTilda) of a solver state as a foam time directory,
+    in foam's ascii or binary format."""
     d = Path(directory)
     d.mkdir(parents=True, exist_ok=True)
-    write_field(d / "p", "p", p, mesh, dimensions="[1 -1 -2 0 0 0 0]")
-    write_field(d / "U", "U", U, mesh, dimensions="[0 1 -1 0 0 0 0]")
-    write_field(d / "T", "T", T, mesh, dimensions="[0 0 0 1 0 0 0]")
+    write_field(d / "p", "p", p, mesh, dimensions="[1 -1 -2 0 0 0 0]", fmt=fmt)
+    write_field(d / "U", "U", U, mesh, dimensions="[0 1 -1 0 0 0 0]", fmt=fmt)
+    write_field(d / "T", "T", T, mesh, dimensions="[0 0 0 1 0 0 0]", fmt=fmt)
     if nuTilda is not None:
-        write_field(d / "nuTilda", "nuTilda", nuTilda, mesh, dimensions="[0 2 -1 0 0 0 0]")
+        write_field(d / "nuTilda", "nuTilda", nuTilda, mesh, dimensions="[0 2 -1 0 0 0 0]", fmt=fmt)
 
 
 def read_state(directory, mesh: _mesh.PolyMesh):
@@ -504,7 +567,7 @@ def read_state(directory, mesh: _mesh.PolyMesh):
     N = mesh.n_cells
 
     def cells(name, vec):
-        if not (d / name).exists():
+        if not (d / name).exists() and not (d / (name + ".gz")).exists():
             return None
         v, _ = read_field(d / name)
         if isinstance(v, np.ndarray):

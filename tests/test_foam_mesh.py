@@ -331,3 +331,53 @@ def test_binary_malformed_files_are_rejected(tmp_path):
                  b"\n2\n(" + off.tobytes() + b")\n5\n(" + np.arange(5, dtype="<i4").tobytes() + b")")
     with pytest.raises(ValueError, match="5 vertices"):
         foam.read_faces(tmp_path / "faces")
+
+
+def test_binary_state_round_trip(tmp_path):
+    """p, U, T, nuTilda written as binary foam fields (internal and patch
+    value lists raw) read back bit for bit, gzipped files too, with the
+    patch entries parsed around the raw blocks."""
+    m = M.forward_step_3d_hybrid(nx=12, ny=4, nz=3, jitter=0.25)
+    rng = np.random.default_rng(7)
+    N = m.n_cells
+    # values whose bytes include ';', '{', '}' and ')' exercise the raw blocks
+    p = rng.uniform(0.5, 2.0, N)
+    p[:4] = np.frombuffer(b";;;;;;;;{{{{}}}}))))))((((((;{}(" , dtype="<f8")
+    U = rng.normal(size=(N, 3))
+    T = rng.uniform(0.8, 1.2, N)
+    nut = rng.uniform(0, 1e-3, N)
+    foam.write_state(tmp_path / "1", m, p, U, T, nut, fmt="binary")
+    assert b"format      binary" in (tmp_path / "1" / "p").read_bytes()[:300]
+    p2, U2, T2, n2 = foam.read_state(tmp_path / "1", m)
+    assert np.array_equal(p, p2, equal_nan=True) and np.array_equal(U, U2)
+    assert np.array_equal(T, T2) and np.array_equal(nut, n2)
+    _, bnd = foam.read_field(tmp_path / "1" / "U")
+    for patch in m.patches:
+        e = bnd[patch.name]
+        if patch.type == M.EMPTY:
+            assert e["type"] == "empty"
+        else:
+            assert e["type"] == "calculated"
+            assert np.array_equal(e["value"], U[m.owner[patch.start:patch.start + patch.size]])
+    # gzipped, as foam writes under writeCompression
+    import gzip
+    for name in ("p", "U", "T", "nuTilda"):
+        f = tmp_path / "1" / name
+        (tmp_path / "1" / (name + ".gz")).write_bytes(gzip.compress(f.read_bytes()))
+        f.unlink()
+    p3, U3, _, _ = foam.read_state(tmp_path / "1", m)
+    assert np.array_equal(p, p3, equal_nan=True) and np.array_equal(U, U3)
+
+
+def test_binary_field_with_an_empty_patch_list(tmp_path):
+    """foam writes an empty binary list as its count alone."""
+    vals = np.array([1.5, -2.0, 3.25])
+    body = (b"FoamFile\n{\n    version 2.0;\n    format binary;\n    arch \"LSB;label=32;scalar=64\";\n"
+            b"    class volScalarField;\n    object p;\n}\ndimensions [1 -1 -2 0 0 0 0];\n\n"
+            b"internalField   nonuniform List<scalar> 3\n(" + vals.astype("<f8").tobytes() + b");\n\n"
+            b"boundaryField\n{\n    a\n    {\n        type calculated;\n        value nonuniform List<scalar> 0\n;\n"
+            b"    }\n    b\n    {\n        type fixedValue;\n        value uniform 2;\n    }\n}\n")
+    (tmp_path / "p").write_bytes(body)
+    internal, bnd = foam.read_field(tmp_path / "p")
+    assert np.array_equal(internal, vals)
+    assert bnd["a"]["value"].size == 0 and bnd["b"]["value"] == 2.0
