@@ -22,6 +22,8 @@ steadyCheck.C:69-98).
     SARC1 state stays a fixed point over the steps where the old times are
     copies (deltaT0 GREAT) and the step where they are distinct.
 """
+import functools
+
 import numpy as np
 import pytest
 
@@ -111,7 +113,14 @@ def test_dual_needs_dual2nd(opts):
 
 
 def sa_steady(model="SAneg"):
-    """A converged first-order SA airfoil state (p, U, T, nuTilda)."""
+    """A converged first-order SA airfoil state (p, U, T, nuTilda), each
+    converged once per model and copied for every test."""
+    c, prim = _sa_steady(model)
+    return c, tuple(np.array(a) for a in prim)
+
+
+@functools.lru_cache(maxsize=None)
+def _sa_steady(model):
     c = cases.naca0012_turbulent(ni=65, nj=17, first_cell=1e-2, reynolds=1e5, flux="HLL", limiter="upwind",
                                  model=model).with_options(**{"timeControls.maxCo": 500.0})
     o = OracleSolver(c.mesh, c.bcs, c.options)
