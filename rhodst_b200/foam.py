@@ -675,7 +675,7 @@ def read_case(directory, time: str = "0"):
     from .cases import Case, _vector_limiter  # noqa: F401  (Case type)
     d = Path(directory)
     poly = d / "constant" / "polyMesh"
-    if (poly / "points").exists():
+    if (poly / "points").exists() or (poly / "points.gz").exists():
         m = read_polymesh(poly)
     elif (poly / "blockMeshDict").exists():
         m = block_mesh(read_dict(poly / "blockMeshDict"))

@@ -381,3 +381,20 @@ def test_binary_field_with_an_empty_patch_list(tmp_path):
     internal, bnd = foam.read_field(tmp_path / "p")
     assert np.array_equal(internal, vals)
     assert bnd["a"]["value"].size == 0 and bnd["b"]["value"] == 2.0
+
+
+@pytest.mark.skipif(not CASE.exists(), reason="RHODST_REFERENCE does not name a reference tree")
+def test_case_reader_on_a_binary_copy_of_the_tutorial(tmp_path):
+    """The tutorial case with its polyMesh rewritten in foam's binary,
+    compact and gzipped form reads as the ascii case does."""
+    import shutil
+    d = tmp_path / "RAE2822"
+    shutil.copytree(CASE, d, ignore=shutil.ignore_patterns("sets", "*Zones"))
+    m = foam.read_polymesh(d / "constant/polyMesh")
+    for f in ("points", "faces", "owner", "neighbour", "boundary"):
+        (d / "constant/polyMesh" / f).unlink()
+    foam.write_polymesh(d / "constant/polyMesh", m, fmt="binary", compact=True, compress=True)
+    a, b = foam.read_case(CASE), foam.read_case(d)
+    _same_mesh(a.mesh, b.mesh)
+    assert a.bcs == b.bcs and a.options == b.options
+    assert np.array_equal(a.p, b.p) and np.array_equal(a.U, b.U) and np.array_equal(a.nuTilda, b.nuTilda)
